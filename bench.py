@@ -1,0 +1,406 @@
+#!/usr/bin/env python3
+"""Benchmark of the fermion-solve hot path on B200.
+
+Workload (one step = one full solve from a zero initial guess):
+  Shamir domain-wall fermions, 16^3 x 32 lattice, Ls = 16, M5 = 1.8,
+  m_f = 0.01, periodic in space and antiperiodic in time; seeded SU(3) links
+  U = exp(i 0.3 H); source = MatPcDag of a wall source built from a seeded
+  Gaussian 4D field (upper chirality on s = 0, lower on s = Ls-1, the
+  Ffour2five placement); CG on MatPcDagMatPc to a true residual of 1e-10.
+
+Metric: time to a true residual of 1e-10 (seconds, lower is better) of the
+mixed-precision CG (FP64 reliable updates and solution, FP16-storage inner
+iteration), reported next to the plain FP64 CG of this library on the same
+system, the dslash HBM bandwidth against the measured peak, the end-to-end
+time through the host-pointer C ABI, and the reference's CPU code timed on a
+bounded sample on this host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (under torchrun) every rank solves its own copy of the system on
+its own GPU (one solve does not shard without a halo exchange); the reported
+time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time to true residual 1e-10, mixed/batched vs FP64 CG on B200; dslash HBM GB/s"
+L4 = (16, 16, 16, 32)
+LS = 16
+M5 = 1.8
+MF = 0.01
+SEED = 20261203
+STOP = 1e-10
+# Iterations of the plain FP64 CG to a true residual of 1e-10 on this
+# workload, as measured by this library's FP64 CG (it runs the reference's
+# InvCgShift algorithm).  Only the reference arm uses it, to turn its
+# per-iteration CPU time into a time to solution without running the
+# multi-hour CPU solve.
+FP64_CG_ITERS = 1000
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+
+        def rd():
+            for line in self.proc.stdout:
+                self.samples.append([x.strip() for x in line.split(",")])
+
+        self.thread = threading.Thread(target=rd, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for k, n in enumerate(names):
+                    if s[3 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def wall_source(L, ls, eta4d):
+    """Ffour2five placement on the odd preconditioned checkerboard: slice 0
+    holds the upper chirality of eta on the odd sites, slice Ls-1 the lower
+    chirality on the 4D parity (Ls-1+1)%2 sites (f_dwf_base.C:961)."""
+    vol = int(np.prod(L))
+    vh = vol // 2
+    src = np.zeros((ls, vh, 24))
+    # eta4d: [parity][vh][24] in checkerboard order
+    par0 = 1  # slice 0 on parity (0 + 1) % 2
+    parl = (ls - 1 + 1) % 2
+    src[0, :, :12] = eta4d[par0, :, :12]
+    src[ls - 1, :, 12:] = eta4d[parl, :, 12:]
+    return src.reshape(-1)
+
+
+def setup_system(device: int):
+    from cps_veloc_b200 import _abi as A
+    from cps_veloc_b200.dirac import DiracOpDwf, Lattice, gen_gauge, gen_gaussian
+
+    A.check(A.lib().cpsgpu_set_device(device))
+    u = gen_gauge(L4, seed=SEED, width=0.3)
+    lat = Lattice(L4, (1, 1, 1, -1))
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=MF, ls=LS, m5=M5)
+    vol = int(np.prod(L4))
+    eta = gen_gaussian(vol * 24, seed=SEED, stream=1).reshape(2, vol // 2, 24)
+    b = D.MatPcDag(wall_source(L4, LS, eta))
+    return A, lat, D, u, b
+
+
+def field(A, D, prec, host=None):
+    h = C.c_void_p()
+    A.check(A.lib().cpsgpu_field_create(D._h, prec, 1, C.byref(h)))
+    if host is not None:
+        A.check(A.lib().cpsgpu_field_upload(h, A.dptr(np.ascontiguousarray(host))))
+    return h
+
+
+def solve_dev(A, D, x, bf, zero, prec, delta=0.1):
+    a = A.CgArg()
+    A.lib().cpsgpu_cg_arg_default(C.byref(a))
+    a.stop_rsd = STOP
+    a.max_num_iter = 100000
+    a.precision = prec
+    a.delta = delta
+    a.chunk = 16
+    r = A.CgResult()
+    A.check(A.lib().cpsgpu_field_upload(x, A.dptr(zero)))
+    A.check(A.lib().cpsgpu_invcg_field(D._h, x, bf, C.byref(a), C.byref(r)))
+    if r.status != A.CONVERGED:
+        raise RuntimeError(f"solve did not converge: status {r.status}, true_res {r.true_res}")
+    return r
+
+
+def cpu_reference_sample(u, iters: int, reps: int = 1) -> dict:
+    """The reference's own DWF dslash (oracle/_ref, compiled from the
+    reference sources) timed on this host: time-to-solution extrapolated as
+    4 dslash per CG iteration x iterations."""
+    from oracle.loader import REF_SO, apply_bc_signs, load_reference, p
+
+    if not REF_SO.exists():
+        return cpu_port_sample(u, iters, reps)
+    nthreads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    R = load_reference()
+    R.ref_init(*L4, LS, M5, 1.5, 0.5, -1)
+    us = apply_bc_signs(u, L4, (1, 1, 1, -1))
+    n = 24 * LS * int(np.prod(L4)) // 2
+    x = np.random.default_rng(1).normal(size=n)
+    y = np.zeros(n)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        R.ref_dwf_dslash(p(y), p(us), p(x), MF, 1, 0)
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    per_iter = 4 * t
+    return {"value": per_iter * iters, "unit": "s", "cores": nthreads, "kind": "reference",
+            "sample": f"{reps} x dwf_dslash (reference noarch, 16^3x32x16) = {t:.3f} s each; "
+                      f"x4 per CG iteration x {iters} iterations (wilson_dslash itself is single-threaded)",
+            "s_per_iteration": per_iter}
+
+
+def cpu_port_sample(u, iters: int, reps: int = 1) -> dict:
+    import ctypes
+
+    from oracle.loader import OracleGeom, load_oracle, p
+
+    O = load_oracle()
+    g = OracleGeom.make(L4, LS, (1, 1, 1, -1))
+    n = 24 * LS * int(np.prod(L4)) // 2
+    x = np.random.default_rng(1).normal(size=n)
+    y = np.zeros(n)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.orc_dwf_dslash(ctypes.byref(g), p(y), p(u), p(x), MF, 1, 0)
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    return {"value": 4 * t * iters, "unit": "s", "cores": 1, "kind": "port",
+            "sample": f"{reps} x oracle dwf_dslash = {t:.3f} s; x4 per iteration x {iters} iterations",
+            "s_per_iteration": 4 * t}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from cps_veloc_b200.dirac import gen_gauge
+
+    u = gen_gauge(L4, seed=SEED, width=0.3)
+    vals = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        info = cpu_reference_sample(u, FP64_CG_ITERS, reps=1)
+        if k >= args.warmup:
+            vals.append(info["value"])
+    v = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "DWF 16^3x32 Ls=16 M5=1.8 mf=0.01 CG on MatPcDagMatPc to true residual 1e-10",
+                   "lattice": list(L4), "ls": LS, "extrapolated_from_iterations": FP64_CG_ITERS},
+        "cpu_baseline": {k: info[k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "s"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sloppy", default="half", choices=["half", "single"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    ws, rank, local = dist_env()
+    dist = init_dist(ws)
+    A, lat, D, u, b = setup_system(local)
+    sloppy = A.HALF if args.sloppy == "half" else A.SINGLE
+    n = D.f_size
+    zero = np.zeros(n)
+    bf = field(A, D, A.DOUBLE, b)
+    x = field(A, D, A.DOUBLE, zero)
+    for prec in (A.DOUBLE, A.SINGLE, A.HALF):
+        D.autotune(prec)
+
+    # plain FP64 CG (the comparison point of the metric)
+    solve_dev(A, D, x, bf, zero, A.DOUBLE)  # warm-up
+    fp64 = [solve_dev(A, D, x, bf, zero, A.DOUBLE) for _ in range(max(1, args.fp64_steps))]
+    x64 = np.empty(n)
+    A.check(A.lib().cpsgpu_field_download(x, A.dptr(x64)))
+
+    # mixed precision: W warm-up solves, K timed solves
+    for _ in range(args.warmup):
+        solve_dev(A, D, x, bf, zero, sloppy)
+    if dist:
+        dist.barrier()
+    lat.synchronize()
+    with ClockSampler(local) as clk:
+        res = [solve_dev(A, D, x, bf, zero, sloppy) for _ in range(args.steps)]
+        lat.synchronize()
+    if dist:
+        dist.barrier()
+    xm = np.empty(n)
+    A.check(A.lib().cpsgpu_field_download(x, A.dptr(xm)))
+    t_mixed = max_over_ranks(dist, statistics.median(r.seconds for r in res))
+    t_fp64 = max_over_ranks(dist, statistics.median(r.seconds for r in fp64))
+
+    # dominant kernel: the inner solver's dslash, timed alone from HBM
+    pk = peaks()
+    ms = C.c_double()
+    by = C.c_double()
+    A.check(A.lib().cpsgpu_time_dslash(D._h, sloppy, 1, 0, 50, C.byref(ms), C.byref(by)))
+    dsl = {}
+    for name, prec in (("fp64", A.DOUBLE), ("fp32", A.SINGLE), ("half", A.HALF)):
+        m2, b2 = C.c_double(), C.c_double()
+        A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, 30, C.byref(m2), C.byref(b2)))
+        gbs = b2.value / (m2.value * 1e-3) / 1e9
+        dsl[name] = {"ms": m2.value, "GB_s": gbs, "frac_of_measured_hbm": gbs / pk["hbm_gbs"],
+                     "GFLOP_s": (1320 + 48) * L4[0] * L4[1] * L4[2] * L4[3] // 2 * LS / (m2.value * 1e-3) / 1e9}
+    achieved = by.value / (ms.value * 1e-3) / 1e9
+
+    # end to end through the host-pointer C ABI: H2D source + guess, D2H solution
+    pin_b = C.c_void_p()
+    pin_x = C.c_void_p()
+    A.check(A.lib().cpsgpu_host_alloc(n * 8, C.byref(pin_b)))
+    A.check(A.lib().cpsgpu_host_alloc(n * 8, C.byref(pin_x)))
+    hb = np.ctypeslib.as_array(C.cast(pin_b, C.POINTER(C.c_double)), shape=(n,))
+    hx = np.ctypeslib.as_array(C.cast(pin_x, C.POINTER(C.c_double)), shape=(n,))
+    hb[:] = b
+    e2e_t = []
+    arg = A.CgArg()
+    A.lib().cpsgpu_cg_arg_default(C.byref(arg))
+    arg.stop_rsd, arg.max_num_iter, arg.precision, arg.chunk = STOP, 100000, sloppy, 16
+    for k in range(max(1, args.steps)):
+        hx[:] = 0.0
+        r = A.CgResult()
+        t0 = time.perf_counter()
+        A.check(A.lib().cpsgpu_invcg(D._h, A.dptr(hx), A.dptr(hb), C.byref(arg), C.byref(r)))
+        e2e_t.append(time.perf_counter() - t0)
+        if r.status != A.CONVERGED or r.true_res > STOP:
+            raise RuntimeError("end-to-end solve failed")
+    e2e = max_over_ranks(dist, statistics.median(e2e_t))
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_sample(u, fp64[0].iterations, reps=1)
+        except Exception as e:  # noqa: BLE001
+            cpu = {"error": str(e)}
+
+    rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f16" if sloppy == A.HALF else "f64+f32", "data": "synthetic",
+            "config": {
+                "workload": "DWF 16^3x32 Ls=16 M5=1.8 mf=0.01 CG on MatPcDagMatPc to true residual 1e-10",
+                "lattice": list(L4), "ls": LS, "m5": M5, "mf": MF, "bc": "periodic xyz, antiperiodic t",
+                "gauge": "U=exp(i 0.3 H), seed 20261203", "source": "MatPcDag of a Gaussian wall source",
+                "inner": "fp16 storage + per-site norm, fp32 arithmetic" if sloppy == A.HALF else "fp32",
+                "l2": "inputs larger than L2 (FP64 vectors 192 MiB; each solve streams GBs)",
+                "parallelism": f"{ws} independent replicas" if ws > 1 else "1 GPU"},
+            "fp64_cg": {"time_s": t_fp64, "iterations": fp64[0].iterations, "true_res": fp64[0].true_res},
+            "mixed_cg": {"time_s": t_mixed, "iterations": res[0].iterations,
+                         "reliable_updates": res[0].reliable_updates, "true_res": res[0].true_res,
+                         "rel_err_vs_fp64": rel_err},
+            "speedup_vs_fp64_cg": t_fp64 / t_mixed,
+            "dslash": dsl,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                         "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32"),
+                         "peak_source": pk["source"]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
+            "clocks": clk.summary(),
+            "gpu_launches": int(sum(r.kernels for r in res)),
+        }
+        print(json.dumps(out), flush=True)
+    A.lib().cpsgpu_host_free(pin_b)
+    A.lib().cpsgpu_host_free(pin_x)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

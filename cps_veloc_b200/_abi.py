@@ -1,0 +1,122 @@
+"""ctypes binding of the C ABI in include/cpsgpu.h.
+
+The library is the in-tree ``libcpsgpu.so`` built by ``cps_veloc_b200.build``;
+loading fails loudly if it is missing (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libcpsgpu.so"
+
+DOUBLE, SINGLE, HALF = 0, 1, 2
+WILSON, DWF, MOBIUS = 0, 1, 2
+MS_SINGLE, MS_MULTI, MS_GENERAL = 0, 1, 2
+CONVERGED, MAX_ITER, BREAKDOWN, NONFINITE = 1, 2, 3, 4
+
+_dp = C.POINTER(C.c_double)
+
+
+class DiracArg(C.Structure):
+    _fields_ = [("kind", C.c_int), ("ls", C.c_int), ("mass", C.c_double), ("m5", C.c_double),
+                ("mobius_b", C.c_double), ("mobius_c", C.c_double)]
+
+
+class CgArg(C.Structure):
+    _fields_ = [("stop_rsd", C.c_double), ("max_num_iter", C.c_int), ("src_norm_sq", C.c_double),
+                ("shift", C.c_double), ("precision", C.c_int), ("delta", C.c_double), ("chunk", C.c_int),
+                ("use_graph", C.c_int)]
+
+
+class CgResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("true_res", C.c_double),
+                ("reliable_updates", C.c_int), ("seconds", C.c_double), ("kernels", C.c_longlong)]
+
+
+class CpsGpuError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise CpsGpuError(f"{LIB_PATH} is missing: run `python -m cps_veloc_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        vp = C.c_void_p
+        sigs = {
+            "cpsgpu_version": (C.c_char_p, []),
+            "cpsgpu_last_error": (C.c_char_p, []),
+            "cpsgpu_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+            "cpsgpu_set_device": (C.c_int, [C.c_int]),
+            "cpsgpu_lattice_create": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(vp)]),
+            "cpsgpu_lattice_destroy": (C.c_int, [vp]),
+            "cpsgpu_import_gauge": (C.c_int, [vp, _dp, C.c_int]),
+            "cpsgpu_gauge_info": (C.c_int, [vp, _dp, C.POINTER(C.c_int)]),
+            "cpsgpu_synchronize": (C.c_int, [vp]),
+            "cpsgpu_dirac_create": (C.c_int, [vp, C.POINTER(DiracArg), C.POINTER(vp)]),
+            "cpsgpu_dirac_destroy": (C.c_int, [vp]),
+            "cpsgpu_dirac_info": (C.c_int, [vp, _dp, _dp]),
+            "cpsgpu_dslash": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_matpc": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
+            "cpsgpu_matpc_dag_matpc": (C.c_int, [vp, _dp, _dp, _dp, C.c_int]),
+            "cpsgpu_mobius_dslash_4": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_mobius_m5inv": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
+            "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
+            "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_invcg_multi": (C.c_int, [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(CgArg),
+                                             C.POINTER(CgResult)]),
+            "cpsgpu_minvcg": (C.c_int, [vp, C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
+                                        C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_field_create": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(vp)]),
+            "cpsgpu_field_destroy": (C.c_int, [vp]),
+            "cpsgpu_field_upload": (C.c_int, [vp, _dp]),
+            "cpsgpu_field_download": (C.c_int, [vp, _dp]),
+            "cpsgpu_field_gaussian": (C.c_int, [vp, C.c_ulonglong]),
+            "cpsgpu_dslash_field": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+            "cpsgpu_mdagm_field": (C.c_int, [vp, vp, vp]),
+            "cpsgpu_invcg_field": (C.c_int, [vp, vp, vp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
+            "cpsgpu_time_mdagm": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),
+            "cpsgpu_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
+            "cpsgpu_host_free": (C.c_int, [vp]),
+            "cpsgpu_gen_gauge": (C.c_int, [C.POINTER(C.c_int), C.c_ulonglong, C.c_double, _dp]),
+            "cpsgpu_gen_gaussian": (C.c_int, [_dp, C.c_long, C.c_ulonglong, C.c_uint]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc != 0:
+        msg = lib().cpsgpu_last_error().decode(errors="replace")
+        raise CpsGpuError(f"cpsgpu error {rc}: {msg}")
+    return rc
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def ints(v) -> C.Array:
+    return (C.c_int * len(v))(*v)
+
+
+def declared_symbols(header: Path) -> list[str]:
+    """Function names declared in a C header (``cpsgpu_*(``)."""
+    import re
+
+    text = header.read_text()
+    return sorted(set(re.findall(r"\b(cpsgpu_[a-z0-9_]+)\s*\(", text)))

@@ -1,0 +1,550 @@
+// The C ABI (include/cpsgpu.h): argument checking, object lifetimes,
+// host <-> device staging in CPS storage order, and error translation.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/cpsgpu.h"
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+#include "solver.h"
+
+namespace cpsgpu {
+void gen_gauge(const int L[4], uint64_t seed, double width, double *out);
+void gen_gaussian(double *out, long n, uint64_t seed, unsigned stream);
+int autotune(Dirac &D, int prec, int nrhs);
+double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes);
+double time_mdagm(Dirac &D, int prec, int reps, double *bytes);
+int minvcg(Dirac &D, double *const *psi, const double *chi, double chi_norm, const double *shift, int nshift,
+           double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine);
+}  // namespace cpsgpu
+
+using namespace cpsgpu;
+
+struct cpsgpu_lattice_s {
+  std::unique_ptr<Lattice> L;
+};
+
+struct cpsgpu_dirac_s {
+  cpsgpu_lattice_s *lat;
+  std::unique_ptr<Dirac> D;
+  // host-path workspace
+  Field in[3], out[3];
+  OpWork w[3];
+  std::unique_ptr<CgSolver> solvers[3];
+};
+
+struct cpsgpu_field_s {
+  cpsgpu_dirac_s *d;
+  Field f;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    g_err.clear();
+    return f();
+  } catch (const Error &e) {
+    return fail(e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(CPSGPU_ERR_STATE, e.what());
+  }
+}
+
+int check_prec(int p) {
+  if (p != CPSGPU_DOUBLE && p != CPSGPU_SINGLE && p != CPSGPU_HALF) throw Error(CPSGPU_ERR_ARG, "bad precision");
+  return p;
+}
+
+size_t vec_reals(const cpsgpu_dirac_s *d) { return (size_t)24 * d->D->ls * d->D->lat->vh; }
+
+// upload a CPS-order host vector (nrhs copies at `stride` reals apart, or an
+// array of pointers) into f
+void upload(Lattice &L, Field &f, const double *const *host, int nrhs) {
+  size_t n = (size_t)24 * f.vh * f.ls;
+  L.staging.ensure(n * nrhs * sizeof(double));
+  for (int k = 0; k < nrhs; k++)
+    CPSGPU_CUDA(cudaMemcpyAsync(L.staging.as<double>() + n * k, host[k], n * sizeof(double), cudaMemcpyHostToDevice,
+                                L.stream));
+  launch_import_fermion(L.stream, f.prec, f.view(), L.staging.as<double>());
+}
+
+void download(Lattice &L, const Field &f, double *const *host, int nrhs) {
+  size_t n = (size_t)24 * f.vh * f.ls;
+  L.staging.ensure(n * nrhs * sizeof(double));
+  launch_export_fermion(L.stream, f.prec, f.view(), L.staging.as<double>());
+  for (int k = 0; k < nrhs; k++)
+    CPSGPU_CUDA(cudaMemcpyAsync(host[k], L.staging.as<double>() + n * k, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                L.stream));
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+}
+
+void need_gauge(const cpsgpu_dirac_s *d) {
+  if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+}
+
+void ensure_partials(Lattice &L, int ls, int nrhs) {
+  size_t nblk = (size_t)((L.vh + 31) / 32) * ls + 1024;
+  L.partials.ensure(nblk * 2 * nrhs * sizeof(double));
+}
+
+CgArgs to_args(const cpsgpu_cg_arg *a) {
+  CgArgs c;
+  c.stop_rsd = a->stop_rsd;
+  c.max_num_iter = a->max_num_iter;
+  c.src_norm_sq = a->src_norm_sq;
+  c.shift = a->shift;
+  c.delta = a->delta > 0 ? a->delta : 0.1;
+  c.chunk = a->chunk > 0 ? a->chunk : 8;
+  c.use_graph = a->use_graph;
+  return c;
+}
+
+void to_result(const CgResult &r, cpsgpu_cg_result *o) {
+  o->iterations = r.iterations;
+  o->status = r.status;
+  o->true_res = r.true_res;
+  o->reliable_updates = r.reliable_updates;
+  o->seconds = r.seconds;
+  o->kernels = r.kernels;
+}
+
+CgSolver &solver_for(cpsgpu_dirac_s *d, int prec, int nrhs) {
+  auto &s = d->solvers[prec];
+  if (!s) s.reset(new CgSolver(*d->D, prec));
+  if (s->nrhs != nrhs || !s->b64.data.ptr) s->setup(nrhs);
+  return *s;
+}
+}  // namespace
+
+extern "C" {
+
+const char *cpsgpu_version(void) { return "cpsgpu 0.1 (sm_100a)"; }
+const char *cpsgpu_last_error(void) { return g_err.c_str(); }
+
+int cpsgpu_device_count(int *count) {
+  return guarded([&] {
+    if (!count) throw Error(CPSGPU_ERR_ARG, "null count");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    *count = (e == cudaSuccess) ? n : 0;
+    if (e != cudaSuccess) cudaGetLastError();
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_set_device(int device) {
+  return guarded([&] {
+    CPSGPU_CUDA(cudaSetDevice(device));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_lattice_create(const int node_sites[4], const int bc[4], cpsgpu_lattice *lat) {
+  return guarded([&] {
+    if (!node_sites || !bc || !lat) throw Error(CPSGPU_ERR_ARG, "null argument");
+    double b[4];
+    for (int k = 0; k < 4; k++) {
+      if (bc[k] != 1 && bc[k] != -1) throw Error(CPSGPU_ERR_ARG, "bc must be +1 or -1");
+      b[k] = bc[k];
+    }
+    auto *l = new cpsgpu_lattice_s;
+    try {
+      l->L.reset(new Lattice(node_sites, b));
+    } catch (...) {
+      delete l;
+      throw;
+    }
+    *lat = l;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_lattice_destroy(cpsgpu_lattice lat) {
+  return guarded([&] {
+    delete lat;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_import_gauge(cpsgpu_lattice lat, const double *u, int signs_applied) {
+  return guarded([&] {
+    if (!lat || !u) throw Error(CPSGPU_ERR_ARG, "null argument");
+    import_gauge(*lat->L, u, signs_applied);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_gauge_info(cpsgpu_lattice lat, double *recon_err, int *recon12) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    if (recon_err) *recon_err = lat->L->recon_err;
+    if (recon12) *recon12 = lat->L->use_recon12 ? 1 : 0;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_synchronize(cpsgpu_lattice lat) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    CPSGPU_CUDA(cudaStreamSynchronize(lat->L->stream));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *a, cpsgpu_dirac *d) {
+  return guarded([&] {
+    if (!lat || !a || !d) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (a->kind < CPSGPU_WILSON || a->kind > CPSGPU_MOBIUS) throw Error(CPSGPU_ERR_ARG, "unknown fermion kind");
+    auto *o = new cpsgpu_dirac_s;
+    o->lat = lat;
+    try {
+      o->D.reset(new Dirac(lat->L.get(), a->kind, a->ls, a->mass, a->m5, a->mobius_b, a->mobius_c));
+      ensure_partials(*lat->L, o->D->ls, 1);
+    } catch (...) {
+      delete o;
+      throw;
+    }
+    *d = o;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dirac_destroy(cpsgpu_dirac d) {
+  return guarded([&] {
+    delete d;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dirac_info(cpsgpu_dirac d, double *kappa, double *kappa_c) {
+  return guarded([&] {
+    if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
+    if (kappa) *kappa = d->D->kappa;
+    if (kappa_c) *kappa_c = d->D->kappa_c;
+    return CPSGPU_OK;
+  });
+}
+
+// ---- host-vector operators
+int cpsgpu_dslash(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if ((cb != 0 && cb != 1) || (dag != 0 && dag != 1)) throw Error(CPSGPU_ERR_ARG, "cb and dag must be 0 or 1");
+    check_prec(prec);
+    need_gauge(d);
+    if (d->D->kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "Mobius: use cpsgpu_mobius_dslash_4");
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    op_dslash(*d->D, prec, d->out[prec].view(), d->in[prec].view(), cb, dag);
+    download(L, d->out[prec], &out, 1);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_matpc(cpsgpu_dirac d, double *out, const double *in, int dag, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    check_prec(prec);
+    need_gauge(d);
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    op_matpc(*d->D, prec, d->out[prec].view(), d->in[prec].view(), dag ? 1 : 0, d->w[prec], nullptr, 0, 0);
+    download(L, d->out[prec], &out, 1);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double *dot, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    check_prec(prec);
+    need_gauge(d);
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    SolverScalars *st = L.scratch_st.as<SolverScalars>();
+    CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
+    op_mdagm(*d->D, prec, d->out[prec].view(), d->in[prec].view(), d->w[prec], st, RED_STORE);
+    download(L, d->out[prec], &out, 1);
+    if (dot) {
+      SolverScalars h;
+      CPSGPU_CUDA(cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost));
+      *dot = h.sum[0];
+    }
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if ((cb != 0 && cb != 1) || (dag != 0 && dag != 1)) throw Error(CPSGPU_ERR_ARG, "cb and dag must be 0 or 1");
+    check_prec(prec);
+    need_gauge(d);
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    op_mobius_dslash4(*d->D, prec, d->out[prec].view(), d->in[prec].view(), cb, dag, d->w[prec]);
+    download(L, d->out[prec], &out, 1);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_mobius_m5inv(cpsgpu_dirac d, double *out, const double *in, int dag, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    check_prec(prec);
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    op_mobius_m5inv(*d->D, prec, d->out[prec].view(), d->in[prec].view(), dag ? 1 : 0);
+    download(L, d->out[prec], &out, 1);
+    return CPSGPU_OK;
+  });
+}
+
+// ---- solvers
+void cpsgpu_cg_arg_default(cpsgpu_cg_arg *a) {
+  if (!a) return;
+  a->stop_rsd = 1e-8;
+  a->max_num_iter = 10000;
+  a->src_norm_sq = 0.0;
+  a->shift = 0.0;
+  a->precision = CPSGPU_DOUBLE;
+  a->delta = 0.1;
+  a->chunk = 8;
+  a->use_graph = 1;
+}
+
+int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
+                       const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res) {
+  return guarded([&] {
+    if (!d || !sol || !src || !arg || !res || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    if (nrhs > 64) throw Error(CPSGPU_ERR_ARG, "at most 64 right-hand sides per call");
+    if (arg->max_num_iter < 1) throw Error(CPSGPU_ERR_ARG, "max_num_iter must be >= 1");
+    for (int k = 0; k < nrhs; k++)
+      if (!sol[k] || !src[k]) throw Error(CPSGPU_ERR_ARG, "null vector");
+    check_prec(arg->precision);
+    need_gauge(d);
+    Lattice &L = *d->D->lat;
+    CgSolver &S = solver_for(d, arg->precision, nrhs);
+    upload(L, S.b64, src, nrhs);
+    upload(L, S.x64, sol, nrhs);
+    std::vector<CgResult> r;
+    S.run(to_args(arg), r);
+    download(L, S.x64, sol, nrhs);
+    for (int k = 0; k < nrhs; k++) to_result(r[k], res + k);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res) {
+  return cpsgpu_invcg_multi(d, &sol, &src, 1, arg, res);
+}
+
+int cpsgpu_minvcg(cpsgpu_dirac d, double *const *psi, const double *chi, double chi_norm, const double *shift,
+                  int nshift, double *rsdcg, int type, const double *alpha, int max_num_iter, int precision,
+                  int refine, int *iterations) {
+  return guarded([&] {
+    if (!d || !psi || !chi || !shift || !rsdcg || nshift < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    if (type < 0 || type > 2) throw Error(CPSGPU_ERR_ARG, "bad multishift type");
+    if (type == CPSGPU_MS_SINGLE && !alpha) throw Error(CPSGPU_ERR_ARG, "SINGLE needs alpha");
+    check_prec(precision);
+    need_gauge(d);
+    int k = minvcg(*d->D, psi, chi, chi_norm, shift, nshift, rsdcg, type, alpha, max_num_iter, precision, refine);
+    if (iterations) *iterations = k;
+    return CPSGPU_OK;
+  });
+}
+
+// ---- device fields
+int cpsgpu_field_create(cpsgpu_dirac d, int precision, int nrhs, cpsgpu_field *f) {
+  return guarded([&] {
+    if (!d || !f || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(precision);
+    auto *o = new cpsgpu_field_s;
+    o->d = d;
+    try {
+      o->f.create(precision, d->D->lat->vh, d->D->ls, nrhs);
+    } catch (...) {
+      delete o;
+      throw;
+    }
+    *f = o;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_destroy(cpsgpu_field f) {
+  return guarded([&] {
+    delete f;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_upload(cpsgpu_field f, const double *host) {
+  return guarded([&] {
+    if (!f || !host) throw Error(CPSGPU_ERR_ARG, "null argument");
+    Lattice &L = *f->d->D->lat;
+    size_t n = (size_t)24 * f->f.vh * f->f.ls;
+    std::vector<const double *> ptrs(f->f.nrhs);
+    for (int k = 0; k < f->f.nrhs; k++) ptrs[k] = host + n * k;
+    upload(L, f->f, ptrs.data(), f->f.nrhs);
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_download(cpsgpu_field f, double *host) {
+  return guarded([&] {
+    if (!f || !host) throw Error(CPSGPU_ERR_ARG, "null argument");
+    Lattice &L = *f->d->D->lat;
+    size_t n = (size_t)24 * f->f.vh * f->f.ls;
+    std::vector<double *> ptrs(f->f.nrhs);
+    for (int k = 0; k < f->f.nrhs; k++) ptrs[k] = host + n * k;
+    download(L, f->f, ptrs.data(), f->f.nrhs);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_gaussian(cpsgpu_field f, unsigned long long seed) {
+  return guarded([&] {
+    if (!f) throw Error(CPSGPU_ERR_ARG, "null field");
+    size_t n = (size_t)24 * f->f.vh * f->f.ls * f->f.nrhs;
+    std::vector<double> h(n);
+    gen_gaussian(h.data(), (long)n, seed, 0);
+    Lattice &L = *f->d->D->lat;
+    size_t per = n / f->f.nrhs;
+    std::vector<const double *> ptrs(f->f.nrhs);
+    for (int k = 0; k < f->f.nrhs; k++) ptrs[k] = h.data() + per * k;
+    upload(L, f->f, ptrs.data(), f->f.nrhs);
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dslash_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    need_gauge(d);
+    op_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_mdagm_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    need_gauge(d);
+    op_mdagm(*d->D, in->f.prec, out->f.view(), in->f.view(), d->w[in->f.prec], nullptr, 0);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,
+                       cpsgpu_cg_result *res) {
+  return guarded([&] {
+    if (!d || !sol || !src || !arg || !res) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (sol->f.prec != PREC_DOUBLE || src->f.prec != PREC_DOUBLE) throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+    if (sol->f.nrhs != src->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    check_prec(arg->precision);
+    need_gauge(d);
+    int nrhs = src->f.nrhs;
+    CgSolver &S = solver_for(d, arg->precision, nrhs);
+    Lattice &L = *d->D->lat;
+    CPSGPU_CUDA(cudaMemcpyAsync(S.b64.data.ptr, src->f.data.ptr, src->f.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+    CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, sol->f.data.ptr, sol->f.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+    std::vector<CgResult> r;
+    S.run(to_args(arg), r);
+    CPSGPU_CUDA(cudaMemcpyAsync(sol->f.data.ptr, S.x64.data.ptr, sol->f.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    for (int k = 0; k < nrhs; k++) to_result(r[k], res + k);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned) {
+  return guarded([&] {
+    if (!d || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    need_gauge(d);
+    int n = autotune(*d->D, prec, nrhs);
+    if (tuned) *tuned = n;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_time_dslash(cpsgpu_dirac d, int prec, int cb, int dag, int reps, double *ms, double *bytes) {
+  return guarded([&] {
+    if (!d || reps < 1 || !ms) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    need_gauge(d);
+    *ms = time_dslash(*d->D, prec, cb ? 1 : 0, dag ? 1 : 0, reps, bytes);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_time_mdagm(cpsgpu_dirac d, int prec, int reps, double *ms, double *bytes) {
+  return guarded([&] {
+    if (!d || reps < 1 || !ms) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    need_gauge(d);
+    *ms = time_mdagm(*d->D, prec, reps, bytes);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_host_alloc(size_t bytes, void **ptr) {
+  return guarded([&] {
+    if (!ptr) throw Error(CPSGPU_ERR_ARG, "null pointer");
+    CPSGPU_CUDA(cudaMallocHost(ptr, bytes));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_host_free(void *ptr) {
+  return guarded([&] {
+    if (ptr) CPSGPU_CUDA(cudaFreeHost(ptr));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_gen_gauge(const int node_sites[4], unsigned long long seed, double width, double *u) {
+  return guarded([&] {
+    if (!node_sites || !u) throw Error(CPSGPU_ERR_ARG, "null argument");
+    for (int k = 0; k < 4; k++)
+      if (node_sites[k] <= 0 || (node_sites[k] & 1)) throw Error(CPSGPU_ERR_ARG, "extents must be positive and even");
+    gen_gauge(node_sites, seed, width, u);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_gen_gaussian(double *out, long n, unsigned long long seed, unsigned int stream) {
+  return guarded([&] {
+    if (!out || n < 0) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    gen_gaussian(out, n, seed, stream);
+    return CPSGPU_OK;
+  });
+}
+
+}  // extern "C"

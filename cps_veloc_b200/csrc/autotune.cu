@@ -1,0 +1,96 @@
+// Autotuner: times candidate block shapes of the hop kernels on the live
+// lattice and records the fastest in the launch table (tune.cpp).  A shape
+// is (sites per block) x (slices per block); the mixing epilogue of the
+// Mobius operator needs all slices of a site in one block, so only its
+// site count varies.
+#include <vector>
+
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+#include "tune.h"
+
+namespace cpsgpu {
+
+namespace {
+SpinorView none() { return SpinorView(); }
+
+float time_launch(const Dirac &D, HopLaunch &Lh, const Field &in, const Field &out, const Field &x,
+                  SolverScalars *st, cudaEvent_t e0, cudaEvent_t e1) {
+  cudaStream_t s = D.lat->stream;
+  for (int k = 0; k < 2; k++) launch_hop(D, Lh, in.view(), out.view(), x.view(), none(), none(), none(), none(), st);
+  CPSGPU_CUDA(cudaEventRecord(e0, s));
+  const int reps = 5;
+  for (int k = 0; k < reps; k++) launch_hop(D, Lh, in.view(), out.view(), x.view(), none(), none(), none(), none(), st);
+  CPSGPU_CUDA(cudaEventRecord(e1, s));
+  CPSGPU_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  return ms / reps;
+}
+}  // namespace
+
+int autotune(Dirac &D, int prec, int nrhs) {
+  Lattice &L = *D.lat;
+  const int recon = L.recon(prec);
+  Field in(prec, L.vh, D.ls, nrhs), out(prec, L.vh, D.ls, nrhs), x(prec, L.vh, D.ls, nrhs);
+  launch_zero(L.stream, in);
+  launch_zero(L.stream, x);
+  size_t nblk = (size_t)((L.vh + 15) / 16) * D.ls + 1024;
+  L.partials.ensure(nblk * 2 * nrhs * sizeof(double));
+  cudaEvent_t e0, e1;
+  CPSGPU_CUDA(cudaEventCreate(&e0));
+  CPSGPU_CUDA(cudaEventCreate(&e1));
+  int tuned = 0;
+  // plain hop shapes (also used by the AXPY / CG / RES epilogues)
+  {
+    HopLaunch Lh;
+    Lh.prec = prec;
+    Lh.ep = EP_STORE;
+    Lh.cb = 1;
+    std::vector<dim3> cand;
+    const int bxs[] = {16, 32, 64, 128, 256};
+    const int bss[] = {1, 2, 4, 8, 16};
+    for (int bx : bxs)
+      for (int bs : bss)
+        if (bx * bs <= 256 && bx * bs >= 64 && bs <= (D.ls > 1 ? D.ls : 1)) cand.push_back(dim3(bx, bs));
+    TuneKey key{prec, recon, EP_STORE, D.kind, D.ls};
+    float best = 1e30f;
+    dim3 bestb = hop_block(key, false);
+    for (auto b : cand) {
+      tune_set(key, b);
+      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
+      if (t < best) { best = t; bestb = b; }
+    }
+    const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
+    for (int ep : eps) {
+      tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb);
+      tuned++;
+    }
+  }
+  if (D.kind == KIND_MOBIUS) {
+    HopLaunch Lh;
+    Lh.prec = prec;
+    Lh.ep = EP_MIX;
+    Lh.cb = 1;
+    Lh.mix = D.mixQ.as<double>();
+    TuneKey key{prec, recon, EP_MIX, D.kind, D.ls};
+    float best = 1e30f;
+    dim3 bestb = hop_block(key, true);
+    for (int bx = 1; bx * D.ls <= 256; bx *= 2) {
+      dim3 b(bx, D.ls);
+      tune_set(key, b);
+      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
+      if (t < best) { best = t; bestb = b; }
+    }
+    const int eps[] = {EP_MIX, EP_MIX_AXPY, EP_MIX_CG, EP_MIX_RES};
+    for (int ep : eps) {
+      tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb);
+      tuned++;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return tuned;
+}
+
+}  // namespace cpsgpu

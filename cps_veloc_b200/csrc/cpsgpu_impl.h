@@ -1,0 +1,169 @@
+// Host-side structures of the library behind the C ABI (include/cpsgpu.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fields.cuh"
+#include "reduce.cuh"
+
+namespace cpsgpu {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CPSGPU_CUDA(call)                                                                   \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      throw ::cpsgpu::Error(-3, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+// Owning device allocation.
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t n) { alloc(n); }
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
+    if (this != &o) { release(); ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0; }
+    return *this;
+  }
+  ~DeviceBuffer() { release(); }
+  void alloc(size_t n) {
+    release();
+    if (n) CPSGPU_CUDA(cudaMalloc(&ptr, n));
+    bytes = n;
+  }
+  void ensure(size_t n) { if (n > bytes) alloc(n); }
+  void release() { if (ptr) cudaFree(ptr); ptr = nullptr; bytes = 0; }
+  template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// A fermion field in one precision: nrhs x ls slices of vh sites.
+struct Field {
+  int prec = PREC_DOUBLE;
+  long vh = 0;
+  int ls = 1, nrhs = 1;
+  DeviceBuffer data, norm;
+  Field() = default;
+  Field(int p, long vh_, int ls_, int nrhs_) { create(p, vh_, ls_, nrhs_); }
+  void create(int p, long vh_, int ls_, int nrhs_);
+  size_t site_bytes() const;
+  size_t sites() const { return (size_t)vh * ls * nrhs; }
+  SpinorView view() const {
+    SpinorView v;
+    v.data = data.ptr;
+    v.norm = norm.as<float>();
+    v.vh = vh;
+    v.ls = ls;
+    v.nrhs = nrhs;
+    return v;
+  }
+  // view of right-hand side k alone
+  SpinorView view_rhs(int k) const;
+};
+
+enum DiracKind { KIND_WILSON = 0, KIND_DWF = 1, KIND_MOBIUS = 2 };
+
+struct Lattice {
+  int L[4];
+  long vh;
+  double bc[4];
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // gauge field copies: FP64 full and compressed, FP32 and FP16 compressed
+  DeviceBuffer gD18, gD12, gS12, gH12;
+  bool have_gauge = false;
+  double recon_err = 0.0;  // max |row2 - conj(row0 x row1)| over all links
+  bool use_recon12 = true; // FP64 operator reads 12-real links
+  DeviceBuffer staging;    // CPS-order host mirror on the device
+  DeviceBuffer partials;   // per-block reduction partials
+  DeviceBuffer scratch_st; // SolverScalars for operator-only reductions
+  double *pinned = nullptr;  // small pinned host buffer for scalars
+  Lattice(const int L_[4], const double bc_[4]);
+  ~Lattice();
+  GaugeView gauge(int prec) const;
+  int recon(int prec) const { return (prec == PREC_DOUBLE && !use_recon12) ? 18 : 12; }
+};
+
+struct Dirac {
+  Lattice *lat;
+  int kind;
+  int ls;
+  double mass, m5, b, c;
+  double kappa;  // Wilson kappa, DWF kappa_5, Mobius kappa_b
+  double kappa_c;
+  // Mobius s-mixing matrices, each [2][ls][ls] (upper, lower chirality):
+  //   P = B M5inv, Q = B M5inv kappa_b, R = kappa_b M5inv^+ B^+ (-kappa_b),
+  //   S = M5inv^+ B^+, and the pieces B, B^+, M5inv, M5inv^+ on their own.
+  DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id;
+  std::vector<double> hM5i, hM5id, hB, hBd;
+  Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_);
+};
+
+// ---- kernels / launchers (hop.cu, blas.cu) ----
+struct OpWork {
+  Field t1, t2, t0;  // operator temporaries, one precision
+};
+
+// Launch one hop with epilogue; see hop.cuh for the meaning of each field.
+struct HopLaunch {
+  int prec = PREC_DOUBLE;   // hop precision
+  int pr = PREC_DOUBLE;     // r/p precision (CG/RES)
+  int px = PREC_DOUBLE;     // sol precision (CG)
+  int ep = 0;
+  int cb = 0, dag = 0;
+  int norm = 0, red_op = 0, gate = 0;
+  const double *mix = nullptr;
+  std::vector<double> coef;  // per slice
+};
+void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
+                const SpinorView &x, const SpinorView &r, const SpinorView &sol, const SpinorView &p,
+                const SpinorView &b, SolverScalars *st);
+
+// out = Mix in (per chirality Ls x Ls), all slices
+void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
+                const SolverScalars *st = nullptr, int gate = 0);
+
+// vector kernels
+void launch_convert(cudaStream_t s, int pdst, const SpinorView &dst, int psrc, const SpinorView &src);
+void launch_zero(cudaStream_t s, const Field &f);
+// p = r + beta p (gated on st->done)
+void launch_xpay(cudaStream_t s, int prec, const SpinorView &p, const SpinorView &r, SolverScalars *st, int nrhs);
+// x64 += xs; xs = 0 (gated on st->reliable)
+void launch_accum_reliable(cudaStream_t s, const SpinorView &x64, int pxs, const SpinorView &xs, SolverScalars *st, int nrhs,
+                           int force);
+// |f|^2 (+ finalize op)
+void launch_norm(cudaStream_t s, int prec, const SpinorView &f, SolverScalars *st, double *partials, int op, int gate);
+// st[k] <- value (host-side init through a kernel so graphs can replay it)
+void launch_init_scalars(cudaStream_t s, SolverScalars *st, int nrhs, const SolverScalars &init);
+
+// CPS order <-> device layout
+void launch_import_fermion(cudaStream_t s, int prec, const SpinorView &dst, const double *staging);
+void launch_export_fermion(cudaStream_t s, int prec, const SpinorView &src, double *staging);
+void import_gauge(Lattice &L, const double *host_wilson_order, int signs_applied);
+
+// operators (operators.cu)
+void op_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag);
+void op_matpc(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag, OpWork &w,
+              SolverScalars *st, int norm, int red_op);
+void op_mdagm(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, OpWork &w,
+              SolverScalars *st, int red_op_dot);
+void op_mobius_dslash4(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
+                       OpWork &w);
+void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag);
+
+// kernels enqueued by this library (graph replays counted by the solver)
+long long &launch_counter();
+
+// workspace sizing helper
+void ensure_field(Field &f, int prec, long vh, int ls, int nrhs);
+
+}  // namespace cpsgpu

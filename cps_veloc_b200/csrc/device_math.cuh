@@ -1,0 +1,127 @@
+// Device arithmetic for the fermion operators: complex numbers, SU(3)
+// links (full 18-real or compressed 12-real), Dirac spinors, and the
+// spin projection (1 -/+ gamma_mu) used by every hop.
+//
+// Spinor components are held in registers as 24 reals in the reference's
+// element order, index 2*(colour + 3*spin) + re/im (wilson_dslash.C:60), so
+// chiral halves are reals 0-11 (gamma_5 = +1) and 12-23 (gamma_5 = -1).
+//
+// The gamma-matrix convention is the one the reference expands in
+// OneMinusPlusGammaTimesPsi (wilson_dslash.C:64-128).  Because (1 + k g_mu)
+// has rank 2, each hop is computed on a two-spin half spinor h = P psi,
+// multiplied by the link, and reconstructed: the same value as the
+// reference's full four-spin product, at half the flops (the 1320 flops per
+// site the reference counts, wilson_dslash.C:515).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace cpsgpu {
+
+template <typename R> struct cplx {
+  R re, im;
+};
+
+template <typename R> __device__ __forceinline__ cplx<R> mk(R a, R b) { return {a, b}; }
+template <typename R> __device__ __forceinline__ cplx<R> operator+(cplx<R> a, cplx<R> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename R> __device__ __forceinline__ cplx<R> operator-(cplx<R> a, cplx<R> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename R> __device__ __forceinline__ cplx<R> operator*(cplx<R> a, cplx<R> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename R> __device__ __forceinline__ cplx<R> conj(cplx<R> a) { return {a.re, -a.im}; }
+// a * conj(b)
+template <typename R> __device__ __forceinline__ cplx<R> mul_conj(cplx<R> a, cplx<R> b) {
+  return {a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im};
+}
+// conj(a) * b
+template <typename R> __device__ __forceinline__ cplx<R> conj_mul(cplx<R> a, cplx<R> b) {
+  return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+}
+// i * a
+template <typename R> __device__ __forceinline__ cplx<R> times_i(cplx<R> a) { return {-a.im, a.re}; }
+
+// SU(3) matrix, m[row][col]
+template <typename R> struct su3 {
+  cplx<R> m[3][3];
+};
+
+// third row of an SU(3) matrix from its first two: r2 = conj(r0 x r1)
+template <typename R> __device__ __forceinline__ void reconstruct_row2(su3<R> &u) {
+  u.m[2][0] = conj(u.m[0][1] * u.m[1][2] - u.m[0][2] * u.m[1][1]);
+  u.m[2][1] = conj(u.m[0][2] * u.m[1][0] - u.m[0][0] * u.m[1][2]);
+  u.m[2][2] = conj(u.m[0][0] * u.m[1][1] - u.m[0][1] * u.m[1][0]);
+}
+
+// Half spinor: two spin components of a colour vector.
+template <typename R> struct half_spinor {
+  cplx<R> h[2][3];
+};
+
+template <typename R> __device__ __forceinline__ cplx<R> sp(const R *v, int spin, int col) {
+  return {v[2 * (col + 3 * spin)], v[2 * (col + 3 * spin) + 1]};
+}
+
+// h = first two spin rows of (1 + k gamma_mu) psi.
+template <typename R>
+__device__ __forceinline__ half_spinor<R> project(const R *psi, int mu, R k) {
+  half_spinor<R> h;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    cplx<R> p0 = sp(psi, 0, c), p1 = sp(psi, 1, c), p2 = sp(psi, 2, c), p3 = sp(psi, 3, c);
+    cplx<R> a, b;
+    switch (mu) {
+      case 0: a = times_i(p3); b = times_i(p2); break;             // g_x: rows (0,3,+i) (1,2,+i)
+      case 1: a = mk(-p3.re, -p3.im); b = p2; break;                // g_y: rows (0,3,-1) (1,2,+1)
+      case 2: a = times_i(p2); b = mk(p3.im, -p3.re); break;        // g_z: rows (0,2,+i) (1,3,-i)
+      default: a = p2; b = p3; break;                               // g_t: rows (0,2,+1) (1,3,+1)
+    }
+    h.h[0][c] = mk(p0.re + k * a.re, p0.im + k * a.im);
+    h.h[1][c] = mk(p1.re + k * b.re, p1.im + k * b.im);
+  }
+  return h;
+}
+
+// acc += w * (full four-spin spinor rebuilt from the half spinor g = U h),
+// the rows 2,3 of (1 + k gamma_mu) expressed through rows 0,1.
+template <typename R>
+__device__ __forceinline__ void reconstruct_acc(R *acc, const half_spinor<R> &g, int mu, R k, R w) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    cplx<R> g0 = g.h[0][c], g1 = g.h[1][c];
+    cplx<R> r2, r3;
+    switch (mu) {
+      case 0: { cplx<R> a = times_i(g1), b = times_i(g0); r2 = mk(-k * a.re, -k * a.im); r3 = mk(-k * b.re, -k * b.im); } break;
+      case 1: r2 = mk(k * g1.re, k * g1.im); r3 = mk(-k * g0.re, -k * g0.im); break;
+      case 2: { cplx<R> a = times_i(g0), b = times_i(g1); r2 = mk(-k * a.re, -k * a.im); r3 = mk(k * b.re, k * b.im); } break;
+      default: r2 = mk(k * g0.re, k * g0.im); r3 = mk(k * g1.re, k * g1.im); break;
+    }
+    acc[2 * (c + 0)] += w * g0.re;      acc[2 * (c + 0) + 1] += w * g0.im;
+    acc[2 * (c + 3)] += w * g1.re;      acc[2 * (c + 3) + 1] += w * g1.im;
+    acc[2 * (c + 6)] += w * r2.re;      acc[2 * (c + 6) + 1] += w * r2.im;
+    acc[2 * (c + 9)] += w * r3.re;      acc[2 * (c + 9) + 1] += w * r3.im;
+  }
+}
+
+// g = U h  (dagger = false) or U^dagger h (dagger = true)
+template <typename R>
+__device__ __forceinline__ half_spinor<R> link_mul(const su3<R> &u, const half_spinor<R> &h, bool dagger) {
+  half_spinor<R> g;
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      cplx<R> v = mk<R>(0, 0);
+      if (!dagger) {
+#pragma unroll
+        for (int b = 0; b < 3; b++) v = v + u.m[a][b] * h.h[s][b];
+      } else {
+#pragma unroll
+        for (int b = 0; b < 3; b++) v = v + conj_mul(u.m[b][a], h.h[s][b]);
+      }
+      g.h[s][a] = v;
+    }
+  return g;
+}
+
+}  // namespace cpsgpu

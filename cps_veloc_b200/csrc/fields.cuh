@@ -1,0 +1,225 @@
+// Device storage of gauge links and fermion fields, in three precisions.
+//
+// Layout in HBM (site-SoA, one 16- or 8-byte group per load):
+//   fermion field: group g of checkerboard site i in slice sl = rhs*Ls + s at
+//       data[(sl * NG + g) * vh + i]
+//     double: 12 groups of double2 (2 reals)      192 B / site
+//     single:  6 groups of float4  (4 reals)       96 B / site
+//     half:    3 groups of 8 x fp16 (uint4)        48 B / site
+//              + one float norm per site at norm[sl * vh + i]  (52 B / site)
+//   gauge field: group g of the link (parity p, direction mu, site i) at
+//       data[((p * 4 + mu) * NG + g) * vh + i]
+//     double, 18 reals: 9 x double2   double, 12 reals: 6 x double2
+//     single, 12 reals: 3 x float4    half, 12 reals: 3 x (4 x fp16, uint2)
+// A warp reading group g of 32 consecutive sites touches 512 (or 256)
+// contiguous bytes, so every spinor and link load is a fully coalesced
+// 128-bit (or 64-bit) access.
+//
+// The 12-real form keeps the first two rows of each SU(3) link; the third is
+// rebuilt in registers as conj(row0 x row1).  That identity holds only for
+// det U = +1, which is why antiperiodic boundary signs are never folded into
+// the stored links: the sign is applied to the hop instead.
+#pragma once
+#include "device_math.cuh"
+
+namespace cpsgpu {
+
+enum Precision { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
+
+template <int P> struct PrecTraits;
+template <> struct PrecTraits<PREC_DOUBLE> {
+  using real = double;
+  static constexpr int NG = 12;          // spinor groups
+  static constexpr int SITE_BYTES = 192;
+};
+template <> struct PrecTraits<PREC_SINGLE> {
+  using real = float;
+  static constexpr int NG = 6;
+  static constexpr int SITE_BYTES = 96;
+};
+template <> struct PrecTraits<PREC_HALF> {
+  using real = float;
+  static constexpr int NG = 3;
+  static constexpr int SITE_BYTES = 52;
+};
+
+// Non-owning device view of a fermion field.
+struct SpinorView {
+  void *data = nullptr;
+  float *norm = nullptr;  // half precision only
+  long vh = 0;            // checkerboard sites per slice
+  int ls = 1;             // slices per right-hand side
+  int nrhs = 1;
+};
+
+// Non-owning device view of a gauge field.
+struct GaugeView {
+  const void *data = nullptr;
+  long vh = 0;
+};
+
+template <int P> struct SpinorIO;
+
+template <> struct SpinorIO<PREC_DOUBLE> {
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, double *v) {
+    const double2 *d = reinterpret_cast<const double2 *>(f.data) + sl * 12 * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 12; g++) {
+      double2 q = __ldg(d + g * f.vh);
+      v[2 * g] = q.x;
+      v[2 * g + 1] = q.y;
+    }
+  }
+  static __device__ __forceinline__ void store(const SpinorView &f, long sl, long i, const double *v) {
+    double2 *d = reinterpret_cast<double2 *>(f.data) + sl * 12 * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 12; g++) d[g * f.vh] = make_double2(v[2 * g], v[2 * g + 1]);
+  }
+  // one chiral half: reals [12*half, 12*half+12)
+  static __device__ __forceinline__ void load_half(const SpinorView &f, long sl, long i, int half, double *v) {
+    const double2 *d = reinterpret_cast<const double2 *>(f.data) + (sl * 12 + 6 * half) * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+      double2 q = __ldg(d + g * f.vh);
+      v[2 * g] = q.x;
+      v[2 * g + 1] = q.y;
+    }
+  }
+};
+
+template <> struct SpinorIO<PREC_SINGLE> {
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, float *v) {
+    const float4 *d = reinterpret_cast<const float4 *>(f.data) + sl * 6 * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+      float4 q = __ldg(d + g * f.vh);
+      v[4 * g] = q.x; v[4 * g + 1] = q.y; v[4 * g + 2] = q.z; v[4 * g + 3] = q.w;
+    }
+  }
+  static __device__ __forceinline__ void store(const SpinorView &f, long sl, long i, const float *v) {
+    float4 *d = reinterpret_cast<float4 *>(f.data) + sl * 6 * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 6; g++) d[g * f.vh] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+  }
+  static __device__ __forceinline__ void load_half(const SpinorView &f, long sl, long i, int half, float *v) {
+    const float4 *d = reinterpret_cast<const float4 *>(f.data) + (sl * 6 + 3 * half) * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 3; g++) {
+      float4 q = __ldg(d + g * f.vh);
+      v[4 * g] = q.x; v[4 * g + 1] = q.y; v[4 * g + 2] = q.z; v[4 * g + 3] = q.w;
+    }
+  }
+};
+
+__device__ __forceinline__ void unpack8(uint4 q, float s, float *v) {
+  const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    float2 f = __half22float2(h[k]);
+    v[2 * k] = f.x * s;
+    v[2 * k + 1] = f.y * s;
+  }
+}
+
+// Half precision: 24 fp16 values scaled by a per-site float norm (the
+// largest magnitude in the spinor), so every stored value lies in [-1, 1].
+template <> struct SpinorIO<PREC_HALF> {
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, float *v) {
+    const uint4 *d = reinterpret_cast<const uint4 *>(f.data) + sl * 3 * f.vh + i;
+    float s = __ldg(f.norm + sl * f.vh + i);
+#pragma unroll
+    for (int g = 0; g < 3; g++) unpack8(__ldg(d + g * f.vh), s, v + 8 * g);
+  }
+  static __device__ __forceinline__ void store(const SpinorView &f, long sl, long i, const float *v) {
+    float m = 0.f;
+#pragma unroll
+    for (int k = 0; k < 24; k++) m = fmaxf(m, fabsf(v[k]));
+    float inv = (m > 0.f) ? 1.0f / m : 0.f;
+    uint4 *d = reinterpret_cast<uint4 *>(f.data) + sl * 3 * f.vh + i;
+#pragma unroll
+    for (int g = 0; g < 3; g++) {
+      uint4 q;
+      __half2 *h = reinterpret_cast<__half2 *>(&q);
+#pragma unroll
+      for (int k = 0; k < 4; k++) h[k] = __floats2half2_rn(v[8 * g + 2 * k] * inv, v[8 * g + 2 * k + 1] * inv);
+      d[g * f.vh] = q;
+    }
+    f.norm[sl * f.vh + i] = m;
+  }
+  static __device__ __forceinline__ void load_half(const SpinorView &f, long sl, long i, int half, float *v) {
+    // a chiral half spans 1.5 groups; load the two groups it touches
+    const uint4 *d = reinterpret_cast<const uint4 *>(f.data) + sl * 3 * f.vh + i;
+    float s = __ldg(f.norm + sl * f.vh + i);
+    float tmp[16];
+    if (half == 0) {
+      unpack8(__ldg(d), s, tmp);
+      unpack8(__ldg(d + f.vh), s, tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[k];
+    } else {
+      unpack8(__ldg(d + f.vh), s, tmp);
+      unpack8(__ldg(d + 2 * f.vh), s, tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[4 + k];
+    }
+  }
+};
+
+// ---- gauge links ----
+template <int P, int RECON> struct LinkIO;
+
+template <> struct LinkIO<PREC_DOUBLE, 18> {
+  static constexpr int NG = 9;
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<double> &u) {
+    const double2 *d = reinterpret_cast<const double2 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      double2 q = __ldg(d + k * g.vh);
+      u.m[k / 3][k % 3] = {q.x, q.y};
+    }
+  }
+};
+template <> struct LinkIO<PREC_DOUBLE, 12> {
+  static constexpr int NG = 6;
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<double> &u) {
+    const double2 *d = reinterpret_cast<const double2 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      double2 q = __ldg(d + k * g.vh);
+      u.m[k / 3][k % 3] = {q.x, q.y};
+    }
+    reconstruct_row2(u);
+  }
+};
+template <> struct LinkIO<PREC_SINGLE, 12> {
+  static constexpr int NG = 3;
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
+    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float4 q = __ldg(d + k * g.vh);
+      int e = 2 * k;
+      u.m[e / 3][e % 3] = {q.x, q.y};
+      u.m[(e + 1) / 3][(e + 1) % 3] = {q.z, q.w};
+    }
+    reconstruct_row2(u);
+  }
+};
+template <> struct LinkIO<PREC_HALF, 12> {
+  static constexpr int NG = 3;
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
+    const uint2 *d = reinterpret_cast<const uint2 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      uint2 q = __ldg(d + k * g.vh);
+      const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+      float2 a = __half22float2(h[0]), b = __half22float2(h[1]);
+      int e = 2 * k;
+      u.m[e / 3][e % 3] = {a.x, a.y};
+      u.m[(e + 1) / 3][(e + 1) % 3] = {b.x, b.y};
+    }
+    reconstruct_row2(u);
+  }
+};
+
+}  // namespace cpsgpu

@@ -1,0 +1,119 @@
+// Launch configuration and template dispatch of the hop kernel (hop.cuh).
+#include <cstring>
+
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+#include "tune.h"
+
+namespace cpsgpu {
+
+namespace {
+
+using HopFn = void (*)(const HopParams, const HopViews, SolverScalars *, double *);
+
+template <int P, int RECON, int EP, int PR, int PX>
+HopFn get() {
+  return hop_kernel<P, RECON, EP, PR, PX>;
+}
+
+template <int P, int RECON>
+HopFn pick_ep(int ep, int pr, int px) {
+  constexpr int PXS = (P == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  switch (ep) {
+    case EP_STORE: return get<P, RECON, EP_STORE, P, P>();
+    case EP_AXPY: return get<P, RECON, EP_AXPY, P, P>();
+    case EP_MIX: return get<P, RECON, EP_MIX, P, P>();
+    case EP_MIX_AXPY: return get<P, RECON, EP_MIX_AXPY, P, P>();
+    case EP_CG:
+      if (pr == P && px == PXS) return get<P, RECON, EP_CG, P, PXS>();
+      break;
+    case EP_MIX_CG:
+      if (pr == P && px == PXS) return get<P, RECON, EP_MIX_CG, P, PXS>();
+      break;
+    case EP_RES:
+    case EP_MIX_RES:
+      if constexpr (P == PREC_DOUBLE) {
+        if (ep == EP_RES) {
+          if (pr == PREC_DOUBLE) return get<P, RECON, EP_RES, PREC_DOUBLE, P>();
+          if (pr == PREC_SINGLE) return get<P, RECON, EP_RES, PREC_SINGLE, P>();
+          if (pr == PREC_HALF) return get<P, RECON, EP_RES, PREC_HALF, P>();
+        } else {
+          if (pr == PREC_DOUBLE) return get<P, RECON, EP_MIX_RES, PREC_DOUBLE, P>();
+          if (pr == PREC_SINGLE) return get<P, RECON, EP_MIX_RES, PREC_SINGLE, P>();
+          if (pr == PREC_HALF) return get<P, RECON, EP_MIX_RES, PREC_HALF, P>();
+        }
+      }
+      break;
+  }
+  throw Error(-2, "hop: unsupported epilogue/precision combination");
+}
+
+HopFn pick(int prec, int recon, int ep, int pr, int px) {
+  if (prec == PREC_DOUBLE) return recon == 18 ? pick_ep<PREC_DOUBLE, 18>(ep, pr, px) : pick_ep<PREC_DOUBLE, 12>(ep, pr, px);
+  if (prec == PREC_SINGLE) return pick_ep<PREC_SINGLE, 12>(ep, pr, px);
+  return pick_ep<PREC_HALF, 12>(ep, pr, px);
+}
+
+size_t real_size(int prec) { return prec == PREC_DOUBLE ? 8 : 4; }
+
+}  // namespace
+
+void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
+                const SpinorView &x, const SpinorView &r, const SpinorView &sol, const SpinorView &p,
+                const SpinorView &b, SolverScalars *st) {
+  const Lattice &lat = *D.lat;
+  HopParams hp;
+  memset(&hp, 0, sizeof(hp));
+  for (int k = 0; k < 4; k++) {
+    hp.L[k] = lat.L[k];
+    hp.bc[k] = lat.bc[k];
+  }
+  hp.hx = lat.L[0] / 2;
+  hp.vh = lat.vh;
+  hp.ls = D.ls;
+  hp.cb = L.cb;
+  hp.dag = L.dag;
+  hp.dwf = (D.kind == KIND_DWF);
+  hp.h5 = 2.0;                 // 2 / a5, a5inv = 1
+  hp.h5wall = -2.0 * D.mass;   // -2 m_f / a5
+  for (int s = 0; s < D.ls && s < MAX_LS; s++) hp.coef[s] = L.coef.empty() ? 0.0 : L.coef[(size_t)s < L.coef.size() ? s : 0];
+  hp.mix = L.mix;
+  hp.norm = L.norm;
+  hp.red_op = L.red_op;
+  hp.gate = L.gate;
+
+  HopViews v;
+  v.U = lat.gauge(L.prec);
+  v.in = in;
+  v.out = out;
+  v.x = x;
+  v.r = r;
+  v.sol = sol;
+  v.p = p;
+  v.b = b;
+
+  const int recon = lat.recon(L.prec);
+  HopFn fn = pick(L.prec, recon, L.ep, L.pr, L.px);
+  const bool mix = ep_mix(L.ep);
+  TuneKey key{L.prec, recon, L.ep, D.kind, D.ls};
+  dim3 block = hop_block(key, mix);
+  dim3 grid((unsigned)((lat.vh + block.x - 1) / block.x), (unsigned)((D.ls + block.y - 1) / block.y),
+            (unsigned)in.nrhs);
+  size_t smem = 0;
+  if (mix) {
+    smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double);
+    static thread_local std::vector<std::pair<HopFn, size_t>> raised;
+    bool done = false;
+    for (auto &e : raised)
+      if (e.first == fn && e.second >= smem) done = true;
+    if (!done) {
+      CPSGPU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      raised.push_back({fn, smem});
+    }
+  }
+  fn<<<grid, block, smem, lat.stream>>>(hp, v, st, lat.partials.as<double>());
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+}
+
+}  // namespace cpsgpu

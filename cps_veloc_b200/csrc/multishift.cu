@@ -1,0 +1,300 @@
+// Multishift CG (DiracOp::MInvCG, minvcg.C:47-353), device resident.
+//
+// One iteration is: the M half of MatPcDagMatPc on p_0 (reducing <p,(A+m_0)p>,
+// whose last block runs the shifted z / beta recurrences for every shift),
+// the M^dagger half with the residual update r += b A p_0 and |r|^2 fused in
+// (last block: per-shift convergence), then one kernel that, per site, reads
+// r once and updates psi_s and p_s of every shift still running.  The
+// scalars never leave the device.
+//
+// precision CPSGPU_SINGLE runs the recurrences on FP32 vectors (solutions
+// accumulated in FP64) and then refines every shift with the
+// reliable-update CG on MatPcDagMatPc + shift_s to its own residual.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/cpsgpu.h"
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+#include "solver.h"
+
+namespace cpsgpu {
+
+namespace {
+
+template <int P> using RealT = typename PrecTraits<P>::real;
+
+// psi_s += w_s (-bs_s) p_s for shifts running at the start of the iteration,
+// then p_0 = r + a p_0, p_s = z_s r + as_s p_s for shifts still running.
+template <int P>
+__global__ void ms_update_kernel(SpinorView r, const SpinorView *pv, const SpinorView *psiv, SpinorView chi,
+                                 const MsScalars *ms, const SolverScalars *st, int use_chi) {
+  if (ms->upd_done_iter == ms->k) return;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const long per = r.vh * r.ls;
+  if (idx >= (size_t)per) return;
+  const long sl = (long)(idx / r.vh), i = (long)(idx % r.vh);
+  const int n = ms->nshift;
+  const bool single = (ms->type == 0);
+  const bool more = (st->done == 0);
+  RealT<P> rv[24];
+  SpinorIO<P>::load(r, sl, i, rv);
+  double acc0[24];
+  if (single) SpinorIO<PREC_DOUBLE>::load(psiv[0], sl, i, acc0);
+  double c[24];
+  if (use_chi) SpinorIO<PREC_DOUBLE>::load(chi, sl, i, c);
+  for (int s = 0; s < n; s++) {
+    const bool upd = !ms->conv_prev[s];
+    const bool adv = more && !ms->conv[s];
+    if (!upd && !adv) continue;
+    RealT<P> pp[24];
+    SpinorIO<P>::load(pv[s], sl, i, pp);
+    if (upd) {
+      const double f = -ms->bs[s] * ms->weight[s];
+      if (single) {
+#pragma unroll
+        for (int k = 0; k < 24; k++) acc0[k] += f * (use_chi ? c[k] : double(pp[k]));
+      } else {
+        double y[24];
+        SpinorIO<PREC_DOUBLE>::load(psiv[s], sl, i, y);
+#pragma unroll
+        for (int k = 0; k < 24; k++) y[k] += f * (use_chi ? c[k] : double(pp[k]));
+        SpinorIO<PREC_DOUBLE>::store(psiv[s], sl, i, y);
+      }
+    }
+    if (adv) {
+      const RealT<P> zr = (s == 0) ? RealT<P>(1) : RealT<P>(ms->z[ms->iz][s]);
+      const RealT<P> ap = (s == 0) ? RealT<P>(ms->a) : RealT<P>(ms->as[s]);
+#pragma unroll
+      for (int k = 0; k < 24; k++) pp[k] = zr * rv[k] + ap * pp[k];
+      SpinorIO<P>::store(pv[s], sl, i, pp);
+    }
+  }
+  if (single) SpinorIO<PREC_DOUBLE>::store(psiv[0], sl, i, acc0);
+}
+
+__global__ void ms_mark_kernel(MsScalars *ms) { ms->upd_done_iter = ms->k; }
+
+}  // namespace
+
+int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm, const double *shift, int nshift,
+           double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine) {
+  if (nshift > MS_MAX) throw Error(-1, "at most 64 shifts");
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  const int P = (precision == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  if (P != PREC_DOUBLE && L.recon_err > 1e-5) throw Error(-1, "sloppy multishift needs SU(3) links");
+  const long vh = L.vh;
+  const int ls = D.ls;
+  const size_t nreal = (size_t)24 * vh * ls;
+  // the sloppy path refines every shift, so it keeps individual solutions
+  const int dev_type = (P != PREC_DOUBLE && type == 0) ? 1 : type;
+  const int npsi = (dev_type == 0) ? 1 : nshift;
+
+  Field chi64(PREC_DOUBLE, vh, ls, 1), r(P, vh, ls, 1), tmp64(PREC_DOUBLE, vh, ls, 1);
+  std::vector<Field> p(nshift), psi(npsi);
+  for (int k = 0; k < nshift; k++) p[k].create(P, vh, ls, 1);
+  for (int k = 0; k < npsi; k++) psi[k].create(PREC_DOUBLE, vh, ls, 1);
+  OpWork w;
+  ensure_field(w.t1, P, vh, ls, 1);
+  ensure_field(w.t2, P, vh, ls, 1);
+  if (D.kind == KIND_MOBIUS) ensure_field(w.t0, P, vh, ls, 1);
+  size_t nblk = (size_t)((vh + 31) / 32) * ls + 1024;
+  L.partials.ensure(nblk * 2 * sizeof(double));
+
+  L.staging.ensure(nreal * sizeof(double));
+  CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, chi_h, nreal * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_import_fermion(s, PREC_DOUBLE, chi64.view(), L.staging.as<double>());
+  if (dev_type == 2) {
+    // GENERAL accumulates into the given solutions (only MULTI zeroes them)
+    for (int k = 0; k < npsi; k++) {
+      CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, psi_h[k], nreal * sizeof(double), cudaMemcpyHostToDevice, s));
+      launch_import_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+    }
+  } else {
+    for (int k = 0; k < npsi; k++) launch_zero(s, psi[k]);
+    if (type == 0 && dev_type == 0) {
+      CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, psi_h[0], nreal * sizeof(double), cudaMemcpyHostToDevice, s));
+      launch_import_fermion(s, PREC_DOUBLE, psi[0].view(), L.staging.as<double>());
+    }
+  }
+
+  DeviceBuffer stbuf(sizeof(SolverScalars)), msbuf(sizeof(MsScalars));
+  SolverScalars *st = stbuf.as<SolverScalars>();
+  MsScalars *msd = msbuf.as<MsScalars>();
+  SolverScalars st0;
+  memset(&st0, 0, sizeof(st0));
+  st0.shift = shift[0];
+  st0.ext = msd;
+
+  // r = chi (SINGLE / MULTI) or chi - A psi_0 (GENERAL); cp = |r|^2
+  double cp = chi_norm;
+  CPSGPU_CUDA(cudaMemcpyAsync(st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+  if (dev_type == 2) {
+    CgSolver tmp(D, PREC_DOUBLE);
+    tmp.setup(1);
+    CPSGPU_CUDA(cudaMemcpyAsync(tmp.b64.data.ptr, chi64.data.ptr, chi64.data.bytes, cudaMemcpyDeviceToDevice, s));
+    // A psi_0 without shift: residual chi - A psi_0 through the RES epilogue
+    SolverScalars z0 = st0;
+    z0.shift = 0.0;
+    SolverScalars *tst = tmp.st.as<SolverScalars>();
+    CPSGPU_CUDA(cudaMemcpyAsync(tst, &z0, sizeof(z0), cudaMemcpyHostToDevice, s));
+    tmp.emit_mdagm(PREC_DOUBLE, psi[0].view(), tmp.wd, EP_RES, 0, RED_STORE, GATE_NONE, tmp64.view(), PREC_DOUBLE,
+                   SpinorView(), PREC_DOUBLE);
+    SolverScalars h;
+    CPSGPU_CUDA(cudaMemcpyAsync(&h, tst, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    cp = h.sum[0];
+    launch_convert(s, P, r.view(), PREC_DOUBLE, tmp64.view());
+  } else {
+    launch_convert(s, P, r.view(), PREC_DOUBLE, chi64.view());
+  }
+  for (int k = 0; k < nshift; k++) launch_convert(s, P, p[k].view(), P, r.view());
+
+  MsScalars ms0;
+  memset(&ms0, 0, sizeof(ms0));
+  ms0.nshift = nshift;
+  ms0.first = 1;
+  ms0.type = dev_type;
+  ms0.max_iter = max_num_iter;
+  ms0.cp = cp;
+  ms0.c = cp;
+  ms0.upd_done_iter = -1;
+  for (int k = 0; k < nshift; k++) {
+    ms0.mass[k] = shift[k];
+    ms0.rsd_sq[k] = cp * rsdcg[k] * rsdcg[k];  // minvcg.C:134-137
+    ms0.weight[k] = (dev_type == 0) ? alpha[k] : 1.0;
+  }
+  CPSGPU_CUDA(cudaMemcpyAsync(msd, &ms0, sizeof(ms0), cudaMemcpyHostToDevice, s));
+
+  std::vector<SpinorView> pv(nshift), psiv(npsi);
+  for (int k = 0; k < nshift; k++) pv[k] = p[k].view();
+  for (int k = 0; k < npsi; k++) psiv[k] = psi[k].view();
+  DeviceBuffer pvd(sizeof(SpinorView) * nshift), psivd(sizeof(SpinorView) * npsi);
+  CPSGPU_CUDA(cudaMemcpyAsync(pvd.ptr, pv.data(), pvd.bytes, cudaMemcpyHostToDevice, s));
+  CPSGPU_CUDA(cudaMemcpyAsync(psivd.ptr, psiv.data(), psivd.bytes, cudaMemcpyHostToDevice, s));
+
+  // one iteration: M half (reduce <p,(A+m0)p>), M^dagger half with the
+  // residual update, then the per-shift vector updates.
+  auto iteration = [&](int use_chi) {
+    const bool mob = (D.kind == KIND_MOBIUS);
+    HopLaunch Lh;
+    Lh.prec = P;
+    Lh.gate = GATE_RUNNING;
+    Lh.dag = 0;
+    const SpinorView in = p[0].view();
+    if (mob) {
+      launch_mix(D, P, D.mixP.as<double>(), in, w.t0.view(), st, GATE_RUNNING);
+      Lh.ep = EP_MIX;
+      Lh.cb = 1;
+      Lh.mix = D.mixQ.as<double>();
+      launch_hop(D, Lh, w.t0.view(), w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(),
+                 SpinorView(), st);
+      Lh.mix = nullptr;
+      Lh.coef.assign(ls, -D.kappa);
+    } else {
+      Lh.ep = EP_STORE;
+      Lh.cb = 1;
+      launch_hop(D, Lh, in, w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
+      Lh.coef.assign(ls, -D.kappa * D.kappa);
+    }
+    Lh.ep = EP_AXPY;
+    Lh.cb = 0;
+    Lh.norm = 1;
+    Lh.red_op = RED_MS_PAP;
+    launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
+    Lh.norm = 0;
+    Lh.dag = 1;
+    Lh.cb = 1;
+    if (mob) {
+      Lh.ep = EP_MIX;
+      Lh.mix = D.mixR.as<double>();
+    } else {
+      Lh.ep = EP_STORE;
+    }
+    launch_hop(D, Lh, w.t2.view(), w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(),
+               SpinorView(), st);
+    Lh.cb = 0;
+    Lh.red_op = RED_MS_RR;
+    Lh.pr = P;
+    Lh.px = px_of(P);
+    if (mob) Lh.mix = D.mixS.as<double>();
+    Lh.ep = mob ? EP_MIX_CG : EP_CG;
+    launch_hop(D, Lh, w.t1.view(), SpinorView(), w.t2.view(), r.view(), SpinorView(), in, SpinorView(), st);
+    size_t per = (size_t)vh * ls;
+    if (P == PREC_DOUBLE)
+      ms_update_kernel<PREC_DOUBLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
+          r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
+    else
+      ms_update_kernel<PREC_SINGLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
+          r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
+    CPSGPU_CUDA(cudaGetLastError());
+    ms_mark_kernel<<<1, 1, 0, s>>>(msd);
+    CPSGPU_CUDA(cudaGetLastError());
+  };
+
+  iteration(1);  // the initial step of minvcg.C:140-188 (psi update from chi)
+  MsScalars mh;
+  SolverScalars sh;
+  const int chunk = 8;
+  for (int guard = 0; guard < max_num_iter / chunk + 4; guard++) {
+    CPSGPU_CUDA(cudaMemcpyAsync(&sh, st, sizeof(sh), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    if (sh.done) break;
+    for (int k = 0; k < chunk; k++) iteration(0);
+  }
+  CPSGPU_CUDA(cudaMemcpyAsync(&mh, msd, sizeof(mh), cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  // achieved residuals (minvcg.C:315-327)
+  for (int k = nshift - 1; k >= 0; k--) {
+    if (mh.conv[k])
+      rsdcg[k] = std::sqrt(mh.rsd_out[k]);
+    else
+      rsdcg[k] = std::sqrt(mh.c * mh.z[mh.iz][k] * mh.z[mh.iz][k]);
+  }
+  const int iters = mh.k + 1;
+
+  if (P != PREC_DOUBLE && refine) {
+    // FP64 refinement of every shift with the reliable-update CG
+    CgSolver cg(D, PREC_SINGLE);
+    cg.setup(1);
+    for (int k = 0; k < nshift; k++) {
+      CPSGPU_CUDA(cudaMemcpyAsync(cg.b64.data.ptr, chi64.data.ptr, chi64.data.bytes, cudaMemcpyDeviceToDevice, s));
+      CPSGPU_CUDA(cudaMemcpyAsync(cg.x64.data.ptr, psi[k].data.ptr, psi[k].data.bytes, cudaMemcpyDeviceToDevice, s));
+      CgArgs a;
+      a.stop_rsd = ms0.rsd_sq[k] > 0 ? std::sqrt(ms0.rsd_sq[k] / cp) : 1e-10;
+      a.max_num_iter = max_num_iter;
+      a.shift = shift[k];
+      a.src_norm_sq = 0.0;
+      std::vector<CgResult> res;
+      cg.run(a, res);
+      CPSGPU_CUDA(cudaMemcpyAsync(psi[k].data.ptr, cg.x64.data.ptr, psi[k].data.bytes, cudaMemcpyDeviceToDevice, s));
+      rsdcg[k] = res[0].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327 reports
+    }
+  }
+
+  // outputs
+  if (type == 0 && dev_type != 0) {
+    // SINGLE requested: psi_h[0] += sum_s alpha_s psi_s
+    std::vector<double> acc(nreal), tmp(nreal);
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    for (size_t q = 0; q < nreal; q++) acc[q] = psi_h[0][q];
+    for (int k = 0; k < nshift; k++) {
+      launch_export_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      CPSGPU_CUDA(cudaMemcpyAsync(tmp.data(), L.staging.ptr, nreal * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CPSGPU_CUDA(cudaStreamSynchronize(s));
+      for (size_t q = 0; q < nreal; q++) acc[q] += alpha[k] * tmp[q];
+    }
+    for (size_t q = 0; q < nreal; q++) psi_h[0][q] = acc[q];
+  } else {
+    for (int k = 0; k < npsi; k++) {
+      launch_export_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      CPSGPU_CUDA(cudaMemcpyAsync(psi_h[k], L.staging.ptr, nreal * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+  }
+  return iters;
+}
+
+}  // namespace cpsgpu

@@ -1,0 +1,320 @@
+// Even-odd preconditioned operators built from the fused hop kernel.
+//
+//   Wilson  MatPc  = 1 - kappa^2 D_oe D_eo              (wilson_m.C:49-93)
+//   DWF     MatPc  = 1 - kappa_5^2 D D, D = 4D + 5D hop   (dwf_m.C:31-63)
+//   Mobius  MatPc  = 1 - kappa_b D_4 M5^-1 kappa_b D_4 M5^-1   (SYM2,
+//           zmobius_m-sym2.h:5-127) and its dagger (zmobius_mdag-sym2.h)
+//
+// For Mobius every s-local factor between two hops (M5^-1, the b/c
+// mixing of zmobius_dslash_4, the kappa_b scalings) is folded into one Ls x
+// Ls matrix per chirality, precomputed here in FP64, so MatPc is
+//   out = in - kappa_b W0 ( Q W1 ( P in ) )        (3 kernels)
+//   MatPcDag: out = in + S W0^+ ( R W1^+ in )       (2 kernels)
+// where W is the plain Wilson hop of every slice.
+#include <cmath>
+#include <complex>
+#include <cstring>
+
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+
+namespace cpsgpu {
+
+using cd = std::complex<double>;
+
+// ---------------------------------------------------------------- lattice
+Lattice::Lattice(const int L_[4], const double bc_[4]) {
+  for (int k = 0; k < 4; k++) {
+    if (L_[k] <= 0 || (L_[k] & 1)) throw Error(-1, "lattice extents must be positive and even");
+    L[k] = L_[k];
+    bc[k] = bc_[k];
+  }
+  vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+  CPSGPU_CUDA(cudaGetDevice(&device));
+  CPSGPU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CPSGPU_CUDA(cudaMallocHost(&pinned, 64 * sizeof(double)));
+  scratch_st.alloc(sizeof(SolverScalars) * 4);
+  CPSGPU_CUDA(cudaMemsetAsync(scratch_st.ptr, 0, scratch_st.bytes, stream));
+}
+
+Lattice::~Lattice() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+  if (pinned) cudaFreeHost(pinned);
+}
+
+GaugeView Lattice::gauge(int prec) const {
+  GaugeView g;
+  g.vh = vh;
+  if (prec == PREC_DOUBLE)
+    g.data = use_recon12 ? gD12.ptr : gD18.ptr;
+  else if (prec == PREC_SINGLE)
+    g.data = gS12.ptr;
+  else
+    g.data = gH12.ptr;
+  return g;
+}
+
+// ---------------------------------------------------------------- Mobius matrices
+namespace {
+
+// Dense M5^-1 as the reference's recurrences apply it (zmobius_m5inv.C
+// :247-396 for dag 0, :534-679 for dag 1): the same scalar recurrence along
+// s for every site and component, run here on the unit vectors.
+void m5inv_columns(int ls, const std::vector<cd> &K, double mass, int dag, std::vector<cd> &up,
+                   std::vector<cd> &dn) {
+  up.assign((size_t)ls * ls, 0.0);
+  dn.assign((size_t)ls * ls, 0.0);
+  cd inv_d_last, prod = 1.0;
+  if (!dag) {
+    for (int s = 0; s < ls; s++) prod *= -K[s];
+    inv_d_last = 1.0 / (1.0 + prod * mass);
+  } else {
+    for (int s = 0; s < ls; s++) prod *= K[s];
+    inv_d_last = std::conj(1.0 / (1.0 + prod * mass));
+  }
+  std::vector<cd> v(ls), w(ls);
+  for (int col = 0; col < ls; col++) {
+    for (int s = 0; s < ls; s++) v[s] = w[s] = (s == col) ? 1.0 : 0.0;
+    if (!dag) {
+      w[ls - 1] *= inv_d_last;
+      cd fl = K[ls - 1] * mass * inv_d_last;
+      for (int s = 0; s + 1 < ls; s++) {
+        v[s + 1] += -K[s + 1] * v[s];
+        w[ls - 1] += fl * w[s];
+        fl *= -K[s];
+      }
+      cd p = 1.0;
+      for (int s = 0; s < ls - 1; s++) p *= -K[s];
+      cd fr = -p * mass * inv_d_last;
+      for (int s = ls - 2; s >= 0; s--) {
+        v[s] += fr * v[ls - 1];
+        w[s] += -K[s] * w[s + 1];
+        fr /= -K[s];
+      }
+      v[ls - 1] *= inv_d_last;
+    } else {
+      v[ls - 1] *= inv_d_last;
+      cd fr = std::conj(K[0]) * mass * inv_d_last;
+      for (int s = 0; s + 1 < ls; s++) {
+        v[ls - 1] += fr * v[s];
+        w[s + 1] += -std::conj(K[s]) * w[s];
+        fr *= -std::conj(K[s + 1]);
+      }
+      cd p = 1.0;
+      for (int s = 0; s < ls - 2; s++) p *= -K[s];
+      p *= -K[ls - 1];
+      cd fl = -std::conj(p) * mass * inv_d_last;
+      for (int s = ls - 2; s >= 0; s--) {
+        v[s] += -std::conj(K[s + 1]) * v[s + 1];
+        w[s] += fl * w[ls - 1];
+        if (s > 0) fl /= -std::conj(K[s - 1]);
+      }
+      w[ls - 1] *= inv_d_last;
+    }
+    for (int s = 0; s < ls; s++) {
+      up[(size_t)s * ls + col] = v[s];
+      dn[(size_t)s * ls + col] = w[s];
+    }
+  }
+}
+
+// b/c mixing of zmobius_dslash_4 (dag 0): b_s psi(s) + c-weighted fifth-
+// direction hop with -m_f at the walls (zmobius_dslash_5_plus.C:125-374).
+void bmix(int ls, const std::vector<cd> &b, const std::vector<cd> &c, double mass, std::vector<cd> &up,
+          std::vector<cd> &dn) {
+  up.assign((size_t)ls * ls, 0.0);
+  dn.assign((size_t)ls * ls, 0.0);
+  for (int s = 0; s < ls; s++) {
+    up[(size_t)s * ls + s] += b[s];
+    dn[(size_t)s * ls + s] += b[s];
+    if (s == 0) up[(size_t)s * ls + ls - 1] += -mass * c[0];
+    else up[(size_t)s * ls + s - 1] += c[s];
+    if (s == ls - 1) dn[(size_t)s * ls + 0] += -mass * c[ls - 1];
+    else dn[(size_t)s * ls + s + 1] += c[s];
+  }
+}
+
+std::vector<cd> matmul(int n, const std::vector<cd> &a, const std::vector<cd> &b) {
+  std::vector<cd> r((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++)
+      for (int j = 0; j < n; j++) r[(size_t)i * n + j] += a[(size_t)i * n + k] * b[(size_t)k * n + j];
+  return r;
+}
+std::vector<cd> adjoint(int n, const std::vector<cd> &a) {
+  std::vector<cd> r((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) r[(size_t)i * n + j] = std::conj(a[(size_t)j * n + i]);
+  return r;
+}
+std::vector<cd> diag_left(int n, const std::vector<cd> &d, const std::vector<cd> &a) {
+  std::vector<cd> r(a);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) r[(size_t)i * n + j] *= d[i];
+  return r;
+}
+std::vector<cd> diag_right(int n, const std::vector<cd> &a, const std::vector<cd> &d) {
+  std::vector<cd> r(a);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) r[(size_t)i * n + j] *= d[j];
+  return r;
+}
+
+// pack [upper; lower] real parts (real b, c give real matrices)
+std::vector<double> pack(int n, const std::vector<cd> &up, const std::vector<cd> &dn) {
+  std::vector<double> r(2 * (size_t)n * n);
+  for (size_t k = 0; k < (size_t)n * n; k++) {
+    r[k] = up[k].real();
+    r[(size_t)n * n + k] = dn[k].real();
+  }
+  return r;
+}
+
+void upload(DeviceBuffer &buf, const std::vector<double> &h) {
+  buf.alloc(h.size() * sizeof(double));
+  CPSGPU_CUDA(cudaMemcpy(buf.ptr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+}  // namespace
+
+Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_)
+    : lat(l), kind(kind_), ls(ls_), mass(mass_), m5(m5_), b(b_), c(c_), kappa(0), kappa_c(0) {
+  if (kind == KIND_WILSON) {
+    ls = 1;
+    kappa = 1.0 / (2.0 * (mass + 4.0));  // d_op_wilson.C:134-137
+    return;
+  }
+  if (ls < 2 || ls > MAX_LS) throw Error(-1, "Ls must be in [2, 32]");
+  if (kind == KIND_DWF) {
+    kappa = 1.0 / (2.0 * (4.0 + 1.0 - m5));  // dwf_init.C:97-98, a5inv = 1
+    return;
+  }
+  // Mobius: d_op_mobius.C:112-131
+  kappa = 1.0 / (2.0 * (b * (4.0 - m5) + 1.0));
+  kappa_c = 1.0 / (2.0 * (c * (4.0 - m5) - 1.0));
+  std::vector<cd> bv(ls, b), cv(ls, c), kb(ls, kappa), K(ls, kappa / kappa_c);
+  std::vector<cd> m0u, m0d, m1u, m1d, bu, bd;
+  m5inv_columns(ls, K, mass, 0, m0u, m0d);
+  m5inv_columns(ls, K, mass, 1, m1u, m1d);
+  bmix(ls, bv, cv, mass, bu, bd);
+  std::vector<cd> bdu = adjoint(ls, bu), bdd = adjoint(ls, bd);
+  std::vector<cd> mkb(ls);
+  for (int s = 0; s < ls; s++) mkb[s] = -std::conj(kb[s]);
+  std::vector<cd> ckb(ls);
+  for (int s = 0; s < ls; s++) ckb[s] = std::conj(kb[s]);
+  // P = B M5inv ; Q = B M5inv kappa_b
+  std::vector<cd> Pu = matmul(ls, bu, m0u), Pd = matmul(ls, bd, m0d);
+  std::vector<cd> Qu = diag_right(ls, Pu, kb), Qd = diag_right(ls, Pd, kb);
+  // S = M5inv^+ B^+ ; R = conj(kappa_b) S (-conj(kappa_b))
+  std::vector<cd> Su = matmul(ls, m1u, bdu), Sd = matmul(ls, m1d, bdd);
+  std::vector<cd> Ru = diag_right(ls, diag_left(ls, ckb, Su), mkb), Rd = diag_right(ls, diag_left(ls, ckb, Sd), mkb);
+  hM5i = pack(ls, m0u, m0d);
+  hM5id = pack(ls, m1u, m1d);
+  hB = pack(ls, bu, bd);
+  hBd = pack(ls, bdu, bdd);
+  upload(mixP, pack(ls, Pu, Pd));
+  upload(mixQ, pack(ls, Qu, Qd));
+  upload(mixR, pack(ls, Ru, Rd));
+  upload(mixS, pack(ls, Su, Sd));
+  upload(mixB, hB);
+  upload(mixBd, hBd);
+  upload(mixM5i, hM5i);
+  upload(mixM5id, hM5id);
+}
+
+// ---------------------------------------------------------------- operators
+static SpinorView none() { return SpinorView(); }
+
+void op_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag) {
+  HopLaunch L;
+  L.prec = prec;
+  L.ep = EP_STORE;
+  L.cb = cb;
+  L.dag = dag;
+  launch_hop(D, L, in, out, none(), none(), none(), none(), none(), nullptr);
+}
+
+void op_mobius_dslash4(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
+                       OpWork &w) {
+  if (D.kind != KIND_MOBIUS) throw Error(-1, "dslash_4: not a Mobius operator");
+  if (!dag) {
+    ensure_field(w.t0, prec, D.lat->vh, D.ls, in.nrhs);
+    launch_mix(D, prec, D.mixB.as<double>(), in, w.t0.view());
+    op_dslash(D, prec, out, w.t0.view(), cb, 0);
+  } else {
+    HopLaunch L;
+    L.prec = prec;
+    L.ep = EP_MIX;
+    L.cb = cb;
+    L.dag = 1;
+    L.mix = D.mixBd.as<double>();
+    launch_hop(D, L, in, out, none(), none(), none(), none(), none(), nullptr);
+  }
+}
+
+void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag) {
+  if (D.kind != KIND_MOBIUS) throw Error(-1, "m5inv: not a Mobius operator");
+  launch_mix(D, prec, dag ? D.mixM5id.as<double>() : D.mixM5i.as<double>(), in, out);
+}
+
+// out = MatPc in (dag = 0) or MatPc^+ in (dag = 1).  With norm, the last
+// kernel reduces |out|^2 and |in|^2 into st with red_op.
+void op_matpc(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag, OpWork &w,
+              SolverScalars *st, int norm, int red_op) {
+  const Lattice &lat = *D.lat;
+  ensure_field(w.t1, prec, lat.vh, D.ls, in.nrhs);
+  HopLaunch L;
+  L.prec = prec;
+  L.dag = dag;
+  if (D.kind != KIND_MOBIUS) {
+    L.ep = EP_STORE;
+    L.cb = 1;
+    launch_hop(D, L, in, w.t1.view(), none(), none(), none(), none(), none(), st);
+    L.ep = EP_AXPY;
+    L.cb = 0;
+    L.coef.assign(D.ls, -D.kappa * D.kappa);
+    L.norm = norm;
+    L.red_op = red_op;
+    launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
+    return;
+  }
+  if (!dag) {
+    ensure_field(w.t0, prec, lat.vh, D.ls, in.nrhs);
+    launch_mix(D, prec, D.mixP.as<double>(), in, w.t0.view());
+    L.ep = EP_MIX;
+    L.cb = 1;
+    L.mix = D.mixQ.as<double>();
+    launch_hop(D, L, w.t0.view(), w.t1.view(), none(), none(), none(), none(), none(), st);
+    L.ep = EP_AXPY;
+    L.cb = 0;
+    L.mix = nullptr;
+    L.coef.assign(D.ls, -D.kappa);
+    L.norm = norm;
+    L.red_op = red_op;
+    launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
+  } else {
+    L.ep = EP_MIX;
+    L.cb = 1;
+    L.mix = D.mixR.as<double>();
+    launch_hop(D, L, in, w.t1.view(), none(), none(), none(), none(), none(), st);
+    L.ep = EP_MIX_AXPY;
+    L.cb = 0;
+    L.mix = D.mixS.as<double>();
+    L.norm = norm;
+    L.red_op = red_op;
+    launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
+  }
+}
+
+// out = MatPc^+ MatPc in; st->sum[0] = |MatPc in|^2 (the reference's dot).
+void op_mdagm(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, OpWork &w, SolverScalars *st,
+              int red_op_dot) {
+  ensure_field(w.t2, prec, D.lat->vh, D.ls, in.nrhs);
+  op_matpc(D, prec, w.t2.view(), in, 0, w, st, st ? 1 : 0, red_op_dot);
+  op_matpc(D, prec, out, w.t2.view(), 1, w, st, 0, 0);
+}
+
+}  // namespace cpsgpu

@@ -1,0 +1,271 @@
+// Device-resident Krylov solvers on MatPcDagMatPc.
+//
+//   cg_solve  CG of DiracOp::InvCgShift (inv_cg.C:84-448), same stop test
+//             |r|^2 <= stop_rsd^2 |b|^2, same iteration bookkeeping (returns
+//             itr + 1) and the true residual recomputed in FP64 at the end.
+//             With a sloppy precision (FP32 or FP16 + per-site norm) it runs
+//             as a reliable-update mixed-precision CG: the Krylov iteration
+//             in the sloppy precision, the solution accumulated in FP64 at
+//             every reliable update, where the FP64 true residual b - A x
+//             replaces the iterated one and decides convergence.  Every
+//             global reduction is done in FP64.
+//
+// One CG iteration is a fixed sequence of kernels, all of which read their
+// scalars (alpha, beta, stop flags) from device memory and return at once
+// when the solve is finished, so the host enqueues iterations in chunks
+// (captured once as a CUDA graph) and only polls a pinned flag between
+// chunks, one chunk behind, so the GPU never waits for the host.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+#include "solver.h"
+
+namespace cpsgpu {
+
+namespace {
+SpinorView none() { return SpinorView(); }
+}  // namespace
+
+void CgSolver::setup(int nrhs_) {
+  Lattice &L = *D.lat;
+  nrhs = nrhs_;
+  const long vh = L.vh;
+  const int ls = D.ls;
+  ensure_field(b64, PREC_DOUBLE, vh, ls, nrhs);
+  ensure_field(x64, PREC_DOUBLE, vh, ls, nrhs);
+  ensure_field(r, sloppy, vh, ls, nrhs);
+  ensure_field(p, sloppy, vh, ls, nrhs);
+  const int px = (sloppy == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  if (sloppy != PREC_DOUBLE) {
+    ensure_field(xs, px, vh, ls, nrhs);
+    ensure_field(rtmp, PREC_DOUBLE, vh, ls, nrhs);
+  }
+  ensure_field(ws.t1, sloppy, vh, ls, nrhs);
+  ensure_field(ws.t2, sloppy, vh, ls, nrhs);
+  if (D.kind == KIND_MOBIUS) ensure_field(ws.t0, sloppy, vh, ls, nrhs);
+  ensure_field(wd.t1, PREC_DOUBLE, vh, ls, nrhs);
+  ensure_field(wd.t2, PREC_DOUBLE, vh, ls, nrhs);
+  if (D.kind == KIND_MOBIUS) ensure_field(wd.t0, PREC_DOUBLE, vh, ls, nrhs);
+  st.ensure(sizeof(SolverScalars) * nrhs);
+  // partials: 2 values per block; the smallest hop block is 32 threads
+  size_t nblk = (size_t)((vh + 31) / 32) * ls + 1024;
+  L.partials.ensure(nblk * 2 * nrhs * sizeof(double));
+  drop_graph();
+}
+
+void CgSolver::drop_graph() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
+  graph_exec = nullptr;
+  graph = nullptr;
+}
+
+CgSolver::~CgSolver() { drop_graph(); }
+
+// Emit out-of-place MatPcDagMatPc on `in` with a final epilogue.
+//   final == EP_CG: r -= alpha A in; sol += alpha in; RED_CG_RR
+//   final == EP_RES: r_out = b - A in; reduce with red_op
+// The M half reduces |M in|^2 (RED_PAP) when pap is set.
+void CgSolver::emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_ep, int pap, int red_op, int gate,
+                          const SpinorView &rv, int pr, const SpinorView &solv, int px) {
+  SolverScalars *stp = st.as<SolverScalars>();
+  const bool mob = (D.kind == KIND_MOBIUS);
+  HopLaunch Lh;
+  Lh.prec = prec;
+  Lh.gate = gate;
+  // ---- M = MatPc ----
+  Lh.dag = 0;
+  if (mob) {
+    launch_mix(D, prec, D.mixP.as<double>(), in, w.t0.view(), stp, gate);
+    Lh.ep = EP_MIX;
+    Lh.cb = 1;
+    Lh.mix = D.mixQ.as<double>();
+    launch_hop(D, Lh, w.t0.view(), w.t1.view(), none(), none(), none(), none(), none(), stp);
+    Lh.mix = nullptr;
+    Lh.coef.assign(D.ls, -D.kappa);
+  } else {
+    Lh.ep = EP_STORE;
+    Lh.cb = 1;
+    launch_hop(D, Lh, in, w.t1.view(), none(), none(), none(), none(), none(), stp);
+    Lh.coef.assign(D.ls, -D.kappa * D.kappa);
+  }
+  Lh.ep = EP_AXPY;
+  Lh.cb = 0;
+  Lh.norm = pap;
+  Lh.red_op = RED_PAP;
+  launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, none(), none(), none(), none(), stp);
+  // ---- M^dagger ----
+  Lh.norm = 0;
+  Lh.dag = 1;
+  Lh.cb = 1;
+  if (mob) {
+    Lh.ep = EP_MIX;
+    Lh.mix = D.mixR.as<double>();
+  } else {
+    Lh.ep = EP_STORE;
+  }
+  launch_hop(D, Lh, w.t2.view(), w.t1.view(), none(), none(), none(), none(), none(), stp);
+  Lh.cb = 0;
+  Lh.red_op = red_op;
+  Lh.pr = pr;
+  Lh.px = px;
+  if (mob) Lh.mix = D.mixS.as<double>();
+  if (final_ep == EP_CG) {
+    Lh.ep = mob ? EP_MIX_CG : EP_CG;
+    launch_hop(D, Lh, w.t1.view(), none(), w.t2.view(), rv, solv, in, none(), stp);
+  } else {
+    Lh.ep = mob ? EP_MIX_RES : EP_RES;
+    launch_hop(D, Lh, w.t1.view(), none(), w.t2.view(), rv, in, none(), b64.view(), stp);
+  }
+}
+
+void CgSolver::emit_iteration() {
+  Lattice &L = *D.lat;
+  const int px = (sloppy == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  SolverScalars *stp = st.as<SolverScalars>();
+  const SpinorView solv = (sloppy == PREC_DOUBLE) ? x64.view() : xs.view();
+  emit_mdagm(sloppy, p.view(), ws, EP_CG, 1, RED_CG_RR, GATE_RUNNING, r.view(), sloppy, solv, px);
+  if (sloppy != PREC_DOUBLE) {
+    // reliable update (kernels return at once unless one is pending)
+    launch_accum_reliable(L.stream, x64.view(), px, xs.view(), stp, nrhs, 0);
+    emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_RELIABLE, GATE_RELIABLE, r.view(), sloppy, none(),
+               PREC_DOUBLE);
+  }
+  launch_xpay(L.stream, sloppy, p.view(), r.view(), stp, nrhs);
+}
+
+// Poll the done flags of all right-hand sides (pinned copy issued earlier).
+static bool all_done(const int *flags, int n) {
+  for (int k = 0; k < n; k++)
+    if (flags[k] == 0) return false;
+  return true;
+}
+
+void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  SolverScalars *stp = st.as<SolverScalars>();
+  if (sloppy != PREC_DOUBLE && L.recon_err > 1e-5)
+    throw Error(-1, "mixed precision needs SU(3) links (12-real reconstruction failed)");
+  const long long k0 = launch_counter();
+  cudaEvent_t tev0, tev1;
+  CPSGPU_CUDA(cudaEventCreate(&tev0));
+  CPSGPU_CUDA(cudaEventCreate(&tev1));
+  CPSGPU_CUDA(cudaEventRecord(tev0, s));
+
+  // |b|^2 per right-hand side
+  launch_init_scalars(s, stp, nrhs, SolverScalars{});
+  launch_norm(s, PREC_DOUBLE, b64.view(), stp, L.partials.as<double>(), RED_STORE, GATE_NONE);
+  std::vector<SolverScalars> host(nrhs);
+  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  std::vector<SolverScalars> init(nrhs);
+  for (int k = 0; k < nrhs; k++) {
+    SolverScalars z;
+    memset(&z, 0, sizeof(z));
+    double bn = host[k].sum[0];
+    z.src_norm = (a.src_norm_sq > 0) ? a.src_norm_sq : bn;
+    z.stop = z.src_norm * a.stop_rsd * a.stop_rsd;
+    z.max_iter = a.max_num_iter - 1;  // inv_cg.C:275
+    z.shift = a.shift;
+    z.delta2 = (sloppy == PREC_DOUBLE) ? 0.0 : a.delta * a.delta;
+    init[k] = z;
+  }
+  CPSGPU_CUDA(cudaMemcpyAsync(stp, init.data(), sizeof(SolverScalars) * nrhs, cudaMemcpyHostToDevice, s));
+
+  // r = b - A x0 (FP64), p = r
+  Field &rinit = (sloppy == PREC_DOUBLE) ? r : rtmp;
+  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_INIT, GATE_NONE, rinit.view(), PREC_DOUBLE, none(),
+             PREC_DOUBLE);
+  if (sloppy != PREC_DOUBLE) {
+    launch_convert(s, sloppy, r.view(), PREC_DOUBLE, rtmp.view());
+    launch_zero(s, xs);
+  }
+  launch_convert(s, sloppy, p.view(), sloppy, r.view());
+
+  // iterate in chunks
+  const int chunk = a.chunk > 0 ? a.chunk : 8;
+  if (graph_exec && graph_chunk != chunk) drop_graph();
+  if (a.use_graph && !graph_exec) {
+    const long long c0 = launch_counter();
+    CPSGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    try {
+      for (int k = 0; k < chunk; k++) emit_iteration();
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CPSGPU_CUDA(cudaStreamEndCapture(s, &graph));
+    CPSGPU_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+    graph_kernels = launch_counter() - c0;
+    graph_chunk = chunk;
+  }
+  long long replayed = 0;
+  int *flags = reinterpret_cast<int *>(L.pinned);  // [2][nrhs] ring
+  if (nrhs * 2 > 64 * 2) throw Error(-1, "too many right-hand sides for the poll buffer");
+  cudaEvent_t ev[2];
+  CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  const long max_chunks = (long)a.max_num_iter / chunk + 4;
+  long launched = 0;
+  int slot = 0;
+  bool finished = false;
+  for (long c = 0; c < max_chunks && !finished; c++) {
+    if (graph_exec) {
+      CPSGPU_CUDA(cudaGraphLaunch(graph_exec, s));
+      replayed += graph_kernels;
+    } else
+      for (int k = 0; k < chunk; k++) emit_iteration();
+    for (int k = 0; k < nrhs; k++)
+      CPSGPU_CUDA(cudaMemcpyAsync(flags + slot * nrhs + k, &stp[k].done, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaEventRecord(ev[slot], s));
+    launched++;
+    if (launched >= 2) {
+      // look at the chunk before this one while this one runs
+      int prev = 1 - slot;
+      CPSGPU_CUDA(cudaEventSynchronize(ev[prev]));
+      if (all_done(flags + prev * nrhs, nrhs)) finished = true;
+    }
+    slot = 1 - slot;
+  }
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+
+  // final solution and true residual in FP64 (inv_cg.C:403-415)
+  if (sloppy != PREC_DOUBLE) launch_accum_reliable(s, x64.view(), px_of(sloppy), xs.view(), stp, nrhs, 1);
+  ensure_field(rtmp, PREC_DOUBLE, L.vh, D.ls, nrhs);
+  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  std::vector<SolverScalars> fin = host;
+  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_STORE, GATE_NONE, rtmp.view(), PREC_DOUBLE, none(),
+             PREC_DOUBLE);
+  CPSGPU_CUDA(cudaEventRecord(tev1, s));
+  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  float dev_ms = 0.f;
+  CPSGPU_CUDA(cudaEventElapsedTime(&dev_ms, tev0, tev1));
+  cudaEventDestroy(tev0);
+  cudaEventDestroy(tev1);
+  const long long kernels = launch_counter() - k0 + replayed;
+  res.resize(nrhs);
+  for (int k = 0; k < nrhs; k++) {
+    CgResult &o = res[k];
+    o.iterations = fin[k].iter + 1;
+    o.status = fin[k].done ? fin[k].done : ST_MAX_ITER;
+    o.true_res = std::sqrt(host[k].sum[0] / fin[k].src_norm);
+    o.reliable_updates = fin[k].n_reliable;
+    o.seconds = dev_ms * 1e-3;
+    o.final_rr = fin[k].rr;
+    o.kernels = kernels;
+  }
+}
+
+int px_of(int sloppy) { return sloppy == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE; }
+
+}  // namespace cpsgpu

@@ -1,0 +1,57 @@
+// Krylov solvers (solver.cu, multishift.cu).
+#pragma once
+#include <vector>
+
+#include "cpsgpu_impl.h"
+
+namespace cpsgpu {
+
+struct CgArgs {
+  double stop_rsd = 1e-8;
+  int max_num_iter = 10000;
+  double src_norm_sq = 0.0;  // 0: computed from the source (inv_cg.C:166-169)
+  double shift = 0.0;
+  double delta = 0.1;        // reliable-update threshold (mixed precision)
+  int chunk = 8;             // iterations per captured graph
+  int use_graph = 1;
+};
+
+struct CgResult {
+  int iterations = 0;        // reference convention: iterations done + 1
+  int status = 0;
+  double true_res = 0.0;     // |b - A x| / |b|
+  int reliable_updates = 0;
+  double seconds = 0.0;
+  double final_rr = 0.0;
+  long long kernels = 0;     // kernels executed (early-exit ones included)
+};
+
+int px_of(int sloppy);
+
+// Solves (MatPcDagMatPc + shift) x = b for nrhs right-hand sides at once
+// (each with its own scalars and convergence) in precision `sloppy`
+// (PREC_DOUBLE: plain FP64 CG).  b64 and x64 (initial guess in, solution
+// out) are filled by the caller.
+struct CgSolver {
+  Dirac &D;
+  int sloppy;
+  int nrhs = 0;
+  Field b64, x64, r, p, xs, rtmp;
+  OpWork ws, wd;
+  DeviceBuffer st;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long graph_kernels = 0;
+  int graph_chunk = 0;
+
+  CgSolver(Dirac &d, int sloppy_prec) : D(d), sloppy(sloppy_prec) {}
+  ~CgSolver();
+  void setup(int nrhs);
+  void run(const CgArgs &a, std::vector<CgResult> &res);
+  void drop_graph();
+  void emit_iteration();
+  void emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_ep, int pap, int red_op, int gate,
+                  const SpinorView &rv, int pr, const SpinorView &solv, int px);
+};
+
+}  // namespace cpsgpu

@@ -1,0 +1,243 @@
+"""Python mirror of the reference's operator and solver interface for the
+fermion-solve hot path, on top of the C ABI.
+
+Names and argument meanings follow the reference's C++ classes so callers
+(and the parity tests) read like CPS code:
+
+  Lattice            geometry + resident gauge field (GJP geometry, the
+                     Lattice gauge field, BondCond as a per-direction sign)
+  DiracOpWilson      d_op_wilson.C: Dslash, MatPc, MatPcDag, MatPcDagMatPc,
+                     InvCg, MInvCG
+  DiracOpDwf         d_op_dwf.C: same set on the 5D-preconditioned field
+  DiracOpMobius      d_op_mobius.C: same set (SYM2), plus Dslash4 / M5inv
+
+Vectors are numpy float64 arrays in CPS storage order (include/cpsgpu.h).
+Errors raise CpsGpuError instead of exiting the process as ERR.General does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi as A
+from ._abi import check, dptr, lib
+
+
+def gen_gauge(node_sites, seed: int = 20261203, width: float = 0.3) -> np.ndarray:
+    """Seeded SU(3) field U = exp(i width H), WILSON order, no boundary signs."""
+    vol = int(np.prod(node_sites))
+    u = np.empty(vol * 4 * 18)
+    check(lib().cpsgpu_gen_gauge(A.ints(node_sites), seed, width, dptr(u)))
+    return u
+
+
+def gen_gaussian(n: int, seed: int = 20261203, stream: int = 0) -> np.ndarray:
+    out = np.empty(n)
+    check(lib().cpsgpu_gen_gaussian(dptr(out), n, seed, stream))
+    return out
+
+
+class Lattice:
+    def __init__(self, node_sites, bc=(1, 1, 1, -1)):
+        self.node_sites = tuple(int(x) for x in node_sites)
+        self.bc = tuple(int(b) for b in bc)
+        self.vol = int(np.prod(self.node_sites))
+        h = C.c_void_p()
+        check(lib().cpsgpu_lattice_create(A.ints(self.node_sites), A.ints(self.bc), C.byref(h)))
+        self._h = h
+
+    def import_gauge(self, u: np.ndarray, signs_applied: bool = False) -> None:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.size != self.vol * 72:
+            raise ValueError("gauge field must hold vol*4*18 reals")
+        check(lib().cpsgpu_import_gauge(self._h, dptr(u), 1 if signs_applied else 0))
+
+    def gauge_info(self):
+        e = C.c_double()
+        r = C.c_int()
+        check(lib().cpsgpu_gauge_info(self._h, C.byref(e), C.byref(r)))
+        return e.value, bool(r.value)
+
+    def synchronize(self):
+        check(lib().cpsgpu_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cpsgpu_lattice_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class CgResult:
+    iterations: int
+    status: int
+    true_res: float
+    reliable_updates: int
+    seconds: float
+    kernels: int = 0
+
+
+class _DiracOp:
+    kind = A.WILSON
+
+    def __init__(self, lat: Lattice, mass: float, ls: int = 1, m5: float = 1.8, b: float = 1.0, c: float = 0.0):
+        self.lat = lat
+        arg = A.DiracArg(self.kind, ls, mass, m5, b, c)
+        h = C.c_void_p()
+        check(lib().cpsgpu_dirac_create(lat._h, C.byref(arg), C.byref(h)))
+        self._h = h
+        self.ls = ls if self.kind != A.WILSON else 1
+        self.mass = mass
+        k, kc = C.c_double(), C.c_double()
+        check(lib().cpsgpu_dirac_info(h, C.byref(k), C.byref(kc)))
+        self.kappa, self.kappa_c = k.value, kc.value
+
+    @property
+    def f_size(self) -> int:
+        """reals in one preconditioned vector (InvCgShift's f_size_cb)"""
+        return 24 * self.ls * self.lat.vol // 2
+
+    def _vec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != self.f_size:
+            raise ValueError(f"vector must hold {self.f_size} reals")
+        return x
+
+    def Dslash(self, inp, cb: int, dag: int = 0, prec: int = A.DOUBLE) -> np.ndarray:
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_dslash(self._h, dptr(out), dptr(inp), cb, dag, prec))
+        return out
+
+    def MatPc(self, inp, prec: int = A.DOUBLE) -> np.ndarray:
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_matpc(self._h, dptr(out), dptr(inp), 0, prec))
+        return out
+
+    def MatPcDag(self, inp, prec: int = A.DOUBLE) -> np.ndarray:
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_matpc(self._h, dptr(out), dptr(inp), 1, prec))
+        return out
+
+    def MatPcDagMatPc(self, inp, prec: int = A.DOUBLE):
+        """returns (M^+ M in, |M in|^2) as DiracOp::MatPcDagMatPc(out, in, &dot)"""
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        dot = C.c_double()
+        check(lib().cpsgpu_matpc_dag_matpc(self._h, dptr(out), dptr(inp), C.byref(dot), prec))
+        return out, dot.value
+
+    def _cg_arg(self, stop_rsd, max_num_iter, src_norm_sq, shift, precision, delta, chunk, use_graph):
+        a = A.CgArg()
+        lib().cpsgpu_cg_arg_default(C.byref(a))
+        a.stop_rsd = stop_rsd
+        a.max_num_iter = max_num_iter
+        a.src_norm_sq = src_norm_sq
+        a.shift = shift
+        a.precision = precision
+        a.delta = delta
+        a.chunk = chunk
+        a.use_graph = 1 if use_graph else 0
+        return a
+
+    def InvCg(self, sol, src, stop_rsd=1e-8, max_num_iter=10000, src_norm_sq=0.0, shift=0.0,
+              precision=A.DOUBLE, delta=0.1, chunk=8, use_graph=True) -> CgResult:
+        """DiracOp::InvCg(out, in, src_norm_sq, true_res): sol is the initial guess, updated in place."""
+        src = self._vec(src)
+        if not (isinstance(sol, np.ndarray) and sol.dtype == np.float64 and sol.flags.c_contiguous):
+            raise TypeError("sol must be a C-contiguous float64 array (updated in place)")
+        self._vec(sol)
+        a = self._cg_arg(stop_rsd, max_num_iter, src_norm_sq, shift, precision, delta, chunk, use_graph)
+        r = A.CgResult()
+        check(lib().cpsgpu_invcg(self._h, dptr(sol), dptr(src), C.byref(a), C.byref(r)))
+        return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
+
+    def InvCgMulti(self, sols, srcs, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.1,
+                   chunk=8, use_graph=True):
+        n = len(srcs)
+        srcs = [self._vec(s) for s in srcs]
+        for s in sols:
+            self._vec(s)
+        sp = (A._dp * n)(*[dptr(s) for s in sols])
+        bp = (A._dp * n)(*[dptr(s) for s in srcs])
+        a = self._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, precision, delta, chunk, use_graph)
+        res = (A.CgResult * n)()
+        check(lib().cpsgpu_invcg_multi(self._h, sp, bp, n, C.byref(a), res))
+        return [CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels) for r in res]
+
+    def MInvCG(self, psi, chi, chi_norm, shifts, rsdcg, type=A.MS_MULTI, alpha=None, max_num_iter=10000,
+               precision=A.DOUBLE, refine=True):
+        """DiracOp::MInvCG: psi list updated in place; rsdcg (np array) overwritten; returns k."""
+        chi = self._vec(chi)
+        n = len(shifts)
+        sh = np.ascontiguousarray(shifts, dtype=np.float64)
+        if not (isinstance(rsdcg, np.ndarray) and rsdcg.dtype == np.float64):
+            raise TypeError("rsdcg must be a float64 array")
+        al = np.ascontiguousarray(alpha if alpha is not None else np.ones(n), dtype=np.float64)
+        pp = (A._dp * len(psi))(*[dptr(p) for p in psi])
+        k = C.c_int()
+        check(lib().cpsgpu_minvcg(self._h, pp, dptr(chi), chi_norm, dptr(sh), n, dptr(rsdcg), type, dptr(al),
+                                  max_num_iter, precision, 1 if refine else 0, C.byref(k)))
+        return k.value
+
+    def autotune(self, prec=A.DOUBLE, nrhs=1) -> int:
+        t = C.c_int()
+        check(lib().cpsgpu_autotune(self._h, prec, nrhs, C.byref(t)))
+        return t.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cpsgpu_dirac_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DiracOpWilson(_DiracOp):
+    kind = A.WILSON
+
+    def __init__(self, lat: Lattice, mass: float):
+        super().__init__(lat, mass, ls=1)
+
+
+class DiracOpDwf(_DiracOp):
+    kind = A.DWF
+
+    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8):
+        super().__init__(lat, mass, ls=ls, m5=m5)
+
+
+class DiracOpMobius(_DiracOp):
+    kind = A.MOBIUS
+
+    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8, b: float = 1.5, c: float = 0.5):
+        super().__init__(lat, mass, ls=ls, m5=m5, b=b, c=c)
+
+    def Dslash(self, inp, cb, dag=0, prec=A.DOUBLE):
+        raise NotImplementedError("Mobius: use Dslash4 (zmobius_dslash_4)")
+
+    def Dslash4(self, inp, cb: int, dag: int = 0, prec: int = A.DOUBLE) -> np.ndarray:
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_mobius_dslash_4(self._h, dptr(out), dptr(inp), cb, dag, prec))
+        return out
+
+    def M5inv(self, inp, dag: int = 0, prec: int = A.DOUBLE) -> np.ndarray:
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_mobius_m5inv(self._h, dptr(out), dptr(inp), dag, prec))
+        return out

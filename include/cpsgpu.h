@@ -1,0 +1,224 @@
+/* cpsgpu: B200-native fermion-solve hot path of CPS (Columbia Physics System)
+ * behind a C ABI.
+ *
+ * The library keeps the gauge field and fermion fields resident on one GPU
+ * and implements, as hand-written sm_100a kernels, the even-odd
+ * preconditioned Wilson, Shamir domain-wall and Mobius operators and the CG
+ * and multishift-CG solvers that CPS's DiracOp classes run on the CPU.
+ * A CPS build calls these entry points from a thin C++ shim (see
+ * INTEGRATION.md); every function replaces the reference interface cited in
+ * its comment (paths relative to the reference's cps_pp tree).
+ *
+ * Conventions shared with the reference:
+ *   - vectors are host arrays of doubles in CPS storage order:
+ *       Wilson:  [cb site][spin][colour][re,im], 24 reals per site, the
+ *                preconditioned (odd) checkerboard (convert_func.C:452-490);
+ *       DWF:     [s][cb site][24], slice s on 4D parity (s+cb)%2
+ *                (dwf_dslash_4.C:107-137, convert.C:728-760);
+ *       Mobius:  [s][cb site][24], every slice on one 4D parity
+ *                (DWF_4D_EOPREC_EE, convert.C:797-851);
+ *     with cb site = (x/2) + (Lx/2)*(y + Ly*(z + Lz*t));
+ *   - the gauge field is in WILSON order, [parity (even first)][cb site]
+ *     [mu][3x3 complex, element (row,col) at 2*(row+3*col)]
+ *     (convert_func.C:361-410, wilson_dslash.C:54);
+ *   - boundary conditions are per direction (+1 periodic, -1 antiperiodic).
+ *     The reference multiplies the boundary links by the sign while a DiracOp
+ *     is alive (Lattice::BondCond, lattice_base.C:5336); pass signs_applied=1
+ *     to cpsgpu_import_gauge for such a field.  The library removes the signs
+ *     from its copy and applies them to the hops instead, which keeps every
+ *     stored link in SU(3) so 12-real compression stays exact.
+ *
+ * Errors: every function returns CPSGPU_OK (0) or a negative code, with a
+ * message from cpsgpu_last_error().  Where the reference exits the process
+ * (ERR.General, CG breakdown at inv_cg.C:326-329), the library returns a
+ * status instead; the shim maps it back to ERR.* to keep CPS's behaviour.
+ */
+#ifndef CPSGPU_H
+#define CPSGPU_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPSGPU_OK 0
+#define CPSGPU_ERR_ARG (-1)
+#define CPSGPU_ERR_UNSUPPORTED (-2)
+#define CPSGPU_ERR_CUDA (-3)
+#define CPSGPU_ERR_STATE (-4)
+
+/* solver status (cpsgpu_cg_result.status) */
+#define CPSGPU_CONVERGED 1
+#define CPSGPU_MAX_ITER 2
+#define CPSGPU_BREAKDOWN 3 /* p.Ap == 0 */
+#define CPSGPU_NONFINITE 4
+
+/* fermion actions */
+#define CPSGPU_WILSON 0
+#define CPSGPU_DWF 1
+#define CPSGPU_MOBIUS 2
+
+/* precisions */
+#define CPSGPU_DOUBLE 0
+#define CPSGPU_SINGLE 1
+#define CPSGPU_HALF 2 /* FP16 storage with a per-site FP32 norm, FP32 arithmetic */
+
+/* multishift solve types (enum MultiShiftSolveType, include/alg/enum_int.h:233-238) */
+#define CPSGPU_MS_SINGLE 0
+#define CPSGPU_MS_MULTI 1
+#define CPSGPU_MS_GENERAL 2
+
+typedef struct cpsgpu_lattice_s *cpsgpu_lattice;
+typedef struct cpsgpu_dirac_s *cpsgpu_dirac;
+typedef struct cpsgpu_field_s *cpsgpu_field;
+
+/* ---- version and errors ---- */
+const char *cpsgpu_version(void);
+const char *cpsgpu_last_error(void);
+int cpsgpu_device_count(int *count);
+/* select the CUDA device for objects created afterwards on this thread */
+int cpsgpu_set_device(int device);
+
+/* ---- geometry and gauge field ---- */
+/* Local lattice geometry on the current CUDA device.  Replaces the GJP
+ * geometry (GlobalJobParameter::Initialize, include/util/gjp.h:823) and the
+ * Lattice constructor's gauge allocation (lattice_base.C:320-325). */
+int cpsgpu_lattice_create(const int node_sites[4], const int bc[4], cpsgpu_lattice *lat);
+int cpsgpu_lattice_destroy(cpsgpu_lattice lat);
+/* Upload a WILSON-order gauge field (the field Lattice::Convert(WILSON)
+ * produces, convert.C:141-260).  Stores FP64 (18- and 12-real), FP32 and
+ * FP16 12-real copies on the device. */
+int cpsgpu_import_gauge(cpsgpu_lattice lat, const double *u_wilson, int signs_applied);
+/* max |row2 - conj(row0 x row1)| over all links, and whether FP64 uses 12 reals */
+int cpsgpu_gauge_info(cpsgpu_lattice lat, double *recon_err, int *fp64_recon12);
+int cpsgpu_synchronize(cpsgpu_lattice lat);
+
+/* ---- Dirac operators ---- */
+typedef struct {
+  int kind;        /* CPSGPU_WILSON / CPSGPU_DWF / CPSGPU_MOBIUS */
+  int ls;          /* fifth-dimension extent (ignored for Wilson) */
+  double mass;     /* CgArg.mass (cg_arg.h:17-36) */
+  double m5;       /* DoArg.dwf_height */
+  double mobius_b; /* DoArgExt.mobius_b_coeff */
+  double mobius_c; /* DoArgExt.mobius_c_coeff */
+} cpsgpu_dirac_arg;
+
+/* Replaces the DiracOpWilson / DiracOpDwf / DiracOpMobius constructors
+ * (d_op_wilson.C:54-137, d_op_dwf.C:67-100, d_op_mobius.C:57-140): kappa
+ * = 1/(2(m+4)) (Wilson), 1/(2(5-M5)) (DWF), kappa_b and kappa_c (Mobius). */
+int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *arg, cpsgpu_dirac *d);
+int cpsgpu_dirac_destroy(cpsgpu_dirac d);
+int cpsgpu_dirac_info(cpsgpu_dirac d, double *kappa, double *kappa_c);
+
+/* Host-vector operators; vectors hold one preconditioned checkerboard in
+ * CPS order, n = 24 * Ls * Vol/2 doubles; prec selects the device precision
+ * (inputs and outputs are FP64 on the host either way). */
+/* Wilson: wilson_dslash (wilson.h:226, wilson_dslash.C:173-515).
+ * DWF: dwf_dslash = 4D hop of every slice + fifth-direction hop
+ * (dwf_dslash.C:32-51).  Reads cb, writes 1-cb. */
+int cpsgpu_dslash(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);
+/* DiracOp*::MatPc / MatPcDag: wilson_m / wilson_mdag (wilson_m.C:49, wilson_mdag.C:50),
+ * dwf_m / dwf_mdag (dwf_m.C:31, dwf_mdag.C:32), zmobius_m_sym2 /
+ * zmobius_mdag_sym2 (zmobius_m-sym2.h:5, zmobius_mdag-sym2.h:4). */
+int cpsgpu_matpc(cpsgpu_dirac d, double *out, const double *in, int dag, int prec);
+/* DiracOp*::MatPcDagMatPc(out, in, dot): wilson_mdagm (wilson_mdagm.C:83),
+ * dwf_mdagm (dwf_mdagm.C:32), zmobius_mdagm (zmobius_mdagm.C:32).
+ * *dot = |MatPc in|^2 when dot is non-null. */
+int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double *dot, int prec);
+/* Mobius pieces: zmobius_dslash_4 (zmobius_dslash_4.C:209) and the
+ * out-of-place zmobius_m5inv (zmobius_m5inv.C:822). */
+int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);
+int cpsgpu_mobius_m5inv(cpsgpu_dirac d, double *out, const double *in, int dag, int prec);
+
+/* ---- solvers ---- */
+typedef struct {
+  double stop_rsd;     /* CgArg.stop_rsd: stop when |r| <= stop_rsd |b| */
+  int max_num_iter;    /* CgArg.max_num_iter */
+  double src_norm_sq;  /* 0: computed (inv_cg.C:166-169) */
+  double shift;        /* solve (MatPcDagMatPc + shift) x = b */
+  int precision;       /* CPSGPU_DOUBLE: plain FP64 CG; SINGLE / HALF: mixed precision */
+  double delta;        /* reliable-update threshold (mixed precision); 0: default 0.1 */
+  int chunk;           /* iterations per CUDA-graph launch; 0: default 8 */
+  int use_graph;       /* capture the iteration chunk in a CUDA graph */
+} cpsgpu_cg_arg;
+
+typedef struct {
+  int iterations;       /* as DiracOp::InvCg returns it: iterations done + 1 */
+  int status;           /* CPSGPU_CONVERGED / MAX_ITER / BREAKDOWN / NONFINITE */
+  double true_res;      /* |b - A x| / |b|, recomputed in FP64 (inv_cg.C:403-415) */
+  int reliable_updates; /* mixed precision only */
+  double seconds;       /* device time of the solve (CUDA events on the library stream) */
+  long long kernels;    /* kernels this library executed for the solve */
+} cpsgpu_cg_result;
+
+void cpsgpu_cg_arg_default(cpsgpu_cg_arg *arg);
+
+/* DiracOp::InvCg(out, in, src_norm_sq, true_res) -> InvCgShift
+ * (inv_cg.C:84-454): sol holds the initial guess on entry. */
+int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg_arg *arg,
+                 cpsgpu_cg_result *res);
+/* nrhs independent solves in one batched launch sequence (each gauge link
+ * load serves every right-hand side); the multi-source
+ * DiracOpMobius::MatInv(std::vector<Vector*>...) (d_op_mobius.C:407) loops
+ * InvCg over the same set. res has nrhs entries. */
+int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
+                       const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* DiracOp::MInvCG (minvcg.C:47-353): multishift CG on MatPcDagMatPc +
+ * shift[k].  rsdcg[k] in: stop residuals, out: achieved residuals; returns
+ * the iteration count through *iterations as the reference returns it.
+ * precision CPSGPU_DOUBLE runs the reference's FP64 recurrences; SINGLE runs
+ * them in FP32 and then refines every shift with FP64-true-residual CG to
+ * rsdcg[k] (refine != 0). */
+int cpsgpu_minvcg(cpsgpu_dirac d, double *const *psi, const double *chi, double chi_norm, const double *shift,
+                  int nshift, double *rsdcg, int type, const double *alpha, int max_num_iter, int precision,
+                  int refine, int *iterations);
+
+/* ---- device-resident fields ---- */
+int cpsgpu_field_create(cpsgpu_dirac d, int precision, int nrhs, cpsgpu_field *f);
+int cpsgpu_field_destroy(cpsgpu_field f);
+int cpsgpu_field_upload(cpsgpu_field f, const double *host);
+int cpsgpu_field_download(cpsgpu_field f, double *host);
+int cpsgpu_field_gaussian(cpsgpu_field f, unsigned long long seed);
+/* out = dslash(in) (precision of the fields, which must match) */
+int cpsgpu_dslash_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag);
+int cpsgpu_mdagm_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in);
+/* solve with FP64 fields already on the device (sol: initial guess in,
+ * solution out); arg->precision selects plain or mixed CG */
+int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,
+                       cpsgpu_cg_result *res);
+
+/* ---- tuning ---- */
+/* Time candidate block shapes of every hop kernel the operator uses, at
+ * precision prec, and keep the fastest.  Returns the number of tuned keys. */
+int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned);
+
+/* ---- measurement ----
+ * Time `reps` back-to-back launches of the operator's hop kernel
+ * (Dslash for Wilson / DWF, the Wilson hop of every slice for Mobius) at
+ * precision prec, with CUDA events on the library's stream.  The launches
+ * rotate over enough distinct input/output fields that the working set
+ * exceeds the L2 cache, so every launch streams from HBM.  Returns the mean
+ * device time per launch and the algorithmic bytes one launch must move
+ * (input and output spinors once, every link once). */
+int cpsgpu_time_dslash(cpsgpu_dirac d, int prec, int cb, int dag, int reps, double *ms_per_launch,
+                       double *bytes_per_launch);
+/* Same for one MatPcDagMatPc application (all its kernels); bytes counts
+ * every kernel's compulsory traffic. */
+int cpsgpu_time_mdagm(cpsgpu_dirac d, int prec, int reps, double *ms_per_apply, double *bytes_per_apply);
+
+/* ---- pinned host memory for fast host<->device copies ---- */
+int cpsgpu_host_alloc(size_t bytes, void **ptr);
+int cpsgpu_host_free(void *ptr);
+
+/* ---- seeded synthetic inputs (host code, no GPU needed) ---- */
+/* U = exp(i width H), H a Gaussian Hermitian traceless 3x3 per link, then
+ * reunitarised to SU(3); written in WILSON order without boundary signs.
+ * Deterministic in (seed, site, mu). */
+int cpsgpu_gen_gauge(const int node_sites[4], unsigned long long seed, double width, double *u_wilson);
+/* n unit-variance Gaussian reals, deterministic in (seed, stream, index) */
+int cpsgpu_gen_gaussian(double *out, long n, unsigned long long seed, unsigned int stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,171 @@
+"""Test infrastructure only: ctypes loaders for the oracle libraries.
+
+liboracle.so  the C restatement (oracle.c), built here or on any box by
+              ``make -C oracle oracle`` (gcc only);
+libcpsref.so  the reference's own noarch kernels compiled from the
+              reference source tree (``make -C oracle ref``).  Available only
+              where the reference tree exists or the .so was built before.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+ORACLE_SO = OUT / "liboracle.so"
+REF_SO = OUT / "libcpsref.so"
+REF_SRC = Path(os.environ.get("CPS_REF", "/root/reference/cps_pp"))
+
+_dp = C.POINTER(C.c_double)
+
+
+class OracleGeom(C.Structure):
+    _fields_ = [("L", C.c_int * 4), ("ls", C.c_int), ("bc", C.c_double * 4)]
+
+    @classmethod
+    def make(cls, L, ls=1, bc=(1, 1, 1, -1)):
+        g = cls()
+        for k in range(4):
+            g.L[k] = L[k]
+            g.bc[k] = bc[k]
+        g.ls = ls
+        return g
+
+
+class OracleMobius(C.Structure):
+    _fields_ = [("b", C.c_double * 128), ("c", C.c_double * 128), ("kappa_b", C.c_double * 128),
+                ("K", C.c_double * 128)]
+
+
+MDAGM_FN = C.CFUNCTYPE(None, C.c_void_p, _dp, _dp, _dp)
+
+
+def _make(target: str) -> None:
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    env.pop("CC", None)
+    cmd = ["make", "-s", "-C", str(HERE), target, f"REF={REF_SRC}"]
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"building oracle target {target} failed:\n{r.stdout}\n{r.stderr}")
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = HERE / "oracle.c"
+    if force or not ORACLE_SO.exists() or ORACLE_SO.stat().st_mtime < max(src.stat().st_mtime,
+                                                                           (HERE / "oracle.h").stat().st_mtime):
+        _make("oracle")
+    return ORACLE_SO
+
+
+def build_reference() -> Path:
+    if not REF_SO.exists():
+        if not REF_SRC.exists():
+            raise FileNotFoundError("reference sources not available and libcpsref.so not prebuilt")
+        _make("ref")
+    return REF_SO
+
+
+def reference_available() -> bool:
+    return REF_SO.exists() or REF_SRC.exists()
+
+
+_oracle = None
+_ref = None
+
+
+def load_oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        L = C.CDLL(str(build_oracle()))
+        g = C.POINTER(OracleGeom)
+        m = C.POINTER(OracleMobius)
+        i, d = C.c_int, C.c_double
+        sig = {
+            "orc_wilson_dslash": [g, _dp, _dp, _dp, i, i],
+            "orc_wilson_m": [g, _dp, _dp, _dp, d, i],
+            "orc_wilson_mdagm": [g, _dp, _dp, _dp, d, _dp],
+            "orc_dwf_dslash": [g, _dp, _dp, _dp, d, i, i],
+            "orc_dwf_m": [g, _dp, _dp, _dp, d, d, i],
+            "orc_dwf_mdagm": [g, _dp, _dp, _dp, d, d, _dp],
+            "orc_mobius_dslash_4": [g, m, _dp, _dp, _dp, i, i, d],
+            "orc_mobius_m5inv": [g, m, _dp, d, i],
+            "orc_mobius_m": [g, m, _dp, _dp, _dp, d, i],
+            "orc_mobius_mdagm": [g, m, _dp, _dp, _dp, d, _dp],
+        }
+        for k, a in sig.items():
+            getattr(L, k).argtypes = a
+            getattr(L, k).restype = None
+        L.orc_mobius_params.argtypes = [m, i, d, d, d]
+        L.orc_mobius_params.restype = None
+        L.orc_invcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, d, d, i, _dp, _dp]
+        L.orc_invcg.restype = i
+        L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]
+        L.orc_minvcg.restype = i
+        _oracle = L
+    return _oracle
+
+
+def load_reference() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        L = C.CDLL(str(build_reference()))
+        i, d = C.c_int, C.c_double
+        L.ref_init.argtypes = [i, i, i, i, i, d, d, d, i]
+        L.ref_init.restype = i
+        for k in ("ref_dwf_kappa", "ref_mobius_kappa_b", "ref_mobius_kappa_c"):
+            getattr(L, k).restype = d
+        sig = {
+            "ref_wilson_dslash": [_dp, _dp, _dp, i, i],
+            "ref_wilson_m": [_dp, _dp, _dp, d],
+            "ref_wilson_mdag": [_dp, _dp, _dp, d],
+            "ref_wilson_mdagm": [_dp, _dp, _dp, _dp, d],
+            "ref_dwf_dslash": [_dp, _dp, _dp, d, i, i],
+            "ref_dwf_dslash_4": [_dp, _dp, _dp, i, i],
+            "ref_dwf_dslash_5_plus": [_dp, _dp, d, i],
+            "ref_dwf_m": [_dp, _dp, _dp, d],
+            "ref_dwf_mdag": [_dp, _dp, _dp, d],
+            "ref_dwf_mdagm": [_dp, _dp, _dp, _dp, d],
+            "ref_zmobius_dslash_4": [_dp, _dp, _dp, i, i, d],
+            "ref_zmobius_m5inv": [_dp, d, i],
+            "ref_zmobius_m": [_dp, _dp, _dp, d],
+            "ref_zmobius_mdag": [_dp, _dp, _dp, d],
+            "ref_zmobius_mdagm": [_dp, _dp, _dp, _dp, d],
+        }
+        for k, a in sig.items():
+            getattr(L, k).argtypes = a
+            getattr(L, k).restype = None
+        _ref = L
+    return _ref
+
+
+def p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def apply_bc_signs(u: np.ndarray, L, bc) -> np.ndarray:
+    """The reference's BondCond on a WILSON-order field: links of direction mu
+    at x_mu = L_mu - 1 times bc[mu] (lattice_base.C:5336)."""
+    u = u.copy().reshape(2, -1, 4, 18)
+    vh = u.shape[1]
+    hx = L[0] // 2
+    for par in range(2):
+        i = np.arange(vh)
+        r = i // hx
+        y = r % L[1]
+        r = r // L[1]
+        z = r % L[2]
+        t = r // L[2]
+        x = 2 * (i % hx) + ((y + z + t + par) & 1)
+        c = [x, y, z, t]
+        for mu in range(4):
+            if bc[mu] < 0:
+                sel = c[mu] == L[mu] - 1
+                u[par, sel, mu, :] *= -1.0
+    return u.reshape(-1)

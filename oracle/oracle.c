@@ -1,0 +1,584 @@
+/* Test infrastructure only: the CPU oracle (see oracle.h).
+ *
+ * Each function restates the arithmetic of the reference routine cited in
+ * its comment; file:line citations are to the reference's cps_pp tree.
+ * Written for clarity, not speed: plain loops, FP64, single thread.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cplx;
+
+/* ---------------------------------------------------------------------- */
+/* geometry                                                                */
+/* ---------------------------------------------------------------------- */
+static long vol_cb(const orc_geom *g) {
+  return (long)g->L[0] * g->L[1] * g->L[2] * g->L[3] / 2;
+}
+
+/* checkerboard index of a site (wilson_dslash.C:288) */
+static long cb_index(const orc_geom *g, const int x[4]) {
+  return x[0] / 2 + (long)(g->L[0] / 2) * (x[1] + g->L[1] * (x[2] + (long)g->L[2] * x[3]));
+}
+
+/* coordinates of checkerboard site i on 4D parity p */
+static void cb_coords(const orc_geom *g, long i, int p, int x[4]) {
+  int hx = g->L[0] / 2;
+  long r = i / hx;
+  x[1] = (int)(r % g->L[1]);
+  r /= g->L[1];
+  x[2] = (int)(r % g->L[2]);
+  x[3] = (int)(r / g->L[2]);
+  x[0] = 2 * (int)(i % hx) + ((x[1] + x[2] + x[3] + p) & 1);
+}
+
+/* ---------------------------------------------------------------------- */
+/* spin and colour algebra                                                 */
+/* ---------------------------------------------------------------------- */
+/* gamma_mu as (column, factor) for each row, in the basis the reference's
+ * OneMinusPlusGammaTimesPsi expands (wilson_dslash.C:64-128); gamma_5 =
+ * diag(1,1,-1,-1) (chiral halves are reals 0-11 and 12-23). */
+static const int g_col[4][4] = {{3, 2, 1, 0}, {3, 2, 1, 0}, {2, 3, 0, 1}, {2, 3, 0, 1}};
+static const cplx g_fac_tab[4][4] = {
+    {I, I, -I, -I}, {-1, 1, 1, -1}, {I, -I, -I, I}, {1, 1, 1, 1}};
+
+/* link element (row, col) of direction mu at gauge site gs
+ * (UELEM, wilson_dslash.C:54): stored column-major within the matrix. */
+static cplx link(const double *u, long gs, int mu, int row, int col) {
+  const double *m = u + 72 * gs + 18 * mu + 2 * (row + 3 * col);
+  return m[0] + I * m[1];
+}
+
+static cplx ferm(const double *f, long site, int spin, int col) {
+  const double *p = f + 24 * site + 2 * (col + 3 * spin);
+  return p[0] + I * p[1];
+}
+
+/* acc += sign * Ulink * (1 + k gamma_mu) psi, Ulink = U or U^dagger */
+static void hop_term(cplx acc[4][3], const double *u, long gs, int mu, int herm,
+                     const double *psi, long ns, double k, double sign) {
+  cplx chi[4][3];
+  for (int s = 0; s < 4; s++)
+    for (int c = 0; c < 3; c++)
+      chi[s][c] = ferm(psi, ns, s, c) + k * g_fac_tab[mu][s] * ferm(psi, ns, g_col[mu][s], c);
+  for (int s = 0; s < 4; s++)
+    for (int a = 0; a < 3; a++) {
+      cplx v = 0;
+      for (int b = 0; b < 3; b++)
+        v += (herm ? conj(link(u, gs, mu, b, a)) : link(u, gs, mu, a, b)) * chi[s][b];
+      acc[s][a] += sign * v;
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Wilson                                                                  */
+/* ---------------------------------------------------------------------- */
+/* wilson_dslash.C:173-515.  Output parity cbn = 1-cb.  Forward hop: link at
+ * the output site, U (1 - sdag gamma) psi(x+mu); backward hop: link at x-mu,
+ * U^dagger (1 + sdag gamma) psi(x-mu).  A hop that wraps in direction mu
+ * picks up bc[mu]. */
+void orc_wilson_dslash(const orc_geom *g, double *chi, const double *u,
+                       const double *psi, int cb, int dag) {
+  long vh = vol_cb(g);
+  int cbn = 1 - cb;
+  double sdag = dag ? -1.0 : 1.0;
+  for (long i = 0; i < vh; i++) {
+    int x[4];
+    cb_coords(g, i, cbn, x);
+    cplx acc[4][3] = {{0}};
+    for (int mu = 0; mu < 4; mu++) {
+      int xp[4] = {x[0], x[1], x[2], x[3]};
+      int wrap = (x[mu] == g->L[mu] - 1);
+      xp[mu] = wrap ? 0 : x[mu] + 1;
+      hop_term(acc, u, i + vh * cbn, mu, 0, psi, cb_index(g, xp), -sdag,
+               wrap ? g->bc[mu] : 1.0);
+    }
+    for (int mu = 0; mu < 4; mu++) {
+      int xm[4] = {x[0], x[1], x[2], x[3]};
+      int wrap = (x[mu] == 0);
+      xm[mu] = wrap ? g->L[mu] - 1 : x[mu] - 1;
+      long j = cb_index(g, xm);
+      hop_term(acc, u, j + vh * cb, mu, 1, psi, j, sdag, wrap ? g->bc[mu] : 1.0);
+    }
+    double *o = chi + 24 * i;
+    for (int s = 0; s < 4; s++)
+      for (int c = 0; c < 3; c++) {
+        o[2 * (c + 3 * s)] = creal(acc[s][c]);
+        o[2 * (c + 3 * s) + 1] = cimag(acc[s][c]);
+      }
+  }
+}
+
+/* wilson_m.C:49-93 (dag=0) and wilson_mdag.C:50-96 (dag=1):
+ * chi = psi - kappa^2 D_oe D_eo psi. */
+void orc_wilson_m(const orc_geom *g, double *chi, const double *u,
+                  const double *psi, double kappa, int dag) {
+  long n = 24 * vol_cb(g);
+  double *tmp = malloc(sizeof(double) * n);
+  orc_wilson_dslash(g, tmp, u, psi, 1, dag);
+  orc_wilson_dslash(g, chi, u, tmp, 0, dag);
+  for (long k = 0; k < n; k++) chi[k] = psi[k] - kappa * kappa * chi[k];
+  free(tmp);
+}
+
+/* wilson_mdagm.C:83-154 */
+void orc_wilson_mdagm(const orc_geom *g, double *chi, const double *u,
+                      const double *psi, double kappa, double *dot) {
+  long n = 24 * vol_cb(g);
+  double *t = malloc(sizeof(double) * n);
+  orc_wilson_m(g, t, u, psi, kappa, 0);
+  if (dot) {
+    double s = 0;
+    for (long k = 0; k < n; k++) s += t[k] * t[k];
+    *dot = s;
+  }
+  orc_wilson_m(g, chi, u, t, kappa, 1);
+  free(t);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Shamir DWF                                                              */
+/* ---------------------------------------------------------------------- */
+/* dwf_dslash.C:32-51 = dwf_dslash_4 (dwf_dslash_4.C:68-154: slice s uses 4D
+ * parity (s+cb)%2) + dwf_dslash_5_plus (dwf_dslash_5_plus_omp.C:115-271:
+ * out[s] += 2/a5 * P in[s-1] on one chiral half and P' in[s+1] on the other,
+ * the walls weighted by -2 m_f / a5).  a5inv = 1. */
+void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
+                    const double *in, double mass, int cb, int dag) {
+  long vh = vol_cb(g);
+  int ls = g->ls;
+  long slice = 24 * vh;
+  for (int s = 0; s < ls; s++)
+    orc_wilson_dslash(g, out + s * slice, u, in + s * slice, (s + cb) % 2, dag);
+  const double two_a5 = 2.0, wall = -2.0 * mass;
+  /* half fed from s-1 is the upper one for D, the lower one for D^dagger */
+  int from_below = dag ? 12 : 0, from_above = dag ? 0 : 12;
+  for (int s = 0; s < ls; s++) {
+    int sb = (s == 0) ? ls - 1 : s - 1;
+    int sa = (s == ls - 1) ? 0 : s + 1;
+    double fb = (s == 0) ? wall : two_a5;
+    double fa = (s == ls - 1) ? wall : two_a5;
+    for (long i = 0; i < vh; i++) {
+      double *o = out + s * slice + 24 * i;
+      const double *ib = in + sb * slice + 24 * i;
+      const double *ia = in + sa * slice + 24 * i;
+      for (int k = 0; k < 12; k++) {
+        o[from_below + k] += fb * ib[from_below + k];
+        o[from_above + k] += fa * ia[from_above + k];
+      }
+    }
+  }
+}
+
+/* dwf_m.C:31-63 (dag 0), dwf_mdag.C:32-63 (dag 1): out = in - kappa5^2 D D in,
+ * kappa5 = 1 / (2 (4 + a5inv - M5))  (dwf_init.C:97-98) */
+void orc_dwf_m(const orc_geom *g, double *out, const double *u,
+               const double *in, double mass, double m5, int dag) {
+  long n = 24 * vol_cb(g) * g->ls;
+  double kappa = 1.0 / (2.0 * (4.0 + 1.0 - m5));
+  double *tmp = malloc(sizeof(double) * n);
+  orc_dwf_dslash(g, tmp, u, in, mass, 1, dag);
+  orc_dwf_dslash(g, out, u, tmp, mass, 0, dag);
+  for (long k = 0; k < n; k++) out[k] = -kappa * kappa * out[k] + in[k];
+  free(tmp);
+}
+
+/* dwf_mdagm.C:32-62 */
+void orc_dwf_mdagm(const orc_geom *g, double *out, const double *u,
+                   const double *in, double mass, double m5, double *dot) {
+  long n = 24 * vol_cb(g) * g->ls;
+  double *t = malloc(sizeof(double) * n);
+  orc_dwf_m(g, t, u, in, mass, m5, 0);
+  if (dot) {
+    double s = 0;
+    for (long k = 0; k < n; k++) s += t[k] * t[k];
+    *dot = s;
+  }
+  orc_dwf_m(g, out, u, t, mass, m5, 1);
+  free(t);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Mobius (zMobius kernels with real or complex per-s coefficients)        */
+/* ---------------------------------------------------------------------- */
+/* DiracOpMobius ctor, d_op_mobius.C:112-131 */
+void orc_mobius_params(orc_mobius *mp, int ls, double b, double c, double m5) {
+  double kb = 1.0 / (2.0 * (b * (4.0 - m5) + 1.0));
+  double kc = 1.0 / (2.0 * (c * (4.0 - m5) - 1.0));
+  for (int s = 0; s < ls; s++) {
+    mp->b[s] = b;
+    mp->c[s] = c;
+    mp->kappa_b[s] = kb;
+    mp->K[s] = kb / kc;
+  }
+}
+
+static cplx fget(const double *f, long idx) { return f[2 * idx] + I * f[2 * idx + 1]; }
+static void fset(double *f, long idx, cplx v) {
+  f[2 * idx] = creal(v);
+  f[2 * idx + 1] = cimag(v);
+}
+
+/* out[s] += fact-weighted fifth-direction hop of in, zmobius_dslash_5_plus.C
+ * :125-374.  Complex index: 12 per site, 0-5 upper chiral half, 6-11 lower. */
+static void mobius_hop5_acc(const orc_geom *g, int ls, const cplx *coef,
+                            double *out, const double *in, double mass, int dag) {
+  long vh = vol_cb(g);
+  long slice = 12 * vh; /* complex numbers per s-slice */
+  cplx f[64];
+  for (int s = 0; s < ls; s++) f[s] = dag ? conj(coef[s]) : coef[s];
+  for (int s = 0; s < ls; s++) {
+    int sb = (s == 0) ? ls - 1 : s - 1;
+    int sa = (s == ls - 1) ? 0 : s + 1;
+    cplx fb, fa; /* weights of the terms from s-1 and s+1 */
+    if (!dag) {
+      fb = (s == 0) ? -mass * f[0] : f[s];
+      fa = (s == ls - 1) ? -mass * f[ls - 1] : f[s];
+    } else {
+      fb = (s == 0) ? -mass * f[ls - 1] : f[s - 1];
+      fa = (s == ls - 1) ? -mass * f[0] : f[s + 1];
+    }
+    int hb = dag ? 6 : 0, ha = dag ? 0 : 6;
+    for (long i = 0; i < vh; i++)
+      for (int k = 0; k < 6; k++) {
+        long o1 = s * slice + 12 * i + hb + k, i1 = sb * slice + 12 * i + hb + k;
+        long o2 = s * slice + 12 * i + ha + k, i2 = sa * slice + 12 * i + ha + k;
+        fset(out, o1, fget(out, o1) + fb * fget(in, i1));
+        fset(out, o2, fget(out, o2) + fa * fget(in, i2));
+      }
+  }
+}
+
+/* zmobius_dslash_4.C:34-221.  dag 0: tmp[s] = b_s in[s] + c-hop5(in), then
+ * a Wilson hop of every slice from parity cb.  dag 1: Wilson hop^dagger of
+ * every slice, then conj(b_s) tmp[s] + conj(c)-hop5^dagger(tmp). */
+void orc_mobius_dslash_4(const orc_geom *g, const orc_mobius *mp, double *out,
+                         const double *u, const double *in, int cb, int dag,
+                         double mass) {
+  int ls = g->ls;
+  long vh = vol_cb(g), slice = 24 * vh;
+  double *tmp = malloc(sizeof(double) * slice * ls);
+  if (!dag) {
+    for (int s = 0; s < ls; s++)
+      for (long k = 0; k < 12 * vh; k++) fset(tmp, s * 12 * vh + k, mp->b[s] * fget(in, s * 12 * vh + k));
+    mobius_hop5_acc(g, ls, mp->c, tmp, in, mass, 0);
+    for (int s = 0; s < ls; s++)
+      orc_wilson_dslash(g, out + s * slice, u, tmp + s * slice, cb, 0);
+  } else {
+    for (int s = 0; s < ls; s++)
+      orc_wilson_dslash(g, tmp + s * slice, u, in + s * slice, cb, 1);
+    for (int s = 0; s < ls; s++)
+      for (long k = 0; k < 12 * vh; k++) fset(out, s * 12 * vh + k, conj(mp->b[s]) * fget(tmp, s * 12 * vh + k));
+    mobius_hop5_acc(g, ls, mp->c, out, tmp, mass, 1);
+  }
+  free(tmp);
+}
+
+/* M5^-1 in place, zmobius_m5inv_cmplx_dag0 (zmobius_m5inv.C:247-396) and
+ * _dag1 (:534-679).  For each site and each of the 6 complex components of a
+ * chiral half the reference runs the same scalar recurrence along s; v is
+ * the upper-half component, w the lower-half one. */
+void orc_mobius_m5inv(const orc_geom *g, const orc_mobius *mp, double *inout,
+                      double mass, int dag) {
+  int ls = g->ls;
+  long vh = vol_cb(g), slice = 12 * vh;
+  const cplx *K = mp->K;
+  cplx inv_d_last, prod = 1.0;
+  if (!dag) {
+    for (int s = 0; s < ls; s++) prod *= -K[s];
+    inv_d_last = 1.0 / (1.0 + prod * mass);
+  } else {
+    for (int s = 0; s < ls; s++) prod *= K[s];
+    inv_d_last = conj(1.0 / (1.0 + prod * mass));
+  }
+  cplx v[64], w[64];
+  for (long i = 0; i < vh; i++)
+    for (int k = 0; k < 6; k++) {
+      for (int s = 0; s < ls; s++) {
+        v[s] = fget(inout, s * slice + 12 * i + k);
+        w[s] = fget(inout, s * slice + 12 * i + 6 + k);
+      }
+      if (!dag) {
+        w[ls - 1] *= inv_d_last;
+        cplx fl = K[ls - 1] * mass * inv_d_last;
+        for (int s = 0; s <= ls - 2; s++) {
+          v[s + 1] += -K[s + 1] * v[s];
+          w[ls - 1] += fl * w[s];
+          fl *= -K[s];
+        }
+        cplx p = 1.0;
+        for (int s = 0; s < ls - 1; s++) p *= -K[s];
+        cplx fr = -p * mass * inv_d_last;
+        for (int s = ls - 2; s >= 0; s--) {
+          v[s] += fr * v[ls - 1];
+          w[s] += -K[s] * w[s + 1];
+          fr /= -K[s];
+        }
+        v[ls - 1] *= inv_d_last;
+      } else {
+        v[ls - 1] *= inv_d_last;
+        cplx fr = conj(K[0]) * mass * inv_d_last;
+        for (int s = 0; s <= ls - 2; s++) {
+          v[ls - 1] += fr * v[s];
+          w[s + 1] += -conj(K[s]) * w[s];
+          fr *= -conj(K[s + 1]);
+        }
+        cplx p = 1.0;
+        for (int s = 0; s < ls - 2; s++) p *= -K[s];
+        p *= -K[ls - 1];
+        cplx fl = -conj(p) * mass * inv_d_last;
+        for (int s = ls - 2; s >= 0; s--) {
+          v[s] += -conj(K[s + 1]) * v[s + 1];
+          w[s] += fl * w[ls - 1];
+          if (s > 0) fl /= -conj(K[s - 1]);
+        }
+        w[ls - 1] *= inv_d_last;
+      }
+      for (int s = 0; s < ls; s++) {
+        fset(inout, s * slice + 12 * i + k, v[s]);
+        fset(inout, s * slice + 12 * i + 6 + k, w[s]);
+      }
+    }
+}
+
+static void scale_slices(double *f, long vh, int ls, const cplx *fac, double sign, int conjugate) {
+  for (int s = 0; s < ls; s++) {
+    cplx a = sign * (conjugate ? conj(fac[s]) : fac[s]);
+    for (long k = 0; k < 12 * vh; k++) fset(f, s * 12 * vh + k, a * fget(f, s * 12 * vh + k));
+  }
+}
+
+/* SYM2 preconditioned operator: zmobius_m-sym2.h:5-127 (dag 0) and
+ * zmobius_mdag-sym2.h:4-109 (dag 1). */
+void orc_mobius_m(const orc_geom *g, const orc_mobius *mp, double *out,
+                  const double *u, const double *in, double mass, int dag) {
+  int ls = g->ls;
+  long vh = vol_cb(g), n = 24 * vh * ls;
+  double *t2 = malloc(sizeof(double) * n);
+  if (!dag) {
+    memcpy(t2, in, sizeof(double) * n);
+    orc_mobius_m5inv(g, mp, t2, mass, 0);
+    orc_mobius_dslash_4(g, mp, out, u, t2, 1, 0, mass);
+    scale_slices(out, vh, ls, mp->kappa_b, 1.0, 0);
+    orc_mobius_m5inv(g, mp, out, mass, 0);
+    orc_mobius_dslash_4(g, mp, t2, u, out, 0, 0, mass);
+    scale_slices(t2, vh, ls, mp->kappa_b, -1.0, 0);
+    for (long k = 0; k < n; k++) out[k] = in[k] + t2[k];
+  } else {
+    memcpy(out, in, sizeof(double) * n);
+    scale_slices(out, vh, ls, mp->kappa_b, -1.0, 1);
+    orc_mobius_dslash_4(g, mp, t2, u, out, 1, 1, mass);
+    orc_mobius_m5inv(g, mp, t2, mass, 1);
+    scale_slices(t2, vh, ls, mp->kappa_b, 1.0, 1);
+    orc_mobius_dslash_4(g, mp, out, u, t2, 0, 1, mass);
+    orc_mobius_m5inv(g, mp, out, mass, 1);
+    for (long k = 0; k < n; k++) out[k] += in[k];
+  }
+  free(t2);
+}
+
+/* zmobius_mdagm.C:32-59 */
+void orc_mobius_mdagm(const orc_geom *g, const orc_mobius *mp, double *out,
+                      const double *u, const double *in, double mass,
+                      double *dot) {
+  long n = 24 * vol_cb(g) * g->ls;
+  double *t = malloc(sizeof(double) * n);
+  orc_mobius_m(g, mp, t, u, in, mass, 0);
+  if (dot) {
+    double s = 0;
+    for (long k = 0; k < n; k++) s += t[k] * t[k];
+    *dot = s;
+  }
+  orc_mobius_m(g, mp, out, u, t, mass, 1);
+  free(t);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Krylov solvers                                                          */
+/* ---------------------------------------------------------------------- */
+static double norm2(const double *a, long n) {
+  double s = 0;
+  for (long k = 0; k < n; k++) s += a[k] * a[k];
+  return s;
+}
+
+/* DiracOp::InvCgShift, inv_cg.C:84-448 */
+int orc_invcg(orc_mdagm_fn op, void *ctx, long n, double *sol,
+              const double *src, double src_norm_sq, double stop_rsd,
+              int max_num_iter, double *true_res, const double *shift) {
+  double *res = malloc(sizeof(double) * n), *dir = malloc(sizeof(double) * n),
+         *mmp = malloc(sizeof(double) * n);
+  if (src_norm_sq == 0) src_norm_sq = norm2(src, n);
+  double stp_cnd = src_norm_sq * stop_rsd * stop_rsd;
+  op(ctx, mmp, sol, 0);
+  if (shift)
+    for (long k = 0; k < n; k++) mmp[k] = *shift * sol[k] + mmp[k];
+  for (long k = 0; k < n; k++) res[k] = src[k] - mmp[k];
+  memcpy(dir, res, sizeof(double) * n);
+  double rr = norm2(res, n), prv, d, a, b;
+  int itr = 0, max_itr = max_num_iter - 1;
+  if (rr <= stp_cnd) max_itr = 0;
+  for (int i = 0; i < max_itr; i++) {
+    itr++;
+    prv = rr;
+    op(ctx, mmp, dir, &d);
+    if (shift) {
+      for (long k = 0; k < n; k++) mmp[k] = *shift * dir[k] + mmp[k];
+      d += *shift * norm2(dir, n);
+    }
+    if (d == 0.0) {
+      fprintf(stderr, "orc_invcg: d = 0\n");
+      break;
+    }
+    a = prv / d;
+    for (long k = 0; k < n; k++) sol[k] = a * dir[k] + sol[k];
+    for (long k = 0; k < n; k++) res[k] = -a * mmp[k] + res[k];
+    rr = norm2(res, n);
+    if (rr <= stp_cnd) break;
+    b = rr / prv;
+    for (long k = 0; k < n; k++) dir[k] = b * dir[k] + res[k];
+  }
+  op(ctx, mmp, sol, 0);
+  if (shift)
+    for (long k = 0; k < n; k++) mmp[k] = *shift * sol[k] + mmp[k];
+  for (long k = 0; k < n; k++) res[k] = src[k] - mmp[k];
+  if (true_res) *true_res = sqrt(norm2(res, n) / src_norm_sq);
+  free(res);
+  free(dir);
+  free(mmp);
+  return itr + 1;
+}
+
+/* DiracOp::MInvCG, minvcg.C:47-353 (Jegerlehner's shifted recurrences). */
+int orc_minvcg(orc_mdagm_fn op, void *ctx, long n, double **psi,
+               const double *chi, double chi_norm, const double *mass,
+               int nmass, double *rsdcg, int type, const double *alpha,
+               int max_num_iter) {
+  double *r = malloc(sizeof(double) * n), *Ap = malloc(sizeof(double) * n);
+  double **p = malloc(sizeof(double *) * nmass);
+  for (int s = 0; s < nmass; s++) p[s] = malloc(sizeof(double) * n);
+  int *conv = calloc(nmass, sizeof(int));
+  double *bs = malloc(sizeof(double) * nmass), *z[2], *rsd_sq = malloc(sizeof(double) * nmass);
+  z[0] = malloc(sizeof(double) * nmass);
+  z[1] = malloc(sizeof(double) * nmass);
+  double a, as, b, bp, c, cp, d, css = 0;
+  if (type == 1)
+    for (int s = 0; s < nmass; s++) memset(psi[s], 0, sizeof(double) * n);
+  if (type == 0 || type == 1) {
+    memcpy(r, chi, sizeof(double) * n);
+    cp = chi_norm;
+  } else {
+    op(ctx, r, psi[0], 0);
+    for (long k = 0; k < n; k++) r[k] = chi[k] - r[k];
+    cp = norm2(r, n);
+  }
+  for (int s = 0; s < nmass; s++) memcpy(p[s], r, sizeof(double) * n);
+  for (int s = 0; s < nmass; s++) rsd_sq[s] = cp * rsdcg[s] * rsdcg[s];
+
+  /* d = <p, A p> */
+  if (mass[0] > 0) {
+    op(ctx, Ap, p[0], 0);
+    for (long k = 0; k < n; k++) Ap[k] = mass[0] * p[0][k] + Ap[k];
+    d = 0;
+    for (long k = 0; k < n; k++) d += p[0][k] * Ap[k];
+  } else {
+    op(ctx, Ap, p[0], &d);
+  }
+  b = -cp / d;
+  z[0][0] = z[1][0] = 1.0;
+  bs[0] = b;
+  int iz = 1;
+  for (int s = 1; s < nmass; s++) {
+    z[1 - iz][s] = 1.0;
+    z[iz][s] = 1.0 / (1.0 - b * (mass[s] - mass[0]));
+    bs[s] = b * z[iz][s];
+  }
+  for (long k = 0; k < n; k++) r[k] = b * Ap[k] + r[k];
+  c = norm2(r, n);
+  if (type == 0) {
+    for (int s = 0; s < nmass; s++) {
+      double bt = bs[s] * alpha[s];
+      for (long k = 0; k < n; k++) psi[0][k] = -bt * chi[k] + psi[0][k];
+    }
+  } else {
+    for (int s = 0; s < nmass; s++)
+      for (long k = 0; k < n; k++) psi[s][k] = -bs[s] * chi[k] + psi[s][k];
+  }
+  int convP = (c < rsd_sq[0]) ? 1 : 0;
+  int k;
+  for (k = 1; k <= max_num_iter && !convP; k++) {
+    a = c / cp;
+    for (int s = 0; s < nmass; s++) {
+      if (conv[s]) continue;
+      if (s == 0) {
+        for (long q = 0; q < n; q++) p[0][q] = a * p[0][q] + r[q];
+      } else {
+        as = a * (z[iz][s] * bs[s]) / (z[1 - iz][s] * b);
+        for (long q = 0; q < n; q++) p[s][q] = z[iz][s] * r[q] + as * p[s][q];
+      }
+    }
+    cp = c;
+    if (mass[0] > 0) {
+      op(ctx, Ap, p[0], 0);
+      for (long q = 0; q < n; q++) Ap[q] = mass[0] * p[0][q] + Ap[q];
+      d = 0;
+      for (long q = 0; q < n; q++) d += p[0][q] * Ap[q];
+    } else {
+      op(ctx, Ap, p[0], &d);
+    }
+    bp = b;
+    b = -cp / d;
+    bs[0] = b;
+    iz = 1 - iz;
+    for (int s = 1; s < nmass; s++) {
+      if (conv[s]) continue;
+      double zt = z[1 - iz][s] * z[iz][s] * bp /
+                  (b * a * (z[iz][s] - z[1 - iz][s]) +
+                   z[iz][s] * bp * (1 - b * (mass[s] - mass[0])));
+      bs[s] = b * zt / z[1 - iz][s];
+      z[iz][s] = zt;
+    }
+    for (long q = 0; q < n; q++) r[q] = b * Ap[q] + r[q];
+    c = norm2(r, n);
+    if (type == 0) {
+      for (int s = 0; s < nmass; s++) {
+        if (conv[s]) continue;
+        for (long q = 0; q < n; q++) psi[0][q] = -bs[s] * alpha[s] * p[s][q] + psi[0][q];
+      }
+    } else {
+      for (int s = 0; s < nmass; s++) {
+        if (conv[s]) continue;
+        for (long q = 0; q < n; q++) psi[s][q] = -bs[s] * p[s][q] + psi[s][q];
+      }
+    }
+    for (int s = 0; s < nmass; s++) {
+      if (conv[s]) continue;
+      css = c * z[iz][s] * z[iz][s];
+      conv[s] = (css < rsd_sq[s]) ? 1 : 0;
+      if (conv[s]) rsdcg[s] = css;
+    }
+    convP = conv[0];
+    if (convP)
+      for (int s = 0; s < nmass; s++)
+        if (!conv[s]) convP = 0;
+  }
+  for (int s = nmass - 1; s >= 0; s--) {
+    if (conv[s])
+      rsdcg[s] = sqrt(rsdcg[s]);
+    else
+      rsdcg[s] = sqrt(c * z[iz][s] * z[iz][s]);
+  }
+  for (int s = 0; s < nmass; s++) free(p[s]);
+  free(p);
+  free(r);
+  free(Ap);
+  free(conv);
+  free(bs);
+  free(z[0]);
+  free(z[1]);
+  free(rsd_sq);
+  return k;
+}

@@ -1,0 +1,94 @@
+/* Test infrastructure only: the CPU oracle.
+ *
+ * A plain-C, FP64 restatement of the reference's fermion-solve hot path
+ * (Wilson / Shamir-DWF / Mobius even-odd preconditioned operators and the
+ * CG / multishift-CG loops).  Only tests/, the smoke check and the bench's
+ * CPU-baseline leg use it, always as the checker, never as the product.
+ *
+ * Storage orders are the reference's own (so reference outputs compare
+ * element by element):
+ *   gauge   WILSON order: u[72*(i + Vh*p) + 18*mu + 2*(row + 3*col) + re/im],
+ *           p = 4D parity (even first), i = checkerboard index
+ *           (x/2) + (Lx/2)*(y + Ly*(z + Lz*t))      (convert_func.C:361-410,
+ *           wilson_dslash.C:54, :288, :307)
+ *   fermion f[24*(s*Vh + i) + 2*(colour + 3*spin) + re/im]  (wilson_dslash.C:60)
+ * Unlike the reference, the gauge field here carries NO boundary signs: the
+ * per-direction sign bc[mu] is applied to every hop that wraps the lattice in
+ * direction mu (the reference bakes the same sign into the links at
+ * x_mu = L_mu - 1 with Lattice::BondCond, lattice_base.C:5336).
+ */
+#ifndef CPS_ORACLE_H
+#define CPS_ORACLE_H
+#include <complex.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int L[4];      /* local lattice extent x,y,z,t (all even) */
+  int ls;        /* fifth-dimension extent (1 for Wilson) */
+  double bc[4];  /* +1 periodic, -1 antiperiodic, per direction */
+} orc_geom;
+
+/* Wilson hopping term (wilson_dslash.C:173-515): reads psi on checkerboard
+ * cb, writes chi on 1-cb; dag selects D^dagger. */
+void orc_wilson_dslash(const orc_geom *g, double *chi, const double *u,
+                       const double *psi, int cb, int dag);
+/* wilson_m.C:49, wilson_mdag.C:50, wilson_mdagm.C:83 */
+void orc_wilson_m(const orc_geom *g, double *chi, const double *u,
+                  const double *psi, double kappa, int dag);
+void orc_wilson_mdagm(const orc_geom *g, double *chi, const double *u,
+                      const double *psi, double kappa, double *dot);
+
+/* Shamir DWF, 5D even-odd (dwf_dslash.C:32, dwf_dslash_4.C:68,
+ * dwf_dslash_5_plus_omp.C:115, dwf_m.C:31, dwf_mdag.C:32, dwf_mdagm.C:32).
+ * a5inv is fixed at 1 as in the reference's default DoArg. */
+void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
+                    const double *in, double mass, int cb, int dag);
+void orc_dwf_m(const orc_geom *g, double *out, const double *u,
+               const double *in, double mass, double m5, int dag);
+void orc_dwf_mdagm(const orc_geom *g, double *out, const double *u,
+                   const double *in, double mass, double m5, double *dot);
+
+/* Mobius through the complex-coefficient (zMobius) kernels, 4D even-odd,
+ * SYM2 preconditioning.  b, c, kappa_b, K = kappa_b/kappa_c per s.
+ * zmobius_dslash_4.C:34-221, zmobius_dslash_5_plus.C:125-374,
+ * zmobius_m5inv.C:247-396 and :534-679, zmobius_m-sym2.h:5-127,
+ * zmobius_mdag-sym2.h:4-109, zmobius_mdagm.C:32-59. */
+typedef struct {
+  double complex b[64], c[64], kappa_b[64], K[64];
+} orc_mobius;
+void orc_mobius_params(orc_mobius *mp, int ls, double b, double c, double m5);
+void orc_mobius_dslash_4(const orc_geom *g, const orc_mobius *mp, double *out,
+                         const double *u, const double *in, int cb, int dag,
+                         double mass);
+void orc_mobius_m5inv(const orc_geom *g, const orc_mobius *mp, double *inout,
+                      double mass, int dag);
+void orc_mobius_m(const orc_geom *g, const orc_mobius *mp, double *out,
+                  const double *u, const double *in, double mass, int dag);
+void orc_mobius_mdagm(const orc_geom *g, const orc_mobius *mp, double *out,
+                      const double *u, const double *in, double mass,
+                      double *dot);
+
+/* CG on MatPcDagMatPc (+shift): DiracOp::InvCgShift, inv_cg.C:84-448.
+ * The operator is a callback: out = MdagM in, *dot = |M in|^2 when dot!=0.
+ * Returns itr+1 as the reference does; *true_res = |b - A x| / |b|. */
+typedef void (*orc_mdagm_fn)(void *ctx, double *out, const double *in,
+                             double *dot);
+int orc_invcg(orc_mdagm_fn op, void *ctx, long n, double *sol,
+              const double *src, double src_norm_sq, double stop_rsd,
+              int max_num_iter, double *true_res, const double *shift);
+
+/* Multishift CG: DiracOp::MInvCG, minvcg.C:47-353.  type 0 SINGLE,
+ * 1 MULTI, 2 GENERAL (enum_int.h:233-238).  RsdCG is overwritten with the
+ * achieved residuals; returns the iteration count k as the reference does. */
+int orc_minvcg(orc_mdagm_fn op, void *ctx, long n, double **psi,
+               const double *chi, double chi_norm, const double *shift,
+               int nshift, double *rsdcg, int type, const double *alpha,
+               int max_num_iter);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

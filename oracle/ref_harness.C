@@ -1,0 +1,139 @@
+// Test infrastructure only: a C-callable harness around the reference's
+// own noarch kernels (compiled from the reference sources by
+// oracle/Makefile into oracle/_ref/libcpsref.so).  Nothing in the product
+// links this; tests/ load it to pin the oracle restatement and the CUDA
+// kernels to the reference's arithmetic.
+//
+// Geometry and parameters are set through the reference's own
+// GlobalJobParameter::Initialize(const DoArg&) (include/util/gjp.h:823),
+// the Wilson/Dwf workspace through wilson_init / dwf_init
+// (d_op_wilson/noarch/wilson_init.C:52, d_op_dwf/noarch/dwf_init.C:41),
+// and the Mobius per-s coefficient arrays exactly as the DiracOpMobius
+// constructor fills them (d_op_mobius/d_op_mobius.C:105-131).
+//
+// All vectors are passed in the reference's own storage orders:
+//   gauge field  WILSON order, [parity(even first)][cb site][mu][col][row][re,im]
+//                (convert_func.C:361-410), boundary signs already applied by
+//                the caller (the reference's BondCond, lattice_base.C:5336);
+//   fermions     [s][cb site][spin][colour][re,im]  (wilson_dslash.C:60).
+#include <config.h>
+#include <util/data_types.h>
+#include <util/dirac_op.h>
+#include <util/vector.h>
+#include <util/wilson.h>
+#include <util/dwf.h>
+#include <util/zmobius.h>
+#include <util/gjp.h>
+#include <alg/do_arg.h>
+#include <cstring>
+#include <vector>
+
+USING_NAMESPACE_CPS
+
+namespace cps {
+// zmobius_m5inv in-place form (d_op_zmobius/noarch/zmobius_m5inv.C:807)
+void zmobius_m5inv(Vector *inout, Float mass, int dag, Zmobus *arg, Complex *K);
+}
+
+static Dwf g_dwf;          // DWF and Mobius library argument
+static bool g_have_dwf = false;
+static Wilson g_wilson;    // Wilson library argument (Fwilson's static struct)
+static bool g_have_wilson = false;
+
+extern "C" {
+
+// Configure the reference for one geometry.  bc_t: 1 periodic, -1 antiperiodic
+// (only the BndCndType GJP records; the sign itself is on the links).
+int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
+             double mobius_b, double mobius_c, int bc_t) {
+  DoArg d;
+  d.x_node_sites = lx; d.y_node_sites = ly; d.z_node_sites = lz;
+  d.t_node_sites = lt; d.s_node_sites = ls;
+  d.x_nodes = d.y_nodes = d.z_nodes = d.t_nodes = d.s_nodes = 1;
+  d.x_bc = d.y_bc = d.z_bc = BND_CND_PRD;
+  d.t_bc = (bc_t < 0) ? BND_CND_APRD : BND_CND_PRD;
+  d.dwf_height = m5;
+  d.dwf_a5_inv = 1.0;
+  GJP.Initialize(d);
+  GJP.Mobius_b(mobius_b);
+  GJP.Mobius_c(mobius_c);
+  GJP.ZMobius_PC_Type(ZMOB_PC_SYM2);
+
+  wilson_init(&g_wilson);
+  g_have_wilson = true;
+  if (ls > 0) {
+    dwf_init(&g_dwf);
+    g_have_dwf = true;
+    // as in DiracOpMobius::DiracOpMobius (d_op_mobius.C:100-131)
+    Dwf *m = &g_dwf;
+    m->ls = ls;
+    m->pc_type = ZMOB_PC_SYM2;
+    m->mobius_kappa_b = 1.0 / (2 * (mobius_b * (4 - m5) + 1.0));
+    m->mobius_kappa_c = 1.0 / (2 * (mobius_c * (4 - m5) - 1.0));
+    m->zmobius_b.assign(ls, Complex(mobius_b, 0));
+    m->zmobius_c.assign(ls, Complex(mobius_c, 0));
+    m->zmobius_kappa_b.assign(ls, Complex(m->mobius_kappa_b, 0));
+    m->zmobius_kappa_c.assign(ls, Complex(m->mobius_kappa_c, 0));
+    m->zmobius_kappa_ratio.resize(ls);
+    for (int i = 0; i < ls; i++)
+      m->zmobius_kappa_ratio[i] = m->zmobius_kappa_b[i] / m->zmobius_kappa_c[i];
+  }
+  return 0;
+}
+
+double ref_dwf_kappa(void) { return g_dwf.dwf_kappa; }
+double ref_mobius_kappa_b(void) { return g_dwf.mobius_kappa_b; }
+double ref_mobius_kappa_c(void) { return g_dwf.mobius_kappa_c; }
+
+// ---- Wilson (include/util/wilson.h:226-282) ----
+void ref_wilson_dslash(double *chi, double *u, double *psi, int cb, int dag) {
+  wilson_dslash(chi, u, psi, cb, dag, &g_wilson);
+}
+void ref_wilson_m(double *chi, double *u, double *psi, double kappa) {
+  wilson_m(chi, u, psi, kappa, &g_wilson);
+}
+void ref_wilson_mdag(double *chi, double *u, double *psi, double kappa) {
+  wilson_mdag(chi, u, psi, kappa, &g_wilson);
+}
+void ref_wilson_mdagm(double *chi, double *u, double *psi, double *dot, double kappa) {
+  wilson_mdagm(chi, u, psi, dot, kappa, &g_wilson);
+}
+
+// ---- Shamir DWF (include/util/dwf.h:97-248) ----
+void ref_dwf_dslash(double *out, double *u, double *in, double mass, int cb, int dag) {
+  dwf_dslash((Vector *)out, (Matrix *)u, (Vector *)in, mass, cb, dag, &g_dwf);
+}
+void ref_dwf_dslash_4(double *out, double *u, double *in, int cb, int dag) {
+  dwf_dslash_4((Vector *)out, (Matrix *)u, (Vector *)in, cb, dag, &g_dwf);
+}
+void ref_dwf_dslash_5_plus(double *out, double *in, double mass, int dag) {
+  dwf_dslash_5_plus((Vector *)out, (Vector *)in, mass, dag, &g_dwf);
+}
+void ref_dwf_m(double *out, double *u, double *in, double mass) {
+  dwf_m((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
+}
+void ref_dwf_mdag(double *out, double *u, double *in, double mass) {
+  dwf_mdag((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
+}
+void ref_dwf_mdagm(double *out, double *u, double *in, double *dot, double mass) {
+  dwf_mdagm((Vector *)out, (Matrix *)u, (Vector *)in, dot, mass, &g_dwf);
+}
+
+// ---- Mobius through the zMobius kernels (include/util/zmobius.h:66-229) ----
+void ref_zmobius_dslash_4(double *out, double *u, double *in, int cb, int dag, double mass) {
+  zmobius_dslash_4((Vector *)out, (Matrix *)u, (Vector *)in, cb, dag, &g_dwf, mass);
+}
+void ref_zmobius_m5inv(double *inout, double mass, int dag) {
+  zmobius_m5inv((Vector *)inout, mass, dag, &g_dwf, g_dwf.zmobius_kappa_ratio.data());
+}
+void ref_zmobius_m(double *out, double *u, double *in, double mass) {
+  zmobius_m((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
+}
+void ref_zmobius_mdag(double *out, double *u, double *in, double mass) {
+  zmobius_mdag((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
+}
+void ref_zmobius_mdagm(double *out, double *u, double *in, double *dot, double mass) {
+  zmobius_mdagm((Vector *)out, (Matrix *)u, (Vector *)in, dot, mass, &g_dwf);
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+"""Shared helpers for the tests: seeded inputs and oracle wrappers."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from oracle.loader import MDAGM_FN, OracleGeom, OracleMobius, p
+
+
+def rel(a, b) -> float:
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def vh_of(L) -> int:
+    return int(np.prod(L)) // 2
+
+
+class OracleOps:
+    """The oracle's operators on one geometry (gauge field without signs)."""
+
+    def __init__(self, O, L, u, ls=1, bc=(1, 1, 1, -1), m5=1.8, b=1.5, c=0.5):
+        self.O = O
+        self.L = tuple(L)
+        self.u = np.ascontiguousarray(u)
+        self.ls = ls
+        self.g = OracleGeom.make(L, ls, bc)
+        self.g1 = OracleGeom.make(L, 1, bc)
+        self.m5 = m5
+        self.mp = OracleMobius()
+        if ls > 1:
+            O.orc_mobius_params(C.byref(self.mp), ls, b, c, m5)
+        self.n = 24 * ls * vh_of(L)
+
+    def z(self):
+        return np.zeros(self.n)
+
+    def wilson_dslash(self, x, cb, dag):
+        y = self.z()
+        self.O.orc_wilson_dslash(C.byref(self.g1), p(y), p(self.u), p(x), cb, dag)
+        return y
+
+    def wilson_mdagm(self, x, kappa):
+        y = self.z()
+        d = C.c_double()
+        self.O.orc_wilson_mdagm(C.byref(self.g1), p(y), p(self.u), p(x), kappa, C.byref(d))
+        return y, d.value
+
+    def wilson_m(self, x, kappa, dag):
+        y = self.z()
+        self.O.orc_wilson_m(C.byref(self.g1), p(y), p(self.u), p(x), kappa, dag)
+        return y
+
+    def dwf_dslash(self, x, mass, cb, dag):
+        y = self.z()
+        self.O.orc_dwf_dslash(C.byref(self.g), p(y), p(self.u), p(x), mass, cb, dag)
+        return y
+
+    def dwf_m(self, x, mass, dag):
+        y = self.z()
+        self.O.orc_dwf_m(C.byref(self.g), p(y), p(self.u), p(x), mass, self.m5, dag)
+        return y
+
+    def dwf_mdagm(self, x, mass):
+        y = self.z()
+        d = C.c_double()
+        self.O.orc_dwf_mdagm(C.byref(self.g), p(y), p(self.u), p(x), mass, self.m5, C.byref(d))
+        return y, d.value
+
+    def mobius_dslash_4(self, x, mass, cb, dag):
+        y = self.z()
+        self.O.orc_mobius_dslash_4(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(x), cb, dag, mass)
+        return y
+
+    def mobius_m5inv(self, x, mass, dag):
+        y = np.ascontiguousarray(x).copy()
+        self.O.orc_mobius_m5inv(C.byref(self.g), C.byref(self.mp), p(y), mass, dag)
+        return y
+
+    def mobius_m(self, x, mass, dag):
+        y = self.z()
+        self.O.orc_mobius_m(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(x), mass, dag)
+        return y
+
+    def mobius_mdagm(self, x, mass):
+        y = self.z()
+        d = C.c_double()
+        self.O.orc_mobius_mdagm(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(x), mass, C.byref(d))
+        return y, d.value
+
+    # ---- solvers over an operator callback
+    def _op(self, kind, mass, kappa):
+        O, u, g = self.O, self.u, self.g
+
+        def fn(ctx, out, inp, dot):
+            if kind == "wilson":
+                O.orc_wilson_mdagm(C.byref(self.g1), out, p(u), inp, kappa, dot)
+            elif kind == "dwf":
+                O.orc_dwf_mdagm(C.byref(g), out, p(u), inp, mass, self.m5, dot)
+            else:
+                O.orc_mobius_mdagm(C.byref(g), C.byref(self.mp), out, p(u), inp, mass, dot)
+
+        return MDAGM_FN(fn)
+
+    def invcg(self, kind, src, sol0=None, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, shift=None):
+        sol = np.zeros(self.n) if sol0 is None else np.ascontiguousarray(sol0).copy()
+        tr = C.c_double()
+        fn = self._op(kind, mass, kappa)
+        sh = C.c_double(shift) if shift is not None else None
+        it = self.O.orc_invcg(fn, None, self.n, p(sol), p(src), 0.0, stop_rsd, max_num_iter, C.byref(tr),
+                              C.byref(sh) if sh is not None else None)
+        return sol, it, tr.value
+
+    def minvcg(self, kind, chi, shifts, rsd, mass=0.0, kappa=0.0, type=1, alpha=None, max_num_iter=10000,
+               psi0=None):
+        n = len(shifts)
+        npsi = 1 if type == 0 else n
+        psi = [np.zeros(self.n) if psi0 is None else np.ascontiguousarray(psi0[k]).copy() for k in range(npsi)]
+        arr = (C.POINTER(C.c_double) * npsi)(*[p(x) for x in psi])
+        rs = np.ascontiguousarray(rsd, dtype=np.float64).copy()
+        sh = np.ascontiguousarray(shifts, dtype=np.float64)
+        al = np.ascontiguousarray(alpha if alpha is not None else np.ones(n), dtype=np.float64)
+        fn = self._op(kind, mass, kappa)
+        chi = np.ascontiguousarray(chi)
+        k = self.O.orc_minvcg(fn, None, self.n, arr, p(chi), float(chi @ chi), p(sh), n, p(rs), type, p(al),
+                              max_num_iter)
+        return psi, k, rs

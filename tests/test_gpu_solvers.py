@@ -1,0 +1,141 @@
+"""Device-resident solvers against the oracle's CG / multishift CG:
+FP64 CG with the reference's bookkeeping, mixed-precision (FP32 and FP16
+inner) reliable-update CG to a true residual of 1e-10, batched
+right-hand sides, multishift CG, and host-side failure injection."""
+import numpy as np
+import pytest
+
+from cps_veloc_b200 import _abi as A
+from cps_veloc_b200.dirac import DiracOpDwf, DiracOpMobius, DiracOpWilson, Lattice, gen_gauge, gen_gaussian
+from helpers import OracleOps, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _wilson(oracle, L=(8, 8, 8, 8), seed=71):
+    u = gen_gauge(L, seed=seed)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpWilson(lat, mass=1 / (2 * 0.12) - 4)
+    return D, OracleOps(oracle, L, u, ls=1)
+
+
+def test_wilson_cg_matches_oracle(oracle):
+    """8^4 Wilson, kappa 0.12, stop 1e-8 (the plain CPU-runnable case)."""
+    D, ops = _wilson(oracle)
+    b = gen_gaussian(ops.n, seed=72)
+    xo, ito, tro = ops.invcg("wilson", b, kappa=D.kappa, stop_rsd=1e-8)
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-8)
+    assert r.status == A.CONVERGED
+    assert abs(r.iterations - ito) <= 1
+    assert r.true_res < 1e-8
+    assert rel(x, xo) < 1e-9
+
+
+def test_cg_bookkeeping_and_graph_equivalence(oracle):
+    D, ops = _wilson(oracle, L=(4, 4, 4, 8))
+    b = gen_gaussian(ops.n, seed=73)
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-14, max_num_iter=7)
+    _, ito, _ = ops.invcg("wilson", b, kappa=D.kappa, stop_rsd=1e-14, max_num_iter=7)
+    assert r.iterations == ito == 7 and r.status == A.MAX_ITER
+    x1, x2 = np.zeros(ops.n), np.zeros(ops.n)
+    r1 = D.InvCg(x1, b, stop_rsd=1e-10, use_graph=True, chunk=5)
+    r2 = D.InvCg(x2, b, stop_rsd=1e-10, use_graph=False, chunk=3)
+    assert r1.iterations == r2.iterations and np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("prec", [A.DOUBLE, A.SINGLE, A.HALF])
+def test_dwf_cg_true_residual(oracle, prec):
+    L, ls, mass = (4, 4, 4, 8), 8, 0.05
+    u = gen_gauge(L, seed=81)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    b = gen_gaussian(ops.n, seed=82)
+    xo, ito, _ = ops.invcg("dwf", b, mass=mass, stop_rsd=1e-11)
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-10, precision=prec)
+    assert r.status == A.CONVERGED and r.true_res <= 1e-10
+    assert rel(x, xo) < 1e-8
+    if prec != A.DOUBLE:
+        assert r.reliable_updates >= 1
+        assert r.iterations < 2.0 * ito
+
+
+@pytest.mark.parametrize("prec", [A.DOUBLE, A.HALF])
+def test_mobius_cg_true_residual(oracle, prec):
+    L, ls, mass = (4, 4, 4, 4), 8, 0.05
+    u = gen_gauge(L, seed=91)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    b = gen_gaussian(ops.n, seed=92)
+    xo, _, _ = ops.invcg("mobius", b, mass=mass, stop_rsd=1e-11)
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-10, precision=prec)
+    assert r.status == A.CONVERGED and r.true_res <= 1e-10
+    assert rel(x, xo) < 1e-8
+
+
+def test_multi_rhs_matches_single(oracle):
+    L, ls = (4, 4, 4, 8), 4
+    u = gen_gauge(L, seed=101)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=0.1, ls=ls)
+    srcs = [gen_gaussian(D.f_size, seed=102 + k) for k in range(3)]
+    sols = [np.zeros(D.f_size) for _ in srcs]
+    res = D.InvCgMulti(sols, srcs, stop_rsd=1e-10, precision=A.SINGLE)
+    for s, x, r in zip(srcs, sols, res):
+        y = np.zeros(D.f_size)
+        r1 = D.InvCg(y, s, stop_rsd=1e-10, precision=A.SINGLE)
+        assert r.status == A.CONVERGED and r.true_res <= 1e-10
+        assert r.iterations == r1.iterations
+        assert rel(x, y) < 1e-12
+
+
+def test_minvcg_fp64_matches_oracle(oracle):
+    D, ops = _wilson(oracle, L=(4, 4, 4, 8))
+    chi = gen_gaussian(ops.n, seed=111)
+    shifts = [0.02, 0.2, 1.0, 5.0]
+    psi_o, ko, rso = ops.minvcg("wilson", chi, shifts, [1e-10] * 4, kappa=D.kappa, type=1)
+    psi = [np.zeros(ops.n) for _ in shifts]
+    rs = np.full(4, 1e-10)
+    k = D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, type=A.MS_MULTI)
+    assert abs(k - ko) <= 1
+    for s in range(4):
+        assert rel(psi[s], psi_o[s]) < 1e-9
+        assert rs[s] / np.linalg.norm(chi) < 1e-10
+
+
+def test_minvcg_single_type_and_sloppy_refine(oracle):
+    D, ops = _wilson(oracle, L=(4, 4, 4, 8))
+    chi = gen_gaussian(ops.n, seed=112)
+    shifts = [0.01, 0.1, 1.0]
+    alpha = [0.5, -1.0, 2.0]
+    psi_o, _, _ = ops.minvcg("wilson", chi, shifts, [1e-10] * 3, kappa=D.kappa, type=0, alpha=alpha)
+    psi = [np.zeros(ops.n)]
+    rs = np.full(3, 1e-10)
+    D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, type=A.MS_SINGLE, alpha=alpha)
+    assert rel(psi[0], psi_o[0]) < 1e-9
+    # FP32 multishift + FP64 refinement of each shift
+    psi2 = [np.zeros(ops.n) for _ in shifts]
+    rs2 = np.full(3, 1e-10)
+    D.MInvCG(psi2, chi, float(chi @ chi), shifts, rs2, type=A.MS_MULTI, precision=A.SINGLE)
+    for s, sh in enumerate(shifts):
+        Ax, _ = ops.wilson_mdagm(psi2[s], D.kappa)
+        assert rel(Ax + sh * psi2[s], chi) <= 1e-10
+
+
+def test_failure_injection_nonfinite_source(oracle):
+    """A NaN planted in the host source must come back as a status, not a fault."""
+    D, ops = _wilson(oracle, L=(4, 4, 4, 4))
+    b = gen_gaussian(ops.n, seed=121)
+    b[17] = np.nan
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-10, max_num_iter=50)
+    assert r.status == A.NONFINITE

@@ -1,0 +1,96 @@
+"""The oracle restatement against the reference's own kernels, compiled from
+the reference sources (oracle/Makefile, target ``ref``), on geometries and
+parameters beyond the golden set: boundary-condition variants, a minimal
+2^4 lattice, odd and even Ls, zero and large masses."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import OracleOps, rel, vh_of
+from oracle.loader import apply_bc_signs, p
+from cps_veloc_b200.dirac import gen_gauge, gen_gaussian
+
+TOL = 1e-13
+
+
+def _ref_setup(R, L, ls, bc, m5=1.8, b=1.5, c=0.5):
+    # the reference harness records only the t boundary; x,y,z stay periodic
+    assert bc[0] == bc[1] == bc[2] == 1
+    R.ref_init(*L, ls, m5, b, c, bc[3])
+
+
+@pytest.mark.parametrize("L,bc", [((4, 4, 4, 4), (1, 1, 1, -1)), ((2, 2, 2, 2), (1, 1, 1, 1)),
+                                  ((4, 2, 6, 4), (1, 1, 1, -1)), ((6, 4, 2, 8), (1, 1, 1, 1))])
+def test_wilson_vs_reference(oracle, reference, L, bc):
+    _ref_setup(reference, L, 2, bc)
+    u = gen_gauge(L, seed=11)
+    us = apply_bc_signs(u, L, bc)
+    ops = OracleOps(oracle, L, u, ls=1, bc=bc)
+    psi = gen_gaussian(24 * vh_of(L), seed=3)
+    for cb in (0, 1):
+        for dag in (0, 1):
+            y = np.zeros_like(psi)
+            reference.ref_wilson_dslash(p(y), p(us), p(psi), cb, dag)
+            assert rel(ops.wilson_dslash(psi, cb, dag), y) < TOL
+    for kappa in (0.12, 0.125):
+        y = np.zeros_like(psi)
+        d = C.c_double()
+        reference.ref_wilson_mdagm(p(y), p(us), p(psi), C.byref(d), kappa)
+        yo, do = ops.wilson_mdagm(psi, kappa)
+        assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
+
+
+@pytest.mark.parametrize("L,ls,mass", [((4, 4, 4, 4), 4, 0.01), ((2, 4, 2, 4), 8, 0.1),
+                                       ((4, 2, 2, 8), 5, 0.0), ((2, 2, 4, 4), 2, 1.0)])
+def test_dwf_vs_reference(oracle, reference, L, ls, mass):
+    bc = (1, 1, 1, -1)
+    _ref_setup(reference, L, ls, bc)
+    u = gen_gauge(L, seed=5)
+    us = apply_bc_signs(u, L, bc)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc)
+    psi = gen_gaussian(24 * ls * vh_of(L), seed=4)
+    assert abs(reference.ref_dwf_kappa() - 1 / (2 * (5 - 1.8))) < 1e-15
+    for cb in (0, 1):
+        for dag in (0, 1):
+            y = np.zeros_like(psi)
+            reference.ref_dwf_dslash(p(y), p(us), p(psi), mass, cb, dag)
+            assert rel(ops.dwf_dslash(psi, mass, cb, dag), y) < TOL
+    for dag, fn in ((0, reference.ref_dwf_m), (1, reference.ref_dwf_mdag)):
+        y = np.zeros_like(psi)
+        fn(p(y), p(us), p(psi), mass)
+        assert rel(ops.dwf_m(psi, mass, dag), y) < TOL
+    y = np.zeros_like(psi)
+    d = C.c_double()
+    reference.ref_dwf_mdagm(p(y), p(us), p(psi), C.byref(d), mass)
+    yo, do = ops.dwf_mdagm(psi, mass)
+    assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
+
+
+@pytest.mark.parametrize("L,ls,mass,b,c", [((4, 4, 4, 4), 4, 0.01, 1.5, 0.5), ((2, 4, 2, 4), 6, 0.1, 1.5, 0.5),
+                                           ((4, 2, 2, 4), 5, 0.005, 2.0, 1.0), ((2, 2, 4, 4), 8, 0.3, 1.0, 0.0)])
+def test_mobius_vs_reference(oracle, reference, L, ls, mass, b, c):
+    bc = (1, 1, 1, -1)
+    _ref_setup(reference, L, ls, bc, b=b, c=c)
+    u = gen_gauge(L, seed=9)
+    us = apply_bc_signs(u, L, bc)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc, b=b, c=c)
+    psi = gen_gaussian(24 * ls * vh_of(L), seed=8)
+    for dag in (0, 1):
+        y = psi.copy()
+        reference.ref_zmobius_m5inv(p(y), mass, dag)
+        assert rel(ops.mobius_m5inv(psi, mass, dag), y) < TOL
+    for cb in (0, 1):
+        for dag in (0, 1):
+            y = np.zeros_like(psi)
+            reference.ref_zmobius_dslash_4(p(y), p(us), p(psi), cb, dag, mass)
+            assert rel(ops.mobius_dslash_4(psi, mass, cb, dag), y) < TOL
+    for dag, fn in ((0, reference.ref_zmobius_m), (1, reference.ref_zmobius_mdag)):
+        y = np.zeros_like(psi)
+        fn(p(y), p(us), p(psi), mass)
+        assert rel(ops.mobius_m(psi, mass, dag), y) < TOL
+    y = np.zeros_like(psi)
+    d = C.c_double()
+    reference.ref_zmobius_mdagm(p(y), p(us), p(psi), C.byref(d), mass)
+    yo, do = ops.mobius_mdagm(psi, mass)
+    assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
