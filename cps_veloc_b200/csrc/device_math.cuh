@@ -82,6 +82,14 @@ __device__ __forceinline__ half_spinor<R> project(const R *psi, int mu, R k) {
   return h;
 }
 
+template <typename R>
+__device__ __forceinline__ void negate(half_spinor<R> &h) {
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) h.h[s][c] = mk(-h.h[s][c].re, -h.h[s][c].im);
+}
+
 // acc += w * (full four-spin spinor rebuilt from the half spinor g = U h),
 // the rows 2,3 of (1 + k gamma_mu) expressed through rows 0,1.
 template <typename R>

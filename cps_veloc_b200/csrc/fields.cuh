@@ -165,6 +165,117 @@ template <> struct SpinorIO<PREC_HALF> {
   }
 };
 
+// ---- one slice of a field, 32-bit site indices ----
+// Slice<P>(f, sl) points at slice sl; load(j) reads site j with the group
+// stride vh.  Site indices are 32-bit (vh < 2^31 for any lattice that fits).
+template <int P> struct Slice;
+template <> struct Slice<PREC_DOUBLE> {
+  const double2 *d;
+  int vh;
+  __device__ __forceinline__ Slice(const SpinorView &f, long sl)
+      : d(reinterpret_cast<const double2 *>(f.data) + sl * 12 * f.vh), vh((int)f.vh) {}
+  __device__ __forceinline__ void load(int j, double *v) const {
+#pragma unroll
+    for (int g = 0; g < 12; g++) {
+      double2 q = __ldg(d + j + g * vh);
+      v[2 * g] = q.x;
+      v[2 * g + 1] = q.y;
+    }
+  }
+  __device__ __forceinline__ void load_half(int j, int half, double *v) const {
+    const double2 *b = d + 6 * half * vh + j;
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+      double2 q = __ldg(b + g * vh);
+      v[2 * g] = q.x;
+      v[2 * g + 1] = q.y;
+    }
+  }
+};
+template <> struct Slice<PREC_SINGLE> {
+  const float4 *d;
+  int vh;
+  __device__ __forceinline__ Slice(const SpinorView &f, long sl)
+      : d(reinterpret_cast<const float4 *>(f.data) + sl * 6 * f.vh), vh((int)f.vh) {}
+  __device__ __forceinline__ void load(int j, float *v) const {
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+      float4 q = __ldg(d + j + g * vh);
+      v[4 * g] = q.x; v[4 * g + 1] = q.y; v[4 * g + 2] = q.z; v[4 * g + 3] = q.w;
+    }
+  }
+  __device__ __forceinline__ void load_half(int j, int half, float *v) const {
+    const float4 *b = d + 3 * half * vh + j;
+#pragma unroll
+    for (int g = 0; g < 3; g++) {
+      float4 q = __ldg(b + g * vh);
+      v[4 * g] = q.x; v[4 * g + 1] = q.y; v[4 * g + 2] = q.z; v[4 * g + 3] = q.w;
+    }
+  }
+};
+template <> struct Slice<PREC_HALF> {
+  const uint4 *d;
+  const float *n;
+  int vh;
+  __device__ __forceinline__ Slice(const SpinorView &f, long sl)
+      : d(reinterpret_cast<const uint4 *>(f.data) + sl * 3 * f.vh), n(f.norm + sl * f.vh), vh((int)f.vh) {}
+  __device__ __forceinline__ void load(int j, float *v) const {
+    const float s = __ldg(n + j);
+#pragma unroll
+    for (int g = 0; g < 3; g++) unpack8(__ldg(d + j + g * vh), s, v + 8 * g);
+  }
+  __device__ __forceinline__ void load_half(int j, int half, float *v) const {
+    const float s = __ldg(n + j);
+    float tmp[16];
+    if (half == 0) {
+      unpack8(__ldg(d + j), s, tmp);
+      unpack8(__ldg(d + j + vh), s, tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[k];
+    } else {
+      unpack8(__ldg(d + j + vh), s, tmp);
+      unpack8(__ldg(d + j + 2 * vh), s, tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[4 + k];
+    }
+  }
+};
+
+// ---- 4-real chunks (reals 4c .. 4c+3) for register-light epilogues ----
+template <int P> struct Chunk4;
+template <> struct Chunk4<PREC_DOUBLE> {
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, int c, double *v) {
+    const double2 *d = reinterpret_cast<const double2 *>(f.data) + (sl * 12 + 2 * c) * f.vh + i;
+    double2 a = __ldg(d), b = __ldg(d + f.vh);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  static __device__ __forceinline__ void store(const SpinorView &f, long sl, long i, int c, const double *v) {
+    double2 *d = reinterpret_cast<double2 *>(f.data) + (sl * 12 + 2 * c) * f.vh + i;
+    d[0] = make_double2(v[0], v[1]);
+    d[f.vh] = make_double2(v[2], v[3]);
+  }
+};
+template <> struct Chunk4<PREC_SINGLE> {
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, int c, float *v) {
+    float4 q = __ldg(reinterpret_cast<const float4 *>(f.data) + (sl * 6 + c) * f.vh + i);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  }
+  static __device__ __forceinline__ void store(const SpinorView &f, long sl, long i, int c, const float *v) {
+    reinterpret_cast<float4 *>(f.data)[(sl * 6 + c) * f.vh + i] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <> struct Chunk4<PREC_HALF> {
+  // 4 fp16 = one half of a 16-byte group; stores need the whole site (norm)
+  static __device__ __forceinline__ void load(const SpinorView &f, long sl, long i, int c, float *v) {
+    const uint2 *d = reinterpret_cast<const uint2 *>(f.data) + 2 * ((sl * 3 + (c >> 1)) * f.vh + i) + (c & 1);
+    const float s = __ldg(f.norm + sl * f.vh + i);
+    uint2 q = __ldg(d);
+    const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+    float2 a = __half22float2(h[0]), b = __half22float2(h[1]);
+    v[0] = a.x * s; v[1] = a.y * s; v[2] = b.x * s; v[3] = b.y * s;
+  }
+};
+
 // ---- gauge links ----
 template <int P, int RECON> struct LinkIO;
 

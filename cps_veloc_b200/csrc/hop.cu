@@ -11,9 +11,11 @@ namespace {
 
 using HopFn = void (*)(const HopParams, const HopViews, SolverScalars *, double *);
 
+bool g_dag = false;  // set by launch_hop before pick()
+
 template <int P, int RECON, int EP, int PR, int PX>
 HopFn get() {
-  return hop_kernel<P, RECON, EP, PR, PX>;
+  return g_dag ? hop_kernel<P, RECON, EP, PR, PX, true> : hop_kernel<P, RECON, EP, PR, PX, false>;
 }
 
 template <int P, int RECON>
@@ -69,6 +71,9 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
     hp.bc[k] = lat.bc[k];
   }
   hp.hx = lat.L[0] / 2;
+  hp.dhx.init(hp.hx);
+  hp.dly.init(lat.L[1]);
+  hp.dlz.init(lat.L[2]);
   hp.vh = lat.vh;
   hp.ls = D.ls;
   hp.cb = L.cb;
@@ -93,12 +98,14 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   v.b = b;
 
   const int recon = lat.recon(L.prec);
+  g_dag = (L.dag != 0);
   HopFn fn = pick(L.prec, recon, L.ep, L.pr, L.px);
   const bool mix = ep_mix(L.ep);
   TuneKey key{L.prec, recon, L.ep, D.kind, D.ls};
   dim3 block = hop_block(key, mix);
-  dim3 grid((unsigned)((lat.vh + block.x - 1) / block.x), (unsigned)((D.ls + block.y - 1) / block.y),
-            (unsigned)in.nrhs);
+  const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
+  hp.nsg = (D.ls + block.y - 1) / block.y;
+  dim3 grid(nsb * hp.nsg, 1, (unsigned)in.nrhs);
   size_t smem = 0;
   if (mix) {
     smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double);

@@ -47,11 +47,33 @@ __host__ __device__ constexpr bool ep_axpy(int e) { return e == EP_AXPY || e == 
 // Gating of a launch on the solver state.
 enum Gate { GATE_NONE = 0, GATE_RUNNING = 1, GATE_RELIABLE = 2 };
 
+// n / d for 0 <= n < 2^31 by multiply-high (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994): with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1, q = (mulhi(n,m) + n) >> s.
+struct FastDiv {
+  unsigned m;
+  int s;
+  int d;
+  __host__ void init(int d_) {
+    d = d_;
+    s = 0;
+    while ((1u << s) < (unsigned)d) s++;
+    unsigned long long num = ((1ull << 32) * ((1ull << s) - (unsigned)d));
+    m = (unsigned)(num / (unsigned)d + 1);
+    if (d == 1) { m = 0; s = 0; }
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi((unsigned)n, m) + (unsigned)n) >> s);
+  }
+};
+
 struct HopParams {
   int L[4];
   int hx;           // L[0] / 2
   long vh;          // checkerboard volume
   int ls;
+  FastDiv dhx, dly, dlz;  // divisions by L[0]/2, L[1], L[2]
+  int nsg;          // slice groups in the launch (grid is site-block major, slice-group minor)
   double bc[4];     // boundary sign per direction
   int cb;           // input checkerboard (as the reference's cb argument)
   int dag;
@@ -72,81 +94,89 @@ struct HopViews {
   SpinorView b;           // RES: right-hand side (double)
 };
 
-__device__ __forceinline__ long site_cb(int x, int hx, int y, int z, int t, const int *L) {
-  return (long)(x >> 1) + (long)hx * (y + (long)L[1] * (z + (long)L[2] * t));
-}
-
 // acc = sum over mu of the forward and backward hops into output site i,
 // slice sl, whose 4D parity is pout (input parity pin = 1 - pout).
-template <int P, int RECON>
-__device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v, long i, long sl,
+// All site arithmetic is 32-bit; the coordinates come from three
+// multiply-high divisions and each neighbour index from i by a stride.
+template <int P, int RECON, bool DAG>
+__device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v, int i, long sl,
                                          int pout, typename PrecTraits<P>::real *acc) {
   using R = typename PrecTraits<P>::real;
   const int pin = 1 - pout;
-  const int hx = hp.hx;
-  const long xh = i % hx;
-  long rem = i / hx;
-  const int y = (int)(rem % hp.L[1]);
-  rem /= hp.L[1];
-  const int z = (int)(rem % hp.L[2]);
-  const int t = (int)(rem / hp.L[2]);
-  const int x = 2 * (int)xh + ((y + z + t + pout) & 1);
+  const int hx = hp.hx, Ly = hp.L[1], Lz = hp.L[2];
+  const int q1 = hp.dhx.div(i);
+  const int xh = i - q1 * hx;
+  const int q2 = hp.dly.div(q1);
+  const int y = q1 - q2 * Ly;
+  const int t = hp.dlz.div(q2);
+  const int z = q2 - t * Lz;
+  const int x = 2 * xh + ((y + z + t + pout) & 1);
   const int c[4] = {x, y, z, t};
-  const R sdag = hp.dag ? R(-1) : R(1);
+  const int stride[4] = {0, hx, hx * Ly, hx * Ly * Lz};
+  const Slice<P> in(v.in, sl);
+  // sdag is a compile-time +-1, so every (1 -+ gamma) sign folds into adds
+  constexpr R sdag = DAG ? R(-1) : R(1);
 #pragma unroll
   for (int k = 0; k < 24; k++) acc[k] = R(0);
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     // forward: U_mu(x) (1 - sdag g_mu) psi(x + mu)
     {
-      int cn[4] = {c[0], c[1], c[2], c[3]};
-      bool wrap = (c[mu] == hp.L[mu] - 1);
-      cn[mu] = wrap ? 0 : c[mu] + 1;
-      long j = site_cb(cn[0], hx, cn[1], cn[2], cn[3], hp.L);
+      const bool wrap = (c[mu] == hp.L[mu] - 1);
+      int j;
+      if (mu == 0) j = i - xh + ((wrap ? 0 : x + 1) >> 1);
+      else j = wrap ? i - (hp.L[mu] - 1) * stride[mu] : i + stride[mu];
       R psi[24];
-      SpinorIO<P>::load(v.in, sl, j, psi);
+      in.load(j, psi);
       su3<R> u;
       LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
       half_spinor<R> h = project(psi, mu, -sdag);
+      if (wrap && hp.bc[mu] < 0) negate(h);
       half_spinor<R> g = link_mul(u, h, false);
-      R w = wrap ? R(hp.bc[mu]) : R(1);
-      reconstruct_acc(acc, g, mu, -sdag, w);
+      reconstruct_acc(acc, g, mu, -sdag, R(1));
     }
     // backward: U_mu(x - mu)^dagger (1 + sdag g_mu) psi(x - mu)
     {
-      int cn[4] = {c[0], c[1], c[2], c[3]};
-      bool wrap = (c[mu] == 0);
-      cn[mu] = wrap ? hp.L[mu] - 1 : c[mu] - 1;
-      long j = site_cb(cn[0], hx, cn[1], cn[2], cn[3], hp.L);
+      const bool wrap = (c[mu] == 0);
+      int j;
+      if (mu == 0) j = i - xh + ((wrap ? hp.L[0] - 1 : x - 1) >> 1);
+      else j = wrap ? i + (hp.L[mu] - 1) * stride[mu] : i - stride[mu];
       R psi[24];
-      SpinorIO<P>::load(v.in, sl, j, psi);
+      in.load(j, psi);
       su3<R> u;
       LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
       half_spinor<R> h = project(psi, mu, sdag);
+      if (wrap && hp.bc[mu] < 0) negate(h);
       half_spinor<R> g = link_mul(u, h, true);
-      R w = wrap ? R(hp.bc[mu]) : R(1);
-      reconstruct_acc(acc, g, mu, sdag, w);
+      reconstruct_acc(acc, g, mu, sdag, R(1));
     }
   }
 }
 
 // Fifth-direction hop of the Shamir DWF operator, accumulated into acc.
-template <int P>
-__device__ __forceinline__ void hop5_dwf(const HopParams &hp, const HopViews &v, long i, int s, long rhs,
+template <int P, bool DAG>
+__device__ __forceinline__ void hop5_dwf(const HopParams &hp, const HopViews &v, int i, int s, long rhs,
                                          typename PrecTraits<P>::real *acc) {
   using R = typename PrecTraits<P>::real;
   const int ls = hp.ls;
   // the half fed from s-1 is the upper one for D, the lower one for D^dagger
-  const int hb = hp.dag ? 1 : 0, ha = 1 - hb;
+  // (register arrays are only ever indexed with compile-time offsets)
   const int sb = (s == 0) ? ls - 1 : s - 1, sa = (s == ls - 1) ? 0 : s + 1;
   const R wb = R((s == 0) ? hp.h5wall : hp.h5), wa = R((s == ls - 1) ? hp.h5wall : hp.h5);
-  R q[12];
-  SpinorIO<P>::load_half(v.in, rhs * ls + sb, i, hb, q);
+  R q[12], w[12];
+  if constexpr (!DAG) {
+    Slice<P>(v.in, rhs * ls + sb).load_half(i, 0, q);
+    Slice<P>(v.in, rhs * ls + sa).load_half(i, 1, w);
+  } else {
+    Slice<P>(v.in, rhs * ls + sa).load_half(i, 0, q);
+    Slice<P>(v.in, rhs * ls + sb).load_half(i, 1, w);
+  }
+  const R wq = DAG ? wa : wb, ww = DAG ? wb : wa;
 #pragma unroll
-  for (int k = 0; k < 12; k++) acc[12 * hb + k] += wb * q[k];
-  SpinorIO<P>::load_half(v.in, rhs * ls + sa, i, ha, q);
-#pragma unroll
-  for (int k = 0; k < 12; k++) acc[12 * ha + k] += wa * q[k];
+  for (int k = 0; k < 12; k++) {
+    acc[k] += wq * q[k];
+    acc[12 + k] += ww * w[k];
+  }
 }
 
 template <typename R>
@@ -158,16 +188,29 @@ __device__ __forceinline__ double norm2_24(const R *a) {
 }
 
 // PR: precision of r and p (CG/RES epilogues); PX: precision of sol.
-template <int P, int RECON, int EP, int PR, int PX>
-__global__ void __launch_bounds__(256) hop_kernel(const HopParams hp, const HopViews v, SolverScalars *st,
-                                                  double *partials) {
+// Minimum resident 256-thread blocks per SM the register allocator must
+// allow (2 = at most 128 registers per thread).
+#ifndef CPSGPU_HOP_MINB_DOUBLE
+#define CPSGPU_HOP_MINB_DOUBLE 2
+#endif
+#ifndef CPSGPU_HOP_MINB_SLOPPY
+#define CPSGPU_HOP_MINB_SLOPPY 3
+#endif
+
+template <int P, int RECON, int EP, int PR, int PX, bool DAG>
+__global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE : CPSGPU_HOP_MINB_SLOPPY) hop_kernel(const HopParams hp, const HopViews v, SolverScalars *st,
+                                                     double *partials) {
   using R = typename PrecTraits<P>::real;
   const long rhs = blockIdx.z;
   if (hp.gate == GATE_RUNNING && st[rhs].done) return;
   if (hp.gate == GATE_RELIABLE && (st[rhs].done || !st[rhs].reliable)) return;
 
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y * blockDim.y + threadIdx.y;
+  // consecutive blocks take the slice groups of one site block, so the
+  // fifth-direction neighbours a block reads were just read from HBM by its
+  // neighbours and are still in L2
+  const int sgrp = blockIdx.x % hp.nsg, sblk = blockIdx.x / hp.nsg;
+  const int i = sblk * blockDim.x + threadIdx.x;
+  const int s = sgrp * blockDim.y + threadIdx.y;
   const bool active = (i < hp.vh) && (s < hp.ls);
   const long sl = rhs * hp.ls + s;
   const int pin = hp.dwf ? ((s + hp.cb) & 1) : hp.cb;
@@ -175,8 +218,8 @@ __global__ void __launch_bounds__(256) hop_kernel(const HopParams hp, const HopV
 
   R acc[24];
   if (active) {
-    hop_site<P, RECON>(hp, v, i, sl, pout, acc);
-    if (hp.dwf) hop5_dwf<P>(hp, v, i, s, rhs, acc);
+    hop_site<P, RECON, DAG>(hp, v, i, sl, pout, acc);
+    if (hp.dwf) hop5_dwf<P, DAG>(hp, v, i, s, rhs, acc);
   }
 
   if constexpr (ep_mix(EP)) {
@@ -210,69 +253,97 @@ __global__ void __launch_bounds__(256) hop_kernel(const HopParams hp, const HopV
   if constexpr (EP == EP_STORE || EP == EP_MIX) {
     if (active) SpinorIO<P>::store(v.out, sl, i, acc);
   } else if constexpr (ep_axpy(EP)) {
+    // out = x + c hop, streamed 4 reals at a time (few live registers)
     double red[2] = {0.0, 0.0};
     if (active) {
-      R xv[24];
-      SpinorIO<P>::load(v.x, sl, i, xv);
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
 #pragma unroll
-      for (int k = 0; k < 24; k++) acc[k] = xv[k] + cf * acc[k];
-      SpinorIO<P>::store(v.out, sl, i, acc);
-      if (hp.norm) {
-        red[0] = norm2_24(acc);
-        red[1] = norm2_24(xv);
+      for (int c = 0; c < 6; c++) {
+        R xv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (hp.norm) red[1] += double(xv[k]) * double(xv[k]);
+          acc[4 * c + k] = xv[k] + cf * acc[4 * c + k];
+          if (hp.norm) red[0] += double(acc[4 * c + k]) * double(acc[4 * c + k]);
+        }
+        if constexpr (P != PREC_HALF) Chunk4<P>::store(v.out, sl, i, c, acc + 4 * c);
       }
+      if constexpr (P == PREC_HALF) SpinorIO<P>::store(v.out, sl, i, acc);
     }
     if (hp.norm) grid_reduce_finalize<2>(red, partials, st, hp.red_op);
   } else if constexpr (ep_cg(EP)) {
+    // q = x + c hop + shift p;  r -= alpha q;  sol += alpha p;  |r|^2
     using RR = typename PrecTraits<PR>::real;
     using RX = typename PrecTraits<PX>::real;
     double red[1] = {0.0};
     if (active) {
-      R xv[24];
-      SpinorIO<P>::load(v.x, sl, i, xv);
-      RR pv[24], rv[24];
-      RX sv[24];
-      SpinorIO<PR>::load(v.p, sl, i, pv);
-      SpinorIO<PR>::load(v.r, sl, i, rv);
-      if (v.sol.data) SpinorIO<PX>::load(v.sol, sl, i, sv);
-      else
-#pragma unroll
-        for (int k = 0; k < 24; k++) sv[k] = RX(0);
       const double alpha = st[rhs].alpha;
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
       const R sh = R(st[rhs].shift);
       const RR a = RR(alpha);
       const RX ax = RX(alpha);
+      const bool with_sol = (v.sol.data != nullptr);  // the multishift solver keeps its own solutions
+      RR rfull[PR == PREC_HALF ? 24 : 1];
 #pragma unroll
-      for (int k = 0; k < 24; k++) {
-        R q = xv[k] + cf * acc[k] + sh * R(pv[k]);
-        rv[k] = rv[k] - a * RR(q);
-        sv[k] = sv[k] + ax * RX(pv[k]);
+      for (int c = 0; c < 6; c++) {
+        R xv[4];
+        RR pv[4], rv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+        Chunk4<PR>::load(v.p, sl, i, c, pv);
+        Chunk4<PR>::load(v.r, sl, i, c, rv);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          R q = xv[k] + cf * acc[4 * c + k] + sh * R(pv[k]);
+          rv[k] = rv[k] - a * RR(q);
+          red[0] += double(rv[k]) * double(rv[k]);
+        }
+        if constexpr (PR == PREC_HALF) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
+        } else {
+          Chunk4<PR>::store(v.r, sl, i, c, rv);
+        }
+        if (with_sol) {
+          RX sv[4];
+          Chunk4<PX>::load(v.sol, sl, i, c, sv);
+#pragma unroll
+          for (int k = 0; k < 4; k++) sv[k] = sv[k] + ax * RX(pv[k]);
+          if constexpr (PX != PREC_HALF) Chunk4<PX>::store(v.sol, sl, i, c, sv);
+        }
       }
-      SpinorIO<PR>::store(v.r, sl, i, rv);
-      // the multishift solver updates its solutions itself (no sol view)
-      if (v.sol.data) SpinorIO<PX>::store(v.sol, sl, i, sv);
-      red[0] = norm2_24(rv);
+      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
     grid_reduce_finalize<1>(red, partials, st, hp.red_op);
   } else if constexpr (ep_res(EP)) {
+    // r = b - (x + c hop + shift sol), stored in r's precision;  |r|^2
+    using RR = typename PrecTraits<PR>::real;
     double red[1] = {0.0};
     if (active) {
-      R xv[24], bv[24], sv[24];
-      SpinorIO<P>::load(v.x, sl, i, xv);
-      SpinorIO<P>::load(v.b, sl, i, bv);
-      SpinorIO<P>::load(v.sol, sl, i, sv);
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
       const R sh = R(st[rhs].shift);
+      RR rfull[PR == PREC_HALF ? 24 : 1];
 #pragma unroll
-      for (int k = 0; k < 24; k++) acc[k] = bv[k] - (xv[k] + cf * acc[k] + sh * sv[k]);
-      red[0] = norm2_24(acc);
-      using RR = typename PrecTraits<PR>::real;
-      RR rv[24];
+      for (int c = 0; c < 6; c++) {
+        R xv[4], bv[4], sv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+        Chunk4<P>::load(v.b, sl, i, c, bv);
+        Chunk4<P>::load(v.sol, sl, i, c, sv);
+        RR rv[4];
 #pragma unroll
-      for (int k = 0; k < 24; k++) rv[k] = RR(acc[k]);
-      SpinorIO<PR>::store(v.r, sl, i, rv);
+        for (int k = 0; k < 4; k++) {
+          R q = bv[k] - (xv[k] + cf * acc[4 * c + k] + sh * sv[k]);
+          red[0] += double(q) * double(q);
+          rv[k] = RR(q);
+        }
+        if constexpr (PR == PREC_HALF) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
+        } else {
+          Chunk4<PR>::store(v.r, sl, i, c, rv);
+        }
+      }
+      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
     grid_reduce_finalize<1>(red, partials, st, hp.red_op);
   }
