@@ -66,6 +66,7 @@ def lib() -> C.CDLL:
             "cpsgpu_dslash": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_matpc": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
             "cpsgpu_matpc_dag_matpc": (C.c_int, [vp, _dp, _dp, _dp, C.c_int]),
+            "cpsgpu_matpc_dag_matpc_noalloc": (C.c_int, [vp, vp, vp, _dp]),
             "cpsgpu_mobius_dslash_4": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_mobius_m5inv": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),

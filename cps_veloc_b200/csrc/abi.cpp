@@ -17,6 +17,7 @@ void gen_gaussian(double *out, long n, uint64_t seed, unsigned stream);
 int autotune(Dirac &D, int prec, int nrhs);
 double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes);
 double time_mdagm(Dirac &D, int prec, int reps, double *bytes);
+double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
 int minvcg(Dirac &D, double *const *psi, const double *chi, double chi_norm, const double *shift, int nshift,
            double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine);
 }  // namespace cpsgpu
@@ -287,6 +288,16 @@ int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double
       CPSGPU_CUDA(cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost));
       *dot = h.sum[0];
     }
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_matpc_dag_matpc_noalloc(cpsgpu_dirac d, double *out_dev, const double *in_dev, double *dot) {
+  return guarded([&] {
+    if (!d || !out_dev || !in_dev) throw Error(CPSGPU_ERR_ARG, "null argument");
+    need_gauge(d);
+    const double r = matpc_dag_matpc_noalloc(*d->D, out_dev, in_dev);
+    if (dot) *dot = r;
     return CPSGPU_OK;
   });
 }

@@ -125,6 +125,22 @@ int cpsgpu_matpc(cpsgpu_dirac d, double *out, const double *in, int dag, int pre
  * dwf_mdagm (dwf_mdagm.C:32), zmobius_mdagm (zmobius_mdagm.C:32).
  * *dot = |MatPc in|^2 when dot is non-null. */
 int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double *dot, int prec);
+/* No counterpart in the reference.  The same FP64 MatPcDagMatPc for callers
+ * that cannot allocate device memory when they apply the operator (their
+ * device memory belongs to their own pool allocator, or they cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree).  in_dev and out_dev are
+ * caller-owned device pointers holding one FP64 field in the library's
+ * device layout: reals (2g, 2g+1) of CPS site i in slice s at
+ * double2 index (s*12 + g)*Vol/2 + i.  Every temporary lives in one fixed
+ * 64 MiB device array that the library holds on each GPU it is used on until
+ * the process exits, so the call allocates nothing; operators whose two FP64
+ * fields do not fit in it (more than about 170k 5D sites) are rejected with
+ * CPSGPU_ERR_ARG.  Wilson and DWF only.  The first call on a device looks up
+ * that array's address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (from several threads or
+ * streams) race.  *dot = |MatPc in|^2 when dot is non-null.  Returns when the
+ * result is in out_dev; the caller must have finished writing in_dev. */
+int cpsgpu_matpc_dag_matpc_noalloc(cpsgpu_dirac d, double *out_dev, const double *in_dev, double *dot);
 /* Mobius pieces: zmobius_dslash_4 (zmobius_dslash_4.C:209) and the
  * out-of-place zmobius_m5inv (zmobius_m5inv.C:822). */
 int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);
