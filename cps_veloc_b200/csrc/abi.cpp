@@ -195,6 +195,16 @@ int cpsgpu_gauge_info(cpsgpu_lattice lat, double *recon_err, int *recon12) {
   });
 }
 
+int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    if (prec != CPSGPU_SINGLE && prec != CPSGPU_HALF) throw Error(CPSGPU_ERR_ARG, "FP32 or FP16 only");
+    if (reals != 12 && reals != 18) throw Error(CPSGPU_ERR_ARG, "reals must be 12 or 18");
+    lat->L->sloppy_recon[prec] = reals;
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_synchronize(cpsgpu_lattice lat) {
   return guarded([&] {
     if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");

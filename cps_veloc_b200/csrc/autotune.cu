@@ -31,7 +31,6 @@ float time_launch(const Dirac &D, HopLaunch &Lh, const Field &in, const Field &o
 
 int autotune(Dirac &D, int prec, int nrhs) {
   Lattice &L = *D.lat;
-  const int recon = L.recon(prec);
   Field in(prec, L.vh, D.ls, nrhs), out(prec, L.vh, D.ls, nrhs), x(prec, L.vh, D.ls, nrhs);
   launch_zero(L.stream, in);
   launch_zero(L.stream, x);
@@ -41,8 +40,15 @@ int autotune(Dirac &D, int prec, int nrhs) {
   CPSGPU_CUDA(cudaEventCreate(&e0));
   CPSGPU_CUDA(cudaEventCreate(&e1));
   int tuned = 0;
-  // plain hop shapes (also used by the AXPY / CG / RES epilogues)
-  {
+  // plain hop shapes (also used by the AXPY / CG / RES epilogues); for FP32
+  // and FP16 also the stored link form (12 reals rebuilt, or all 18)
+  std::vector<int> recons;
+  if (prec == PREC_DOUBLE) recons.push_back(L.recon(prec));
+  else recons = {12, 18};
+  float best_recon_t = 1e30f;
+  int best_recon = recons[0];
+  for (int recon : recons) {
+    if (prec != PREC_DOUBLE) L.sloppy_recon[prec] = recon;
     HopLaunch Lh;
     Lh.prec = prec;
     Lh.ep = EP_STORE;
@@ -66,7 +72,27 @@ int autotune(Dirac &D, int prec, int nrhs) {
       tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb);
       tuned++;
     }
+    if (prec != PREC_DOUBLE) {
+      // the link form is chosen on a whole MatPcDagMatPc: its epilogue
+      // kernels need more registers than the plain hop
+      OpWork w;
+      SolverScalars *st = L.scratch_st.as<SolverScalars>();
+      CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
+      for (int k = 0; k < 2; k++) op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
+      CPSGPU_CUDA(cudaEventRecord(e0, L.stream));
+      for (int k = 0; k < 3; k++) op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
+      CPSGPU_CUDA(cudaEventRecord(e1, L.stream));
+      CPSGPU_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_recon_t) {
+        best_recon_t = ms;
+        best_recon = recon;
+      }
+    }
   }
+  if (prec != PREC_DOUBLE) L.sloppy_recon[prec] = best_recon;
+  const int recon = L.recon(prec);
   if (D.kind == KIND_MOBIUS) {
     HopLaunch Lh;
     Lh.prec = prec;

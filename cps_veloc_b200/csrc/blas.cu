@@ -211,7 +211,8 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
 
 __global__ void gauge_import_kernel(const double *src, long vh, int L0, int L1, int L2, int L3, double bc0,
                                     double bc1, double bc2, double bc3, int signs_applied, double2 *d18,
-                                    double2 *d12, float4 *s12, uint2 *h12, double *recon_err) {
+                                    double2 *d12, float4 *s12, uint2 *h12, float4 *s18, uint4 *h18,
+                                    double *recon_err) {
   long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over 2 * vh * 4
   if (idx >= 8 * vh) return;
   const int mu = (int)(idx % 4);
@@ -245,6 +246,25 @@ __global__ void gauge_import_kernel(const double *src, long vh, int L0, int L1, 
     h[0] = __floats2half2_rn((float)a.re, (float)a.im);
     h[1] = __floats2half2_rn((float)b.re, (float)b.im);
     h12[(gbase * 3 + k) * vh + i] = q;
+  }
+  // full links (layouts at LinkIO<PREC_SINGLE / PREC_HALF, 18>)
+  for (int k = 0; k < 4; k++) {
+    cplx<double> a = u[(2 * k) / 3][(2 * k) % 3], b = u[(2 * k + 1) / 3][(2 * k + 1) % 3];
+    s18[(gbase * 4 + k) * vh + i] = make_float4((float)a.re, (float)a.im, (float)b.re, (float)b.im);
+  }
+  reinterpret_cast<float2 *>(s18 + 32 * vh)[gbase * vh + i] = make_float2((float)u[2][2].re, (float)u[2][2].im);
+  for (int k = 0; k < 2; k++) {
+    uint4 q;
+    __half2 *h = reinterpret_cast<__half2 *>(&q);
+    for (int c = 0; c < 4; c++) {
+      cplx<double> a = u[(4 * k + c) / 3][(4 * k + c) % 3];
+      h[c] = __floats2half2_rn((float)a.re, (float)a.im);
+    }
+    h18[(gbase * 2 + k) * vh + i] = q;
+  }
+  {
+    __half2 h = __floats2half2_rn((float)u[2][2].re, (float)u[2][2].im);
+    reinterpret_cast<__half2 *>(h18 + 16 * vh)[gbase * vh + i] = h;
   }
   su3<double> w;
   for (int row = 0; row < 3; row++)
@@ -375,13 +395,15 @@ void import_gauge(Lattice &L, const double *host, int signs_applied) {
   L.gD12.ensure(nlinks * 12 * sizeof(double));
   L.gS12.ensure(nlinks * 12 * sizeof(float));
   L.gH12.ensure(nlinks * 12 * sizeof(__half));
+  L.gS18.ensure(nlinks * 18 * sizeof(float));
+  L.gH18.ensure(nlinks * 18 * sizeof(__half));
   CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, host, nlinks * 18 * sizeof(double), cudaMemcpyHostToDevice, L.stream));
   DeviceBuffer err(sizeof(double));
   CPSGPU_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(double), L.stream));
   gauge_import_kernel<<<blocks_for(nlinks), TPB, 0, L.stream>>>(
       L.staging.as<double>(), vh, L.L[0], L.L[1], L.L[2], L.L[3], L.bc[0], L.bc[1], L.bc[2], L.bc[3],
       signs_applied, L.gD18.as<double2>(), L.gD12.as<double2>(), L.gS12.as<float4>(), L.gH12.as<uint2>(),
-      err.as<double>());
+      L.gS18.as<float4>(), L.gH18.as<uint4>(), err.as<double>());
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;
   double e = 0.0;

@@ -80,6 +80,7 @@ struct Lattice {
   cudaStream_t stream = nullptr;
   // gauge field copies: FP64 full and compressed, FP32 and FP16 compressed
   DeviceBuffer gD18, gD12, gS12, gH12;
+  DeviceBuffer gS18, gH18;  // full-link FP32 / FP16 copies (fields.cuh LinkIO<.., 18>)
   bool have_gauge = false;
   double recon_err = 0.0;  // max |row2 - conj(row0 x row1)| over all links
   bool use_recon12 = true; // FP64 operator reads 12-real links
@@ -90,7 +91,13 @@ struct Lattice {
   Lattice(const int L_[4], const double bc_[4]);
   ~Lattice();
   GaugeView gauge(int prec) const;
-  int recon(int prec) const { return (prec == PREC_DOUBLE && !use_recon12) ? 18 : 12; }
+  // reals per stored link a precision reads: FP64 uses 12 when the links are
+  // SU(3); FP32 / FP16 use sloppy_recon[prec] (12 or 18, set by the autotuner)
+  int sloppy_recon[3] = {12, 18, 18};
+  int recon(int prec) const {
+    if (prec == PREC_DOUBLE) return use_recon12 ? 12 : 18;
+    return sloppy_recon[prec];
+  }
 };
 
 struct Dirac {

@@ -121,6 +121,16 @@ __device__ __forceinline__ void unpack8(uint4 q, float s, float *v) {
   }
 }
 
+__device__ __forceinline__ void unpack8_raw(uint4 q, float *v) {
+  const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    float2 f = __half22float2(h[k]);
+    v[2 * k] = f.x;
+    v[2 * k + 1] = f.y;
+  }
+}
+
 // Half precision: 24 fp16 values scaled by a per-site float norm (the
 // largest magnitude in the spinor), so every stored value lies in [-1, 1].
 template <> struct SpinorIO<PREC_HALF> {
@@ -182,6 +192,15 @@ template <> struct Slice<PREC_DOUBLE> {
       v[2 * g + 1] = q.y;
     }
   }
+  // values and their common scale (always 1 here; FP16 storage returns its norm)
+  __device__ __forceinline__ void load_raw(int j, double *v, double &scale) const {
+    load(j, v);
+    scale = 1.0;
+  }
+  __device__ __forceinline__ void load_half_raw(int j, int half, double *v, double &scale) const {
+    load_half(j, half, v);
+    scale = 1.0;
+  }
   __device__ __forceinline__ void load_half(int j, int half, double *v) const {
     const double2 *b = d + 6 * half * vh + j;
 #pragma unroll
@@ -204,6 +223,14 @@ template <> struct Slice<PREC_SINGLE> {
       v[4 * g] = q.x; v[4 * g + 1] = q.y; v[4 * g + 2] = q.z; v[4 * g + 3] = q.w;
     }
   }
+  __device__ __forceinline__ void load_raw(int j, float *v, float &scale) const {
+    load(j, v);
+    scale = 1.0f;
+  }
+  __device__ __forceinline__ void load_half_raw(int j, int half, float *v, float &scale) const {
+    load_half(j, half, v);
+    scale = 1.0f;
+  }
   __device__ __forceinline__ void load_half(int j, int half, float *v) const {
     const float4 *b = d + 3 * half * vh + j;
 #pragma unroll
@@ -223,6 +250,28 @@ template <> struct Slice<PREC_HALF> {
     const float s = __ldg(n + j);
 #pragma unroll
     for (int g = 0; g < 3; g++) unpack8(__ldg(d + j + g * vh), s, v + 8 * g);
+  }
+  // the stored values unscaled, and the site's norm: the caller folds the
+  // norm into a multiply it does anyway (24 fewer multiplies per site)
+  __device__ __forceinline__ void load_raw(int j, float *v, float &scale) const {
+    scale = __ldg(n + j);
+#pragma unroll
+    for (int g = 0; g < 3; g++) unpack8_raw(__ldg(d + j + g * vh), v + 8 * g);
+  }
+  __device__ __forceinline__ void load_half_raw(int j, int half, float *v, float &scale) const {
+    scale = __ldg(n + j);
+    float tmp[16];
+    if (half == 0) {
+      unpack8_raw(__ldg(d + j), tmp);
+      unpack8_raw(__ldg(d + j + vh), tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[k];
+    } else {
+      unpack8_raw(__ldg(d + j + vh), tmp);
+      unpack8_raw(__ldg(d + j + 2 * vh), tmp + 8);
+#pragma unroll
+      for (int k = 0; k < 12; k++) v[k] = tmp[4 + k];
+    }
   }
   __device__ __forceinline__ void load_half(int j, int half, float *v) const {
     const float s = __ldg(n + j);
@@ -330,6 +379,50 @@ template <> struct LinkIO<PREC_HALF, 12> {
       u.m[(e + 1) / 3][(e + 1) % 3] = {b.x, b.y};
     }
     reconstruct_row2(u);
+  }
+};
+
+// Full 18-real sloppy links: no third-row rebuild (24 fewer flops per link),
+// for kernels bound by instruction issue rather than by HBM.
+//   FP32: elements 0-7 as four float4 (two complex each) at
+//         f4[((p*4 + mu)*4 + k)*vh + i], element 8 as float2 at
+//         f2[(p*4 + mu)*vh + i] after the 32*vh float4            (72 B)
+//   FP16: elements 0-7 as two uint4 (four complex each) at
+//         u4[((p*4 + mu)*2 + k)*vh + i], element 8 as one half2 at
+//         u1[(p*4 + mu)*vh + i] after the 16*vh uint4             (36 B)
+template <> struct LinkIO<PREC_SINGLE, 18> {
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
+    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * 4) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float4 q = __ldg(d + k * g.vh);
+      u.m[(2 * k) / 3][(2 * k) % 3] = {q.x, q.y};
+      u.m[(2 * k + 1) / 3][(2 * k + 1) % 3] = {q.z, q.w};
+    }
+    const float2 *e = reinterpret_cast<const float2 *>(reinterpret_cast<const float4 *>(g.data) + 32 * g.vh) +
+                      (p * 4 + mu) * g.vh + i;
+    float2 q = __ldg(e);
+    u.m[2][2] = {q.x, q.y};
+  }
+};
+template <> struct LinkIO<PREC_HALF, 18> {
+  static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
+    const uint4 *d = reinterpret_cast<const uint4 *>(g.data) + ((p * 4 + mu) * 2) * g.vh + i;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      uint4 q = __ldg(d + k * g.vh);
+      const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float2 a = __half22float2(h[c]);
+        u.m[(4 * k + c) / 3][(4 * k + c) % 3] = {a.x, a.y};
+      }
+    }
+    const unsigned *e = reinterpret_cast<const unsigned *>(reinterpret_cast<const uint4 *>(g.data) + 16 * g.vh) +
+                        (p * 4 + mu) * g.vh + i;
+    unsigned q = __ldg(e);
+    float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q));
+    u.m[2][2] = {a.x, a.y};
   }
 };
 

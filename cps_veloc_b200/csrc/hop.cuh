@@ -126,14 +126,14 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
       int j;
       if (mu == 0) j = i - xh + ((wrap ? 0 : x + 1) >> 1);
       else j = wrap ? i - (hp.L[mu] - 1) * stride[mu] : i + stride[mu];
-      R psi[24];
-      in.load(j, psi);
+      R psi[24], sc;
+      in.load_raw(j, psi, sc);
       su3<R> u;
       LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
       half_spinor<R> h = project(psi, mu, -sdag);
-      if (wrap && hp.bc[mu] < 0) negate(h);
       half_spinor<R> g = link_mul(u, h, false);
-      reconstruct_acc(acc, g, mu, -sdag, R(1));
+      // the storage scale and the boundary sign ride on the accumulating FMAs
+      reconstruct_acc(acc, g, mu, -sdag, (wrap && hp.bc[mu] < 0) ? -sc : sc);
     }
     // backward: U_mu(x - mu)^dagger (1 + sdag g_mu) psi(x - mu)
     {
@@ -141,14 +141,13 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
       int j;
       if (mu == 0) j = i - xh + ((wrap ? hp.L[0] - 1 : x - 1) >> 1);
       else j = wrap ? i + (hp.L[mu] - 1) * stride[mu] : i - stride[mu];
-      R psi[24];
-      in.load(j, psi);
+      R psi[24], sc;
+      in.load_raw(j, psi, sc);
       su3<R> u;
       LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
       half_spinor<R> h = project(psi, mu, sdag);
-      if (wrap && hp.bc[mu] < 0) negate(h);
       half_spinor<R> g = link_mul(u, h, true);
-      reconstruct_acc(acc, g, mu, sdag, R(1));
+      reconstruct_acc(acc, g, mu, sdag, (wrap && hp.bc[mu] < 0) ? -sc : sc);
     }
   }
 }
@@ -163,15 +162,15 @@ __device__ __forceinline__ void hop5_dwf(const HopParams &hp, const HopViews &v,
   // (register arrays are only ever indexed with compile-time offsets)
   const int sb = (s == 0) ? ls - 1 : s - 1, sa = (s == ls - 1) ? 0 : s + 1;
   const R wb = R((s == 0) ? hp.h5wall : hp.h5), wa = R((s == ls - 1) ? hp.h5wall : hp.h5);
-  R q[12], w[12];
+  R q[12], w[12], sq_, sw_;
   if constexpr (!DAG) {
-    Slice<P>(v.in, rhs * ls + sb).load_half(i, 0, q);
-    Slice<P>(v.in, rhs * ls + sa).load_half(i, 1, w);
+    Slice<P>(v.in, rhs * ls + sb).load_half_raw(i, 0, q, sq_);
+    Slice<P>(v.in, rhs * ls + sa).load_half_raw(i, 1, w, sw_);
   } else {
-    Slice<P>(v.in, rhs * ls + sa).load_half(i, 0, q);
-    Slice<P>(v.in, rhs * ls + sb).load_half(i, 1, w);
+    Slice<P>(v.in, rhs * ls + sa).load_half_raw(i, 0, q, sq_);
+    Slice<P>(v.in, rhs * ls + sb).load_half_raw(i, 1, w, sw_);
   }
-  const R wq = DAG ? wa : wb, ww = DAG ? wb : wa;
+  const R wq = (DAG ? wa : wb) * sq_, ww = (DAG ? wb : wa) * sw_;
 #pragma unroll
   for (int k = 0; k < 12; k++) {
     acc[k] += wq * q[k];

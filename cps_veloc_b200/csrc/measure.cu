@@ -13,7 +13,8 @@ namespace {
 size_t spinor_bytes(int prec) { return prec == PREC_DOUBLE ? 192 : prec == PREC_SINGLE ? 96 : 52; }
 size_t link_bytes(int prec, int recon) {
   if (prec == PREC_DOUBLE) return recon == 18 ? 144 : 96;
-  return prec == PREC_SINGLE ? 48 : 24;
+  if (prec == PREC_SINGLE) return recon == 18 ? 72 : 48;
+  return recon == 18 ? 36 : 24;
 }
 
 // enough field pairs that the rotation's working set is > 2 x L2

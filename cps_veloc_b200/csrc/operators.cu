@@ -51,9 +51,9 @@ GaugeView Lattice::gauge(int prec) const {
   if (prec == PREC_DOUBLE)
     g.data = use_recon12 ? gD12.ptr : gD18.ptr;
   else if (prec == PREC_SINGLE)
-    g.data = gS12.ptr;
+    g.data = recon(prec) == 18 ? gS18.ptr : gS12.ptr;
   else
-    g.data = gH12.ptr;
+    g.data = recon(prec) == 18 ? gH18.ptr : gH12.ptr;
   return g;
 }
 

@@ -92,6 +92,9 @@ int cpsgpu_import_gauge(cpsgpu_lattice lat, const double *u_wilson, int signs_ap
 /* max |row2 - conj(row0 x row1)| over all links, and whether FP64 uses 12 reals */
 int cpsgpu_gauge_info(cpsgpu_lattice lat, double *recon_err, int *fp64_recon12);
 int cpsgpu_synchronize(cpsgpu_lattice lat);
+/* Stored link form of the FP32 or FP16 operator: 12 reals (third row rebuilt
+ * in registers) or 18.  cpsgpu_autotune picks the faster; this overrides it. */
+int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals);
 
 /* ---- Dirac operators ---- */
 typedef struct {

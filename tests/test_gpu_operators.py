@@ -16,6 +16,17 @@ TOL = {A.DOUBLE: 1e-13, A.SINGLE: 2e-6, A.HALF: 5e-3}
 PRECS = [A.DOUBLE, A.SINGLE, A.HALF]
 
 
+@pytest.fixture(params=[18, 12], ids=["links18", "links12"])
+def link_reals(request):
+    """FP32 / FP16 operators read full links or rebuild the third row."""
+    return request.param
+
+
+def _set_links(lat, reals):
+    for prec in (A.SINGLE, A.HALF):
+        A.check(A.lib().cpsgpu_set_link_reals(lat._h, prec, reals))
+
+
 def _lat(L, u, bc=(1, 1, 1, -1), signs=False):
     lat = Lattice(L, bc)
     lat.import_gauge(apply_bc_signs(u, L, bc) if signs else u, signs_applied=signs)
@@ -24,10 +35,11 @@ def _lat(L, u, bc=(1, 1, 1, -1), signs=False):
 
 @pytest.mark.parametrize("L,bc", [((4, 4, 4, 4), (1, 1, 1, -1)), ((8, 8, 8, 8), (1, 1, 1, -1)),
                                   ((4, 6, 2, 8), (-1, 1, -1, -1)), ((2, 2, 2, 2), (1, 1, 1, 1))])
-def test_wilson_operators(oracle, L, bc):
+def test_wilson_operators(oracle, link_reals, L, bc):
     u = gen_gauge(L, seed=31)
     ops = OracleOps(oracle, L, u, ls=1, bc=bc)
     lat = _lat(L, u, bc)
+    _set_links(lat, link_reals)
     D = DiracOpWilson(lat, mass=1 / (2 * 0.12) - 4)
     assert D.kappa == pytest.approx(0.12, rel=1e-15)
     psi = gen_gaussian(ops.n, seed=32)
@@ -71,10 +83,11 @@ def test_non_su3_links_use_18_reals(oracle):
 
 
 @pytest.mark.parametrize("L,ls,mass", [((4, 4, 4, 8), 8, 0.01), ((4, 2, 4, 4), 5, 0.1), ((2, 2, 2, 2), 2, 0.5)])
-def test_dwf_operators(oracle, L, ls, mass):
+def test_dwf_operators(oracle, link_reals, L, ls, mass):
     u = gen_gauge(L, seed=41)
     ops = OracleOps(oracle, L, u, ls=ls)
     lat = _lat(L, u)
+    _set_links(lat, link_reals)
     D = DiracOpDwf(lat, mass=mass, ls=ls, m5=1.8)
     psi = gen_gaussian(ops.n, seed=42)
     for prec in PRECS:
@@ -90,10 +103,11 @@ def test_dwf_operators(oracle, L, ls, mass):
 
 @pytest.mark.parametrize("L,ls,mass,b,c", [((4, 4, 4, 8), 12, 0.005, 1.5, 0.5), ((4, 2, 4, 4), 5, 0.1, 2.0, 1.0),
                                            ((2, 2, 4, 4), 4, 0.3, 1.0, 0.0)])
-def test_mobius_operators(oracle, L, ls, mass, b, c):
+def test_mobius_operators(oracle, link_reals, L, ls, mass, b, c):
     u = gen_gauge(L, seed=51)
     ops = OracleOps(oracle, L, u, ls=ls, b=b, c=c)
     lat = _lat(L, u)
+    _set_links(lat, link_reals)
     D = DiracOpMobius(lat, mass=mass, ls=ls, m5=1.8, b=b, c=c)
     psi = gen_gaussian(ops.n, seed=52)
     for prec in PRECS:
