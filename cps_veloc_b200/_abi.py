@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
             "cpsgpu_gauge_info": (C.c_int, [vp, _dp, C.POINTER(C.c_int)]),
             "cpsgpu_synchronize": (C.c_int, [vp]),
             "cpsgpu_set_link_reals": (C.c_int, [vp, C.c_int, C.c_int]),
+            "cpsgpu_get_rhs_tile": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_set_rhs_tile": (C.c_int, [vp, C.c_int, C.c_int]),
             "cpsgpu_dirac_create": (C.c_int, [vp, C.POINTER(DiracArg), C.POINTER(vp)]),
             "cpsgpu_dirac_destroy": (C.c_int, [vp]),
             "cpsgpu_dirac_info": (C.c_int, [vp, _dp, _dp]),

@@ -1,5 +1,6 @@
 // The C ABI (include/cpsgpu.h): argument checking, object lifetimes,
 // host <-> device staging in CPS storage order, and error translation.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -511,6 +512,24 @@ int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned) {
     need_gauge(d);
     int n = autotune(*d->D, prec, nrhs);
     if (tuned) *tuned = n;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_get_rhs_tile(cpsgpu_dirac d, int prec, int nrhs, int *tile) {
+  return guarded([&] {
+    if (!d || nrhs < 1 || !tile) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    *tile = std::max(1, std::min(d->D->rhs_tile(prec, nrhs), nrhs));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
+  return guarded([&] {
+    if (!d || tile < 0) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    d->D->rtile[prec] = tile;
     return CPSGPU_OK;
   });
 }

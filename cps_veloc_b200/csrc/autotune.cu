@@ -93,6 +93,26 @@ int autotune(Dirac &D, int prec, int nrhs) {
   }
   if (prec != PREC_DOUBLE) L.sloppy_recon[prec] = best_recon;
   const int recon = L.recon(prec);
+  if (nrhs > 1) {
+    // right-hand-side tile: how many solves' blocks of the same sites run
+    // back to back (link reuse across right-hand sides)
+    HopLaunch Lh;
+    Lh.prec = prec;
+    Lh.ep = D.kind == KIND_MOBIUS ? EP_MIX : EP_STORE;
+    Lh.mix = D.kind == KIND_MOBIUS ? D.mixQ.as<double>() : nullptr;
+    Lh.cb = 1;
+    float best = 1e30f;
+    int bestr = 1;
+    const int tiles[] = {1, 2, 4, 8, 12, 16};
+    for (int r : tiles) {
+      if (r > nrhs) break;
+      D.rtile[prec] = r;
+      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
+      if (t < best) { best = t; bestr = r; }
+    }
+    D.rtile[prec] = bestr;
+    tuned++;
+  }
   if (D.kind == KIND_MOBIUS) {
     HopLaunch Lh;
     Lh.prec = prec;

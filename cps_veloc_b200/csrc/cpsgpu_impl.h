@@ -113,6 +113,13 @@ struct Dirac {
   DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id;
   std::vector<double> hM5i, hM5id, hB, hBd;
   Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_);
+  // right-hand sides per hop tile (consecutive blocks share links across
+  // this many solves), per precision, set by the autotuner; 0 = untuned
+  int rtile[3] = {0, 0, 0};
+  int rhs_tile(int prec, int nrhs) const {
+    const int t = rtile[prec];
+    return t > 0 ? t : (nrhs < 4 ? nrhs : 4);
+  }
 };
 
 // ---- kernels / launchers (hop.cu, blas.cu) ----

@@ -1,4 +1,5 @@
 // Launch configuration and template dispatch of the hop kernel (hop.cuh).
+#include <algorithm>
 #include <cstring>
 
 #include "cpsgpu_impl.h"
@@ -105,7 +106,9 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   dim3 block = hop_block(key, mix);
   const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
   hp.nsg = (D.ls + block.y - 1) / block.y;
-  dim3 grid(nsb * hp.nsg, 1, (unsigned)in.nrhs);
+  hp.nrhs = in.nrhs;
+  hp.rtile = std::max(1, std::min(D.rhs_tile(L.prec, in.nrhs), in.nrhs));
+  dim3 grid(nsb * hp.nsg * hp.rtile, 1, (unsigned)((in.nrhs + hp.rtile - 1) / hp.rtile));
   size_t smem = 0;
   if (mix) {
     smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double);

@@ -74,6 +74,8 @@ struct HopParams {
   int ls;
   FastDiv dhx, dly, dlz;  // divisions by L[0]/2, L[1], L[2]
   int nsg;          // slice groups in the launch (grid is site-block major, slice-group minor)
+  int rtile;        // right-hand sides per tile: consecutive blocks take the same sites of rtile solves
+  int nrhs;         // right-hand sides in the launch
   double bc[4];     // boundary sign per direction
   int cb;           // input checkerboard (as the reference's cb argument)
   int dag;
@@ -200,14 +202,17 @@ template <int P, int RECON, int EP, int PR, int PX, bool DAG>
 __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE : CPSGPU_HOP_MINB_SLOPPY) hop_kernel(const HopParams hp, const HopViews v, SolverScalars *st,
                                                      double *partials) {
   using R = typename PrecTraits<P>::real;
-  const long rhs = blockIdx.z;
+  // blockIdx.x = (site block, slice group, rhs within the tile), rhs fastest:
+  // consecutive blocks read the same links (for rtile solves) and the same
+  // fifth-direction neighbourhoods, which are then still in L1 / L2
+  const int rin = blockIdx.x % hp.rtile, sb = blockIdx.x / hp.rtile;
+  const long rhs = (long)blockIdx.z * hp.rtile + rin;
+  if (rhs >= hp.nrhs) return;  // the last tile may be partial
   if (hp.gate == GATE_RUNNING && st[rhs].done) return;
   if (hp.gate == GATE_RELIABLE && (st[rhs].done || !st[rhs].reliable)) return;
+  const unsigned nblk = gridDim.x / hp.rtile;  // blocks of one solve
 
-  // consecutive blocks take the slice groups of one site block, so the
-  // fifth-direction neighbours a block reads were just read from HBM by its
-  // neighbours and are still in L2
-  const int sgrp = blockIdx.x % hp.nsg, sblk = blockIdx.x / hp.nsg;
+  const int sgrp = sb % hp.nsg, sblk = sb / hp.nsg;
   const int i = sblk * blockDim.x + threadIdx.x;
   const int s = sgrp * blockDim.y + threadIdx.y;
   const bool active = (i < hp.vh) && (s < hp.ls);
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       }
       if constexpr (P == PREC_HALF) SpinorIO<P>::store(v.out, sl, i, acc);
     }
-    if (hp.norm) grid_reduce_finalize<2>(red, partials, st, hp.red_op);
+    if (hp.norm) grid_reduce_finalize<2>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
   } else if constexpr (ep_cg(EP)) {
     // q = x + c hop + shift p;  r -= alpha q;  sol += alpha p;  |r|^2
     using RR = typename PrecTraits<PR>::real;
@@ -313,7 +318,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       }
       if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
-    grid_reduce_finalize<1>(red, partials, st, hp.red_op);
+    grid_reduce_finalize<1>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
   } else if constexpr (ep_res(EP)) {
     // r = b - (x + c hop + shift sol), stored in r's precision;  |r|^2
     using RR = typename PrecTraits<PR>::real;
@@ -344,7 +349,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       }
       if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
-    grid_reduce_finalize<1>(red, partials, st, hp.red_op);
+    grid_reduce_finalize<1>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
   }
 }
 

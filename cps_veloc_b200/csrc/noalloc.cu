@@ -126,6 +126,8 @@ void hop(const Dirac &D, int ep, int cb, int dag, int norm, const SpinorView &in
   dim3 block = hop_block(TuneKey{PREC_DOUBLE, recon, ep, D.kind, D.ls}, false);
   const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
   hp.nsg = (D.ls + block.y - 1) / block.y;
+  hp.rtile = 1;
+  hp.nrhs = 1;
   dim3 grid(nsb * hp.nsg, 1, 1);
   pick(recon, ep, dag)<<<grid, block, 0, lat.stream>>>(hp, v, st, partials);
   CPSGPU_CUDA(cudaGetLastError());

@@ -217,20 +217,19 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
 }
 
-// Reduce NV values over the whole grid slice belonging to one solve
-// (blocks with the same blockIdx.z) and finalize in its last block.
-// partials must hold NV * gridDim.x * gridDim.y doubles per solve.
+// Reduce NV values over the nblk blocks belonging to solve `solve` (this
+// block is number blk of them) and finalize in the last one to arrive.
+// partials must hold NV * nblk doubles per solve.
 // Must be called by every thread of the block (no early returns before it).
 template <int NV>
-__device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverScalars *st, int op) {
+__device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverScalars *st, int op, unsigned solve,
+                                     unsigned blk, unsigned nblk) {
   __shared__ double sm[32][NV];
   __shared__ bool last;
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthr = blockDim.x * blockDim.y;
   const int lane = tid & 31, warp = tid >> 5, nwarp = (nthr + 31) >> 5;
-  const unsigned nblk = gridDim.x * gridDim.y;
-  const unsigned blk = blockIdx.x + gridDim.x * blockIdx.y;
-  double *part = partials + (size_t)blockIdx.z * nblk * NV;
+  double *part = partials + (size_t)solve * nblk * NV;
   warp_sum(v);
   if (lane == 0)
 #pragma unroll
@@ -243,7 +242,7 @@ __device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverSc
       part[blk * NV + k] = s;
     }
     __threadfence();
-    unsigned t = atomicAdd(&st[blockIdx.z].ticket, 1u);
+    unsigned t = atomicAdd(&st[solve].ticket, 1u);
     last = (t == nblk - 1);
   }
   __syncthreads();
@@ -265,9 +264,16 @@ __device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverSc
     double tot[4] = {0, 0, 0, 0};
     for (int k = 0; k < NV; k++)
       for (int w = 0; w < nwarp; w++) tot[k] += sm[w][k];
-    finalize_scalars(&st[blockIdx.z], op, tot);
-    st[blockIdx.z].ticket = 0;
+    finalize_scalars(&st[solve], op, tot);
+    st[solve].ticket = 0;
   }
+}
+
+// The common case: one solve per blockIdx.z, all its blocks in x and y.
+template <int NV>
+__device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverScalars *st, int op) {
+  grid_reduce_finalize<NV>(v, partials, st, op, blockIdx.z, blockIdx.x + gridDim.x * blockIdx.y,
+                           gridDim.x * gridDim.y);
 }
 
 }  // namespace cpsgpu

@@ -195,6 +195,15 @@ class _DiracOp:
         check(lib().cpsgpu_autotune(self._h, prec, nrhs, C.byref(t)))
         return t.value
 
+    def rhs_tile(self, prec=A.DOUBLE, nrhs=1) -> int:
+        """right-hand sides per hop tile a batched launch of nrhs uses"""
+        t = C.c_int()
+        check(lib().cpsgpu_get_rhs_tile(self._h, prec, nrhs, C.byref(t)))
+        return t.value
+
+    def set_rhs_tile(self, prec: int, tile: int) -> None:
+        check(lib().cpsgpu_set_rhs_tile(self._h, prec, tile))
+
     def close(self):
         if getattr(self, "_h", None):
             lib().cpsgpu_dirac_destroy(self._h)

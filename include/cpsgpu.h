@@ -208,8 +208,15 @@ int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const
 
 /* ---- tuning ---- */
 /* Time candidate block shapes of every hop kernel the operator uses, at
- * precision prec, and keep the fastest.  Returns the number of tuned keys. */
+ * precision prec, and keep the fastest; with nrhs > 1 also the right-hand-
+ * side tile.  Returns the number of tuned keys. */
 int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned);
+/* Right-hand-side tile of batched hops at precision prec (no counterpart in
+ * the reference): consecutive thread blocks apply the same links to `tile`
+ * solves before moving on.  get returns the tile a launch of nrhs right-hand
+ * sides uses; set overrides the autotuner (0 restores the default). */
+int cpsgpu_get_rhs_tile(cpsgpu_dirac d, int prec, int nrhs, int *tile);
+int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile);
 
 /* ---- measurement ----
  * Time `reps` back-to-back launches of the operator's hop kernel
