@@ -47,11 +47,11 @@ MF = 0.01
 SEED = 20261203
 STOP = 1e-10
 # Iterations of the plain FP64 CG to a true residual of 1e-10 on this
-# workload, as measured by this library's FP64 CG (it runs the reference's
-# InvCgShift algorithm).  Only the reference arm uses it, to turn its
-# per-iteration CPU time into a time to solution without running the
-# multi-hour CPU solve.
-FP64_CG_ITERS = 1000
+# workload, as measured by this library's FP64 CG on a B200 (196; it runs the
+# reference's InvCgShift algorithm step for step).  Only the reference arm
+# uses it, to turn its per-iteration CPU time into a time to solution without
+# running the multi-hour CPU solve.
+FP64_CG_ITERS = 196
 
 
 def peaks() -> dict:
@@ -221,6 +221,110 @@ def cpu_port_sample(u, iters: int, reps: int = 1) -> dict:
             "s_per_iteration": 4 * t}
 
 
+def _dev_time(A, fn, D, prec, reps):
+    ms, by = C.c_double(), C.c_double()
+    A.check(fn(D._h, prec, reps, C.byref(ms), C.byref(by)))
+    return ms.value, by.value
+
+
+def extra_batched(A, D, sloppy) -> dict:
+    """12 point sources (the spin-colour unit vectors at one seeded site) on
+    the headline system: one batched mixed-precision solve against 12
+    sequential mixed solves and 12 sequential FP64 solves."""
+    D.autotune(sloppy, nrhs=12)
+    site = int(np.random.default_rng(SEED + 4).integers(0, D.f_size // 24))
+    srcs = []
+    for k in range(12):
+        e = np.zeros(D.f_size)
+        e[24 * site + 2 * k] = 1.0
+        srcs.append(e)
+    sols = [np.zeros(D.f_size) for _ in srcs]
+    D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=sloppy)  # warm-up (graph capture)
+    sols = [np.zeros(D.f_size) for _ in srcs]
+    res = D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=sloppy)
+    t_batch = res[0].seconds
+    seq_mixed, seq_fp64, it64 = 0.0, 0.0, []
+    for e in srcs:
+        y = np.zeros(D.f_size)
+        seq_mixed += D.InvCg(y, e, stop_rsd=STOP, precision=sloppy).seconds
+        y = np.zeros(D.f_size)
+        r = D.InvCg(y, e, stop_rsd=STOP)
+        seq_fp64 += r.seconds
+        it64.append(r.iterations)
+    ok = all(r.status == A.CONVERGED and r.true_res <= STOP for r in res)
+    return {"rhs": 12, "rhs_tile": D.rhs_tile(sloppy, 12), "all_converged_1e-10": ok,
+            "batched_mixed_s": t_batch, "per_rhs_batched_mixed_s": t_batch / 12,
+            "sequential_mixed_s": seq_mixed, "sequential_fp64_s": seq_fp64,
+            "iterations_mixed": [r.iterations for r in res], "iterations_fp64": it64,
+            "speedup_batched_mixed_vs_fp64_single_rhs": seq_fp64 / t_batch,
+            "speedup_batched_vs_sequential_mixed": seq_mixed / t_batch}
+
+
+def extra_mobius(A) -> dict:
+    """Mobius 24^3x64, Ls=12, b=1.5, c=0.5, M5=1.8, m_f=0.005, 12-real links:
+    FP64 CG against the FP16-storage inner solve with FP64 defect correction."""
+    from cps_veloc_b200.dirac import DiracOpMobius, Lattice, gen_gauge, gen_gaussian
+
+    L, ls = (24, 24, 24, 64), 12
+    lat = Lattice(L, (1, 1, 1, -1))
+    lat.import_gauge(gen_gauge(L, seed=SEED + 3, width=0.3))
+    D = DiracOpMobius(lat, mass=0.005, ls=ls, m5=M5, b=1.5, c=0.5)
+    for prec in (A.DOUBLE, A.HALF):
+        D.autotune(prec)
+    b = gen_gaussian(D.f_size, seed=SEED, stream=3)
+    x = np.zeros(D.f_size)
+    r64 = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000)
+    x = np.zeros(D.f_size)
+    rh = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
+    pk = peaks()["hbm_gbs"]
+    out = {"lattice": list(L), "ls": ls, "b": 1.5, "c": 0.5, "mf": 0.005,
+           "fp64_cg": {"time_s": r64.seconds, "iterations": r64.iterations, "true_res": r64.true_res},
+           "half_inner_cg": {"time_s": rh.seconds, "iterations": rh.iterations, "true_res": rh.true_res,
+                             "reliable_updates": rh.reliable_updates},
+           "iteration_inflation": rh.iterations / r64.iterations,
+           "speedup_vs_fp64_cg": r64.seconds / rh.seconds}
+    for name, prec in (("fp64", A.DOUBLE), ("half", A.HALF)):
+        ms, by = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
+        flops = 48 * ls * D.f_size // 24  # dense Ls x Ls, both chiralities
+        out[f"m5inv_{name}"] = {"ms": ms, "GB_s": by / ms / 1e6, "frac_of_measured_hbm": by / ms / 1e6 / pk,
+                                "flop_per_byte": flops / by, "unit": "CUDA cores (dense Ls x Ls from shared memory)"}
+        m2, b2 = C.c_double(), C.c_double()
+        A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, 20, C.byref(m2), C.byref(b2)))
+        out[f"hop_{name}"] = {"ms": m2.value, "GB_s": b2.value / m2.value / 1e6}
+    D.close()
+    lat.close()
+    return out
+
+
+def extra_multishift(A) -> dict:
+    """Wilson 32^3x64, kappa=0.125, 16 shifts log-spaced in [1e-4, 10]: FP64
+    multishift CG against FP32 multishift + FP64 refinement of every shift
+    (wall time of the host-vector call, transfers of 16 solutions included)."""
+    from cps_veloc_b200.dirac import DiracOpWilson, Lattice, gen_gauge, gen_gaussian
+
+    L = (32, 32, 32, 64)
+    lat = Lattice(L, (1, 1, 1, -1))
+    lat.import_gauge(gen_gauge(L, seed=SEED + 5, width=0.3))
+    D = DiracOpWilson(lat, mass=1 / (2 * 0.125) - 4)
+    for prec in (A.DOUBLE, A.SINGLE):
+        D.autotune(prec)
+    shifts = list(np.logspace(-4, 1, 16))
+    chi = gen_gaussian(D.f_size, seed=SEED, stream=5)
+    out = {"lattice": list(L), "kappa": 0.125, "shifts": len(shifts)}
+    for name, prec in (("fp64", A.DOUBLE), ("fp32_then_fp64_refine", A.SINGLE)):
+        psi = [np.zeros(D.f_size) for _ in shifts]
+        rs = np.full(len(shifts), STOP)
+        t0 = time.perf_counter()
+        k = D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, precision=prec)
+        t = time.perf_counter() - t0
+        y, _ = D.MatPcDagMatPc(psi[0])
+        worst = float(np.linalg.norm(chi - y - shifts[0] * psi[0]) / np.linalg.norm(chi))
+        out[name] = {"wall_s": t, "iterations": k, "true_res_smallest_shift": worst}
+    D.close()
+    lat.close()
+    return out
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -285,6 +389,8 @@ def main(argv=None) -> int:
     ap.add_argument("--sloppy", default="half", choices=["half", "single"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other systems (12 point sources, Mobius 24^3x64, multishift 32^3x64)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -365,6 +471,12 @@ def main(argv=None) -> int:
         except Exception as e:  # noqa: BLE001
             cpu = {"error": str(e)}
 
+    extras = None
+    if rank == 0 and not args.no_extras:
+        extras = {"batched_12_point_sources": extra_batched(A, D, sloppy),
+                  "mobius_24x64_ls12": extra_mobius(A),
+                  "multishift_wilson_32x64": extra_multishift(A)}
+
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
     if rank == 0:
         out = {
@@ -391,6 +503,7 @@ def main(argv=None) -> int:
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
             "clocks": clk.summary(),
+            "other_systems": extras,
             "gpu_launches": int(sum(r.kernels for r in res)),
         }
         print(json.dumps(out), flush=True)

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
             "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_mdagm": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),
+            "cpsgpu_time_m5inv": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
             "cpsgpu_host_free": (C.c_int, [vp]),
             "cpsgpu_gen_gauge": (C.c_int, [C.POINTER(C.c_int), C.c_ulonglong, C.c_double, _dp]),

@@ -18,6 +18,7 @@ void gen_gaussian(double *out, long n, uint64_t seed, unsigned stream);
 int autotune(Dirac &D, int prec, int nrhs);
 double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes);
 double time_mdagm(Dirac &D, int prec, int reps, double *bytes);
+double time_m5inv(Dirac &D, int prec, int reps, double *bytes);
 double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
 int minvcg(Dirac &D, double *const *psi, const double *chi, double chi_norm, const double *shift, int nshift,
            double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine);
@@ -512,6 +513,16 @@ int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned) {
     need_gauge(d);
     int n = autotune(*d->D, prec, nrhs);
     if (tuned) *tuned = n;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_time_m5inv(cpsgpu_dirac d, int prec, int reps, double *ms, double *bytes) {
+  return guarded([&] {
+    if (!d || reps < 1 || !ms) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    need_gauge(d);
+    *ms = time_m5inv(*d->D, prec, reps, bytes);
     return CPSGPU_OK;
   });
 }

@@ -185,20 +185,21 @@ __global__ void mix_kernel(SpinorView in, SpinorView out, const double *mix, int
   const bool active = i < in.vh;
   R a[24];
   if (active) SpinorIO<P>::load(in, rhs * ls + s, i, a);
-  R *mine = sm + ((size_t)s * blockDim.x + threadIdx.x) * 24;
+  // [ls][24][BX]: a warp's shared-memory accesses are consecutive words
+  R *mine = sm + (size_t)s * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-  for (int k = 0; k < 24; k++) mine[k] = active ? a[k] : R(0);
+  for (int k = 0; k < 24; k++) mine[k * blockDim.x] = active ? a[k] : R(0);
   __syncthreads();
   if (!active) return;
 #pragma unroll
   for (int k = 0; k < 24; k++) a[k] = R(0);
   for (int t = 0; t < ls; t++) {
     const R mu_ = R(mx[s * ls + t]), md_ = R(mx[ls * ls + s * ls + t]);
-    const R *src = sm + ((size_t)t * blockDim.x + threadIdx.x) * 24;
+    const R *src = sm + (size_t)t * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < 12; k++) a[k] += mu_ * src[k];
+    for (int k = 0; k < 12; k++) a[k] += mu_ * src[k * blockDim.x];
 #pragma unroll
-    for (int k = 12; k < 24; k++) a[k] += md_ * src[k];
+    for (int k = 12; k < 24; k++) a[k] += md_ * src[k * blockDim.x];
   }
   SpinorIO<P>::store(out, rhs * ls + s, i, a);
 }

@@ -229,14 +229,14 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
   if constexpr (ep_mix(EP)) {
     // all Ls slices of this block's sites: out(s) = sum_t Mix_chi[s][t] acc(t)
     extern __shared__ unsigned char smraw[];
-    R *sm = reinterpret_cast<R *>(smraw);  // [ls][BX][24]
+    R *sm = reinterpret_cast<R *>(smraw);  // [ls][24][BX]: a warp's accesses are consecutive words
     double *mx = reinterpret_cast<double *>(sm + (size_t)hp.ls * blockDim.x * 24);
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
     for (int k = tid; k < 2 * hp.ls * hp.ls; k += blockDim.x * blockDim.y) mx[k] = hp.mix[k];
     if (s < hp.ls) {
-      R *mine = sm + ((size_t)s * blockDim.x + threadIdx.x) * 24;
+      R *mine = sm + (size_t)s * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-      for (int k = 0; k < 24; k++) mine[k] = active ? acc[k] : R(0);
+      for (int k = 0; k < 24; k++) mine[k * blockDim.x] = active ? acc[k] : R(0);
     }
     __syncthreads();
     if (active) {
@@ -245,11 +245,11 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       for (int t2 = 0; t2 < hp.ls; t2++) {
         const R mu_ = R(mx[s * hp.ls + t2]);
         const R md_ = R(mx[hp.ls * hp.ls + s * hp.ls + t2]);
-        const R *src = sm + ((size_t)t2 * blockDim.x + threadIdx.x) * 24;
+        const R *src = sm + (size_t)t2 * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-        for (int k = 0; k < 12; k++) acc[k] += mu_ * src[k];
+        for (int k = 0; k < 12; k++) acc[k] += mu_ * src[k * blockDim.x];
 #pragma unroll
-        for (int k = 12; k < 24; k++) acc[k] += md_ * src[k];
+        for (int k = 12; k < 24; k++) acc[k] += md_ * src[k * blockDim.x];
       }
     }
   }

@@ -75,6 +75,35 @@ double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes)
   return ms / reps;
 }
 
+// The standalone Mobius M5^-1 (dense Ls x Ls per chirality, CUDA cores,
+// matrices in shared memory), timed like time_dslash.
+double time_m5inv(Dirac &D, int prec, int reps, double *bytes) {
+  if (D.kind != KIND_MOBIUS) throw Error(-2, "M5^-1 timing: Mobius operators only");
+  Lattice &L = *D.lat;
+  const size_t sites = (size_t)L.vh * D.ls;
+  const int rot = rotation(sites * 2 * spinor_bytes(prec));
+  std::vector<Field> in(rot), out(rot);
+  for (int k = 0; k < rot; k++) {
+    in[k].create(prec, L.vh, D.ls, 1);
+    out[k].create(prec, L.vh, D.ls, 1);
+    fill(L, in[k]);
+  }
+  for (int k = 0; k < 3; k++) op_mobius_m5inv(D, prec, out[k % rot].view(), in[k % rot].view(), 0);
+  cudaEvent_t e0, e1;
+  CPSGPU_CUDA(cudaEventCreate(&e0));
+  CPSGPU_CUDA(cudaEventCreate(&e1));
+  CPSGPU_CUDA(cudaEventRecord(e0, L.stream));
+  for (int k = 0; k < reps; k++) op_mobius_m5inv(D, prec, out[k % rot].view(), in[k % rot].view(), 0);
+  CPSGPU_CUDA(cudaEventRecord(e1, L.stream));
+  CPSGPU_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (bytes) *bytes = (double)sites * 2 * spinor_bytes(prec);
+  return ms / reps;
+}
+
 double time_mdagm(Dirac &D, int prec, int reps, double *bytes) {
   Lattice &L = *D.lat;
   const size_t sites = (size_t)L.vh * D.ls;

@@ -231,6 +231,10 @@ int cpsgpu_time_dslash(cpsgpu_dirac d, int prec, int cb, int dag, int reps, doub
 /* Same for one MatPcDagMatPc application (all its kernels); bytes counts
  * every kernel's compulsory traffic. */
 int cpsgpu_time_mdagm(cpsgpu_dirac d, int prec, int reps, double *ms_per_apply, double *bytes_per_apply);
+/* Same for the Mobius M5^-1 alone (zmobius_m5inv, zmobius_m5inv.C:534):
+ * the dense Ls x Ls contraction per chirality on the CUDA cores; bytes =
+ * input and output spinors once. */
+int cpsgpu_time_m5inv(cpsgpu_dirac d, int prec, int reps, double *ms_per_apply, double *bytes_per_apply);
 
 /* ---- pinned host memory for fast host<->device copies ---- */
 int cpsgpu_host_alloc(size_t bytes, void **ptr);
