@@ -131,7 +131,7 @@ __global__ void norm_kernel(SpinorView f, SolverScalars *st, double *partials, i
 #pragma unroll
     for (int k = 0; k < 24; k++) v[0] += double(a[k]) * double(a[k]);
   }
-  grid_reduce_finalize<1>(v, partials, st, op);
+  block_partial<1>(v, partials);
 }
 
 __global__ void init_scalars_kernel(SolverScalars *st, int nrhs, SolverScalars init) {
@@ -336,6 +336,16 @@ void launch_norm(cudaStream_t s, int prec, const SpinorView &f, SolverScalars *s
   if (prec == PREC_DOUBLE) norm_kernel<PREC_DOUBLE><<<grid, TPB, 0, s>>>(f, st, partials, op, gate);
   else if (prec == PREC_SINGLE) norm_kernel<PREC_SINGLE><<<grid, TPB, 0, s>>>(f, st, partials, op, gate);
   else norm_kernel<PREC_HALF><<<grid, TPB, 0, s>>>(f, st, partials, op, gate);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+  launch_finalize(s, 1, partials, st, op, grid.x * grid.y, f.nrhs, gate);
+}
+
+void launch_finalize(cudaStream_t s, int nv, const double *partials, SolverScalars *st, int op, unsigned nblk,
+                     int nsolves, int gate) {
+  if (nv == 1) finalize_kernel<1><<<nsolves, FINALIZE_THREADS, 0, s>>>(partials, st, op, nblk, gate);
+  else if (nv == 2) finalize_kernel<2><<<nsolves, FINALIZE_THREADS, 0, s>>>(partials, st, op, nblk, gate);
+  else throw Error(-2, "finalize: 1 or 2 values per reduction");
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;
 }

@@ -156,6 +156,10 @@ void launch_accum_reliable(cudaStream_t s, const SpinorView &x64, int pxs, const
                            int force);
 // |f|^2 (+ finalize op)
 void launch_norm(cudaStream_t s, int prec, const SpinorView &f, SolverScalars *st, double *partials, int op, int gate);
+// sum the per-block partials (nv values each, nblk blocks per solve) of the
+// preceding reducing kernel and update each solve's scalars with op
+void launch_finalize(cudaStream_t s, int nv, const double *partials, SolverScalars *st, int op, unsigned nblk,
+                     int nsolves, int gate);
 // st[k] <- value (host-side init through a kernel so graphs can replay it)
 void launch_init_scalars(cudaStream_t s, SolverScalars *st, int nrhs, const SolverScalars &init);
 

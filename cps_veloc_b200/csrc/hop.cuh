@@ -21,6 +21,8 @@
 //     dense Ls x Ls matrix per chirality applied in the MIX epilogue from
 //     shared memory (a block then holds all Ls slices of its sites).
 #pragma once
+#include <type_traits>
+
 #include "fields.cuh"
 #include "reduce.cuh"
 
@@ -257,8 +259,12 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
   if constexpr (EP == EP_STORE || EP == EP_MIX) {
     if (active) SpinorIO<P>::store(v.out, sl, i, acc);
   } else if constexpr (ep_axpy(EP)) {
-    // out = x + c hop, streamed 4 reals at a time (few live registers)
-    double red[2] = {0.0, 0.0};
+    // out = x + c hop, streamed 4 reals at a time (few live registers).
+    // A thread sums its own 24 squares in the arithmetic precision (FP32 for
+    // the sloppy operators: no FP64 conversions per value); everything from
+    // the per-thread partial sums on is FP64.
+    using RA = typename std::conditional<P == PREC_DOUBLE, double, float>::type;
+    RA n_out = RA(0), n_x = RA(0);
     if (active) {
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
 #pragma unroll
@@ -267,20 +273,21 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
         Chunk4<P>::load(v.x, sl, i, c, xv);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          if (hp.norm) red[1] += double(xv[k]) * double(xv[k]);
+          if (hp.norm) n_x += xv[k] * xv[k];
           acc[4 * c + k] = xv[k] + cf * acc[4 * c + k];
-          if (hp.norm) red[0] += double(acc[4 * c + k]) * double(acc[4 * c + k]);
+          if (hp.norm) n_out += acc[4 * c + k] * acc[4 * c + k];
         }
         if constexpr (P != PREC_HALF) Chunk4<P>::store(v.out, sl, i, c, acc + 4 * c);
       }
       if constexpr (P == PREC_HALF) SpinorIO<P>::store(v.out, sl, i, acc);
     }
-    if (hp.norm) grid_reduce_finalize<2>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
+    double red[2] = {double(n_out), double(n_x)};
+    if (hp.norm) block_partial<2>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
   } else if constexpr (ep_cg(EP)) {
     // q = x + c hop + shift p;  r -= alpha q;  sol += alpha p;  |r|^2
     using RR = typename PrecTraits<PR>::real;
     using RX = typename PrecTraits<PX>::real;
-    double red[1] = {0.0};
+    RR n_r = RR(0);  // this thread's |r|^2 in r's arithmetic precision
     if (active) {
       const double alpha = st[rhs].alpha;
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
@@ -300,7 +307,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
         for (int k = 0; k < 4; k++) {
           R q = xv[k] + cf * acc[4 * c + k] + sh * R(pv[k]);
           rv[k] = rv[k] - a * RR(q);
-          red[0] += double(rv[k]) * double(rv[k]);
+          n_r += rv[k] * rv[k];
         }
         if constexpr (PR == PREC_HALF) {
 #pragma unroll
@@ -318,7 +325,8 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       }
       if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
-    grid_reduce_finalize<1>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
+    double red[1] = {double(n_r)};
+    block_partial<1>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
   } else if constexpr (ep_res(EP)) {
     // r = b - (x + c hop + shift sol), stored in r's precision;  |r|^2
     using RR = typename PrecTraits<PR>::real;
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
       }
       if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
     }
-    grid_reduce_finalize<1>(red, partials, st, hp.red_op, (unsigned)rhs, (unsigned)sb, nblk);
+    block_partial<1>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
   }
 }
 

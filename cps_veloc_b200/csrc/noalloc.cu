@@ -131,6 +131,10 @@ void hop(const Dirac &D, int ep, int cb, int dag, int norm, const SpinorView &in
   dim3 grid(nsb * hp.nsg, 1, 1);
   pick(recon, ep, dag)<<<grid, block, 0, lat.stream>>>(hp, v, st, partials);
   CPSGPU_CUDA(cudaGetLastError());
+  if (norm) {  // sum the per-block partials of |out|^2, |x|^2 into st->sum
+    finalize_kernel<2><<<1, FINALIZE_THREADS, 0, lat.stream>>>(partials, st, RED_STORE, grid.x, GATE_NONE);
+    CPSGPU_CUDA(cudaGetLastError());
+  }
 }
 
 SpinorView view_of(void *p, const Dirac &D) {
@@ -162,8 +166,7 @@ double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in) {
   void *t1 = base + c.scalars + c.partials;
   void *t2 = base + c.scalars + c.partials + c.field;
   cudaStream_t s = D.lat->stream;
-  // the array keeps the previous call's contents: the reduction ticket and
-  // sums must start at zero
+  // the array keeps the previous call's contents: start from zeroed scalars
   CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), s));
   const SpinorView vin = view_of(const_cast<double *>(in), D), vout = view_of(out, D);
   const SpinorView v1 = view_of(t1, D), v2 = view_of(t2, D);

@@ -2,11 +2,10 @@
 // scalars.
 //
 // Every reducing kernel sums its per-thread values in a fixed order (warp
-// shuffle, then warps in index order), writes one partial per block, and
-// the last block to finish (found with an atomic ticket, no spin-waiting)
-// adds the partials in block order and updates the solver scalars.  Results
-// are therefore bit-reproducible run to run, and the host never has to read
-// a scalar to keep the Krylov loop going.
+// shuffle, then warps in index order) and writes one partial per block; a
+// small finalize kernel then adds one solve's partials in block order and
+// updates its scalars.  Results are therefore bit-reproducible run to run,
+// and the host never has to read a scalar to keep the Krylov loop going.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -40,11 +39,10 @@ struct SolverScalars {
   int n_reliable;   // reliable updates performed
   int pad[1];
   void *ext;        // solver-specific extension (multishift scalars)
-  unsigned int ticket;
-  unsigned int pad2[3];
+  unsigned int pad2[4];
 };
 
-// What the last block does with the reduced sums.
+// What the finalize step does with the reduced sums.
 enum ReduceOp {
   RED_STORE = 0,      // sum[] only
   RED_PAP = 1,        // sum[0] = |M p|^2, sum[1] = |p|^2: d, alpha
@@ -217,45 +215,64 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
 }
 
-// Reduce NV values over the nblk blocks belonging to solve `solve` (this
-// block is number blk of them) and finalize in the last one to arrive.
-// partials must hold NV * nblk doubles per solve.
-// Must be called by every thread of the block (no early returns before it).
+// Global reductions are two-step and deterministic: every block of the
+// reducing kernel writes its own NV partial sums (block_partial), and a
+// following finalize_kernel sums one solve's partials in a fixed order and
+// updates its scalars (finalize_scalars).  No block waits on another, no
+// atomics: the order of the additions never depends on scheduling.
+
+// Sum NV values over the block; thread 0 writes them as partial number blk of
+// solve `solve` (partials hold NV * nblk doubles per solve).  Must be called
+// by every thread of the block.
 template <int NV>
-__device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverScalars *st, int op, unsigned solve,
-                                     unsigned blk, unsigned nblk) {
+__device__ void block_partial(double (&v)[NV], double *partials, unsigned solve, unsigned blk, unsigned nblk) {
   __shared__ double sm[32][NV];
-  __shared__ bool last;
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthr = blockDim.x * blockDim.y;
   const int lane = tid & 31, warp = tid >> 5, nwarp = (nthr + 31) >> 5;
-  double *part = partials + (size_t)solve * nblk * NV;
   warp_sum(v);
   if (lane == 0)
 #pragma unroll
     for (int k = 0; k < NV; k++) sm[warp][k] = v[k];
   __syncthreads();
   if (tid == 0) {
+    double *part = partials + ((size_t)solve * nblk + blk) * NV;
     for (int k = 0; k < NV; k++) {
       double s = 0.0;
       for (int w = 0; w < nwarp; w++) s += sm[w][k];
-      part[blk * NV + k] = s;
+      part[k] = s;
     }
-    __threadfence();
-    unsigned t = atomicAdd(&st[solve].ticket, 1u);
-    last = (t == nblk - 1);
   }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+}
+
+// The common case: one solve per blockIdx.z, all its blocks in x and y.
+template <int NV>
+__device__ void block_partial(double (&v)[NV], double *partials) {
+  block_partial<NV>(v, partials, blockIdx.z, blockIdx.x + gridDim.x * blockIdx.y, gridDim.x * gridDim.y);
+}
+
+constexpr int FINALIZE_THREADS = 256;
+
+// One block per solve: sum its nblk partials (thread-strided, then the warp
+// and block trees, always in the same order) and finalize its scalars.  The
+// gate is the one the reducing kernel had, so a solve it skipped is skipped
+// here too.
+template <int NV>
+__global__ void __launch_bounds__(FINALIZE_THREADS)
+    finalize_kernel(const double *partials, SolverScalars *st, int op, unsigned nblk, int gate) {
+  const unsigned solve = blockIdx.x;
+  if (gate == 1 && st[solve].done) return;                              // GATE_RUNNING
+  if (gate == 2 && (st[solve].done || !st[solve].reliable)) return;     // GATE_RELIABLE
+  __shared__ double sm[FINALIZE_THREADS / 32][NV];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double *part = partials + (size_t)solve * nblk * NV;
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) acc[k] = 0.0;
-  for (unsigned b = tid; b < nblk; b += nthr)
+  for (unsigned b = tid; b < nblk; b += FINALIZE_THREADS)
 #pragma unroll
-    for (int k = 0; k < NV; k++) acc[k] += __ldcg(part + b * NV + k);
+    for (int k = 0; k < NV; k++) acc[k] += part[(size_t)b * NV + k];
   warp_sum(acc);
-  __syncthreads();
   if (lane == 0)
 #pragma unroll
     for (int k = 0; k < NV; k++) sm[warp][k] = acc[k];
@@ -263,17 +280,9 @@ __device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverSc
   if (tid == 0) {
     double tot[4] = {0, 0, 0, 0};
     for (int k = 0; k < NV; k++)
-      for (int w = 0; w < nwarp; w++) tot[k] += sm[w][k];
+      for (int w = 0; w < FINALIZE_THREADS / 32; w++) tot[k] += sm[w][k];
     finalize_scalars(&st[solve], op, tot);
-    st[solve].ticket = 0;
   }
-}
-
-// The common case: one solve per blockIdx.z, all its blocks in x and y.
-template <int NV>
-__device__ void grid_reduce_finalize(double (&v)[NV], double *partials, SolverScalars *st, int op) {
-  grid_reduce_finalize<NV>(v, partials, st, op, blockIdx.z, blockIdx.x + gridDim.x * blockIdx.y,
-                           gridDim.x * gridDim.y);
 }
 
 }  // namespace cpsgpu
