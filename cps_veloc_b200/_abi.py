@@ -13,6 +13,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "libcpsgpu.so"
 
 DOUBLE, SINGLE, HALF = 0, 1, 2
+LINKS_F32_12, LINKS_F32_18 = 112, 118  # link forms of the FP16 operator that read FP32 links
 WILSON, DWF, MOBIUS = 0, 1, 2
 MS_SINGLE, MS_MULTI, MS_GENERAL = 0, 1, 2
 CONVERGED, MAX_ITER, BREAKDOWN, NONFINITE = 1, 2, 3, 4

@@ -201,7 +201,9 @@ int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals) {
   return guarded([&] {
     if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
     if (prec != CPSGPU_SINGLE && prec != CPSGPU_HALF) throw Error(CPSGPU_ERR_ARG, "FP32 or FP16 only");
-    if (reals != 12 && reals != 18) throw Error(CPSGPU_ERR_ARG, "reals must be 12 or 18");
+    const bool f32 = (reals == CPSGPU_LINKS_F32_12 || reals == CPSGPU_LINKS_F32_18);
+    if (reals != 12 && reals != 18 && !(f32 && prec == CPSGPU_HALF))
+      throw Error(CPSGPU_ERR_ARG, "reals must be 12 or 18 (or FP32 links for the FP16 operator)");
     lat->L->sloppy_recon[prec] = reals;
     return CPSGPU_OK;
   });

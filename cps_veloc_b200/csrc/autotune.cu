@@ -44,6 +44,7 @@ int autotune(Dirac &D, int prec, int nrhs) {
   // and FP16 also the stored link form (12 reals rebuilt, or all 18)
   std::vector<int> recons;
   if (prec == PREC_DOUBLE) recons.push_back(L.recon(prec));
+  else if (prec == PREC_HALF) recons = {12, 18, LINK_F32_12, LINK_F32_18};
   else recons = {12, 18};
   float best_recon_t = 1e30f;
   int best_recon = recons[0];

@@ -92,7 +92,8 @@ struct Lattice {
   ~Lattice();
   GaugeView gauge(int prec) const;
   // reals per stored link a precision reads: FP64 uses 12 when the links are
-  // SU(3); FP32 / FP16 use sloppy_recon[prec] (12 or 18, set by the autotuner)
+  // SU(3); FP32 / FP16 use sloppy_recon[prec] (12 or 18, set by the autotuner;
+  // the FP16 operator may also read FP32 links, LINK_F32_12 / LINK_F32_18)
   int sloppy_recon[3] = {12, 18, 18};
   int recon(int prec) const {
     if (prec == PREC_DOUBLE) return use_recon12 ? 12 : 18;

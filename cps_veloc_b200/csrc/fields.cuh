@@ -425,5 +425,11 @@ template <> struct LinkIO<PREC_HALF, 18> {
     u.m[2][2] = {a.x, a.y};
   }
 };
+// FP16 spinors with FP32 links (LINK_F32_12 / LINK_F32_18): the links cost
+// no conversions; their extra bytes are shared by every slice of a site.
+constexpr int LINK_F32_12 = 112;
+constexpr int LINK_F32_18 = 118;
+template <> struct LinkIO<PREC_HALF, LINK_F32_12> : LinkIO<PREC_SINGLE, 12> {};
+template <> struct LinkIO<PREC_HALF, LINK_F32_18> : LinkIO<PREC_SINGLE, 18> {};
 
 }  // namespace cpsgpu

@@ -54,6 +54,8 @@ HopFn pick_ep(int ep, int pr, int px) {
 HopFn pick(int prec, int recon, int ep, int pr, int px) {
   if (prec == PREC_DOUBLE) return recon == 18 ? pick_ep<PREC_DOUBLE, 18>(ep, pr, px) : pick_ep<PREC_DOUBLE, 12>(ep, pr, px);
   if (prec == PREC_SINGLE) return recon == 18 ? pick_ep<PREC_SINGLE, 18>(ep, pr, px) : pick_ep<PREC_SINGLE, 12>(ep, pr, px);
+  if (recon == LINK_F32_18) return pick_ep<PREC_HALF, LINK_F32_18>(ep, pr, px);
+  if (recon == LINK_F32_12) return pick_ep<PREC_HALF, LINK_F32_12>(ep, pr, px);
   return recon == 18 ? pick_ep<PREC_HALF, 18>(ep, pr, px) : pick_ep<PREC_HALF, 12>(ep, pr, px);
 }
 

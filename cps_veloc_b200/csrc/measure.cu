@@ -13,7 +13,8 @@ namespace {
 size_t spinor_bytes(int prec) { return prec == PREC_DOUBLE ? 192 : prec == PREC_SINGLE ? 96 : 52; }
 size_t link_bytes(int prec, int recon) {
   if (prec == PREC_DOUBLE) return recon == 18 ? 144 : 96;
-  if (prec == PREC_SINGLE) return recon == 18 ? 72 : 48;
+  if (prec == PREC_SINGLE || recon == LINK_F32_18 || recon == LINK_F32_12)
+    return (recon == 18 || recon == LINK_F32_18) ? 72 : 48;
   return recon == 18 ? 36 : 24;
 }
 

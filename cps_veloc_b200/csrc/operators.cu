@@ -50,8 +50,8 @@ GaugeView Lattice::gauge(int prec) const {
   g.vh = vh;
   if (prec == PREC_DOUBLE)
     g.data = use_recon12 ? gD12.ptr : gD18.ptr;
-  else if (prec == PREC_SINGLE)
-    g.data = recon(prec) == 18 ? gS18.ptr : gS12.ptr;
+  else if (prec == PREC_SINGLE || recon(prec) == LINK_F32_18 || recon(prec) == LINK_F32_12)
+    g.data = (recon(prec) == 18 || recon(prec) == LINK_F32_18) ? gS18.ptr : gS12.ptr;
   else
     g.data = recon(prec) == 18 ? gH18.ptr : gH12.ptr;
   return g;

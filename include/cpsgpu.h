@@ -93,7 +93,11 @@ int cpsgpu_import_gauge(cpsgpu_lattice lat, const double *u_wilson, int signs_ap
 int cpsgpu_gauge_info(cpsgpu_lattice lat, double *recon_err, int *fp64_recon12);
 int cpsgpu_synchronize(cpsgpu_lattice lat);
 /* Stored link form of the FP32 or FP16 operator: 12 reals (third row rebuilt
- * in registers) or 18.  cpsgpu_autotune picks the faster; this overrides it. */
+ * in registers) or 18, in the operator's precision; the FP16 operator may
+ * also read FP32 links (CPSGPU_LINKS_F32_12 / _18: no conversions in the
+ * kernel).  cpsgpu_autotune picks the fastest; this overrides it. */
+#define CPSGPU_LINKS_F32_12 112
+#define CPSGPU_LINKS_F32_18 118
 int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals);
 
 /* ---- Dirac operators ---- */

@@ -16,13 +16,18 @@ TOL = {A.DOUBLE: 1e-13, A.SINGLE: 2e-6, A.HALF: 5e-3}
 PRECS = [A.DOUBLE, A.SINGLE, A.HALF]
 
 
-@pytest.fixture(params=[18, 12], ids=["links18", "links12"])
+@pytest.fixture(params=[18, 12, "f32"], ids=["links18", "links12", "f32links"])
 def link_reals(request):
-    """FP32 / FP16 operators read full links or rebuild the third row."""
+    """FP32 / FP16 operators read full links or rebuild the third row; the
+    FP16 operator may read FP32 links (12 reals here, 18 for FP32)."""
     return request.param
 
 
 def _set_links(lat, reals):
+    if reals == "f32":
+        A.check(A.lib().cpsgpu_set_link_reals(lat._h, A.SINGLE, 18))
+        A.check(A.lib().cpsgpu_set_link_reals(lat._h, A.HALF, A.LINKS_F32_12))
+        return
     for prec in (A.SINGLE, A.HALF):
         A.check(A.lib().cpsgpu_set_link_reals(lat._h, prec, reals))
 
