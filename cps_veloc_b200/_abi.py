@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
             "cpsgpu_mobius_m5inv": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_invcg_multi": (C.c_int, [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(CgArg),
                                              C.POINTER(CgResult)]),
             "cpsgpu_minvcg": (C.c_int, [vp, C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,

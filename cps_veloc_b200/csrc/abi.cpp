@@ -385,6 +385,70 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
   return cpsgpu_invcg_multi(d, &sol, &src, 1, arg, res);
 }
 
+// DiracOp*::MatInv with the CG inverter, both checkerboards on the device.
+//   Wilson / DWF (d_op_wilson.C:257-334, d_op_dwf.C:316-492), halves [odd | even]:
+//     temp = kappa Dslash(in_e, CHKB_EVEN) + in_o;  b = MatPcDag temp;  CG;
+//     out_e = kappa Dslash(out_o, CHKB_ODD) + in_e
+//   Mobius SYM2 (d_op_mobius.C:407-700), halves [even | odd]:
+//     temp = kappa_b Dslash_4(M5^-1 in_e, CHKB_EVEN) + in_o;  guess out_o <- M5 out_o;
+//     b = MatPcDag temp;  CG;  out_o <- M5^-1 out_o;
+//     out_e = M5^-1 (kappa_b Dslash_4(out_o, CHKB_ODD) + in_e);  out *= 2 kappa_b
+int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res) {
+  return guarded([&] {
+    if (!d || !out || !in || !arg || !res) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (arg->max_num_iter < 1) throw Error(CPSGPU_ERR_ARG, "max_num_iter must be >= 1");
+    check_prec(arg->precision);
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    const cudaStream_t s = L.stream;
+    const size_t half = vec_reals(d);
+    const bool mob = (D.kind == KIND_MOBIUS);
+    // the CG's checkerboard and the other one, as the reference orders them
+    const double *in_cg = mob ? in + half : in, *in_other = mob ? in : in + half;
+    double *out_cg = mob ? out + half : out, *out_other = mob ? out : out + half;
+    Field fo(PREC_DOUBLE, L.vh, D.ls, 1), t1(PREC_DOUBLE, L.vh, D.ls, 1), t2(PREC_DOUBLE, L.vh, D.ls, 1);
+    OpWork &w = d->w[PREC_DOUBLE];
+    CgSolver &S = solver_for(d, arg->precision, 1);
+    upload(L, fo, &in_other, 1);  // in_e
+    upload(L, t2, &in_cg, 1);     // in_o
+    if (!mob) {
+      op_dslash(D, PREC_DOUBLE, t1.view(), fo.view(), 0, 0);
+      launch_axpby(s, t1.view(), D.kappa, t1.view(), t2.view());
+    } else {
+      op_mobius_m5inv(D, PREC_DOUBLE, t1.view(), fo.view(), 0);
+      Field t3(PREC_DOUBLE, L.vh, D.ls, 1);
+      op_mobius_dslash4(D, PREC_DOUBLE, t3.view(), t1.view(), 0, 0, w);
+      launch_axpby(s, t1.view(), D.kappa, t3.view(), t2.view());
+    }
+    op_matpc(D, PREC_DOUBLE, S.b64.view(), t1.view(), 1, w, nullptr, 0, 0);
+    upload(L, S.x64, &out_cg, 1);
+    if (mob) {  // SYM2 guess: x <- M5 x
+      launch_mix(D, PREC_DOUBLE, D.mixM5.as<double>(), S.x64.view(), t1.view());
+      CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, t1.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    std::vector<CgResult> r;
+    S.run(to_args(arg), r);
+    if (!mob) {
+      op_dslash(D, PREC_DOUBLE, t1.view(), S.x64.view(), 1, 0);
+      launch_axpby(s, t2.view(), D.kappa, t1.view(), fo.view());
+      download(L, S.x64, &out_cg, 1);
+      download(L, t2, &out_other, 1);
+    } else {
+      op_mobius_m5inv(D, PREC_DOUBLE, t1.view(), S.x64.view(), 0);  // out_o
+      op_mobius_dslash4(D, PREC_DOUBLE, t2.view(), t1.view(), 1, 0, w);
+      launch_axpby(s, t2.view(), D.kappa, t2.view(), fo.view());
+      op_mobius_m5inv(D, PREC_DOUBLE, fo.view(), t2.view(), 0);     // out_e
+      launch_scale(s, 2.0 * D.kappa, t1.view());
+      launch_scale(s, 2.0 * D.kappa, fo.view());
+      download(L, t1, &out_cg, 1);
+      download(L, fo, &out_other, 1);
+    }
+    to_result(r[0], res);
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_minvcg(cpsgpu_dirac d, double *const *psi, const double *chi, double chi_norm, const double *shift,
                   int nshift, double *rsdcg, int type, const double *alpha, int max_num_iter, int precision,
                   int refine, int *iterations) {

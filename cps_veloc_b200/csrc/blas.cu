@@ -94,6 +94,30 @@ __global__ void xpay_kernel(SpinorView p, SpinorView r, const SolverScalars *st,
   SpinorIO<P>::store(p, sl, i, b);
 }
 
+// out = a x + y (fTimesV1PlusV2), FP64
+__global__ void axpby_kernel(SpinorView out, double a, SpinorView x, SpinorView y, size_t n) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  long sl = (long)(idx / x.vh), i = (long)(idx % x.vh);
+  double xv[24], yv[24];
+  SpinorIO<PREC_DOUBLE>::load(x, sl, i, xv);
+  SpinorIO<PREC_DOUBLE>::load(y, sl, i, yv);
+#pragma unroll
+  for (int k = 0; k < 24; k++) yv[k] = fma(a, xv[k], yv[k]);
+  SpinorIO<PREC_DOUBLE>::store(out, sl, i, yv);
+}
+
+__global__ void scale_kernel(double a, SpinorView f, size_t n) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  long sl = (long)(idx / f.vh), i = (long)(idx % f.vh);
+  double v[24];
+  SpinorIO<PREC_DOUBLE>::load(f, sl, i, v);
+#pragma unroll
+  for (int k = 0; k < 24; k++) v[k] *= a;
+  SpinorIO<PREC_DOUBLE>::store(f, sl, i, v);
+}
+
 // x64 += xs; xs = 0  (reliable update: solution accumulated in FP64)
 template <int PXS>
 __global__ void accum_kernel(SpinorView x, SpinorView xs, const SolverScalars *st, int force) {
@@ -294,6 +318,20 @@ void launch_convert(cudaStream_t s, int pdst, const SpinorView &dst, int psrc, c
   if (pdst == PREC_DOUBLE) convert_dispatch<PREC_DOUBLE>(s, dst, psrc, src, n);
   else if (pdst == PREC_SINGLE) convert_dispatch<PREC_SINGLE>(s, dst, psrc, src, n);
   else convert_dispatch<PREC_HALF>(s, dst, psrc, src, n);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+}
+
+void launch_axpby(cudaStream_t s, const SpinorView &out, double a, const SpinorView &x, const SpinorView &y) {
+  size_t n = (size_t)x.vh * x.ls * x.nrhs;
+  axpby_kernel<<<blocks_for(n), TPB, 0, s>>>(out, a, x, y, n);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+}
+
+void launch_scale(cudaStream_t s, double a, const SpinorView &f) {
+  size_t n = (size_t)f.vh * f.ls * f.nrhs;
+  scale_kernel<<<blocks_for(n), TPB, 0, s>>>(a, f, n);
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;
 }

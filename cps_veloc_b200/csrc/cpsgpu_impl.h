@@ -111,7 +111,7 @@ struct Dirac {
   // Mobius s-mixing matrices, each [2][ls][ls] (upper, lower chirality):
   //   P = B M5inv, Q = B M5inv kappa_b, R = kappa_b M5inv^+ B^+ (-kappa_b),
   //   S = M5inv^+ B^+, and the pieces B, B^+, M5inv, M5inv^+ on their own.
-  DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id;
+  DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id, mixM5;
   std::vector<double> hM5i, hM5id, hB, hBd;
   Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_);
   // right-hand sides per hop tile (consecutive blocks share links across
@@ -148,6 +148,9 @@ void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &i
                 const SolverScalars *st = nullptr, int gate = 0);
 
 // vector kernels
+// out = a x + y and f *= a, FP64 fields
+void launch_axpby(cudaStream_t s, const SpinorView &out, double a, const SpinorView &x, const SpinorView &y);
+void launch_scale(cudaStream_t s, double a, const SpinorView &f);
 void launch_convert(cudaStream_t s, int pdst, const SpinorView &dst, int psrc, const SpinorView &src);
 void launch_zero(cudaStream_t s, const Field &f);
 // p = r + beta p (gated on st->done)

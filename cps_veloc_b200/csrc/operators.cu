@@ -223,6 +223,11 @@ Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_
   upload(mixBd, hBd);
   upload(mixM5i, hM5i);
   upload(mixM5id, hM5id);
+  // M5 = 1 + K D5, what MatInv applies to the initial guess (the b/c mixing
+  // form with b = 1, c = K)
+  std::vector<cd> m5u, m5d;
+  bmix(ls, std::vector<cd>(ls, 1.0), K, mass, m5u, m5d);
+  upload(mixM5, pack(ls, m5u, m5d));
 }
 
 // ---------------------------------------------------------------- operators

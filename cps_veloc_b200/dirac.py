@@ -162,6 +162,22 @@ class _DiracOp:
         check(lib().cpsgpu_invcg(self._h, dptr(sol), dptr(src), C.byref(a), C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
 
+    def MatInv(self, out, src, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.1, chunk=8,
+               use_graph=True) -> CgResult:
+        """DiracOp*::MatInv(out, in, true_res) with CG: both checkerboards
+        (2 * f_size reals; Wilson/DWF [odd | even], Mobius [even | odd]).
+        out's CG checkerboard is the initial guess; out is updated in place."""
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        if src.size != 2 * self.f_size:
+            raise ValueError(f"vectors must hold {2 * self.f_size} reals (both checkerboards)")
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                and out.size == src.size):
+            raise TypeError("out must be a C-contiguous float64 array like src (updated in place)")
+        a = self._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, precision, delta, chunk, use_graph)
+        r = A.CgResult()
+        check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
+        return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
+
     def InvCgMulti(self, sols, srcs, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.1,
                    chunk=8, use_graph=True):
         n = len(srcs)

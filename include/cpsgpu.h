@@ -186,6 +186,13 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
  * InvCg over the same set. res has nrhs entries. */
 int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
                        const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* DiracOp*::MatInv(out, in, true_res) with the CG inverter
+ * (d_op_wilson.C:257-334, d_op_dwf.C:316-492, d_op_mobius.C:407-700, SYM2):
+ * the solve on both checkerboards.  in and out hold 2 * 24*Ls*Vh reals in
+ * the reference's order: Wilson and DWF [odd | even], Mobius [even | odd];
+ * out's CG checkerboard (odd) is the initial guess.  The source is not
+ * modified (PRESERVE_YES).  res describes the CG on the odd checkerboard. */
+int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
 /* DiracOp::MInvCG (minvcg.C:47-353): multishift CG on MatPcDagMatPc +
  * shift[k].  rsdcg[k] in: stop residuals, out: achieved residuals; returns
  * the iteration count through *iterations as the reference returns it.

@@ -97,6 +97,7 @@ def load_oracle() -> C.CDLL:
             "orc_mobius_m5inv": [g, m, _dp, d, i],
             "orc_mobius_m": [g, m, _dp, _dp, _dp, d, i],
             "orc_mobius_mdagm": [g, m, _dp, _dp, _dp, d, _dp],
+            "orc_mobius_m5": [g, m, _dp, d],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a
@@ -105,6 +106,11 @@ def load_oracle() -> C.CDLL:
         L.orc_mobius_params.restype = None
         L.orc_invcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, d, d, i, _dp, _dp]
         L.orc_invcg.restype = i
+        L.orc_wilson_matinv.argtypes = [g, _dp, _dp, _dp, d, d, i, _dp]
+        L.orc_dwf_matinv.argtypes = [g, _dp, _dp, _dp, d, d, d, i, _dp]
+        L.orc_mobius_matinv.argtypes = [g, m, _dp, _dp, _dp, d, d, i, _dp]
+        for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
+            getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]
         L.orc_minvcg.restype = i
         _oracle = L
@@ -133,6 +139,7 @@ def load_reference() -> C.CDLL:
             "ref_dwf_mdagm": [_dp, _dp, _dp, _dp, d],
             "ref_zmobius_dslash_4": [_dp, _dp, _dp, i, i, d],
             "ref_zmobius_m5inv": [_dp, d, i],
+            "ref_zmobius_kappa_dslash_5_plus": [_dp, _dp, d, i],
             "ref_zmobius_m": [_dp, _dp, _dp, d],
             "ref_zmobius_mdag": [_dp, _dp, _dp, d],
             "ref_zmobius_mdagm": [_dp, _dp, _dp, _dp, d],

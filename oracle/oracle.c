@@ -582,3 +582,108 @@ int orc_minvcg(orc_mdagm_fn op, void *ctx, long n, double **psi,
   free(rsd_sq);
   return k;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Full-lattice solves (DiracOp*::MatInv with the CG inverter)             */
+/* ---------------------------------------------------------------------- */
+void orc_mobius_m5(const orc_geom *g, const orc_mobius *mp, double *inout, double mass) {
+  long n = 24 * vol_cb(g) * g->ls;
+  double *t = malloc(sizeof(double) * n);
+  memcpy(t, inout, sizeof(double) * n);
+  mobius_hop5_acc(g, g->ls, mp->K, inout, t, mass, 0);
+  free(t);
+}
+
+typedef struct {
+  const orc_geom *g;
+  const orc_mobius *mp;
+  const double *u;
+  double mass, m5, kappa;
+  int kind; /* 0 Wilson, 1 DWF, 2 Mobius */
+} matinv_ctx;
+
+static void matinv_mdagm(void *vctx, double *out, const double *in, double *dot) {
+  const matinv_ctx *c = (const matinv_ctx *)vctx;
+  if (c->kind == 0) orc_wilson_mdagm(c->g, out, c->u, in, c->kappa, dot);
+  else if (c->kind == 1) orc_dwf_mdagm(c->g, out, c->u, in, c->mass, c->m5, dot);
+  else orc_mobius_mdagm(c->g, c->mp, out, c->u, in, c->mass, dot);
+}
+
+/* out[k] = a * x[k] + y[k] (fTimesV1PlusV2) */
+static void axpy_to(double *out, double a, const double *x, const double *y, long n) {
+  for (long k = 0; k < n; k++) out[k] = a * x[k] + y[k];
+}
+
+/* Wilson and DWF share the steps (d_op_wilson.C:257-334, d_op_dwf.C:316-492):
+ * temp = kappa Dslash(in_even, CHKB_EVEN) + in_odd; b = MatPcDag temp;
+ * CG on the odd checkerboard; out_even = kappa Dslash(out_odd, CHKB_ODD) + in_even. */
+static int wilson_dwf_matinv(const matinv_ctx *c, double *out, const double *in, double stop_rsd,
+                             int max_num_iter, double *true_res) {
+  const orc_geom *g = c->g;
+  long half = 24 * vol_cb(g) * g->ls;
+  const double *in_odd = in, *in_even = in + half;
+  double *out_odd = out, *out_even = out + half;
+  double *temp = malloc(sizeof(double) * half), *b = malloc(sizeof(double) * half);
+  if (c->kind == 0) orc_wilson_dslash(g, temp, c->u, in_even, 0, 0);
+  else orc_dwf_dslash(g, temp, c->u, in_even, c->mass, 0, 0);
+  axpy_to(temp, c->kappa, temp, in_odd, half);
+  if (c->kind == 0) orc_wilson_m(g, b, c->u, temp, c->kappa, 1);
+  else orc_dwf_m(g, b, c->u, temp, c->mass, c->m5, 1);
+  int iter = orc_invcg(matinv_mdagm, (void *)c, half, out_odd, b, 0.0, stop_rsd, max_num_iter, true_res, 0);
+  if (c->kind == 0) orc_wilson_dslash(g, temp, c->u, out_odd, 1, 0);
+  else orc_dwf_dslash(g, temp, c->u, out_odd, c->mass, 1, 0);
+  axpy_to(out_even, c->kappa, temp, in_even, half);
+  free(temp);
+  free(b);
+  return iter;
+}
+
+int orc_wilson_matinv(const orc_geom *g, double *out, const double *u, const double *in, double kappa,
+                      double stop_rsd, int max_num_iter, double *true_res) {
+  matinv_ctx c = {g, 0, u, 0.0, 0.0, kappa, 0};
+  return wilson_dwf_matinv(&c, out, in, stop_rsd, max_num_iter, true_res);
+}
+
+int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double *in, double mass, double m5,
+                   double stop_rsd, int max_num_iter, double *true_res) {
+  matinv_ctx c = {g, 0, u, mass, m5, 1.0 / (2.0 * (4.0 + 1.0 - m5)), 1};  /* dwf_kappa, a5inv = 1 */
+  return wilson_dwf_matinv(&c, out, in, stop_rsd, max_num_iter, true_res);
+}
+
+/* d_op_mobius.C:407-700, SYM2 (real b, c: kappa_b the same for every s). */
+int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                      double mass, double stop_rsd, int max_num_iter, double *true_res) {
+  long half = 24 * vol_cb(g) * g->ls;
+  const double *even_in = in, *odd_in = in + half;
+  double *even_out = out, *odd_out = out + half;
+  double *temp = malloc(sizeof(double) * half), *temp2 = malloc(sizeof(double) * half),
+         *b = malloc(sizeof(double) * half);
+  const double kb = creal(mp->kappa_b[0]);
+  /* source: temp = kappa_b Dslash_4(M5^-1 in_even, CHKB_EVEN) + in_odd (:482-490) */
+  memcpy(temp, even_in, sizeof(double) * half);
+  orc_mobius_m5inv(g, mp, temp, mass, 0);
+  orc_mobius_dslash_4(g, mp, temp2, u, temp, 0, 0, mass);
+  axpy_to(temp, kb, temp2, odd_in, half);
+  /* guess: odd_out <- M5 odd_out (:503-515) */
+  orc_mobius_m5(g, mp, odd_out, mass);
+  /* CG on MatPcDag temp (:540-548) */
+  orc_mobius_m(g, mp, b, u, temp, mass, 1);
+  matinv_ctx c = {g, mp, u, mass, 0.0, 0.0, 2};
+  int iter = orc_invcg(matinv_mdagm, &c, half, odd_out, b, 0.0, stop_rsd, max_num_iter, true_res, 0);
+  /* odd_out <- M5^-1 odd_out; even_out = M5^-1 (kappa_b Dslash_4(odd_out, CHKB_ODD)) + M5^-1 in_even
+   * (:629-646) */
+  orc_mobius_m5inv(g, mp, odd_out, mass, 0);
+  orc_mobius_dslash_4(g, mp, temp, u, odd_out, 1, 0, mass);
+  for (long k = 0; k < half; k++) temp[k] *= kb;
+  memcpy(even_out, temp, sizeof(double) * half);
+  orc_mobius_m5inv(g, mp, even_out, mass, 0);
+  memcpy(temp, even_in, sizeof(double) * half);
+  orc_mobius_m5inv(g, mp, temp, mass, 0);
+  for (long k = 0; k < half; k++) even_out[k] += temp[k];
+  /* out *= 2 kappa_b (:667-677) */
+  for (long k = 0; k < 2 * half; k++) out[k] *= 2.0 * kb;
+  free(temp);
+  free(temp2);
+  free(b);
+  return iter;
+}

@@ -71,6 +71,12 @@ void orc_mobius_mdagm(const orc_geom *g, const orc_mobius *mp, double *out,
                       const double *u, const double *in, double mass,
                       double *dot);
 
+/* M5 = 1 + K D5 applied in place (the fifth-direction part with the
+ * kappa ratio K per s): what DiracOpMobius::MatInv applies to the initial
+ * guess for SYM2 (d_op_mobius.C:505-515 via zmobius_kappa_dslash_5_plus_cmplx,
+ * zmobius_dslash_5_plus.C:125-374, which accumulates into its output). */
+void orc_mobius_m5(const orc_geom *g, const orc_mobius *mp, double *inout, double mass);
+
 /* CG on MatPcDagMatPc (+shift): DiracOp::InvCgShift, inv_cg.C:84-448.
  * The operator is a callback: out = MdagM in, *dot = |M in|^2 when dot!=0.
  * Returns itr+1 as the reference does; *true_res = |b - A x| / |b|. */
@@ -87,6 +93,21 @@ int orc_minvcg(orc_mdagm_fn op, void *ctx, long n, double **psi,
                const double *chi, double chi_norm, const double *shift,
                int nshift, double *rsdcg, int type, const double *alpha,
                int max_num_iter);
+
+/* Full-lattice solves, DiracOp*::MatInv with the CG inverter.  in and out
+ * hold both checkerboards, half = 24*ls*Vh reals each: Wilson and DWF put
+ * the odd checkerboard (the one the CG solves on) first, Mobius the even
+ * one first, as the reference does.  out holds the initial guess of the
+ * CG's checkerboard on entry.  Returns the CG's iteration count.
+ *   orc_wilson_matinv  d_op_wilson.C:257-334  (kappa = Wilson kappa)
+ *   orc_dwf_matinv     d_op_dwf.C:316-492     (kappa = DWF kappa_5)
+ *   orc_mobius_matinv  d_op_mobius.C:407-700  (SYM2) */
+int orc_wilson_matinv(const orc_geom *g, double *out, const double *u, const double *in, double kappa,
+                      double stop_rsd, int max_num_iter, double *true_res);
+int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double *in, double mass, double m5,
+                   double stop_rsd, int max_num_iter, double *true_res);
+int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                      double mass, double stop_rsd, int max_num_iter, double *true_res);
 
 #ifdef __cplusplus
 }

@@ -126,6 +126,11 @@ void ref_zmobius_dslash_4(double *out, double *u, double *in, int cb, int dag, d
 void ref_zmobius_m5inv(double *inout, double mass, int dag) {
   zmobius_m5inv((Vector *)inout, mass, dag, &g_dwf, g_dwf.zmobius_kappa_ratio.data());
 }
+// zmobius_dslash_5_plus.C:125: out += the kappa-ratio-weighted fifth-direction hop of in
+void ref_zmobius_kappa_dslash_5_plus(double *out, double *in, double mass, int dag) {
+  zmobius_kappa_dslash_5_plus_cmplx((Vector *)out, (Vector *)in, mass, dag, &g_dwf,
+                                    g_dwf.zmobius_kappa_ratio.data());
+}
 void ref_zmobius_m(double *out, double *u, double *in, double mass) {
   zmobius_m((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
 }

@@ -78,6 +78,27 @@ class OracleOps:
         self.O.orc_mobius_m5inv(C.byref(self.g), C.byref(self.mp), p(y), mass, dag)
         return y
 
+    def mobius_m5(self, x, mass):
+        y = np.ascontiguousarray(x).copy()
+        self.O.orc_mobius_m5(C.byref(self.g), C.byref(self.mp), p(y), mass)
+        return y
+
+    def matinv(self, kind, src, out0=None, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000):
+        """DiracOp*::MatInv on both checkerboards (see oracle.h for the halves' order)"""
+        out = np.zeros(2 * self.n) if out0 is None else np.ascontiguousarray(out0).copy()
+        src = np.ascontiguousarray(src)
+        tr = C.c_double()
+        if kind == "wilson":
+            it = self.O.orc_wilson_matinv(C.byref(self.g1), p(out), p(self.u), p(src), kappa, stop_rsd,
+                                          max_num_iter, C.byref(tr))
+        elif kind == "dwf":
+            it = self.O.orc_dwf_matinv(C.byref(self.g), p(out), p(self.u), p(src), mass, self.m5, stop_rsd,
+                                       max_num_iter, C.byref(tr))
+        else:
+            it = self.O.orc_mobius_matinv(C.byref(self.g), C.byref(self.mp), p(out), p(self.u), p(src), mass,
+                                          stop_rsd, max_num_iter, C.byref(tr))
+        return out, it, tr.value
+
     def mobius_m(self, x, mass, dag):
         y = self.z()
         self.O.orc_mobius_m(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(x), mass, dag)

@@ -139,3 +139,32 @@ def test_failure_injection_nonfinite_source(oracle):
     x = np.zeros(ops.n)
     r = D.InvCg(x, b, stop_rsd=1e-10, max_num_iter=50)
     assert r.status == A.NONFINITE
+
+
+@pytest.mark.parametrize("kind,L,ls,mass", [("wilson", (4, 4, 4, 8), 1, 0.1), ("dwf", (4, 4, 4, 8), 8, 0.05),
+                                           ("mobius", (4, 4, 4, 4), 8, 0.05)])
+@pytest.mark.parametrize("prec", [A.DOUBLE, A.SINGLE])
+def test_matinv_matches_oracle(oracle, kind, L, ls, mass, prec):
+    """DiracOp*::MatInv on both checkerboards against the oracle's
+    restatement (d_op_wilson.C:257, d_op_dwf.C:316, d_op_mobius.C:407)."""
+    u = gen_gauge(L, seed=131)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    if kind == "wilson":
+        D = DiracOpWilson(lat, mass=mass)
+    elif kind == "dwf":
+        D = DiracOpDwf(lat, mass=mass, ls=ls)
+    else:
+        D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    ops = OracleOps(oracle, L, u, ls=ls, b=1.5, c=0.5)
+    src = gen_gaussian(2 * D.f_size, seed=132)
+    guess = gen_gaussian(2 * D.f_size, seed=133) * 1e-3  # a non-zero initial guess
+    xo, ito, tro = ops.matinv(kind, src, out0=guess, mass=mass, kappa=D.kappa, stop_rsd=1e-12)
+    x = guess.copy()
+    src0 = src.copy()
+    r = D.MatInv(x, src, stop_rsd=1e-12, precision=prec)
+    assert np.array_equal(src, src0)  # the source is preserved
+    assert r.status == A.CONVERGED and r.true_res <= 1e-12
+    assert rel(x, xo) < 1e-9
+    if prec == A.DOUBLE:
+        assert abs(r.iterations - ito) <= 1

@@ -80,6 +80,10 @@ def test_mobius_vs_reference(oracle, reference, L, ls, mass, b, c):
         y = psi.copy()
         reference.ref_zmobius_m5inv(p(y), mass, dag)
         assert rel(ops.mobius_m5inv(psi, mass, dag), y) < TOL
+    # M5 = 1 + K D5 (zmobius_kappa_dslash_5_plus_cmplx accumulates into its output)
+    y = psi.copy()
+    reference.ref_zmobius_kappa_dslash_5_plus(p(y), p(psi), mass, 0)
+    assert rel(ops.mobius_m5(psi, mass), y) < TOL
     for cb in (0, 1):
         for dag in (0, 1):
             y = np.zeros_like(psi)

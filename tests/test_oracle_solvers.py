@@ -78,3 +78,43 @@ def test_mobius_cg(oracle):
     x, it, tr = ops.invcg("mobius", b, mass=0.1, stop_rsd=1e-10)
     Ax, _ = ops.mobius_mdagm(x, 0.1)
     assert tr < 2e-10 and rel(Ax, b) < 2e-10
+
+
+def _full_m(ops, kind, x, kappa, mass=0.0):
+    """The unpreconditioned operator on [odd | even] halves: 1 - kappa Dslash"""
+    n = ops.n
+    xo, xe = x[:n], x[n:]
+    if kind == "wilson":
+        ho, he = ops.wilson_dslash(xe, 0, 0), ops.wilson_dslash(xo, 1, 0)
+    else:
+        ho, he = ops.dwf_dslash(xe, mass, 0, 0), ops.dwf_dslash(xo, mass, 1, 0)
+    return np.concatenate([xo - kappa * ho, xe - kappa * he])
+
+
+@pytest.mark.parametrize("kind", ["wilson", "dwf"])
+def test_matinv_solves_the_full_operator(oracle, kind):
+    """DiracOpWilson/Dwf::MatInv (d_op_wilson.C:257, d_op_dwf.C:316): the
+    returned field solves the unpreconditioned system on both checkerboards."""
+    L = (4, 4, 4, 4)
+    ls = 1 if kind == "wilson" else 4
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=31), ls=ls)
+    b = gen_gaussian(2 * ops.n, seed=32)
+    kappa = 0.12 if kind == "wilson" else 1 / (2 * (5 - 1.8))
+    x, it, tr = ops.matinv(kind, b, mass=0.1, kappa=kappa, stop_rsd=1e-12)
+    assert tr < 1e-11 and it > 2
+    assert rel(_full_m(ops, kind, x, kappa, mass=0.1), b) < 1e-9
+
+
+def test_mobius_m5_and_m5inv_are_inverse(oracle):
+    L = (4, 4, 2, 4)
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=33), ls=6, b=1.5, c=0.5)
+    x = gen_gaussian(ops.n, seed=34)
+    assert rel(ops.mobius_m5inv(ops.mobius_m5(x, 0.05), 0.05, 0), x) < 1e-13
+
+
+def test_mobius_matinv_converges(oracle):
+    L = (4, 4, 2, 4)
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=35), ls=6, b=1.5, c=0.5)
+    b = gen_gaussian(2 * ops.n, seed=36)
+    x, it, tr = ops.matinv("mobius", b, mass=0.05, stop_rsd=1e-12)
+    assert tr < 1e-11 and it > 2 and np.all(np.isfinite(x))
