@@ -15,10 +15,18 @@ LIB_PATH = Path(__file__).resolve().parent / "libcpsgpu.so"
 DOUBLE, SINGLE, HALF = 0, 1, 2
 LINKS_F32_12, LINKS_F32_18 = 112, 118  # link forms of the FP16 operator that read FP32 links
 WILSON, DWF, MOBIUS = 0, 1, 2
+
+
+class StrOrd:
+    """StrOrdType values (enum_int.h:87-97) the host conversions take"""
+    CANONICAL = 0
+    WILSON = 2
+
 MS_SINGLE, MS_MULTI, MS_GENERAL = 0, 1, 2
 CONVERGED, MAX_ITER, BREAKDOWN, NONFINITE = 1, 2, 3, 4
 
 _dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
 
 
 class DiracArg(C.Structure):
@@ -76,6 +84,10 @@ def lib() -> C.CDLL:
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_fconvert": (C.c_int, [_ip, C.c_int, _dp, C.c_int, C.c_int]),
+            "cpsgpu_gconvert": (C.c_int, [_ip, _dp, C.c_int, C.c_int]),
+            "cpsgpu_four2five": (C.c_int, [_ip, C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_five2four": (C.c_int, [_ip, C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_invcg_multi": (C.c_int, [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(CgArg),
                                              C.POINTER(CgResult)]),
             "cpsgpu_minvcg": (C.c_int, [vp, C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,

@@ -20,6 +20,10 @@ double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes)
 double time_mdagm(Dirac &D, int prec, int reps, double *bytes);
 double time_m5inv(Dirac &D, int prec, int reps, double *bytes);
 double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
+void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
+void gconvert(const int node_sites[4], double *u, int to, int from);
+void four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
+void five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb);
 int minvcg(Dirac &D, double *const *psi, const double *chi, double chi_norm, const double *shift, int nshift,
            double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine);
 }  // namespace cpsgpu
@@ -205,6 +209,35 @@ int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals) {
     if (reals != 12 && reals != 18 && !(f32 && prec == CPSGPU_HALF))
       throw Error(CPSGPU_ERR_ARG, "reals must be 12 or 18 (or FP32 links for the FP16 operator)");
     lat->L->sloppy_recon[prec] = reals;
+    return CPSGPU_OK;
+  });
+}
+
+// ---- host-side storage orders (convert.cpp)
+int cpsgpu_fconvert(const int node_sites[4], int ls, double *f, int to, int from) {
+  return guarded([&] {
+    fconvert(node_sites, ls, f, to, from);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_gconvert(const int node_sites[4], double *u, int to, int from) {
+  return guarded([&] {
+    gconvert(node_sites, u, to, from);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb) {
+  return guarded([&] {
+    four2five(node_sites, ls, five, four, s_u, s_l, ncb);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb) {
+  return guarded([&] {
+    five2four(node_sites, ls, four, five, s_u, s_l, ncb);
     return CPSGPU_OK;
   });
 }

@@ -39,6 +39,48 @@ def gen_gaussian(n: int, seed: int = 20261203, stream: int = 0) -> np.ndarray:
     return out
 
 
+StrOrd = A.StrOrd
+
+
+def fconvert(node_sites, ls: int, f: np.ndarray, to: int, frm: int) -> None:
+    """FwilsonTypes / FdwfBase::Fconvert (CANONICAL <-> WILSON) in place"""
+    _inplace(f, 24 * ls * int(np.prod(node_sites)))
+    check(lib().cpsgpu_fconvert(A.ints(node_sites), ls, dptr(f), to, frm))
+
+
+def gconvert(node_sites, u: np.ndarray, to: int, frm: int) -> None:
+    """Lattice::Convert of the gauge field (CANONICAL <-> WILSON) in place"""
+    _inplace(u, 72 * int(np.prod(node_sites)))
+    check(lib().cpsgpu_gconvert(A.ints(node_sites), dptr(u), to, frm))
+
+
+def four2five(node_sites, ls: int, four: np.ndarray, s_u: int, s_l: int, ncb: int = 2) -> np.ndarray:
+    """FdwfBase::Ffour2five: the 5D field with the 4D one on the walls"""
+    v4 = int(np.prod(node_sites)) * ncb // 2
+    four = np.ascontiguousarray(four, dtype=np.float64)
+    if four.size != 24 * v4:
+        raise ValueError("4D field size")
+    five = np.empty(24 * ls * v4)
+    check(lib().cpsgpu_four2five(A.ints(node_sites), ls, dptr(five), dptr(four), s_u, s_l, ncb))
+    return five
+
+
+def five2four(node_sites, ls: int, five: np.ndarray, s_u: int, s_l: int, ncb: int = 2) -> np.ndarray:
+    """FdwfBase::Ffive2four: the 4D field read off the walls"""
+    v4 = int(np.prod(node_sites)) * ncb // 2
+    five = np.ascontiguousarray(five, dtype=np.float64)
+    if five.size != 24 * ls * v4:
+        raise ValueError("5D field size")
+    four = np.empty(24 * v4)
+    check(lib().cpsgpu_five2four(A.ints(node_sites), ls, dptr(four), dptr(five), s_u, s_l, ncb))
+    return four
+
+
+def _inplace(a, n):
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size == n):
+        raise TypeError(f"expected a C-contiguous float64 array of {n} reals (converted in place)")
+
+
 class Lattice:
     def __init__(self, node_sites, bc=(1, 1, 1, -1)):
         self.node_sites = tuple(int(x) for x in node_sites)

@@ -100,6 +100,28 @@ int cpsgpu_synchronize(cpsgpu_lattice lat);
 #define CPSGPU_LINKS_F32_18 118
 int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals);
 
+/* ---- storage orders on the host (no device work) ----
+ * StrOrdType values (enum_int.h:87-97).  Fields hold both checkerboards.
+ *   cpsgpu_fconvert  FwilsonTypes::Fconvert / FdwfBase::Fconvert
+ *                    (convert.C:444-562, :639-1000): fermion, 24*ls*vol reals
+ *                    in place; ls = 1 for a 4D field.  4D WILSON order puts
+ *                    the odd checkerboard first; 5D WILSON is the DWF
+ *                    even-odd order (odd part: slice s holds the 4D sites of
+ *                    parity (s+1)%2).
+ *   cpsgpu_gconvert  Lattice::Convert for the gauge field (convert.C:141-420):
+ *                    72*vol reals in place; WILSON = even parity first, each
+ *                    link stored transposed (col, row).
+ *   cpsgpu_four2five / cpsgpu_five2four  FdwfBase::Ffour2five / Ffive2four
+ *                    (f_dwf_base.C:961, :1068): the upper spin half of slice
+ *                    s_u and the lower one of slice s_l carry the 4D field;
+ *                    ncb = 2 for both checkerboards, 1 for one. */
+#define CPSGPU_STR_CANONICAL 0
+#define CPSGPU_STR_WILSON 2
+int cpsgpu_fconvert(const int node_sites[4], int ls, double *f, int to, int from);
+int cpsgpu_gconvert(const int node_sites[4], double *u, int to, int from);
+int cpsgpu_four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
+int cpsgpu_five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb);
+
 /* ---- Dirac operators ---- */
 typedef struct {
   int kind;        /* CPSGPU_WILSON / CPSGPU_DWF / CPSGPU_MOBIUS */

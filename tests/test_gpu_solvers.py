@@ -168,3 +168,32 @@ def test_matinv_matches_oracle(oracle, kind, L, ls, mass, prec):
     assert rel(x, xo) < 1e-9
     if prec == A.DOUBLE:
         assert abs(r.iterations - ito) <= 1
+
+
+def test_dwf_propagator_flow_from_canonical_fields(oracle):
+    """What a propagator job does around the solve: a CANONICAL gauge field and
+    4D source, Ffour2five onto the walls, Fconvert to WILSON, MatInv,
+    Fconvert back and Ffive2four, against the same steps on the oracle."""
+    from cps_veloc_b200.dirac import StrOrd, fconvert, five2four, four2five, gconvert
+
+    L, ls, mass = (4, 4, 4, 8), 8, 0.05
+    u_w = gen_gauge(L, seed=141)
+    u_c = u_w.copy()
+    gconvert(L, u_c, StrOrd.CANONICAL, StrOrd.WILSON)  # as a reader would deliver it
+    u = u_c.copy()
+    gconvert(L, u, StrOrd.WILSON, StrOrd.CANONICAL)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    src4 = gen_gaussian(24 * int(np.prod(L)), seed=142)
+    src5 = four2five(L, ls, src4, 0, ls - 1)
+    fconvert(L, ls, src5, StrOrd.WILSON, StrOrd.CANONICAL)
+    x = np.zeros_like(src5)
+    r = D.MatInv(x, src5, stop_rsd=1e-12)
+    xo, _, _ = ops.matinv("dwf", src5, mass=mass, stop_rsd=1e-12)
+    assert r.status == A.CONVERGED and rel(x, xo) < 1e-9
+    fconvert(L, ls, x, StrOrd.CANONICAL, StrOrd.WILSON)
+    prop = five2four(L, ls, x, ls - 1, 0)
+    fconvert(L, ls, xo, StrOrd.CANONICAL, StrOrd.WILSON)
+    assert rel(prop, five2four(L, ls, xo, ls - 1, 0)) < 1e-9
