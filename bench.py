@@ -156,7 +156,7 @@ def field(A, D, prec, host=None):
     return h
 
 
-def solve_dev(A, D, x, bf, zero, prec, delta=0.1):
+def solve_dev(A, D, x, bf, zero, prec, delta=0.0):
     a = A.CgArg()
     A.lib().cpsgpu_cg_arg_default(C.byref(a))
     a.stop_rsd = STOP

@@ -111,7 +111,10 @@ CgArgs to_args(const cpsgpu_cg_arg *a) {
   c.max_num_iter = a->max_num_iter;
   c.src_norm_sq = a->src_norm_sq;
   c.shift = a->shift;
-  c.delta = a->delta > 0 ? a->delta : 0.1;
+  // reliable-update threshold: measured on DWF 16^3x32, Ls=16, the FP32 inner
+  // solve is fastest at 0.01 (fewer FP64 updates, no extra iterations), the
+  // FP16 one at 0.1 (smaller values inflate its iteration count)
+  c.delta = a->delta > 0 ? a->delta : (a->precision == CPSGPU_SINGLE ? 0.01 : 0.1);
   c.chunk = a->chunk > 0 ? a->chunk : 8;
   c.use_graph = a->use_graph;
   return c;
@@ -387,7 +390,7 @@ void cpsgpu_cg_arg_default(cpsgpu_cg_arg *a) {
   a->src_norm_sq = 0.0;
   a->shift = 0.0;
   a->precision = CPSGPU_DOUBLE;
-  a->delta = 0.1;
+  a->delta = 0.0;
   a->chunk = 8;
   a->use_graph = 1;
 }

@@ -251,7 +251,7 @@ __device__ void block_partial(double (&v)[NV], double *partials) {
   block_partial<NV>(v, partials, blockIdx.z, blockIdx.x + gridDim.x * blockIdx.y, gridDim.x * gridDim.y);
 }
 
-constexpr int FINALIZE_THREADS = 256;
+constexpr int FINALIZE_THREADS = 1024;
 
 // One block per solve: sum its nblk partials (thread-strided, then the warp
 // and block trees, always in the same order) and finalize its scalars.  The
@@ -269,7 +269,21 @@ __global__ void __launch_bounds__(FINALIZE_THREADS)
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) acc[k] = 0.0;
-  for (unsigned b = tid; b < nblk; b += FINALIZE_THREADS)
+  // eight independent loads in flight per thread (the sum order stays fixed)
+  constexpr int U = 8;
+  unsigned b = tid;
+  for (; b + (U - 1) * FINALIZE_THREADS < nblk; b += U * FINALIZE_THREADS) {
+    double v[U][NV];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int k = 0; k < NV; k++) v[u][k] = part[(size_t)(b + u * FINALIZE_THREADS) * NV + k];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int k = 0; k < NV; k++) acc[k] += v[u][k];
+  }
+  for (; b < nblk; b += FINALIZE_THREADS)
 #pragma unroll
     for (int k = 0; k < NV; k++) acc[k] += part[(size_t)b * NV + k];
   warp_sum(acc);

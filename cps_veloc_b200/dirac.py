@@ -193,7 +193,7 @@ class _DiracOp:
         return a
 
     def InvCg(self, sol, src, stop_rsd=1e-8, max_num_iter=10000, src_norm_sq=0.0, shift=0.0,
-              precision=A.DOUBLE, delta=0.1, chunk=8, use_graph=True) -> CgResult:
+              precision=A.DOUBLE, delta=0.0, chunk=8, use_graph=True) -> CgResult:
         """DiracOp::InvCg(out, in, src_norm_sq, true_res): sol is the initial guess, updated in place."""
         src = self._vec(src)
         if not (isinstance(sol, np.ndarray) and sol.dtype == np.float64 and sol.flags.c_contiguous):
@@ -204,7 +204,7 @@ class _DiracOp:
         check(lib().cpsgpu_invcg(self._h, dptr(sol), dptr(src), C.byref(a), C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
 
-    def MatInv(self, out, src, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.1, chunk=8,
+    def MatInv(self, out, src, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.0, chunk=8,
                use_graph=True) -> CgResult:
         """DiracOp*::MatInv(out, in, true_res) with CG: both checkerboards
         (2 * f_size reals; Wilson/DWF [odd | even], Mobius [even | odd]).
@@ -220,7 +220,7 @@ class _DiracOp:
         check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
 
-    def InvCgMulti(self, sols, srcs, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.1,
+    def InvCgMulti(self, sols, srcs, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.0,
                    chunk=8, use_graph=True):
         n = len(srcs)
         srcs = [self._vec(s) for s in srcs]

@@ -182,7 +182,7 @@ typedef struct {
   double src_norm_sq;  /* 0: computed (inv_cg.C:166-169) */
   double shift;        /* solve (MatPcDagMatPc + shift) x = b */
   int precision;       /* CPSGPU_DOUBLE: plain FP64 CG; SINGLE / HALF: mixed precision */
-  double delta;        /* reliable-update threshold (mixed precision); 0: default 0.1 */
+  double delta;        /* reliable-update threshold (mixed precision); 0: 0.01 for FP32, 0.1 for FP16 */
   int chunk;           /* iterations per CUDA-graph launch; 0: default 8 */
   int use_graph;       /* capture the iteration chunk in a CUDA graph */
 } cpsgpu_cg_arg;
