@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
             "cpsgpu_set_rhs_tile": (C.c_int, [vp, C.c_int, C.c_int]),
             "cpsgpu_dirac_create": (C.c_int, [vp, C.POINTER(DiracArg), C.POINTER(vp)]),
             "cpsgpu_dirac_destroy": (C.c_int, [vp]),
+            "cpsgpu_dirac_set_zmobius": (C.c_int, [vp, _dp, _dp]),
             "cpsgpu_dirac_info": (C.c_int, [vp, _dp, _dp]),
             "cpsgpu_dslash": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_matpc": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),

@@ -271,6 +271,23 @@ int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *a, cpsgpu_di
   });
 }
 
+int cpsgpu_dirac_set_zmobius(cpsgpu_dirac d, const double *b, const double *c) {
+  return guarded([&] {
+    if (!d || !b || !c) throw Error(CPSGPU_ERR_ARG, "null argument");
+    Dirac &D = *d->D;
+    if (D.kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "complex b_s, c_s: Mobius operators only");
+    std::vector<std::complex<double>> bs(D.ls), cs(D.ls);
+    for (int s = 0; s < D.ls; s++) {
+      bs[s] = {b[2 * s], b[2 * s + 1]};
+      cs[s] = {c[2 * s], c[2 * s + 1]};
+    }
+    CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));  // no launch may still read the old matrices
+    D.build_mobius(bs, cs);
+    for (auto &s : d->solvers) s.reset();  // captured graphs hold the old matrices
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_dirac_destroy(cpsgpu_dirac d) {
   return guarded([&] {
     delete d;
@@ -440,6 +457,7 @@ int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg
     const cudaStream_t s = L.stream;
     const size_t half = vec_reals(d);
     const bool mob = (D.kind == KIND_MOBIUS);
+    if (D.cplx) throw Error(CPSGPU_ERR_ARG, "MatInv: real Mobius coefficients only");
     // the CG's checkerboard and the other one, as the reference orders them
     const double *in_cg = mob ? in + half : in, *in_other = mob ? in : in + half;
     double *out_cg = mob ? out + half : out, *out_other = mob ? out : out + half;

@@ -194,7 +194,7 @@ __global__ void export_kernel(SpinorView src, double *dst, size_t n) {
 // out(s) = sum_t Mix_chi[s][t] in(t), block = (BX sites, all Ls slices)
 template <int P>
 __global__ void mix_kernel(SpinorView in, SpinorView out, const double *mix, int ls, const SolverScalars *st,
-                           int gate) {
+                           int gate, int cplx) {
   using R = RealT<P>;
   if (gate == GATE_RUNNING && st[blockIdx.z].done) return;
   if (gate == GATE_RELIABLE && (st[blockIdx.z].done || !st[blockIdx.z].reliable)) return;
@@ -202,7 +202,7 @@ __global__ void mix_kernel(SpinorView in, SpinorView out, const double *mix, int
   R *sm = reinterpret_cast<R *>(smraw);
   double *mx = reinterpret_cast<double *>(sm + (size_t)ls * blockDim.x * 24);
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  for (int k = tid; k < 2 * ls * ls; k += blockDim.x * blockDim.y) mx[k] = mix[k];
+  for (int k = tid; k < 2 * ls * ls * (cplx ? 2 : 1); k += blockDim.x * blockDim.y) mx[k] = mix[k];
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int s = threadIdx.y;
   const long rhs = blockIdx.z;
@@ -217,13 +217,29 @@ __global__ void mix_kernel(SpinorView in, SpinorView out, const double *mix, int
   if (!active) return;
 #pragma unroll
   for (int k = 0; k < 24; k++) a[k] = R(0);
-  for (int t = 0; t < ls; t++) {
-    const R mu_ = R(mx[s * ls + t]), md_ = R(mx[ls * ls + s * ls + t]);
-    const R *src = sm + (size_t)t * 24 * blockDim.x + threadIdx.x;
+  if (!cplx) {
+    for (int t = 0; t < ls; t++) {
+      const R mu_ = R(mx[s * ls + t]), md_ = R(mx[ls * ls + s * ls + t]);
+      const R *src = sm + (size_t)t * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < 12; k++) a[k] += mu_ * src[k * blockDim.x];
+      for (int k = 0; k < 12; k++) a[k] += mu_ * src[k * blockDim.x];
 #pragma unroll
-    for (int k = 12; k < 24; k++) a[k] += md_ * src[k * blockDim.x];
+      for (int k = 12; k < 24; k++) a[k] += md_ * src[k * blockDim.x];
+    }
+  } else {
+    // complex entries ([..][re, im]) on the (re, im) pairs of the spinor
+    for (int t = 0; t < ls; t++) {
+      const double *pu = mx + 2 * (s * ls + t), *pd = mx + 2 * (ls * ls + s * ls + t);
+      const R ur = R(pu[0]), ui = R(pu[1]), dr = R(pd[0]), di = R(pd[1]);
+      const R *src = sm + (size_t)t * 24 * blockDim.x + threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) {
+        const R xr = src[k * blockDim.x], xi = src[(k + 1) * blockDim.x];
+        const R mr = k < 12 ? ur : dr, mi = k < 12 ? ui : di;
+        a[k] += mr * xr - mi * xi;
+        a[k + 1] += mr * xi + mi * xr;
+      }
+    }
   }
   SpinorIO<P>::store(out, rhs * ls + s, i, a);
 }
@@ -420,17 +436,17 @@ void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &i
   dim3 block(p2, ls);
   dim3 grid((unsigned)((in.vh + p2 - 1) / p2), 1, in.nrhs);
   size_t rs = prec == PREC_DOUBLE ? 8 : 4;
-  size_t smem = (size_t)ls * p2 * 24 * rs + 2 * (size_t)ls * ls * sizeof(double);
+  size_t smem = (size_t)ls * p2 * 24 * rs + 2 * (size_t)ls * ls * sizeof(double) * (D.cplx ? 2 : 1);
   cudaStream_t s = D.lat->stream;
   if (prec == PREC_DOUBLE) {
     CPSGPU_CUDA(cudaFuncSetAttribute(mix_kernel<PREC_DOUBLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mix_kernel<PREC_DOUBLE><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate);
+    mix_kernel<PREC_DOUBLE><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate, D.cplx ? 1 : 0);
   } else if (prec == PREC_SINGLE) {
     CPSGPU_CUDA(cudaFuncSetAttribute(mix_kernel<PREC_SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mix_kernel<PREC_SINGLE><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate);
+    mix_kernel<PREC_SINGLE><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate, D.cplx ? 1 : 0);
   } else {
     CPSGPU_CUDA(cudaFuncSetAttribute(mix_kernel<PREC_HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mix_kernel<PREC_HALF><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate);
+    mix_kernel<PREC_HALF><<<grid, block, smem, s>>>(in, out, mix, ls, st, gate, D.cplx ? 1 : 0);
   }
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;

@@ -1,5 +1,6 @@
 // Host-side structures of the library behind the C ABI (include/cpsgpu.h).
 #pragma once
+#include <complex>
 #include <cuda_runtime.h>
 #include <stdexcept>
 #include <string>
@@ -112,8 +113,15 @@ struct Dirac {
   //   P = B M5inv, Q = B M5inv kappa_b, R = kappa_b M5inv^+ B^+ (-kappa_b),
   //   S = M5inv^+ B^+, and the pieces B, B^+, M5inv, M5inv^+ on their own.
   DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id, mixM5;
-  std::vector<double> hM5i, hM5id, hB, hBd;
+  // complex per-slice b_s, c_s (zMobius): every matrix above is complex,
+  // stored [2][ls][ls][re, im], and the -kappa_b(s) of MatPc is the complex
+  // diagonal mixKb applied in a mixing epilogue
+  bool cplx = false;
+  DeviceBuffer mixKb;
+  std::vector<double> hM5i, hM5id, hB, hBd;  // host copies of the packed M5^-1 and B matrices
   Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_);
+  // (re)build the Mobius matrices from per-slice coefficients
+  void build_mobius(const std::vector<std::complex<double>> &bs, const std::vector<std::complex<double>> &cs);
   // right-hand sides per hop tile (consecutive blocks share links across
   // this many solves), per precision, set by the autotuner; 0 = untuned
   int rtile[3] = {0, 0, 0};

@@ -86,6 +86,7 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   hp.h5wall = -2.0 * D.mass;   // -2 m_f / a5
   for (int s = 0; s < D.ls && s < MAX_LS; s++) hp.coef[s] = L.coef.empty() ? 0.0 : L.coef[(size_t)s < L.coef.size() ? s : 0];
   hp.mix = L.mix;
+  hp.mix_cplx = (L.mix != nullptr && D.cplx) ? 1 : 0;
   hp.norm = L.norm;
   hp.red_op = L.red_op;
   hp.gate = L.gate;
@@ -113,7 +114,7 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   dim3 grid(nsb * hp.nsg * hp.rtile, 1, (unsigned)((in.nrhs + hp.rtile - 1) / hp.rtile));
   size_t smem = 0;
   if (mix) {
-    smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double);
+    smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double) * (D.cplx ? 2 : 1);
     static thread_local std::vector<std::pair<HopFn, size_t>> raised;
     bool done = false;
     for (auto &e : raised)

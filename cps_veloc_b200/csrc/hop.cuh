@@ -85,7 +85,8 @@ struct HopParams {
   double h5;        // DWF fifth-dir weight 2/a5
   double h5wall;    // DWF wall weight -2 m_f / a5
   double coef[MAX_LS];  // per-slice coefficient of the AXPY/CG/RES epilogues
-  const double *mix;    // [2][ls][ls] row-major, upper then lower chirality
+  const double *mix;    // [2][ls][ls] row-major, upper then lower chirality ([..][re, im] if mix_cplx)
+  int mix_cplx;         // complex mixing matrices (zMobius)
   int norm;         // AXPY: accumulate reductions
   int red_op;       // ReduceOp for the finalize
   int gate;         // Gate
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
     R *sm = reinterpret_cast<R *>(smraw);  // [ls][24][BX]: a warp's accesses are consecutive words
     double *mx = reinterpret_cast<double *>(sm + (size_t)hp.ls * blockDim.x * 24);
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    for (int k = tid; k < 2 * hp.ls * hp.ls; k += blockDim.x * blockDim.y) mx[k] = hp.mix[k];
+    const int nmx = 2 * hp.ls * hp.ls * (hp.mix_cplx ? 2 : 1);
+    for (int k = tid; k < nmx; k += blockDim.x * blockDim.y) mx[k] = hp.mix[k];
     if (s < hp.ls) {
       R *mine = sm + (size_t)s * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
@@ -244,14 +246,35 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
     if (active) {
 #pragma unroll
       for (int k = 0; k < 24; k++) acc[k] = R(0);
-      for (int t2 = 0; t2 < hp.ls; t2++) {
-        const R mu_ = R(mx[s * hp.ls + t2]);
-        const R md_ = R(mx[hp.ls * hp.ls + s * hp.ls + t2]);
-        const R *src = sm + (size_t)t2 * 24 * blockDim.x + threadIdx.x;
+      if (!hp.mix_cplx) {
+        for (int t2 = 0; t2 < hp.ls; t2++) {
+          const R mu_ = R(mx[s * hp.ls + t2]);
+          const R md_ = R(mx[hp.ls * hp.ls + s * hp.ls + t2]);
+          const R *src = sm + (size_t)t2 * 24 * blockDim.x + threadIdx.x;
 #pragma unroll
-        for (int k = 0; k < 12; k++) acc[k] += mu_ * src[k * blockDim.x];
+          for (int k = 0; k < 12; k++) acc[k] += mu_ * src[k * blockDim.x];
 #pragma unroll
-        for (int k = 12; k < 24; k++) acc[k] += md_ * src[k * blockDim.x];
+          for (int k = 12; k < 24; k++) acc[k] += md_ * src[k * blockDim.x];
+        }
+      } else {
+        // complex entries on (re, im) pairs
+        for (int t2 = 0; t2 < hp.ls; t2++) {
+          const double *pu = mx + 2 * (s * hp.ls + t2), *pd = mx + 2 * (hp.ls * hp.ls + s * hp.ls + t2);
+          const R ur = R(pu[0]), ui = R(pu[1]), dr = R(pd[0]), di = R(pd[1]);
+          const R *src = sm + (size_t)t2 * 24 * blockDim.x + threadIdx.x;
+#pragma unroll
+          for (int k = 0; k < 12; k += 2) {
+            const R xr = src[k * blockDim.x], xi = src[(k + 1) * blockDim.x];
+            acc[k] += ur * xr - ui * xi;
+            acc[k + 1] += ur * xi + ui * xr;
+          }
+#pragma unroll
+          for (int k = 12; k < 24; k += 2) {
+            const R xr = src[k * blockDim.x], xi = src[(k + 1) * blockDim.x];
+            acc[k] += dr * xr - di * xi;
+            acc[k + 1] += dr * xi + di * xr;
+          }
+        }
       }
     }
   }

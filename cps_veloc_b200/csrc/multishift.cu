@@ -200,10 +200,15 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
       Lh.coef.assign(ls, -D.kappa * D.kappa);
     }
     Lh.ep = EP_AXPY;
+    if (mob && D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
+      Lh.ep = EP_MIX_AXPY;
+      Lh.mix = D.mixKb.as<double>();
+    }
     Lh.cb = 0;
     Lh.norm = 1;
     Lh.red_op = RED_MS_PAP;
     launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
+    Lh.mix = nullptr;
     Lh.norm = 0;
     Lh.dag = 1;
     Lh.cb = 1;

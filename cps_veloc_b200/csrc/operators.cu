@@ -173,6 +173,18 @@ std::vector<double> pack(int n, const std::vector<cd> &up, const std::vector<cd>
   return r;
 }
 
+// pack [upper; lower] as complex: [2][n][n][re, im]
+std::vector<double> pack_complex(int n, const std::vector<cd> &up, const std::vector<cd> &dn) {
+  std::vector<double> r(4 * (size_t)n * n);
+  for (size_t k = 0; k < (size_t)n * n; k++) {
+    r[2 * k] = up[k].real();
+    r[2 * k + 1] = up[k].imag();
+    r[2 * ((size_t)n * n + k)] = dn[k].real();
+    r[2 * ((size_t)n * n + k) + 1] = dn[k].imag();
+  }
+  return r;
+}
+
 void upload(DeviceBuffer &buf, const std::vector<double> &h) {
   buf.alloc(h.size() * sizeof(double));
   CPSGPU_CUDA(cudaMemcpy(buf.ptr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -192,14 +204,30 @@ Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_
     kappa = 1.0 / (2.0 * (4.0 + 1.0 - m5));  // dwf_init.C:97-98, a5inv = 1
     return;
   }
-  // Mobius: d_op_mobius.C:112-131
-  kappa = 1.0 / (2.0 * (b * (4.0 - m5) + 1.0));
-  kappa_c = 1.0 / (2.0 * (c * (4.0 - m5) - 1.0));
-  std::vector<cd> bv(ls, b), cv(ls, c), kb(ls, kappa), K(ls, kappa / kappa_c);
+  // Mobius: d_op_mobius.C:112-131 (real b, c: the same for every slice)
+  build_mobius(std::vector<cd>(ls, b), std::vector<cd>(ls, c));
+}
+
+// Per-slice kappa_b, kappa_c and K = kappa_b / kappa_c as the zMobius
+// operator sets them (d_op_zmobius.C:246-292, a5inv = 1), and every s-local
+// matrix the operators apply.
+void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
+  std::vector<cd> kb(ls), kc(ls), K(ls);
+  cplx = false;
+  for (int s = 0; s < ls; s++) {
+    kb[s] = 1.0 / (2.0 * (bs[s] * (4.0 - m5) + 1.0));
+    kc[s] = 1.0 / (2.0 * (cs[s] * (4.0 - m5) - 1.0));
+    K[s] = kb[s] / kc[s];
+    cplx = cplx || bs[s].imag() != 0.0 || cs[s].imag() != 0.0;
+  }
+  b = bs[0].real();
+  c = cs[0].real();
+  kappa = kb[0].real();
+  kappa_c = kc[0].real();
   std::vector<cd> m0u, m0d, m1u, m1d, bu, bd;
   m5inv_columns(ls, K, mass, 0, m0u, m0d);
   m5inv_columns(ls, K, mass, 1, m1u, m1d);
-  bmix(ls, bv, cv, mass, bu, bd);
+  bmix(ls, bs, cs, mass, bu, bd);
   std::vector<cd> bdu = adjoint(ls, bu), bdd = adjoint(ls, bd);
   std::vector<cd> mkb(ls);
   for (int s = 0; s < ls; s++) mkb[s] = -std::conj(kb[s]);
@@ -211,23 +239,30 @@ Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_
   // S = M5inv^+ B^+ ; R = conj(kappa_b) S (-conj(kappa_b))
   std::vector<cd> Su = matmul(ls, m1u, bdu), Sd = matmul(ls, m1d, bdd);
   std::vector<cd> Ru = diag_right(ls, diag_left(ls, ckb, Su), mkb), Rd = diag_right(ls, diag_left(ls, ckb, Sd), mkb);
-  hM5i = pack(ls, m0u, m0d);
-  hM5id = pack(ls, m1u, m1d);
-  hB = pack(ls, bu, bd);
-  hBd = pack(ls, bdu, bdd);
-  upload(mixP, pack(ls, Pu, Pd));
-  upload(mixQ, pack(ls, Qu, Qd));
-  upload(mixR, pack(ls, Ru, Rd));
-  upload(mixS, pack(ls, Su, Sd));
-  upload(mixB, hB);
-  upload(mixBd, hBd);
-  upload(mixM5i, hM5i);
-  upload(mixM5id, hM5id);
   // M5 = 1 + K D5, what MatInv applies to the initial guess (the b/c mixing
   // form with b = 1, c = K)
   std::vector<cd> m5u, m5d;
   bmix(ls, std::vector<cd>(ls, 1.0), K, mass, m5u, m5d);
-  upload(mixM5, pack(ls, m5u, m5d));
+  // -kappa_b(s) on both chiralities (zmobius_m-sym2.h: the last step of MatPc)
+  std::vector<cd> kbm((size_t)ls * ls, 0.0);
+  for (int s = 0; s < ls; s++) kbm[(size_t)s * ls + s] = -kb[s];
+  auto packm = [&](const std::vector<cd> &up, const std::vector<cd> &dn) {
+    return cplx ? pack_complex(ls, up, dn) : pack(ls, up, dn);
+  };
+  hM5i = packm(m0u, m0d);
+  hM5id = packm(m1u, m1d);
+  hB = packm(bu, bd);
+  hBd = packm(bdu, bdd);
+  upload(mixP, packm(Pu, Pd));
+  upload(mixQ, packm(Qu, Qd));
+  upload(mixR, packm(Ru, Rd));
+  upload(mixS, packm(Su, Sd));
+  upload(mixB, hB);
+  upload(mixBd, hBd);
+  upload(mixM5i, hM5i);
+  upload(mixM5id, hM5id);
+  upload(mixM5, packm(m5u, m5d));
+  upload(mixKb, packm(kbm, kbm));
 }
 
 // ---------------------------------------------------------------- operators
@@ -293,10 +328,15 @@ void op_matpc(const Dirac &D, int prec, const SpinorView &out, const SpinorView 
     L.cb = 1;
     L.mix = D.mixQ.as<double>();
     launch_hop(D, L, w.t0.view(), w.t1.view(), none(), none(), none(), none(), none(), st);
-    L.ep = EP_AXPY;
     L.cb = 0;
-    L.mix = nullptr;
-    L.coef.assign(D.ls, -D.kappa);
+    if (D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
+      L.ep = EP_MIX_AXPY;
+      L.mix = D.mixKb.as<double>();
+    } else {
+      L.ep = EP_AXPY;
+      L.mix = nullptr;
+      L.coef.assign(D.ls, -D.kappa);
+    }
     L.norm = norm;
     L.red_op = red_op;
     launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);

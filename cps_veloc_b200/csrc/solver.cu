@@ -93,10 +93,15 @@ void CgSolver::emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_e
     Lh.coef.assign(D.ls, -D.kappa * D.kappa);
   }
   Lh.ep = EP_AXPY;
+  if (mob && D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
+    Lh.ep = EP_MIX_AXPY;
+    Lh.mix = D.mixKb.as<double>();
+  }
   Lh.cb = 0;
   Lh.norm = pap;
   Lh.red_op = RED_PAP;
   launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, none(), none(), none(), none(), stp);
+  Lh.mix = nullptr;
   // ---- M^dagger ----
   Lh.norm = 0;
   Lh.dag = 1;

@@ -297,6 +297,14 @@ class DiracOpMobius(_DiracOp):
     def Dslash(self, inp, cb, dag=0, prec=A.DOUBLE):
         raise NotImplementedError("Mobius: use Dslash4 (zmobius_dslash_4)")
 
+    def set_zmobius(self, b, c) -> None:
+        """complex per-slice b_s, c_s (DiracOpZMobius)"""
+        b = np.ascontiguousarray(np.asarray(b, dtype=np.complex128).view(np.float64))
+        c = np.ascontiguousarray(np.asarray(c, dtype=np.complex128).view(np.float64))
+        if b.size != 2 * self.ls or c.size != 2 * self.ls:
+            raise ValueError("b and c need Ls complex values")
+        check(lib().cpsgpu_dirac_set_zmobius(self._h, dptr(b), dptr(c)))
+
     def Dslash4(self, inp, cb: int, dag: int = 0, prec: int = A.DOUBLE) -> np.ndarray:
         inp = self._vec(inp)
         out = np.empty_like(inp)

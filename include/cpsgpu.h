@@ -137,6 +137,12 @@ typedef struct {
  * = 1/(2(m+4)) (Wilson), 1/(2(5-M5)) (DWF), kappa_b and kappa_c (Mobius). */
 int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *arg, cpsgpu_dirac *d);
 int cpsgpu_dirac_destroy(cpsgpu_dirac d);
+/* Complex per-slice Mobius coefficients (DiracOpZMobius, d_op_zmobius.C
+ * :246-292): b and c hold 2*Ls doubles each, (re, im) of b_s and c_s.
+ * kappa_b(s) = 1/(2(b_s(4 - M5) + 1)), kappa_c(s) = 1/(2(c_s(4 - M5) - 1)).
+ * Every operator and solver of the Mobius handle then uses them;
+ * cpsgpu_matinv stays real-only (it scales by the real kappa_b). */
+int cpsgpu_dirac_set_zmobius(cpsgpu_dirac d, const double *b, const double *c);
 int cpsgpu_dirac_info(cpsgpu_dirac d, double *kappa, double *kappa_c);
 
 /* Host-vector operators; vectors hold one preconditioned checkerboard in

@@ -140,6 +140,7 @@ def load_reference() -> C.CDLL:
             "ref_zmobius_dslash_4": [_dp, _dp, _dp, i, i, d],
             "ref_zmobius_m5inv": [_dp, d, i],
             "ref_zmobius_kappa_dslash_5_plus": [_dp, _dp, d, i],
+            "ref_set_zmobius": [_dp, _dp],
             "ref_zmobius_m": [_dp, _dp, _dp, d],
             "ref_zmobius_mdag": [_dp, _dp, _dp, d],
             "ref_zmobius_mdagm": [_dp, _dp, _dp, _dp, d],

@@ -81,6 +81,20 @@ int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
   return 0;
 }
 
+// Complex per-slice coefficients, set as DiracOpZMobius's reset_mobius_arg
+// does (d_op_zmobius.C:246-292, a5inv = 1); b and c hold (re, im) per slice.
+void ref_set_zmobius(const double *b, const double *c) {
+  Dwf *m = &g_dwf;
+  const double m5 = GJP.DwfHeight();
+  for (int s = 0; s < m->ls; s++) {
+    m->zmobius_b[s] = Complex(b[2 * s], b[2 * s + 1]);
+    m->zmobius_c[s] = Complex(c[2 * s], c[2 * s + 1]);
+    m->zmobius_kappa_b[s] = 1.0 / (2. * (m->zmobius_b[s] * (4 - m5) + 1.0));
+    m->zmobius_kappa_c[s] = 1.0 / (2. * (m->zmobius_c[s] * (4 - m5) - 1.0));
+    m->zmobius_kappa_ratio[s] = m->zmobius_kappa_b[s] / m->zmobius_kappa_c[s];
+  }
+}
+
 double ref_dwf_kappa(void) { return g_dwf.dwf_kappa; }
 double ref_mobius_kappa_b(void) { return g_dwf.mobius_kappa_b; }
 double ref_mobius_kappa_c(void) { return g_dwf.mobius_kappa_c; }

@@ -33,6 +33,16 @@ class OracleOps:
             O.orc_mobius_params(C.byref(self.mp), ls, b, c, m5)
         self.n = 24 * ls * vh_of(L)
 
+    def set_zmobius(self, b, c):
+        """complex per-slice b_s, c_s with kappa_b, K as DiracOpZMobius sets them
+        (d_op_zmobius.C:246-292, a5inv = 1)"""
+        for s in range(self.ls):
+            kb = 1 / (2 * (b[s] * (4 - self.m5) + 1))
+            kc = 1 / (2 * (c[s] * (4 - self.m5) - 1))
+            for name, v in (("b", b[s]), ("c", c[s]), ("kappa_b", kb), ("K", kb / kc)):
+                arr = getattr(self.mp, name)
+                arr[2 * s], arr[2 * s + 1] = complex(v).real, complex(v).imag
+
     def z(self):
         return np.zeros(self.n)
 

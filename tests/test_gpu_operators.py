@@ -135,3 +135,26 @@ def test_reductions_are_deterministic(oracle):
     outs = [D.MatPcDagMatPc(psi) for _ in range(3)]
     for y, d in outs[1:]:
         assert d == outs[0][1] and np.array_equal(y, outs[0][0])
+
+
+@pytest.mark.parametrize("L,ls,mass", [((4, 4, 4, 8), 8, 0.01), ((4, 2, 4, 4), 5, 0.1)])
+def test_zmobius_operators(oracle, L, ls, mass):
+    """Complex per-slice b_s, c_s (DiracOpZMobius) in every precision"""
+    u = gen_gauge(L, seed=53)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    b = np.array([1.5 + 0.25j * np.sin(1.0 + s) for s in range(ls)])
+    c = b - 1.0
+    ops.set_zmobius(b, c)
+    lat = _lat(L, u)
+    D = DiracOpMobius(lat, mass=mass, ls=ls, m5=1.8, b=1.5, c=0.5)
+    D.set_zmobius(b, c)
+    psi = gen_gaussian(ops.n, seed=54)
+    for prec in PRECS:
+        for dag in (0, 1):
+            assert rel(D.M5inv(psi, dag, prec), ops.mobius_m5inv(psi, mass, dag)) < TOL[prec]
+            for cb in (0, 1):
+                assert rel(D.Dslash4(psi, cb, dag, prec), ops.mobius_dslash_4(psi, mass, cb, dag)) < TOL[prec]
+            assert rel((D.MatPcDag if dag else D.MatPc)(psi, prec), ops.mobius_m(psi, mass, dag)) < TOL[prec]
+        y, d = D.MatPcDagMatPc(psi, prec)
+        yo, do = ops.mobius_mdagm(psi, mass)
+        assert rel(y, yo) < TOL[prec] and abs(d / do - 1) < TOL[prec]

@@ -197,3 +197,24 @@ def test_dwf_propagator_flow_from_canonical_fields(oracle):
     prop = five2four(L, ls, x, ls - 1, 0)
     fconvert(L, ls, xo, StrOrd.CANONICAL, StrOrd.WILSON)
     assert rel(prop, five2four(L, ls, xo, ls - 1, 0)) < 1e-9
+
+
+@pytest.mark.parametrize("prec", [A.DOUBLE, A.SINGLE])
+def test_zmobius_cg_true_residual(oracle, prec):
+    L, ls, mass = (4, 4, 4, 4), 8, 0.05
+    u = gen_gauge(L, seed=151)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    zb = np.array([1.5 + 0.25j * np.sin(1.0 + s) for s in range(ls)])
+    D.set_zmobius(zb, zb - 1.0)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    ops.set_zmobius(zb, zb - 1.0)
+    b = gen_gaussian(ops.n, seed=152)
+    xo, _, _ = ops.invcg("mobius", b, mass=mass, stop_rsd=1e-11)
+    x = np.zeros(ops.n)
+    r = D.InvCg(x, b, stop_rsd=1e-10, precision=prec)
+    assert r.status == A.CONVERGED and r.true_res <= 1e-10
+    assert rel(x, xo) < 1e-8
+    with pytest.raises(A.CpsGpuError):  # MatInv stays real-only, as the reference's scaling is
+        D.MatInv(np.zeros(2 * D.f_size), gen_gaussian(2 * D.f_size, seed=153))

@@ -98,3 +98,40 @@ def test_mobius_vs_reference(oracle, reference, L, ls, mass, b, c):
     reference.ref_zmobius_mdagm(p(y), p(us), p(psi), C.byref(d), mass)
     yo, do = ops.mobius_mdagm(psi, mass)
     assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
+
+
+def zmobius_coefficients(ls):
+    """complex b_s, c_s (b_s - c_s = 1) of the kind zMobius approximations use"""
+    b = np.array([1.5 + 0.25j * np.sin(1.0 + s) for s in range(ls)])
+    return b, b - 1.0
+
+
+@pytest.mark.parametrize("L,ls,mass", [((4, 4, 2, 4), 6, 0.05), ((2, 2, 4, 4), 5, 0.1)])
+def test_zmobius_vs_reference(oracle, reference, L, ls, mass):
+    """Complex per-slice coefficients (DiracOpZMobius) through the same kernels"""
+    bc = (1, 1, 1, -1)
+    _ref_setup(reference, L, ls, bc, b=1.5, c=0.5)
+    zb, zc = zmobius_coefficients(ls)
+    reference.ref_set_zmobius(p(np.ascontiguousarray(zb.view(np.float64))), p(np.ascontiguousarray(zc.view(np.float64))))
+    u = gen_gauge(L, seed=19)
+    us = apply_bc_signs(u, L, bc)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc)
+    ops.set_zmobius(zb, zc)
+    psi = gen_gaussian(24 * ls * vh_of(L), seed=18)
+    for dag in (0, 1):
+        y = psi.copy()
+        reference.ref_zmobius_m5inv(p(y), mass, dag)
+        assert rel(ops.mobius_m5inv(psi, mass, dag), y) < TOL
+        for cb in (0, 1):
+            y = np.zeros_like(psi)
+            reference.ref_zmobius_dslash_4(p(y), p(us), p(psi), cb, dag, mass)
+            assert rel(ops.mobius_dslash_4(psi, mass, cb, dag), y) < TOL
+    for dag, fn in ((0, reference.ref_zmobius_m), (1, reference.ref_zmobius_mdag)):
+        y = np.zeros_like(psi)
+        fn(p(y), p(us), p(psi), mass)
+        assert rel(ops.mobius_m(psi, mass, dag), y) < TOL
+    y = np.zeros_like(psi)
+    d = C.c_double()
+    reference.ref_zmobius_mdagm(p(y), p(us), p(psi), C.byref(d), mass)
+    yo, do = ops.mobius_mdagm(psi, mass)
+    assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
