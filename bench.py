@@ -53,6 +53,12 @@ STOP = 1e-10
 # uses it, to turn its per-iteration CPU time into a time to solution without
 # running the multi-hour CPU solve.
 FP64_CG_ITERS = 196
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the dslash timed below on this workload, from single-launch ncu captures
+# (hop_kernel store epilogue, cold L2), keyed by (precision, stored link form).
+# The algorithmic bytes are 226.5 MB (FP32, 12-real links), 239.0 MB (FP32,
+# 18), 127.9 MB (FP16, 18).
+DSLASH_TRAFFIC = {(1, 12): 132.54e6 + 76.52e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.54e6}
 
 
 def peaks() -> dict:
@@ -448,6 +454,8 @@ def main(argv=None) -> int:
         dsl[name] = {"ms": m2.value, "GB_s": gbs, "frac_of_measured_hbm": gbs / pk["hbm_gbs"],
                      "GFLOP_s": (1320 + 48) * L4[0] * L4[1] * L4[2] * L4[3] // 2 * LS / (m2.value * 1e-3) / 1e9}
     achieved = by.value / (ms.value * 1e-3) / 1e9
+    form = lat.link_reals(sloppy)
+    traffic = DSLASH_TRAFFIC.get((sloppy, form))
 
     # end to end through the host-pointer C ABI: H2D source + guess, D2H solution
     pin_b = C.c_void_p()
@@ -507,8 +515,10 @@ def main(argv=None) -> int:
                 "true_res": ro[0].true_res, "speedup_vs_fp64_cg": t_fp64 / t_other},
             "dslash": dsl,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "traffic": None,
-                         "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32"),
+                         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "algorithmic_bytes": by.value, "traffic_unit": "bytes per launch (ncu, single launch)",
+                         "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32")
+                         + f", {form}-real links",
                          "peak_source": pk["source"]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
             "cpsgpu_gauge_info": (C.c_int, [vp, _dp, C.POINTER(C.c_int)]),
             "cpsgpu_synchronize": (C.c_int, [vp]),
             "cpsgpu_set_link_reals": (C.c_int, [vp, C.c_int, C.c_int]),
+            "cpsgpu_get_link_reals": (C.c_int, [vp, C.c_int, _ip]),
             "cpsgpu_get_rhs_tile": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
             "cpsgpu_set_rhs_tile": (C.c_int, [vp, C.c_int, C.c_int]),
             "cpsgpu_dirac_create": (C.c_int, [vp, C.POINTER(DiracArg), C.POINTER(vp)]),
@@ -85,6 +86,8 @@ def lib() -> C.CDLL:
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_bicgstab": (C.c_int, [vp, _dp, _dp, C.c_double, C.c_int, C.POINTER(CgArg), C.POINTER(C.c_int),
+                                          _dp]),
             "cpsgpu_fconvert": (C.c_int, [_ip, C.c_int, _dp, C.c_int, C.c_int]),
             "cpsgpu_gconvert": (C.c_int, [_ip, _dp, C.c_int, C.c_int]),
             "cpsgpu_four2five": (C.c_int, [_ip, C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int]),

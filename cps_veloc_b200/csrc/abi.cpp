@@ -20,6 +20,8 @@ double time_dslash(Dirac &D, int prec, int cb, int dag, int reps, double *bytes)
 double time_mdagm(Dirac &D, int prec, int reps, double *bytes);
 double time_m5inv(Dirac &D, int prec, int reps, double *bytes);
 double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
+int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, double stop_rsd, int max_num_iter,
+             double *true_res);
 void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
 void gconvert(const int node_sites[4], double *u, int to, int from);
 void four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
@@ -212,6 +214,15 @@ int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals) {
     if (reals != 12 && reals != 18 && !(f32 && prec == CPSGPU_HALF))
       throw Error(CPSGPU_ERR_ARG, "reals must be 12 or 18 (or FP32 links for the FP16 operator)");
     lat->L->sloppy_recon[prec] = reals;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_get_link_reals(cpsgpu_lattice lat, int prec, int *reals) {
+  return guarded([&] {
+    if (!lat || !reals) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (prec != CPSGPU_SINGLE && prec != CPSGPU_HALF) throw Error(CPSGPU_ERR_ARG, "FP32 or FP16 only");
+    *reals = lat->L->sloppy_recon[prec];
     return CPSGPU_OK;
   });
 }
@@ -499,6 +510,27 @@ int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg
       download(L, fo, &out_other, 1);
     }
     to_result(r[0], res);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_bicgstab(cpsgpu_dirac d, double *psi, const double *chi, double chi_norm, int n, const cpsgpu_cg_arg *arg,
+                    int *iterations, double *true_res) {
+  return guarded([&] {
+    if (!d || !psi || !chi || !arg) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (n < 1 || n > 10) throw Error(CPSGPU_ERR_ARG, "BiCGstab(n): n in [1, 10] (bicgstab.C:67-70)");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    Field fp(PREC_DOUBLE, L.vh, D.ls, 1), fc(PREC_DOUBLE, L.vh, D.ls, 1);
+    const double *pp = psi;
+    upload(L, fp, &pp, 1);
+    upload(L, fc, &chi, 1);
+    double tr = 0.0;
+    const int k = bicgstab(D, fp, fc, chi_norm, n, arg->stop_rsd, arg->max_num_iter, &tr);
+    download(L, fp, &psi, 1);
+    if (iterations) *iterations = k;
+    if (true_res) *true_res = tr;
     return CPSGPU_OK;
   });
 }

@@ -102,6 +102,16 @@ class Lattice:
         check(lib().cpsgpu_gauge_info(self._h, C.byref(e), C.byref(r)))
         return e.value, bool(r.value)
 
+    def set_link_reals(self, prec: int, reals: int) -> None:
+        """stored link form of the FP32/FP16 operators: 12 or 18 reals, or
+        LINKS_F32_12 / LINKS_F32_18 (FP32 links for the FP16 operator)"""
+        check(lib().cpsgpu_set_link_reals(self._h, prec, reals))
+
+    def link_reals(self, prec: int) -> int:
+        r = C.c_int()
+        check(lib().cpsgpu_get_link_reals(self._h, prec, C.byref(r)))
+        return r.value
+
     def synchronize(self):
         check(lib().cpsgpu_synchronize(self._h))
 
@@ -219,6 +229,19 @@ class _DiracOp:
         r = A.CgResult()
         check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
+
+    def BiCGstab(self, psi, chi, n=1, chi_norm=0.0, stop_rsd=1e-8, max_num_iter=10000):
+        """DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res) on MatPc:
+        psi (initial guess) updated in place; returns (k, true_res) as the
+        reference does (true_res absolute, 0 unless converged)"""
+        chi = self._vec(chi)
+        if not (isinstance(psi, np.ndarray) and psi.dtype == np.float64 and psi.flags.c_contiguous):
+            raise TypeError("psi must be a C-contiguous float64 array (updated in place)")
+        self._vec(psi)
+        a = self._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, A.DOUBLE, 0.0, 8, True)
+        k, tr = C.c_int(), C.c_double()
+        check(lib().cpsgpu_bicgstab(self._h, dptr(psi), dptr(chi), chi_norm, n, C.byref(a), C.byref(k), C.byref(tr)))
+        return k.value, tr.value
 
     def InvCgMulti(self, sols, srcs, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.0,
                    chunk=8, use_graph=True):

@@ -99,6 +99,7 @@ int cpsgpu_synchronize(cpsgpu_lattice lat);
 #define CPSGPU_LINKS_F32_12 112
 #define CPSGPU_LINKS_F32_18 118
 int cpsgpu_set_link_reals(cpsgpu_lattice lat, int prec, int reals);
+int cpsgpu_get_link_reals(cpsgpu_lattice lat, int prec, int *reals);
 
 /* ---- storage orders on the host (no device work) ----
  * StrOrdType values (enum_int.h:87-97).  Fields hold both checkerboards.
@@ -214,6 +215,15 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
  * InvCg over the same set. res has nrhs entries. */
 int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
                        const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res)
+ * (bicgstab.C:35-229): BiCGstab(n) on MatPc itself (not the normal
+ * equations), psi the initial guess, stop |r|^2 < stop_rsd^2 chi_norm with
+ * arg->stop_rsd and arg->max_num_iter (chi_norm 0: computed).  *iterations
+ * is the reference's k; *true_res = |r| (absolute, as the reference reports
+ * it; 0 when not converged).  FP64 on the device; the solver's complex
+ * scalars are host recurrences. */
+int cpsgpu_bicgstab(cpsgpu_dirac d, double *psi, const double *chi, double chi_norm, int n, const cpsgpu_cg_arg *arg,
+                    int *iterations, double *true_res);
 /* DiracOp*::MatInv(out, in, true_res) with the CG inverter
  * (d_op_wilson.C:257-334, d_op_dwf.C:316-492, d_op_mobius.C:407-700, SYM2):
  * the solve on both checkerboards.  in and out hold 2 * 24*Ls*Vh reals in

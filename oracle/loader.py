@@ -43,6 +43,7 @@ class OracleMobius(C.Structure):
 
 
 MDAGM_FN = C.CFUNCTYPE(None, C.c_void_p, _dp, _dp, _dp)
+MATPC_FN = C.CFUNCTYPE(None, C.c_void_p, _dp, _dp)
 
 
 def _make(target: str) -> None:
@@ -109,6 +110,8 @@ def load_oracle() -> C.CDLL:
         L.orc_wilson_matinv.argtypes = [g, _dp, _dp, _dp, d, d, i, _dp]
         L.orc_dwf_matinv.argtypes = [g, _dp, _dp, _dp, d, d, d, i, _dp]
         L.orc_mobius_matinv.argtypes = [g, m, _dp, _dp, _dp, d, d, i, _dp]
+        L.orc_bicgstab.argtypes = [MATPC_FN, C.c_void_p, C.c_long, _dp, _dp, d, i, d, i, _dp]
+        L.orc_bicgstab.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

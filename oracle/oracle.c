@@ -687,3 +687,100 @@ int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, cons
   free(b);
   return iter;
 }
+
+/* ---------------------------------------------------------------------- */
+/* BiCGstab(n): DiracOpWilsonTypes::BiCGstab, bicgstab.C:35-229             */
+/* ---------------------------------------------------------------------- */
+/* <a, b> = sum conj(a) b (compDotProduct, vector_util.C:889-903) */
+static cplx cdot(const double *a, const double *b, long n) {
+  double re = 0, im = 0;
+  for (long k = 0; k < n; k += 2) {
+    re += a[k] * b[k] + a[k + 1] * b[k + 1];
+    im += a[k] * b[k + 1] - a[k + 1] * b[k];
+  }
+  return re + I * im;
+}
+/* a = f c + d (cTimesV1PlusV2, vector_util.C:912-922) */
+static void caxpy(double *a, cplx f, const double *c, const double *d, long n) {
+  const double re = creal(f), im = cimag(f);
+  for (long k = 0; k < n; k += 2) {
+    const double cr = c[k], ci = c[k + 1];
+    a[k] = re * cr - im * ci + d[k];
+    a[k + 1] = re * ci + im * cr + d[k + 1];
+  }
+}
+
+int orc_bicgstab(orc_matpc_fn matpc, void *ctx, long f_size, double *psi, const double *chi, double chi_norm,
+                 int nn, double stop_rsd, int max_num_iter, double *true_res) {
+  enum { NMAX = 10 };
+  if (nn <= 0 || nn > NMAX) return -1;
+  double *r[NMAX + 1], *u[NMAX + 1];
+  for (int i = 0; i <= nn; i++) {
+    r[i] = calloc(f_size, sizeof(double));
+    u[i] = calloc(f_size, sizeof(double));
+  }
+  double *r0 = calloc(f_size, sizeof(double));
+  cplx rho0 = 1.0, rho1, alpha = 0.0, omega = 1.0, beta;
+  double sigma[NMAX + 1];
+  cplx gamma[NMAX + 1], gamma_p[NMAX + 1], gamma_pp[NMAX + 1], tau[NMAX + 1][NMAX + 1];
+  int converged = 0, k;
+  if (chi_norm == 0.0) chi_norm = norm2(chi, f_size);
+  if (chi_norm == 0.0) {
+    memset(psi, 0, sizeof(double) * f_size);
+    for (int i = 0; i <= nn; i++) { free(r[i]); free(u[i]); }
+    free(r0);
+    return 0;
+  }
+  const double rsd_sq = chi_norm * stop_rsd * stop_rsd;
+  matpc(ctx, r[0], psi);
+  for (long q = 0; q < f_size; q++) r[0][q] = chi[q] - r[0][q];
+  sigma[0] = norm2(r[0], f_size);
+  memcpy(r0, r[0], sizeof(double) * f_size);
+  memset(u[0], 0, sizeof(double) * f_size);
+  for (k = 1; k <= max_num_iter && !converged; k += nn) {
+    rho0 *= -omega;
+    for (int j = 0; j < nn; j++) { /* BiCG part */
+      rho1 = cdot(r0, r[j], f_size);
+      beta = alpha * rho1 / rho0;
+      rho0 = rho1;
+      for (int i = 0; i <= j; i++) caxpy(u[i], -beta, u[i], r[i], f_size);
+      matpc(ctx, u[j + 1], u[j]);
+      alpha = rho0 / cdot(r0, u[j + 1], f_size);
+      for (int i = 0; i <= j; i++) caxpy(r[i], -alpha, u[i + 1], r[i], f_size);
+      matpc(ctx, r[j + 1], r[j]);
+      caxpy(psi, alpha, u[0], psi, f_size);
+    }
+    for (int j = 1; j <= nn; j++) { /* MR part */
+      for (int i = 1; i < j; i++) {
+        tau[i][j] = cdot(r[i], r[j], f_size) / sigma[i];
+        caxpy(r[j], -tau[i][j], r[i], r[j], f_size);
+      }
+      sigma[j] = norm2(r[j], f_size);
+      gamma_p[j] = cdot(r[j], r[0], f_size) / sigma[j];
+    }
+    gamma[nn] = gamma_p[nn];
+    omega = gamma[nn];
+    for (int j = nn - 1; j > 0; j--) {
+      gamma[j] = gamma_p[j];
+      for (int i = j + 1; i <= nn; i++) gamma[j] -= tau[j][i] * gamma[i];
+    }
+    for (int j = 1; j < nn; j++) {
+      gamma_pp[j] = gamma[j + 1];
+      for (int i = j + 1; i < nn; i++) gamma_pp[j] += tau[j][i] * gamma[i + 1];
+    }
+    caxpy(u[0], -gamma[nn], u[nn], u[0], f_size);
+    caxpy(psi, gamma[1], r[0], psi, f_size);
+    caxpy(r[0], -gamma_p[nn], r[nn], r[0], f_size);
+    for (int j = 1; j < nn; j++) {
+      caxpy(u[0], -gamma[j], u[j], u[0], f_size);
+      caxpy(psi, gamma_pp[j], r[j], psi, f_size);
+      caxpy(r[0], -gamma_p[j], r[j], r[0], f_size);
+    }
+    sigma[0] = norm2(r[0], f_size);
+    if (sigma[0] < rsd_sq) converged = 1;
+  }
+  if (converged && true_res) *true_res = sqrt(sigma[0]);
+  for (int i = 0; i <= nn; i++) { free(r[i]); free(u[i]); }
+  free(r0);
+  return k;
+}

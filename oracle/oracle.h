@@ -94,6 +94,15 @@ int orc_minvcg(orc_mdagm_fn op, void *ctx, long n, double **psi,
                int nshift, double *rsdcg, int type, const double *alpha,
                int max_num_iter);
 
+/* BiCGstab(n) on MatPc (not the normal equations): DiracOpWilsonTypes::
+ * BiCGstab, bicgstab.C:35-229, step for step (complex dot products
+ * <a, b> = sum conj(a) b).  Returns the reference's k (the loop counter after
+ * the loop); *true_res = |r| (absolute, as the reference reports it), set
+ * only when converged.  matpc(ctx, out, in): out = MatPc in. */
+typedef void (*orc_matpc_fn)(void *ctx, double *out, const double *in);
+int orc_bicgstab(orc_matpc_fn matpc, void *ctx, long f_size, double *psi, const double *chi, double chi_norm,
+                 int n, double stop_rsd, int max_num_iter, double *true_res);
+
 /* Full-lattice solves, DiracOp*::MatInv with the CG inverter.  in and out
  * hold both checkerboards, half = 24*ls*Vh reals each: Wilson and DWF put
  * the odd checkerboard (the one the CG solves on) first, Mobius the even

@@ -5,7 +5,7 @@ import ctypes as C
 
 import numpy as np
 
-from oracle.loader import MDAGM_FN, OracleGeom, OracleMobius, p
+from oracle.loader import MATPC_FN, MDAGM_FN, OracleGeom, OracleMobius, p
 
 
 def rel(a, b) -> float:
@@ -142,6 +142,25 @@ class OracleOps:
         it = self.O.orc_invcg(fn, None, self.n, p(sol), p(src), 0.0, stop_rsd, max_num_iter, C.byref(tr),
                               C.byref(sh) if sh is not None else None)
         return sol, it, tr.value
+
+    def bicgstab(self, kind, chi, n=1, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, psi0=None):
+        """BiCGstab(n) on MatPc (bicgstab.C:35-229): returns psi, k, true_res"""
+        O, u = self.O, self.u
+
+        def fn(ctx, out, inp):
+            if kind == "wilson":
+                O.orc_wilson_m(C.byref(self.g1), out, p(u), inp, kappa, 0)
+            elif kind == "dwf":
+                O.orc_dwf_m(C.byref(self.g), out, p(u), inp, mass, self.m5, 0)
+            else:
+                O.orc_mobius_m(C.byref(self.g), C.byref(self.mp), out, p(u), inp, mass, 0)
+
+        cb = MATPC_FN(fn)
+        psi = np.zeros(self.n) if psi0 is None else np.ascontiguousarray(psi0).copy()
+        tr = C.c_double()
+        k = self.O.orc_bicgstab(cb, None, self.n, p(psi), p(np.ascontiguousarray(chi)), 0.0, n, stop_rsd,
+                                max_num_iter, C.byref(tr))
+        return psi, k, tr.value
 
     def minvcg(self, kind, chi, shifts, rsd, mass=0.0, kappa=0.0, type=1, alpha=None, max_num_iter=10000,
                psi0=None):

@@ -218,3 +218,61 @@ def test_zmobius_cg_true_residual(oracle, prec):
     assert rel(x, xo) < 1e-8
     with pytest.raises(A.CpsGpuError):  # MatInv stays real-only, as the reference's scaling is
         D.MatInv(np.zeros(2 * D.f_size), gen_gaussian(2 * D.f_size, seed=153))
+
+
+@pytest.mark.parametrize("kind,L,ls,n,iters", [
+    ("wilson", (4, 4, 4, 8), 1, 1, None), ("wilson", (4, 4, 4, 8), 1, 3, None), ("dwf", (4, 4, 4, 4), 4, 3, None),
+    ("dwf", (4, 4, 4, 8), 8, 1, 6), ("mobius", (4, 4, 4, 4), 8, 2, 6), ("zmobius", (4, 4, 4, 4), 8, 1, 6)])
+def test_bicgstab_matches_oracle(oracle, kind, L, ls, n, iters):
+    """DiracOpWilsonTypes::BiCGstab(n) (bicgstab.C:35-229) on MatPc against the
+    oracle's restatement.  Converging cases: the same k (to one sweep), the
+    same solution and a true residual below stop_rsd.  On the 5D operators at
+    these sizes BiCGstab(n) does not converge (in the oracle alike) and its
+    iterates are chaotic: in the oracle itself a 1e-15 relative change of chi
+    grows to 1e-10 by iteration 8 and to O(1) by iteration 16.  Those cases
+    stop after max_num_iter = 6 and compare the iterate itself."""
+    mass = 0.1
+    u = gen_gauge(L, seed=161)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    ops = OracleOps(oracle, L, u, ls=ls, b=1.5, c=0.5)
+    if kind == "wilson":
+        D = DiracOpWilson(lat, mass=mass)
+    elif kind == "dwf":
+        D = DiracOpDwf(lat, mass=mass, ls=ls)
+    else:
+        D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+        if kind == "zmobius":
+            zb = np.array([1.5 + 0.25j * np.cos(0.5 + s) for s in range(ls)])
+            D.set_zmobius(zb, zb - 1.0)
+            ops.set_zmobius(zb, zb - 1.0)
+    chi = gen_gaussian(D.f_size, seed=162)
+    guess = gen_gaussian(D.f_size, seed=163) * 1e-3 if kind == "wilson" else np.zeros(D.f_size)
+    okind = "mobius" if kind == "zmobius" else kind
+    mx = iters if iters else 2000
+    xo, ko, tro = ops.bicgstab(okind, chi, n=n, mass=mass, kappa=D.kappa, stop_rsd=1e-12, psi0=guess,
+                               max_num_iter=mx)
+    x = guess.copy()
+    k, tr = D.BiCGstab(x, chi, n=n, stop_rsd=1e-12, max_num_iter=mx)
+    if iters:
+        assert k == ko == 1 + n * ((iters + n - 1) // n) and tr == tro == 0.0
+        assert rel(x, xo) < 1e-9
+        return
+    assert 1 < ko < mx and abs(k - ko) <= n
+    assert 0 < tr < 1e-12 * np.linalg.norm(chi)
+    assert rel(x, xo) < 1e-9
+    r = chi - D.MatPc(x)
+    assert np.linalg.norm(r) < 2e-12 * np.linalg.norm(chi)
+
+
+def test_bicgstab_zero_source_and_argument_checks(oracle):
+    lat = Lattice((4, 4, 4, 4))
+    lat.import_gauge(gen_gauge((4, 4, 4, 4), seed=164))
+    D = DiracOpWilson(lat, mass=0.1)
+    x = np.ones(D.f_size)
+    k, tr = D.BiCGstab(x, np.zeros(D.f_size), n=2)
+    assert k == 0 and tr == 0.0 and not x.any()
+    with pytest.raises(A.CpsGpuError):
+        D.BiCGstab(x, np.ones(D.f_size), n=11)  # n_max = 10 (bicgstab.C:67-70)
+    k, tr = D.BiCGstab(x, gen_gaussian(D.f_size, seed=165), n=2, stop_rsd=1e-14, max_num_iter=4)
+    assert k == 5 and tr == 0.0

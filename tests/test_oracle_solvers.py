@@ -118,3 +118,38 @@ def test_mobius_matinv_converges(oracle):
     b = gen_gaussian(2 * ops.n, seed=36)
     x, it, tr = ops.matinv("mobius", b, mass=0.05, stop_rsd=1e-12)
     assert tr < 1e-11 and it > 2 and np.all(np.isfinite(x))
+
+
+@pytest.mark.parametrize("n", [1, 2, 4])
+@pytest.mark.parametrize("kind", ["wilson", "dwf", "mobius"])
+def test_bicgstab_solves_matpc(oracle, kind, n):
+    """DiracOpWilsonTypes::BiCGstab (bicgstab.C:35-229) on MatPc itself: the
+    reported |r| is the true residual of the returned psi, below stop_rsd |chi|,
+    and k advances in steps of n from 1."""
+    L = (4, 4, 2, 4)
+    ls = 1 if kind == "wilson" else 4
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=41), ls=ls)
+    chi = gen_gaussian(ops.n, seed=42 + n)
+    stop = 1e-10
+    psi, k, tr = ops.bicgstab(kind, chi, n=n, mass=0.1, kappa=0.12, stop_rsd=stop)
+    if kind == "wilson":
+        r = chi - ops.wilson_m(psi, 0.12, 0)
+    elif kind == "dwf":
+        r = chi - ops.dwf_m(psi, 0.1, 0)
+    else:
+        r = chi - ops.mobius_m(psi, 0.1, 0)
+    nc = np.linalg.norm(chi)
+    assert (k - 1) % n == 0 and k > 1
+    assert 0 < tr < stop * nc
+    # the recursed residual tracks the true one to rounding
+    assert abs(np.linalg.norm(r) - tr) < 1e-3 * tr + 1e-13 * nc
+
+
+def test_bicgstab_zero_source_and_no_convergence(oracle):
+    L = (4, 4, 2, 4)
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=43), ls=1)
+    psi, k, tr = ops.bicgstab("wilson", np.zeros(ops.n), psi0=np.ones(ops.n), kappa=0.12)
+    assert k == 0 and not psi.any() and tr == 0.0
+    chi = gen_gaussian(ops.n, seed=44)
+    psi, k, tr = ops.bicgstab("wilson", chi, n=2, kappa=0.12, stop_rsd=1e-14, max_num_iter=4)
+    assert k == 5 and tr == 0.0  # two sweeps of n = 2, true_res untouched
