@@ -34,6 +34,11 @@ class DiracArg(C.Structure):
                 ("mobius_b", C.c_double), ("mobius_c", C.c_double)]
 
 
+class ForceArg(C.Structure):
+    """cpsgpu_force_arg: the reference's ForceArg (L1, L2, Linf)"""
+    _fields_ = [("L1", C.c_double), ("L2", C.c_double), ("Linf", C.c_double)]
+
+
 class CgArg(C.Structure):
     _fields_ = [("stop_rsd", C.c_double), ("max_num_iter", C.c_int), ("src_norm_sq", C.c_double),
                 ("shift", C.c_double), ("precision", C.c_int), ("delta", C.c_double), ("chunk", C.c_int),
@@ -86,6 +91,9 @@ def lib() -> C.CDLL:
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_calc_hmd_force_vecs": (C.c_int, [vp, _dp, _dp, _dp]),
+            "cpsgpu_evolve_mom_fforce": (C.c_int, [vp, _dp, _dp, C.c_double, C.POINTER(ForceArg)]),
+            "cpsgpu_time_fforce": (C.c_int, [vp, C.c_int, _dp, _dp, _dp]),
             "cpsgpu_bicgstab": (C.c_int, [vp, _dp, _dp, C.c_double, C.c_int, C.POINTER(CgArg), C.POINTER(C.c_int),
                                           _dp]),
             "cpsgpu_fconvert": (C.c_int, [_ip, C.c_int, _dp, C.c_int, C.c_int]),

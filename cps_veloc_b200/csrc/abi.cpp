@@ -43,6 +43,9 @@ struct cpsgpu_dirac_s {
   Field in[3], out[3];
   OpWork w[3];
   std::unique_ptr<CgSolver> solvers[3];
+  // HMC force workspace: CalcHmdForceVecs' fields and the momentum field
+  std::unique_ptr<ForceVecs> fv;
+  DeviceBuffer mom;
 };
 
 struct cpsgpu_field_s {
@@ -510,6 +513,99 @@ int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg
       download(L, fo, &out_other, 1);
     }
     to_result(r[0], res);
+    return CPSGPU_OK;
+  });
+}
+
+namespace {
+ForceVecs &force_vecs(cpsgpu_dirac d, const double *chi) {
+  Dirac &D = *d->D;
+  Lattice &L = *D.lat;
+  if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+  if (!d->fv) d->fv.reset(new ForceVecs());
+  ensure_field(d->in[PREC_DOUBLE], PREC_DOUBLE, L.vh, D.ls, 1);
+  upload(L, d->in[PREC_DOUBLE], &chi, 1);
+  calc_hmd_force_vecs(D, *d->fv, d->in[PREC_DOUBLE].view());
+  return *d->fv;
+}
+}  // namespace
+
+int cpsgpu_calc_hmd_force_vecs(cpsgpu_dirac d, double *f_out, double *f_in, const double *chi) {
+  return guarded([&] {
+    if (!d || !f_out || !f_in || !chi) throw Error(CPSGPU_ERR_ARG, "null argument");
+    need_gauge(d);
+    ForceVecs &fv = force_vecs(d, chi);
+    Lattice &L = *d->D->lat;
+    const size_t half = (size_t)24 * L.vh * d->D->ls;
+    double *o1 = f_out, *e1 = f_out + half, *o2 = f_in, *e2 = f_in + half;
+    download(L, fv.v1o, &o1, 1);
+    download(L, fv.v1e, &e1, 1);
+    download(L, fv.v2o, &o2, 1);
+    download(L, fv.v2e, &e2, 1);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *chi, double dt, cpsgpu_force_arg *out) {
+  return guarded([&] {
+    if (!d || !mom || !chi) throw Error(CPSGPU_ERR_ARG, "null argument");
+    need_gauge(d);
+    ForceVecs &fv = force_vecs(d, chi);
+    Lattice &L = *d->D->lat;
+    const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
+    d->mom.ensure(bytes);
+    CPSGPU_CUDA(cudaMemcpyAsync(d->mom.ptr, mom, bytes, cudaMemcpyHostToDevice, L.stream));
+    double f[3];
+    fforce_update(*d->D, fv, d->mom.as<double>(), dt, f);
+    CPSGPU_CUDA(cudaMemcpyAsync(mom, d->mom.ptr, bytes, cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    if (out) {
+      out->L1 = f[0];
+      out->L2 = f[1];
+      out->Linf = f[2];
+    }
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes) {
+  return guarded([&] {
+    if (!d || reps < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+    if (!d->fv) d->fv.reset(new ForceVecs());
+    Field chi(PREC_DOUBLE, L.vh, D.ls, 1);
+    std::vector<double> h((size_t)24 * L.vh * D.ls);
+    gen_gaussian(h.data(), (long)h.size(), 20261203ull, 9);
+    const double *hp = h.data();
+    upload(L, chi, &hp, 1);
+    const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
+    d->mom.ensure(bytes);
+    CPSGPU_CUDA(cudaMemsetAsync(d->mom.ptr, 0, bytes, L.stream));
+    cudaEvent_t e[3];
+    for (auto &x : e) CPSGPU_CUDA(cudaEventCreate(&x));
+    float t_all = 0.f, t_k = 0.f;
+    for (int k = 0; k < reps + 2; k++) {
+      CPSGPU_CUDA(cudaEventRecord(e[0], L.stream));
+      calc_hmd_force_vecs(D, *d->fv, chi.view());
+      CPSGPU_CUDA(cudaEventRecord(e[1], L.stream));
+      fforce_update(D, *d->fv, d->mom.as<double>(), 0.01, nullptr);
+      CPSGPU_CUDA(cudaEventRecord(e[2], L.stream));
+      CPSGPU_CUDA(cudaEventSynchronize(e[2]));
+      float a = 0.f, b = 0.f;
+      CPSGPU_CUDA(cudaEventElapsedTime(&a, e[0], e[2]));
+      CPSGPU_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+      if (k >= 2) {
+        t_all += a;
+        t_k += b;
+      }
+    }
+    for (auto &x : e) cudaEventDestroy(x);
+    if (ms_total) *ms_total = t_all / reps;
+    if (ms_kernel) *ms_kernel = t_k / reps;
+    if (kernel_bytes) *kernel_bytes = fforce_bytes(D);
     return CPSGPU_OK;
   });
 }

@@ -190,6 +190,16 @@ void op_mobius_dslash4(const Dirac &D, int prec, const SpinorView &out, const Sp
                        OpWork &w);
 void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag);
 
+// HMC fermion force (force.cu): CalcHmdForceVecs' four half fields and the
+// force loop of EvolveMomFforce on a CANONICAL momentum field in device memory
+struct ForceVecs {
+  Field v1o, v1e, v2o, v2e;
+  OpWork w;
+};
+void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi);
+void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, double out[3]);
+double fforce_bytes(const Dirac &D);
+
 // kernels enqueued by this library (graph replays counted by the solver)
 long long &launch_counter();
 

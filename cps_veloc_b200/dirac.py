@@ -230,6 +230,24 @@ class _DiracOp:
         check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
 
+    def CalcHmdForceVecs(self, chi):
+        """DiracOp*::CalcHmdForceVecs: returns (f_out, f_in), full fields in
+        WILSON order: (chi, D chi) and (-kappa^2 MatPc chi, D^dag of it)"""
+        chi = self._vec(chi)
+        f_out, f_in = np.empty(2 * self.f_size), np.empty(2 * self.f_size)
+        check(lib().cpsgpu_calc_hmd_force_vecs(self._h, dptr(f_out), dptr(f_in), dptr(chi)))
+        return f_out, f_in
+
+    def EvolveMomFforce(self, mom, chi, dt):
+        """Fwilson / FdwfBase::EvolveMomFforce: mom (CANONICAL Matrix field,
+        4 * vol * 18 reals, updated in place) += the fermion force of chi;
+        returns the reference's ForceArg as (L1, L2, Linf)"""
+        chi = self._vec(chi)
+        _inplace(mom, 4 * self.lat.vol * 18)
+        fa = A.ForceArg()
+        check(lib().cpsgpu_evolve_mom_fforce(self._h, dptr(mom), dptr(chi), dt, C.byref(fa)))
+        return fa.L1, fa.L2, fa.Linf
+
     def BiCGstab(self, psi, chi, n=1, chi_norm=0.0, stop_rsd=1e-8, max_num_iter=10000):
         """DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res) on MatPc:
         psi (initial guess) updated in place; returns (k, true_res) as the

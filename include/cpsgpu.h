@@ -215,6 +215,28 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
  * InvCg over the same set. res has nrhs entries. */
 int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
                        const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* ---- HMC fermion force (Wilson and Shamir DWF) ----
+ * The reference's ForceArg (alg/force_arg.h): L1 = mean |F|, L2 = rms |F|,
+ * Linf = max |F| over links, |F|^2 = Matrix::norm() = -2 Re tr F^2. */
+typedef struct {
+  double L1, L2, Linf;
+} cpsgpu_force_arg;
+/* DiracOpWilson / DiracOpDwf::CalcHmdForceVecs(chi) (d_op_wilson.C:466-507,
+ * d_op_dwf.C:682-733): f_out = (chi, D chi), f_in = (-kappa^2 MatPc chi,
+ * D^dag of it), full fields in WILSON order ([odd half][even half], before
+ * the reference's conversion to CANONICAL); chi is the odd half. */
+int cpsgpu_calc_hmd_force_vecs(cpsgpu_dirac d, double *f_out, double *f_in, const double *chi);
+/* Fwilson::EvolveMomFforce(mom, chi, mass, dt) (f_wilson.C:470-687) and
+ * FdwfBase::EvolveMomFforce (f_dwf_base_force.C:41-300): mom += the fermion
+ * force of the pseudofermion solution chi (odd half, WILSON order) for a
+ * step dt; mom is the CANONICAL Matrix field [site][mu][3][3][re, im] with
+ * the lexicographic site x + Lx (y + Ly (z + Lz t)).  The operator's own mass
+ * plays the reference's mass argument.  Wilson and DWF handles only. */
+int cpsgpu_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *chi, double dt, cpsgpu_force_arg *out);
+/* Device timing of CalcHmdForceVecs + the force update on a Gaussian chi
+ * (ms per call, ms of the force kernel alone, its algorithmic bytes). */
+int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes);
+
 /* DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res)
  * (bicgstab.C:35-229): BiCGstab(n) on MatPc itself (not the normal
  * equations), psi the initial guess, stop |r|^2 < stop_rsd^2 chi_norm with

@@ -99,6 +99,9 @@ def load_oracle() -> C.CDLL:
             "orc_mobius_m": [g, m, _dp, _dp, _dp, d, i],
             "orc_mobius_mdagm": [g, m, _dp, _dp, _dp, d, _dp],
             "orc_mobius_m5": [g, m, _dp, d],
+            "orc_sproj_tr": [i, i, _dp, _dp, _dp, i, i, i],
+            "orc_force_matrix": [_dp, _dp, _dp, _dp, d],
+            "orc_fforce": [g, _dp, _dp, _dp, _dp, d, _dp],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a
@@ -147,6 +150,8 @@ def load_reference() -> C.CDLL:
             "ref_zmobius_m": [_dp, _dp, _dp, d],
             "ref_zmobius_mdag": [_dp, _dp, _dp, d],
             "ref_zmobius_mdagm": [_dp, _dp, _dp, _dp, d],
+            "ref_sproj_tr": [i, _dp, _dp, _dp, i, i, i],
+            "ref_force_matrix": [_dp, _dp, _dp, _dp, d],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a

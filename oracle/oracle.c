@@ -784,3 +784,131 @@ int orc_bicgstab(orc_matpc_fn matpc, void *ctx, long f_size, double *psi, const 
   free(r0);
   return k;
 }
+
+/* ---------------------------------------------------------------------- */
+/* HMC fermion force                                                       */
+/* ---------------------------------------------------------------------- */
+/* f_(i,j) = sum over blocks and spins of [(1 + sign gamma_mu) v]_(s,i)
+ * conj(w_(s,j)) (sprojTr{X,Y,Z,T}{p,m}, f_wilson_types/noarch/sproj_tr.C):
+ * blocks of 24 reals, v_stride / w_stride extra reals between blocks. */
+void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w, int nblk, int v_stride,
+                  int w_stride) {
+  cplx acc[3][3] = {{0}};
+  for (int b = 0; b < nblk; b++) {
+    const double *vb = v + (long)b * (24 + v_stride), *wb = w + (long)b * (24 + w_stride);
+    for (int s = 0; s < 4; s++) {
+      cplx a[3];
+      for (int c = 0; c < 3; c++)
+        a[c] = ferm(vb, 0, s, c) + sign * g_fac_tab[mu][s] * ferm(vb, 0, g_col[mu][s], c);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) acc[i][j] += a[i] * conj(ferm(wb, 0, s, j));
+    }
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      f[2 * (3 * i + j)] = creal(acc[i][j]);
+      f[2 * (3 * i + j) + 1] = cimag(acc[i][j]);
+    }
+}
+
+/* The per-link matrix steps of the force loop (f_wilson.C:642-656,
+ * f_dwf_base_force.C:268-285) on row-major 3x3 matrices: F = U T;
+ * F <- 1/2 (F - F^dag) - 1/3 i Im tr(...) (Matrix::TrLessAntiHermMatrix,
+ * su3_util.C:79-91); F *= coeff; norm = -2 Re tr(F F) (Matrix::norm). */
+void orc_force_matrix(double *f, double *norm, const double *U, const double *T, double coeff) {
+  cplx F[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      cplx s = 0;
+      for (int k = 0; k < 3; k++)
+        s += (U[2 * (3 * i + k)] + I * U[2 * (3 * i + k) + 1]) * (T[2 * (3 * k + j)] + I * T[2 * (3 * k + j) + 1]);
+      F[i][j] = s;
+    }
+  cplx A[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) A[i][j] = 0.5 * (F[i][j] - conj(F[j][i]));
+  const double c = (cimag(A[0][0]) + cimag(A[1][1]) + cimag(A[2][2])) / 3.0;
+  for (int i = 0; i < 3; i++) A[i][i] -= I * c;
+  double tr = 0.0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      A[i][j] *= coeff;
+    }
+  for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++) tr += creal(A[i][k] * A[k][i]);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      f[2 * (3 * i + j)] = creal(A[i][j]);
+      f[2 * (3 * i + j) + 1] = cimag(A[i][j]);
+    }
+  *norm = -2.0 * tr;
+}
+
+/* position (in sites) of 4D site x, slice s in a full WILSON-order fermion
+ * (convert_func.C:429-494 for ls = 1: odd checkerboard first; convert.C:
+ * 704-760 for ls > 1: [odd part][even part], slice s of the odd part
+ * holding 4D parity (s+1)%2) */
+static long wilson_site(const orc_geom *g, const int x[4], int s) {
+  const int p = (x[0] + x[1] + x[2] + x[3]) & 1;
+  const long vh = vol_cb(g), c = cb_index(g, x);
+  if (g->ls == 1) return c + vh * (1 - p);
+  return (((p + s) & 1) ? 0 : (long)g->ls * vh) + (long)s * vh + c;
+}
+
+/* The force loop of FdwfBase::EvolveMomFforce (f_dwf_base_force.C:41-300;
+ * ls = 1 is Fwilson::EvolveMomFforce, f_wilson.C:470-687) after
+ * CalcHmdForceVecs: v1 = (chi, D chi), v2 = (-kappa^2 MatPc chi, D^dag of
+ * it) as full fermion fields in WILSON order (the reference converts them to
+ * CANONICAL first; indexing the WILSON order directly reads the same values).
+ * Per site x and direction mu, with the sum over slices s:
+ *   T = sproj(1 - g_mu)[v1(x+mu), v2(x)] + sproj(1 + g_mu)[v2(x+mu), v1(x)],
+ *   mom(x, mu) += coeff TrLessAntiHerm(U_mu(x) T)  in the reference's step
+ * order (orc_force_matrix), coeff = -2 dt, negated where x+mu wraps an
+ * antiperiodic direction.  mom is CANONICAL: [lexicographic site][mu][row][col][re,im].
+ * out = {L1, L2, Linf} as the reference's ForceArg(L1/(4V), sqrt(L2/(4V)), Linf). */
+void orc_fforce(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2, double dt,
+                double out[3]) {
+  const long vol = 2 * vol_cb(g);
+  double L1 = 0.0, L2 = 0.0, Linf = 0.0;
+  for (int mu = 0; mu < 4; mu++)
+    for (int t = 0; t < g->L[3]; t++)
+      for (int z = 0; z < g->L[2]; z++)
+        for (int y = 0; y < g->L[1]; y++)
+          for (int xx = 0; xx < g->L[0]; xx++) {
+            const int x[4] = {xx, y, z, t};
+            int xp[4] = {xx, y, z, t};
+            double coeff = -2.0 * dt;
+            xp[mu] = (x[mu] + 1) % g->L[mu];
+            if (x[mu] + 1 == g->L[mu] && g->bc[mu] < 0) coeff = -coeff;
+            double T1[18] = {0}, T2[18] = {0}, tmp[18];
+            for (int s = 0; s < g->ls; s++) {
+              const long o = wilson_site(g, x, s), op = wilson_site(g, xp, s);
+              orc_sproj_tr(mu, -1, tmp, v1 + 24 * op, v2 + 24 * o, 1, 0, 0);
+              for (int k = 0; k < 18; k++) T1[k] += tmp[k];
+              orc_sproj_tr(mu, +1, tmp, v2 + 24 * op, v1 + 24 * o, 1, 0, 0);
+              for (int k = 0; k < 18; k++) T2[k] += tmp[k];
+            }
+            for (int k = 0; k < 18; k++) T1[k] += T2[k];
+            /* U_mu(x) as a row-major matrix */
+            const int p = (xx + y + z + t) & 1;
+            const long gs = cb_index(g, x) + vol_cb(g) * p;
+            double U[18];
+            for (int i = 0; i < 3; i++)
+              for (int j = 0; j < 3; j++) {
+                const cplx e = link(u, gs, mu, i, j);
+                U[2 * (3 * i + j)] = creal(e);
+                U[2 * (3 * i + j) + 1] = cimag(e);
+              }
+            double F[18], n;
+            orc_force_matrix(F, &n, U, T1, coeff);
+            double *m = mom + 18 * (4 * (xx + (long)g->L[0] * (y + (long)g->L[1] * (z + (long)g->L[2] * t))) + mu);
+            for (int k = 0; k < 18; k++) m[k] += F[k];
+            const double a = sqrt(n);
+            L1 += a;
+            L2 += n;
+            if (a > Linf) Linf = a;
+          }
+  out[0] = L1 / (4.0 * vol);
+  out[1] = sqrt(L2 / (4.0 * vol));
+  out[2] = Linf;
+}

@@ -118,6 +118,14 @@ int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double
 int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
                       double mass, double stop_rsd, int max_num_iter, double *true_res);
 
+/* HMC fermion force (Fwilson / FdwfBase::EvolveMomFforce): sprojTr, the
+ * per-link matrix steps and the whole force loop; see oracle.c. */
+void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w, int nblk, int v_stride,
+                  int w_stride);
+void orc_force_matrix(double *f, double *norm, const double *U, const double *T, double coeff);
+void orc_fforce(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2, double dt,
+                double out[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,7 @@
 #include <util/dwf.h>
 #include <util/zmobius.h>
 #include <util/gjp.h>
+#include <util/sproj_tr.h>
 #include <alg/do_arg.h>
 #include <cstring>
 #include <vector>
@@ -153,6 +154,27 @@ void ref_zmobius_mdag(double *out, double *u, double *in, double mass) {
 }
 void ref_zmobius_mdagm(double *out, double *u, double *in, double *dot, double mass) {
   zmobius_mdagm((Vector *)out, (Matrix *)u, (Vector *)in, dot, mass, &g_dwf);
+}
+
+// ---- HMC fermion force pieces ----
+// sprojTr{X,Y,Z,T}{m,p} (f_wilson_types/noarch/sproj_tr.C), indexed as the
+// SprojType enum orders them (alg/enum_int.h: XM..TM = 0..3, XP..TP = 4..7)
+void ref_sproj_tr(int which, double *f, double *v, double *w, int nblk, int v_stride, int w_stride) {
+  typedef void (*fn)(IFloat *, IFloat *, IFloat *, int, int, int);
+  static const fn tab[8] = {sprojTrXm, sprojTrYm, sprojTrZm, sprojTrTm,
+                            sprojTrXp, sprojTrYp, sprojTrZp, sprojTrTp};
+  tab[which](f, v, w, nblk, v_stride, w_stride);
+}
+// the per-link steps of the force loop through the reference's Matrix
+// (util/vector.h): F = U T, F = TrLessAntiHerm with F^dag, F *= coeff, norm()
+void ref_force_matrix(double *f, double *norm, double *U, double *T, double coeff) {
+  Matrix a, b;
+  a.DotMEqual(*(const Matrix *)U, *(const Matrix *)T);
+  b.Dagger(a);
+  a.TrLessAntiHermMatrix(b);
+  a *= coeff;
+  *norm = a.norm();
+  std::memcpy(f, &a, 18 * sizeof(double));
 }
 
 }  // extern "C"

@@ -143,6 +143,29 @@ class OracleOps:
                               C.byref(sh) if sh is not None else None)
         return sol, it, tr.value
 
+    def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
+        """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,
+        d_op_dwf.C:682-733): v1 = (chi, D chi), v2 = (psi, D^dag psi) with
+        psi = -kappa^2 MatPc chi, full fields in WILSON order"""
+        if kind == "wilson":
+            psi = -kappa * kappa * self.wilson_m(chi, kappa, 0)
+            rho, sigma = self.wilson_dslash(chi, 1, 0), self.wilson_dslash(psi, 1, 1)
+        else:
+            k5 = 1 / (2 * (5 - self.m5))
+            psi = -k5 * k5 * self.dwf_m(chi, mass, 0)
+            rho, sigma = self.dwf_dslash(chi, mass, 1, 0), self.dwf_dslash(psi, mass, 1, 1)
+        return np.concatenate([chi, rho]), np.concatenate([psi, sigma])
+
+    def fforce(self, kind, chi, dt, mass=0.0, kappa=0.0, mom=None):
+        """Fwilson / FdwfBase::EvolveMomFforce: returns (mom + force, (L1, L2, Linf))"""
+        v1, v2 = self.force_vecs(kind, chi, mass, kappa)
+        vol = int(np.prod(self.L))
+        m = np.zeros(4 * vol * 18) if mom is None else np.ascontiguousarray(mom).copy()
+        out = np.zeros(3)
+        g = self.g1 if kind == "wilson" else self.g
+        self.O.orc_fforce(C.byref(g), p(m), p(self.u), p(v1), p(v2), dt, p(out))
+        return m, tuple(out)
+
     def bicgstab(self, kind, chi, n=1, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, psi0=None):
         """BiCGstab(n) on MatPc (bicgstab.C:35-229): returns psi, k, true_res"""
         O, u = self.O, self.u

@@ -135,3 +135,33 @@ def test_zmobius_vs_reference(oracle, reference, L, ls, mass):
     reference.ref_zmobius_mdagm(p(y), p(us), p(psi), C.byref(d), mass)
     yo, do = ops.mobius_mdagm(psi, mass)
     assert rel(yo, y) < TOL and abs(do / d.value - 1) < TOL
+
+
+@pytest.mark.parametrize("which", range(8))
+@pytest.mark.parametrize("nblk,vs,ws", [(1, 0, 0), (3, 0, 0), (4, 24, 48)])
+def test_sproj_tr_vs_reference(oracle, reference, which, nblk, vs, ws):
+    """sprojTr{X,Y,Z,T}{m,p} (sproj_tr.C): the oracle's (1 -+ gamma_mu) spin
+    projection and trace against the reference's eight routines, with blocks
+    and strides as FdwfBase::EvolveMomFforce passes them."""
+    v = gen_gaussian((24 + vs) * nblk, seed=170 + which)
+    w = gen_gaussian((24 + ws) * nblk, seed=180 + which)
+    f_ref, f_orc = np.zeros(18), np.zeros(18)
+    reference.ref_sproj_tr(which, p(f_ref), p(v), p(w), nblk, vs, ws)
+    oracle.orc_sproj_tr(which % 4, -1 if which < 4 else 1, p(f_orc), p(v), p(w), nblk, vs, ws)
+    assert rel(f_orc, f_ref) < 1e-14
+
+
+def test_force_matrix_steps_vs_reference(oracle, reference):
+    """The per-link steps of the force loop (F = U T, TrLessAntiHermMatrix
+    with F^dag, *= coeff, Matrix::norm) against the reference's Matrix class."""
+    for k in range(5):
+        U = gen_gaussian(18, seed=190 + k)
+        T = gen_gaussian(18, seed=200 + k)
+        fr, fo = np.zeros(18), np.zeros(18)
+        nr, no = C.c_double(), C.c_double()
+        reference.ref_force_matrix(p(fr), C.byref(nr), p(U), p(T), -0.37)
+        oracle.orc_force_matrix(p(fo), C.byref(no), p(U), p(T), -0.37)
+        assert rel(fo, fr) < 1e-14 and abs(no.value - nr.value) <= 1e-14 * abs(nr.value)
+        # traceless and antihermitian
+        m = fo[0::2].reshape(3, 3) + 1j * fo[1::2].reshape(3, 3)
+        assert np.abs(m + m.conj().T).max() < 1e-15 and abs(np.trace(m)) < 1e-15
