@@ -332,6 +332,19 @@ def extra_multishift(A) -> dict:
     return out
 
 
+def extra_force(A, D, pk) -> dict:
+    """HMC fermion force on the headline DWF system (FdwfBase::EvolveMomFforce):
+    CalcHmdForceVecs (MatPc + two Dslash in FP64) plus the fused force kernel,
+    device-resident, event-timed; the kernel's algorithmic bytes are v1, v2
+    (both parities, all slices) read once, the FP64 links read once and the
+    momentum field read and written."""
+    tot, ker, by = C.c_double(), C.c_double(), C.c_double()
+    A.check(A.lib().cpsgpu_time_fforce(D._h, 20, C.byref(tot), C.byref(ker), C.byref(by)))
+    gbs = by.value / (ker.value * 1e-3) / 1e9
+    return {"ms_per_call": tot.value, "force_kernel_ms": ker.value, "force_kernel_GB_s": gbs,
+            "force_kernel_frac_of_measured_hbm": gbs / pk["hbm_gbs"], "force_kernel_bytes": by.value}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -490,7 +503,8 @@ def main(argv=None) -> int:
     if rank == 0 and not args.no_extras:
         extras = {"batched_12_point_sources": extra_batched(A, D, sloppy),
                   "mobius_24x64_ls12": extra_mobius(A),
-                  "multishift_wilson_32x64": extra_multishift(A)}
+                  "multishift_wilson_32x64": extra_multishift(A),
+                  "hmc_force_dwf_16x32_ls16": extra_force(A, D, pk)}
 
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
     if rank == 0:

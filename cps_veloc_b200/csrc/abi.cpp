@@ -553,11 +553,50 @@ int cpsgpu_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *chi, dou
     ForceVecs &fv = force_vecs(d, chi);
     Lattice &L = *d->D->lat;
     const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
-    d->mom.ensure(bytes);
+    d->mom.ensure(2 * bytes);
     CPSGPU_CUDA(cudaMemcpyAsync(d->mom.ptr, mom, bytes, cudaMemcpyHostToDevice, L.stream));
     double f[3];
     fforce_update(*d->D, fv, d->mom.as<double>(), dt, f);
     CPSGPU_CUDA(cudaMemcpyAsync(mom, d->mom.ptr, bytes, cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    if (out) {
+      out->L1 = f[0];
+      out->L2 = f[1];
+      out->Linf = f[2];
+    }
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *const *sol, int degree,
+                                  const double *alpha, double dt, int force_measure, cpsgpu_force_arg *out) {
+  return guarded([&] {
+    if (!d || !mom || (degree > 0 && (!sol || !alpha))) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (degree < 0) throw Error(CPSGPU_ERR_ARG, "degree must be >= 0");
+    for (int k = 0; k < degree; k++)
+      if (!sol[k]) throw Error(CPSGPU_ERR_ARG, "null solution vector");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+    const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
+    d->mom.ensure(2 * bytes);
+    double *m = d->mom.as<double>(), *tmp = m + bytes / sizeof(double);
+    CPSGPU_CUDA(cudaMemcpyAsync(m, mom, bytes, cudaMemcpyHostToDevice, L.stream));
+    // FORCE_MEASURE_YES: the poles accumulate into a zeroed field whose norms
+    // are measured before it is added to mom (f_wilson.C:689-757)
+    double *acc = force_measure ? tmp : m;
+    if (force_measure) CPSGPU_CUDA(cudaMemsetAsync(tmp, 0, bytes, L.stream));
+    for (int k = 0; k < degree; k++) {
+      ForceVecs &fv = force_vecs(d, sol[k]);
+      fforce_update(D, fv, acc, dt * alpha[k], nullptr);
+    }
+    double f[3] = {0.0, 0.0, 0.0};
+    if (force_measure) {
+      mom_norms(L, tmp, f);
+      mom_add(L, m, tmp);
+    }
+    CPSGPU_CUDA(cudaMemcpyAsync(mom, m, bytes, cudaMemcpyDeviceToHost, L.stream));
     CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
     if (out) {
       out->L1 = f[0];

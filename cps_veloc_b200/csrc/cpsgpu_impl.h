@@ -199,6 +199,9 @@ struct ForceVecs {
 void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi);
 void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, double out[3]);
 double fforce_bytes(const Dirac &D);
+// ForceArg of a whole momentum field (per-link Matrix::norm) and mom += x
+void mom_norms(Lattice &L, const double *mom, double out[3]);
+void mom_add(Lattice &L, double *mom, const double *x);
 
 // kernels enqueued by this library (graph replays counted by the solver)
 long long &launch_counter();

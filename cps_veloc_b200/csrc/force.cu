@@ -274,6 +274,72 @@ __global__ void __launch_bounds__(1024) force_finalize_kernel(const double *part
   }
 }
 
+// per-link Matrix::norm() = -2 Re tr M^2 of a CANONICAL Matrix field: block
+// partials of sum |M|, sum |M|^2 and max |M| (as fforce_kernel writes them)
+__global__ void __launch_bounds__(256) mom_norm_kernel(const double *mom, long nlink, double *partials) {
+  const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double red[3] = {0.0, 0.0, 0.0};
+  if (l < nlink) {
+    const double2 *m = reinterpret_cast<const double2 *>(mom + 18 * l);
+    cplx<double> A[3][3];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const double2 q = m[k];
+      A[k / 3][k % 3] = {q.x, q.y};
+    }
+    double tr = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) tr += A[a][b].re * A[b][a].re - A[a][b].im * A[b][a].im;
+    const double n = -2.0 * tr;
+    red[0] = sqrt(fmax(n, 0.0));
+    red[1] = n;
+    red[2] = red[0];
+  }
+  __shared__ double sm[8][3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    red[0] += __shfl_down_sync(0xffffffffu, red[0], o);
+    red[1] += __shfl_down_sync(0xffffffffu, red[1], o);
+    red[2] = fmax(red[2], __shfl_down_sync(0xffffffffu, red[2], o));
+  }
+  if (lane == 0) {
+    sm[warp][0] = red[0];
+    sm[warp][1] = red[1];
+    sm[warp][2] = red[2];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0, mx = 0.0;
+    for (int k = 0; k < (int)(blockDim.x + 31) / 32; k++) {
+      s0 += sm[k][0];
+      s1 += sm[k][1];
+      mx = fmax(mx, sm[k][2]);
+    }
+    partials[3 * blockIdx.x] = s0;
+    partials[3 * blockIdx.x + 1] = s1;
+    partials[3 * blockIdx.x + 2] = mx;
+  }
+}
+
+__global__ void add_kernel(double *y, const double *x, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) y[k] += x[k];
+}
+
+// the reduced sums of the last reduction -> the reference's ForceArg
+void force_arg_of(Lattice &L, const double *res, double out[3]) {
+  double h[3];
+  CPSGPU_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+  const double links = 4.0 * 2.0 * (double)L.vh;
+  out[0] = h[0] / links;
+  out[1] = std::sqrt(h[1] / links);
+  out[2] = h[2];
+}
+
 }  // namespace
 
 void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi) {
@@ -324,15 +390,28 @@ void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, 
   force_finalize_kernel<<<1, 1024, 0, L.stream>>>(part, nblk, res);
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter() += 2;
-  if (out) {
-    double h[3];
-    CPSGPU_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
-    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
-    const double vol4 = 4.0 * 2.0 * (double)L.vh;
-    out[0] = h[0] / vol4;
-    out[1] = std::sqrt(h[1] / vol4);
-    out[2] = h[2];
-  }
+  if (out) force_arg_of(L, res, out);
+}
+
+void mom_norms(Lattice &L, const double *mom, double out[3]) {
+  const long nlink = 4 * 2 * L.vh;
+  const unsigned nblk = (unsigned)((nlink + 255) / 256);
+  L.partials.ensure((size_t)nblk * 3 * sizeof(double) + 3 * sizeof(double));
+  double *part = L.partials.as<double>();
+  double *res = part + (size_t)nblk * 3;
+  mom_norm_kernel<<<nblk, 256, 0, L.stream>>>(mom, nlink, part);
+  CPSGPU_CUDA(cudaGetLastError());
+  force_finalize_kernel<<<1, 1024, 0, L.stream>>>(part, nblk, res);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter() += 2;
+  force_arg_of(L, res, out);
+}
+
+void mom_add(Lattice &L, double *mom, const double *x) {
+  const long n = 4 * 2 * L.vh * 18;
+  add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, L.stream>>>(mom, x, n);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
 }
 
 // algorithmic bytes of one force-kernel launch: v1, v2 read once (both

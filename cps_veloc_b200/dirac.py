@@ -248,6 +248,21 @@ class _DiracOp:
         check(lib().cpsgpu_evolve_mom_fforce(self._h, dptr(mom), dptr(chi), dt, C.byref(fa)))
         return fa.L1, fa.L2, fa.Linf
 
+    def RHMC_EvolveMomFforce(self, mom, sol, alpha, dt, force_measure=False):
+        """Fwilson / FdwfBase::RHMC_EvolveMomFforce over the poles sol[k] with
+        steps dt * alpha[k]; returns (L1, L2, Linf) of the summed force when
+        force_measure, else zeros (as the reference)"""
+        _inplace(mom, 4 * self.lat.vol * 18)
+        sols = [self._vec(x) for x in sol]
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        if alpha.size != len(sols):
+            raise ValueError("one alpha per pole")
+        arr = (A._dp * max(1, len(sols)))(*[dptr(x) for x in sols])
+        fa = A.ForceArg()
+        check(lib().cpsgpu_rhmc_evolve_mom_fforce(self._h, dptr(mom), arr, len(sols), dptr(alpha), dt,
+                                                  1 if force_measure else 0, C.byref(fa)))
+        return fa.L1, fa.L2, fa.Linf
+
     def BiCGstab(self, psi, chi, n=1, chi_norm=0.0, stop_rsd=1e-8, max_num_iter=10000):
         """DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res) on MatPc:
         psi (initial guess) updated in place; returns (k, true_res) as the

@@ -233,6 +233,14 @@ int cpsgpu_calc_hmd_force_vecs(cpsgpu_dirac d, double *f_out, double *f_in, cons
  * the lexicographic site x + Lx (y + Ly (z + Lz t)).  The operator's own mass
  * plays the reference's mass argument.  Wilson and DWF handles only. */
 int cpsgpu_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *chi, double dt, cpsgpu_force_arg *out);
+/* Fwilson / FdwfBase::RHMC_EvolveMomFforce(mom, sol, degree, isz, alpha,
+ * mass, dt, sol_d, force_measure) (f_wilson.C:689-757, f_dwf_base.C:1424):
+ * mom += sum over the poles k < degree of the force of sol[k] with step
+ * dt alpha[k].  force_measure != 0 (FORCE_MEASURE_YES): the poles are summed
+ * into a zeroed field first, *out = the ForceArg of that sum, then it is
+ * added to mom; otherwise they accumulate into mom directly and *out = 0. */
+int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *const *sol, int degree,
+                                  const double *alpha, double dt, int force_measure, cpsgpu_force_arg *out);
 /* Device timing of CalcHmdForceVecs + the force update on a Gaussian chi
  * (ms per call, ms of the force kernel alone, its algorithmic bytes). */
 int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes);

@@ -59,3 +59,27 @@ def test_force_rejects_mobius_and_bad_sizes(oracle):
     W = DiracOpWilson(lat, mass=0.1)
     with pytest.raises(TypeError):
         W.EvolveMomFforce(np.zeros(10), np.zeros(W.f_size), 0.1)
+
+
+@pytest.mark.parametrize("measure", [False, True])
+def test_rhmc_evolve_mom_fforce(oracle, measure):
+    """RHMC_EvolveMomFforce (f_wilson.C:689-757): the pole sum, and with
+    FORCE_MEASURE_YES the ForceArg of the summed force (Matrix::norm per link)."""
+    kind, L, ls, bc = "dwf", (4, 4, 4, 4), 4, (1, 1, 1, -1)
+    D, ops, mass = _setup(oracle, kind, L, ls, bc, 227)
+    sols = [gen_gaussian(D.f_size, seed=228 + k) for k in range(3)]
+    alpha = np.array([0.5, -0.125, 2.0])
+    dt = 0.02
+    mom0 = gen_gaussian(4 * int(np.prod(L)) * 18, seed=231)
+    tot = np.zeros_like(mom0)
+    for s_, a in zip(sols, alpha):
+        tot, _ = ops.fforce(kind, s_, dt * a, mass=mass, kappa=D.kappa, mom=tot)
+    mom = mom0.copy()
+    fa = D.RHMC_EvolveMomFforce(mom, sols, alpha, dt, force_measure=measure)
+    assert rel(mom - mom0, tot) < 1e-12
+    if measure:
+        t = (tot[0::2] + 1j * tot[1::2]).reshape(-1, 3, 3)
+        n = np.sqrt(np.maximum(-2 * np.einsum("lab,lba->l", t, t).real, 0))
+        assert np.allclose(fa, (n.mean(), np.sqrt(np.mean(n ** 2)), n.max()), rtol=1e-12, atol=0)
+    else:
+        assert fa == (0.0, 0.0, 0.0)
