@@ -39,6 +39,16 @@ class ForceArg(C.Structure):
     _fields_ = [("L1", C.c_double), ("L2", C.c_double), ("Linf", C.c_double)]
 
 
+class NerscHeader(C.Structure):
+    """cpsgpu_nersc_header"""
+    _fields_ = [("dims", C.c_int * 4), ("recon_row_3", C.c_int), ("fp_format", C.c_int), ("plaquette", C.c_double),
+                ("link_trace", C.c_double), ("checksum", C.c_uint), ("sequence_number", C.c_int),
+                ("ensemble_id", C.c_char * 128), ("ensemble_label", C.c_char * 128), ("creator", C.c_char * 128)]
+
+
+FP_FORMATS = {"IEEE32": 3, "IEEE32BIG": 4, "IEEE32LITTLE": 5, "IEEE64": 6, "IEEE64BIG": 7, "IEEE64LITTLE": 8}
+
+
 class CgArg(C.Structure):
     _fields_ = [("stop_rsd", C.c_double), ("max_num_iter", C.c_int), ("src_norm_sq", C.c_double),
                 ("shift", C.c_double), ("precision", C.c_int), ("delta", C.c_double), ("chunk", C.c_int),
@@ -91,6 +101,11 @@ def lib() -> C.CDLL:
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_gauge_plaquette": (C.c_int, [vp, _dp, _dp]),
+            "cpsgpu_nersc_read": (C.c_int, [C.c_char_p, _ip, _dp, C.POINTER(NerscHeader)]),
+            "cpsgpu_nersc_write": (C.c_int, [C.c_char_p, _ip, _dp, C.c_int, C.c_int, C.POINTER(NerscHeader),
+                                             C.POINTER(NerscHeader)]),
+            "cpsgpu_lattice_load_nersc": (C.c_int, [vp, C.c_char_p, C.c_double, C.POINTER(NerscHeader), _dp]),
             "cpsgpu_calc_hmd_force_vecs": (C.c_int, [vp, _dp, _dp, _dp]),
             "cpsgpu_evolve_mom_fforce": (C.c_int, [vp, _dp, _dp, C.c_double, C.POINTER(ForceArg)]),
             "cpsgpu_time_fforce": (C.c_int, [vp, C.c_int, _dp, _dp, _dp]),

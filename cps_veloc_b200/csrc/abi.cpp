@@ -1,6 +1,7 @@
 // The C ABI (include/cpsgpu.h): argument checking, object lifetimes,
 // host <-> device staging in CPS storage order, and error translation.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -23,6 +24,9 @@ double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
 int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, double stop_rsd, int max_num_iter,
              double *true_res);
 void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
+void nersc_read(const char *path, const int node_sites[4], double *u, cpsgpu_nersc_header *hdr);
+void nersc_write(const char *path, const int node_sites[4], const double *u, int recon_row_3, int fp_format,
+                 const cpsgpu_nersc_header *meta, cpsgpu_nersc_header *out);
 void gconvert(const int node_sites[4], double *u, int to, int from);
 void four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
 void five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb);
@@ -226,6 +230,61 @@ int cpsgpu_get_link_reals(cpsgpu_lattice lat, int prec, int *reals) {
     if (!lat || !reals) throw Error(CPSGPU_ERR_ARG, "null argument");
     if (prec != CPSGPU_SINGLE && prec != CPSGPU_HALF) throw Error(CPSGPU_ERR_ARG, "FP32 or FP16 only");
     *reals = lat->L->sloppy_recon[prec];
+    return CPSGPU_OK;
+  });
+}
+
+// ---- gauge configurations (gauge.cu, nersc.cpp)
+int cpsgpu_gauge_plaquette(cpsgpu_lattice lat, double *plaq, double *link_trace) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    Lattice &L = *lat->L;
+    if (!L.have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+    double sp = 0.0, sl = 0.0;
+    gauge_sums(L, &sp, &sl);
+    const double vol = 2.0 * (double)L.vh;
+    if (plaq) *plaq = sp / (18.0 * vol);
+    if (link_trace) *link_trace = sl / (12.0 * vol);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_nersc_read(const char *path, const int node_sites[4], double *u, cpsgpu_nersc_header *hdr) {
+  return guarded([&] {
+    nersc_read(path, node_sites, u, hdr);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_nersc_write(const char *path, const int node_sites[4], const double *u, int recon_row_3, int fp_format,
+                       const cpsgpu_nersc_header *meta, cpsgpu_nersc_header *out) {
+  return guarded([&] {
+    nersc_write(path, node_sites, u, recon_row_3, fp_format, meta, out);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_lattice_load_nersc(cpsgpu_lattice lat, const char *path, double check_precision, cpsgpu_nersc_header *hdr,
+                              double *plaq) {
+  return guarded([&] {
+    if (!lat || !path) throw Error(CPSGPU_ERR_ARG, "null argument");
+    Lattice &L = *lat->L;
+    const long vol = 2 * L.vh;
+    std::vector<double> u((size_t)vol * 72);
+    cpsgpu_nersc_header h;
+    nersc_read(path, L.L, u.data(), &h);
+    gconvert(L.L, u.data(), CPSGPU_STR_WILSON, CPSGPU_STR_CANONICAL);
+    import_gauge(L, u.data(), 0);
+    double sp = 0.0;
+    gauge_sums(L, &sp, nullptr);
+    const double p = sp / (18.0 * (double)vol);
+    if (plaq) *plaq = p;
+    if (hdr) *hdr = h;
+    if (std::fabs((p - h.plaquette) / p) > check_precision) {
+      char msg[128];
+      std::snprintf(msg, sizeof msg, "plaquette check failed: computed %.10g, header %.10g", p, h.plaquette);
+      throw Error(CPSGPU_ERR_ARG, msg);
+    }
     return CPSGPU_OK;
   });
 }

@@ -199,6 +199,10 @@ struct ForceVecs {
 void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi);
 void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, double out[3]);
 double fforce_bytes(const Dirac &D);
+// plaquette and link-trace sums of the resident links (gauge.cu) and of a
+// CANONICAL host field (nersc.cpp)
+void gauge_sums(Lattice &L, double *sum_plaq, double *sum_link);
+void host_gauge_sums(const int L[4], const double *u, double *sum_plaq, double *sum_link);
 // ForceArg of a whole momentum field (per-link Matrix::norm) and mom += x
 void mom_norms(Lattice &L, const double *mom, double out[3]);
 void mom_add(Lattice &L, double *mom, const double *x);

@@ -76,6 +76,38 @@ def five2four(node_sites, ls: int, five: np.ndarray, s_u: int, s_l: int, ncb: in
     return four
 
 
+def _header(h) -> dict:
+    name = {v: k for k, v in A.FP_FORMATS.items()}
+    return {"dims": tuple(h.dims), "recon_row_3": bool(h.recon_row_3), "floating_point": name.get(h.fp_format),
+            "plaquette": h.plaquette, "link_trace": h.link_trace, "checksum": h.checksum,
+            "sequence_number": h.sequence_number, "ensemble_id": h.ensemble_id.decode(),
+            "ensemble_label": h.ensemble_label.decode(), "creator": h.creator.decode()}
+
+
+def nersc_read(path, node_sites):
+    """ReadLatticeParallel::read of a NERSC archive: (CANONICAL links, header)"""
+    u = np.empty(72 * int(np.prod(node_sites)))
+    h = A.NerscHeader()
+    check(lib().cpsgpu_nersc_read(str(path).encode(), A.ints(node_sites), dptr(u), C.byref(h)))
+    return u, _header(h)
+
+
+def nersc_write(path, node_sites, u, recon_row_3=True, floating_point="IEEE64BIG", ensemble_id="",
+                ensemble_label="", sequence_number=0, creator=""):
+    """WriteLatticeParallel::write of a CANONICAL field; returns the header written"""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    if u.size != 72 * int(np.prod(node_sites)):
+        raise ValueError("gauge field size")
+    meta = A.NerscHeader()
+    meta.ensemble_id, meta.ensemble_label, meta.creator = (s.encode()[:127] for s in
+                                                           (ensemble_id, ensemble_label, creator))
+    meta.sequence_number = sequence_number
+    out = A.NerscHeader()
+    check(lib().cpsgpu_nersc_write(str(path).encode(), A.ints(node_sites), dptr(u), 1 if recon_row_3 else 0,
+                                   A.FP_FORMATS[floating_point], C.byref(meta), C.byref(out)))
+    return _header(out)
+
+
 def _inplace(a, n):
     if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size == n):
         raise TypeError(f"expected a C-contiguous float64 array of {n} reals (converted in place)")
@@ -111,6 +143,18 @@ class Lattice:
         r = C.c_int()
         check(lib().cpsgpu_get_link_reals(self._h, prec, C.byref(r)))
         return r.value
+
+    def plaquette(self):
+        """(SumReTrPlaq / (18 V), sum Re tr U / (12 V)) of the resident links"""
+        p, t = C.c_double(), C.c_double()
+        check(lib().cpsgpu_gauge_plaquette(self._h, C.byref(p), C.byref(t)))
+        return p.value, t.value
+
+    def load_nersc(self, path, check_precision=0.01):
+        """ReadLatticeParallel::read into this lattice; returns (plaquette, header)"""
+        h, p = A.NerscHeader(), C.c_double()
+        check(lib().cpsgpu_lattice_load_nersc(self._h, str(path).encode(), check_precision, C.byref(h), C.byref(p)))
+        return p.value, _header(h)
 
     def synchronize(self):
         check(lib().cpsgpu_synchronize(self._h))

@@ -215,6 +215,49 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
  * InvCg over the same set. res has nrhs entries. */
 int cpsgpu_invcg_multi(cpsgpu_dirac d, double *const *sol, const double *const *src, int nrhs,
                        const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* ---- gauge configurations ----
+ * Plaquette and link trace of the resident (unsigned) links, normalised as
+ * the NERSC header and ReadLatticeParallel's check use them:
+ * plaq = Lattice::SumReTrPlaq() / (18 V) (lattice_base.C:2878-3060),
+ * link_trace = sum over links of Re tr U / (12 V). */
+int cpsgpu_gauge_plaquette(cpsgpu_lattice lat, double *plaq, double *link_trace);
+
+/* NERSC archive format (ReadLatticePar.C, WriteLatticePar.C, latheader.C,
+ * fpconv.C); fp formats in the reference's FP_FORMAT order. */
+#define CPSGPU_FP_IEEE32 3
+#define CPSGPU_FP_IEEE32BIG 4
+#define CPSGPU_FP_IEEE32LITTLE 5
+#define CPSGPU_FP_IEEE64 6
+#define CPSGPU_FP_IEEE64BIG 7
+#define CPSGPU_FP_IEEE64LITTLE 8
+typedef struct {
+  int dims[4];
+  int recon_row_3;           /* 1: DATATYPE = 4D_SU3_GAUGE (two rows stored), 0: 4D_SU3_GAUGE_3x3 */
+  int fp_format;             /* CPSGPU_FP_* */
+  double plaquette;          /* PLAQUETTE (read: as the reference parses it, %f) */
+  double link_trace;         /* LINK_TRACE */
+  unsigned int checksum;     /* CHECKSUM */
+  int sequence_number;
+  char ensemble_id[128], ensemble_label[128], creator[128];
+} cpsgpu_nersc_header;
+/* ReadLatticeParallel::read without the lattice: parse the header, check
+ * the dimensions, read the links (u: CANONICAL [site][mu][3][3][re, im]),
+ * verify the checksum (error on a mismatch) and rebuild the third rows of
+ * a two-row file. */
+int cpsgpu_nersc_read(const char *path, const int node_sites[4], double *u, cpsgpu_nersc_header *hdr);
+/* WriteLatticeParallel::write of a CANONICAL host field: header (plaquette
+ * and link trace computed from u, periodic boundaries as the reference
+ * records them, meta: ensemble id / label / sequence number / creator, may
+ * be NULL) and data in fp_format, two rows per link when recon_row_3. */
+int cpsgpu_nersc_write(const char *path, const int node_sites[4], const double *u, int recon_row_3, int fp_format,
+                       const cpsgpu_nersc_header *meta, cpsgpu_nersc_header *out);
+/* ReadLatticeParallel::read into the lattice: read (as above), import the
+ * links (no boundary signs) and fail when the plaquette of the imported
+ * field deviates from the header's by more than check_precision (relative;
+ * the reference's default is 0.01).  *plaq = the computed plaquette. */
+int cpsgpu_lattice_load_nersc(cpsgpu_lattice lat, const char *path, double check_precision, cpsgpu_nersc_header *hdr,
+                              double *plaq);
+
 /* ---- HMC fermion force (Wilson and Shamir DWF) ----
  * The reference's ForceArg (alg/force_arg.h): L1 = mean |F|, L2 = rms |F|,
  * Linf = max |F| over links, |F|^2 = Matrix::norm() = -2 Re tr F^2. */

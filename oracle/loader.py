@@ -156,6 +156,8 @@ def load_reference() -> C.CDLL:
         for k, a in sig.items():
             getattr(L, k).argtypes = a
             getattr(L, k).restype = None
+        L.ref_fp_checksum.argtypes = [C.c_char_p, i, i]
+        L.ref_fp_checksum.restype = C.c_uint
         _ref = L
     return _ref
 

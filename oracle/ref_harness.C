@@ -25,6 +25,7 @@
 #include <util/zmobius.h>
 #include <util/gjp.h>
 #include <util/sproj_tr.h>
+#include <util/fpconv.h>
 #include <alg/do_arg.h>
 #include <cstring>
 #include <vector>
@@ -154,6 +155,14 @@ void ref_zmobius_mdag(double *out, double *u, double *in, double mass) {
 }
 void ref_zmobius_mdagm(double *out, double *u, double *in, double *dot, double mass) {
   zmobius_mdagm((Vector *)out, (Matrix *)u, (Vector *)in, dot, mass, &g_dwf);
+}
+
+// ---- NERSC archives: FPConv::checksum (fpconv.C:320-360) of n_words file
+// values in the given FP_FORMAT (the enum order of fpconv.C:12-22)
+unsigned int ref_fp_checksum(char *data, int n_values, int format) {
+  FPConv fp;
+  fp.setFileFormat((FP_FORMAT)format);
+  return fp.checksum(data, n_values, (FP_FORMAT)format);
 }
 
 // ---- HMC fermion force pieces ----
