@@ -24,6 +24,8 @@ double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in);
 int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, double stop_rsd, int max_num_iter,
              double *true_res);
 void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
+void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
+               double *error);
 void nersc_read(const char *path, const int node_sites[4], double *u, cpsgpu_nersc_header *hdr);
 void nersc_write(const char *path, const int node_sites[4], const double *u, int recon_row_3, int fp_format,
                  const cpsgpu_nersc_header *meta, cpsgpu_nersc_header *out);
@@ -704,6 +706,36 @@ int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_ke
     if (ms_total) *ms_total = t_all / reps;
     if (ms_kernel) *ms_kernel = t_k / reps;
     if (kernel_bytes) *kernel_bytes = fforce_bytes(D);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_minresext(cpsgpu_dirac d, double *psi, const double *phi, double *const *v, double *const *vm,
+                     int degree, double *error) {
+  return guarded([&] {
+    if (!d || !psi || !phi || (degree > 0 && (!v || !vm))) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (degree < 0 || degree > 16) throw Error(CPSGPU_ERR_ARG, "degree must be in [0, 16]");
+    for (int k = 0; k < degree; k++)
+      if (!v[k] || !vm[k]) throw Error(CPSGPU_ERR_ARG, "null basis vector");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    Field fpsi(PREC_DOUBLE, L.vh, D.ls, 1), fphi(PREC_DOUBLE, L.vh, D.ls, 1);
+    upload(L, fphi, &phi, 1);
+    std::vector<Field> fv(degree), fvm(degree);
+    for (int k = 0; k < degree; k++) {
+      fv[k].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      fvm[k].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      const double *h = v[k];
+      upload(L, fv[k], &h, 1);
+    }
+    minresext(D, fpsi, fphi, fv, fvm, error);
+    download(L, fpsi, &psi, 1);
+    for (int k = 0; k < degree; k++) {
+      double *h = v[k], *hm = vm[k];
+      download(L, fv[k], &h, 1);
+      download(L, fvm[k], &hm, 1);
+    }
     return CPSGPU_OK;
   });
 }

@@ -1,9 +1,10 @@
-// BiCGstab(n) on MatPc: DiracOpWilsonTypes::BiCGstab (bicgstab.C:35-229),
-// step for step, with every vector on the device.  The solver's complex
-// scalars (rho, alpha, omega, tau, gamma) are the reference's short host
-// recurrences; each global dot product <a, b> = sum conj(a) b
-// (compDotProduct, vector_util.C:889-903) is a device reduction read back
-// by the host, so the loop is host-driven (a few reductions per MatPc).
+// Host-driven Krylov routines with every vector on the device:
+//   BiCGstab(n) on MatPc: DiracOpWilsonTypes::BiCGstab (bicgstab.C:35-229);
+//   the chronological initial guess DiracOp::MinResExt (minresext.C:30-150).
+// Their complex scalars (rho, alpha, omega, tau, gamma; the small Gram
+// matrix) are the reference's short host computations, step for step; each
+// global dot product <a, b> = sum conj(a) b (compDotProduct,
+// vector_util.C:889-903) is a device reduction read back by the host.
 #include <complex>
 #include <vector>
 
@@ -86,6 +87,15 @@ struct Ctx {
     launch_counter()++;
   }
   void matpc(Field &out, const Field &in) { op_matpc(D, PREC_DOUBLE, out.view(), in.view(), 0, w, nullptr, 0, 0); }
+  // out = MatPcDagMatPc in; returns |MatPc in|^2
+  double mdagm(Field &out, const Field &in) {
+    CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
+    op_mdagm(D, PREC_DOUBLE, out.view(), in.view(), w, st, RED_STORE);
+    double s = 0.0;
+    CPSGPU_CUDA(cudaMemcpyAsync(&s, st->sum, sizeof(s), cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return s;
+  }
 };
 
 }  // namespace
@@ -168,6 +178,68 @@ int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, do
   if (converged && true_res) *true_res = std::sqrt(sigma[0]);
   CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
   return k;
+}
+
+void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
+               double *error) {
+  const int degree = (int)v.size();
+  Lattice &L = *D.lat;
+  if (degree == 0) {  // no guess requested: psi = 0
+    launch_zero(L.stream, psi);
+    if (error) *error = 1.0;
+    return;
+  }
+  if (degree > 16) throw Error(-1, "MinResExt: at most 16 previous solutions");
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  std::vector<std::vector<cd>> G(degree, std::vector<cd>(degree));
+  std::vector<cd> a(degree), b(degree);
+  cd xp;
+  // orthonormalise the basis
+  for (int i = 0; i < degree; i++) {
+    launch_scale(L.stream, 1.0 / std::sqrt(c.norm2(v[i])), v[i].view());
+    for (int j = i + 1; j < degree; j++) {
+      xp = c.dot(v[i], v[j]);
+      c.caxpy(v[j], -xp, v[i], v[j]);
+    }
+  }
+  for (int i = 0; i < degree; i++) {
+    b[i] = c.dot(v[i], phi);
+    G[i][i] = cd(c.mdagm(vm[i], v[i]), 0.0);
+  }
+  for (int j = 0; j < degree; j++)
+    for (int k = j + 1; k < degree; k++) {
+      G[j][k] = c.dot(v[j], vm[k]);
+      G[k][j] = std::conj(G[j][k]);
+    }
+  // Gauss-Jordan elimination with the reference's (diagonal) pivoting
+  for (int i = 0; i < degree; i++) {
+    int k = i;
+    for (int j = i + 1; j < degree; j++)
+      if (std::abs(G[j][j]) > std::abs(G[k][k])) k = j;
+    if (k != i) {
+      std::swap(b[k], b[i]);
+      std::swap(G[k], G[i]);
+    }
+    for (int j = i + 1; j < degree; j++) {
+      xp = G[j][i] / G[i][i];
+      b[j] -= xp * b[i];
+      for (int kk = 0; kk < degree; kk++) G[j][kk] -= xp * G[i][kk];
+    }
+  }
+  Field r(PREC_DOUBLE, L.vh, D.ls, 1);
+  launch_zero(L.stream, psi);
+  CPSGPU_CUDA(cudaMemcpyAsync(r.data.ptr, phi.data.ptr, r.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+  for (int i = degree - 1; i >= 0; i--) {
+    a[i] = 0.0;
+    for (int j = i + 1; j < degree; j++) a[i] += G[i][j] * a[j];
+    a[i] = (b[i] - a[i]) / G[i][i];
+    c.caxpy(psi, a[i], v[i], psi);
+    c.caxpy(r, -a[i], vm[i], r);
+  }
+  if (error) *error = std::sqrt(c.norm2(r) / c.norm2(phi));
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
 }
 
 }  // namespace cpsgpu

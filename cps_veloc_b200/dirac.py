@@ -307,6 +307,40 @@ class _DiracOp:
                                                   1 if force_measure else 0, C.byref(fa)))
         return fa.L1, fa.L2, fa.Linf
 
+    def MinResExt(self, psi, phi, v, vm):
+        """DiracOp::MinResExt: psi (updated in place) = the chronological guess
+        from the previous solutions v (orthonormalised in place); vm[i] =
+        MatPcDagMatPc v[i]; returns |phi - A psi| / |phi|"""
+        phi = self._vec(phi)
+        _inplace(psi, self.f_size)
+        for x in list(v) + list(vm):
+            _inplace(x, self.f_size)
+        if len(v) != len(vm):
+            raise ValueError("v and vm must have the same length")
+        n = max(1, len(v))
+        pv = (A._dp * n)(*[dptr(x) for x in v])
+        pm = (A._dp * n)(*[dptr(x) for x in vm])
+        err = C.c_double()
+        check(lib().cpsgpu_minresext(self._h, dptr(psi), dptr(phi), pv, pm, len(v), C.byref(err)))
+        return err.value
+
+    def FmatEvlInv(self, f_out, f_in, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE):
+        """Fwilson / FdwfBase::FmatEvlInv (f_dwf_base.C:189-214): InvCg of
+        MatPcDagMatPc f_out = f_in from the guess in f_out; returns
+        (iterations, true_res) as the reference returns iter and sets
+        cg_arg->true_rsd"""
+        r = self.InvCg(f_out, f_in, stop_rsd=stop_rsd, max_num_iter=max_num_iter, precision=precision)
+        return r.iterations, r.true_res
+
+    def FmatEvlMInv(self, f_out, f_in, shift, stop_rsd, type_=A.MS_MULTI, alpha=None, precision=A.DOUBLE):
+        """FdwfBase::FmatEvlMInv (f_dwf_base.C:232-275): MInvCG with the source
+        norm computed here and each shift's stop_rsd; returns (iterations,
+        true_rsd per shift) as the reference writes cg_arg[s]->true_rsd"""
+        f_in = self._vec(f_in)
+        rs = np.array(stop_rsd, dtype=np.float64).copy()
+        k = self.MInvCG(f_out, f_in, float(f_in @ f_in), shift, rs, type=type_, alpha=alpha, precision=precision)
+        return k, rs
+
     def BiCGstab(self, psi, chi, n=1, chi_norm=0.0, stop_rsd=1e-8, max_num_iter=10000):
         """DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res) on MatPc:
         psi (initial guess) updated in place; returns (k, true_res) as the

@@ -288,6 +288,13 @@ int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *con
  * (ms per call, ms of the force kernel alone, its algorithmic bytes). */
 int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes);
 
+/* DiracOp::MinResExt(psi, phi, v, vm, degree) (minresext.C:30-150): the
+ * chronological initial guess psi for MatPcDagMatPc psi = phi from degree
+ * previous solutions v[] (orthonormalised in place, as the reference does),
+ * vm[i] = MatPcDagMatPc v[i] written; *error = |phi - A psi| / |phi| (the
+ * reference prints it).  degree 0: psi = 0. */
+int cpsgpu_minresext(cpsgpu_dirac d, double *psi, const double *phi, double *const *v, double *const *vm,
+                     int degree, double *error);
 /* DiracOpWilsonTypes::BiCGstab(psi, chi, chi_norm, n, true_res)
  * (bicgstab.C:35-229): BiCGstab(n) on MatPc itself (not the normal
  * equations), psi the initial guess, stop |r|^2 < stop_rsd^2 chi_norm with

@@ -115,6 +115,9 @@ def load_oracle() -> C.CDLL:
         L.orc_mobius_matinv.argtypes = [g, m, _dp, _dp, _dp, d, d, i, _dp]
         L.orc_bicgstab.argtypes = [MATPC_FN, C.c_void_p, C.c_long, _dp, _dp, d, i, d, i, _dp]
         L.orc_bicgstab.restype = i
+        L.orc_minresext.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), i,
+                                    _dp]
+        L.orc_minresext.restype = None
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

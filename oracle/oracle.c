@@ -912,3 +912,72 @@ void orc_fforce(const orc_geom *g, double *mom, const double *u, const double *v
   out[1] = sqrt(L2 / (4.0 * vol));
   out[2] = Linf;
 }
+
+/* ---------------------------------------------------------------------- */
+/* chronological initial guess                                             */
+/* ---------------------------------------------------------------------- */
+/* DiracOp::MinResExt (d_op_base/comsrc/minresext.C:30-150), step for step:
+ * orthonormalise the previous solutions v[] in place, vm[i] = A v[i] with
+ * A = MatPcDagMatPc, G = v^dag A v, b = v^dag phi, Gauss-Jordan with the
+ * reference's diagonal pivoting, then psi = sum a_i v_i; *error =
+ * |phi - A psi| / |phi|.  degree 0: psi = 0. */
+void orc_minresext(orc_mdagm_fn op, void *ctx, long n, double *psi, const double *phi, double **v, double **vm,
+                   int degree, double *error) {
+  if (degree <= 0) {
+    memset(psi, 0, sizeof(double) * n);
+    if (error) *error = 1.0;
+    return;
+  }
+  cplx G[16][16], a[16], b[16], xp;
+  for (int i = 0; i < degree; i++) {
+    const double s = 1.0 / sqrt(norm2(v[i], n));
+    for (long k = 0; k < n; k++) v[i][k] *= s;
+    for (int j = i + 1; j < degree; j++) {
+      xp = cdot(v[i], v[j], n);
+      caxpy(v[j], -xp, v[i], v[j], n);
+    }
+  }
+  for (int i = 0; i < degree; i++) {
+    double dot = 0.0;
+    b[i] = cdot(v[i], phi, n);
+    op(ctx, vm[i], v[i], &dot);
+    G[i][i] = dot;
+  }
+  for (int j = 0; j < degree; j++)
+    for (int k = j + 1; k < degree; k++) {
+      G[j][k] = cdot(v[j], vm[k], n);
+      G[k][j] = conj(G[j][k]);
+    }
+  for (int i = 0; i < degree; i++) {
+    int k = i;
+    for (int j = i + 1; j < degree; j++)
+      if (cabs(G[j][j]) > cabs(G[k][k])) k = j;
+    if (k != i) {
+      xp = b[k];
+      b[k] = b[i];
+      b[i] = xp;
+      for (int j = 0; j < degree; j++) {
+        xp = G[k][j];
+        G[k][j] = G[i][j];
+        G[i][j] = xp;
+      }
+    }
+    for (int j = i + 1; j < degree; j++) {
+      xp = G[j][i] / G[i][i];
+      b[j] -= xp * b[i];
+      for (int kk = 0; kk < degree; kk++) G[j][kk] -= xp * G[i][kk];
+    }
+  }
+  double *r = malloc(sizeof(double) * n);
+  memset(psi, 0, sizeof(double) * n);
+  memcpy(r, phi, sizeof(double) * n);
+  for (int i = degree - 1; i >= 0; i--) {
+    a[i] = 0.0;
+    for (int j = i + 1; j < degree; j++) a[i] += G[i][j] * a[j];
+    a[i] = (b[i] - a[i]) / G[i][i];
+    caxpy(psi, a[i], v[i], psi, n);
+    caxpy(r, -a[i], vm[i], r, n);
+  }
+  if (error) *error = sqrt(norm2(r, n) / norm2(phi, n));
+  free(r);
+}

@@ -118,6 +118,12 @@ int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double
 int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
                       double mass, double stop_rsd, int max_num_iter, double *true_res);
 
+/* DiracOp::MinResExt (minresext.C): the chronological initial guess over an
+ * MatPcDagMatPc callback; v[] is orthonormalised in place, vm[i] = A v[i].
+ * At most 16 previous solutions. */
+void orc_minresext(orc_mdagm_fn op, void *ctx, long n, double *psi, const double *phi, double **v, double **vm,
+                   int degree, double *error);
+
 /* HMC fermion force (Fwilson / FdwfBase::EvolveMomFforce): sprojTr, the
  * per-link matrix steps and the whole force loop; see oracle.c. */
 void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w, int nblk, int v_stride,

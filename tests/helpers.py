@@ -143,6 +143,18 @@ class OracleOps:
                               C.byref(sh) if sh is not None else None)
         return sol, it, tr.value
 
+    def minresext(self, kind, phi, v, mass=0.0, kappa=0.0):
+        """DiracOp::MinResExt: returns (psi, v orthonormalised, vm, error)"""
+        v = [np.ascontiguousarray(x).copy() for x in v]
+        vm = [np.zeros(self.n) for _ in v]
+        psi = np.zeros(self.n)
+        err = C.c_double()
+        pv = (C.POINTER(C.c_double) * max(1, len(v)))(*[p(x) for x in v])
+        pm = (C.POINTER(C.c_double) * max(1, len(v)))(*[p(x) for x in vm])
+        self.O.orc_minresext(self._op(kind, mass, kappa), None, self.n, p(psi), p(np.ascontiguousarray(phi)), pv,
+                             pm, len(v), C.byref(err))
+        return psi, v, vm, err.value
+
     def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
         """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,
         d_op_dwf.C:682-733): v1 = (chi, D chi), v2 = (psi, D^dag psi) with

@@ -276,3 +276,57 @@ def test_bicgstab_zero_source_and_argument_checks(oracle):
         D.BiCGstab(x, np.ones(D.f_size), n=11)  # n_max = 10 (bicgstab.C:67-70)
     k, tr = D.BiCGstab(x, gen_gaussian(D.f_size, seed=165), n=2, stop_rsd=1e-14, max_num_iter=4)
     assert k == 5 and tr == 0.0
+
+
+@pytest.mark.parametrize("kind,L,ls,degree", [("wilson", (4, 4, 4, 8), 1, 4), ("dwf", (4, 4, 4, 8), 8, 3),
+                                              ("mobius", (4, 4, 4, 4), 8, 2), ("dwf", (4, 4, 4, 4), 4, 0)])
+def test_minresext_matches_oracle(oracle, kind, L, ls, degree):
+    """DiracOp::MinResExt (minresext.C:30-150) against the oracle: the same
+    guess, the same orthonormalised basis and A v, the same residual."""
+    mass = 0.1
+    u = gen_gauge(L, seed=171)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    if kind == "wilson":
+        D = DiracOpWilson(lat, mass=mass)
+    elif kind == "dwf":
+        D = DiracOpDwf(lat, mass=mass, ls=ls)
+    else:
+        D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    ops = OracleOps(oracle, L, u, ls=ls, b=1.5, c=0.5)
+    phi = gen_gaussian(D.f_size, seed=172)
+    basis = [gen_gaussian(D.f_size, seed=173 + k) for k in range(degree)]
+    po, vo, vmo, eo = ops.minresext(kind, phi, basis, mass=mass, kappa=D.kappa)
+    psi = np.ones(D.f_size)
+    v = [b.copy() for b in basis]
+    vm = [np.zeros(D.f_size) for _ in basis]
+    err = D.MinResExt(psi, phi, v, vm)
+    if degree == 0:
+        assert not psi.any()
+        return
+    assert rel(psi, po) < 1e-11 and abs(err - eo) < 1e-11 * eo
+    for k in range(degree):
+        assert rel(v[k], vo[k]) < 1e-12 and rel(vm[k], vmo[k]) < 1e-12
+
+
+def test_fmatevl_wrappers(oracle):
+    """FmatEvlInv / FmatEvlMInv (f_dwf_base.C:189-275): the Lattice-level
+    entries the HMC calls, over InvCg and MInvCG."""
+    L, ls, mass = (4, 4, 4, 8), 8, 0.1
+    u = gen_gauge(L, seed=181)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    b = gen_gaussian(D.f_size, seed=182)
+    x = np.zeros(D.f_size)
+    it, tr = D.FmatEvlInv(x, b, stop_rsd=1e-11)
+    xo, ito, _ = ops.invcg("dwf", b, mass=mass, stop_rsd=1e-11)
+    assert abs(it - ito) <= 1 and tr <= 1e-11 and rel(x, xo) < 1e-9
+    shifts = [0.0, 0.05, 0.5]
+    outs = [np.zeros(D.f_size) for _ in shifts]
+    k, rs = D.FmatEvlMInv(outs, b, shifts, [1e-10] * 3)
+    for s_, o in zip(shifts, outs):
+        y, _ = ops.dwf_mdagm(o, mass)
+        assert rel(y + s_ * o, b) < 1e-9
+    assert k > 1 and len(rs) == 3

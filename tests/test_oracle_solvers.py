@@ -153,3 +153,25 @@ def test_bicgstab_zero_source_and_no_convergence(oracle):
     chi = gen_gaussian(ops.n, seed=44)
     psi, k, tr = ops.bicgstab("wilson", chi, n=2, kappa=0.12, stop_rsd=1e-14, max_num_iter=4)
     assert k == 5 and tr == 0.0  # two sweeps of n = 2, true_res untouched
+
+
+@pytest.mark.parametrize("kind", ["wilson", "dwf"])
+def test_minresext_properties(oracle, kind):
+    """DiracOp::MinResExt (minresext.C): the basis comes back orthonormal,
+    vm[i] = A v[i], and a basis holding the exact solution gives it back."""
+    L = (4, 4, 2, 4)
+    ls = 1 if kind == "wilson" else 4
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=51), ls=ls)
+    phi = gen_gaussian(ops.n, seed=52)
+    x, _, _ = ops.invcg(kind, phi, mass=0.1, kappa=0.12, stop_rsd=1e-13)
+    basis = [gen_gaussian(ops.n, seed=53), 3.0 * x + 0.1 * gen_gaussian(ops.n, seed=54), x]
+    psi, v, vm, err = ops.minresext(kind, phi, basis, mass=0.1, kappa=0.12)
+    assert rel(psi, x) < 1e-10 and err < 1e-10
+    for i in range(3):
+        for j in range(3):
+            d = np.dot(v[i], v[j])  # real part of the complex inner product
+            assert abs(d - (i == j)) < 1e-12
+    y, _ = (ops.wilson_mdagm(v[1], 0.12) if kind == "wilson" else ops.dwf_mdagm(v[1], 0.1))
+    assert rel(vm[1], y) < 1e-14
+    psi0, _, _, e0 = ops.minresext(kind, phi, [], mass=0.1, kappa=0.12)
+    assert not psi0.any()
