@@ -582,7 +582,7 @@ namespace {
 ForceVecs &force_vecs(cpsgpu_dirac d, const double *chi) {
   Dirac &D = *d->D;
   Lattice &L = *D.lat;
-  if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+  if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
   if (!d->fv) d->fv.reset(new ForceVecs());
   ensure_field(d->in[PREC_DOUBLE], PREC_DOUBLE, L.vh, D.ls, 1);
   upload(L, d->in[PREC_DOUBLE], &chi, 1);
@@ -598,7 +598,10 @@ int cpsgpu_calc_hmd_force_vecs(cpsgpu_dirac d, double *f_out, double *f_in, cons
     ForceVecs &fv = force_vecs(d, chi);
     Lattice &L = *d->D->lat;
     const size_t half = (size_t)24 * L.vh * d->D->ls;
-    double *o1 = f_out, *e1 = f_out + half, *o2 = f_in, *e2 = f_in + half;
+    // WILSON order of the halves: [odd][even] (Wilson, DWF), [even][odd] (Mobius)
+    const bool mob = d->D->kind == KIND_MOBIUS;
+    double *o1 = mob ? f_out + half : f_out, *e1 = mob ? f_out : f_out + half;
+    double *o2 = mob ? f_in + half : f_in, *e2 = mob ? f_in : f_in + half;
     download(L, fv.v1o, &o1, 1);
     download(L, fv.v1e, &e1, 1);
     download(L, fv.v2o, &o2, 1);
@@ -639,7 +642,7 @@ int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *con
     need_gauge(d);
     Dirac &D = *d->D;
     Lattice &L = *D.lat;
-    if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+    if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
     const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
     d->mom.ensure(2 * bytes);
     double *m = d->mom.as<double>(), *tmp = m + bytes / sizeof(double);
@@ -674,7 +677,7 @@ int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_ke
     need_gauge(d);
     Dirac &D = *d->D;
     Lattice &L = *D.lat;
-    if (D.kind == KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for Wilson and DWF operators");
+    if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
     if (!d->fv) d->fv.reset(new ForceVecs());
     Field chi(PREC_DOUBLE, L.vh, D.ls, 1);
     std::vector<double> h((size_t)24 * L.vh * D.ls);

@@ -194,6 +194,7 @@ void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const Spin
 // force loop of EvolveMomFforce on a CANONICAL momentum field in device memory
 struct ForceVecs {
   Field v1o, v1e, v2o, v2e;
+  Field t1, t2;  // Mobius temporaries
   OpWork w;
 };
 void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi);

@@ -42,7 +42,8 @@ struct ForceParams {
   long vh;
   int ls;
   double bc[4];
-  double dt;
+  double scale;    // mom += scale TrLessAntiHerm(U T), negated where x+mu wraps an antiperiodic direction
+  int mobius;      // halves hold one 4D parity in every slice (Mobius) instead of the 5D parity (DWF)
 };
 
 struct ForceViews {
@@ -51,10 +52,13 @@ struct ForceViews {
   double *mom;                    // CANONICAL [site][mu][18]
 };
 
-// the half of a full field that holds 4D parity p in slice s: the odd part
-// holds parity (s + 1) % 2 (convert.C:704-760; ls = 1: the odd sites)
-__device__ __forceinline__ const SpinorView &part(const SpinorView &o, const SpinorView &e, int p, int s) {
-  return ((p + s) & 1) ? o : e;
+// the half of a full field that holds 4D parity p in slice s: for Wilson
+// and DWF the odd part holds parity (s + 1) % 2 (convert.C:704-760; ls = 1:
+// the odd sites); for Mobius each half holds one 4D parity in every slice
+// (convert.C:797-851)
+__device__ __forceinline__ const SpinorView &part(const SpinorView &o, const SpinorView &e, int p, int s,
+                                                  int mobius) {
+  return (mobius ? p : ((p + s) & 1)) ? o : e;
 }
 
 // T += sum over the two projected spins of h_a (x) conj(h_w)
@@ -85,12 +89,12 @@ __device__ __forceinline__ void force_trace(const ForceParams &fp, const ForceVi
   for (int s = s0; s < fp.ls; s += ds) {
     double a[24], w[24];
     // sprojTr(1 - g_mu)[v1(x+mu), v2(x)]
-    SpinorIO<PREC_DOUBLE>::load(part(v.v1o, v.v1e, q, s), s, j, a);
-    SpinorIO<PREC_DOUBLE>::load(part(v.v2o, v.v2e, p, s), s, i, w);
+    SpinorIO<PREC_DOUBLE>::load(part(v.v1o, v.v1e, q, s, fp.mobius), s, j, a);
+    SpinorIO<PREC_DOUBLE>::load(part(v.v2o, v.v2e, p, s, fp.mobius), s, i, w);
     outer_acc(T, project(a, MU, -1.0), project(w, MU, -1.0));
     // sprojTr(1 + g_mu)[v2(x+mu), v1(x)]
-    SpinorIO<PREC_DOUBLE>::load(part(v.v2o, v.v2e, q, s), s, j, a);
-    SpinorIO<PREC_DOUBLE>::load(part(v.v1o, v.v1e, p, s), s, i, w);
+    SpinorIO<PREC_DOUBLE>::load(part(v.v2o, v.v2e, q, s, fp.mobius), s, j, a);
+    SpinorIO<PREC_DOUBLE>::load(part(v.v1o, v.v1e, p, s, fp.mobius), s, i, w);
     outer_acc(T, project(a, MU, 1.0), project(w, MU, 1.0));
   }
 }
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(FORCE_TPB, 3) fforce_kernel(const ForceParams 
       }
     // 1/2 (F - F^dag), traceless, times coeff (Matrix::TrLessAntiHermMatrix)
     const double bcmu = mu == 0 ? fp.bc[0] : mu == 1 ? fp.bc[1] : mu == 2 ? fp.bc[2] : fp.bc[3];
-    const double coeff = (wrap && bcmu < 0) ? 2.0 * fp.dt : -2.0 * fp.dt;
+    const double coeff = (wrap && bcmu < 0) ? -fp.scale : fp.scale;
     cplx<double> A[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
@@ -343,10 +347,27 @@ void force_arg_of(Lattice &L, const double *res, double out[3]) {
 }  // namespace
 
 void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi) {
-  if (D.kind == KIND_MOBIUS) throw Error(-1, "CalcHmdForceVecs: Wilson and DWF operators only");
+  if (D.kind == KIND_MOBIUS && D.cplx) throw Error(-1, "the fermion force is built for real Mobius b, c");
   const Lattice &L = *D.lat;
-  for (Field *f : {&fv.v1o, &fv.v1e, &fv.v2o, &fv.v2e})
+  for (Field *f : {&fv.v1o, &fv.v1e, &fv.v2o, &fv.v2e, &fv.t1, &fv.t2})
     if (f->data.ptr == nullptr || f->vh != L.vh || f->ls != D.ls) f->create(PREC_DOUBLE, L.vh, D.ls, 1);
+  if (D.kind == KIND_MOBIUS) {
+    // Fmobius::EvolveMomFforce(mom, frm, mass, step) (f_mobius.C:847-887):
+    // phi1 = MatPc frm, phi2 = frm, then DiracOpMobius::CalcHmdForceVecs(v1,
+    // v2, phi1, phi2) for SYM2 (d_op_mobius.C:1015-1100):
+    //   phi2 <- M5^-1 phi2;  v1 = (M5^-dag Dslash4^dag phi1, phi1);
+    //   v2 = (Booee M5^-1 Dslash4 phi2, Booee phi2)   [even half, odd half]
+    // (the reference overwrites the caller's frm with M5^-1 frm; t2 holds it here)
+    op_matpc(D, PREC_DOUBLE, fv.v1o.view(), chi, 0, fv.w, nullptr, 0, 0);  // phi1
+    op_mobius_m5inv(D, PREC_DOUBLE, fv.t2.view(), chi, 0);                 // phi2
+    op_mobius_dslash4(D, PREC_DOUBLE, fv.t1.view(), fv.t2.view(), 1, 0, fv.w);
+    op_mobius_m5inv(D, PREC_DOUBLE, fv.v1e.view(), fv.t1.view(), 0);
+    launch_mix(D, PREC_DOUBLE, D.mixB.as<double>(), fv.v1e.view(), fv.v2e.view());
+    launch_mix(D, PREC_DOUBLE, D.mixB.as<double>(), fv.t2.view(), fv.v2o.view());
+    op_mobius_dslash4(D, PREC_DOUBLE, fv.t1.view(), fv.v1o.view(), 1, 1, fv.w);
+    op_mobius_m5inv(D, PREC_DOUBLE, fv.v1e.view(), fv.t1.view(), 1);
+    return;
+  }
   // f_out = (chi, D chi)
   CPSGPU_CUDA(cudaMemcpyAsync(fv.v1o.data.ptr, chi.data, fv.v1o.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
   op_dslash(D, PREC_DOUBLE, fv.v1e.view(), fv.v1o.view(), 1, 0);
@@ -357,6 +378,7 @@ void calc_hmd_force_vecs(const Dirac &D, ForceVecs &fv, const SpinorView &chi) {
 }
 
 void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, double out[3]) {
+  const bool mob = D.kind == KIND_MOBIUS;
   Lattice &L = *D.lat;
   ForceParams fp;
   for (int k = 0; k < 4; k++) {
@@ -366,12 +388,16 @@ void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, 
   fp.hx = L.L[0] / 2;
   fp.vh = L.vh;
   fp.ls = D.ls;
-  fp.dt = dt;
+  // Fwilson / FdwfBase: coeff = -2 dt.  Fmobius: FforceWilsonType with
+  // coef = -step adds -coef TrLessAntiHerm(U T) with the roles of v1 and v2
+  // exchanged in T (fforce_wilson_type.C do_site_force)
+  fp.scale = mob ? dt : -2.0 * dt;
+  fp.mobius = mob ? 1 : 0;
   ForceViews v;
-  v.v1o = fv.v1o.view();
-  v.v1e = fv.v1e.view();
-  v.v2o = fv.v2o.view();
-  v.v2e = fv.v2e.view();
+  v.v1o = (mob ? fv.v2o : fv.v1o).view();
+  v.v1e = (mob ? fv.v2e : fv.v1e).view();
+  v.v2o = (mob ? fv.v1o : fv.v2o).view();
+  v.v2e = (mob ? fv.v1e : fv.v2e).view();
   v.U.data = L.gD18.ptr;
   v.U.vh = L.vh;
   v.mom = mom;

@@ -267,14 +267,20 @@ typedef struct {
 /* DiracOpWilson / DiracOpDwf::CalcHmdForceVecs(chi) (d_op_wilson.C:466-507,
  * d_op_dwf.C:682-733): f_out = (chi, D chi), f_in = (-kappa^2 MatPc chi,
  * D^dag of it), full fields in WILSON order ([odd half][even half], before
- * the reference's conversion to CANONICAL); chi is the odd half. */
+ * the reference's conversion to CANONICAL); chi is the odd half.
+ * Mobius (real b, c; SYM2): the vectors Fmobius::EvolveMomFforce builds,
+ * DiracOpMobius::CalcHmdForceVecs(f_out, f_in, MatPc chi, chi)
+ * (d_op_mobius.C:1015-1100, f_mobius.C:847-887), [even half][odd half];
+ * chi is left unchanged (the reference overwrites it with M5^-1 chi). */
 int cpsgpu_calc_hmd_force_vecs(cpsgpu_dirac d, double *f_out, double *f_in, const double *chi);
-/* Fwilson::EvolveMomFforce(mom, chi, mass, dt) (f_wilson.C:470-687) and
- * FdwfBase::EvolveMomFforce (f_dwf_base_force.C:41-300): mom += the fermion
- * force of the pseudofermion solution chi (odd half, WILSON order) for a
- * step dt; mom is the CANONICAL Matrix field [site][mu][3][3][re, im] with
- * the lexicographic site x + Lx (y + Ly (z + Lz t)).  The operator's own mass
- * plays the reference's mass argument.  Wilson and DWF handles only. */
+/* Fwilson::EvolveMomFforce(mom, chi, mass, dt) (f_wilson.C:470-687),
+ * FdwfBase::EvolveMomFforce (f_dwf_base_force.C:41-300) and
+ * Fmobius::EvolveMomFforce(mom, frm, mass, step_size) (f_mobius.C:847-887,
+ * FforceWilsonType): mom += the fermion force of the pseudofermion solution
+ * chi (the preconditioned half, WILSON order) for a step dt; mom is the
+ * CANONICAL Matrix field [site][mu][3][3][re, im] with the lexicographic site
+ * x + Lx (y + Ly (z + Lz t)).  The operator's own mass plays the reference's
+ * mass argument.  Mobius: real b, c (not zMobius). */
 int cpsgpu_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *chi, double dt, cpsgpu_force_arg *out);
 /* Fwilson / FdwfBase::RHMC_EvolveMomFforce(mom, sol, degree, isz, alpha,
  * mass, dt, sol_d, force_measure) (f_wilson.C:689-757, f_dwf_base.C:1424):

@@ -102,6 +102,8 @@ def load_oracle() -> C.CDLL:
             "orc_sproj_tr": [i, i, _dp, _dp, _dp, i, i, i],
             "orc_force_matrix": [_dp, _dp, _dp, _dp, d],
             "orc_fforce": [g, _dp, _dp, _dp, _dp, d, _dp],
+            "orc_mobius_booee": [g, m, _dp, _dp, d],
+            "orc_fforce_wilson_type": [g, _dp, _dp, _dp, _dp, d, _dp],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a
@@ -154,6 +156,12 @@ def load_reference() -> C.CDLL:
             "ref_zmobius_mdag": [_dp, _dp, _dp, d],
             "ref_zmobius_mdagm": [_dp, _dp, _dp, _dp, d],
             "ref_sproj_tr": [i, _dp, _dp, _dp, i, i, i],
+            "ref_mobius_dslash_4": [_dp, _dp, _dp, i, i, d],
+            "ref_mobius_m5inv": [_dp, _dp, d, i],
+            "ref_mobius_booee": [_dp, _dp, d],
+            "ref_mobius_kappa_dslash_5_plus": [_dp, _dp, d, i, d],
+            "ref_mobius_m": [_dp, _dp, _dp, d],
+            "ref_fforce_wilson_type": [_dp, _dp, _dp, _dp, i, d, _dp],
             "ref_force_matrix": [_dp, _dp, _dp, _dp, d],
         }
         for k, a in sig.items():

@@ -981,3 +981,69 @@ void orc_minresext(orc_mdagm_fn op, void *ctx, long n, double *psi, const double
   if (error) *error = sqrt(norm2(r, n) / norm2(phi, n));
   free(r);
 }
+
+/* mobius_Booee (d_op_mobius/noarch/mobius_dslash_4.C:40-88), dag 0:
+ * out(s) = b_s in(s) + the c-weighted fifth-direction hop of in (with the
+ * -mass wall terms, mobius_kappa_dslash_5_plus). */
+void orc_mobius_booee(const orc_geom *g, const orc_mobius *mp, double *out, const double *in, double mass) {
+  const long vh = vol_cb(g), slice = 12 * vh;
+  for (int s = 0; s < g->ls; s++)
+    for (long k = 0; k < slice; k++) fset(out, s * slice + k, mp->b[s] * fget(in, s * slice + k));
+  mobius_hop5_acc(g, g->ls, mp->c, out, in, mass, 0);
+}
+
+/* The force loop of FforceWilsonType::run (f_wilson_types/fforce_wilson_type.C,
+ * do_internal / do_surface with do_site_force), which Fmobius::EvolveMomFforce
+ * (f_mobius.C:749-846) calls on the Mobius force vectors: per link,
+ *   T = sum_s sprojTr(1 - g_mu)[v2(x+mu), v1(x)] + sprojTr(1 + g_mu)[v1(x+mu), v2(x)],
+ *   mom(x, mu) += -coef TrLessAntiHerm(U_mu(x) T),
+ * U carrying the boundary signs (Fmobius applies BondCond around it; here
+ * the sign is applied where x+mu wraps an antiperiodic direction).  v1, v2
+ * are full Mobius fields in their WILSON order: [even half][odd half], every
+ * slice holding the same 4D parity (convert.C:797-851).  out = ForceArg. */
+void orc_fforce_wilson_type(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2,
+                            double coef, double out[3]) {
+  const long vh = vol_cb(g), vol = 2 * vh;
+  double L1 = 0.0, L2 = 0.0, Linf = 0.0;
+  for (int mu = 0; mu < 4; mu++)
+    for (int t = 0; t < g->L[3]; t++)
+      for (int z = 0; z < g->L[2]; z++)
+        for (int y = 0; y < g->L[1]; y++)
+          for (int xx = 0; xx < g->L[0]; xx++) {
+            const int x[4] = {xx, y, z, t};
+            int xp[4] = {xx, y, z, t};
+            xp[mu] = (x[mu] + 1) % g->L[mu];
+            const double sign = (x[mu] + 1 == g->L[mu] && g->bc[mu] < 0) ? -1.0 : 1.0;
+            const int p = (xx + y + z + t) & 1, pp = 1 - p;
+            const long o0 = (p ? (long)g->ls * vh : 0) + cb_index(g, x);
+            const long p0 = (pp ? (long)g->ls * vh : 0) + cb_index(g, xp);
+            double T1[18] = {0}, T2[18] = {0}, tmp[18];
+            for (int s = 0; s < g->ls; s++) {
+              const long o = o0 + (long)s * vh, op = p0 + (long)s * vh;
+              orc_sproj_tr(mu, -1, tmp, v2 + 24 * op, v1 + 24 * o, 1, 0, 0);
+              for (int k = 0; k < 18; k++) T1[k] += tmp[k];
+              orc_sproj_tr(mu, +1, tmp, v1 + 24 * op, v2 + 24 * o, 1, 0, 0);
+              for (int k = 0; k < 18; k++) T2[k] += tmp[k];
+            }
+            for (int k = 0; k < 18; k++) T1[k] += T2[k];
+            const long gs = cb_index(g, x) + vh * p;
+            double U[18];
+            for (int i = 0; i < 3; i++)
+              for (int j = 0; j < 3; j++) {
+                const cplx e = sign * link(u, gs, mu, i, j);
+                U[2 * (3 * i + j)] = creal(e);
+                U[2 * (3 * i + j) + 1] = cimag(e);
+              }
+            double F[18], n;
+            orc_force_matrix(F, &n, U, T1, -coef);
+            double *m = mom + 18 * (4 * (xx + (long)g->L[0] * (y + (long)g->L[1] * (z + (long)g->L[2] * t))) + mu);
+            for (int k = 0; k < 18; k++) m[k] += F[k];
+            const double a = sqrt(n);
+            L1 += a;
+            L2 += n;
+            if (a > Linf) Linf = a;
+          }
+  out[0] = L1 / (4.0 * vol);
+  out[1] = sqrt(L2 / (4.0 * vol));
+  out[2] = Linf;
+}

@@ -131,6 +131,10 @@ void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w,
 void orc_force_matrix(double *f, double *norm, const double *U, const double *T, double coeff);
 void orc_fforce(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2, double dt,
                 double out[3]);
+/* mobius_Booee and the force loop Fmobius uses (FforceWilsonType::run) */
+void orc_mobius_booee(const orc_geom *g, const orc_mobius *mp, double *out, const double *in, double mass);
+void orc_fforce_wilson_type(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2,
+                            double coef, double out[3]);
 
 #ifdef __cplusplus
 }

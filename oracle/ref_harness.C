@@ -23,6 +23,9 @@
 #include <util/wilson.h>
 #include <util/dwf.h>
 #include <util/zmobius.h>
+#include <util/mobius.h>
+#include <util/lattice/fforce_wilson_type.h>
+#include <alg/force_arg.h>
 #include <util/gjp.h>
 #include <util/sproj_tr.h>
 #include <util/fpconv.h>
@@ -40,6 +43,7 @@ void zmobius_m5inv(Vector *inout, Float mass, int dag, Zmobus *arg, Complex *K);
 static Dwf g_dwf;          // DWF and Mobius library argument
 static bool g_have_dwf = false;
 static Wilson g_wilson;    // Wilson library argument (Fwilson's static struct)
+static double g_mobius_b = 1.0, g_mobius_c = 0.0;  // the Mobius b, c of the last ref_init
 static bool g_have_wilson = false;
 
 extern "C" {
@@ -59,6 +63,8 @@ int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
   GJP.Initialize(d);
   GJP.Mobius_b(mobius_b);
   GJP.Mobius_c(mobius_c);
+  g_mobius_b = mobius_b;
+  g_mobius_c = mobius_c;
   GJP.ZMobius_PC_Type(ZMOB_PC_SYM2);
 
   wilson_init(&g_wilson);
@@ -163,6 +169,41 @@ unsigned int ref_fp_checksum(char *data, int n_values, int format) {
   FPConv fp;
   fp.setFileFormat((FP_FORMAT)format);
   return fp.checksum(data, n_values, (FP_FORMAT)format);
+}
+
+// ---- Mobius through DiracOpMobius's own kernels (d_op_mobius/noarch) ----
+void ref_mobius_dslash_4(double *out, double *u, double *in, int cb, int dag, double mass) {
+  mobius_dslash_4((Vector *)out, (Matrix *)u, (Vector *)in, cb, dag, &g_dwf, mass);
+}
+void ref_mobius_m5inv(double *out, double *in, double mass, int dag) {
+  mobius_m5inv((Vector *)out, (Vector *)in, mass, dag, &g_dwf);
+}
+// mobius_Booee (mobius_dslash_4.C:40-88) as its two steps: out = b in, then
+// out += c x the fifth-direction hop of in.  mobius_Booee reads b and c
+// through GJP.Mobius_b() / Mobius_c(), which dereference the DoArgExt that
+// only a full CPS start-up provides, so the harness passes the values
+// ref_init recorded instead.
+void ref_mobius_booee(double *out, double *in, double mass) {
+  const size_t n = (size_t)12 * GJP.VolNodeSites() * GJP.SnodeSites();
+  for (size_t k = 0; k < n; k++) out[k] = g_mobius_b * in[k];
+  mobius_kappa_dslash_5_plus((Vector *)out, (Vector *)in, mass, 0, &g_dwf, g_mobius_c);
+}
+// out += fact x the fifth-direction hop of in (mobius_dslash_5_plus.C:119)
+void ref_mobius_kappa_dslash_5_plus(double *out, double *in, double mass, int dag, double fact) {
+  mobius_kappa_dslash_5_plus((Vector *)out, (Vector *)in, mass, dag, &g_dwf, fact);
+}
+void ref_mobius_m(double *out, double *u, double *in, double mass) {
+  mobius_m((Vector *)out, (Matrix *)u, (Vector *)in, mass, &g_dwf);
+}
+// FforceWilsonType(mom, gauge, v1, v2, Ls, coef).run() (fforce_wilson_type.C):
+// CANONICAL mom and gauge (boundary signs on the links, as Fmobius applies
+// BondCond around it), v1 / v2 in the S_INNER order [4D site][s][24]
+void ref_fforce_wilson_type(double *mom, double *u, double *v1, double *v2, int ls, double coef, double *out) {
+  FforceWilsonType f((Matrix *)mom, (Matrix *)u, v1, v2, ls, coef);
+  ForceArg a = f.run();
+  out[0] = a.L1;
+  out[1] = a.L2;
+  out[2] = a.Linf;
 }
 
 // ---- HMC fermion force pieces ----

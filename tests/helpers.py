@@ -17,6 +17,27 @@ def vh_of(L) -> int:
     return int(np.prod(L)) // 2
 
 
+def s_inner(v, L, ls, layout):
+    """A full WILSON-order fermion field in the S_INNER CANONICAL order
+    [lexicographic site][s][24] that FforceWilsonType reads
+    (Fconvert(S_INNER, CANONICAL)); layout "dwf" (Wilson/DWF halves [odd][even],
+    slice s of the odd half holding 4D parity (s+1)%2) or "mobius" ([even][odd],
+    one 4D parity per half)."""
+    lx, ly, lz, lt = L
+    vh = lx * ly * lz * lt // 2
+    t, z, y, x = np.meshgrid(*(np.arange(n) for n in (lt, lz, ly, lx)), indexing="ij")
+    x, y, z, t = (a.ravel() for a in (x, y, z, t))
+    par = (x + y + z + t) & 1
+    cb = x // 2 + (lx // 2) * (y + ly * (z + lz * t))
+    pos = np.empty((x.size, ls), dtype=np.int64)
+    for s in range(ls):
+        if layout == "dwf":
+            pos[:, s] = np.where(((par + s) & 1) == 1, 0, ls * vh) + s * vh + cb
+        else:
+            pos[:, s] = np.where(par == 1, ls * vh, 0) + s * vh + cb
+    return np.asarray(v).reshape(-1, 24)[pos.ravel()].ravel()
+
+
 class OracleOps:
     """The oracle's operators on one geometry (gauge field without signs)."""
 
@@ -167,6 +188,30 @@ class OracleOps:
             psi = -k5 * k5 * self.dwf_m(chi, mass, 0)
             rho, sigma = self.dwf_dslash(chi, mass, 1, 0), self.dwf_dslash(psi, mass, 1, 1)
         return np.concatenate([chi, rho]), np.concatenate([psi, sigma])
+
+    def mobius_booee(self, x, mass):
+        y = self.z()
+        self.O.orc_mobius_booee(C.byref(self.g), C.byref(self.mp), p(y), p(np.ascontiguousarray(x)), mass)
+        return y
+
+    def mobius_force_vecs(self, phi1, phi2, mass):
+        """DiracOpMobius::CalcHmdForceVecs(v1, v2, phi1, phi2), SYM2
+        (d_op_mobius.C:1015-1100): full fields [even half][odd half]"""
+        phi2 = self.mobius_m5inv(phi2, mass, 0)  # the reference overwrites phi2 with this
+        v2_e = self.mobius_booee(self.mobius_m5inv(self.mobius_dslash_4(phi2, mass, 1, 0), mass, 0), mass)
+        v2_o = self.mobius_booee(phi2, mass)
+        v1_e = self.mobius_m5inv(self.mobius_dslash_4(phi1, mass, 1, 1), mass, 1)
+        return np.concatenate([v1_e, phi1]), np.concatenate([v2_e, v2_o])
+
+    def mobius_fforce(self, frm, step, mass, mom=None):
+        """Fmobius::EvolveMomFforce(mom, frm, mass, step) (f_mobius.C:847-887):
+        phi1 = MatPc frm, phi2 = frm, FforceWilsonType with coef = -step"""
+        v1, v2 = self.mobius_force_vecs(self.mobius_m(frm, mass, 0), frm, mass)
+        vol = int(np.prod(self.L))
+        m = np.zeros(4 * vol * 18) if mom is None else np.ascontiguousarray(mom).copy()
+        out = np.zeros(3)
+        self.O.orc_fforce_wilson_type(C.byref(self.g), p(m), p(self.u), p(v1), p(v2), -step, p(out))
+        return m, tuple(out)
 
     def fforce(self, kind, chi, dt, mass=0.0, kappa=0.0, mom=None):
         """Fwilson / FdwfBase::EvolveMomFforce: returns (mom + force, (L1, L2, Linf))"""

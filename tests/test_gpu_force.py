@@ -49,11 +49,34 @@ def test_evolve_mom_fforce_matches_oracle(oracle, kind, L, ls, bc):
     assert rel(mom - mom0, 2 * (mo - mom0)) < 1e-12
 
 
-def test_force_rejects_mobius_and_bad_sizes(oracle):
+@pytest.mark.parametrize("L,ls,bc", [((4, 4, 4, 8), 8, (1, 1, 1, -1)), ((8, 4, 4, 4), 4, (-1, 1, 1, 1))])
+def test_mobius_force_matches_oracle(oracle, L, ls, bc):
+    """Fmobius::EvolveMomFforce (SYM2): the force vectors and the force."""
+    u = gen_gauge(L, seed=232)
+    lat = Lattice(L, bc)
+    lat.import_gauge(u)
+    mass = 0.05
+    D = DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc, b=1.5, c=0.5)
+    frm = gen_gaussian(D.f_size, seed=233)
+    f_out, f_in = D.CalcHmdForceVecs(frm)
+    v1, v2 = ops.mobius_force_vecs(ops.mobius_m(frm, mass, 0), frm, mass)
+    assert rel(f_out, v1) < 1e-13 and rel(f_in, v2) < 1e-13
+    mom0 = gen_gaussian(4 * int(np.prod(L)) * 18, seed=234)
+    mo, fo = ops.mobius_fforce(frm, 0.21, mass, mom=mom0)
+    mom = mom0.copy()
+    fg = D.EvolveMomFforce(mom, frm, 0.21)
+    assert rel(mom - mom0, mo - mom0) < 1e-12
+    assert np.allclose(fg, fo, rtol=1e-12, atol=0)
+
+
+def test_force_rejects_zmobius_and_bad_sizes(oracle):
     L = (4, 4, 4, 4)
     lat = Lattice(L)
     lat.import_gauge(gen_gauge(L, seed=226))
     D = DiracOpMobius(lat, mass=0.1, ls=4)
+    zb = np.array([1.5 + 0.1j] * 4)
+    D.set_zmobius(zb, zb - 1.0)
     with pytest.raises(A.CpsGpuError):
         D.EvolveMomFforce(np.zeros(4 * 256 * 18), np.zeros(D.f_size), 0.1)
     W = DiracOpWilson(lat, mass=0.1)

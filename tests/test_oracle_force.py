@@ -81,3 +81,30 @@ def test_force_accumulates_and_scales_with_dt(oracle):
     assert np.allclose(np.array(a2), 0.25 * np.array(a1), rtol=1e-13)
     fz, az = ops.fforce("wilson", np.zeros(ops.n), 1.0, kappa=0.12)
     assert not fz.any() and az == (0.0, 0.0, 0.0)
+
+
+def test_mobius_force_normalisation(oracle):
+    """Fmobius::EvolveMomFforce with SYM2 preconditioning: the force it adds is
+    the gradient of S = phi . (MatPc^dag MatPc)^-1 phi up to the factor
+    2 kappa_b^2, dS/deps = -2 kappa_b^2 sum <X, F>.  The reference applies
+    coef *= 2 kappa_b^2 only for the ORIG and SYM1 preconditionings
+    (f_mobius.C:818-823), and the library reproduces its SYM2 force as is."""
+    L, ls, mass = (4, 4, 2, 4), 4, 0.1
+    b, c, m5 = 1.5, 0.5, 1.8
+    u = gen_gauge(L, seed=217)
+    ops = OracleOps(oracle, L, u, ls=ls, b=b, c=c)
+    phi = gen_gaussian(ops.n, seed=218)
+    chi, _, _ = ops.invcg("mobius", phi, mass=mass, stop_rsd=1e-13)
+    F, _ = ops.mobius_fforce(chi, 1.0, mass)
+    Fm = (F[0::2] + 1j * F[1::2]).reshape(-1, 4, 3, 3)
+    X = _random_su3_algebra(np.random.default_rng(219), Fm.shape[0])
+
+    def S(eps):
+        o2 = OracleOps(oracle, L, _perturb(u, L, X, eps), ls=ls, b=b, c=c)
+        c2, _, _ = o2.invcg("mobius", phi, mass=mass, stop_rsd=1e-13)
+        return float(np.dot(c2, phi))
+
+    eps = 1e-5
+    dS = (S(eps) - S(-eps)) / (2 * eps)
+    kb = 1 / (2 * (b * (4 - m5) + 1))
+    assert abs(dS + 2 * kb * kb * np.sum((np.conj(X) * Fm).real)) < 1e-7 * abs(dS)

@@ -165,3 +165,67 @@ def test_force_matrix_steps_vs_reference(oracle, reference):
         # traceless and antihermitian
         m = fo[0::2].reshape(3, 3) + 1j * fo[1::2].reshape(3, 3)
         assert np.abs(m + m.conj().T).max() < 1e-15 and abs(np.trace(m)) < 1e-15
+
+
+def _canonical_signed(u, L, bc):
+    from cps_veloc_b200.dirac import StrOrd, gconvert
+    us = apply_bc_signs(u, L, bc)
+    gconvert(L, us, StrOrd.CANONICAL, StrOrd.WILSON)
+    return us
+
+
+def test_dwf_force_vs_reference_force_loop(oracle, reference):
+    """The oracle's force loop (orc_fforce) against the reference's own
+    FforceWilsonType::run (fforce_wilson_type.C) on the same DWF force
+    vectors: FforceWilsonType takes v1 and v2 in the other roles, the
+    signed links and coef = 2 dt."""
+    from helpers import s_inner
+    L, ls, mass, dt = (4, 4, 4, 4), 4, 0.1, 0.3
+    bc = (1, 1, 1, -1)
+    _ref_setup(reference, L, ls, bc)
+    u = gen_gauge(L, seed=241)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc)
+    chi = gen_gaussian(ops.n, seed=242)
+    mo, fo = ops.fforce("dwf", chi, dt, mass=mass)
+    v1, v2 = ops.force_vecs("dwf", chi, mass=mass)
+    mom, out = np.zeros(4 * 256 * 18), np.zeros(3)
+    reference.ref_fforce_wilson_type(p(mom), p(_canonical_signed(u, L, bc)), p(s_inner(v2, L, ls, "dwf")),
+                                     p(s_inner(v1, L, ls, "dwf")), ls, 2 * dt, p(out))
+    assert rel(mo, mom) < 1e-14 and np.allclose(fo, out, rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("L,ls,mass,b,c", [((4, 4, 4, 4), 4, 0.1, 1.5, 0.5), ((4, 2, 2, 4), 6, 0.02, 2.0, 1.0)])
+def test_mobius_force_vs_reference(oracle, reference, L, ls, mass, b, c):
+    """Fmobius::EvolveMomFforce (f_mobius.C:847-887) composed from the
+    reference's own kernels (mobius_m, mobius_m5inv, mobius_dslash_4, the
+    two steps of mobius_Booee) and FforceWilsonType::run, against the
+    oracle's restatement (OracleOps.mobius_fforce)."""
+    from helpers import s_inner
+    bc = (1, 1, 1, -1)
+    _ref_setup(reference, L, ls, bc, b=b, c=c)
+    u = gen_gauge(L, seed=243)
+    us = apply_bc_signs(u, L, bc)
+    ops = OracleOps(oracle, L, u, ls=ls, bc=bc, b=b, c=c)
+    n = ops.n
+    x = gen_gaussian(n, seed=244)
+    y = np.zeros(n)
+    reference.ref_mobius_booee(p(y), p(x), mass)
+    assert rel(ops.mobius_booee(x, mass), y) < TOL
+    frm, step = gen_gaussian(n, seed=245), 0.37
+
+    def ref(fn, *a):
+        out = np.zeros(n)
+        fn(p(out), *a)
+        return out
+
+    phi1 = ref(reference.ref_mobius_m, p(us), p(frm), mass)
+    phi2 = ref(reference.ref_mobius_m5inv, p(frm), mass, 0)
+    tmp2 = ref(reference.ref_mobius_m5inv, p(ref(reference.ref_mobius_dslash_4, p(us), p(phi2), 1, 0, mass)), mass, 0)
+    v2 = np.concatenate([ref(reference.ref_mobius_booee, p(tmp2), mass), ref(reference.ref_mobius_booee, p(phi2), mass)])
+    tmp4 = ref(reference.ref_mobius_dslash_4, p(us), p(phi1), 1, 1, mass)
+    v1 = np.concatenate([ref(reference.ref_mobius_m5inv, p(tmp4), mass, 1), phi1])
+    mom, out = np.zeros(4 * int(np.prod(L)) * 18), np.zeros(3)
+    reference.ref_fforce_wilson_type(p(mom), p(_canonical_signed(u, L, bc)), p(s_inner(v1, L, ls, "mobius")),
+                                     p(s_inner(v2, L, ls, "mobius")), ls, -step, p(out))
+    mo, fo = ops.mobius_fforce(frm, step, mass)
+    assert rel(mo, mom) < 1e-13 and np.allclose(fo, out, rtol=1e-12, atol=0)
