@@ -100,15 +100,18 @@ __device__ __forceinline__ void force_trace(const ForceParams &fp, const ForceVi
 }
 
 // Block = blockDim.x sites x 4 directions x blockDim.z slice groups of one
-// parity (blockIdx.y): the four links of a site sit in one warp, or in
-// neighbouring warps of one block, so the spinors at x that all four read
-// come from one request or from L1; thread (tx, mu, g) sums the slices g,
-// g + blockDim.z, ...; the groups' sums are added in a fixed order through
-// shared memory and group 0 finishes the link.
+// parity: the four links of a site sit in neighbouring warps of one block,
+// so the spinors at x that all four read come from L1; thread (tx, mu, g)
+// sums the slices g, g + blockDim.z, ...; the groups' sums are added in a
+// fixed order through shared memory and group 0 finishes the link.  The two
+// parities of a site block are consecutive blocks (blockIdx.x = 2 site block
+// + parity), so a half field read as v(x) by one is still in L2 when the
+// other reads it as v(x+mu): with all blocks of one parity first, every
+// half came from DRAM twice.
 __global__ void __launch_bounds__(FORCE_TPB, 3) fforce_kernel(const ForceParams fp, const ForceViews v,
                                                                  double *partials) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int p = blockIdx.y, mu = threadIdx.y;
+  const int i = (blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+  const int p = blockIdx.x & 1, mu = threadIdx.y;
   const bool active = i < fp.vh;
   double red[3] = {0.0, 0.0, 0.0};  // L1, L2 and Linf of this thread
   int x = 0, y = 0, z = 0, t = 0, j = 0;
@@ -405,7 +408,7 @@ void fforce_update(const Dirac &D, const ForceVecs &fv, double *mom, double dt, 
   // projections) and the four directions of a site share L1
   const int sg = 1;
   const dim3 block(FORCE_TPB / (4 * sg), 4, sg);
-  const dim3 grid((unsigned)((L.vh + block.x - 1) / block.x), 2);
+  const dim3 grid(2 * (unsigned)((L.vh + block.x - 1) / block.x));
   const size_t smem = sg > 1 ? (size_t)sg * 18 * 4 * block.x * sizeof(double) : 0;
   const unsigned nblk = grid.x * grid.y;
   L.partials.ensure((size_t)nblk * 3 * sizeof(double) + 3 * sizeof(double));

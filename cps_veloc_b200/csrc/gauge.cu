@@ -35,11 +35,12 @@ __device__ __forceinline__ void mat_mul(cplx<double> (&c)[3][3], const su3<doubl
     }
 }
 
-// thread per (checkerboard site, parity): sum over mu < nu of
+// thread per (checkerboard site, parity), the two parities of a site block
+// in consecutive blocks (their links are each other's neighbours): sum over mu < nu of
 // Re tr[U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag] and sum over mu of Re tr U_mu(x)
 __global__ void __launch_bounds__(GTPB) plaq_kernel(const GaugeGeom g, const GaugeView U, double *partials) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int p = blockIdx.y;
+  const int i = (blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+  const int p = blockIdx.x & 1;
   double v[2] = {0.0, 0.0};
   if (i < g.vh) {
     int r = i / g.hx;
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(GTPB) plaq_kernel(const GaugeGeom g, const Gau
         v[0] += s;
       }
   }
-  block_partial<2>(v, partials, 0, blockIdx.x + gridDim.x * blockIdx.y, gridDim.x * gridDim.y);
+  block_partial<2>(v, partials, 0, blockIdx.x, gridDim.x);
 }
 
 }  // namespace
@@ -98,8 +99,8 @@ void gauge_sums(Lattice &L, double *sum_plaq, double *sum_link) {
   GaugeView U;
   U.data = L.gD18.ptr;
   U.vh = L.vh;
-  const dim3 grid((unsigned)((L.vh + GTPB - 1) / GTPB), 2);
-  const unsigned nblk = grid.x * grid.y;
+  const unsigned nblk = 2 * (unsigned)((L.vh + GTPB - 1) / GTPB);
+  const dim3 grid(nblk);
   L.partials.ensure((size_t)nblk * 2 * sizeof(double));
   SolverScalars *st = L.scratch_st.as<SolverScalars>();
   plaq_kernel<<<grid, GTPB, 0, L.stream>>>(g, U, L.partials.as<double>());

@@ -5,7 +5,8 @@ precision, from HBM (the launches rotate over fields larger than L2):
 
 Prints one line per precision: ms per Dslash, GB/s of its algorithmic bytes,
 ms per MatPcDagMatPc and its GB/s.  Under a profiler, --reps 1 and
---no-mdagm keep the launch count small.
+--no-mdagm keep the launch count small.  --force times the HMC fermion force
+instead (CalcHmdForceVecs + the force kernel, FP64; Wilson, DWF, Mobius).
 """
 from __future__ import annotations
 
@@ -26,6 +27,7 @@ def main(argv=None) -> int:
     ap.add_argument("--reps", type=int, default=40)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-mdagm", action="store_true")
+    ap.add_argument("--force", action="store_true", help="time the HMC fermion force instead")
     ap.add_argument("--link-reals", type=int, default=0,
                     help="link form of the FP32/FP16 operators (12, 18, 112, 118; 0: default or autotuned)")
     args = ap.parse_args(argv)
@@ -38,6 +40,12 @@ def main(argv=None) -> int:
         D = DiracOpDwf(lat, mass=args.mass, ls=args.ls)
     else:
         D = DiracOpMobius(lat, mass=args.mass, ls=args.ls)
+    if args.force:
+        tot, ker, by = C.c_double(), C.c_double(), C.c_double()
+        A.check(A.lib().cpsgpu_time_fforce(D._h, args.reps, C.byref(tot), C.byref(ker), C.byref(by)))
+        print(f"force: {tot.value:.4f} ms per call; force kernel {ker.value:.4f} ms "
+              f"{by.value / ker.value / 1e6:.0f} GB/s ({by.value:.0f} B)", flush=True)
+        return 0
     for prec in (int(p) for p in args.prec.split(",")):
         if not args.no_autotune:
             D.autotune(prec)
