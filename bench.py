@@ -306,7 +306,9 @@ def extra_mobius(A) -> dict:
 def extra_multishift(A) -> dict:
     """Wilson 32^3x64, kappa=0.125, 16 shifts log-spaced in [1e-4, 10]: FP64
     multishift CG against FP32 multishift + FP64 refinement of every shift
-    (wall time of the host-vector call, transfers of 16 solutions included)."""
+    (wall time of the host-vector call, transfers of 16 solutions included;
+    after one untimed call, into solution arrays already resident in host
+    memory as a caller's would be)."""
     from cps_veloc_b200.dirac import DiracOpWilson, Lattice, gen_gauge, gen_gaussian
 
     L = (32, 32, 32, 64)
@@ -318,12 +320,15 @@ def extra_multishift(A) -> dict:
     shifts = list(np.logspace(-4, 1, 16))
     chi = gen_gaussian(D.f_size, seed=SEED, stream=5)
     out = {"lattice": list(L), "kappa": 0.125, "shifts": len(shifts)}
+    psi = [np.full(D.f_size, 0.0) for _ in shifts]  # touched: resident host memory
     for name, prec in (("fp64", A.DOUBLE), ("fp32_then_fp64_refine", A.SINGLE)):
-        psi = [np.zeros(D.f_size) for _ in shifts]
-        rs = np.full(len(shifts), STOP)
-        t0 = time.perf_counter()
-        k = D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, precision=prec)
-        t = time.perf_counter() - t0
+        for rep in range(2):  # the first call allocates the device workspace
+            for x in psi:
+                x.fill(0.0)
+            rs = np.full(len(shifts), STOP)
+            t0 = time.perf_counter()
+            k = D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, precision=prec)
+            t = time.perf_counter() - t0
         y, _ = D.MatPcDagMatPc(psi[0])
         worst = float(np.linalg.norm(chi - y - shifts[0] * psi[0]) / np.linalg.norm(chi))
         out[name] = {"wall_s": t, "iterations": k, "true_res_smallest_shift": worst}

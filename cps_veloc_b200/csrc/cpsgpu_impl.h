@@ -102,6 +102,18 @@ struct Lattice {
   }
 };
 
+struct OpWork {
+  Field t1, t2, t0;  // operator temporaries, one precision
+};
+
+// Multishift CG workspace (multishift.cu), kept across calls on one operator.
+struct MsWork {
+  Field chi, r, tmp;
+  std::vector<Field> p, psi;
+  DeviceBuffer st, ms, pv, psiv;
+  OpWork w;
+};
+
 struct Dirac {
   Lattice *lat;
   int kind;
@@ -125,6 +137,7 @@ struct Dirac {
   // right-hand sides per hop tile (consecutive blocks share links across
   // this many solves), per precision, set by the autotuner; 0 = untuned
   int rtile[3] = {0, 0, 0};
+  MsWork ms;  // multishift workspace
   int rhs_tile(int prec, int nrhs) const {
     const int t = rtile[prec];
     return t > 0 ? t : (nrhs < 4 ? nrhs : 4);
@@ -132,10 +145,6 @@ struct Dirac {
 };
 
 // ---- kernels / launchers (hop.cu, blas.cu) ----
-struct OpWork {
-  Field t1, t2, t0;  // operator temporaries, one precision
-};
-
 // Launch one hop with epilogue; see hop.cuh for the meaning of each field.
 struct HopLaunch {
   int prec = PREC_DOUBLE;   // hop precision

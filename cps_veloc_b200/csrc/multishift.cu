@@ -3,8 +3,9 @@
 // One iteration is: the M half of MatPcDagMatPc on p_0 (reducing <p,(A+m_0)p>,
 // whose last block runs the shifted z / beta recurrences for every shift),
 // the M^dagger half with the residual update r += b A p_0 and |r|^2 fused in
-// (last block: per-shift convergence), then one kernel that, per site, reads
-// r once and updates psi_s and p_s of every shift still running.  The
+// (last block: per-shift convergence), then one kernel that updates psi_s
+// and p_s of every shift still running (a thread per site and shift; a thread
+// per site summing over the shifts when only the weighted sum is kept).  The
 // scalars never leave the device.
 //
 // precision CPSGPU_SINGLE runs the recurrences on FP32 vectors (solutions
@@ -74,6 +75,47 @@ __global__ void ms_update_kernel(SpinorView r, const SpinorView *pv, const Spino
   if (single) SpinorIO<PREC_DOUBLE>::store(psiv[0], sl, i, acc0);
 }
 
+// The same update with one thread per (site, shift), for solutions kept
+// per shift (types MULTI and GENERAL): blockIdx.x = site block x nshift +
+// shift, so the blocks of one site block are consecutive and r is read from
+// L2 by all but the first shift.
+template <int P>
+__global__ void __launch_bounds__(128) ms_update_shift_kernel(SpinorView r, const SpinorView *pv,
+                                                              const SpinorView *psiv, SpinorView chi,
+                                                              const MsScalars *ms, const SolverScalars *st,
+                                                              int use_chi) {
+  if (ms->upd_done_iter == ms->k) return;
+  const int n = ms->nshift;
+  const int s = blockIdx.x % n;
+  const size_t idx = (size_t)(blockIdx.x / n) * blockDim.x + threadIdx.x;
+  const long per = r.vh * r.ls;
+  if (idx >= (size_t)per) return;
+  const long sl = (long)(idx / r.vh), i = (long)(idx % r.vh);
+  const bool upd = !ms->conv_prev[s];
+  const bool adv = (st->done == 0) && !ms->conv[s];
+  if (!upd && !adv) return;
+  RealT<P> pp[24];
+  SpinorIO<P>::load(pv[s], sl, i, pp);
+  if (upd) {
+    const double f = -ms->bs[s] * ms->weight[s];
+    double y[24], c[24];
+    SpinorIO<PREC_DOUBLE>::load(psiv[s], sl, i, y);
+    if (use_chi) SpinorIO<PREC_DOUBLE>::load(chi, sl, i, c);
+#pragma unroll
+    for (int k = 0; k < 24; k++) y[k] += f * (use_chi ? c[k] : double(pp[k]));
+    SpinorIO<PREC_DOUBLE>::store(psiv[s], sl, i, y);
+  }
+  if (adv) {
+    RealT<P> rv[24];
+    SpinorIO<P>::load(r, sl, i, rv);
+    const RealT<P> zr = (s == 0) ? RealT<P>(1) : RealT<P>(ms->z[ms->iz][s]);
+    const RealT<P> ap = (s == 0) ? RealT<P>(ms->a) : RealT<P>(ms->as[s]);
+#pragma unroll
+    for (int k = 0; k < 24; k++) pp[k] = zr * rv[k] + ap * pp[k];
+    SpinorIO<P>::store(pv[s], sl, i, pp);
+  }
+}
+
 __global__ void ms_mark_kernel(MsScalars *ms) { ms->upd_done_iter = ms->k; }
 
 }  // namespace
@@ -92,11 +134,18 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   const int dev_type = (P != PREC_DOUBLE && type == 0) ? 1 : type;
   const int npsi = (dev_type == 0) ? 1 : nshift;
 
-  Field chi64(PREC_DOUBLE, vh, ls, 1), r(P, vh, ls, 1), tmp64(PREC_DOUBLE, vh, ls, 1);
-  std::vector<Field> p(nshift), psi(npsi);
-  for (int k = 0; k < nshift; k++) p[k].create(P, vh, ls, 1);
-  for (int k = 0; k < npsi; k++) psi[k].create(PREC_DOUBLE, vh, ls, 1);
-  OpWork w;
+  // workspace kept on the operator across calls (allocated on first use)
+  MsWork &mw = D.ms;
+  Field &chi64 = mw.chi, &r = mw.r, &tmp64 = mw.tmp;
+  ensure_field(chi64, PREC_DOUBLE, vh, ls, 1);
+  ensure_field(r, P, vh, ls, 1);
+  ensure_field(tmp64, PREC_DOUBLE, vh, ls, 1);
+  if (mw.p.size() < (size_t)nshift) mw.p.resize(nshift);
+  if (mw.psi.size() < (size_t)npsi) mw.psi.resize(npsi);
+  std::vector<Field> &p = mw.p, &psi = mw.psi;
+  for (int k = 0; k < nshift; k++) ensure_field(p[k], P, vh, ls, 1);
+  for (int k = 0; k < npsi; k++) ensure_field(psi[k], PREC_DOUBLE, vh, ls, 1);
+  OpWork &w = mw.w;
   ensure_field(w.t1, P, vh, ls, 1);
   ensure_field(w.t2, P, vh, ls, 1);
   if (D.kind == KIND_MOBIUS) ensure_field(w.t0, P, vh, ls, 1);
@@ -120,9 +169,10 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     }
   }
 
-  DeviceBuffer stbuf(sizeof(SolverScalars)), msbuf(sizeof(MsScalars));
-  SolverScalars *st = stbuf.as<SolverScalars>();
-  MsScalars *msd = msbuf.as<MsScalars>();
+  mw.st.ensure(sizeof(SolverScalars));
+  mw.ms.ensure(sizeof(MsScalars));
+  SolverScalars *st = mw.st.as<SolverScalars>();
+  MsScalars *msd = mw.ms.as<MsScalars>();
   SolverScalars st0;
   memset(&st0, 0, sizeof(st0));
   st0.shift = shift[0];
@@ -171,9 +221,11 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   std::vector<SpinorView> pv(nshift), psiv(npsi);
   for (int k = 0; k < nshift; k++) pv[k] = p[k].view();
   for (int k = 0; k < npsi; k++) psiv[k] = psi[k].view();
-  DeviceBuffer pvd(sizeof(SpinorView) * nshift), psivd(sizeof(SpinorView) * npsi);
-  CPSGPU_CUDA(cudaMemcpyAsync(pvd.ptr, pv.data(), pvd.bytes, cudaMemcpyHostToDevice, s));
-  CPSGPU_CUDA(cudaMemcpyAsync(psivd.ptr, psiv.data(), psivd.bytes, cudaMemcpyHostToDevice, s));
+  mw.pv.ensure(sizeof(SpinorView) * MS_MAX);
+  mw.psiv.ensure(sizeof(SpinorView) * MS_MAX);
+  DeviceBuffer &pvd = mw.pv, &psivd = mw.psiv;
+  CPSGPU_CUDA(cudaMemcpyAsync(pvd.ptr, pv.data(), sizeof(SpinorView) * nshift, cudaMemcpyHostToDevice, s));
+  CPSGPU_CUDA(cudaMemcpyAsync(psivd.ptr, psiv.data(), sizeof(SpinorView) * npsi, cudaMemcpyHostToDevice, s));
 
   // one iteration: M half (reduce <p,(A+m0)p>), M^dagger half with the
   // residual update, then the per-shift vector updates.
@@ -228,12 +280,21 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     Lh.ep = mob ? EP_MIX_CG : EP_CG;
     launch_hop(D, Lh, w.t1.view(), SpinorView(), w.t2.view(), r.view(), SpinorView(), in, SpinorView(), st);
     size_t per = (size_t)vh * ls;
-    if (P == PREC_DOUBLE)
+    if (dev_type != 0) {
+      const unsigned g = (unsigned)((per + 127) / 128) * (unsigned)nshift;
+      if (P == PREC_DOUBLE)
+        ms_update_shift_kernel<PREC_DOUBLE><<<g, 128, 0, s>>>(r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(),
+                                                              chi64.view(), msd, st, use_chi);
+      else
+        ms_update_shift_kernel<PREC_SINGLE><<<g, 128, 0, s>>>(r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(),
+                                                              chi64.view(), msd, st, use_chi);
+    } else if (P == PREC_DOUBLE) {
       ms_update_kernel<PREC_DOUBLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
           r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
-    else
+    } else {
       ms_update_kernel<PREC_SINGLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
           r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
+    }
     CPSGPU_CUDA(cudaGetLastError());
     ms_mark_kernel<<<1, 1, 0, s>>>(msd);
     CPSGPU_CUDA(cudaGetLastError());
