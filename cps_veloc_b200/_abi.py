@@ -111,6 +111,8 @@ def lib() -> C.CDLL:
             "cpsgpu_time_fforce": (C.c_int, [vp, C.c_int, _dp, _dp, _dp]),
             "cpsgpu_rhmc_evolve_mom_fforce": (C.c_int, [vp, _dp, C.POINTER(_dp), C.c_int, _dp, C.c_double, C.c_int,
                                                         C.POINTER(ForceArg)]),
+            "cpsgpu_inveigcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.c_int, C.c_int, C.POINTER(_dp), _dp,
+                                          C.POINTER(C.POINTER(C.c_float)), _dp, C.c_int, _dp, C.c_int, _ip, _dp]),
             "cpsgpu_minresext": (C.c_int, [vp, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp]),
             "cpsgpu_bicgstab": (C.c_int, [vp, _dp, _dp, C.c_double, C.c_int, C.POINTER(CgArg), C.POINTER(C.c_int),
                                           _dp]),

@@ -26,6 +26,9 @@ int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, do
 void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
 void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
                double *error);
+int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
+             std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<std::complex<double>> &invH,
+             const double *restart, int restart_len, double *true_res);
 void nersc_read(const char *path, const int node_sites[4], double *u, cpsgpu_nersc_header *hdr);
 void nersc_write(const char *path, const int node_sites[4], const double *u, int recon_row_3, int fp_format,
                  const cpsgpu_nersc_header *meta, cpsgpu_nersc_header *out);
@@ -709,6 +712,48 @@ int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_ke
     if (ms_total) *ms_total = t_all / reps;
     if (ms_kernel) *ms_kernel = t_k / reps;
     if (kernel_bytes) *kernel_bytes = fforce_bytes(D);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_inveigcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg_arg *arg, int nev, int m,
+                    double *const *V, double *M, float *const *U, const double *invH, int def_len,
+                    const double *restart, int restart_len, int *iterations, double *true_res) {
+  return guarded([&] {
+    if (!d || !sol || !src || !arg) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (nev < 0 || def_len < 0 || restart_len < 0) throw Error(CPSGPU_ERR_ARG, "negative count");
+    if (nev > 0 && m <= 2 * nev) throw Error(CPSGPU_ERR_ARG, "m should be larger than 2*nev (inv_eig_cg.C:133)");
+    if (nev > 0 && (!V || !M)) throw Error(CPSGPU_ERR_ARG, "null V or M");
+    if (def_len > 0 && (!U || !invH)) throw Error(CPSGPU_ERR_ARG, "null U or invH");
+    if (restart_len > 0 && !restart) throw Error(CPSGPU_ERR_ARG, "null restart");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    const size_t nreal = (size_t)24 * L.vh * D.ls;
+    Field fsol(PREC_DOUBLE, L.vh, D.ls, 1), fsrc(PREC_DOUBLE, L.vh, D.ls, 1);
+    upload(L, fsrc, &src, 1);
+    std::vector<Field> fv(nev > 0 ? m : 0), fu(def_len);
+    for (auto &f : fv) f.create(PREC_DOUBLE, L.vh, D.ls, 1);
+    std::vector<double> h(def_len > 0 ? nreal : 0);
+    for (int k = 0; k < def_len; k++) {
+      if (!U[k]) throw Error(CPSGPU_ERR_ARG, "null deflation vector");
+      for (size_t q = 0; q < nreal; q++) h[q] = (double)U[k][q];
+      fu[k].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      const double *hp = h.data();
+      upload(L, fu[k], &hp, 1);
+    }
+    std::vector<std::complex<double>> ih((size_t)def_len * def_len);
+    for (size_t k = 0; k < ih.size(); k++) ih[k] = {invH[2 * k], invH[2 * k + 1]};
+    double tr = 0.0;
+    const int it = inveigcg(D, fsol, fsrc, arg->stop_rsd, arg->max_num_iter, nev, m, fv, M, fu, ih, restart,
+                            restart_len, &tr);
+    download(L, fsol, &sol, 1);
+    for (int k = 0; k < (int)fv.size(); k++) {
+      double *hv = V[k];
+      if (hv) download(L, fv[k], &hv, 1);
+    }
+    if (iterations) *iterations = it;
+    if (true_res) *true_res = tr;
     return CPSGPU_OK;
   });
 }

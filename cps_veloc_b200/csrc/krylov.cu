@@ -1,0 +1,489 @@
+// Host-driven Krylov routines with every vector on the device:
+//   BiCGstab(n) on MatPc: DiracOpWilsonTypes::BiCGstab (bicgstab.C:35-229);
+//   the chronological initial guess DiracOp::MinResExt (minresext.C:30-150).
+// Their complex scalars (rho, alpha, omega, tau, gamma; the small Gram
+// matrix) are the reference's short host computations, step for step; each
+// global dot product <a, b> = sum conj(a) b (compDotProduct,
+// vector_util.C:889-903) is a device reduction read back by the host.
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include "cpsgpu_impl.h"
+#include "hop.cuh"
+
+namespace cpsgpu {
+
+namespace {
+
+constexpr int TPB = 256;
+
+// per-block partials of <a, b> (re, im), one thread per 5D site
+__global__ void cdot_kernel(SpinorView a, SpinorView b, double *partials, size_t n) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (idx < n) {
+    const long sl = (long)(idx / a.vh), i = (long)(idx % a.vh);
+    double x[24], y[24];
+    SpinorIO<PREC_DOUBLE>::load(a, sl, i, x);
+    SpinorIO<PREC_DOUBLE>::load(b, sl, i, y);
+#pragma unroll
+    for (int k = 0; k < 24; k += 2) {
+      v[0] += x[k] * y[k] + x[k + 1] * y[k + 1];
+      v[1] += x[k] * y[k + 1] - x[k + 1] * y[k];
+    }
+  }
+  block_partial<2>(v, partials);
+}
+
+// a = f c + d, f complex (cTimesV1PlusV2, vector_util.C:912-922)
+__global__ void caxpy_kernel(SpinorView a, double re, double im, SpinorView c, SpinorView d, size_t n) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const long sl = (long)(idx / a.vh), i = (long)(idx % a.vh);
+  double x[24], y[24];
+  SpinorIO<PREC_DOUBLE>::load(c, sl, i, x);
+  SpinorIO<PREC_DOUBLE>::load(d, sl, i, y);
+#pragma unroll
+  for (int k = 0; k < 24; k += 2) {
+    const double cr = x[k], ci = x[k + 1];
+    y[k] += re * cr - im * ci;
+    y[k + 1] += re * ci + im * cr;
+  }
+  SpinorIO<PREC_DOUBLE>::store(a, sl, i, y);
+}
+
+using cd = std::complex<double>;
+
+struct Ctx {
+  Dirac &D;
+  Lattice &L;
+  OpWork w;
+  SolverScalars *st;
+  double *partials;
+  size_t sites;
+  unsigned blocks() const { return (unsigned)((sites + TPB - 1) / TPB); }
+
+  cd dot(const Field &a, const Field &b) {
+    cdot_kernel<<<blocks(), TPB, 0, L.stream>>>(a.view(), b.view(), partials, sites);
+    CPSGPU_CUDA(cudaGetLastError());
+    launch_counter()++;
+    launch_finalize(L.stream, 2, partials, st, RED_STORE, blocks(), 1, GATE_NONE);
+    double s[2];
+    CPSGPU_CUDA(cudaMemcpyAsync(s, st->sum, sizeof(s), cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return {s[0], s[1]};
+  }
+  double norm2(const Field &a) {
+    launch_norm(L.stream, PREC_DOUBLE, a.view(), st, partials, RED_STORE, GATE_NONE);
+    double s = 0.0;
+    CPSGPU_CUDA(cudaMemcpyAsync(&s, st->sum, sizeof(s), cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return s;
+  }
+  // a = f c + d
+  void caxpy(Field &a, cd f, const Field &c, const Field &d) {
+    caxpy_kernel<<<blocks(), TPB, 0, L.stream>>>(a.view(), f.real(), f.imag(), c.view(), d.view(), sites);
+    CPSGPU_CUDA(cudaGetLastError());
+    launch_counter()++;
+  }
+  void matpc(Field &out, const Field &in) { op_matpc(D, PREC_DOUBLE, out.view(), in.view(), 0, w, nullptr, 0, 0); }
+  // out = MatPcDagMatPc in; returns |MatPc in|^2
+  double mdagm(Field &out, const Field &in) {
+    CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
+    op_mdagm(D, PREC_DOUBLE, out.view(), in.view(), w, st, RED_STORE);
+    double s = 0.0;
+    CPSGPU_CUDA(cudaMemcpyAsync(&s, st->sum, sizeof(s), cudaMemcpyDeviceToHost, L.stream));
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return s;
+  }
+};
+
+// out[j][k] = sum_i V[i][k] QZ[i + m j] for j < rank: the Ritz vectors of
+// an eigCG restart as combinations of the m Lanczos vectors
+// (eigcg_vec_mult, inv_eig_cg.C:76-126).  A thread per real, VM_R outputs
+// in registers at a time; V reads are coalesced, QZ is read uniformly.
+constexpr int VM_R = 16;
+__global__ void __launch_bounds__(256) vec_mult_kernel(const double *const *V, int m, const double *QZ, int rank,
+                                                       double *const *out, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    for (int j0 = 0; j0 < rank; j0 += VM_R) {
+      double acc[VM_R];
+#pragma unroll
+      for (int q = 0; q < VM_R; q++) acc[q] = 0.0;
+      for (int i = 0; i < m; i++) {
+        const double v = V[i][k];
+#pragma unroll
+        for (int q = 0; q < VM_R; q++)
+          if (j0 + q < rank) acc[q] = fma(v, QZ[i + m * (j0 + q)], acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < VM_R; q++)
+        if (j0 + q < rank) out[j0 + q][k] = acc[q];
+    }
+}
+
+// Real symmetric eigenproblem by cyclic Jacobi rotations (Golub and Van
+// Loan, Matrix Computations, section 8.5).  ap: packed lower triangle
+// (i(i+1)/2 + j); evec[k n + i] = component k of eigenvector i.  The
+// reference's eigen_solver (eigen_solver.C:40) has the same layout, but its
+// QL step leaves the eigenvector update commented out, so the vectors it
+// returns are the Householder transform, not eigenvectors; these are.
+void sym_eigen(const std::vector<double> &ap, int n, std::vector<double> &evec, std::vector<double> &eval) {
+  std::vector<double> a((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j <= i; j++) a[(size_t)i * n + j] = a[(size_t)j * n + i] = ap[(size_t)i * (i + 1) / 2 + j];
+  evec.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) evec[(size_t)i * n + i] = 1.0;
+  double fro = 0.0;
+  for (double x : a) fro += x * x;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) off += 2.0 * a[(size_t)p * n + q] * a[(size_t)p * n + q];
+    if (off <= 1e-30 * fro) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = a[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double theta = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        auto rot = [&](double &x, double &y) {
+          const double u = x, w = y;
+          x = cs * u - sn * w;
+          y = sn * u + cs * w;
+        };
+        for (int k = 0; k < n; k++) rot(a[(size_t)k * n + p], a[(size_t)k * n + q]);
+        for (int k = 0; k < n; k++) rot(a[(size_t)p * n + k], a[(size_t)q * n + k]);
+        for (int k = 0; k < n; k++) rot(evec[(size_t)k * n + p], evec[(size_t)k * n + q]);
+      }
+  }
+  eval.resize(n);
+  for (int i = 0; i < n; i++) eval[i] = a[(size_t)i * n + i];
+}
+
+// indices of the nev smallest eigenvalues, as min_eig_index (inv_eig_cg.C:37-51) picks them
+void min_eig_index(std::vector<int> &index, int nev, const std::vector<double> &eig, int n) {
+  index.resize(nev);
+  for (int i = 0; i < nev; i++) index[i] = i;
+  for (int i = nev; i < n; i++) {
+    int mx = 0;
+    for (int j = 1; j < nev; j++)
+      if (eig[index[j]] > eig[index[mx]]) mx = j;
+    if (eig[i] < eig[index[mx]]) index[mx] = i;
+  }
+}
+
+}  // namespace
+
+int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, double stop_rsd, int max_num_iter,
+             double *true_res) {
+  constexpr int NMAX = 10;
+  if (nn <= 0 || nn > NMAX) throw Error(-1, "BiCGstab: n must be in [1, 10]");
+  Lattice &L = *D.lat;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  CPSGPU_CUDA(cudaMemsetAsync(c.st, 0, sizeof(SolverScalars), L.stream));
+  std::vector<Field> r(nn + 1), u(nn + 1);
+  for (int i = 0; i <= nn; i++) {
+    r[i].create(PREC_DOUBLE, L.vh, D.ls, 1);
+    u[i].create(PREC_DOUBLE, L.vh, D.ls, 1);
+  }
+  Field r0(PREC_DOUBLE, L.vh, D.ls, 1);
+  cd rho0 = 1.0, rho1, alpha = 0.0, omega = 1.0, beta;
+  double sigma[NMAX + 1];
+  cd gamma[NMAX + 1], gamma_p[NMAX + 1], gamma_pp[NMAX + 1], tau[NMAX + 1][NMAX + 1];
+  int converged = 0, k;
+
+  if (chi_norm == 0.0) chi_norm = c.norm2(chi);
+  if (chi_norm == 0.0) {  // the solution of a zero source is zero
+    launch_zero(L.stream, psi);
+    return 0;
+  }
+  const double rsd_sq = chi_norm * stop_rsd * stop_rsd;
+  // r[0] = chi - MatPc psi;  r0 = r[0];  u[0] = 0
+  c.matpc(r[0], psi);
+  c.caxpy(r[0], -1.0, r[0], chi);
+  sigma[0] = c.norm2(r[0]);
+  CPSGPU_CUDA(cudaMemcpyAsync(r0.data.ptr, r[0].data.ptr, r0.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+  launch_zero(L.stream, u[0]);
+
+  for (k = 1; k <= max_num_iter && !converged; k += nn) {
+    rho0 *= -omega;
+    for (int j = 0; j < nn; j++) {  // BiCG part
+      rho1 = c.dot(r0, r[j]);
+      beta = alpha * rho1 / rho0;
+      rho0 = rho1;
+      for (int i = 0; i <= j; i++) c.caxpy(u[i], -beta, u[i], r[i]);
+      c.matpc(u[j + 1], u[j]);
+      alpha = rho0 / c.dot(r0, u[j + 1]);
+      for (int i = 0; i <= j; i++) c.caxpy(r[i], -alpha, u[i + 1], r[i]);
+      c.matpc(r[j + 1], r[j]);
+      c.caxpy(psi, alpha, u[0], psi);
+    }
+    for (int j = 1; j <= nn; j++) {  // MR part
+      for (int i = 1; i < j; i++) {
+        tau[i][j] = c.dot(r[i], r[j]) / sigma[i];
+        c.caxpy(r[j], -tau[i][j], r[i], r[j]);
+      }
+      sigma[j] = c.norm2(r[j]);
+      gamma_p[j] = c.dot(r[j], r[0]) / sigma[j];
+    }
+    gamma[nn] = gamma_p[nn];
+    omega = gamma[nn];
+    for (int j = nn - 1; j > 0; j--) {
+      gamma[j] = gamma_p[j];
+      for (int i = j + 1; i <= nn; i++) gamma[j] -= tau[j][i] * gamma[i];
+    }
+    for (int j = 1; j < nn; j++) {
+      gamma_pp[j] = gamma[j + 1];
+      for (int i = j + 1; i < nn; i++) gamma_pp[j] += tau[j][i] * gamma[i + 1];
+    }
+    c.caxpy(u[0], -gamma[nn], u[nn], u[0]);
+    c.caxpy(psi, gamma[1], r[0], psi);
+    c.caxpy(r[0], -gamma_p[nn], r[nn], r[0]);
+    for (int j = 1; j < nn; j++) {
+      c.caxpy(u[0], -gamma[j], u[j], u[0]);
+      c.caxpy(psi, gamma_pp[j], r[j], psi);
+      c.caxpy(r[0], -gamma_p[j], r[j], r[0]);
+    }
+    sigma[0] = c.norm2(r[0]);
+    if (sigma[0] < rsd_sq) converged = 1;
+  }
+  if (converged && true_res) *true_res = std::sqrt(sigma[0]);
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+  return k;
+}
+
+void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
+               double *error) {
+  const int degree = (int)v.size();
+  Lattice &L = *D.lat;
+  if (degree == 0) {  // no guess requested: psi = 0
+    launch_zero(L.stream, psi);
+    if (error) *error = 1.0;
+    return;
+  }
+  if (degree > 16) throw Error(-1, "MinResExt: at most 16 previous solutions");
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  std::vector<std::vector<cd>> G(degree, std::vector<cd>(degree));
+  std::vector<cd> a(degree), b(degree);
+  cd xp;
+  // orthonormalise the basis
+  for (int i = 0; i < degree; i++) {
+    launch_scale(L.stream, 1.0 / std::sqrt(c.norm2(v[i])), v[i].view());
+    for (int j = i + 1; j < degree; j++) {
+      xp = c.dot(v[i], v[j]);
+      c.caxpy(v[j], -xp, v[i], v[j]);
+    }
+  }
+  for (int i = 0; i < degree; i++) {
+    b[i] = c.dot(v[i], phi);
+    G[i][i] = cd(c.mdagm(vm[i], v[i]), 0.0);
+  }
+  for (int j = 0; j < degree; j++)
+    for (int k = j + 1; k < degree; k++) {
+      G[j][k] = c.dot(v[j], vm[k]);
+      G[k][j] = std::conj(G[j][k]);
+    }
+  // Gauss-Jordan elimination with the reference's (diagonal) pivoting
+  for (int i = 0; i < degree; i++) {
+    int k = i;
+    for (int j = i + 1; j < degree; j++)
+      if (std::abs(G[j][j]) > std::abs(G[k][k])) k = j;
+    if (k != i) {
+      std::swap(b[k], b[i]);
+      std::swap(G[k], G[i]);
+    }
+    for (int j = i + 1; j < degree; j++) {
+      xp = G[j][i] / G[i][i];
+      b[j] -= xp * b[i];
+      for (int kk = 0; kk < degree; kk++) G[j][kk] -= xp * G[i][kk];
+    }
+  }
+  Field r(PREC_DOUBLE, L.vh, D.ls, 1);
+  launch_zero(L.stream, psi);
+  CPSGPU_CUDA(cudaMemcpyAsync(r.data.ptr, phi.data.ptr, r.data.bytes, cudaMemcpyDeviceToDevice, L.stream));
+  for (int i = degree - 1; i >= 0; i--) {
+    a[i] = 0.0;
+    for (int j = i + 1; j < degree; j++) a[i] += G[i][j] * a[j];
+    a[i] = (b[i] - a[i]) / G[i][i];
+    c.caxpy(psi, a[i], v[i], psi);
+    c.caxpy(r, -a[i], vm[i], r);
+  }
+  if (error) *error = std::sqrt(c.norm2(r) / c.norm2(phi));
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+}
+
+
+// DiracOp::InvEigCg (inv_eig_cg.C:129-635): CG on A = MatPcDagMatPc, FP64,
+// with the eigCG bookkeeping (nev > 0) and low-mode deflation (U, invH).
+// The CG steps and their order are the reference's; the small matrices (T,
+// Q, H and their eigenproblems) live on the host, every vector on the
+// device.  V holds the m Lanczos vectors (on return: the last restart's Ritz
+// vectors first, M their Ritz values).  Returns the reference's iter.
+int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
+             std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<cd> &invH,
+             const double *restart, int restart_len, double *true_res) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  const int def_len = (int)U.size();
+  const size_t nreal = (size_t)24 * L.vh * D.ls;
+  Field r(PREC_DOUBLE, L.vh, D.ls, 1), dir(PREC_DOUBLE, L.vh, D.ls, 1), mmp(PREC_DOUBLE, L.vh, D.ls, 1);
+  Field mmp_prev;
+  if (nev > 0) mmp_prev.create(PREC_DOUBLE, L.vh, D.ls, 1);
+  const double src_norm_sq = c.norm2(src);
+  const double stp = src_norm_sq * stop_rsd * stop_rsd;
+  auto copy = [&](Field &dst, const Field &from) {
+    CPSGPU_CUDA(cudaMemcpyAsync(dst.data.ptr, from.data.ptr, dst.data.bytes, cudaMemcpyDeviceToDevice, s));
+  };
+  // out = sum_ii (invH <U, rhs>)_ii U_ii
+  auto deflate = [&](const Field &rhs, Field &out) {
+    std::vector<cd> ub(def_len), w(def_len, 0.0);
+    for (int ii = 0; ii < def_len; ii++) ub[ii] = c.dot(U[ii], rhs);
+    for (int ii = 0; ii < def_len; ii++)
+      for (int jj = 0; jj < def_len; jj++) w[ii] += invH[(size_t)ii * def_len + jj] * ub[jj];
+    launch_zero(s, out);
+    for (int ii = 0; ii < def_len; ii++) c.caxpy(out, w[ii], U[ii], out);
+  };
+  launch_zero(s, sol);
+  if (def_len > 0) deflate(src, sol);
+  c.mdagm(mmp, sol);
+  launch_axpby(s, r.view(), -1.0, mmp.view(), src.view());  // r = src - A sol
+  copy(dir, r);
+  double res_cur = c.norm2(r), res_prv = res_cur;
+
+  const int nev2 = 2 * nev;
+  std::vector<double> T, Tt, Y, Q, QZ, H, EIG, Mv;
+  std::vector<int> INDEX;
+  std::vector<Field> W;
+  DeviceBuffer vptr, wptr, qzbuf;
+  if (nev > 0) {
+    T.assign((size_t)m * (m + 1) / 2, 0.0);
+    Q.assign((size_t)m * nev2, 0.0);
+    QZ.assign((size_t)m * nev2, 0.0);
+    H.assign((size_t)nev2 * (nev2 + 1) / 2, 0.0);
+    W.resize(nev2);
+    for (auto &f : W) f.create(PREC_DOUBLE, L.vh, D.ls, 1);
+    std::vector<double *> vp(m), wp(nev2);
+    for (int i = 0; i < m; i++) vp[i] = V[i].data.as<double>();
+    for (int i = 0; i < nev2; i++) wp[i] = W[i].data.as<double>();
+    vptr.alloc(sizeof(double *) * m);
+    wptr.alloc(sizeof(double *) * nev2);
+    qzbuf.alloc(sizeof(double) * m * nev2);
+    CPSGPU_CUDA(cudaMemcpyAsync(vptr.ptr, vp.data(), sizeof(double *) * m, cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(wptr.ptr, wp.data(), sizeof(double *) * nev2, cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+  }
+  auto tidx = [](int i, int j) { return (size_t)i * (i + 1) / 2 + j; };  // packed lower triangle, j <= i
+  int i_eig = 0, restarted = 0, iter;
+  double alpha = 1.0, beta = 0.0, alpha_old = 0.0, beta_old = 0.0;
+  for (iter = 0; iter < max_iter; iter++) {
+    if (nev > 0 && i_eig == m) copy(mmp_prev, mmp);
+    res_prv = res_cur;
+    const double pAp = c.mdagm(mmp, dir);
+    if (pAp == 0) break;
+    if (nev > 0) {
+      if (i_eig != 0) T[tidx(i_eig - 1, i_eig - 1)] = 1.0 / alpha + beta_old / alpha_old;
+      if (i_eig == m) {
+        // restart: the nev lowest eigenvectors of T(m) and of T(m-1) (padded)
+        Tt.assign(T.begin(), T.begin() + (size_t)m * (m - 1) / 2);
+        sym_eigen(Tt, m - 1, Y, EIG);
+        min_eig_index(INDEX, nev, EIG, m - 1);
+        for (int i = nev; i < nev2; i++) {
+          for (int j = 0; j < m - 1; j++) Q[(size_t)j * nev2 + i] = Y[(size_t)j * (m - 1) + INDEX[i - nev]];
+          Q[(size_t)(m - 1) * nev2 + i] = 0.0;
+        }
+        sym_eigen(T, m, Y, EIG);
+        min_eig_index(INDEX, nev, EIG, m);
+        for (int i = 0; i < nev; i++)
+          for (int j = 0; j < m; j++) Q[(size_t)j * nev2 + i] = Y[(size_t)j * m + INDEX[i]];
+        // Gram-Schmidt of the second set against the first, dropping dependent vectors
+        int rank = nev;
+        for (int i = nev; i < nev2; i++) {
+          for (int j = 0; j < rank; j++) {
+            double xy = 0.0;
+            for (int k = 0; k < m; k++) xy += Q[(size_t)k * nev2 + i] * Q[(size_t)k * nev2 + j];
+            for (int k = 0; k < m; k++) Q[(size_t)k * nev2 + i] -= xy * Q[(size_t)k * nev2 + j];
+          }
+          double xx = 0.0;
+          for (int k = 0; k < m; k++) xx += Q[(size_t)k * nev2 + i] * Q[(size_t)k * nev2 + i];
+          if (xx > 1e-16) {
+            xx = 1.0 / std::sqrt(xx);
+            for (int k = 0; k < m; k++) Q[(size_t)k * nev2 + rank] = xx * Q[(size_t)k * nev2 + i];
+            rank++;
+          }
+        }
+        // H = Q^T T Q, its eigenpairs: the Ritz values M and QZ = Q Z
+        for (int i = 0; i < rank; i++)
+          for (int j = 0; j <= i; j++) {
+            double h = 0.0;
+            for (int l = 0; l < m; l++)
+              for (int k = 0; k < m; k++)
+                h += Q[(size_t)l * nev2 + i] * (k <= l ? T[tidx(l, k)] : T[tidx(k, l)]) * Q[(size_t)k * nev2 + j];
+            H[tidx(i, j)] = h;
+          }
+        std::vector<double> Hp(H.begin(), H.begin() + (size_t)rank * (rank + 1) / 2);
+        sym_eigen(Hp, rank, Y, Mv);
+        for (int i = 0; i < nev2; i++) M[i] = i < rank ? Mv[i] : 0.0;
+        for (int j = 0; j < rank; j++)
+          for (int i = 0; i < m; i++) {
+            double z = 0.0;
+            for (int k = 0; k < rank; k++) z += Q[(size_t)i * nev2 + k] * Y[(size_t)j + (size_t)k * rank];
+            QZ[(size_t)i + (size_t)m * j] = z;
+          }
+        CPSGPU_CUDA(cudaMemcpyAsync(qzbuf.ptr, QZ.data(), sizeof(double) * m * rank, cudaMemcpyHostToDevice, s));
+        const unsigned g = (unsigned)std::min<size_t>((nreal + 255) / 256, 148 * 16);
+        vec_mult_kernel<<<g, 256, 0, s>>>(vptr.as<double *>(), m, qzbuf.as<double>(), rank, wptr.as<double *>(), nreal);
+        CPSGPU_CUDA(cudaGetLastError());
+        launch_counter()++;
+        for (int j = 0; j < rank; j++) copy(V[j], W[j]);
+        // T <- diag(M) plus the coupling row of A r to the Ritz vectors
+        std::fill(T.begin(), T.end(), 0.0);
+        for (int i = 0; i < rank; i++) T[tidx(i, i)] = M[i];
+        i_eig = rank;
+        launch_axpby(s, mmp_prev.view(), -beta, mmp_prev.view(), mmp.view());
+        for (int ii = 0; ii < i_eig; ii++) T[tidx(i_eig, ii)] = c.dot(mmp_prev, V[ii]).real() / std::sqrt(res_cur);
+      } else if (i_eig != 0) {
+        T[tidx(i_eig, i_eig - 1)] = -std::sqrt(beta) / alpha;
+      }
+      copy(V[i_eig], r);
+      launch_scale(s, 1.0 / std::sqrt(res_cur), V[i_eig].view());
+      i_eig++;
+    }
+    alpha_old = alpha;
+    alpha = -res_prv / pAp;
+    launch_axpby(s, r.view(), alpha, mmp.view(), r.view());
+    res_cur = c.norm2(r);
+    alpha = -alpha;
+    beta_old = beta;
+    beta = res_cur / res_prv;
+    launch_axpby(s, sol.view(), alpha, dir.view(), sol.view());
+    launch_axpby(s, dir.view(), beta, dir.view(), r.view());
+    if (restarted < restart_len && def_len > 0 && res_cur < restart[restarted] * restart[restarted] * src_norm_sq) {
+      // deflated restart: sol += U invH U^dag r, r -= A (that), p = r
+      restarted++;
+      deflate(r, dir);
+      launch_axpby(s, sol.view(), 1.0, dir.view(), sol.view());
+      c.mdagm(mmp, dir);
+      launch_axpby(s, r.view(), -1.0, mmp.view(), r.view());
+      res_cur = c.norm2(r);
+      copy(dir, r);
+    }
+    if (res_cur <= stp) break;
+  }
+  c.mdagm(mmp, sol);
+  launch_axpby(s, r.view(), -1.0, mmp.view(), src.view());
+  if (true_res) *true_res = std::sqrt(c.norm2(r) / src_norm_sq);
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  return iter;
+}
+
+}  // namespace cpsgpu

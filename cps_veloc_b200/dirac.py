@@ -307,6 +307,37 @@ class _DiracOp:
                                                   1 if force_measure else 0, C.byref(fa)))
         return fa.L1, fa.L2, fa.Linf
 
+    def InvEigCg(self, sol, src, nev=0, m=0, stop_rsd=1e-8, max_num_iter=10000, U=None, invH=None, restart=()):
+        """DiracOp::InvEigCg (inv_eig_cg.C:129-635): sol (in place) solves
+        MatPcDagMatPc sol = src; returns (iterations, true_res, V, M) with V the
+        m eigCG vectors (the first 2 nev: Ritz vectors) and M the 2 nev Ritz
+        values.  U: deflation vectors (float32), invH their inverse projected
+        matrix (complex, def_len x def_len); restart: the relative residuals of
+        the deflated restarts."""
+        src = self._vec(src)
+        _inplace(sol, self.f_size)
+        V = [np.empty(self.f_size) for _ in range(m if nev > 0 else 0)]
+        M = np.zeros(max(2 * nev, 1))
+        U = [np.ascontiguousarray(u, dtype=np.float32) for u in (U or [])]
+        for u in U:
+            if u.size != self.f_size:
+                raise ValueError("deflation vector size")
+        def_len = len(U)
+        ih = np.ascontiguousarray(invH if invH is not None else np.zeros((max(def_len, 1),) * 2),
+                                  dtype=np.complex128)
+        if def_len and ih.shape != (def_len, def_len):
+            raise ValueError("invH must be def_len x def_len")
+        ihr = ih.view(np.float64).ravel()
+        rs = np.ascontiguousarray(list(restart) or [0.0], dtype=np.float64)
+        a = self._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, A.DOUBLE, 0.0, 8, True)
+        pv = (A._dp * max(1, len(V)))(*([dptr(x) for x in V] or [None]))
+        fp = C.POINTER(C.c_float)
+        pu = (fp * max(1, def_len))(*([u.ctypes.data_as(fp) for u in U] or [None]))
+        it, tr = C.c_int(), C.c_double()
+        check(lib().cpsgpu_inveigcg(self._h, dptr(sol), dptr(src), C.byref(a), nev, m, pv, dptr(M), pu, dptr(ihr),
+                                    def_len, dptr(rs), len(restart), C.byref(it), C.byref(tr)))
+        return it.value, tr.value, V, M[:2 * nev]
+
     def MinResExt(self, psi, phi, v, vm):
         """DiracOp::MinResExt: psi (updated in place) = the chronological guess
         from the previous solutions v (orthonormalised in place); vm[i] =

@@ -294,6 +294,21 @@ int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *con
  * (ms per call, ms of the force kernel alone, its algorithmic bytes). */
 int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes);
 
+/* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
+ * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
+ * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or
+ * from the deflated guess U invH U^dag src, with the eigCG bookkeeping when
+ * nev > 0 (m > 2 nev Lanczos vectors in V, restarted to 2 nev Ritz vectors;
+ * on return V[0..2 nev) the last restart's Ritz vectors, M their Ritz
+ * values, 0 past the rank) and deflated restarts at |r| < restart[i] |src|.
+ * U: def_len FP32 deflation vectors; invH: (U^dag A U)^-1, complex,
+ * row-major, (re, im) pairs.  *iterations = the reference's iter;
+ * *true_res = |src - A sol| / |src|.  Unlike the reference's eigen_solver,
+ * whose QL step leaves the eigenvectors uncomputed (eigen_solver.C:180-185),
+ * the small eigenproblems here return true eigenvectors. */
+int cpsgpu_inveigcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg_arg *arg, int nev, int m,
+                    double *const *V, double *M, float *const *U, const double *invH, int def_len,
+                    const double *restart, int restart_len, int *iterations, double *true_res);
 /* DiracOp::MinResExt(psi, phi, v, vm, degree) (minresext.C:30-150): the
  * chronological initial guess psi for MatPcDagMatPc psi = phi from degree
  * previous solutions v[] (orthonormalised in place, as the reference does),

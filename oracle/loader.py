@@ -120,6 +120,11 @@ def load_oracle() -> C.CDLL:
         L.orc_minresext.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), i,
                                     _dp]
         L.orc_minresext.restype = None
+        L.orc_sym_eigen.argtypes = [_dp, _dp, _dp, i]
+        L.orc_sym_eigen.restype = None
+        L.orc_inveigcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, d, i, i, i, C.POINTER(_dp), _dp, i,
+                                   C.POINTER(_dp), _dp, _dp, i, _dp]
+        L.orc_inveigcg.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]
@@ -167,6 +172,8 @@ def load_reference() -> C.CDLL:
         for k, a in sig.items():
             getattr(L, k).argtypes = a
             getattr(L, k).restype = None
+        L.ref_eigen_solver.argtypes = [_dp, _dp, _dp, i]
+        L.ref_eigen_solver.restype = i
         L.ref_fp_checksum.argtypes = [C.c_char_p, i, i]
         L.ref_fp_checksum.restype = C.c_uint
         _ref = L

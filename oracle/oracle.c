@@ -1047,3 +1047,250 @@ void orc_fforce_wilson_type(const orc_geom *g, double *mom, const double *u, con
   out[1] = sqrt(L2 / (4.0 * vol));
   out[2] = Linf;
 }
+
+/* ---------------------------------------------------------------------- */
+/* eigCG                                                                   */
+/* ---------------------------------------------------------------------- */
+/* Real symmetric eigenproblem by cyclic Jacobi rotations (Golub and Van
+ * Loan, Matrix Computations, section 8.5): Ap is the packed lower triangle
+ * (element (i, j), j <= i, at i(i+1)/2 + j); on return Evec[k n + i] is
+ * component k of eigenvector i and Eval[i] its eigenvalue (unsorted), the
+ * layout the reference's eigen_solver (eigen_solver.C:40) fills. */
+void orc_sym_eigen(const double *Ap, double *Evec, double *Eval, int n) {
+  double *a = malloc(sizeof(double) * n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j <= i; j++) a[i * n + j] = a[j * n + i] = Ap[i * (i + 1) / 2 + j];
+  for (int i = 0; i < n * n; i++) Evec[i] = 0.0;
+  for (int i = 0; i < n; i++) Evec[i * n + i] = 1.0;
+  double fro = 0.0;
+  for (int i = 0; i < n * n; i++) fro += a[i] * a[i];
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) off += 2.0 * a[p * n + q] * a[p * n + q];
+    if (off <= 1e-30 * fro) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = a[p * n + q];
+        if (apq == 0.0) continue;
+        const double theta = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; k++) { /* columns p, q */
+          const double akp = a[k * n + p], akq = a[k * n + q];
+          a[k * n + p] = c * akp - s * akq;
+          a[k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) { /* rows p, q */
+          const double apk = a[p * n + k], aqk = a[q * n + k];
+          a[p * n + k] = c * apk - s * aqk;
+          a[q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; k++) {
+          const double vkp = Evec[k * n + p], vkq = Evec[k * n + q];
+          Evec[k * n + p] = c * vkp - s * vkq;
+          Evec[k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < n; i++) Eval[i] = a[i * n + i];
+  free(a);
+}
+
+/* indices of the nev smallest of EIG[0..n) (min_eig_index, inv_eig_cg.C:37-51) */
+static void min_eig_index(int *index, int nev, const double *eig, int n) {
+  for (int i = 0; i < nev; i++) index[i] = i;
+  for (int i = nev; i < n; i++) {
+    int mx = 0;
+    for (int j = 1; j < nev; j++)
+      if (eig[index[j]] > eig[index[mx]]) mx = j;
+    if (eig[i] < eig[index[mx]]) index[mx] = i;
+  }
+}
+
+/* DiracOp::InvEigCg (d_op_base/comsrc/inv_eig_cg.C:129-635), step for step:
+ * CG on A = MatPcDagMatPc from a zero guess (or the deflated guess
+ * U invH U^dag src when def_len > 0), with the eigCG bookkeeping when
+ * nev > 0: the Lanczos matrix T of the CG coefficients (packed lower
+ * triangle), the normalised residuals kept in V[0..m), and at i_eig == m the
+ * restart to the 2 nev Ritz vectors of T (lowest nev of T(m) and T(m-1),
+ * orthonormalised, H = Q^T T Q diagonalised, V <- V Q Z, T <- diag(M) plus
+ * the coupling row from A r).  Deflated restarts at the residuals
+ * restart[i] |src|.  M receives the 2 nev Ritz values (0 past the rank).
+ * U holds def_len deflation vectors, invH their inverse projected matrix
+ * (complex, row-major, as (re, im) pairs).  Returns the reference's iter
+ * (the loop index it stopped at); *true_res = |src - A sol| / |src|. */
+int orc_inveigcg(orc_mdagm_fn op, void *ctx, long n, double *sol, const double *src, double stop_rsd, int max_iter,
+                 int nev, int m, double **V, double *M, int def_len, double **U, const double *invH,
+                 const double *restart, int restart_len, double *true_res) {
+  const double src_norm_sq = norm2(src, n);
+  const double stp = src_norm_sq * stop_rsd * stop_rsd;
+  double *r = malloc(sizeof(double) * n), *dir = malloc(sizeof(double) * n), *mmp = malloc(sizeof(double) * n);
+  double *mmp_prev = nev > 0 ? malloc(sizeof(double) * n) : NULL;
+  cplx *Ub = def_len > 0 ? malloc(sizeof(cplx) * def_len) : NULL;
+  cplx *invHUb = def_len > 0 ? malloc(sizeof(cplx) * def_len) : NULL;
+  double dummy;
+  memset(sol, 0, sizeof(double) * n);
+  if (def_len > 0) {
+    for (int ii = 0; ii < def_len; ii++) Ub[ii] = cdot(U[ii], src, n);
+    for (int ii = 0; ii < def_len; ii++) {
+      invHUb[ii] = 0.0;
+      for (int jj = 0; jj < def_len; jj++)
+        invHUb[ii] += (invH[2 * (ii * def_len + jj)] + I * invH[2 * (ii * def_len + jj) + 1]) * Ub[jj];
+    }
+    for (int ii = 0; ii < def_len; ii++) caxpy(sol, invHUb[ii], U[ii], sol, n);
+  }
+  op(ctx, mmp, sol, &dummy);
+  for (long q = 0; q < n; q++) r[q] = dir[q] = src[q] - mmp[q];
+  double res_cur = norm2(r, n), res_prv;
+  int i_eig = 0, iter;
+  double alpha = 1.0, beta = 0.0, alpha_old = 0.0, beta_old = 0.0, pAp;
+  const int nev2 = 2 * nev;
+  double *T = NULL, *Tt = NULL, *Y = NULL, *Q = NULL, *QZ = NULL, *H = NULL, *EIG = NULL, **Vn = NULL;
+  int *INDEX = NULL;
+  if (nev > 0) {
+    T = calloc(m * (m + 1) / 2, sizeof(double));
+    Tt = calloc(m * (m + 1) / 2, sizeof(double));
+    Y = calloc(m * m, sizeof(double));
+    Q = calloc(m * nev2, sizeof(double));
+    QZ = calloc(m * nev2, sizeof(double));
+    H = calloc(nev2 * (nev2 + 1) / 2, sizeof(double));
+    EIG = calloc(m, sizeof(double));
+    INDEX = calloc(nev, sizeof(int));
+    Vn = malloc(sizeof(double *) * nev2);
+    for (int j = 0; j < nev2; j++) Vn[j] = malloc(sizeof(double) * n);
+  }
+  int restarted = 0;
+  for (iter = 0; iter < max_iter; iter++) {
+    if (nev > 0 && i_eig == m) memcpy(mmp_prev, mmp, sizeof(double) * n);
+    res_prv = res_cur;
+    op(ctx, mmp, dir, &pAp);
+    if (pAp == 0) break;
+    if (nev > 0) {
+      if (i_eig != 0) T[(i_eig - 1) * i_eig / 2 + i_eig - 1] = 1.0 / alpha + beta_old / alpha_old;
+      if (i_eig == m) {
+        for (int i = 0; i < m * (m - 1) / 2; i++) Tt[i] = T[i];
+        orc_sym_eigen(Tt, Y, EIG, m - 1);
+        min_eig_index(INDEX, nev, EIG, m - 1);
+        for (int i = nev; i < nev2; i++) {
+          for (int j = 0; j < m - 1; j++) Q[j * nev2 + i] = Y[j * (m - 1) + INDEX[i - nev]];
+          Q[(m - 1) * nev2 + i] = 0.0;
+        }
+        for (int i = 0; i < m * (m + 1) / 2; i++) Tt[i] = T[i];
+        orc_sym_eigen(Tt, Y, EIG, m);
+        min_eig_index(INDEX, nev, EIG, m);
+        for (int i = 0; i < nev; i++)
+          for (int j = 0; j < m; j++) Q[j * nev2 + i] = Y[j * m + INDEX[i]];
+        int rank = nev;
+        for (int i = nev; i < nev2; i++) {
+          for (int j = 0; j < rank; j++) {
+            double xy = 0.0;
+            for (int k = 0; k < m; k++) xy += Q[k * nev2 + i] * Q[k * nev2 + j];
+            for (int k = 0; k < m; k++) Q[k * nev2 + i] -= xy * Q[k * nev2 + j];
+          }
+          double xx = 0.0;
+          for (int k = 0; k < m; k++) xx += Q[k * nev2 + i] * Q[k * nev2 + i];
+          if (xx > 1e-16) {
+            xx = 1.0 / sqrt(xx);
+            for (int k = 0; k < m; k++) Q[k * nev2 + rank] = xx * Q[k * nev2 + i];
+            rank++;
+          }
+        }
+        for (int i = 0; i < rank; i++)
+          for (int j = 0; j <= i; j++) {
+            double h = 0.0;
+            for (int l = 0; l < m; l++)
+              for (int k = 0; k < m; k++) {
+                const double tlk = (k <= l) ? T[l * (l + 1) / 2 + k] : T[k * (k + 1) / 2 + l];
+                h += Q[l * nev2 + i] * tlk * Q[k * nev2 + j];
+              }
+            H[i * (i + 1) / 2 + j] = h;
+          }
+        orc_sym_eigen(H, Y, M, rank);
+        for (int i = rank; i < nev2; i++) M[i] = 0.0;
+        for (int j = 0; j < rank; j++)
+          for (int i = 0; i < m; i++) {
+            double z = 0.0;
+            for (int k = 0; k < rank; k++) z += Q[i * nev2 + k] * Y[j + k * rank];
+            QZ[i + m * j] = z;
+          }
+        /* V[j] <- sum_i V[i] QZ[i + m j], j < rank (eigcg_vec_mult) */
+        for (int j = 0; j < rank; j++)
+          for (long q = 0; q < n; q++) {
+            double z = 0.0;
+            for (int i = 0; i < m; i++) z += V[i][q] * QZ[i + m * j];
+            Vn[j][q] = z;
+          }
+        for (int j = 0; j < rank; j++) memcpy(V[j], Vn[j], sizeof(double) * n);
+        for (int i = 0; i < m * (m + 1) / 2; i++) T[i] = 0.0;
+        for (int i = 0; i < rank; i++) T[i * (i + 1) / 2 + i] = M[i];
+        i_eig = rank;
+        for (long q = 0; q < n; q++) mmp_prev[q] = -beta * mmp_prev[q] + mmp[q];
+        for (int ii = 0; ii < i_eig; ii++) {
+          double d = 0.0;
+          for (long q = 0; q < n; q++) d += mmp_prev[q] * V[ii][q];
+          T[i_eig * (i_eig + 1) / 2 + ii] = d / sqrt(res_cur);
+        }
+      } else if (i_eig != 0) {
+        T[i_eig * (i_eig + 1) / 2 + i_eig - 1] = -sqrt(beta) / alpha;
+      }
+      const double sc = 1.0 / sqrt(res_cur);
+      for (long q = 0; q < n; q++) V[i_eig][q] = sc * r[q];
+      i_eig++;
+    }
+    alpha_old = alpha;
+    alpha = -res_prv / pAp;
+    res_cur = 0.0;
+    for (long q = 0; q < n; q++) {
+      r[q] = alpha * mmp[q] + r[q];
+      res_cur += r[q] * r[q];
+    }
+    alpha = -alpha;
+    beta_old = beta;
+    beta = res_cur / res_prv;
+    for (long q = 0; q < n; q++) {
+      sol[q] = alpha * dir[q] + sol[q];
+      dir[q] = beta * dir[q] + r[q];
+    }
+    if (restarted < restart_len && def_len > 0 && res_cur < restart[restarted] * restart[restarted] * src_norm_sq) {
+      restarted++;
+      for (int ii = 0; ii < def_len; ii++) Ub[ii] = cdot(U[ii], r, n);
+      for (int ii = 0; ii < def_len; ii++) {
+        invHUb[ii] = 0.0;
+        for (int jj = 0; jj < def_len; jj++)
+          invHUb[ii] += (invH[2 * (ii * def_len + jj)] + I * invH[2 * (ii * def_len + jj) + 1]) * Ub[jj];
+      }
+      memset(dir, 0, sizeof(double) * n);
+      for (int ii = 0; ii < def_len; ii++) caxpy(dir, invHUb[ii], U[ii], dir, n);
+      for (long q = 0; q < n; q++) sol[q] += dir[q];
+      op(ctx, mmp, dir, &dummy);
+      for (long q = 0; q < n; q++) r[q] -= mmp[q];
+      res_cur = norm2(r, n);
+      memcpy(dir, r, sizeof(double) * n);
+    }
+    if (res_cur <= stp) break;
+  }
+  op(ctx, mmp, sol, &dummy);
+  double tr = 0.0;
+  for (long q = 0; q < n; q++) tr += (src[q] - mmp[q]) * (src[q] - mmp[q]);
+  if (true_res) *true_res = sqrt(tr / src_norm_sq);
+  free(r);
+  free(dir);
+  free(mmp);
+  free(mmp_prev);
+  free(Ub);
+  free(invHUb);
+  if (nev > 0) {
+    for (int j = 0; j < nev2; j++) free(Vn[j]);
+    free(Vn);
+    free(T);
+    free(Tt);
+    free(Y);
+    free(Q);
+    free(QZ);
+    free(H);
+    free(EIG);
+    free(INDEX);
+  }
+  return iter;
+}

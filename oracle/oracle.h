@@ -124,6 +124,14 @@ int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, cons
 void orc_minresext(orc_mdagm_fn op, void *ctx, long n, double *psi, const double *phi, double **v, double **vm,
                    int degree, double *error);
 
+/* eigCG (inv_eig_cg.C): the dense symmetric eigensolver it needs (cyclic
+ * Jacobi; eigen_solver.C's layout) and DiracOp::InvEigCg over an
+ * MatPcDagMatPc callback; see oracle.c. */
+void orc_sym_eigen(const double *Ap, double *Evec, double *Eval, int n);
+int orc_inveigcg(orc_mdagm_fn op, void *ctx, long n, double *sol, const double *src, double stop_rsd, int max_iter,
+                 int nev, int m, double **V, double *M, int def_len, double **U, const double *invH,
+                 const double *restart, int restart_len, double *true_res);
+
 /* HMC fermion force (Fwilson / FdwfBase::EvolveMomFforce): sprojTr, the
  * per-link matrix steps and the whole force loop; see oracle.c. */
 void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w, int nblk, int v_stride,

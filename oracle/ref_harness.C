@@ -36,6 +36,8 @@
 USING_NAMESPACE_CPS
 
 namespace cps {
+// the dense symmetric eigensolver eigCG calls (d_op_base/comsrc/eigen_solver.C:40)
+int eigen_solver(Float *A, Float *Evec, Float *Eval, int n);
 // zmobius_m5inv in-place form (d_op_zmobius/noarch/zmobius_m5inv.C:807)
 void zmobius_m5inv(Vector *inout, Float mass, int dag, Zmobus *arg, Complex *K);
 }
@@ -205,6 +207,9 @@ void ref_fforce_wilson_type(double *mom, double *u, double *v1, double *v2, int 
   out[1] = a.L2;
   out[2] = a.Linf;
 }
+
+// ---- eigCG: eigen_solver (packed lower triangle in, Evec[k n + i] = component k of eigenvector i)
+int ref_eigen_solver(double *A, double *Evec, double *Eval, int n) { return eigen_solver(A, Evec, Eval, n); }
 
 // ---- HMC fermion force pieces ----
 // sprojTr{X,Y,Z,T}{m,p} (f_wilson_types/noarch/sproj_tr.C), indexed as the

@@ -9,6 +9,8 @@
 #include <alg/do_arg.h>
 #include <alg/cg_arg.h>
 #include <util/zmobius.h>
+#include <util/random.h>
+#include <comms/glb.h>
 #include <cstdio>
 #include <cstdlib>
 
@@ -32,4 +34,21 @@ void zmobius_Binv_MIT(Vector *, Float, int, Zmobus *, Complex *, Complex *) {
   fprintf(stderr, "ref_shim: zmobius_Binv_MIT\n");
   abort();
 }
+// eigen_solver.C's Lanczos / Ritz helpers (not the dense eigen_solver the
+// harness calls) reference the lattice random generator and slice sums.
+void slice_sum(Float *, int, int) {
+  fprintf(stderr, "ref_shim: slice_sum\n");
+  abort();
+}
+LatRanGen::LatRanGen() {}
+LatRanGen::~LatRanGen() {}
+void LatRanGen::SetSigma(IFloat) {
+  fprintf(stderr, "ref_shim: LatRanGen::SetSigma\n");
+  abort();
+}
+IFloat LatRanGen::Grand(FermionFieldDimension) {
+  fprintf(stderr, "ref_shim: LatRanGen::Grand\n");
+  abort();
+}
+LatRanGen LRG;
 CPS_END_NAMESPACE

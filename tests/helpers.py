@@ -176,6 +176,25 @@ class OracleOps:
                              pm, len(v), C.byref(err))
         return psi, v, vm, err.value
 
+    def inveigcg(self, kind, src, nev, m, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, U=None,
+                 invH=None, restart=()):
+        """DiracOp::InvEigCg (inv_eig_cg.C:129-635): returns (sol, iter,
+        true_res, V, M)"""
+        sol = np.zeros(self.n)
+        V = [np.zeros(self.n) for _ in range(max(m, 1))]
+        M = np.zeros(max(2 * nev, 1))
+        U = [np.ascontiguousarray(u, dtype=np.float64) for u in (U or [])]
+        def_len = len(U)
+        ih = np.ascontiguousarray(invH if invH is not None else np.zeros(1), dtype=np.complex128).view(np.float64)
+        rs = np.ascontiguousarray(list(restart) or [0.0], dtype=np.float64)
+        tr = C.c_double()
+        pv = (C.POINTER(C.c_double) * len(V))(*[p(x) for x in V])
+        pu = (C.POINTER(C.c_double) * max(1, def_len))(*([p(x) for x in U] or [None]))
+        it = self.O.orc_inveigcg(self._op(kind, mass, kappa), None, self.n, p(sol), p(np.ascontiguousarray(src)),
+                                 stop_rsd, max_num_iter, nev, m, pv, p(M), def_len, pu, p(np.ascontiguousarray(ih)),
+                                 p(rs), len(restart), C.byref(tr))
+        return sol, it, tr.value, V, M
+
     def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
         """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,
         d_op_dwf.C:682-733): v1 = (chi, D chi), v2 = (psi, D^dag psi) with

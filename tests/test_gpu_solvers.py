@@ -330,3 +330,52 @@ def test_fmatevl_wrappers(oracle):
         y, _ = ops.dwf_mdagm(o, mass)
         assert rel(y + s_ * o, b) < 1e-9
     assert k > 1 and len(rs) == 3
+
+
+def _ritz_match(V, M, Vo, Mo):
+    """Ritz values equal after sorting, Ritz vectors equal up to sign"""
+    r = int(np.count_nonzero(Mo))
+    oi, gi = np.argsort(Mo[:r]), np.argsort(M[:r])
+    assert np.allclose(M[:r][gi], Mo[:r][oi], rtol=1e-8, atol=0)
+    for a, b in zip(gi, oi):
+        c = abs(np.dot(V[a], Vo[b])) / (np.linalg.norm(V[a]) * np.linalg.norm(Vo[b]))
+        assert abs(c - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("kind,L,ls,nev,m", [("wilson", (4, 4, 4, 8), 1, 4, 24), ("dwf", (4, 4, 4, 4), 4, 3, 16)])
+def test_inveigcg_matches_oracle(oracle, kind, L, ls, nev, m):
+    """DiracOp::InvEigCg (inv_eig_cg.C:129-635) against the oracle: the same
+    CG (iterations, solution, true residual) and the same Ritz pairs."""
+    mass = 0.1
+    u = gen_gauge(L, seed=191)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpWilson(lat, mass=0.02) if kind == "wilson" else DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    src = gen_gaussian(D.f_size, seed=192)
+    so, ito, tro, Vo, Mo = ops.inveigcg(kind, src, nev, m, mass=mass, kappa=D.kappa, stop_rsd=1e-11)
+    sol = np.ones(D.f_size)
+    it, tr, V, M = D.InvEigCg(sol, src, nev=nev, m=m, stop_rsd=1e-11)
+    assert abs(it - ito) <= 1 and tr < 1e-11 and rel(sol, so) < 1e-10
+    _ritz_match(V, M, Vo, Mo[:2 * nev])
+    # low-mode deflation with the Ritz vectors as FP32 U and invH = (U^dag A U)^-1
+    U = [np.asarray(v, dtype=np.float32) for v in Vo[:nev]]
+    Ud = [x.astype(np.float64) for x in U]
+    AU = [ops.wilson_mdagm(x, D.kappa)[0] if kind == "wilson" else ops.dwf_mdagm(x, mass)[0] for x in Ud]
+    cplx = lambda x: x[0::2] + 1j * x[1::2]
+    Hm = np.array([[np.vdot(cplx(a), cplx(b)) for b in AU] for a in Ud])
+    invH = np.linalg.inv(Hm)
+    so2, ito2, _, _, _ = ops.inveigcg(kind, src, 0, 0, mass=mass, kappa=D.kappa, stop_rsd=1e-11, U=Ud, invH=invH,
+                                      restart=[1e-4])
+    sol2 = np.zeros(D.f_size)
+    it2, tr2, _, _ = D.InvEigCg(sol2, src, stop_rsd=1e-11, U=U, invH=invH, restart=[1e-4])
+    assert abs(it2 - ito2) <= 1 and tr2 < 1e-11 and rel(sol2, so2) < 1e-10
+
+
+def test_inveigcg_argument_checks(oracle):
+    L = (4, 4, 4, 4)
+    lat = Lattice(L)
+    lat.import_gauge(gen_gauge(L, seed=193))
+    D = DiracOpWilson(lat, mass=0.1)
+    with pytest.raises(A.CpsGpuError):
+        D.InvEigCg(np.zeros(D.f_size), np.ones(D.f_size), nev=4, m=8)  # m must exceed 2 nev

@@ -229,3 +229,30 @@ def test_mobius_force_vs_reference(oracle, reference, L, ls, mass, b, c):
                                      p(s_inner(v2, L, ls, "mobius")), ls, -step, p(out))
     mo, fo = ops.mobius_fforce(frm, step, mass)
     assert rel(mo, mom) < 1e-13 and np.allclose(fo, out, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 24])
+def test_dense_eigensolver_vs_reference(oracle, reference, n):
+    """The oracle's Jacobi eigensolver against the reference's eigen_solver
+    (eigen_solver.C:40, Householder tridiagonalisation + implicit QL) on a
+    random symmetric matrix in the packed lower-triangle layout eigCG passes:
+    the same eigenvalues.  The reference's vectors are not eigenvectors: its
+    tqli has the eigenvector update commented out (eigen_solver.C:180-185), so
+    Evec holds tred2's orthogonal transform; the test records that, and the
+    library's eigCG uses true eigenvectors (Evec[k n + i] = component k of
+    vector i)."""
+    rng = np.random.default_rng(250 + n)
+    a = rng.normal(size=(n, n))
+    a = a + a.T
+    packed = np.array([a[i, j] for i in range(n) for j in range(i + 1)])
+    er, vr, eo, vo = np.zeros(n), np.zeros(n * n), np.zeros(n), np.zeros(n * n)
+    reference.ref_eigen_solver(p(packed.copy()), p(vr), p(er), n)
+    oracle.orc_sym_eigen(p(packed), p(vo), p(eo), n)
+    scale = np.abs(er).max()
+    assert np.allclose(np.sort(eo), np.sort(er), rtol=0, atol=1e-12 * scale)
+    Vo, Vr = vo.reshape(n, n), vr.reshape(n, n)
+    assert np.allclose(a @ Vo, Vo * eo, atol=1e-11 * scale)
+    assert np.allclose(Vo.T @ Vo, np.eye(n), atol=1e-12)
+    assert np.allclose(Vr.T @ Vr, np.eye(n), atol=1e-12)  # orthogonal ...
+    if n > 1:
+        assert np.abs(a @ Vr - Vr * er).max() > 1e-3 * scale  # ... but not the eigenvectors

@@ -175,3 +175,56 @@ def test_minresext_properties(oracle, kind):
     assert rel(vm[1], y) < 1e-14
     psi0, _, _, e0 = ops.minresext(kind, phi, [], mass=0.1, kappa=0.12)
     assert not psi0.any()
+
+
+def _dense_mdagm(ops, kappa):
+    """MatPcDagMatPc of a tiny Wilson lattice as a dense real matrix"""
+    A = np.zeros((ops.n, ops.n))
+    for k in range(ops.n):
+        e = np.zeros(ops.n)
+        e[k] = 1.0
+        A[:, k] = ops.wilson_mdagm(e, kappa)[0]
+    return 0.5 * (A + A.T)
+
+
+def test_inveigcg_cg_unchanged_and_ritz_pairs(oracle):
+    """DiracOp::InvEigCg (inv_eig_cg.C): the eigCG bookkeeping leaves the CG
+    iterates untouched (same iterations, same solution), the first 2 nev of V
+    are orthonormal Ritz vectors with M their Rayleigh quotients, and the
+    lowest Ritz value approaches the lowest eigenvalue of MatPcDagMatPc."""
+    L, kappa = (2, 2, 2, 4), 0.1245
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=61), ls=1)
+    A = _dense_mdagm(ops, kappa)
+    ev = np.linalg.eigvalsh(A)
+    src = gen_gaussian(ops.n, seed=62)
+    s0, it0, tr0, _, _ = ops.inveigcg("wilson", src, 0, 0, kappa=kappa, stop_rsd=1e-12)
+    s1, it1, tr1, V, M = ops.inveigcg("wilson", src, 4, 20, kappa=kappa, stop_rsd=1e-12)
+    assert it0 == it1 and np.array_equal(s0, s1) and tr1 < 1e-12
+    xo, _, _ = ops.invcg("wilson", src, kappa=kappa, stop_rsd=1e-12)
+    assert rel(s1, xo) < 1e-9
+    rank = int(np.count_nonzero(M))
+    assert rank >= 4
+    W = np.array(V[:rank])
+    assert np.allclose(W @ W.T, np.eye(rank), atol=1e-8)  # CG residuals stay orthogonal to rounding
+    for j in range(rank):
+        assert abs(W[j] @ A @ W[j] - M[j]) < 1e-9 * ev[-1]
+    assert abs(np.min(M[:rank]) - ev[0]) < 1e-3 * ev[0]
+
+
+def test_inveigcg_deflation(oracle):
+    """Low-mode deflation: with U the Ritz vectors of a previous eigCG solve
+    (FP32, as the reference stores them) and invH = (U^dag A U)^-1, the
+    deflated solve starts from U invH U^dag src, restarts deflated at the
+    given residual, and converges to the same solution in fewer iterations."""
+    L, kappa = (2, 2, 2, 4), 0.1245
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=63), ls=1)
+    src = gen_gaussian(ops.n, seed=64)
+    s0, it0, _, V, M = ops.inveigcg("wilson", src, 4, 20, kappa=kappa, stop_rsd=1e-12)
+    U = [np.asarray(v, dtype=np.float32).astype(np.float64) for v in V[:6]]
+    Uc = [u[0::2] + 1j * u[1::2] for u in U]
+    AU = [ops.wilson_mdagm(u, kappa)[0] for u in U]
+    AUc = [a[0::2] + 1j * a[1::2] for a in AU]
+    Hm = np.array([[np.vdot(Uc[i], AUc[j]) for j in range(6)] for i in range(6)])
+    s1, it1, tr1, _, _ = ops.inveigcg("wilson", src, 0, 0, kappa=kappa, stop_rsd=1e-12, U=U,
+                                      invH=np.linalg.inv(Hm), restart=[1e-5])
+    assert tr1 < 1e-12 and rel(s1, s0) < 1e-9 and it1 < it0
