@@ -49,6 +49,13 @@ class NerscHeader(C.Structure):
 FP_FORMATS = {"IEEE32": 3, "IEEE32BIG": 4, "IEEE32LITTLE": 5, "IEEE64": 6, "IEEE64BIG": 7, "IEEE64LITTLE": 8}
 
 
+class RitzArg(C.Structure):
+    """cpsgpu_ritz_arg (DiracOp::Ritz parameters)"""
+    _fields_ = [("RsdR_a", C.c_double), ("RsdR_r", C.c_double), ("Rsdlam", C.c_double), ("Cutl_zero", C.c_double),
+                ("Cv_fact", C.c_double), ("n_renorm", C.c_int), ("Kalk_Sim", C.c_int), ("N_min", C.c_int),
+                ("N_max", C.c_int), ("MaxCG", C.c_int), ("ProjApsiP", C.c_int), ("neg", C.c_int)]
+
+
 class CgArg(C.Structure):
     _fields_ = [("stop_rsd", C.c_double), ("max_num_iter", C.c_int), ("src_norm_sq", C.c_double),
                 ("shift", C.c_double), ("precision", C.c_int), ("delta", C.c_double), ("chunk", C.c_int),
@@ -111,6 +118,7 @@ def lib() -> C.CDLL:
             "cpsgpu_time_fforce": (C.c_int, [vp, C.c_int, _dp, _dp, _dp]),
             "cpsgpu_rhmc_evolve_mom_fforce": (C.c_int, [vp, _dp, C.POINTER(_dp), C.c_int, _dp, C.c_double, C.c_int,
                                                         C.POINTER(ForceArg)]),
+            "cpsgpu_ritz": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), _dp, _ip]),
             "cpsgpu_inveigcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.c_int, C.c_int, C.POINTER(_dp), _dp,
                                           C.POINTER(C.POINTER(C.c_float)), _dp, C.c_int, _dp, C.c_int, _ip, _dp]),
             "cpsgpu_minresext": (C.c_int, [vp, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp]),

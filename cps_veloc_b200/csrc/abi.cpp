@@ -26,6 +26,7 @@ int bicgstab(Dirac &D, Field &psi, const Field &chi, double chi_norm, int nn, do
 void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
 void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
                double *error);
+int ritz(Dirac &D, std::vector<Field> &psi_all, int N_eig, const RitzArgs &ra, double *lambda_out);
 int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
              std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<std::complex<double>> &invH,
              const double *restart, int restart_len, double *true_res);
@@ -714,6 +715,38 @@ int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_ke
     if (kernel_bytes) *kernel_bytes = fforce_bytes(D);
     return CPSGPU_OK;
   });
+}
+
+int cpsgpu_ritz(cpsgpu_dirac d, double *const *psi_all, int N_eig, const cpsgpu_ritz_arg *arg, double *lambda,
+                int *iterations) {
+  int status = CPSGPU_OK;
+  const int rc = guarded([&] {
+    if (!d || !psi_all || !arg) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (N_eig < 1) throw Error(CPSGPU_ERR_ARG, "N_eig must be >= 1");
+    if (arg->n_renorm < 1) throw Error(CPSGPU_ERR_ARG, "n_renorm must be >= 1");
+    for (int k = 0; k < N_eig; k++)
+      if (!psi_all[k]) throw Error(CPSGPU_ERR_ARG, "null vector");
+    need_gauge(d);
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    std::vector<Field> f(N_eig);
+    for (int k = 0; k < N_eig; k++) {
+      f[k].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      const double *h = psi_all[k];
+      upload(L, f[k], &h, 1);
+    }
+    RitzArgs ra{arg->RsdR_a, arg->RsdR_r, arg->Rsdlam, arg->Cutl_zero, arg->Cv_fact, arg->n_renorm,
+                arg->Kalk_Sim, arg->N_min, arg->N_max, arg->MaxCG, arg->ProjApsiP, arg->neg};
+    double lam = 0.0;
+    const int k = ritz(D, f, N_eig, ra, &lam);
+    double *h = psi_all[N_eig - 1];
+    download(L, f[N_eig - 1], &h, 1);
+    if (lambda) *lambda = lam;
+    if (iterations) *iterations = k < 0 ? arg->MaxCG : k;
+    if (k < 0) status = CPSGPU_MAX_ITER;
+    return CPSGPU_OK;
+  });
+  return rc != CPSGPU_OK ? rc : status;
 }
 
 int cpsgpu_inveigcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg_arg *arg, int nev, int m,

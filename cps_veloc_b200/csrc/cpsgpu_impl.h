@@ -199,6 +199,12 @@ void op_mobius_dslash4(const Dirac &D, int prec, const SpinorView &out, const Sp
                        OpWork &w);
 void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag);
 
+// DiracOp::Ritz parameters (krylov.cu)
+struct RitzArgs {
+  double RsdR_a, RsdR_r, Rsdlam, Cutl_zero, Cv_fact;
+  int n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, neg;
+};
+
 // HMC fermion force (force.cu): CalcHmdForceVecs' four half fields and the
 // force loop of EvolveMomFforce on a CANONICAL momentum field in device memory
 struct ForceVecs {

@@ -486,4 +486,153 @@ int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_it
   return iter;
 }
 
+// DiracOp::Ritz (ritz.C:152-532): the N_eig-th lowest eigenpair of A =
+// MatPcDagMatPc (or -A, RitzMatOper NEG_MATPCDAG_MATPC) by conjugate-gradient
+// minimisation of the Ritz functional orthogonal to psi_all[0..N_eig-1),
+// starting from psi_all[N_eig-1], which receives the eigenvector.  The
+// reference's steps and scalar recurrences (the rotation angle from mu, d,
+// g2, p2; the restart and renormalisation rules) run on the host; every
+// vector stays on the device.  Returns k, or -1 after MaxCG iterations.
+int ritz(Dirac &D, std::vector<Field> &psi_all, int N_eig, const RitzArgs &ra, double *lambda_out) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  Field psi(PREC_DOUBLE, L.vh, D.ls, 1), p(PREC_DOUBLE, L.vh, D.ls, 1), Apsi(PREC_DOUBLE, L.vh, D.ls, 1),
+      Ap(PREC_DOUBLE, L.vh, D.ls, 1);
+  auto ritz_mat = [&](Field &out, const Field &in) {
+    c.mdagm(out, in);
+    if (ra.neg) launch_scale(s, -1.0, out.view());
+  };
+  const int nn = N_eig - 1;
+  auto gram_schm = [&](Field &v, int upto) {  // v -= <psi_all[i], v> psi_all[i]
+    for (int i = 0; i < upto; i++) c.caxpy(v, -c.dot(psi_all[i], v), psi_all[i], v);
+  };
+  auto copy = [&](Field &dst, const Field &from) {
+    CPSGPU_CUDA(cudaMemcpyAsync(dst.data.ptr, from.data.ptr, dst.data.bytes, cudaMemcpyDeviceToDevice, s));
+  };
+  double acc = 2.0e-24;
+  acc *= acc;
+  double rsda_sq = ra.RsdR_a * ra.RsdR_a;
+  const double rsdr_sq = ra.RsdR_r * ra.RsdR_r;
+  rsda_sq = (rsda_sq > acc) ? rsda_sq : acc;
+  copy(psi, psi_all[nn]);
+  gram_schm(psi, nn);
+  double d = std::sqrt(c.norm2(psi)), ct = 1.0 / d, st, mu, lambda, g2, p2, g2_0, del_lam, rsd, s1, s2, s3, a, b;
+  launch_scale(s, ct, psi.view());
+  ritz_mat(Apsi, psi);
+  if (ra.ProjApsiP == 1) gram_schm(Apsi, nn);
+  mu = c.dot(psi, Apsi).real();
+  lambda = mu;
+  launch_axpby(s, p.view(), -lambda, psi.view(), Apsi.view());
+  g2 = c.norm2(p);
+  p2 = g2;
+  g2_0 = g2 * ra.Cv_fact;
+  g2_0 = (g2_0 > acc) ? g2_0 : acc;
+  rsd = rsdr_sq * lambda * lambda;
+  rsd = (rsda_sq > rsd) ? rsda_sq : rsd;
+  int result = -1;
+  if (ra.Kalk_Sim == 0 && ra.N_min <= 0 && g2 <= rsd) {
+    copy(psi_all[nn], psi);
+    result = 0;
+  } else {
+    del_lam = mu;
+    for (int k = 1; k <= ra.MaxCG; ++k) {
+      ritz_mat(Ap, p);
+      if (ra.ProjApsiP == 1) gram_schm(Ap, nn);
+      d = c.dot(p, Ap).real() / p2;
+      s1 = 0.5 * (mu + d);
+      s2 = 0.5 * (mu - d);
+      p2 = 1.0 / std::sqrt(p2);
+      s3 = g2 * p2;
+      a = (s2 > 0.0) ? s2 : -s2;
+      if (a >= s3) {
+        d = s3 / s2;
+        d = std::sqrt(1.0 + d * d);
+        a = a * d;
+      } else {
+        d = s2 / s3;
+        d = std::sqrt(1.0 + d * d);
+        a = s3 * d;
+      }
+      s2 /= a;  // cos(delta)
+      s3 /= a;  // sin(delta)
+      if (s2 > 0) {
+        s2 = 0.5 * (1.0 + s2);
+        d = -std::sqrt(s2);  // sin(theta)
+        s2 = -0.5 * s3 / d;  // cos(theta)
+      } else {
+        s2 = 0.5 * (1.0 - s2);
+        s2 = std::sqrt(s2);  // cos(theta)
+        d = -0.5 * s3 / s2;  // sin(theta)
+      }
+      s1 = 2.0 * a * d * d;
+      mu -= s1;
+      lambda = mu;
+      del_lam = s1;
+      st = d * p2;
+      ct = s2;
+      // psi = ct psi + st p;  Apsi = ct Apsi + st Ap;  g = Ap = Apsi - lambda psi
+      launch_scale(s, ct, psi.view());
+      launch_axpby(s, psi.view(), st, p.view(), psi.view());
+      launch_scale(s, ct, Apsi.view());
+      launch_axpby(s, Apsi.view(), st, Ap.view(), Apsi.view());
+      launch_axpby(s, Ap.view(), -lambda, psi.view(), Apsi.view());
+      s1 = g2;
+      g2 = c.norm2(Ap);
+      rsd = rsdr_sq * lambda * lambda;
+      rsd = (rsda_sq > rsd) ? rsda_sq : rsd;
+      st = ra.Rsdlam * std::fabs(mu);
+      if ((ra.Kalk_Sim == 0 && k >= ra.N_min && (std::fabs(mu) < ra.Cutl_zero || (g2 <= rsd && del_lam <= st))) ||
+          (ra.Kalk_Sim == 1 &&
+           (del_lam <= st || std::fabs(mu) < ra.Cutl_zero || (k >= ra.N_min && (g2 < g2_0 || k >= ra.N_max))))) {
+        gram_schm(psi, nn);
+        d = std::sqrt(c.norm2(psi));
+        launch_scale(s, 1.0 / d, psi.view());
+        ritz_mat(Apsi, psi);
+        mu = c.dot(psi, Apsi).real();
+        lambda = mu;
+        copy(psi_all[nn], psi);
+        result = k;
+        break;
+      }
+      b = ct * g2 / s1;
+      ct *= 0.05 * b;
+      d = std::sqrt(g2);
+      ct /= (p2 * d);
+      if (ct > 1.0) {
+        copy(p, Ap);  // restart: p = g
+      } else {
+        c.caxpy(p, -c.dot(psi, p), psi, p);  // p -= <psi, p> psi
+        launch_axpby(s, p.view(), b, p.view(), Ap.view());
+      }
+      if (k % ra.n_renorm == 0) {
+        gram_schm(psi, nn);
+        d = std::sqrt(c.norm2(psi));
+        launch_scale(s, 1.0 / d, psi.view());
+        ritz_mat(Apsi, psi);
+        if (ra.ProjApsiP == 1) gram_schm(Apsi, nn);
+        mu = c.dot(psi, Apsi).real();
+        lambda = mu;
+        launch_axpby(s, Ap.view(), -lambda, psi.view(), Apsi.view());
+        g2 = c.norm2(Ap);
+        gram_schm(p, nn);
+        c.caxpy(p, -c.dot(psi, p), psi, p);
+        cd xp = g2 - c.dot(Ap, p);
+        xp *= 1.0 / g2;
+        c.caxpy(p, xp, Ap, p);
+      } else if (ra.ProjApsiP == 1 && nn > 0) {
+        gram_schm(psi, nn);
+        gram_schm(p, nn);
+      }
+      p2 = c.norm2(p);
+    }
+    if (result < 0) copy(psi_all[nn], psi);
+  }
+  if (lambda_out) *lambda_out = lambda;
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  return result;
+}
+
 }  // namespace cpsgpu

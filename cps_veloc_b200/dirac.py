@@ -307,6 +307,24 @@ class _DiracOp:
                                                   1 if force_measure else 0, C.byref(fa)))
         return fa.L1, fa.L2, fa.Linf
 
+    def Ritz(self, psi_all, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10, Cutl_zero=0.0, n_renorm=10, Kalk_Sim=0,
+             N_min=0, N_max=1000, Cv_fact=0.0, MaxCG=10000, ProjApsiP=0, neg=False):
+        """DiracOp::Ritz (ritz.C:152-532) on MatPcDagMatPc (its negative when
+        neg): the last of psi_all (updated in place) becomes the eigenvector
+        orthogonal to the others; returns (iterations, lambda).  Raises after
+        MaxCG iterations, as the reference exits."""
+        for x in psi_all:
+            _inplace(x, self.f_size)
+        a = A.RitzArg(RsdR_a, RsdR_r, Rsdlam, Cutl_zero, Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG,
+                      ProjApsiP, 1 if neg else 0)
+        pv = (A._dp * len(psi_all))(*[dptr(x) for x in psi_all])
+        lam, k = C.c_double(), C.c_int()
+        rc = lib().cpsgpu_ritz(self._h, pv, len(psi_all), C.byref(a), C.byref(lam), C.byref(k))
+        if rc == A.MAX_ITER:
+            raise A.CpsGpuError(f"too many CG/Ritz iterations: {k.value}")
+        check(rc)
+        return k.value, lam.value
+
     def InvEigCg(self, sol, src, nev=0, m=0, stop_rsd=1e-8, max_num_iter=10000, U=None, invH=None, restart=()):
         """DiracOp::InvEigCg (inv_eig_cg.C:129-635): sol (in place) solves
         MatPcDagMatPc sol = src; returns (iterations, true_res, V, M) with V the

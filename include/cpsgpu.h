@@ -294,6 +294,21 @@ int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *con
  * (ms per call, ms of the force kernel alone, its algorithmic bytes). */
 int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_kernel, double *kernel_bytes);
 
+/* DiracOp::Ritz(psi_all, N_eig, lambda, RsdR_a, RsdR_r, Rsdlam, Cutl_zero,
+ * n_renorm, Kalk_Sim, N_min, N_max, Cv_fact, MaxCG, ProjApsiP)
+ * (d_op_base/comsrc/ritz.C:152-532): the N_eig-th lowest eigenpair of
+ * MatPcDagMatPc (RitzMatOper MATPCDAG_MATPC; neg != 0: of its negative,
+ * NEG_MATPCDAG_MATPC) by conjugate-gradient minimisation of the Ritz
+ * functional orthogonal to psi_all[0..N_eig-1) (previous eigenvectors),
+ * starting from psi_all[N_eig-1], which receives the eigenvector; *lambda
+ * its eigenvalue, *iterations the reference's count.  Returns
+ * CPSGPU_MAX_ITER (the reference exits) after MaxCG iterations. */
+typedef struct {
+  double RsdR_a, RsdR_r, Rsdlam, Cutl_zero, Cv_fact;
+  int n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, neg;
+} cpsgpu_ritz_arg;
+int cpsgpu_ritz(cpsgpu_dirac d, double *const *psi_all, int N_eig, const cpsgpu_ritz_arg *arg, double *lambda,
+                int *iterations);
 /* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
  * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
  * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or

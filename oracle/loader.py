@@ -125,6 +125,9 @@ def load_oracle() -> C.CDLL:
         L.orc_inveigcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, d, i, i, i, C.POINTER(_dp), _dp, i,
                                    C.POINTER(_dp), _dp, _dp, i, _dp]
         L.orc_inveigcg.restype = i
+        L.orc_ritz.argtypes = [MDAGM_FN, C.c_void_p, i, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, d, i,
+                               i, _dp]
+        L.orc_ritz.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

@@ -1294,3 +1294,170 @@ int orc_inveigcg(orc_mdagm_fn op, void *ctx, long n, double *sol, const double *
   }
   return iter;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Ritz eigensolver                                                        */
+/* ---------------------------------------------------------------------- */
+/* psi -= <vec[i], psi> vec[i] for i < nvec (DiracOp::GramSchm, ritz.C:117-150) */
+static void gram_schm(double *psi, double **vec, int nvec, long n) {
+  for (int i = 0; i < nvec; i++) {
+    const cplx xp = cdot(vec[i], psi, n);
+    caxpy(psi, -xp, vec[i], psi, n);
+  }
+}
+
+static double re_dot(const double *a, const double *b, long n) {
+  double s = 0.0;
+  for (long k = 0; k < n; k++) s += a[k] * b[k];
+  return s;
+}
+
+/* DiracOp::Ritz (d_op_base/comsrc/ritz.C:152-532), step for step: the
+ * N_eig-th lowest eigenvector of A = RitzMat (MatPcDagMatPc, negated when
+ * neg: RitzMatOper NEG_MATPCDAG_MATPC) by conjugate-gradient minimisation
+ * of the Ritz functional orthogonal to psi_all[0..N_eig-1), starting from
+ * psi_all[N_eig-1], which receives the eigenvector; *lambda its eigenvalue.
+ * Returns the iteration count k (0 when the start already satisfies the
+ * test); -1 after MaxCG iterations (the reference then exits). */
+int orc_ritz(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi_all, int N_eig, double RsdR_a,
+             double RsdR_r, double Rsdlam, double Cutl_zero, int n_renorm, int Kalk_Sim, int N_min, int N_max,
+             double Cv_fact, int MaxCG, int ProjApsiP, double *lambda_out) {
+  double *psi = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
+  double *Apsi = malloc(sizeof(double) * n), *Ap = malloc(sizeof(double) * n);
+  double dummy;
+#define RITZMAT(out, in)                                  \
+  do {                                                    \
+    op(ctx, out, in, &dummy);                             \
+    if (neg)                                              \
+      for (long q_ = 0; q_ < n; q_++) (out)[q_] = -(out)[q_]; \
+  } while (0)
+  double acc = 2.0e-24;
+  acc *= acc;
+  double rsda_sq = RsdR_a * RsdR_a;
+  const double rsdr_sq = RsdR_r * RsdR_r;
+  rsda_sq = (rsda_sq > acc) ? rsda_sq : acc;
+  const int nn = N_eig - 1;
+  int result = -1;
+  memcpy(psi, psi_all[nn], sizeof(double) * n);
+  gram_schm(psi, psi_all, nn, n);
+  double d = sqrt(norm2(psi, n)), ct = 1.0 / d, st, mu, lambda, g2, p2, g2_0, del_lam, rsd, s1, s2, s3, a, b;
+  for (long q = 0; q < n; q++) psi[q] *= ct;
+  RITZMAT(Apsi, psi);
+  if (ProjApsiP == 1) gram_schm(Apsi, psi_all, nn, n);
+  mu = re_dot(psi, Apsi, n);
+  lambda = mu;
+  for (long q = 0; q < n; q++) p[q] = -lambda * psi[q] + Apsi[q];
+  g2 = norm2(p, n);
+  p2 = g2;
+  g2_0 = g2 * Cv_fact;
+  g2_0 = (g2_0 > acc) ? g2_0 : acc;
+  rsd = rsdr_sq * lambda * lambda;
+  rsd = (rsda_sq > rsd) ? rsda_sq : rsd;
+  if (Kalk_Sim == 0 && N_min <= 0 && g2 <= rsd) {
+    memcpy(psi_all[nn], psi, sizeof(double) * n);
+    result = 0;
+    goto done;
+  }
+  del_lam = mu;
+  for (int k = 1; k <= MaxCG; ++k) {
+    RITZMAT(Ap, p);
+    if (ProjApsiP == 1) gram_schm(Ap, psi_all, nn, n);
+    d = re_dot(p, Ap, n) / p2;
+    s1 = 0.5 * (mu + d);
+    s2 = 0.5 * (mu - d);
+    p2 = 1.0 / sqrt(p2);
+    s3 = g2 * p2;
+    a = (s2 > 0.0) ? s2 : -s2;
+    if (a >= s3) {
+      d = s3 / s2;
+      d = sqrt(1.0 + d * d);
+      a = a * d;
+    } else {
+      d = s2 / s3;
+      d = sqrt(1.0 + d * d);
+      a = s3 * d;
+    }
+    s2 /= a; /* cos(delta) */
+    s3 /= a; /* sin(delta) */
+    if (s2 > 0) {
+      s2 = 0.5 * (1.0 + s2);
+      d = -sqrt(s2);       /* sin(theta) */
+      s2 = -0.5 * s3 / d;  /* cos(theta) */
+    } else {
+      s2 = 0.5 * (1.0 - s2);
+      s2 = sqrt(s2);       /* cos(theta) */
+      d = -0.5 * s3 / s2;  /* sin(theta) */
+    }
+    s1 = 2.0 * a * d * d;
+    mu -= s1;
+    lambda = mu;
+    del_lam = s1;
+    st = d * p2;
+    ct = s2;
+    for (long q = 0; q < n; q++) {
+      psi[q] = st * p[q] + ct * psi[q];
+      Apsi[q] = st * Ap[q] + ct * Apsi[q];
+    }
+    for (long q = 0; q < n; q++) Ap[q] = -lambda * psi[q] + Apsi[q];
+    s1 = g2;
+    g2 = norm2(Ap, n);
+    rsd = rsdr_sq * lambda * lambda;
+    rsd = (rsda_sq > rsd) ? rsda_sq : rsd;
+    st = Rsdlam * fabs(mu);
+    if ((Kalk_Sim == 0 && k >= N_min && (fabs(mu) < Cutl_zero || (g2 <= rsd && del_lam <= st))) ||
+        (Kalk_Sim == 1 && (del_lam <= st || fabs(mu) < Cutl_zero || (k >= N_min && (g2 < g2_0 || k >= N_max))))) {
+      gram_schm(psi, psi_all, nn, n);
+      d = sqrt(norm2(psi, n));
+      ct = 1.0 / d;
+      for (long q = 0; q < n; q++) psi[q] *= ct;
+      RITZMAT(Apsi, psi);
+      mu = re_dot(psi, Apsi, n);
+      lambda = mu;
+      memcpy(psi_all[nn], psi, sizeof(double) * n);
+      result = k;
+      goto done;
+    }
+    b = ct * g2 / s1;
+    ct *= 0.05 * b;
+    d = sqrt(g2);
+    ct /= (p2 * d);
+    if (ct > 1.0) {
+      memcpy(p, Ap, sizeof(double) * n); /* restart: p = g */
+    } else {
+      const cplx xp = cdot(psi, p, n);
+      caxpy(p, -xp, psi, p, n);
+      for (long q = 0; q < n; q++) p[q] = b * p[q] + Ap[q];
+    }
+    if (k % n_renorm == 0) {
+      gram_schm(psi, psi_all, nn, n);
+      d = sqrt(norm2(psi, n));
+      ct = 1.0 / d;
+      for (long q = 0; q < n; q++) psi[q] *= ct;
+      RITZMAT(Apsi, psi);
+      if (ProjApsiP == 1) gram_schm(Apsi, psi_all, nn, n);
+      mu = re_dot(psi, Apsi, n);
+      lambda = mu;
+      for (long q = 0; q < n; q++) Ap[q] = -lambda * psi[q] + Apsi[q];
+      g2 = norm2(Ap, n);
+      gram_schm(p, psi_all, nn, n);
+      double *pp[1] = {psi};
+      gram_schm(p, pp, 1, n);
+      cplx xq = g2 - cdot(Ap, p, n);
+      xq *= 1.0 / g2;
+      caxpy(p, xq, Ap, p, n);
+    } else if (ProjApsiP == 1 && nn > 0) {
+      gram_schm(psi, psi_all, nn, n);
+      gram_schm(p, psi_all, nn, n);
+    }
+    p2 = norm2(p, n);
+  }
+  memcpy(psi_all[nn], psi, sizeof(double) * n);
+done:
+#undef RITZMAT
+  if (lambda_out) *lambda_out = lambda;
+  free(psi);
+  free(p);
+  free(Apsi);
+  free(Ap);
+  return result;
+}

@@ -132,6 +132,12 @@ int orc_inveigcg(orc_mdagm_fn op, void *ctx, long n, double *sol, const double *
                  int nev, int m, double **V, double *M, int def_len, double **U, const double *invH,
                  const double *restart, int restart_len, double *true_res);
 
+/* DiracOp::Ritz (ritz.C:152-532) over an MatPcDagMatPc callback (negated
+ * when neg); see oracle.c. */
+int orc_ritz(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi_all, int N_eig, double RsdR_a,
+             double RsdR_r, double Rsdlam, double Cutl_zero, int n_renorm, int Kalk_Sim, int N_min, int N_max,
+             double Cv_fact, int MaxCG, int ProjApsiP, double *lambda_out);
+
 /* HMC fermion force (Fwilson / FdwfBase::EvolveMomFforce): sprojTr, the
  * per-link matrix steps and the whole force loop; see oracle.c. */
 void orc_sproj_tr(int mu, int sign, double *f, const double *v, const double *w, int nblk, int v_stride,

@@ -195,6 +195,17 @@ class OracleOps:
                                  p(rs), len(restart), C.byref(tr))
         return sol, it, tr.value, V, M
 
+    def ritz(self, kind, psi_all, mass=0.0, kappa=0.0, neg=False, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10,
+             Cutl_zero=0.0, n_renorm=10, Kalk_Sim=0, N_min=0, N_max=1000, Cv_fact=0.0, MaxCG=10000, ProjApsiP=0):
+        """DiracOp::Ritz (ritz.C:152-532) on the last of psi_all (updated in
+        place): returns (iterations, lambda)"""
+        lam = C.c_double()
+        pv = (C.POINTER(C.c_double) * len(psi_all))(*[p(x) for x in psi_all])
+        k = self.O.orc_ritz(self._op(kind, mass, kappa), None, 1 if neg else 0, self.n, pv, len(psi_all), RsdR_a,
+                            RsdR_r, Rsdlam, Cutl_zero, n_renorm, Kalk_Sim, N_min, N_max, Cv_fact, MaxCG, ProjApsiP,
+                            C.byref(lam))
+        return k, lam.value
+
     def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
         """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,
         d_op_dwf.C:682-733): v1 = (chi, D chi), v2 = (psi, D^dag psi) with

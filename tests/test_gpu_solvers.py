@@ -379,3 +379,24 @@ def test_inveigcg_argument_checks(oracle):
     D = DiracOpWilson(lat, mass=0.1)
     with pytest.raises(A.CpsGpuError):
         D.InvEigCg(np.zeros(D.f_size), np.ones(D.f_size), nev=4, m=8)  # m must exceed 2 nev
+
+
+@pytest.mark.parametrize("kind,L,ls", [("wilson", (4, 4, 4, 4), 1), ("dwf", (4, 4, 2, 4), 4)])
+def test_ritz_matches_oracle(oracle, kind, L, ls):
+    """DiracOp::Ritz (ritz.C:152-532) against the oracle: the two lowest
+    eigenpairs in turn, the same iteration counts, eigenvalues and vectors."""
+    mass = 0.1
+    u = gen_gauge(L, seed=201)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpWilson(lat, mass=0.02) if kind == "wilson" else DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    go, gg = [], []
+    for ne in range(2):
+        x = gen_gaussian(D.f_size, seed=202 + ne)
+        go.append(x.copy())
+        gg.append(x.copy())
+        ko, lo = ops.ritz(kind, go, mass=mass, kappa=D.kappa, RsdR_r=1e-8, Rsdlam=1e-11)
+        k, lam = D.Ritz(gg, RsdR_r=1e-8, Rsdlam=1e-11)
+        assert abs(k - ko) <= 1 and abs(lam - lo) < 1e-11 * lo
+        assert rel(gg[-1], go[-1]) < 1e-7

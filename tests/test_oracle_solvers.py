@@ -228,3 +228,25 @@ def test_inveigcg_deflation(oracle):
     s1, it1, tr1, _, _ = ops.inveigcg("wilson", src, 0, 0, kappa=kappa, stop_rsd=1e-12, U=U,
                                       invH=np.linalg.inv(Hm), restart=[1e-5])
     assert tr1 < 1e-12 and rel(s1, s0) < 1e-9 and it1 < it0
+
+
+def test_ritz_finds_the_lowest_eigenpairs(oracle):
+    """DiracOp::Ritz (ritz.C:152-532): successive calls, each orthogonal to
+    the eigenvectors already found, give the lowest eigenvalues of
+    MatPcDagMatPc in order (checked against a dense diagonalisation of the
+    complex operator); NEG_MATPCDAG_MATPC gives minus the largest."""
+    L, kappa = (2, 2, 2, 4), 0.1245
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=61), ls=1)
+    A = _dense_mdagm(ops, kappa)
+    Ac = A[0::2, 0::2] + 1j * A[1::2, 0::2]
+    ev = np.linalg.eigvalsh(Ac)
+    psis = []
+    for ne in range(3):
+        psis.append(gen_gaussian(ops.n, seed=70 + ne))
+        k, lam = ops.ritz("wilson", psis, kappa=kappa, RsdR_a=1e-10, RsdR_r=1e-9, Rsdlam=1e-12)
+        v = psis[-1][0::2] + 1j * psis[-1][1::2]
+        assert k > 0 and abs(lam - ev[ne]) < 1e-12 * ev[-1]
+        assert np.linalg.norm(Ac @ v - lam * v) < 2e-9 * lam and abs(np.linalg.norm(v) - 1) < 1e-12
+    k, lam = ops.ritz("wilson", [gen_gaussian(ops.n, seed=80)], kappa=kappa, neg=True, RsdR_r=1e-9,
+                      Rsdlam=1e-12)
+    assert abs(lam + ev[-1]) < 1e-12 * ev[-1]
