@@ -27,6 +27,9 @@ void fconvert(const int node_sites[4], int ls, double *f, int to, int from);
 void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, std::vector<Field> &vm,
                double *error);
 int ritz(Dirac &D, std::vector<Field> &psi_all, int N_eig, const RitzArgs &ra, double *lambda_out);
+int jacobi(Dirac &D, std::vector<Field> &psi, int N_eig, double *lambda, std::vector<std::complex<double>> &off,
+           double Toler, int N_max);
+int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda);
 int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
              std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<std::complex<double>> &invH,
              const double *restart, int restart_len, double *true_res);
@@ -744,6 +747,71 @@ int cpsgpu_ritz(cpsgpu_dirac d, double *const *psi_all, int N_eig, const cpsgpu_
     if (lambda) *lambda = lam;
     if (iterations) *iterations = k < 0 ? arg->MaxCG : k;
     if (k < 0) status = CPSGPU_MAX_ITER;
+    return CPSGPU_OK;
+  });
+  return rc != CPSGPU_OK ? rc : status;
+}
+
+namespace {
+std::vector<Field> upload_all(cpsgpu_dirac d, double *const *v, int n) {
+  Dirac &D = *d->D;
+  Lattice &L = *D.lat;
+  std::vector<Field> f(n);
+  for (int k = 0; k < n; k++) {
+    if (!v[k]) throw Error(CPSGPU_ERR_ARG, "null vector");
+    f[k].create(PREC_DOUBLE, L.vh, D.ls, 1);
+    const double *h = v[k];
+    upload(L, f[k], &h, 1);
+  }
+  return f;
+}
+void download_all(cpsgpu_dirac d, std::vector<Field> &f, double *const *v) {
+  Lattice &L = *d->D->lat;
+  for (size_t k = 0; k < f.size(); k++) {
+    double *h = v[k];
+    download(L, f[k], &h, 1);
+  }
+}
+}  // namespace
+
+int cpsgpu_jacobi(cpsgpu_dirac d, double *const *psi, int N_eig, double *lambda, double *off_diag, double toler,
+                  int n_max, int *sweeps) {
+  int status = CPSGPU_OK;
+  const int rc = guarded([&] {
+    if (!d || !psi || !lambda || (N_eig > 1 && !off_diag)) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (N_eig < 1) throw Error(CPSGPU_ERR_ARG, "N_eig must be >= 1");
+    need_gauge(d);
+    std::vector<Field> f = upload_all(d, psi, N_eig);
+    std::vector<std::complex<double>> off((size_t)N_eig * (N_eig - 1) / 2);
+    for (size_t k = 0; k < off.size(); k++) off[k] = {off_diag[2 * k], off_diag[2 * k + 1]};
+    const int k = jacobi(*d->D, f, N_eig, lambda, off, toler, n_max);
+    download_all(d, f, psi);
+    for (size_t q = 0; q < off.size(); q++) {
+      off_diag[2 * q] = off[q].real();
+      off_diag[2 * q + 1] = off[q].imag();
+    }
+    if (sweeps) *sweeps = k;
+    if (k < 0) status = CPSGPU_MAX_ITER;
+    return CPSGPU_OK;
+  });
+  return rc != CPSGPU_OK ? rc : status;
+}
+
+int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_ritz_arg *arg, int N_KS_max,
+                    double *lambda, int *iterations) {
+  int status = CPSGPU_OK;
+  const int rc = guarded([&] {
+    if (!d || !psi || !arg || !lambda) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (N_eig < 1) throw Error(CPSGPU_ERR_ARG, "N_eig must be >= 1");
+    if (arg->n_renorm < 1) throw Error(CPSGPU_ERR_ARG, "n_renorm must be >= 1");
+    need_gauge(d);
+    std::vector<Field> f = upload_all(d, psi, N_eig);
+    RitzArgs ra{arg->RsdR_a, arg->RsdR_r, arg->Rsdlam, arg->Cutl_zero, arg->Cv_fact, arg->n_renorm,
+                arg->Kalk_Sim, arg->N_min, arg->N_max, arg->MaxCG, arg->ProjApsiP, 0};
+    const int r = ritz_ks(*d->D, f, ra, N_KS_max, lambda);
+    download_all(d, f, psi);
+    if (iterations) *iterations = r;
+    if (r < 0) status = CPSGPU_MAX_ITER;
     return CPSGPU_OK;
   });
   return rc != CPSGPU_OK ? rc : status;

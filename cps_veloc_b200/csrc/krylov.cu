@@ -635,4 +635,166 @@ int ritz(Dirac &D, std::vector<Field> &psi_all, int N_eig, const RitzArgs &ra, d
   return result;
 }
 
+// DiracOp::Jacobi (jacobi.C:48-268): Jacobi rotations of the vectors psi
+// that zero the complex off-diagonal elements off[j(j-1)/2 + i] =
+// <psi_i, A psi_j> (i < j) of the small matrix with diagonal lambda, until
+// none exceeds |lambda_i lambda_j| Toler^2; then the pairs sorted by
+// |lambda|.  The 2 x 2 rotations and the bookkeeping of the other elements
+// are the reference's, on the host; the vectors rotate on the device.
+// Returns the sweep count, -1 after N_max sweeps.
+int jacobi(Dirac &D, std::vector<Field> &psi, int N_eig, double *lambda, std::vector<cd> &off, double Toler,
+           int N_max) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  Field t1(PREC_DOUBLE, L.vh, D.ls, 1), t2(PREC_DOUBLE, L.vh, D.ls, 1);
+  auto copy = [&](Field &dst, const Field &from) {
+    CPSGPU_CUDA(cudaMemcpyAsync(dst.data.ptr, from.data.ptr, dst.data.bytes, cudaMemcpyDeviceToDevice, s));
+  };
+  const double tol_sq = Toler * Toler;
+  for (int k = 0; k <= N_max; k++) {
+    int i_rot = 0, ij = 0;
+    for (int j = 1; j < N_eig; j++)
+      for (int i = 0; i < j; i++, ij++) {
+        double dd = std::norm(off[ij]);
+        double ftmp = std::fabs(lambda[i] * lambda[j] * tol_sq);
+        if (dd <= ftmp) continue;
+        i_rot++;
+        dd = std::sqrt(dd);
+        const double acc = 100.0 * dd, diff_l = lambda[j] - lambda[i];
+        double t, cs, sn;
+        ftmp = std::fabs(diff_l);
+        if ((ftmp + acc) == ftmp) {
+          t = dd / diff_l;
+        } else {
+          const double theta = 0.5 * diff_l / dd;
+          t = 1.0 / (std::fabs(theta) + std::sqrt(1.0 + theta * theta));
+          if (theta < 0.0) t = -t;
+        }
+        if (diff_l >= 0) {
+          cs = 1.0 / std::sqrt(1.0 + t * t);
+          sn = -t * cs;
+        } else {
+          sn = 1.0 / std::sqrt(1.0 + t * t);
+          cs = t * sn;
+        }
+        double al1 = cs * cs * lambda[i], al2 = cs * cs * lambda[j];
+        al1 += sn * sn * lambda[j];
+        al2 += sn * sn * lambda[i];
+        ftmp = 2.0 * dd * sn * cs;
+        lambda[i] = al1 + ftmp;
+        lambda[j] = al2 - ftmp;
+        const double v11 = cs;
+        const cd v12 = (sn / dd) * off[ij], v21 = -std::conj(v12);
+        off[ij] = 0.0;
+        // psi_i <- v11 psi_i - v21 psi_j;  psi_j <- v11 psi_j - v12 psi_i
+        copy(t1, psi[i]);
+        launch_scale(s, v11, t1.view());
+        c.caxpy(t1, -v21, psi[j], t1);
+        copy(t2, psi[j]);
+        launch_scale(s, v11, t2.view());
+        c.caxpy(t2, -v12, psi[i], t2);
+        copy(psi[i], t1);
+        copy(psi[j], t2);
+        for (int m = 0; m < N_eig; m++) {
+          if (m == i || m == j) continue;
+          if (m < i) {
+            const int mi = i * (i - 1) / 2 + m, mj = j * (j - 1) / 2 + m;
+            const cd c1 = off[mi] * v11 - off[mj] * v21, c2 = off[mj] * v11 - off[mi] * v12;
+            off[mi] = c1;
+            off[mj] = c2;
+          } else if (m < j) {
+            const int mi = m * (m - 1) / 2 + i, mj = j * (j - 1) / 2 + m;
+            const cd c1 = std::conj(off[mi]) * v11 - off[mj] * v21, c2 = off[mj] * v11 - std::conj(off[mi]) * v12;
+            off[mi] = std::conj(c1);
+            off[mj] = c2;
+          } else {
+            const int mi = m * (m - 1) / 2 + i, mj = m * (m - 1) / 2 + j;
+            const cd c1 = std::conj(off[mi]) * v11 - std::conj(off[mj]) * v21;
+            const cd c2 = std::conj(off[mj]) * v11 - std::conj(off[mi]) * v12;
+            off[mi] = std::conj(c1);
+            off[mj] = std::conj(c2);
+          }
+        }
+      }
+    if (i_rot == 0) {
+      for (int j = 1; j < N_eig; j++)
+        for (int i = 0; i < j; i++)
+          if (std::fabs(lambda[j]) < std::fabs(lambda[i])) {
+            std::swap(lambda[i], lambda[j]);
+            std::swap(psi[i], psi[j]);
+          }
+      CPSGPU_CUDA(cudaStreamSynchronize(s));
+      return k;
+    }
+  }
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  return -1;
+}
+
+// The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig
+// (eigen_wilson.C:89-300): sweeps of Ritz on each vector in turn, the
+// off-diagonal elements <psi_j, A psi_i> and Jacobi, until the largest
+// relative eigenvalue change between sweeps is <= Rsdlam; plain successive
+// Ritz calls when N_eig = 1 or Kalk_Sim = 0.  Returns the total Ritz
+// iteration count, or the reference's -1 (a Ritz call hit MaxCG) / -2 (the
+// sweeps ran out, with its test n_KS >= N_KS_max after the loop).
+int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda) {
+  Lattice &L = *D.lat;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  const int N_eig = (int)psi.size();
+  RitzArgs ra = ra0;
+  ra.Cutl_zero = 0.0;
+  ra.neg = 0;
+  int Kalk_Sim = ra.Kalk_Sim;
+  if (N_eig == 1) Kalk_Sim = 0;
+  if (Kalk_Sim == 0) N_KS_max = 0;
+  std::vector<double> lambda_old(N_eig, 1.0);
+  std::vector<cd> off(N_eig > 1 ? (size_t)N_eig * (N_eig - 1) / 2 : 1, 0.0);
+  Field tmp(PREC_DOUBLE, L.vh, D.ls, 1);
+  int ncg_tot = 0;
+  double lambda_t, del_lamb = 1.0;
+  if (Kalk_Sim == 1) {
+    ra.Kalk_Sim = 1;
+    int n_KS;
+    for (n_KS = 1; n_KS <= N_KS_max && del_lamb > ra.Rsdlam; n_KS++) {
+      int ij = 0;
+      for (int i = 0; i < N_eig; i++) {
+        // Ritz on psi[0..i]: the first i held fixed, psi[i] the start
+        const int ncnt = ritz(D, psi, i + 1, ra, &lambda_t);
+        if (ncnt < 0) return ncnt;
+        ncg_tot += ncnt;
+        lambda[i] = lambda_t;
+        c.mdagm(tmp, psi[i]);
+        for (int j = 0; j < i; j++) off[ij++] = c.dot(psi[j], tmp);
+      }
+      jacobi(D, psi, N_eig, lambda, off, ra.RsdR_a, 50);
+      if (n_KS == 1) {
+        for (int i = 0; i < N_eig; i++) lambda_old[i] = lambda[i];
+      } else {
+        del_lamb = 0.0;
+        for (int i = 0; i < N_eig; i++) {
+          lambda_t = std::fabs((lambda_old[i] - lambda[i]) / lambda[i]);
+          if (lambda_t > del_lamb) del_lamb = lambda_t;
+          lambda_old[i] = lambda[i];
+        }
+      }
+    }
+    if (n_KS >= N_KS_max) return -2;
+  } else {
+    ra.Kalk_Sim = 0;
+    ra.N_min = 0;
+    ra.N_max = 0;
+    for (int i = 0; i < N_eig; i++) {
+      ncg_tot += ritz(D, psi, i + 1, ra, &lambda_t);
+      lambda[i] = lambda_t;
+    }
+  }
+  return ncg_tot;
+}
+
 }  // namespace cpsgpu

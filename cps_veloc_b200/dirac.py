@@ -325,6 +325,42 @@ class _DiracOp:
         check(rc)
         return k.value, lam.value
 
+    def RitzEig(self, psi, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10, Cv_fact=0.1, n_renorm=10, Kalk_Sim=1,
+                N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50):
+        """The Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300): psi
+        (start vectors, updated in place) become the len(psi) lowest
+        eigenvectors of MatPcDagMatPc; returns (total Ritz iterations,
+        eigenvalues).  Raises when a Ritz call or the sweeps run out."""
+        for x in psi:
+            _inplace(x, self.f_size)
+        a = A.RitzArg(RsdR_a, RsdR_r, Rsdlam, 0.0, Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, 0)
+        pv = (A._dp * len(psi))(*[dptr(x) for x in psi])
+        lam = np.zeros(len(psi))
+        k = C.c_int()
+        rc = lib().cpsgpu_ritz_eig(self._h, pv, len(psi), C.byref(a), N_KS_max, dptr(lam), C.byref(k))
+        if rc == A.MAX_ITER:
+            raise A.CpsGpuError(f"RitzEig stopped with code {k.value}")
+        check(rc)
+        return k.value, lam
+
+    def Jacobi(self, psi, lam, off_diag, Toler=1e-10, N_max=50):
+        """DiracOp::Jacobi (jacobi.C:48-268): psi and lam (float64, in place)
+        rotated and sorted; off_diag: complex array of N(N-1)/2, zeroed in
+        place; returns the sweep count"""
+        for x in psi:
+            _inplace(x, self.f_size)
+        _inplace(lam, len(psi))
+        if not (isinstance(off_diag, np.ndarray) and off_diag.dtype == np.complex128 and off_diag.flags.c_contiguous):
+            raise TypeError("off_diag must be a C-contiguous complex128 array")
+        pv = (A._dp * len(psi))(*[dptr(x) for x in psi])
+        k = C.c_int()
+        rc = lib().cpsgpu_jacobi(self._h, pv, len(psi), dptr(lam), off_diag.ctypes.data_as(A._dp), Toler, N_max,
+                                 C.byref(k))
+        if rc == A.MAX_ITER:
+            raise A.CpsGpuError("too many Jacobi iterations")
+        check(rc)
+        return k.value
+
     def InvEigCg(self, sol, src, nev=0, m=0, stop_rsd=1e-8, max_num_iter=10000, U=None, invH=None, restart=()):
         """DiracOp::InvEigCg (inv_eig_cg.C:129-635): sol (in place) solves
         MatPcDagMatPc sol = src; returns (iterations, true_res, V, M) with V the

@@ -309,6 +309,25 @@ typedef struct {
 } cpsgpu_ritz_arg;
 int cpsgpu_ritz(cpsgpu_dirac d, double *const *psi_all, int N_eig, const cpsgpu_ritz_arg *arg, double *lambda,
                 int *iterations);
+/* DiracOp::Jacobi(psi, N_eig, lambda, off_diag, Toler, N_max)
+ * (d_op_base/comsrc/jacobi.C:48-268): Jacobi rotations of the vectors psi
+ * (in place) that diagonalise the small hermitian matrix with diagonal
+ * lambda and off-diagonal elements off_diag[j(j-1)/2 + i] = <psi_i, A psi_j>
+ * (i < j; (re, im) pairs), then the pairs sorted by |lambda|.  *sweeps = the
+ * reference's count; CPSGPU_MAX_ITER after N_max sweeps. */
+int cpsgpu_jacobi(cpsgpu_dirac d, double *const *psi, int N_eig, double *lambda, double *off_diag, double toler,
+                  int n_max, int *sweeps);
+/* The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig(psi, lambda,
+ * valid_eig, eig_arg) (d_op_wilson_types/eigen_wilson.C:89-300): the N_eig
+ * lowest eigenpairs of MatPcDagMatPc by sweeps of Ritz (Kalk_Sim stopping
+ * rules) and Jacobi, until the largest relative eigenvalue change is <=
+ * arg->Rsdlam, at most N_KS_max sweeps; successive Ritz calls when N_eig = 1
+ * or arg->Kalk_Sim = 0.  psi (in place): start vectors in, eigenvectors out;
+ * lambda: eigenvalues.  *iterations = the total Ritz count, or the
+ * reference's -1 / -2 with CPSGPU_MAX_ITER returned.  (The gamma_5-hermitian
+ * projection RitzEig applies afterwards is not part of this call.) */
+int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_ritz_arg *arg, int N_KS_max,
+                    double *lambda, int *iterations);
 /* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
  * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
  * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or

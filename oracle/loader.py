@@ -128,6 +128,11 @@ def load_oracle() -> C.CDLL:
         L.orc_ritz.argtypes = [MDAGM_FN, C.c_void_p, i, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, d, i,
                                i, _dp]
         L.orc_ritz.restype = i
+        L.orc_jacobi.argtypes = [C.POINTER(_dp), C.c_long, i, _dp, _dp, d, i]
+        L.orc_jacobi.restype = i
+        L.orc_ritz_ks.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, i, i, i,
+                                  _dp]
+        L.orc_ritz_ks.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

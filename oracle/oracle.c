@@ -1461,3 +1461,183 @@ done:
   free(Ap);
   return result;
 }
+
+/* DiracOp::Jacobi (d_op_base/comsrc/jacobi.C:48-268), step for step: Jacobi
+ * rotations of the vectors psi[0..N) that zero the complex off-diagonal
+ * elements off_diag[j(j-1)/2 + i] = <psi_i, A psi_j> (i < j) of the small
+ * matrix with diagonal lambda, until no element exceeds
+ * |lambda_i lambda_j| Toler^2; then the pairs sorted by |lambda|.  Returns
+ * the sweep count, -1 after N_max sweeps (the reference exits). */
+int orc_jacobi(double **psi, long n, int N_eig, double *lambda, double *off_diag_ri, double Toler, int N_max) {
+  cplx *off = (cplx *)off_diag_ri; /* (re, im) pairs */
+  const double tol_sq = Toler * Toler;
+  double *t1 = malloc(sizeof(double) * n), *t2 = malloc(sizeof(double) * n);
+  int result = -1;
+  for (int k = 0; k <= N_max; k++) {
+    int i_rot = 0, ij = 0;
+    for (int j = 1; j < N_eig; j++)
+      for (int i = 0; i < j; i++) {
+        double dd = creal(off[ij]) * creal(off[ij]) + cimag(off[ij]) * cimag(off[ij]);
+        double ftmp = fabs(lambda[i] * lambda[j] * tol_sq);
+        if (dd > ftmp) {
+          i_rot++;
+          dd = sqrt(dd);
+          const double acc = 100.0 * dd;
+          const double diff_l = lambda[j] - lambda[i];
+          double t, c, s;
+          ftmp = fabs(diff_l);
+          if ((ftmp + acc) == ftmp) {
+            t = dd / diff_l;
+          } else {
+            const double theta = 0.5 * diff_l / dd;
+            t = sqrt(1.0 + theta * theta);
+            t = 1.0 / (fabs(theta) + t);
+            if (theta < 0.0) t = -t;
+          }
+          if (diff_l >= 0) {
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = -t * c;
+          } else {
+            s = 1.0 / sqrt(1.0 + t * t);
+            c = t * s;
+          }
+          double al1 = c * c * lambda[i], al2 = c * c * lambda[j];
+          al1 += s * s * lambda[j];
+          al2 += s * s * lambda[i];
+          ftmp = 2.0 * dd * s * c;
+          al1 += ftmp;
+          al2 -= ftmp;
+          lambda[i] = al1;
+          lambda[j] = al2;
+          const double v11 = c;
+          const cplx v12 = (s / dd) * off[ij];
+          const cplx v21 = -conj(v12);
+          off[ij] = 0.0;
+          for (long q = 0; q < n; q += 2) {
+            const cplx pi = psi[i][q] + I * psi[i][q + 1], pj = psi[j][q] + I * psi[j][q + 1];
+            const cplx a = v11 * pi - v21 * pj, b = v11 * pj - v12 * pi;
+            t1[q] = creal(a);
+            t1[q + 1] = cimag(a);
+            t2[q] = creal(b);
+            t2[q + 1] = cimag(b);
+          }
+          memcpy(psi[i], t1, sizeof(double) * n);
+          memcpy(psi[j], t2, sizeof(double) * n);
+          for (int m = 0; m < N_eig; m++) {
+            if (m == i || m == j) continue;
+            if (m < i) {
+              const int mi = i * (i - 1) / 2 + m, mj = j * (j - 1) / 2 + m;
+              const cplx c1 = off[mi] * v11 - off[mj] * v21, c2 = off[mj] * v11 - off[mi] * v12;
+              off[mi] = c1;
+              off[mj] = c2;
+            } else if (m < j) {
+              const int mi = m * (m - 1) / 2 + i, mj = j * (j - 1) / 2 + m;
+              const cplx c1 = conj(off[mi]) * v11 - off[mj] * v21, c2 = off[mj] * v11 - conj(off[mi]) * v12;
+              off[mi] = conj(c1);
+              off[mj] = c2;
+            } else {
+              const int mi = m * (m - 1) / 2 + i, mj = m * (m - 1) / 2 + j;
+              const cplx c1 = conj(off[mi]) * v11 - conj(off[mj]) * v21;
+              const cplx c2 = conj(off[mj]) * v11 - conj(off[mi]) * v12;
+              off[mi] = conj(c1);
+              off[mj] = conj(c2);
+            }
+          }
+        }
+        ij++;
+      }
+    if (i_rot == 0) {
+      for (int j = 1; j < N_eig; j++)
+        for (int i = 0; i < j; i++)
+          if (fabs(lambda[j]) < fabs(lambda[i])) {
+            const double f = lambda[i];
+            lambda[i] = lambda[j];
+            lambda[j] = f;
+            memcpy(t1, psi[i], sizeof(double) * n);
+            memcpy(psi[i], psi[j], sizeof(double) * n);
+            memcpy(psi[j], t1, sizeof(double) * n);
+          }
+      result = k;
+      break;
+    }
+  }
+  free(t1);
+  free(t2);
+  return result;
+}
+
+/* The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig
+ * (d_op_wilson_types/eigen_wilson.C:89-300): N_eig lowest eigenpairs of
+ * A = MatPcDagMatPc by sweeps of Ritz on each vector in turn (Kalk_Sim
+ * stopping rules), the off-diagonal elements <psi_j, A psi_i>, and Jacobi
+ * rotations, until the largest relative change of an eigenvalue between
+ * sweeps is <= Rsdlam (at most N_KS_max sweeps).  With N_eig = 1 or
+ * Kalk_Sim = 0, plain successive Ritz calls.  lambda[0..N_eig) receives the
+ * eigenvalues (sorted by |lambda| when Jacobi ran).  Returns the total Ritz
+ * iteration count; -1 if a Ritz call hit MaxCG, -2 if the sweeps ran out
+ * (the reference's codes, including its test n_KS >= N_KS_max after the
+ * loop). */
+int orc_ritz_ks(orc_mdagm_fn op, void *ctx, long n, double **psi, int N_eig, double RsdR_a, double RsdR_r,
+                double Rsdlam, double Cv_fact, int n_renorm, int Kalk_Sim, int N_min, int N_max, int MaxCG,
+                int ProjApsiP, int N_KS_max, double *lambda) {
+  if (N_eig == 1) Kalk_Sim = 0;
+  if (Kalk_Sim == 0) N_KS_max = 0;
+  double *lambda_old = malloc(sizeof(double) * N_eig), lambda_t, dummy;
+  double *off = calloc(N_eig > 1 ? N_eig * (N_eig - 1) : 2, sizeof(double)); /* complex pairs */
+  double *tmp = malloc(sizeof(double) * n);
+  int ncg_tot = 0, result;
+  for (int k = 0; k < N_eig; k++) lambda_old[k] = 1.0;
+  double del_lamb = 1.0;
+  if (Kalk_Sim == 1) {
+    int n_KS;
+    for (n_KS = 1; n_KS <= N_KS_max && del_lamb > Rsdlam; n_KS++) {
+      int ij = 0;
+      for (int nn = 1, i = 0; nn <= N_eig; nn++, i++) {
+        const int ncnt = orc_ritz(op, ctx, 0, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, Kalk_Sim, N_min,
+                                  N_max, Cv_fact, MaxCG, ProjApsiP, &lambda_t);
+        if (ncnt < 0) {
+          result = ncnt;
+          goto done;
+        }
+        ncg_tot += ncnt;
+        lambda[i] = lambda_t;
+        op(ctx, tmp, psi[i], &dummy);
+        for (int j = 0; j < i; j++) {
+          const cplx z = cdot(psi[j], tmp, n);
+          off[2 * ij] = creal(z);
+          off[2 * ij + 1] = cimag(z);
+          ij++;
+        }
+      }
+      orc_jacobi(psi, n, N_eig, lambda, off, RsdR_a, 50);
+      if (n_KS == 1) {
+        for (int i = 0; i < N_eig; i++) lambda_old[i] = lambda[i];
+      } else {
+        del_lamb = 0.0;
+        for (int i = 0; i < N_eig; i++) {
+          lambda_t = fabs((lambda_old[i] - lambda[i]) / lambda[i]);
+          if (lambda_t > del_lamb) del_lamb = lambda_t;
+          lambda_old[i] = lambda[i];
+        }
+      }
+    }
+    if (n_KS >= N_KS_max) {
+      result = -2;
+      goto done;
+    }
+  } else {
+    for (int nn = 1, i = 0; nn <= N_eig; nn++, i++) {
+      const int ncnt = orc_ritz(op, ctx, 0, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, 0, 0, 0, Cv_fact,
+                                MaxCG, ProjApsiP, &lambda_t);
+      ncg_tot += ncnt;
+      lambda_old[i] = lambda_t;
+      lambda[i] = lambda_t;
+    }
+  }
+  result = ncg_tot;
+done:
+  free(lambda_old);
+  free(off);
+  free(tmp);
+  return result;
+}

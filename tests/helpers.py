@@ -206,6 +206,17 @@ class OracleOps:
                             C.byref(lam))
         return k, lam.value
 
+    def ritz_ks(self, kind, psi, mass=0.0, kappa=0.0, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10, Cv_fact=0.1,
+                n_renorm=10, Kalk_Sim=1, N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50):
+        """the Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300) on the
+        vectors psi (updated in place): returns (total Ritz iterations or the
+        reference's negative code, eigenvalues)"""
+        lam = np.zeros(len(psi))
+        pv = (C.POINTER(C.c_double) * len(psi))(*[p(x) for x in psi])
+        r = self.O.orc_ritz_ks(self._op(kind, mass, kappa), None, self.n, pv, len(psi), RsdR_a, RsdR_r, Rsdlam,
+                               Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, N_KS_max, p(lam))
+        return r, lam
+
     def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
         """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,
         d_op_dwf.C:682-733): v1 = (chi, D chi), v2 = (psi, D^dag psi) with
@@ -286,3 +297,20 @@ class OracleOps:
         k = self.O.orc_minvcg(fn, None, self.n, arr, p(chi), float(chi @ chi), p(sh), n, p(rs), type, p(al),
                               max_num_iter)
         return psi, k, rs
+
+
+def mix_pairs(V, seed):
+    """rotate pairs of vectors by random 2 x 2 unitaries (complex vectors as re/im pairs)"""
+    rng = np.random.default_rng(seed)
+    Wc = [v[0::2] + 1j * v[1::2] for v in V]
+    out = []
+    for k in range(0, len(Wc), 2):
+        a, b = rng.normal(size=2) + 1j * rng.normal(size=2)
+        u = np.array([[a, -np.conj(b)], [b, np.conj(a)]]) / np.sqrt(abs(a) ** 2 + abs(b) ** 2)
+        out += [u[0, 0] * Wc[k] + u[0, 1] * Wc[k + 1], u[1, 0] * Wc[k] + u[1, 1] * Wc[k + 1]]
+    res = []
+    for w in out:
+        r = np.empty(2 * w.size)
+        r[0::2], r[1::2] = w.real, w.imag
+        res.append(r)
+    return res

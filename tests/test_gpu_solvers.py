@@ -1,13 +1,17 @@
 """Device-resident solvers against the oracle's CG / multishift CG:
 FP64 CG with the reference's bookkeeping, mixed-precision (FP32 and FP16
 inner) reliable-update CG to a true residual of 1e-10, batched
-right-hand sides, multishift CG, and host-side failure injection."""
+right-hand sides, multishift CG, host-side failure injection, and the
+BiCGstab, MinResExt, eigCG, Ritz, RitzEig and Jacobi routines."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 from cps_veloc_b200 import _abi as A
 from cps_veloc_b200.dirac import DiracOpDwf, DiracOpMobius, DiracOpWilson, Lattice, gen_gauge, gen_gaussian
-from helpers import OracleOps, rel
+from helpers import OracleOps, mix_pairs, rel
+from oracle.loader import p
 
 pytestmark = pytest.mark.gpu
 
@@ -400,3 +404,35 @@ def test_ritz_matches_oracle(oracle, kind, L, ls):
         k, lam = D.Ritz(gg, RsdR_r=1e-8, Rsdlam=1e-11)
         assert abs(k - ko) <= 1 and abs(lam - lo) < 1e-11 * lo
         assert rel(gg[-1], go[-1]) < 1e-7
+
+
+def test_ritz_eig_and_jacobi_match_oracle(oracle):
+    """The Kalkreuter-Simma stage of RitzEig and DiracOp::Jacobi against the
+    oracle: the same iteration count and eigenvalues, the same eigenvectors
+    up to a phase."""
+    L, ls, mass = (4, 4, 2, 4), 4, 0.1
+    u = gen_gauge(L, seed=211)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    start = [gen_gaussian(D.f_size, seed=212 + k) for k in range(4)]
+    po = [x.copy() for x in start]
+    ro, lo = ops.ritz_ks("dwf", po, mass=mass)
+    pg = [x.copy() for x in start]
+    rg, lg = D.RitzEig(pg)
+    assert ro > 0 and abs(rg - ro) <= 4 and np.allclose(lg, lo, rtol=1e-9, atol=0)
+    cplx = lambda x: x[0::2] + 1j * x[1::2]
+    for a, b in zip(pg, po):
+        assert abs(abs(np.vdot(cplx(a), cplx(b))) - 1.0) < 1e-6
+    mixed = mix_pairs(po, 7)
+    AM = [ops.dwf_mdagm(x, mass)[0] for x in mixed]
+    lam = np.array([np.vdot(cplx(x), cplx(y)).real for x, y in zip(mixed, AM)])
+    off = np.array([np.vdot(cplx(mixed[i]), cplx(AM[j])) for j in range(1, 4) for i in range(j)])
+    mg, lamg, offg = [x.copy() for x in mixed], lam.copy(), off.copy()
+    kg = D.Jacobi(mg, lamg, offg)
+    pv = (C.POINTER(C.c_double) * 4)(*[p(x) for x in mixed])
+    ko = oracle.orc_jacobi(pv, ops.n, 4, p(lam), p(off.view(np.float64)), 1e-10, 50)
+    assert kg == ko and np.allclose(lamg, lam, rtol=1e-12, atol=0)
+    for a, b in zip(mg, mixed):
+        assert rel(a, b) < 1e-12

@@ -1,10 +1,13 @@
 """Oracle CG / multishift CG (restatements of inv_cg.C:84-448 and
 minvcg.C:47-353): convergence, the reference's iteration bookkeeping, and
 agreement of the multishift solutions with single-shift solves."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
-from helpers import OracleOps, rel, vh_of
+from helpers import OracleOps, mix_pairs, rel, vh_of
+from oracle.loader import p
 from cps_veloc_b200.dirac import gen_gauge, gen_gaussian
 
 
@@ -250,3 +253,34 @@ def test_ritz_finds_the_lowest_eigenpairs(oracle):
     k, lam = ops.ritz("wilson", [gen_gaussian(ops.n, seed=80)], kappa=kappa, neg=True, RsdR_r=1e-9,
                       Rsdlam=1e-12)
     assert abs(lam + ev[-1]) < 1e-12 * ev[-1]
+
+
+def test_ritz_eig_kalkreuter_simma_and_jacobi(oracle):
+    """The Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300): the four
+    lowest eigenvalues of MatPcDagMatPc, orthonormal eigenvectors, in fewer
+    Ritz iterations than four successive Ritz calls; and DiracOp::Jacobi
+    (jacobi.C) undoing a unitary mixing of eigenvector pairs."""
+    L, kappa = (2, 2, 2, 4), 0.1245
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=61), ls=1)
+    A = _dense_mdagm(ops, kappa)
+    Ac = A[0::2, 0::2] + 1j * A[1::2, 0::2]
+    ev = np.linalg.eigvalsh(Ac)
+    psi = [gen_gaussian(ops.n, seed=90 + k) for k in range(4)]
+    r, lam = ops.ritz_ks("wilson", psi, kappa=kappa)
+    assert r > 0 and np.allclose(lam, ev[:4], rtol=1e-8, atol=0)
+    W = np.array([x[0::2] + 1j * x[1::2] for x in psi])
+    assert np.allclose(W.conj() @ W.T, np.eye(4), atol=1e-12)
+    plain = [gen_gaussian(ops.n, seed=90 + k) for k in range(4)]
+    r0, lam0 = ops.ritz_ks("wilson", plain, kappa=kappa, Kalk_Sim=0, Rsdlam=1e-12, RsdR_r=1e-10)
+    assert np.allclose(lam0, ev[:4], rtol=1e-10, atol=0) and r < r0
+    # Jacobi on a mixed basis
+    mixed = mix_pairs(psi, 5)
+    Mc = [x[0::2] + 1j * x[1::2] for x in mixed]
+    lj = np.array([np.vdot(m, Ac @ m).real for m in Mc])
+    off = np.array([np.vdot(Mc[i], Ac @ Mc[j]) for j in range(1, 4) for i in range(j)])
+    pv = (C.POINTER(C.c_double) * 4)(*[p(x) for x in mixed])
+    k = oracle.orc_jacobi(pv, ops.n, 4, p(lj), p(off.view(np.float64)), 1e-10, 50)
+    assert k >= 1 and np.allclose(lj, lam, rtol=1e-12, atol=0) and np.abs(off).max() < 1e-10 * lam.max()
+    for x, v in zip(mixed, psi):
+        xc, vc = x[0::2] + 1j * x[1::2], v[0::2] + 1j * v[1::2]
+        assert abs(abs(np.vdot(vc, xc)) - 1.0) < 1e-6
