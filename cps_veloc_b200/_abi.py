@@ -120,7 +120,7 @@ def lib() -> C.CDLL:
                                                         C.POINTER(ForceArg)]),
             "cpsgpu_ritz": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), _dp, _ip]),
             "cpsgpu_jacobi": (C.c_int, [vp, C.POINTER(_dp), C.c_int, _dp, _dp, C.c_double, C.c_int, _ip]),
-            "cpsgpu_ritz_eig": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), C.c_int, _dp, _ip]),
+            "cpsgpu_ritz_eig": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), C.c_int, _dp, _ip, _ip]),
             "cpsgpu_inveigcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.c_int, C.c_int, C.POINTER(_dp), _dp,
                                           C.POINTER(C.POINTER(C.c_float)), _dp, C.c_int, _dp, C.c_int, _ip, _dp]),
             "cpsgpu_minresext": (C.c_int, [vp, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp]),

@@ -29,7 +29,8 @@ void minresext(Dirac &D, Field &psi, const Field &phi, std::vector<Field> &v, st
 int ritz(Dirac &D, std::vector<Field> &psi_all, int N_eig, const RitzArgs &ra, double *lambda_out);
 int jacobi(Dirac &D, std::vector<Field> &psi, int N_eig, double *lambda, std::vector<std::complex<double>> &off,
            double Toler, int N_max);
-int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda);
+int ritz_eig(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda_H,
+             int *valid_eig);
 int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
              std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<std::complex<double>> &invH,
              const double *restart, int restart_len, double *true_res);
@@ -798,17 +799,17 @@ int cpsgpu_jacobi(cpsgpu_dirac d, double *const *psi, int N_eig, double *lambda,
 }
 
 int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_ritz_arg *arg, int N_KS_max,
-                    double *lambda, int *iterations) {
+                    double *lambda_H, int *valid_eig, int *iterations) {
   int status = CPSGPU_OK;
   const int rc = guarded([&] {
-    if (!d || !psi || !arg || !lambda) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (!d || !psi || !arg || !lambda_H || !valid_eig) throw Error(CPSGPU_ERR_ARG, "null argument");
     if (N_eig < 1) throw Error(CPSGPU_ERR_ARG, "N_eig must be >= 1");
     if (arg->n_renorm < 1) throw Error(CPSGPU_ERR_ARG, "n_renorm must be >= 1");
     need_gauge(d);
     std::vector<Field> f = upload_all(d, psi, N_eig);
     RitzArgs ra{arg->RsdR_a, arg->RsdR_r, arg->Rsdlam, arg->Cutl_zero, arg->Cv_fact, arg->n_renorm,
-                arg->Kalk_Sim, arg->N_min, arg->N_max, arg->MaxCG, arg->ProjApsiP, 0};
-    const int r = ritz_ks(*d->D, f, ra, N_KS_max, lambda);
+                arg->Kalk_Sim, arg->N_min, arg->N_max, arg->MaxCG, arg->ProjApsiP, arg->neg};
+    const int r = ritz_eig(*d->D, f, ra, N_KS_max, lambda_H, valid_eig);
     download_all(d, f, psi);
     if (iterations) *iterations = r;
     if (r < 0) status = CPSGPU_MAX_ITER;

@@ -734,28 +734,53 @@ int jacobi(Dirac &D, std::vector<Field> &psi, int N_eig, double *lambda, std::ve
   return -1;
 }
 
-// The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig
-// (eigen_wilson.C:89-300): sweeps of Ritz on each vector in turn, the
-// off-diagonal elements <psi_j, A psi_i> and Jacobi, until the largest
-// relative eigenvalue change between sweeps is <= Rsdlam; plain successive
-// Ritz calls when N_eig = 1 or Kalk_Sim = 0.  Returns the total Ritz
-// iteration count, or the reference's -1 (a Ritz call hit MaxCG) / -2 (the
-// sweeps ran out, with its test n_KS >= N_KS_max after the loop).
-int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda) {
+// DiracOpWilsonTypes::RitzEig (eigen_wilson.C:89-586) with RitzEigMat =
+// (-)MatPcDagMatPc.  Kalkreuter-Simma sweeps (lines 187-300): Ritz on each
+// vector in turn, the off-diagonal elements <psi_j, A psi_i> and Jacobi,
+// until the largest relative eigenvalue change between sweeps is <= Rsdlam;
+// plain successive Ritz calls when N_eig = 1 or Kalk_Sim = 0.  Then the
+// projection stage (lines 354-583): rows of the matrix of A between the
+// vectors whose squared norm is below 0.98 lambda_old mark those vectors
+// invalid; every vector from the first invalid one on becomes
+// (1 +- A / sqrt|lambda_old|) psi, normalised; a normalised Gram-Schmidt
+// pass; the matrix elements again and Jacobi with tolerance 1e-5.
+// lambda_H[0..N): the last Jacobi's eigenvalues, lambda_H[N..2N): lambda_old.
+// Returns the total Ritz iteration count, or the reference's -1 (a Ritz call
+// hit MaxCG) / -2 (the sweeps ran out, with its test n_KS >= N_KS_max after
+// the loop), or -3 when a Jacobi call ran out (the reference exits).
+int ritz_eig(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda_H,
+             int *valid_eig) {
   Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
   Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
   L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
   c.partials = L.partials.as<double>();
   const int N_eig = (int)psi.size();
   RitzArgs ra = ra0;
   ra.Cutl_zero = 0.0;
-  ra.neg = 0;
   int Kalk_Sim = ra.Kalk_Sim;
   if (N_eig == 1) Kalk_Sim = 0;
   if (Kalk_Sim == 0) N_KS_max = 0;
-  std::vector<double> lambda_old(N_eig, 1.0);
+  double *lambda = lambda_H, *lambda_old = lambda_H + N_eig;
   std::vector<cd> off(N_eig > 1 ? (size_t)N_eig * (N_eig - 1) / 2 : 1, 0.0);
-  Field tmp(PREC_DOUBLE, L.vh, D.ls, 1);
+  Field tmp(PREC_DOUBLE, L.vh, D.ls, 1), tmp2(PREC_DOUBLE, L.vh, D.ls, 1);
+  auto eig_mat = [&](Field &out, const Field &in) {
+    c.mdagm(out, in);
+    if (ra.neg) launch_scale(s, -1.0, out.view());
+  };
+  auto herm_elements = [&](int n_vec) {
+    int ij = 0;
+    for (int i = 0; i < n_vec; i++) {
+      eig_mat(tmp, psi[i]);
+      lambda[i] = c.dot(psi[i], tmp).real();
+      for (int j = 0; j < i; j++) off[ij++] = c.dot(psi[j], tmp);
+    }
+  };
+  auto normalise = [&](Field &x) { launch_scale(s, 1.0 / std::sqrt(c.norm2(x)), x.view()); };
+  for (int k = 0; k < N_eig; k++) {
+    lambda_old[k] = 1.0;
+    valid_eig[k] = 0;
+  }
   int ncg_tot = 0;
   double lambda_t, del_lamb = 1.0;
   if (Kalk_Sim == 1) {
@@ -769,10 +794,10 @@ int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max
         if (ncnt < 0) return ncnt;
         ncg_tot += ncnt;
         lambda[i] = lambda_t;
-        c.mdagm(tmp, psi[i]);
+        eig_mat(tmp, psi[i]);
         for (int j = 0; j < i; j++) off[ij++] = c.dot(psi[j], tmp);
       }
-      jacobi(D, psi, N_eig, lambda, off, ra.RsdR_a, 50);
+      if (jacobi(D, psi, N_eig, lambda, off, ra.RsdR_a, 50) < 0) return -3;
       if (n_KS == 1) {
         for (int i = 0; i < N_eig; i++) lambda_old[i] = lambda[i];
       } else {
@@ -791,9 +816,61 @@ int ritz_ks(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max
     ra.N_max = 0;
     for (int i = 0; i < N_eig; i++) {
       ncg_tot += ritz(D, psi, i + 1, ra, &lambda_t);
-      lambda[i] = lambda_t;
+      lambda_old[i] = lambda_t;
     }
   }
+  // projection onto the eigenvectors of RitzEigMat itself
+  herm_elements(N_eig);
+  for (int i = 0; i < N_eig; i++) valid_eig[i] = 1;
+  for (bool looping = true; looping;) {
+    looping = false;
+    for (int i = 0; i < N_eig; i++) {
+      if (!valid_eig[i]) continue;
+      const double rEig2 = 1.0 / lambda_old[i];
+      double sum = lambda[i] * lambda[i] * rEig2;
+      int xy = 0;
+      for (int x = 0; x < N_eig; x++)
+        for (int y = 0; y < x; y++) {
+          if ((x == i && valid_eig[y]) || (y == i && valid_eig[x])) sum += std::norm(off[xy]) * rEig2;
+          xy++;
+        }
+      if (sum < 0.98) {
+        valid_eig[i] = 0;
+        looping = true;
+      }
+    }
+  }
+  int N_dp = 0, i;
+  for (i = 0; i < N_eig; i++) {
+    if (valid_eig[i] == 1) N_dp++;
+    else break;
+  }
+  for (i++; i < N_eig; i++) valid_eig[i] = 0;
+  for (; N_dp < N_eig; N_dp++) {
+    valid_eig[N_dp] = 1;
+    const double lam = std::sqrt(std::fabs(lambda_old[N_dp]));
+    eig_mat(tmp, psi[N_dp]);
+    const double sign = c.dot(tmp, psi[N_dp]).real() < 0 ? -1.0 : 1.0;
+    launch_axpby(s, tmp2.view(), sign / lam, tmp.view(), psi[N_dp].view());
+    cd snorm = 0.0, onorm = 0.0;
+    for (int k = 0; k < N_dp; k++) snorm += c.dot(tmp2, psi[k]);
+    launch_axpby(s, tmp.view(), -sign / lam, tmp.view(), psi[N_dp].view());
+    for (int k = 0; k < N_dp; k++) onorm += c.dot(tmp, psi[k]);
+    const Field &pick = std::norm(onorm) > std::norm(snorm) ? tmp2 : tmp;
+    CPSGPU_CUDA(cudaMemcpyAsync(psi[N_dp].data.ptr, pick.data.ptr, pick.data.bytes, cudaMemcpyDeviceToDevice, s));
+    normalise(psi[N_dp]);
+  }
+  // GramSchmNorm(psi[b], psi[a]) (eigen_wilson.C:78-85) for every a < b
+  for (int a = 0; a < N_eig; a++)
+    for (int b = a + 1; b < N_eig; b++) {
+      c.caxpy(psi[b], -c.dot(psi[a], psi[b]), psi[a], psi[b]);
+      normalise(psi[b]);
+    }
+  int min_dim = 0;
+  for (int k = 0; k < N_eig; k++)
+    if (valid_eig[k]) min_dim++;
+  herm_elements(min_dim);
+  if (jacobi(D, psi, min_dim, lambda, off, 1.0e-5, 50) < 0) return -3;
   return ncg_tot;
 }
 

@@ -326,22 +326,26 @@ class _DiracOp:
         return k.value, lam.value
 
     def RitzEig(self, psi, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10, Cv_fact=0.1, n_renorm=10, Kalk_Sim=1,
-                N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50):
-        """The Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300): psi
-        (start vectors, updated in place) become the len(psi) lowest
-        eigenvectors of MatPcDagMatPc; returns (total Ritz iterations,
-        eigenvalues).  Raises when a Ritz call or the sweeps run out."""
+                N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50, neg=False):
+        """DiracOpWilsonTypes::RitzEig (eigen_wilson.C:89-586) with RitzMatOper
+        MATPCDAG_MATPC (NEG_MATPCDAG_MATPC when neg): psi (start vectors,
+        updated in place) become the len(psi) lowest eigenvectors; returns
+        (total Ritz iterations, lambda_H, valid_eig) with lambda_H of
+        2 len(psi) entries (eigenvalues, then the Ritz / Kalkreuter-Simma
+        ones).  Raises when a Ritz call, the sweeps or a Jacobi call run out."""
         for x in psi:
             _inplace(x, self.f_size)
-        a = A.RitzArg(RsdR_a, RsdR_r, Rsdlam, 0.0, Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, 0)
+        a = A.RitzArg(RsdR_a, RsdR_r, Rsdlam, 0.0, Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP,
+                      1 if neg else 0)
         pv = (A._dp * len(psi))(*[dptr(x) for x in psi])
-        lam = np.zeros(len(psi))
+        lam = np.zeros(2 * len(psi))
+        valid = (C.c_int * len(psi))()
         k = C.c_int()
-        rc = lib().cpsgpu_ritz_eig(self._h, pv, len(psi), C.byref(a), N_KS_max, dptr(lam), C.byref(k))
+        rc = lib().cpsgpu_ritz_eig(self._h, pv, len(psi), C.byref(a), N_KS_max, dptr(lam), valid, C.byref(k))
         if rc == A.MAX_ITER:
             raise A.CpsGpuError(f"RitzEig stopped with code {k.value}")
         check(rc)
-        return k.value, lam
+        return k.value, lam, np.array(valid[:])
 
     def Jacobi(self, psi, lam, off_diag, Toler=1e-10, N_max=50):
         """DiracOp::Jacobi (jacobi.C:48-268): psi and lam (float64, in place)

@@ -317,17 +317,23 @@ int cpsgpu_ritz(cpsgpu_dirac d, double *const *psi_all, int N_eig, const cpsgpu_
  * reference's count; CPSGPU_MAX_ITER after N_max sweeps. */
 int cpsgpu_jacobi(cpsgpu_dirac d, double *const *psi, int N_eig, double *lambda, double *off_diag, double toler,
                   int n_max, int *sweeps);
-/* The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig(psi, lambda,
- * valid_eig, eig_arg) (d_op_wilson_types/eigen_wilson.C:89-300): the N_eig
- * lowest eigenpairs of MatPcDagMatPc by sweeps of Ritz (Kalk_Sim stopping
- * rules) and Jacobi, until the largest relative eigenvalue change is <=
- * arg->Rsdlam, at most N_KS_max sweeps; successive Ritz calls when N_eig = 1
- * or arg->Kalk_Sim = 0.  psi (in place): start vectors in, eigenvectors out;
- * lambda: eigenvalues.  *iterations = the total Ritz count, or the
- * reference's -1 / -2 with CPSGPU_MAX_ITER returned.  (The gamma_5-hermitian
- * projection RitzEig applies afterwards is not part of this call.) */
+/* DiracOpWilsonTypes::RitzEig(psi, lambda_H, valid_eig, eig_arg)
+ * (d_op_wilson_types/eigen_wilson.C:89-586) with RitzMatOper
+ * MATPCDAG_MATPC (arg->neg = 0) or NEG_MATPCDAG_MATPC (arg->neg = 1):
+ * Kalkreuter-Simma sweeps of Ritz (Kalk_Sim stopping rules) and Jacobi
+ * until the largest relative eigenvalue change is <= arg->Rsdlam, at most
+ * N_KS_max sweeps (successive Ritz calls when N_eig = 1 or
+ * arg->Kalk_Sim = 0); then the projection stage: vectors failing the
+ * reference's row-norm test replaced by (1 +- A / sqrt|lambda|) psi, a
+ * normalised Gram-Schmidt pass and a last Jacobi (tolerance 1e-5).
+ * psi (in place): start vectors in, eigenvectors out; lambda_H[0..N_eig):
+ * the eigenvalues, lambda_H[N_eig..2 N_eig): the Ritz / KS eigenvalues
+ * (the reference's layout); valid_eig[N_eig].  *iterations = the total
+ * Ritz count, or with CPSGPU_MAX_ITER returned the reference's -1 (MaxCG) /
+ * -2 (N_KS_max), or -3 when a Jacobi call ran out (the reference exits).
+ * The reference's text dump of the matrix to eig_arg->fname is not made. */
 int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_ritz_arg *arg, int N_KS_max,
-                    double *lambda, int *iterations);
+                    double *lambda_H, int *valid_eig, int *iterations);
 /* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
  * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
  * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or

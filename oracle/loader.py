@@ -130,9 +130,9 @@ def load_oracle() -> C.CDLL:
         L.orc_ritz.restype = i
         L.orc_jacobi.argtypes = [C.POINTER(_dp), C.c_long, i, _dp, _dp, d, i]
         L.orc_jacobi.restype = i
-        L.orc_ritz_ks.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, i, i, i,
-                                  _dp]
-        L.orc_ritz_ks.restype = i
+        L.orc_ritz_eig.argtypes = [MDAGM_FN, C.c_void_p, i, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, i,
+                                   i, i, _dp, C.POINTER(i)]
+        L.orc_ritz_eig.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

@@ -1566,34 +1566,74 @@ int orc_jacobi(double **psi, long n, int N_eig, double *lambda, double *off_diag
   return result;
 }
 
-/* The Kalkreuter-Simma stage of DiracOpWilsonTypes::RitzEig
- * (d_op_wilson_types/eigen_wilson.C:89-300): N_eig lowest eigenpairs of
- * A = MatPcDagMatPc by sweeps of Ritz on each vector in turn (Kalk_Sim
- * stopping rules), the off-diagonal elements <psi_j, A psi_i>, and Jacobi
- * rotations, until the largest relative change of an eigenvalue between
- * sweeps is <= Rsdlam (at most N_KS_max sweeps).  With N_eig = 1 or
- * Kalk_Sim = 0, plain successive Ritz calls.  lambda[0..N_eig) receives the
- * eigenvalues (sorted by |lambda| when Jacobi ran).  Returns the total Ritz
- * iteration count; -1 if a Ritz call hit MaxCG, -2 if the sweeps ran out
- * (the reference's codes, including its test n_KS >= N_KS_max after the
- * loop). */
-int orc_ritz_ks(orc_mdagm_fn op, void *ctx, long n, double **psi, int N_eig, double RsdR_a, double RsdR_r,
-                double Rsdlam, double Cv_fact, int n_renorm, int Kalk_Sim, int N_min, int N_max, int MaxCG,
-                int ProjApsiP, int N_KS_max, double *lambda) {
+/* RitzEigMat for RitzMatOper MATPCDAG_MATPC / NEG_MATPCDAG_MATPC
+ * (d_op_wilson_types/d_op_wilson_types.C:189-215) */
+static void ritz_eig_mat(orc_mdagm_fn op, void *ctx, int neg, double *out, const double *in, long n) {
+  double dummy;
+  op(ctx, out, in, &dummy);
+  if (neg)
+    for (long q = 0; q < n; q++) out[q] = -out[q];
+}
+
+/* MatHermElements (eigen_wilson.C:708-740): diag[i] = Re <psi_i, A psi_i>,
+ * off[i(i-1)/2 + j] = <psi_j, A psi_i> for j < i */
+static void mat_herm_elements(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi, int n_vec, double *diag,
+                              cplx *off, double *tmp) {
+  int ij = 0;
+  for (int i = 0; i < n_vec; i++) {
+    ritz_eig_mat(op, ctx, neg, tmp, psi[i], n);
+    diag[i] = creal(cdot(psi[i], tmp, n));
+    for (int j = 0; j < i; j++) off[ij++] = cdot(psi[j], tmp, n);
+  }
+}
+
+static void normalise(double *x, long n) {
+  const double f = 1.0 / sqrt(norm2(x, n));
+  for (long q = 0; q < n; q++) x[q] *= f;
+}
+
+/* DiracOpWilsonTypes::RitzEig (d_op_wilson_types/eigen_wilson.C:89-586),
+ * step for step, with RitzEigMat = (-)MatPcDagMatPc.
+ *  1. Kalkreuter-Simma (lines 187-300): sweeps of Ritz on each vector in
+ *     turn (Kalk_Sim stopping rules), the off-diagonal elements
+ *     <psi_j, A psi_i> and Jacobi rotations (tolerance RsdR_a), until the
+ *     largest relative change of an eigenvalue between sweeps is <= Rsdlam,
+ *     at most N_KS_max sweeps; with N_eig = 1 or Kalk_Sim = 0 successive
+ *     Ritz calls (lines 321-330).
+ *  2. Projection (lines 354-583): the matrix elements of RitzEigMat, the
+ *     eigenvectors whose row of that matrix has a squared norm below 0.98
+ *     lambda_old marked invalid (iterated), every vector from the first
+ *     invalid one on replaced by (1 +- A / sqrt|lambda_old|) psi (the sign
+ *     of <A psi, psi>; of the two the one with the larger overlap with the
+ *     valid vectors), normalised; a normalised Gram-Schmidt pass over all;
+ *     the matrix elements again and Jacobi with tolerance 1e-5.
+ * lambda_H[0..N_eig): the eigenvalues of the last Jacobi;
+ * lambda_H[N_eig..2 N_eig): lambda_old (the Ritz / KS eigenvalues);
+ * valid_eig[0..N_eig).  Returns the total Ritz iteration count; -1 if a
+ * Ritz call hit MaxCG, -2 if the sweeps ran out (the reference's codes,
+ * including its test n_KS >= N_KS_max after the loop), -3 if a Jacobi call
+ * ran out (the reference exits).  The reference's text dump of the matrix
+ * to eig_arg->fname is not reproduced. */
+int orc_ritz_eig(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi, int N_eig, double RsdR_a,
+                 double RsdR_r, double Rsdlam, double Cv_fact, int n_renorm, int Kalk_Sim, int N_min, int N_max,
+                 int MaxCG, int ProjApsiP, int N_KS_max, double *lambda_H, int *valid_eig) {
   if (N_eig == 1) Kalk_Sim = 0;
   if (Kalk_Sim == 0) N_KS_max = 0;
-  double *lambda_old = malloc(sizeof(double) * N_eig), lambda_t, dummy;
-  double *off = calloc(N_eig > 1 ? N_eig * (N_eig - 1) : 2, sizeof(double)); /* complex pairs */
-  double *tmp = malloc(sizeof(double) * n);
+  double *lambda = lambda_H, *lambda_old = lambda_H + N_eig, lambda_t;
+  cplx *off = calloc(N_eig > 1 ? (size_t)N_eig * (N_eig - 1) / 2 : 1, sizeof(cplx));
+  double *tmp = malloc(sizeof(double) * n), *tmp2 = malloc(sizeof(double) * n);
   int ncg_tot = 0, result;
-  for (int k = 0; k < N_eig; k++) lambda_old[k] = 1.0;
+  for (int k = 0; k < N_eig; k++) {
+    lambda_old[k] = 1.0;
+    valid_eig[k] = 0;
+  }
   double del_lamb = 1.0;
   if (Kalk_Sim == 1) {
     int n_KS;
     for (n_KS = 1; n_KS <= N_KS_max && del_lamb > Rsdlam; n_KS++) {
       int ij = 0;
       for (int nn = 1, i = 0; nn <= N_eig; nn++, i++) {
-        const int ncnt = orc_ritz(op, ctx, 0, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, Kalk_Sim, N_min,
+        const int ncnt = orc_ritz(op, ctx, neg, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, Kalk_Sim, N_min,
                                   N_max, Cv_fact, MaxCG, ProjApsiP, &lambda_t);
         if (ncnt < 0) {
           result = ncnt;
@@ -1601,15 +1641,13 @@ int orc_ritz_ks(orc_mdagm_fn op, void *ctx, long n, double **psi, int N_eig, dou
         }
         ncg_tot += ncnt;
         lambda[i] = lambda_t;
-        op(ctx, tmp, psi[i], &dummy);
-        for (int j = 0; j < i; j++) {
-          const cplx z = cdot(psi[j], tmp, n);
-          off[2 * ij] = creal(z);
-          off[2 * ij + 1] = cimag(z);
-          ij++;
-        }
+        ritz_eig_mat(op, ctx, neg, tmp, psi[i], n);
+        for (int j = 0; j < i; j++) off[ij++] = cdot(psi[j], tmp, n);
       }
-      orc_jacobi(psi, n, N_eig, lambda, off, RsdR_a, 50);
+      if (orc_jacobi(psi, n, N_eig, lambda, (double *)off, RsdR_a, 50) < 0) {
+        result = -3;
+        goto done;
+      }
       if (n_KS == 1) {
         for (int i = 0; i < N_eig; i++) lambda_old[i] = lambda[i];
       } else {
@@ -1627,17 +1665,77 @@ int orc_ritz_ks(orc_mdagm_fn op, void *ctx, long n, double **psi, int N_eig, dou
     }
   } else {
     for (int nn = 1, i = 0; nn <= N_eig; nn++, i++) {
-      const int ncnt = orc_ritz(op, ctx, 0, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, 0, 0, 0, Cv_fact,
-                                MaxCG, ProjApsiP, &lambda_t);
-      ncg_tot += ncnt;
+      ncg_tot += orc_ritz(op, ctx, neg, n, psi, nn, RsdR_a, RsdR_r, Rsdlam, 0.0, n_renorm, 0, 0, 0, Cv_fact, MaxCG,
+                          ProjApsiP, &lambda_t);
       lambda_old[i] = lambda_t;
-      lambda[i] = lambda_t;
     }
+  }
+  /* projection onto the eigenvectors of RitzEigMat itself */
+  mat_herm_elements(op, ctx, neg, n, psi, N_eig, lambda, off, tmp);
+  for (int i = 0; i < N_eig; i++) valid_eig[i] = 1;
+  for (int looping = 1; looping;) {
+    looping = 0;
+    for (int i = 0; i < N_eig; i++) {
+      if (!valid_eig[i]) continue;
+      const double rEig2 = 1.0 / lambda_old[i];
+      double sum = lambda[i] * lambda[i] * rEig2;
+      int xy = 0;
+      for (int x = 0; x < N_eig; x++)
+        for (int y = 0; y < x; y++) {
+          if ((x == i && valid_eig[y]) || (y == i && valid_eig[x])) {
+            const double v = cabs(off[xy]);
+            sum += v * v * rEig2;
+          }
+          xy++;
+        }
+      if (sum < 0.98) {
+        valid_eig[i] = 0;
+        looping = 1;
+      }
+    }
+  }
+  int N_dp = 0, i;
+  for (i = 0; i < N_eig; i++) {
+    if (valid_eig[i] == 1) N_dp++;
+    else break;
+  }
+  for (i++; i < N_eig; i++) valid_eig[i] = 0;
+  while (N_dp < N_eig) {
+    valid_eig[N_dp] = 1;
+    const double lam = sqrt(fabs(lambda_old[N_dp]));
+    ritz_eig_mat(op, ctx, neg, tmp, psi[N_dp], n);
+    const double proj = creal(cdot(tmp, psi[N_dp], n));
+    const double sign = proj < 0 ? -1.0 : 1.0;
+    for (long q = 0; q < n; q++) tmp2[q] = sign / lam * tmp[q] + psi[N_dp][q];
+    cplx snorm = 0.0, onorm = 0.0;
+    for (int k = 0; k < N_dp; k++) snorm += cdot(tmp2, psi[k], n);
+    for (long q = 0; q < n; q++) tmp[q] = -sign / lam * tmp[q] + psi[N_dp][q];
+    for (int k = 0; k < N_dp; k++) onorm += cdot(tmp, psi[k], n);
+    const double on = creal(onorm) * creal(onorm) + cimag(onorm) * cimag(onorm);
+    const double sn = creal(snorm) * creal(snorm) + cimag(snorm) * cimag(snorm);
+    memcpy(psi[N_dp], on > sn ? tmp2 : tmp, sizeof(double) * n);
+    normalise(psi[N_dp], n);
+    N_dp++;
+  }
+  /* GramSchmNorm(psi[j], psi[i]) (eigen_wilson.C:78-85) for every i < j */
+  for (int a = 0; a < N_eig; a++)
+    for (int b = a + 1; b < N_eig; b++) {
+      const cplx xp = cdot(psi[a], psi[b], n);
+      caxpy(psi[b], -xp, psi[a], psi[b], n);
+      normalise(psi[b], n);
+    }
+  int min_dim = 0;
+  for (int k = 0; k < N_eig; k++)
+    if (valid_eig[k]) min_dim++;
+  mat_herm_elements(op, ctx, neg, n, psi, min_dim, lambda, off, tmp);
+  if (orc_jacobi(psi, n, min_dim, lambda, (double *)off, 1.0e-5, 50) < 0) {
+    result = -3;
+    goto done;
   }
   result = ncg_tot;
 done:
-  free(lambda_old);
   free(off);
   free(tmp);
+  free(tmp2);
   return result;
 }

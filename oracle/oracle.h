@@ -138,12 +138,12 @@ int orc_ritz(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi_all, int 
              double RsdR_r, double Rsdlam, double Cutl_zero, int n_renorm, int Kalk_Sim, int N_min, int N_max,
              double Cv_fact, int MaxCG, int ProjApsiP, double *lambda_out);
 
-/* DiracOp::Jacobi (jacobi.C:48-268) and the Kalkreuter-Simma stage of
- * RitzEig (eigen_wilson.C:89-300); see oracle.c. */
+/* DiracOp::Jacobi (jacobi.C:48-268) and DiracOpWilsonTypes::RitzEig
+ * (eigen_wilson.C:89-586); see oracle.c. */
 int orc_jacobi(double **psi, long n, int N_eig, double *lambda, double *off_diag_ri, double Toler, int N_max);
-int orc_ritz_ks(orc_mdagm_fn op, void *ctx, long n, double **psi, int N_eig, double RsdR_a, double RsdR_r,
-                double Rsdlam, double Cv_fact, int n_renorm, int Kalk_Sim, int N_min, int N_max, int MaxCG,
-                int ProjApsiP, int N_KS_max, double *lambda);
+int orc_ritz_eig(orc_mdagm_fn op, void *ctx, int neg, long n, double **psi, int N_eig, double RsdR_a,
+                 double RsdR_r, double Rsdlam, double Cv_fact, int n_renorm, int Kalk_Sim, int N_min, int N_max,
+                 int MaxCG, int ProjApsiP, int N_KS_max, double *lambda_H, int *valid_eig);
 
 /* HMC fermion force (Fwilson / FdwfBase::EvolveMomFforce): sprojTr, the
  * per-link matrix steps and the whole force loop; see oracle.c. */

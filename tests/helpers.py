@@ -206,16 +206,18 @@ class OracleOps:
                             C.byref(lam))
         return k, lam.value
 
-    def ritz_ks(self, kind, psi, mass=0.0, kappa=0.0, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10, Cv_fact=0.1,
-                n_renorm=10, Kalk_Sim=1, N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50):
-        """the Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300) on the
-        vectors psi (updated in place): returns (total Ritz iterations or the
-        reference's negative code, eigenvalues)"""
-        lam = np.zeros(len(psi))
+    def ritz_eig(self, kind, psi, mass=0.0, kappa=0.0, neg=False, RsdR_a=1e-10, RsdR_r=1e-8, Rsdlam=1e-10,
+                 Cv_fact=0.1, n_renorm=10, Kalk_Sim=1, N_min=5, N_max=50, MaxCG=10000, ProjApsiP=0, N_KS_max=50):
+        """DiracOpWilsonTypes::RitzEig (eigen_wilson.C:89-586) on the vectors
+        psi (updated in place): returns (total Ritz iterations or the
+        reference's negative code, lambda_H (2 len(psi)), valid_eig)"""
+        lam = np.zeros(2 * len(psi))
+        valid = (C.c_int * len(psi))()
         pv = (C.POINTER(C.c_double) * len(psi))(*[p(x) for x in psi])
-        r = self.O.orc_ritz_ks(self._op(kind, mass, kappa), None, self.n, pv, len(psi), RsdR_a, RsdR_r, Rsdlam,
-                               Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, N_KS_max, p(lam))
-        return r, lam
+        r = self.O.orc_ritz_eig(self._op(kind, mass, kappa), None, 1 if neg else 0, self.n, pv, len(psi), RsdR_a,
+                                RsdR_r, Rsdlam, Cv_fact, n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, N_KS_max,
+                                p(lam), valid)
+        return r, lam, np.array(valid[:])
 
     def force_vecs(self, kind, chi, mass=0.0, kappa=0.0):
         """DiracOpWilson / DiracOpDwf::CalcHmdForceVecs (d_op_wilson.C:466-507,

@@ -406,25 +406,30 @@ def test_ritz_matches_oracle(oracle, kind, L, ls):
         assert rel(gg[-1], go[-1]) < 1e-7
 
 
-def test_ritz_eig_and_jacobi_match_oracle(oracle):
-    """The Kalkreuter-Simma stage of RitzEig and DiracOp::Jacobi against the
-    oracle: the same iteration count and eigenvalues, the same eigenvectors
-    up to a phase."""
-    L, ls, mass = (4, 4, 2, 4), 4, 0.1
+@pytest.mark.parametrize("kind,L,ls,nvec,neg", [("dwf", (4, 4, 2, 4), 4, 4, False), ("wilson", (2, 2, 2, 4), 1, 3, True)])
+def test_ritz_eig_and_jacobi_match_oracle(oracle, kind, L, ls, nvec, neg):
+    """DiracOpWilsonTypes::RitzEig (eigen_wilson.C:89-586: Kalkreuter-Simma
+    sweeps and the projection stage) and DiracOp::Jacobi (jacobi.C:48-268)
+    against the oracle: the same iteration count, eigenvalues and valid
+    flags, the same eigenvectors up to a phase."""
+    mass = 0.1
     u = gen_gauge(L, seed=211)
     lat = Lattice(L)
     lat.import_gauge(u)
-    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    D = DiracOpWilson(lat, mass=0.02) if kind == "wilson" else DiracOpDwf(lat, mass=mass, ls=ls)
     ops = OracleOps(oracle, L, u, ls=ls)
-    start = [gen_gaussian(D.f_size, seed=212 + k) for k in range(4)]
+    start = [gen_gaussian(D.f_size, seed=212 + k) for k in range(nvec)]
     po = [x.copy() for x in start]
-    ro, lo = ops.ritz_ks("dwf", po, mass=mass)
+    ro, lo, vo = ops.ritz_eig(kind, po, mass=mass, kappa=D.kappa, neg=neg)
     pg = [x.copy() for x in start]
-    rg, lg = D.RitzEig(pg)
+    rg, lg, vg = D.RitzEig(pg, neg=neg)
     assert ro > 0 and abs(rg - ro) <= 4 and np.allclose(lg, lo, rtol=1e-9, atol=0)
+    assert vg.tolist() == vo.tolist()
     cplx = lambda x: x[0::2] + 1j * x[1::2]
     for a, b in zip(pg, po):
         assert abs(abs(np.vdot(cplx(a), cplx(b))) - 1.0) < 1e-6
+    if neg or nvec % 2:
+        return
     mixed = mix_pairs(po, 7)
     AM = [ops.dwf_mdagm(x, mass)[0] for x in mixed]
     lam = np.array([np.vdot(cplx(x), cplx(y)).real for x, y in zip(mixed, AM)])

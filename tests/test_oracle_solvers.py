@@ -256,23 +256,32 @@ def test_ritz_finds_the_lowest_eigenpairs(oracle):
 
 
 def test_ritz_eig_kalkreuter_simma_and_jacobi(oracle):
-    """The Kalkreuter-Simma stage of RitzEig (eigen_wilson.C:89-300): the four
-    lowest eigenvalues of MatPcDagMatPc, orthonormal eigenvectors, in fewer
-    Ritz iterations than four successive Ritz calls; and DiracOp::Jacobi
-    (jacobi.C) undoing a unitary mixing of eigenvector pairs."""
+    """DiracOpWilsonTypes::RitzEig (eigen_wilson.C:89-586): the four lowest
+    eigenvalues of MatPcDagMatPc and orthonormal eigenvectors, through the
+    Kalkreuter-Simma sweeps (in fewer Ritz iterations than four successive
+    Ritz calls) and the projection stage; and DiracOp::Jacobi (jacobi.C)
+    undoing a unitary mixing of eigenvector pairs."""
     L, kappa = (2, 2, 2, 4), 0.1245
     ops = OracleOps(oracle, L, gen_gauge(L, seed=61), ls=1)
     A = _dense_mdagm(ops, kappa)
     Ac = A[0::2, 0::2] + 1j * A[1::2, 0::2]
     ev = np.linalg.eigvalsh(Ac)
     psi = [gen_gaussian(ops.n, seed=90 + k) for k in range(4)]
-    r, lam = ops.ritz_ks("wilson", psi, kappa=kappa)
-    assert r > 0 and np.allclose(lam, ev[:4], rtol=1e-8, atol=0)
+    r, lh, valid = ops.ritz_eig("wilson", psi, kappa=kappa)
+    assert r > 0 and np.allclose(lh[:4], ev[:4], rtol=1e-8, atol=0) and np.allclose(lh[4:], ev[:4], rtol=1e-8, atol=0)
+    assert valid.tolist() == [1, 1, 1, 1]
     W = np.array([x[0::2] + 1j * x[1::2] for x in psi])
     assert np.allclose(W.conj() @ W.T, np.eye(4), atol=1e-12)
+    for w, l in zip(W, lh[:4]):
+        assert np.linalg.norm(Ac @ w - l * w) < 1e-4 * l
     plain = [gen_gaussian(ops.n, seed=90 + k) for k in range(4)]
-    r0, lam0 = ops.ritz_ks("wilson", plain, kappa=kappa, Kalk_Sim=0, Rsdlam=1e-12, RsdR_r=1e-10)
-    assert np.allclose(lam0, ev[:4], rtol=1e-10, atol=0) and r < r0
+    r0, lam0, _ = ops.ritz_eig("wilson", plain, kappa=kappa, Kalk_Sim=0, Rsdlam=1e-12, RsdR_r=1e-10)
+    assert np.allclose(lam0[:4], ev[:4], rtol=1e-10, atol=0) and r < r0
+    # RitzMatOper NEG_MATPCDAG_MATPC: the three largest, negated, sorted by |lambda|
+    top = [gen_gaussian(ops.n, seed=95 + k) for k in range(3)]
+    rn, ln, _ = ops.ritz_eig("wilson", top, kappa=kappa, neg=True)
+    assert rn > 0 and np.allclose(ln[:3], -ev[-3:], rtol=1e-8, atol=0)
+    lam = lh[:4]
     # Jacobi on a mixed basis
     mixed = mix_pairs(psi, 5)
     Mc = [x[0::2] + 1j * x[1::2] for x in mixed]
