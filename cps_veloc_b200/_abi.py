@@ -56,6 +56,17 @@ class RitzArg(C.Structure):
                 ("N_max", C.c_int), ("MaxCG", C.c_int), ("ProjApsiP", C.c_int), ("neg", C.c_int)]
 
 
+RITZ_MATPCDAG_MATPC, RITZ_NEG_MATPCDAG_MATPC = 3, 4
+
+
+class LanczosArg(C.Structure):
+    """cpsgpu_lanczos_arg (LanczosArg with its MatrixPolynomialArg)"""
+    _fields_ = [("RitzMat_lanczos", C.c_int), ("RitzMat_convcheck", C.c_int), ("nk_lanczos_vectors", C.c_int),
+                ("nt_lanczos_vectors", C.c_int), ("np_lanczos_vectors", C.c_int), ("eigen_shift", C.c_double),
+                ("stop_residual", C.c_double), ("maxiters", C.c_int), ("conv_check", C.c_int), ("Npol", C.c_int),
+                ("params", C.c_double * 2)]
+
+
 class CgArg(C.Structure):
     _fields_ = [("stop_rsd", C.c_double), ("max_num_iter", C.c_int), ("src_norm_sq", C.c_double),
                 ("shift", C.c_double), ("precision", C.c_int), ("delta", C.c_double), ("chunk", C.c_int),
@@ -121,6 +132,7 @@ def lib() -> C.CDLL:
             "cpsgpu_ritz": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), _dp, _ip]),
             "cpsgpu_jacobi": (C.c_int, [vp, C.POINTER(_dp), C.c_int, _dp, _dp, C.c_double, C.c_int, _ip]),
             "cpsgpu_ritz_eig": (C.c_int, [vp, C.POINTER(_dp), C.c_int, C.POINTER(RitzArg), C.c_int, _dp, _ip, _ip]),
+            "cpsgpu_imp_res_lanczos": (C.c_int, [vp, C.POINTER(C.POINTER(C.c_float)), _dp, C.POINTER(LanczosArg), _ip]),
             "cpsgpu_inveigcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.c_int, C.c_int, C.POINTER(_dp), _dp,
                                           C.POINTER(C.POINTER(C.c_float)), _dp, C.c_int, _dp, C.c_int, _ip, _dp]),
             "cpsgpu_minresext": (C.c_int, [vp, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp]),

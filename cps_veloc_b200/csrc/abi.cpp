@@ -31,6 +31,7 @@ int jacobi(Dirac &D, std::vector<Field> &psi, int N_eig, double *lambda, std::ve
            double Toler, int N_max);
 int ritz_eig(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_max, double *lambda_H,
              int *valid_eig);
+int imp_res_lanczos(Dirac &D, std::vector<Field> &V, double *alpha, const LanczosArgs &a);
 int inveigcg(Dirac &D, Field &sol, const Field &src, double stop_rsd, int max_iter, int nev, int m,
              std::vector<Field> &V, double *M, std::vector<Field> &U, const std::vector<std::complex<double>> &invH,
              const double *restart, int restart_len, double *true_res);
@@ -813,6 +814,55 @@ int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_
     download_all(d, f, psi);
     if (iterations) *iterations = r;
     if (r < 0) status = CPSGPU_MAX_ITER;
+    return CPSGPU_OK;
+  });
+  return rc != CPSGPU_OK ? rc : status;
+}
+
+int cpsgpu_imp_res_lanczos(cpsgpu_dirac d, float *const *V, double *alpha, const cpsgpu_lanczos_arg *arg,
+                           int *restarts) {
+  int status = CPSGPU_OK;
+  const int rc = guarded([&] {
+    if (!d || !V || !alpha || !arg) throw Error(CPSGPU_ERR_ARG, "null argument");
+    Dirac &D = *d->D;
+    if (D.kind == KIND_WILSON)
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "RitzMat(V*,V*,MP*) is not implemented for Wilson fermions");
+    const int nk = arg->nk_lanczos_vectors, nt = arg->nt_lanczos_vectors, np = arg->np_lanczos_vectors;
+    if (nk < 2 || nt < 1 || nt > nk || np < 0) throw Error(CPSGPU_ERR_ARG, "need nk >= 2, 1 <= nt <= nk, np >= 0");
+    if (arg->conv_check < 1 || arg->maxiters < 0) throw Error(CPSGPU_ERR_ARG, "need conv_check >= 1, maxiters >= 0");
+    if (arg->Npol < 2) throw Error(CPSGPU_ERR_ARG, "the Chebyshev filter needs Npol >= 2");
+    auto neg_of = [](int t) {
+      if (t == CPSGPU_RITZ_MATPCDAG_MATPC) return 0;
+      if (t == CPSGPU_RITZ_NEG_MATPCDAG_MATPC) return 1;
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "RitzMatOper not implemented (MATPCDAG_MATPC, NEG_MATPCDAG_MATPC are)");
+    };
+    LanczosArgs la{neg_of(arg->RitzMat_lanczos), neg_of(arg->RitzMat_convcheck), nk, nt, np, arg->maxiters,
+                   arg->conv_check, arg->Npol, arg->stop_residual, arg->params[0], arg->params[1], arg->eigen_shift};
+    const double aa = la.p0 * la.p0, bb = (la.p1 + std::fabs(la.eigen_shift)) * (la.p1 + std::fabs(la.eigen_shift));
+    if (!(aa != bb)) throw Error(CPSGPU_ERR_ARG, "the filter interval is empty (params[0]^2 == (params[1] + |eigen_shift|)^2)");
+    const int m = nk + np;
+    for (int k = 0; k < m; k++)
+      if (!V[k]) throw Error(CPSGPU_ERR_ARG, "null Lanczos vector");
+    need_gauge(d);
+    Lattice &L = *D.lat;
+    const size_t nreal = (size_t)24 * L.vh * D.ls;
+    std::vector<Field> fv(m);
+    for (auto &f : fv) f.create(PREC_SINGLE, L.vh, D.ls, 1);
+    Field f64(PREC_DOUBLE, L.vh, D.ls, 1);
+    std::vector<double> h(nreal);
+    for (size_t q = 0; q < nreal; q++) h[q] = (double)V[0][q];
+    const double *hp = h.data();
+    upload(L, f64, &hp, 1);
+    launch_convert(L.stream, PREC_SINGLE, fv[0].view(), PREC_DOUBLE, f64.view());
+    const int it = imp_res_lanczos(D, fv, alpha, la);
+    for (int k = 0; k < m; k++) {
+      launch_convert(L.stream, PREC_DOUBLE, f64.view(), PREC_SINGLE, fv[k].view());
+      double *o = h.data();
+      download(L, f64, &o, 1);
+      for (size_t q = 0; q < nreal; q++) V[k][q] = (float)h[q];
+    }
+    if (restarts) *restarts = it;
+    if (it < 0) status = CPSGPU_NONFINITE;
     return CPSGPU_OK;
   });
   return rc != CPSGPU_OK ? rc : status;

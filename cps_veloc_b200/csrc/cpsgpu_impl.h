@@ -205,6 +205,14 @@ struct RitzArgs {
   int n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, neg;
 };
 
+// DiracOp::ImpResLanczos (krylov.cu): LanczosArg with the Chebyshev filter's
+// MatrixPolynomialArg; neg_*: RitzMatOper NEG_MATPCDAG_MATPC for the filter /
+// the convergence check
+struct LanczosArgs {
+  int neg_lanczos, neg_conv, nk, nt, np, maxiters, conv_check, Npol;
+  double stop_res, p0, p1, eigen_shift;
+};
+
 // HMC fermion force (force.cu): CalcHmdForceVecs' four half fields and the
 // force loop of EvolveMomFforce on a CANONICAL momentum field in device memory
 struct ForceVecs {

@@ -5,6 +5,7 @@
 // matrix) are the reference's short host computations, step for step; each
 // global dot product <a, b> = sum conj(a) b (compDotProduct,
 // vector_util.C:889-903) is a device reduction read back by the host.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -120,6 +121,71 @@ __global__ void __launch_bounds__(256) vec_mult_kernel(const double *const *V, i
 #pragma unroll
       for (int q = 0; q < VM_R; q++)
         if (j0 + q < rank) out[j0 + q][k] = acc[q];
+    }
+}
+
+// <a, b> of two FP32 fields, accumulated in FP64 (per-block partials)
+__global__ void cdot_f_kernel(SpinorView a, SpinorView b, double *partials, size_t n) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (idx < n) {
+    const long sl = (long)(idx / a.vh), i = (long)(idx % a.vh);
+    float x[24], y[24];
+    SpinorIO<PREC_SINGLE>::load(a, sl, i, x);
+    SpinorIO<PREC_SINGLE>::load(b, sl, i, y);
+#pragma unroll
+    for (int k = 0; k < 24; k += 2) {
+      v[0] += (double)x[k] * y[k] + (double)x[k + 1] * y[k + 1];
+      v[1] += (double)x[k] * y[k + 1] - (double)x[k + 1] * y[k];
+    }
+  }
+  block_partial<2>(v, partials);
+}
+
+// y += f x in FP32, f complex (ZAXPYfloat of lanczos_GramSchm_test)
+__global__ void caxpy_f_kernel(SpinorView y, float re, float im, SpinorView x, size_t n) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const long sl = (long)(idx / y.vh), i = (long)(idx % y.vh);
+  float a[24], b[24];
+  SpinorIO<PREC_SINGLE>::load(x, sl, i, a);
+  SpinorIO<PREC_SINGLE>::load(y, sl, i, b);
+#pragma unroll
+  for (int k = 0; k < 24; k += 2) {
+    b[k] += re * a[k] - im * a[k + 1];
+    b[k + 1] += re * a[k + 1] + im * a[k];
+  }
+  SpinorIO<PREC_SINGLE>::store(y, sl, i, b);
+}
+
+// out = a out + b x + c y (the Chebyshev recurrence), a thread per real
+__global__ void cheb_kernel(double *out, double a, double b, const double *x, double c, const double *y, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    double o = a * out[k];
+    o += b * x[k];
+    if (c != 0.0) o += c * y[k];
+    out[k] = o;
+  }
+}
+
+// out[j][k] = sum_i V[i][k] QZ[i + m j] for j < rank with FP32 vectors and
+// FP64 sums (the Lanczos restart's V Q); out must not alias V
+__global__ void __launch_bounds__(256) vec_mult_f_kernel(const float *const *V, int m, const double *QZ, int rank,
+                                                         float *const *out, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    for (int j0 = 0; j0 < rank; j0 += VM_R) {
+      double acc[VM_R];
+#pragma unroll
+      for (int q = 0; q < VM_R; q++) acc[q] = 0.0;
+      for (int i = 0; i < m; i++) {
+        const double v = V[i][k];
+#pragma unroll
+        for (int q = 0; q < VM_R; q++)
+          if (j0 + q < rank) acc[q] = fma(v, QZ[i + m * (j0 + q)], acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < VM_R; q++)
+        if (j0 + q < rank) out[j0 + q][k] = (float)acc[q];
     }
 }
 
@@ -872,6 +938,296 @@ int ritz_eig(Dirac &D, std::vector<Field> &psi, const RitzArgs &ra0, int N_KS_ma
   herm_elements(min_dim);
   if (jacobi(D, psi, min_dim, lambda, off, 1.0e-5, 50) < 0) return -3;
   return ncg_tot;
+}
+
+// ------------------------------------------------- implicitly restarted Lanczos
+
+namespace {
+
+// tqri / QRtrf / eigsrt (eigen_solver.C:206-305, 1442-1498) on the host:
+// the symmetric tridiagonal (d, e) and its rotations Q (row-major, ld)
+double lz_pythag(double a, double b) {
+  const double aa = std::fabs(a), ab = std::fabs(b);
+  if (aa > ab) return aa * std::sqrt(1.0 + (ab / aa) * (ab / aa));
+  return ab == 0.0 ? 0.0 : ab * std::sqrt(1.0 + (aa / ab) * (aa / ab));
+}
+
+void lz_qrtrf(double *d, double *e, int nk, double *Q, int ld, double dsh, int kmin, int kmax) {
+  auto rot = [&](int k, double c, double s) {
+    for (int i = 0; i < nk; i++) {
+      const double q1 = Q[i * ld + k], q2 = Q[i * ld + k + 1];
+      Q[i * ld + k] = c * q1 - s * q2;
+      Q[i * ld + k + 1] = s * q1 + c * q2;
+    }
+  };
+  auto step = [&](int k, double c, double s) {
+    const double t1 = d[k], t2 = d[k + 1], tb = e[k];
+    d[k] = c * c * t1 + s * s * t2 - 2.0 * c * s * tb;
+    d[k + 1] = s * s * t1 + c * c * t2 + 2.0 * c * s * tb;
+    e[k] = c * s * (t1 - t2) + (c * c - s * s) * tb;
+  };
+  int k = kmin;
+  double den = 1.0 / lz_pythag(d[k] - dsh, e[k]);
+  double c = (d[k] - dsh) * den, s = -e[k] * den;
+  step(k, c, s);
+  double x = -s * e[k + 1];
+  e[k + 1] *= c;
+  rot(k, c, s);
+  for (k = kmin + 1; k < kmax; k++) {
+    den = 1.0 / lz_pythag(x, e[k - 1]);
+    c = e[k - 1] * den;
+    s = -x * den;
+    step(k, c, s);
+    e[k - 1] = c * e[k - 1] - s * x;
+    if (k != kmax - 1) {
+      x = -s * e[k + 1];
+      e[k + 1] *= c;
+    }
+    rot(k, c, s);
+  }
+}
+
+int lz_tqri(double *d, double *e, int nk, int n, double *Q, int ld) {
+  int kmin = 0, kmax = nk - 1, iter = 0;
+  while (iter < n * 100) {
+    const double dsub = d[kmax] - d[kmax - 1];
+    double dd = lz_pythag(dsub, 2.0 * e[kmax - 1]);
+    lz_qrtrf(d, e, nk, Q, ld, 0.5 * (d[kmax - 1] + d[kmax] + (dsub < 0 ? -std::fabs(dd) : std::fabs(dd))), kmin,
+             kmax);
+    int j;
+    for (j = kmax; j >= kmin + 1; j--) {
+      dd = std::fabs(d[j - 1]) + std::fabs(d[j]);
+      if (std::fabs(e[j - 1]) + dd > dd) {
+        kmax = j;
+        break;
+      }
+    }
+    if (j == kmin) return iter;
+    for (j = 0; j < kmax; j++) {
+      dd = std::fabs(d[j]) + std::fabs(d[j + 1]);
+      if (std::fabs(e[j]) + dd > dd) {
+        kmin = j;
+        break;
+      }
+    }
+    iter++;
+  }
+  return iter;
+}
+
+// descending selection sort; with Q its columns follow (the vector-free
+// form keeps the last of equal values, as the reference's >= does)
+void lz_eigsrt(double *d, double *Q, int ld, int n) {
+  for (int i = 0; i < n - 1; i++) {
+    int k = i;
+    double p = d[i];
+    for (int j = i + 1; j < n; j++)
+      if (Q ? d[j] > p : d[j] >= p) {
+        p = d[j];
+        k = j;
+      }
+    if (k != i) {
+      d[k] = d[i];
+      d[i] = p;
+      if (Q)
+        for (int j = 0; j < n; j++) std::swap(Q[j * ld + i], Q[j * ld + k]);
+    }
+  }
+}
+
+struct LzDev {
+  Ctx &c;
+  const LanczosArgs &a;
+  cudaStream_t s;
+  double c0, c1;
+  Field tmp1, tmp2, vtmp, vtmp2, rf;
+  size_t nreal() const { return (size_t)24 * c.sites; }
+  unsigned grid() const { return (unsigned)std::min<size_t>((nreal() + 255) / 256, 148 * 16); }
+  void ritz(Field &out, const Field &in, int neg) {
+    c.mdagm(out, in);
+    if (neg) launch_scale(s, -1.0, out.view());
+  }
+  void cheb(Field &out, double a_, double b_, const Field &x, double c_, const Field &y) {
+    cheb_kernel<<<grid(), 256, 0, s>>>((double *)out.data.ptr, a_, b_, (const double *)x.data.ptr, c_,
+                                       (const double *)y.data.ptr, nreal());
+    CPSGPU_CUDA(cudaGetLastError());
+    launch_counter()++;
+  }
+  // out = T_Npol(Q) in (DiracOpDwf::RitzMat(out, in, cheby_arg), d_op_dwf.C:852-960)
+  void filter(Field &out, const Field &in) {
+    Field *t = &tmp1, *t2 = &tmp2;
+    CPSGPU_CUDA(cudaMemcpyAsync(t2->data.ptr, in.data.ptr, in.data.bytes, cudaMemcpyDeviceToDevice, s));
+    ritz(*t, in, a.neg_lanczos);
+    cheb(*t, 0.5 * c1 * c0, -0.5 * c1, in, 0.0, in);
+    for (int i = 2; i <= a.Npol; i++) {
+      ritz(out, *t, a.neg_lanczos);
+      cheb(out, c1 * c0, -c1, *t, -1.0, *t2);
+      if (i != a.Npol) {
+        std::swap(t, t2);
+        CPSGPU_CUDA(cudaMemcpyAsync(t->data.ptr, out.data.ptr, out.data.bytes, cudaMemcpyDeviceToDevice, s));
+      }
+    }
+  }
+  double ddot(const Field &x, const Field &y) { return c.dot(x, y).real(); }
+  void to_f(Field &dst, const Field &src) { launch_convert(s, PREC_SINGLE, dst.view(), PREC_DOUBLE, src.view()); }
+  void to_d(Field &dst, const Field &src) { launch_convert(s, PREC_DOUBLE, dst.view(), PREC_SINGLE, src.view()); }
+  // lanczos_GramSchm_test (eigen_solver.C:1341-1390): r against V[0..nvec) in FP32
+  void gram_schm_f(Field &r, std::vector<Field> &V, int nvec) {
+    to_f(rf, r);
+    for (int i = 0; i < nvec; i++) {
+      cdot_f_kernel<<<c.blocks(), TPB, 0, s>>>(V[i].view(), rf.view(), c.partials, c.sites);
+      CPSGPU_CUDA(cudaGetLastError());
+      launch_counter()++;
+      launch_finalize(s, 2, c.partials, c.st, RED_STORE, c.blocks(), 1, GATE_NONE);
+      double xp[2];
+      CPSGPU_CUDA(cudaMemcpyAsync(xp, c.st->sum, sizeof(xp), cudaMemcpyDeviceToHost, s));
+      CPSGPU_CUDA(cudaStreamSynchronize(s));
+      caxpy_f_kernel<<<c.blocks(), TPB, 0, s>>>(rf.view(), -(float)xp[0], -(float)xp[1], V[i].view(), c.sites);
+      CPSGPU_CUDA(cudaGetLastError());
+      launch_counter()++;
+    }
+    to_d(r, rf);
+  }
+  // DiracOp::lanczos (lanczos.C:756-883): steps k0..m-1
+  void steps(int k0, int m, Field &r, std::vector<Field> &V, double *alpha, double *beta) {
+    const double ff = std::sqrt(c.norm2(r));
+    launch_axpby(s, vtmp.view(), 1.0 / ff, r.view(), zero_view());
+    to_f(V[k0], vtmp);
+    for (int k = k0; k < m; k++) {
+      to_d(vtmp, V[k]);
+      filter(r, vtmp);
+      if (k > 0) {
+        to_d(vtmp2, V[k - 1]);
+        launch_axpby(s, r.view(), -beta[k - 1], vtmp2.view(), r.view());
+      }
+      alpha[k] = ddot(vtmp, r);
+      launch_axpby(s, r.view(), -alpha[k], vtmp.view(), r.view());
+      beta[k] = std::sqrt(c.norm2(r));
+      if (k > 0) gram_schm_f(r, V, k + 1);
+      if (k == 0 || k + 1 < m) {
+        launch_axpby(s, vtmp.view(), 1.0 / beta[k], r.view(), zero_view());
+        to_f(V[k + 1], vtmp);
+      }
+    }
+  }
+  Field zero;
+  SpinorView zero_view() { return zero.view(); }
+};
+
+}  // namespace
+
+// DiracOp::ImpResLanczos (d_op_base/comsrc/lanczos.C:193-745) for the DWF /
+// Mobius Chebyshev-filtered RitzMat: the reference's steps (its oracle
+// restatement is orc_lanczos) with the float Lanczos vectors V, every
+// vector operation and the filter's MatPcDagMatPc applications on the
+// device, the m x m tridiagonal's QR algebra on the host.  Returns the
+// restart count; -1 on a NaN residual (the reference exits).
+int imp_res_lanczos(Dirac &D, std::vector<Field> &V, double *alpha, const LanczosArgs &a) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  Ctx c{D, L, OpWork(), L.scratch_st.as<SolverScalars>(), nullptr, (size_t)L.vh * D.ls};
+  L.partials.ensure((size_t)c.blocks() * 2 * sizeof(double));
+  c.partials = L.partials.as<double>();
+  const int nk = a.nk, nt = a.nt, np = a.np, m = nk + np;
+  LzDev z{c, a, s};
+  const double aa = a.p0 * a.p0, bb = (a.p1 + std::fabs(a.eigen_shift)) * (a.p1 + std::fabs(a.eigen_shift));
+  z.c1 = 2.0 * (aa + bb) / (aa - bb);
+  z.c0 = 2.0 / (aa + bb);
+  for (Field *f : {&z.tmp1, &z.tmp2, &z.vtmp, &z.vtmp2, &z.zero}) f->create(PREC_DOUBLE, L.vh, D.ls, 1);
+  z.rf.create(PREC_SINGLE, L.vh, D.ls, 1);
+  launch_zero(s, z.zero);
+  Field r(PREC_DOUBLE, L.vh, D.ls, 1), Apsi(PREC_DOUBLE, L.vh, D.ls, 1);
+  std::vector<Field> Vn(m);
+  for (auto &f : Vn) f.create(PREC_SINGLE, L.vh, D.ls, 1);
+  std::vector<double> beta(m, 0.0), ttbeta(m), shifts(m), Q((size_t)m * m), QZ((size_t)m * m);
+  DeviceBuffer vptr, wptr, qzbuf;
+  vptr.alloc(sizeof(float *) * m);
+  wptr.alloc(sizeof(float *) * m);
+  qzbuf.alloc(sizeof(double) * m * m);
+  // Vnew[k] = sum_j V[j] Q[j][k]; entries |Q| <= qmin left out (qmin < 0: none)
+  auto rotate = [&](double qmin) {
+    for (int j = 0; j < m; j++)
+      for (int k = 0; k < m; k++) {
+        const double w = Q[(size_t)j * m + k];
+        QZ[(size_t)j + (size_t)m * k] = (qmin >= 0.0 && !(std::fabs(w) > qmin)) ? 0.0 : w;
+      }
+    std::vector<float *> vp(m), wp(m);
+    for (int j = 0; j < m; j++) {
+      vp[j] = (float *)V[j].data.ptr;
+      wp[j] = (float *)Vn[j].data.ptr;
+    }
+    CPSGPU_CUDA(cudaMemcpyAsync(vptr.ptr, vp.data(), sizeof(float *) * m, cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(wptr.ptr, wp.data(), sizeof(float *) * m, cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(qzbuf.ptr, QZ.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, s));
+    vec_mult_f_kernel<<<z.grid(), 256, 0, s>>>(vptr.as<float *>(), m, qzbuf.as<double>(), m, wptr.as<float *>(),
+                                                z.nreal());
+    CPSGPU_CUDA(cudaGetLastError());
+    launch_counter()++;
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    for (int j = 0; j < m; j++) std::swap(V[j], Vn[j]);
+  };
+  auto identity = [&]() {
+    std::fill(Q.begin(), Q.end(), 0.0);
+    for (int j = 0; j < m; j++) Q[(size_t)j * m + j] = 1.0;
+  };
+  z.to_d(r, V[0]);
+  for (int j = 0; j < m; j++) alpha[j] = 0.0;
+  z.steps(0, m, r, V, alpha, beta.data());
+  int it = 1;
+  while (it <= a.maxiters) {
+    shifts.assign(alpha, alpha + m);
+    ttbeta = beta;
+    identity();
+    lz_tqri(shifts.data(), ttbeta.data(), m, m, Q.data(), m);
+    lz_eigsrt(shifts.data(), nullptr, m, m);
+    identity();
+    for (int i = 0; i < np; i++) lz_qrtrf(alpha, beta.data(), m, Q.data(), m, shifts[nk + i], 0, m - 1);
+    rotate(-1.0);
+    launch_scale(s, Q[(size_t)(m - 1) * m + nk - 1], r.view());
+    if (nk < m) {
+      z.to_d(Apsi, V[nk]);
+      launch_axpby(s, r.view(), beta[nk - 1], Apsi.view(), r.view());
+    }
+    beta[nk - 1] = std::sqrt(c.norm2(r));
+    if (it % a.conv_check == 0) {
+      int Ndone = 0;
+      shifts.assign(alpha, alpha + m);
+      ttbeta = beta;
+      identity();
+      lz_tqri(shifts.data(), ttbeta.data(), nk, m, Q.data(), m);
+      lz_eigsrt(shifts.data(), Q.data(), m, m);
+      for (int k = 0; k < nk; k++) {
+        launch_zero(s, z.vtmp);
+        for (int j = 0; j < nk; j++) {
+          z.to_d(z.vtmp2, V[j]);
+          launch_axpby(s, z.vtmp.view(), Q[(size_t)j * m + k], z.vtmp2.view(), z.vtmp.view());
+        }
+        z.ritz(Apsi, z.vtmp, a.neg_conv);
+        const double bt = std::sqrt(c.norm2(z.vtmp));
+        const double alp = z.ddot(Apsi, z.vtmp) / bt;
+        launch_axpby(s, Apsi.view(), -alp, z.vtmp.view(), Apsi.view());
+        const double rnorm = std::sqrt(c.norm2(Apsi)) / bt;
+        if (rnorm < a.stop_res && k < nt) Ndone++;
+        if (std::isnan(rnorm)) return -1;
+      }
+      if (Ndone == nt) break;
+    }
+    z.steps(nk, m, r, V, alpha, beta.data());
+    it++;
+  }
+  if (it == a.maxiters + 1) it--;
+  shifts.assign(alpha, alpha + m);
+  ttbeta = beta;
+  identity();
+  lz_tqri(shifts.data(), ttbeta.data(), nk, m, Q.data(), m);
+  lz_eigsrt(shifts.data(), Q.data(), m, m);
+  rotate(1e-16);
+  for (int i = 0; i < nt; i++) {
+    z.to_d(z.vtmp, V[i]);
+    z.ritz(Apsi, z.vtmp, a.neg_conv);
+    alpha[i] = z.ddot(Apsi, z.vtmp);
+  }
+  return it;
 }
 
 }  // namespace cpsgpu

@@ -347,6 +347,27 @@ class _DiracOp:
         check(rc)
         return k.value, lam, np.array(valid[:])
 
+    def ImpResLanczos(self, V, nk, nt, np_, Npol, params, stop_residual=1e-6, maxiters=100, conv_check=1,
+                      eigen_shift=0.0, RitzMat_lanczos=A.RITZ_MATPCDAG_MATPC, RitzMat_convcheck=A.RITZ_MATPCDAG_MATPC):
+        """DiracOp::ImpResLanczos (lanczos.C:193-745) with the Chebyshev filter
+        T_Npol of DiracOpDwf / DiracOpMobius::RitzMat (d_op_dwf.C:852-960):
+        V (nk + np float32 vectors, V[0] the start; updated in place) become
+        the Ritz vectors; returns (restarts, alpha) with alpha[:nt] the
+        eigenvalues of MatPcDagMatPc."""
+        if len(V) != nk + np_:
+            raise ValueError("V must hold nk + np vectors")
+        for x in V:
+            if not (isinstance(x, np.ndarray) and x.dtype == np.float32 and x.flags.c_contiguous
+                    and x.size == self.f_size):
+                raise TypeError("Lanczos vectors must be C-contiguous float32 arrays of the fermion size")
+        a = A.LanczosArg(RitzMat_lanczos, RitzMat_convcheck, nk, nt, np_, eigen_shift, stop_residual, maxiters,
+                         conv_check, Npol, (C.c_double * 2)(*params))
+        pv = (C.POINTER(C.c_float) * len(V))(*[x.ctypes.data_as(C.POINTER(C.c_float)) for x in V])
+        alpha = np.zeros(len(V))
+        it = C.c_int()
+        check(lib().cpsgpu_imp_res_lanczos(self._h, pv, dptr(alpha), C.byref(a), C.byref(it)))
+        return it.value, alpha
+
     def Jacobi(self, psi, lam, off_diag, Toler=1e-10, N_max=50):
         """DiracOp::Jacobi (jacobi.C:48-268): psi and lam (float64, in place)
         rotated and sorted; off_diag: complex array of N(N-1)/2, zeroed in

@@ -334,6 +334,36 @@ int cpsgpu_jacobi(cpsgpu_dirac d, double *const *psi, int N_eig, double *lambda,
  * The reference's text dump of the matrix to eig_arg->fname is not made. */
 int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_ritz_arg *arg, int N_KS_max,
                     double *lambda_H, int *valid_eig, int *iterations);
+
+/* RitzMatType values (include/alg/enum_int.h:210-222) the eigensolvers take */
+#define CPSGPU_RITZ_MATPCDAG_MATPC 3
+#define CPSGPU_RITZ_NEG_MATPCDAG_MATPC 4
+/* LanczosArg (include/alg/lanczos_arg.h:32-53) with its MatrixPolynomialArg
+ * (Npol, params[0..1]); mass, precision, save and file fields are the
+ * operator's or the caller's business */
+typedef struct {
+  int RitzMat_lanczos, RitzMat_convcheck; /* CPSGPU_RITZ_* */
+  int nk_lanczos_vectors, nt_lanczos_vectors, np_lanczos_vectors;
+  double eigen_shift, stop_residual;
+  int maxiters, conv_check;
+  int Npol;
+  double params[2];
+} cpsgpu_lanczos_arg;
+/* DiracOp::ImpResLanczos(V, alpha, lanczos_arg) (d_op_base/comsrc/lanczos.C:193-745)
+ * with the Chebyshev-filtered RitzMat of DiracOpDwf / DiracOpMobius
+ * (d_op_dwf.C:852-960, d_op_mobius.C:1279): T_Npol of
+ * (2 A - (a+b)) / (a-b), a = params[0]^2, b = (params[1] + |eigen_shift|)^2.
+ * V: nk + np float vectors of the operator's half-checkerboard size in
+ * WILSON order, V[0] the start vector; on return the Ritz vectors of the
+ * leading nk block, V[0..nt) the wanted eigenvectors; alpha[nk + np]: the
+ * first nt their eigenvalues of the unfiltered RitzMat_convcheck operator.
+ * *restarts = the restart count (maxiters when not converged, as the
+ * reference returns it).  CPSGPU_ERR_UNSUPPORTED for Wilson fermions (the
+ * reference's DiracOp::RitzMat(V*,V*,MP*) is NotImplemented) and other
+ * RitzMat types; CPSGPU_NONFINITE on a NaN residual (the reference exits);
+ * Npol >= 2. */
+int cpsgpu_imp_res_lanczos(cpsgpu_dirac d, float *const *V, double *alpha, const cpsgpu_lanczos_arg *arg,
+                           int *restarts);
 /* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
  * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
  * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or

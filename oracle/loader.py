@@ -133,6 +133,15 @@ def load_oracle() -> C.CDLL:
         L.orc_ritz_eig.argtypes = [MDAGM_FN, C.c_void_p, i, C.c_long, C.POINTER(_dp), i, d, d, d, d, i, i, i, i, i,
                                    i, i, _dp, C.POINTER(i)]
         L.orc_ritz_eig.restype = i
+        L.orc_qrtrf.argtypes = [_dp, _dp, i, _dp, i, d, i, i]
+        L.orc_qrtrf.restype = None
+        L.orc_tqri.argtypes = [_dp, _dp, i, i, _dp, i]
+        L.orc_tqri.restype = i
+        L.orc_eigsrt.argtypes = [_dp, _dp, i, i]
+        L.orc_eigsrt.restype = None
+        L.orc_lanczos.argtypes = [MDAGM_FN, C.c_void_p, i, i, C.c_long, C.POINTER(C.POINTER(C.c_float)), _dp, i, i, i,
+                                  i, d, i, i, d, d, d]
+        L.orc_lanczos.restype = i
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]
@@ -182,6 +191,12 @@ def load_reference() -> C.CDLL:
             getattr(L, k).restype = None
         L.ref_eigen_solver.argtypes = [_dp, _dp, _dp, i]
         L.ref_eigen_solver.restype = i
+        L.ref_tqri.argtypes = [_dp, _dp, i, i, _dp]
+        L.ref_tqri.restype = i
+        L.ref_qrtrf.argtypes = [_dp, _dp, i, i, _dp, d, i, i]
+        L.ref_qrtrf.restype = None
+        L.ref_eigsrt.argtypes = [_dp, _dp, i]
+        L.ref_eigsrt.restype = None
         L.ref_fp_checksum.argtypes = [C.c_char_p, i, i]
         L.ref_fp_checksum.restype = C.c_uint
         _ref = L

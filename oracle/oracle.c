@@ -1739,3 +1739,348 @@ done:
   free(tmp2);
   return result;
 }
+
+/* ---- implicitly restarted Lanczos (DiracOp::ImpResLanczos) ---- */
+
+/* sqrt(a^2 + b^2) without overflow (Numerical Recipes' pythag; the form
+ * eigen_solver.C:199-203 uses) */
+static double lz_pythag(double a, double b) {
+  const double aa = fabs(a), ab = fabs(b);
+  if (aa > ab) return aa * sqrt(1.0 + (ab / aa) * (ab / aa));
+  return ab == 0.0 ? 0.0 : ab * sqrt(1.0 + (aa / ab) * (aa / ab));
+}
+
+/* One implicitly shifted QR step on the symmetric tridiagonal (d, e) over
+ * rows kmin..kmax, shift dsh, Givens bulge chase; the rotations are applied
+ * to columns k, k+1 of the rows 0..nk-1 of Q (Q[i * ld + k]).
+ * QRtrf (eigen_solver.C:248-305), step for step. */
+void orc_qrtrf(double *d, double *e, int nk, double *Q, int ld, double dsh, int kmin, int kmax) {
+  int k = kmin;
+  double den = 1.0 / lz_pythag(d[k] - dsh, e[k]);
+  double c = (d[k] - dsh) * den, s = -e[k] * den;
+  double t1 = d[k], t2 = d[k + 1], tb = e[k];
+  d[k] = c * c * t1 + s * s * t2 - 2.0 * c * s * tb;
+  d[k + 1] = s * s * t1 + c * c * t2 + 2.0 * c * s * tb;
+  e[k] = c * s * (t1 - t2) + (c * c - s * s) * tb;
+  double x = -s * e[k + 1];
+  e[k + 1] *= c;
+  for (int i = 0; i < nk; i++) {
+    const double q1 = Q[i * ld + k], q2 = Q[i * ld + k + 1];
+    Q[i * ld + k] = c * q1 - s * q2;
+    Q[i * ld + k + 1] = s * q1 + c * q2;
+  }
+  for (k = kmin + 1; k < kmax; k++) {
+    den = 1.0 / lz_pythag(x, e[k - 1]);
+    c = e[k - 1] * den;
+    s = -x * den;
+    t1 = d[k];
+    t2 = d[k + 1];
+    tb = e[k];
+    d[k] = c * c * t1 + s * s * t2 - 2.0 * c * s * tb;
+    d[k + 1] = s * s * t1 + c * c * t2 + 2.0 * c * s * tb;
+    e[k] = c * s * (t1 - t2) + (c * c - s * s) * tb;
+    e[k - 1] = c * e[k - 1] - s * x;
+    if (k != kmax - 1) {
+      x = -s * e[k + 1];
+      e[k + 1] *= c;
+    }
+    for (int i = 0; i < nk; i++) {
+      const double q1 = Q[i * ld + k], q2 = Q[i * ld + k + 1];
+      Q[i * ld + k] = c * q1 - s * q2;
+      Q[i * ld + k + 1] = s * q1 + c * q2;
+    }
+  }
+}
+
+/* Eigenvalues of the leading nk x nk block of the tridiagonal (d, e) by
+ * QR steps with the Wilkinson-type shift of the trailing 2 x 2 block and
+ * deflation from both ends; Q accumulates the rotations.  Returns the
+ * step count (at most 100 n).  tqri (eigen_solver.C:206-246). */
+int orc_tqri(double *d, double *e, int nk, int n, double *Q, int ld) {
+  int kmin = 0, kmax = nk - 1, iter = 0;
+  const int maxiter = n * 100;
+  while (iter < maxiter) {
+    const double dsub = d[kmax] - d[kmax - 1];
+    double dd = lz_pythag(dsub, 2.0 * e[kmax - 1]);
+    const double dsh = 0.5 * (d[kmax - 1] + d[kmax] + (dsub < 0 ? -fabs(dd) : fabs(dd)));
+    orc_qrtrf(d, e, nk, Q, ld, dsh, kmin, kmax);
+    int j;
+    for (j = kmax; j >= kmin + 1; j--) {
+      dd = fabs(d[j - 1]) + fabs(d[j]);
+      if (fabs(e[j - 1]) + dd > dd) {
+        kmax = j;
+        break;
+      }
+    }
+    if (j == kmin) return iter;
+    for (j = 0; j < kmax; j++) {
+      dd = fabs(d[j]) + fabs(d[j + 1]);
+      if (fabs(e[j]) + dd > dd) {
+        kmin = j;
+        break;
+      }
+    }
+    iter++;
+  }
+  return iter;
+}
+
+/* selection sort into descending order; with Q (Q != NULL) the columns of
+ * its n rows follow.  eigsrt(d, n) / eigsrt(d, v, n) (eigen_solver.C:1442-1498;
+ * the vector-free one keeps the last of equal values, >=) */
+void orc_eigsrt(double *d, double *Q, int ld, int n) {
+  for (int i = 0; i < n - 1; i++) {
+    int k = i;
+    double p = d[i];
+    for (int j = i + 1; j < n; j++)
+      if (Q ? d[j] > p : d[j] >= p) {
+        p = d[j];
+        k = j;
+      }
+    if (k != i) {
+      d[k] = d[i];
+      d[i] = p;
+      if (Q)
+        for (int j = 0; j < n; j++) {
+          const double t = Q[j * ld + i];
+          Q[j * ld + i] = Q[j * ld + k];
+          Q[j * ld + k] = t;
+        }
+    }
+  }
+}
+
+typedef struct {
+  orc_mdagm_fn op;
+  void *ctx;
+  long n;
+  int neg_lanczos, neg_conv; /* RitzMatOper NEG_MATPCDAG_MATPC for the filter / the check */
+  int Npol;
+  double c0, c1;
+  double *tmp1, *tmp2; /* the filter's work vectors (cheby_arg->tmp1/tmp2) */
+} LzCtx;
+
+/* RitzMat(out, in) for MATPCDAG_MATPC / NEG_MATPCDAG_MATPC (d_op_dwf.C:787-840) */
+static void lz_ritz(const LzCtx *z, int neg, double *out, const double *in) {
+  double dummy;
+  z->op(z->ctx, out, in, &dummy);
+  if (neg)
+    for (long q = 0; q < z->n; q++) out[q] = -out[q];
+}
+
+/* out = T_Npol(Q) in with Q = (2 A - (a + b)) / ... as the reference writes
+ * it: 2Q = c1 (c0 A - 1); T_0 = 1, T_1 = Q, T_{k+1} = 2 Q T_k - T_{k-1}.
+ * DiracOpDwf::RitzMat(out, in, cheby_arg) (d_op_dwf.C:852-960), Npol >= 2. */
+static void lz_cheby(const LzCtx *z, double *out, const double *in) {
+  const long n = z->n;
+  double *tmp = z->tmp1, *tmp2 = z->tmp2;
+  memcpy(tmp2, in, sizeof(double) * n);
+  lz_ritz(z, z->neg_lanczos, tmp, in);
+  for (long q = 0; q < n; q++) tmp[q] *= 0.5 * z->c1 * z->c0;
+  for (long q = 0; q < n; q++) tmp[q] += -0.5 * z->c1 * in[q];
+  for (int i = 2; i <= z->Npol; i++) {
+    lz_ritz(z, z->neg_lanczos, out, tmp);
+    for (long q = 0; q < n; q++) out[q] *= z->c1 * z->c0;
+    for (long q = 0; q < n; q++) out[q] += -z->c1 * tmp[q];
+    for (long q = 0; q < n; q++) out[q] += -1.0 * tmp2[q];
+    if (i != z->Npol) {
+      double *sw = tmp2;
+      tmp2 = tmp;
+      tmp = sw;
+      memcpy(tmp, out, sizeof(double) * n);
+    }
+  }
+}
+
+static double lz_ddot(const double *a, const double *b, long n) {
+  double s = 0.0;
+  for (long q = 0; q < n; q++) s += a[q] * b[q];
+  return s;
+}
+
+/* lanczos_GramSchm_test, float form (eigen_solver.C:1341-1390): r rounded to
+ * float, then for each V_i: xp = <V_i, r> (rounded to float), r -= xp V_i in
+ * float; r back to double.  The reference accumulates each dot product in
+ * float; here it is accumulated in double and rounded. */
+static void lz_gram_schm_f(double *r, float **V, int nvec, long n) {
+  float *rf = malloc(sizeof(float) * n);
+  for (long q = 0; q < n; q++) rf[q] = (float)r[q];
+  for (int i = 0; i < nvec; i++) {
+    double sr = 0.0, si = 0.0;
+    for (long q = 0; q < n; q += 2) {
+      sr += (double)V[i][q] * rf[q] + (double)V[i][q + 1] * rf[q + 1];
+      si += (double)V[i][q] * rf[q + 1] - (double)V[i][q + 1] * rf[q];
+    }
+    const float xr = -(float)sr, xi = -(float)si;
+    for (long q = 0; q < n; q += 2) {
+      const float vr = V[i][q], vi = V[i][q + 1];
+      rf[q] += xr * vr - xi * vi;
+      rf[q + 1] += xr * vi + xi * vr;
+    }
+  }
+  for (long q = 0; q < n; q++) r[q] = rf[q];
+  free(rf);
+}
+
+/* Lanczos steps k0..m-1 on the filtered operator: V[k0] = r / |r| and the
+ * three-term recurrence with a float Gram-Schmidt pass against V[0..k]
+ * after each step; alpha, beta: the tridiagonal.  DiracOp::lanczos
+ * (lanczos.C:756-883). */
+static void lz_steps(const LzCtx *z, int k0, int m, double *Apsi, double *r, float **V, double *alpha, double *beta,
+                     double *vtmp, double *vtmp2) {
+  const long n = z->n;
+  (void)Apsi;
+  const double ff = sqrt(lz_ddot(r, r, n));
+  for (long q = 0; q < n; q++) vtmp[q] = r[q] * (1.0 / ff);
+  for (long q = 0; q < n; q++) V[k0][q] = (float)vtmp[q];
+  for (int k = k0; k < m; k++) {
+    for (long q = 0; q < n; q++) vtmp[q] = V[k][q];
+    lz_cheby(z, r, vtmp);
+    if (k > 0) {
+      for (long q = 0; q < n; q++) vtmp2[q] = V[k - 1][q];
+      for (long q = 0; q < n; q++) r[q] += -beta[k - 1] * vtmp2[q];
+    }
+    alpha[k] = lz_ddot(vtmp, r, n);
+    for (long q = 0; q < n; q++) r[q] += -alpha[k] * vtmp[q];
+    beta[k] = sqrt(lz_ddot(r, r, n));
+    if (k > 0) lz_gram_schm_f(r, V, k + 1, n);
+    if (k == 0 || k + 1 < m) {
+      for (long q = 0; q < n; q++) vtmp[q] = r[q] * (1.0 / beta[k]);
+      for (long q = 0; q < n; q++) V[k + 1][q] = (float)vtmp[q];
+    }
+  }
+}
+
+/* V[k] <- sum_j V[j] Q[j][k] for every k < m (double sums, float store),
+ * the j order increasing; entries of Q with |Q| <= qmin left out */
+static void lz_rotate(float **V, const double *Q, int m, long n, double qmin) {
+  double *acc = malloc(sizeof(double) * m);
+  for (long q = 0; q < n; q++) {
+    for (int k = 0; k < m; k++) acc[k] = 0.0;
+    for (int k = 0; k < m; k++)
+      for (int j = 0; j < m; j++) {
+        const double w = Q[j * m + k];
+        if (fabs(w) > qmin || (qmin < 0 && w != 0.0)) acc[k] += (double)V[j][q] * w;
+      }
+    for (int k = 0; k < m; k++) V[k][q] = (float)acc[k];
+  }
+  free(acc);
+}
+
+/* DiracOp::ImpResLanczos (d_op_base/comsrc/lanczos.C:193-745), step for
+ * step, for the DWF / Mobius Chebyshev-filtered RitzMat: m = nk + np float
+ * Lanczos vectors V (V[0] the start vector); the initial m-step
+ * factorisation; per restart the np unwanted Ritz values of the m x m
+ * tridiagonal (tqri, sorted descending) as exact shifts of np implicit QR
+ * steps (QRtrf), V rotated by Q (its band structure: Q[j][k] = 0 for
+ * j > k + np), the residual r = Q[m-1][nk-1] r + beta[nk-1] V[nk]; every
+ * conv_check restarts the Ritz vectors of the leading nk block checked
+ * against the unfiltered RitzMat (|A v - (v.Av/|v|) v| / |v| < stop_res
+ * for the first nt); then np more Lanczos steps.  At the end V[0..m) are
+ * the Ritz vectors of the leading nk block (entries |Q| <= 1e-16 skipped,
+ * as the reference does) and alpha[0..nt) their Rayleigh quotients on
+ * the unfiltered operator (alpha[nt..m): the tridiagonal's diagonal, as the
+ * reference leaves it).
+ * Returns the restart count; -1 on a NaN residual (the reference exits).
+ * The filter: c1 = 2 (a+b)/(a-b), c0 = 2/(a+b), a = p0^2,
+ * b = (p1 + |eigen_shift|)^2. */
+int orc_lanczos(orc_mdagm_fn op, void *ctx, int neg_lanczos, int neg_conv, long n, float **V, double *alpha, int nk,
+                int nt, int np, int maxiters, double stop_res, int conv_check, int Npol, double p0, double p1,
+                double eigen_shift) {
+  const int m = nk + np;
+  LzCtx z;
+  z.op = op;
+  z.ctx = ctx;
+  z.n = n;
+  z.neg_lanczos = neg_lanczos;
+  z.neg_conv = neg_conv;
+  z.Npol = Npol;
+  const double a = p0 * p0, b = (p1 + fabs(eigen_shift)) * (p1 + fabs(eigen_shift));
+  z.c1 = 2.0 * (a + b) / (a - b);
+  z.c0 = 2.0 / (a + b);
+  z.tmp1 = malloc(sizeof(double) * n);
+  z.tmp2 = malloc(sizeof(double) * n);
+  double *r = malloc(sizeof(double) * n), *Apsi = malloc(sizeof(double) * n);
+  double *vtmp = malloc(sizeof(double) * n), *vtmp2 = malloc(sizeof(double) * n);
+  double *beta = calloc(m, sizeof(double)), *ttbeta = malloc(sizeof(double) * m);
+  double *shifts = malloc(sizeof(double) * m), *Q = malloc(sizeof(double) * m * m);
+  int result = 0;
+  for (long q = 0; q < n; q++) r[q] = V[0][q];
+  for (int j = 0; j < m; j++) alpha[j] = 0.0;
+  lz_steps(&z, 0, m, Apsi, r, V, alpha, beta, vtmp, vtmp2);
+  int it = 1;
+  while (it <= maxiters) {
+    memcpy(shifts, alpha, sizeof(double) * m);
+    memcpy(ttbeta, beta, sizeof(double) * m);
+    for (int j = 0; j < m * m; j++) Q[j] = 0.0;
+    for (int j = 0; j < m; j++) Q[j * m + j] = 1.0;
+    orc_tqri(shifts, ttbeta, m, m, Q, m);
+    orc_eigsrt(shifts, NULL, m, m);
+    for (int j = 0; j < m * m; j++) Q[j] = 0.0;
+    for (int j = 0; j < m; j++) Q[j * m + j] = 1.0;
+    for (int i = 0; i < np; i++) orc_qrtrf(alpha, beta, m, Q, m, shifts[nk + i], 0, m - 1);
+    lz_rotate(V, Q, m, n, -1.0);
+    for (long q = 0; q < n; q++) r[q] *= Q[(m - 1) * m + nk - 1];
+    if (nk < m) {
+      for (long q = 0; q < n; q++) Apsi[q] = V[nk][q];
+      for (long q = 0; q < n; q++) Apsi[q] *= beta[nk - 1];
+      for (long q = 0; q < n; q++) r[q] += Apsi[q];
+    }
+    beta[nk - 1] = sqrt(lz_ddot(r, r, n));
+    if (it % conv_check == 0) {
+      int Ndone = 0;
+      memcpy(shifts, alpha, sizeof(double) * m);
+      memcpy(ttbeta, beta, sizeof(double) * m);
+      for (int j = 0; j < m * m; j++) Q[j] = 0.0;
+      for (int j = 0; j < m; j++) Q[j * m + j] = 1.0;
+      orc_tqri(shifts, ttbeta, nk, m, Q, m);
+      orc_eigsrt(shifts, Q, m, m);
+      for (int k = 0; k < nk; k++) {
+        for (long q = 0; q < n; q++) vtmp[q] = 0.0;
+        for (int j = 0; j < nk; j++) {
+          for (long q = 0; q < n; q++) vtmp2[q] = V[j][q];
+          for (long q = 0; q < n; q++) vtmp[q] = Q[j * m + k] * vtmp2[q] + vtmp[q];
+        }
+        lz_ritz(&z, z.neg_conv, Apsi, vtmp);
+        const double bt = sqrt(lz_ddot(vtmp, vtmp, n));
+        const double alp = lz_ddot(Apsi, vtmp, n) / bt;
+        for (long q = 0; q < n; q++) Apsi[q] = -alp * vtmp[q] + Apsi[q];
+        const double rnorm = sqrt(lz_ddot(Apsi, Apsi, n)) / bt;
+        if (rnorm < stop_res && k < nt) Ndone++;
+        if (isnan(rnorm)) {
+          result = -1;
+          goto done;
+        }
+      }
+      if (Ndone == nt) break;
+    }
+    lz_steps(&z, nk, m, Apsi, r, V, alpha, beta, vtmp, vtmp2);
+    it++;
+  }
+  if (it == maxiters + 1) it--;
+  memcpy(shifts, alpha, sizeof(double) * m);
+  memcpy(ttbeta, beta, sizeof(double) * m);
+  for (int j = 0; j < m * m; j++) Q[j] = 0.0;
+  for (int j = 0; j < m; j++) Q[j * m + j] = 1.0;
+  orc_tqri(shifts, ttbeta, nk, m, Q, m);
+  orc_eigsrt(shifts, Q, m, m);
+  lz_rotate(V, Q, m, n, 1e-16);
+  for (int i = 0; i < nt; i++) {
+    for (long q = 0; q < n; q++) vtmp[q] = V[i][q];
+    lz_ritz(&z, z.neg_conv, Apsi, vtmp);
+    alpha[i] = lz_ddot(Apsi, vtmp, n);
+  }
+  result = it;
+done:
+  free(z.tmp1);
+  free(z.tmp2);
+  free(r);
+  free(Apsi);
+  free(vtmp);
+  free(vtmp2);
+  free(beta);
+  free(ttbeta);
+  free(shifts);
+  free(Q);
+  return result;
+}

@@ -157,7 +157,19 @@ void orc_mobius_booee(const orc_geom *g, const orc_mobius *mp, double *out, cons
 void orc_fforce_wilson_type(const orc_geom *g, double *mom, const double *u, const double *v1, const double *v2,
                             double coef, double out[3]);
 
+/* Implicitly restarted Lanczos, DiracOp::ImpResLanczos (lanczos.C:193-745)
+ * with the Chebyshev-filtered RitzMat (d_op_dwf.C:852-960), and its
+ * tridiagonal helpers tqri / QRtrf / eigsrt (eigen_solver.C); see oracle.c.
+ * Q is row-major with leading dimension ld. */
+void orc_qrtrf(double *d, double *e, int nk, double *Q, int ld, double dsh, int kmin, int kmax);
+int orc_tqri(double *d, double *e, int nk, int n, double *Q, int ld);
+void orc_eigsrt(double *d, double *Q, int ld, int n);
+int orc_lanczos(orc_mdagm_fn op, void *ctx, int neg_lanczos, int neg_conv, long n, float **V, double *alpha, int nk,
+                int nt, int np, int maxiters, double stop_res, int conv_check, int Npol, double p0, double p1,
+                double eigen_shift);
+
 #ifdef __cplusplus
 }
 #endif
+
 #endif

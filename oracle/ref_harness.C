@@ -38,6 +38,11 @@ USING_NAMESPACE_CPS
 namespace cps {
 // the dense symmetric eigensolver eigCG calls (d_op_base/comsrc/eigen_solver.C:40)
 int eigen_solver(Float *A, Float *Evec, Float *Eval, int n);
+// the tridiagonal helpers of ImpResLanczos (d_op_base/comsrc/eigen_solver.C:206-305, 1442-1498)
+int tqri(Float *d, Float *e, int nk, int n, Float **z);
+void QRtrf(Float *d, Float *e, int nk, int n, Float **Q, Float dsh, int kmin, int kmax);
+void eigsrt(Float *d, int n);
+void eigsrt(Float *d, Float **v, int n);
 // zmobius_m5inv in-place form (d_op_zmobius/noarch/zmobius_m5inv.C:807)
 void zmobius_m5inv(Vector *inout, Float mass, int dag, Zmobus *arg, Complex *K);
 }
@@ -210,6 +215,21 @@ void ref_fforce_wilson_type(double *mom, double *u, double *v1, double *v2, int 
 
 // ---- eigCG: eigen_solver (packed lower triangle in, Evec[k n + i] = component k of eigenvector i)
 int ref_eigen_solver(double *A, double *Evec, double *Eval, int n) { return eigen_solver(A, Evec, Eval, n); }
+
+// ---- ImpResLanczos helpers; Q row-major, n x n, passed as row pointers ----
+static std::vector<Float *> rows_of(double *Q, int n) {
+  std::vector<Float *> r(n);
+  for (int i = 0; i < n; i++) r[i] = Q + (size_t)i * n;
+  return r;
+}
+int ref_tqri(double *d, double *e, int nk, int n, double *Q) { return tqri(d, e, nk, n, rows_of(Q, n).data()); }
+void ref_qrtrf(double *d, double *e, int nk, int n, double *Q, double dsh, int kmin, int kmax) {
+  QRtrf(d, e, nk, n, rows_of(Q, n).data(), dsh, kmin, kmax);
+}
+void ref_eigsrt(double *d, double *Q, int n) {
+  if (Q) eigsrt(d, rows_of(Q, n).data(), n);
+  else eigsrt(d, n);
+}
 
 // ---- HMC fermion force pieces ----
 // sprojTr{X,Y,Z,T}{m,p} (f_wilson_types/noarch/sproj_tr.C), indexed as the

@@ -441,3 +441,60 @@ def test_ritz_eig_and_jacobi_match_oracle(oracle, kind, L, ls, nvec, neg):
     assert kg == ko and np.allclose(lamg, lam, rtol=1e-12, atol=0)
     for a, b in zip(mg, mixed):
         assert rel(a, b) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["dwf", "mobius"])
+def test_imp_res_lanczos_matches_oracle(oracle, kind):
+    """DiracOp::ImpResLanczos (lanczos.C:193-745, Chebyshev filter of
+    d_op_dwf.C:852-960 / d_op_mobius.C:1279) against the oracle from the same
+    float start vector: the same restart count, the nt lowest eigenvalues of
+    MatPcDagMatPc (also against a dense diagonalisation), the same Ritz
+    vectors up to a phase."""
+    L, ls, mass = (2, 2, 2, 4), 4, 0.1
+    u = gen_gauge(L, seed=41)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls) if kind == "dwf" else DiracOpMobius(lat, mass=mass, ls=ls, b=1.5, c=0.5)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    n = ops.n
+    mdagm = ops.dwf_mdagm if kind == "dwf" else ops.mobius_mdagm
+    A_ = np.zeros((n, n))
+    for k in range(n):
+        e = np.zeros(n)
+        e[k] = 1.0
+        A_[:, k] = mdagm(e, mass)[0]
+    ev = np.linalg.eigvalsh(A_[0::2, 0::2] + 1j * A_[1::2, 0::2])
+    nk, nt, np_, Npol = 8, 4, 8, 6
+    params = (np.sqrt(1.1 * ev[-1]), np.sqrt(ev[12]))
+    v0 = gen_gaussian(n, seed=5).astype(np.float32)
+    Vo = [np.zeros(n, dtype=np.float32) for _ in range(nk + np_)]
+    Vo[0][:] = v0
+    ao = np.zeros(nk + np_)
+    pv = (C.POINTER(C.c_float) * len(Vo))(*[x.ctypes.data_as(C.POINTER(C.c_float)) for x in Vo])
+    ito = oracle.orc_lanczos(ops._op(kind, mass, 0.0), None, 0, 0, n, pv, p(ao), nk, nt, np_, 100, 1e-5, 1, Npol,
+                             params[0], params[1], 0.0)
+    Vg = [np.zeros(n, dtype=np.float32) for _ in range(nk + np_)]
+    Vg[0][:] = v0
+    itg, ag = D.ImpResLanczos(Vg, nk, nt, np_, Npol, params, stop_residual=1e-5)
+    assert 1 <= ito < 100 and abs(itg - ito) <= 1
+    assert np.allclose(ag[:nt], ao[:nt], rtol=1e-7, atol=0) and np.allclose(ag[:nt], ev[:nt], rtol=1e-7, atol=0)
+    cplx = lambda x: x[0::2].astype(np.float64) + 1j * x[1::2]
+    for a, b in zip(Vg[:nt], Vo[:nt]):
+        c = abs(np.vdot(cplx(a), cplx(b))) / (np.linalg.norm(a) * np.linalg.norm(b))
+        assert abs(c - 1.0) < 1e-5
+
+
+def test_imp_res_lanczos_argument_checks(oracle):
+    L = (2, 2, 2, 4)
+    lat = Lattice(L)
+    lat.import_gauge(gen_gauge(L, seed=42))
+    W = DiracOpWilson(lat, mass=0.1)
+    V = [np.zeros(W.f_size, dtype=np.float32) for _ in range(4)]
+    with pytest.raises(A.CpsGpuError):  # DiracOp::RitzMat(V*,V*,MP*) is NotImplemented for Wilson
+        W.ImpResLanczos(V, 2, 1, 2, 4, (2.0, 0.1))
+    D = DiracOpDwf(lat, mass=0.1, ls=4)
+    V = [np.ones(D.f_size, dtype=np.float32) for _ in range(4)]
+    with pytest.raises(A.CpsGpuError):
+        D.ImpResLanczos(V, 2, 1, 2, 1, (2.0, 0.1))  # Npol < 2
+    with pytest.raises(A.CpsGpuError):
+        D.ImpResLanczos(V, 2, 3, 2, 4, (2.0, 0.1))  # nt > nk

@@ -256,3 +256,43 @@ def test_dense_eigensolver_vs_reference(oracle, reference, n):
     assert np.allclose(Vr.T @ Vr, np.eye(n), atol=1e-12)  # orthogonal ...
     if n > 1:
         assert np.abs(a @ Vr - Vr * er).max() > 1e-3 * scale  # ... but not the eigenvectors
+
+
+@pytest.mark.parametrize("m,nk,np_", [(6, 6, 0), (12, 8, 4), (20, 12, 8)])
+def test_lanczos_tridiagonal_helpers_vs_reference(oracle, reference, m, nk, np_):
+    """The tridiagonal algebra of ImpResLanczos against the reference's own
+    tqri, QRtrf and eigsrt (eigen_solver.C:206-305, 1442-1498), bit for bit:
+    the QR eigenvalues of a leading block with the rotations accumulated,
+    np exact-shift QR steps over the whole matrix, and both sorts."""
+    rng = np.random.default_rng(700 + m)
+    d0, e0 = rng.normal(size=m) + 3.0, np.abs(rng.normal(size=m)) + 0.1
+    e0[-1] = 0.3
+    out = []
+    for lib, fn in ((reference, "ref"), (oracle, "orc")):
+        d, e, Q = d0.copy(), e0.copy(), np.eye(m)
+        it = lib.ref_tqri(p(d), p(e), nk, m, p(Q)) if fn == "ref" else lib.orc_tqri(p(d), p(e), nk, m, p(Q), m)
+        dt, s1, Qs = d.copy(), d.copy(), Q.copy()
+        if fn == "ref":
+            lib.ref_eigsrt(p(s1), None, m)
+            lib.ref_eigsrt(p(d), p(Qs), m)
+        else:
+            lib.orc_eigsrt(p(s1), None, m, m)
+            lib.orc_eigsrt(p(d), p(Qs), m, m)
+        a, b, Qr = d0.copy(), e0.copy(), np.eye(m)
+        for k in range(np_):
+            if fn == "ref":
+                lib.ref_qrtrf(p(a), p(b), m, m, p(Qr), s1[nk + k] if nk + k < m else s1[-1], 0, m - 1)
+            else:
+                lib.orc_qrtrf(p(a), p(b), m, p(Qr), m, s1[nk + k] if nk + k < m else s1[-1], 0, m - 1)
+        out.append((it, dt, s1, d, Qs, a, b, Qr))
+    (ir, *vr), (io, *vo) = out
+    assert ir == io
+    for x, y in zip(vr, vo):
+        assert np.array_equal(x, y)
+    # the leading nk x nk block is diagonalised, its rotations in Q
+    T = np.diag(d0[:nk]) + np.diag(e0[:nk - 1], 1) + np.diag(e0[:nk - 1], -1)
+    dt, Q = vo[0], np.eye(m)
+    oracle.orc_tqri(p(d0.copy()), p(e0.copy()), nk, m, p(Q), m)
+    assert np.allclose(np.sort(dt[:nk]), np.linalg.eigvalsh(T), rtol=0, atol=1e-12 * np.abs(d0).max())
+    Qk = Q[:nk, :nk]
+    assert np.allclose(Qk.T @ T @ Qk, np.diag(dt[:nk]), atol=1e-11 * np.abs(d0).max())

@@ -293,3 +293,37 @@ def test_ritz_eig_kalkreuter_simma_and_jacobi(oracle):
     for x, v in zip(mixed, psi):
         xc, vc = x[0::2] + 1j * x[1::2], v[0::2] + 1j * v[1::2]
         assert abs(abs(np.vdot(vc, xc)) - 1.0) < 1e-6
+
+
+def _f32_ptrs(V):
+    return (C.POINTER(C.c_float) * len(V))(*[x.ctypes.data_as(C.POINTER(C.c_float)) for x in V])
+
+
+@pytest.mark.parametrize("Npol", [2, 6])
+def test_lanczos_lowest_eigenpairs(oracle, Npol):
+    """DiracOp::ImpResLanczos (lanczos.C:193-745) with the Chebyshev filter of
+    DiracOpDwf::RitzMat (d_op_dwf.C:852-960) on DWF MatPcDagMatPc: the nt
+    lowest eigenvalues against a dense diagonalisation, the Ritz vectors
+    (float) orthonormal and eigenvectors to the stopping residual."""
+    L, ls, mass = (2, 2, 2, 4), 4, 0.1
+    ops = OracleOps(oracle, L, gen_gauge(L, seed=41), ls=ls)
+    n = ops.n
+    A = np.zeros((n, n))
+    for k in range(n):
+        e = np.zeros(n)
+        e[k] = 1.0
+        A[:, k] = ops.dwf_mdagm(e, mass)[0]
+    Ac = A[0::2, 0::2] + 1j * A[1::2, 0::2]
+    ev = np.linalg.eigvalsh(Ac)
+    nk, nt, np_ = 8, 4, 8
+    V = [np.zeros(n, dtype=np.float32) for _ in range(nk + np_)]
+    V[0][:] = gen_gaussian(n, seed=5)
+    alpha = np.zeros(nk + np_)
+    it = oracle.orc_lanczos(ops._op("dwf", mass, 0.0), None, 0, 0, n, _f32_ptrs(V), p(alpha), nk, nt, np_, 100, 1e-5,
+                            1, Npol, np.sqrt(ev[-1] * 1.1), np.sqrt(ev[12]), 0.0)
+    assert 1 <= it < 100
+    assert np.allclose(alpha[:nt], ev[:nt], rtol=1e-7, atol=0)
+    W = np.array([x[0::2].astype(np.float64) + 1j * x[1::2] for x in V[:nt]])
+    assert np.allclose(W.conj() @ W.T, np.eye(nt), atol=1e-5)
+    for w, lam in zip(W, alpha[:nt]):
+        assert np.linalg.norm(Ac @ w - lam * w) < 2e-5
