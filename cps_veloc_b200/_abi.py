@@ -56,7 +56,8 @@ class RitzArg(C.Structure):
                 ("N_max", C.c_int), ("MaxCG", C.c_int), ("ProjApsiP", C.c_int), ("neg", C.c_int)]
 
 
-RITZ_MATPCDAG_MATPC, RITZ_NEG_MATPCDAG_MATPC = 3, 4
+RITZ_MAT_HERM, RITZ_MATPC_HERM, RITZ_MATPCDAG_MATPC, RITZ_NEG_MATPCDAG_MATPC = 1, 2, 3, 4
+INV_CG, INV_LOWMODEAPPROX, INV_CG_LOWMODE_DEFL = 0, 3, 4  # InverterType (enum_int.h:707-716)
 
 
 class LanczosArg(C.Structure):
@@ -119,6 +120,12 @@ def lib() -> C.CDLL:
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),
             "cpsgpu_invcg": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_matinv": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_matinv_lowmode": (C.c_int, [vp, _dp, _dp, C.POINTER(CgArg), C.c_int, C.c_char_p, C.c_int,
+                                                C.POINTER(CgResult)]),
+            "cpsgpu_eigencache_load": (C.c_int, [vp, C.c_char_p, C.c_int, C.POINTER(C.POINTER(C.c_float)), _dp]),
+            "cpsgpu_eigencache_clear": (C.c_int, [vp]),
+            "cpsgpu_inv_lowmode_approx": (C.c_int, [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.c_char_p, C.c_int,
+                                                    C.c_int]),
             "cpsgpu_gauge_plaquette": (C.c_int, [vp, _dp, _dp]),
             "cpsgpu_nersc_read": (C.c_int, [C.c_char_p, _ip, _dp, C.POINTER(NerscHeader)]),
             "cpsgpu_nersc_write": (C.c_int, [C.c_char_p, _ip, _dp, C.c_int, C.c_int, C.POINTER(NerscHeader),

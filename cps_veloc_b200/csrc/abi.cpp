@@ -530,9 +530,17 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
 //     temp = kappa_b Dslash_4(M5^-1 in_e, CHKB_EVEN) + in_o;  guess out_o <- M5 out_o;
 //     b = MatPcDag temp;  CG;  out_o <- M5^-1 out_o;
 //     out_e = M5^-1 (kappa_b Dslash_4(out_o, CHKB_ODD) + in_e);  out *= 2 kappa_b
-int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res) {
+namespace {
+// DiracOp*::MatInv for Inverter CG, LOWMODEAPPROX or CG_LOWMODE_DEFL
+// (d_op_dwf.C:316-500, d_op_mobius.C:407-620); eig_name / neig: the
+// low-mode cache of the last two
+int matinv_impl(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res,
+                int inverter, const char *eig_name, int neig) {
   return guarded([&] {
     if (!d || !out || !in || !arg || !res) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (inverter != CPSGPU_INV_CG && inverter != CPSGPU_INV_LOWMODEAPPROX && inverter != CPSGPU_INV_CG_LOWMODE_DEFL)
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "InverterType not implemented");
+    if (inverter != CPSGPU_INV_CG && !eig_name) throw Error(CPSGPU_ERR_ARG, "null eigenvector cache name");
     if (arg->max_num_iter < 1) throw Error(CPSGPU_ERR_ARG, "max_num_iter must be >= 1");
     check_prec(arg->precision);
     need_gauge(d);
@@ -560,13 +568,27 @@ int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg
       launch_axpby(s, t1.view(), D.kappa, t3.view(), t2.view());
     }
     op_matpc(D, PREC_DOUBLE, S.b64.view(), t1.view(), 1, w, nullptr, 0, 0);
-    upload(L, S.x64, &out_cg, 1);
-    if (mob) {  // SYM2 guess: x <- M5 x
-      launch_mix(D, PREC_DOUBLE, D.mixM5.as<double>(), S.x64.view(), t1.view());
-      CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, t1.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
-    }
     std::vector<CgResult> r;
-    S.run(to_args(arg), r);
+    if (inverter == CPSGPU_INV_CG) {
+      upload(L, S.x64, &out_cg, 1);
+      if (mob) {  // SYM2 guess: x <- M5 x
+        launch_mix(D, PREC_DOUBLE, D.mixM5.as<double>(), S.x64.view(), t1.view());
+        CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, t1.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
+      }
+    } else {
+      // the low-mode part of (MatPcDagMatPc)^-1 applied to MatPcDag in_o
+      inv_lowmode_approx(D, {S.x64.view()}, {S.b64.view()}, eig_name, neig, false);
+    }
+    if (inverter != CPSGPU_INV_LOWMODEAPPROX) {
+      S.run(to_args(arg), r);
+    } else {
+      // no CG: the reference reports true_res = 0 (dirac_op.h:96-106)
+      CgResult lm;
+      lm.iterations = 0;
+      lm.status = CPSGPU_CONVERGED;
+      lm.true_res = 0.0;
+      r.push_back(lm);
+    }
     if (!mob) {
       op_dslash(D, PREC_DOUBLE, t1.view(), S.x64.view(), 1, 0);
       launch_axpby(s, t2.view(), D.kappa, t1.view(), fo.view());
@@ -585,6 +607,16 @@ int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg
     to_result(r[0], res);
     return CPSGPU_OK;
   });
+}
+}  // namespace
+
+int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res) {
+  return matinv_impl(d, out, in, arg, res, CPSGPU_INV_CG, nullptr, 0);
+}
+
+int cpsgpu_matinv_lowmode(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, int inverter,
+                          const char *eig_name, int neig, cpsgpu_cg_result *res) {
+  return matinv_impl(d, out, in, arg, res, inverter, eig_name, neig);
 }
 
 namespace {
@@ -817,6 +849,70 @@ int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_
     return CPSGPU_OK;
   });
   return rc != CPSGPU_OK ? rc : status;
+}
+
+int cpsgpu_eigencache_load(cpsgpu_dirac d, const char *name, int neig, const float *const *evecs,
+                           const double *evals) {
+  return guarded([&] {
+    if (!d || !name || (neig > 0 && (!evecs || !evals))) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (neig < 0 || neig > 65535) throw Error(CPSGPU_ERR_ARG, "need 0 <= neig <= 65535");
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    const size_t nreal = (size_t)24 * L.vh * D.ls;
+    std::vector<Field> f(neig);
+    Field f64(PREC_DOUBLE, L.vh, D.ls, 1);
+    std::vector<double> h(nreal);
+    for (int k = 0; k < neig; k++) {
+      if (!evecs[k]) throw Error(CPSGPU_ERR_ARG, "null eigenvector");
+      for (size_t q = 0; q < nreal; q++) h[q] = (double)evecs[k][q];
+      const double *hp = h.data();
+      upload(L, f64, &hp, 1);
+      f[k].create(PREC_SINGLE, L.vh, D.ls, 1);
+      launch_convert(L.stream, PREC_SINGLE, f[k].view(), PREC_DOUBLE, f64.view());
+    }
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    eigencache_store(L, name, std::move(f), evals);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_eigencache_clear(cpsgpu_lattice lat) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    eigencache_clear(*lat->L);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_inv_lowmode_approx(cpsgpu_dirac d, double *const *out, const double *const *in, int len, const char *name,
+                              int neig, int ritz_mat_oper) {
+  return guarded([&] {
+    if (!d || !name || (len > 0 && (!out || !in))) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (len < 0 || neig < 0 || neig > 65535) throw Error(CPSGPU_ERR_ARG, "need len >= 0, 0 <= neig <= 65535");
+    if (ritz_mat_oper < 1 || ritz_mat_oper > 9)
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "RitzMatOper not implemented (inv_lowmode_approx.C:329-346)");
+    Dirac &D = *d->D;
+    Lattice &L = *D.lat;
+    std::vector<Field> fin(len), fout(len);
+    for (int i = 0; i < len; i++) {
+      if (!in[i] || !out[i]) throw Error(CPSGPU_ERR_ARG, "null vector");
+      fin[i].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      fout[i].create(PREC_DOUBLE, L.vh, D.ls, 1);
+      upload(L, fin[i], &in[i], 1);
+    }
+    const bool square = (ritz_mat_oper == CPSGPU_RITZ_MAT_HERM || ritz_mat_oper == CPSGPU_RITZ_MATPC_HERM);
+    std::vector<SpinorView> vo(len), vi(len);
+    for (int i = 0; i < len; i++) {
+      vo[i] = fout[i].view();
+      vi[i] = fin[i].view();
+    }
+    inv_lowmode_approx(D, vo, vi, name, neig, square);
+    for (int i = 0; i < len; i++) {
+      double *o = out[i];
+      download(L, fout[i], &o, 1);
+    }
+    return CPSGPU_OK;
+  });
 }
 
 int cpsgpu_imp_res_lanczos(cpsgpu_dirac d, float *const *V, double *alpha, const cpsgpu_lanczos_arg *arg,

@@ -3,6 +3,7 @@
 #include <complex>
 #include <cuda_runtime.h>
 #include <stdexcept>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,8 @@ struct Field {
 
 enum DiracKind { KIND_WILSON = 0, KIND_DWF = 1, KIND_MOBIUS = 2 };
 
+struct EigenCacheDev;  // lowmode.cu
+
 struct Lattice {
   int L[4];
   long vh;
@@ -89,6 +92,7 @@ struct Lattice {
   DeviceBuffer partials;   // per-block reduction partials
   DeviceBuffer scratch_st; // SolverScalars for operator-only reductions
   double *pinned = nullptr;  // small pinned host buffer for scalars
+  std::vector<std::shared_ptr<EigenCacheDev>> eig_caches;  // named low-mode caches (lowmode.cu)
   Lattice(const int L_[4], const double bc_[4]);
   ~Lattice();
   GaugeView gauge(int prec) const;
@@ -204,6 +208,12 @@ struct RitzArgs {
   double RsdR_a, RsdR_r, Rsdlam, Cutl_zero, Cv_fact;
   int n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, neg;
 };
+
+// low-mode deflation (lowmode.cu)
+void eigencache_store(Lattice &L, const std::string &name, std::vector<Field> &&evecs, const double *evals);
+void eigencache_clear(Lattice &L);
+void inv_lowmode_approx(Dirac &D, const std::vector<SpinorView> &out, const std::vector<SpinorView> &in,
+                        const std::string &name, int neig, bool square);
 
 // DiracOp::ImpResLanczos (krylov.cu): LanczosArg with the Chebyshev filter's
 // MatrixPolynomialArg; neg_*: RitzMatOper NEG_MATPCDAG_MATPC for the filter /

@@ -144,6 +144,10 @@ class Lattice:
         check(lib().cpsgpu_get_link_reals(self._h, prec, C.byref(r)))
         return r.value
 
+    def eigencache_clear(self):
+        """drop every eigenvector cache of this lattice (EigenCacheListCleanup)"""
+        check(lib().cpsgpu_eigencache_clear(self._h))
+
     def plaquette(self):
         """(SumReTrPlaq / (18 V), sum Re tr U / (12 V)) of the resident links"""
         p, t = C.c_double(), C.c_double()
@@ -259,10 +263,13 @@ class _DiracOp:
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
 
     def MatInv(self, out, src, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.0, chunk=8,
-               use_graph=True) -> CgResult:
-        """DiracOp*::MatInv(out, in, true_res) with CG: both checkerboards
-        (2 * f_size reals; Wilson/DWF [odd | even], Mobius [even | odd]).
-        out's CG checkerboard is the initial guess; out is updated in place."""
+               use_graph=True, inverter=A.INV_CG, fname_eigen=None, neig=0) -> CgResult:
+        """DiracOp*::MatInv(out, in, true_res): both checkerboards (2 * f_size
+        reals; Wilson/DWF [odd | even], Mobius [even | odd]), out updated in
+        place.  inverter (CgArg.Inverter): INV_CG (out's CG checkerboard is the
+        initial guess), INV_LOWMODEAPPROX (the low-mode approximation from
+        the cache fname_eigen of neig vectors instead of CG) or
+        INV_CG_LOWMODE_DEFL (that approximation as CG's initial guess)."""
         src = np.ascontiguousarray(src, dtype=np.float64)
         if src.size != 2 * self.f_size:
             raise ValueError(f"vectors must hold {2 * self.f_size} reals (both checkerboards)")
@@ -271,8 +278,38 @@ class _DiracOp:
             raise TypeError("out must be a C-contiguous float64 array like src (updated in place)")
         a = self._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, precision, delta, chunk, use_graph)
         r = A.CgResult()
-        check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
+        if inverter == A.INV_CG:
+            check(lib().cpsgpu_matinv(self._h, dptr(out), dptr(src), C.byref(a), C.byref(r)))
+        else:
+            check(lib().cpsgpu_matinv_lowmode(self._h, dptr(out), dptr(src), C.byref(a), inverter,
+                                              fname_eigen.encode(), neig, C.byref(r)))
         return CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels)
+
+    def EigenCacheLoad(self, name, evecs, evals):
+        """fill the named eigenvector cache (EigenCache, eigen_container.h)
+        on the device: evecs float32 vectors of f_size reals, evals float64"""
+        evecs = [np.ascontiguousarray(v, dtype=np.float32) for v in evecs]
+        for v in evecs:
+            if v.size != self.f_size:
+                raise ValueError(f"eigenvectors must hold {self.f_size} reals")
+        evals = np.ascontiguousarray(evals, dtype=np.float64)
+        if evals.size != len(evecs):
+            raise ValueError("one eigenvalue per eigenvector")
+        pv = (C.POINTER(C.c_float) * max(1, len(evecs)))(*[v.ctypes.data_as(C.POINTER(C.c_float)) for v in evecs])
+        check(lib().cpsgpu_eigencache_load(self._h, name.encode(), len(evecs), pv, dptr(evals)))
+
+    def InvLowModeApprox(self, out, src, fname_eigen, neig, ritz_mat_oper=A.RITZ_MATPCDAG_MATPC):
+        """DiracOp::InvLowModeApprox (inv_lowmode_approx.C:272-512): out[i]
+        (float64, in place) = sum_k <v_k, src[i]> / lambda_k v_k over the
+        cache fname_eigen of neig vectors"""
+        src = [self._vec(x) for x in src]
+        for x in out:
+            _inplace(x, self.f_size)
+        if len(out) != len(src):
+            raise ValueError("one output per source")
+        po = (A._dp * max(1, len(out)))(*[dptr(x) for x in out])
+        pi = (A._dp * max(1, len(src)))(*[dptr(x) for x in src])
+        check(lib().cpsgpu_inv_lowmode_approx(self._h, po, pi, len(src), fname_eigen.encode(), neig, ritz_mat_oper))
 
     def CalcHmdForceVecs(self, chi):
         """DiracOp*::CalcHmdForceVecs: returns (f_out, f_in), full fields in

@@ -336,6 +336,8 @@ int cpsgpu_ritz_eig(cpsgpu_dirac d, double *const *psi, int N_eig, const cpsgpu_
                     double *lambda_H, int *valid_eig, int *iterations);
 
 /* RitzMatType values (include/alg/enum_int.h:210-222) the eigensolvers take */
+#define CPSGPU_RITZ_MAT_HERM 1
+#define CPSGPU_RITZ_MATPC_HERM 2
 #define CPSGPU_RITZ_MATPCDAG_MATPC 3
 #define CPSGPU_RITZ_NEG_MATPCDAG_MATPC 4
 /* LanczosArg (include/alg/lanczos_arg.h:32-53) with its MatrixPolynomialArg
@@ -364,6 +366,26 @@ typedef struct {
  * Npol >= 2. */
 int cpsgpu_imp_res_lanczos(cpsgpu_dirac d, float *const *V, double *alpha, const cpsgpu_lanczos_arg *arg,
                            int *restarts);
+
+/* Eigenvector cache: the reference's EigenCache list (util/eigen_container.h,
+ * EigenCacheListSearch at :432; filled from disk by EigenContainer) as
+ * named caches on the lattice, resident in device memory (FP32).  load:
+ * neig float eigenvectors of d's half-checkerboard size in WILSON order and
+ * their eigenvalues under name (a cache of the same name is replaced);
+ * clear: drop every cache of the lattice. */
+int cpsgpu_eigencache_load(cpsgpu_dirac d, const char *name, int neig, const float *const *evecs,
+                           const double *evals);
+int cpsgpu_eigencache_clear(cpsgpu_lattice lat);
+/* DiracOp::InvLowModeApprox(out, in, fname_eig_root, neig)
+ * (d_op_base/comsrc/inv_lowmode_approx.C:272-512, the path of a cache of
+ * exactly neig vectors): out[i] = sum_k <v_k, in[i]> / lambda_k v_k for the
+ * len sources, with lambda_k squared when ritz_mat_oper is MAT_HERM or
+ * MATPC_HERM (CPSGPU_RITZ_*, RitzMatType values 1..9 accepted as the
+ * reference does).  CPSGPU_ERR_ARG when no cache has this name and neig
+ * (the reference exits).  The compressed-cache path (blockProj2) is not
+ * part of this call. */
+int cpsgpu_inv_lowmode_approx(cpsgpu_dirac d, double *const *out, const double *const *in, int len, const char *name,
+                              int neig, int ritz_mat_oper);
 /* DiracOp::InvEigCg(sol, src, true_res, nev, m, V, vec_len, M, U, invH,
  * def_len, restart, restart_len) (d_op_base/comsrc/inv_eig_cg.C:129-635):
  * CG on MatPcDagMatPc (FP64, arg->stop_rsd, arg->max_num_iter) from zero or
@@ -402,6 +424,17 @@ int cpsgpu_bicgstab(cpsgpu_dirac d, double *psi, const double *chi, double chi_n
  * out's CG checkerboard (odd) is the initial guess.  The source is not
  * modified (PRESERVE_YES).  res describes the CG on the odd checkerboard. */
 int cpsgpu_matinv(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, cpsgpu_cg_result *res);
+/* InverterType values (include/alg/enum_int.h:707-716) MatInv takes */
+#define CPSGPU_INV_CG 0
+#define CPSGPU_INV_LOWMODEAPPROX 3
+#define CPSGPU_INV_CG_LOWMODE_DEFL 4
+/* MatInv with CgArg.Inverter LOWMODEAPPROX (the CG's solution replaced by
+ * the low-mode approximation of InvLowModeApprox, from the cache eig_name
+ * holding neig vectors; res: 0 iterations, true_res 0 as the reference
+ * reports) or CG_LOWMODE_DEFL (that approximation as CG's initial guess):
+ * d_op_dwf.C:468-476, d_op_mobius.C:566-590.  CG: as cpsgpu_matinv. */
+int cpsgpu_matinv_lowmode(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_arg *arg, int inverter,
+                          const char *eig_name, int neig, cpsgpu_cg_result *res);
 /* DiracOp::MInvCG (minvcg.C:47-353): multishift CG on MatPcDagMatPc +
  * shift[k].  rsdcg[k] in: stop residuals, out: achieved residuals; returns
  * the iteration count through *iterations as the reference returns it.

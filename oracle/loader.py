@@ -142,6 +142,9 @@ def load_oracle() -> C.CDLL:
         L.orc_lanczos.argtypes = [MDAGM_FN, C.c_void_p, i, i, C.c_long, C.POINTER(C.POINTER(C.c_float)), _dp, i, i, i,
                                   i, d, i, i, d, d, d]
         L.orc_lanczos.restype = i
+        L.orc_inv_lowmode_approx.argtypes = [C.POINTER(_dp), C.POINTER(_dp), i, C.POINTER(C.POINTER(C.c_float)), _dp,
+                                             i, C.c_long, i]
+        L.orc_inv_lowmode_approx.restype = None
         for k in ("orc_wilson_matinv", "orc_dwf_matinv", "orc_mobius_matinv"):
             getattr(L, k).restype = i
         L.orc_minvcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, C.POINTER(_dp), _dp, d, _dp, i, _dp, i, _dp, i]

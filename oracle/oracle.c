@@ -2084,3 +2084,22 @@ done:
   free(Q);
   return result;
 }
+
+/* DiracOp::InvLowModeApprox (d_op_base/comsrc/inv_lowmode_approx.C:272-512,
+ * the plain cache path at :450-500): out[i] = 0, then for k = 0..neig-1
+ * z_i = <v_k, in_i> / eval_k (v_k float, widened) and out_i = z_i v_k + out_i.
+ * square: the cached eigenvalues are squared first (MAT_HERM, MATPC_HERM). */
+void orc_inv_lowmode_approx(double **out, double **in, int len, float **evecs, const double *evals, int neig,
+                            long n, int square) {
+  double *v = malloc(sizeof(double) * n);
+  for (int i = 0; i < len; i++) memset(out[i], 0, sizeof(double) * n);
+  for (int k = 0; k < neig; k++) {
+    for (long q = 0; q < n; q++) v[q] = evecs[k][q];
+    const double ev = square ? evals[k] * evals[k] : evals[k];
+    for (int i = 0; i < len; i++) {
+      const cplx z = cdot(v, in[i], n) / ev;
+      caxpy(out[i], z, v, out[i], n);
+    }
+  }
+  free(v);
+}

@@ -168,6 +168,10 @@ int orc_lanczos(orc_mdagm_fn op, void *ctx, int neg_lanczos, int neg_conv, long 
                 int nt, int np, int maxiters, double stop_res, int conv_check, int Npol, double p0, double p1,
                 double eigen_shift);
 
+/* DiracOp::InvLowModeApprox (inv_lowmode_approx.C:272-512); see oracle.c */
+void orc_inv_lowmode_approx(double **out, double **in, int len, float **evecs, const double *evals, int neig,
+                            long n, int square);
+
 #ifdef __cplusplus
 }
 #endif

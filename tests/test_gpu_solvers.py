@@ -498,3 +498,76 @@ def test_imp_res_lanczos_argument_checks(oracle):
         D.ImpResLanczos(V, 2, 1, 2, 1, (2.0, 0.1))  # Npol < 2
     with pytest.raises(A.CpsGpuError):
         D.ImpResLanczos(V, 2, 3, 2, 4, (2.0, 0.1))  # nt > nk
+
+
+def _f32p(V):
+    return (C.POINTER(C.c_float) * len(V))(*[x.ctypes.data_as(C.POINTER(C.c_float)) for x in V])
+
+
+def test_inv_lowmode_approx_matches_oracle(oracle):
+    """DiracOp::InvLowModeApprox (inv_lowmode_approx.C:272-512) from a device
+    eigenvector cache against the oracle: 10 sources (two chunks of the
+    dot-product kernel), float vectors, MATPCDAG_MATPC and MAT_HERM
+    (squared eigenvalues); a missing cache is an error."""
+    L, ls = (4, 4, 4, 4), 4
+    lat = Lattice(L)
+    lat.import_gauge(gen_gauge(L, seed=301))
+    D = DiracOpDwf(lat, mass=0.1, ls=ls)
+    rng = np.random.default_rng(302)
+    neig, len_ = 12, 10
+    V = [rng.normal(size=D.f_size).astype(np.float32) for _ in range(neig)]
+    lam = rng.uniform(0.01, 1.0, size=neig)
+    D.EigenCacheLoad("evecs", V, lam)
+    src = [gen_gaussian(D.f_size, seed=303 + k) for k in range(len_)]
+    for oper, sq in ((A.RITZ_MATPCDAG_MATPC, 0), (A.RITZ_MAT_HERM, 1)):
+        out = [np.empty(D.f_size) for _ in range(len_)]
+        D.InvLowModeApprox(out, src, "evecs", neig, ritz_mat_oper=oper)
+        ref = [np.empty(D.f_size) for _ in range(len_)]
+        oracle.orc_inv_lowmode_approx((C.POINTER(C.c_double) * len_)(*[p(x) for x in ref]),
+                                      (C.POINTER(C.c_double) * len_)(*[p(x) for x in src]), len_, _f32p(V), p(lam),
+                                      neig, D.f_size, sq)
+        for a, b in zip(out, ref):
+            assert rel(a, b) < 1e-12
+    with pytest.raises(A.CpsGpuError):
+        D.InvLowModeApprox([np.empty(D.f_size)], src[:1], "evecs", neig - 1)  # no cache of that size
+    lat.eigencache_clear()
+    with pytest.raises(A.CpsGpuError):
+        D.InvLowModeApprox([np.empty(D.f_size)], src[:1], "evecs", neig)
+
+
+def test_matinv_lowmode_inverters(oracle):
+    """MatInv with Inverter LOWMODEAPPROX and CG_LOWMODE_DEFL
+    (d_op_dwf.C:468-476): with every eigenvector of MatPcDagMatPc cached the
+    low-mode approximation is the solve itself (to the FP32 storage of the
+    vectors); with the 16 lowest as CG's initial guess the CG needs fewer
+    iterations and reaches the plain CG's solution."""
+    L, ls, mass = (2, 2, 2, 4), 2, 0.05
+    u = gen_gauge(L, seed=311)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    n = ops.n
+    Am = np.zeros((n, n))
+    for k in range(n):
+        e = np.zeros(n)
+        e[k] = 1.0
+        Am[:, k] = ops.dwf_mdagm(e, mass)[0]
+    w, U = np.linalg.eigh(Am[0::2, 0::2] + 1j * Am[1::2, 0::2])
+    V = []
+    for k in range(n // 2):
+        r = np.empty(n, dtype=np.float32)
+        r[0::2], r[1::2] = U[:, k].real, U[:, k].imag
+        V.append(r)
+    src = gen_gaussian(2 * D.f_size, seed=312)
+    x_cg = np.zeros(2 * D.f_size)
+    r_cg = D.MatInv(x_cg, src, stop_rsd=1e-11)
+    D.EigenCacheLoad("all", V, w)
+    x_lm = np.zeros(2 * D.f_size)
+    r_lm = D.MatInv(x_lm, src, inverter=A.INV_LOWMODEAPPROX, fname_eigen="all", neig=len(V))
+    assert r_lm.iterations == 0 and rel(x_lm, x_cg) < 1e-5
+    D.EigenCacheLoad("low16", V[:16], w[:16])
+    x_d = np.zeros(2 * D.f_size)
+    r_d = D.MatInv(x_d, src, stop_rsd=1e-11, inverter=A.INV_CG_LOWMODE_DEFL, fname_eigen="low16", neig=16)
+    assert r_d.status == A.CONVERGED and r_d.true_res < 1e-11
+    assert r_d.iterations < r_cg.iterations and rel(x_d, x_cg) < 1e-9

@@ -327,3 +327,39 @@ def test_lanczos_lowest_eigenpairs(oracle, Npol):
     assert np.allclose(W.conj() @ W.T, np.eye(nt), atol=1e-5)
     for w, lam in zip(W, alpha[:nt]):
         assert np.linalg.norm(Ac @ w - lam * w) < 2e-5
+
+
+@pytest.mark.parametrize("square", [0, 1])
+def test_inv_lowmode_approx(oracle, square):
+    """DiracOp::InvLowModeApprox (inv_lowmode_approx.C:272-512) against numpy:
+    out_i = sum_k <v_k, in_i> / lambda_k v_k (lambda_k^2 for MAT_HERM), and
+    with a complete eigenbasis of a hermitian matrix it is its inverse."""
+    rng = np.random.default_rng(7)
+    n, neig, len_ = 48, 6, 3
+    V = [rng.normal(size=n).astype(np.float32) for _ in range(neig)]
+    lam = rng.uniform(0.5, 2.0, size=neig)
+    src = [rng.normal(size=n) for _ in range(len_)]
+    out = [np.empty(n) for _ in range(len_)]
+    po = (C.POINTER(C.c_double) * len_)(*[p(x) for x in out])
+    pi = (C.POINTER(C.c_double) * len_)(*[p(x) for x in src])
+    oracle.orc_inv_lowmode_approx(po, pi, len_, _f32_ptrs(V), p(lam), neig, n, square)
+    cplx = lambda x: x[0::2].astype(np.float64) + 1j * x[1::2]
+    ev = lam ** 2 if square else lam
+    for o, s in zip(out, src):
+        ref = sum(np.vdot(cplx(v), cplx(s)) / e * cplx(v) for v, e in zip(V, ev))
+        assert np.allclose(cplx(o), ref, rtol=1e-12, atol=1e-12)
+    # complete orthonormal eigenbasis: the exact inverse (up to FP32 storage of the vectors)
+    m = n // 2
+    H = rng.normal(size=(m, m)) + 1j * rng.normal(size=(m, m))
+    H = H @ H.conj().T + m * np.eye(m)
+    w, U = np.linalg.eigh(H)
+    Vb = []
+    for k in range(m):
+        r = np.empty(n, dtype=np.float32)
+        r[0::2], r[1::2] = U[:, k].real, U[:, k].imag
+        Vb.append(r)
+    b = rng.normal(size=n)
+    x = np.empty(n)
+    oracle.orc_inv_lowmode_approx((C.POINTER(C.c_double) * 1)(p(x)), (C.POINTER(C.c_double) * 1)(p(b)), 1,
+                                  _f32_ptrs(Vb), p(w), m, n, 0)
+    assert np.linalg.norm(H @ cplx(x) - cplx(b)) < 1e-5 * np.linalg.norm(cplx(b))
