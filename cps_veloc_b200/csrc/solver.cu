@@ -15,6 +15,7 @@
 // when the solve is finished, so the host enqueues iterations in chunks
 // (captured once as a CUDA graph) and only polls a pinned flag between
 // chunks, one chunk behind, so the GPU never waits for the host.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -27,6 +28,16 @@ namespace cpsgpu {
 
 namespace {
 SpinorView none() { return SpinorView(); }
+
+// the condition of a reliable-update body: some solve still running has an
+// update pending (the gate the body's kernels apply per right-hand side)
+__global__ void reliable_cond_kernel(cudaGraphConditionalHandle h, const SolverScalars *st, int nrhs) {
+  if (threadIdx.x != 0) return;
+  unsigned any = 0;
+  for (int k = 0; k < nrhs; k++)
+    if (!st[k].done && st[k].reliable) any = 1;
+  cudaGraphSetConditional(h, any);
+}
 }  // namespace
 
 void CgSolver::setup(int nrhs_) {
@@ -63,7 +74,10 @@ void CgSolver::drop_graph() {
   graph = nullptr;
 }
 
-CgSolver::~CgSolver() { drop_graph(); }
+CgSolver::~CgSolver() {
+  drop_graph();
+  if (side) cudaStreamDestroy(side);
+}
 
 // Emit out-of-place MatPcDagMatPc on `in` with a final epilogue.
 //   final == EP_CG: r -= alpha A in; sol += alpha in; RED_CG_RR
@@ -127,17 +141,68 @@ void CgSolver::emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_e
   }
 }
 
-void CgSolver::emit_iteration() {
+// The reliable update: x64 += xs, r = b - A x64 in FP64 (stored in the
+// sloppy precision); its kernels skip every solve without a pending update.
+void CgSolver::emit_reliable_update() {
+  Lattice &L = *D.lat;
+  SolverScalars *stp = st.as<SolverScalars>();
+  launch_accum_reliable(L.stream, x64.view(), px_of(sloppy), xs.view(), stp, nrhs, 0);
+  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_RELIABLE, GATE_RELIABLE, r.view(), sloppy, none(),
+             PREC_DOUBLE);
+}
+
+// One CG iteration.  conditional (while capturing a graph): the reliable
+// update sits in the body of an IF node whose condition a one-thread kernel
+// sets from the solver state, so the iterations without an update do not
+// launch its FP64 operator's grids at all.
+void CgSolver::emit_iteration(bool conditional) {
   Lattice &L = *D.lat;
   const int px = (sloppy == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
   SolverScalars *stp = st.as<SolverScalars>();
   const SpinorView solv = (sloppy == PREC_DOUBLE) ? x64.view() : xs.view();
   emit_mdagm(sloppy, p.view(), ws, EP_CG, 1, RED_CG_RR, GATE_RUNNING, r.view(), sloppy, solv, px);
   if (sloppy != PREC_DOUBLE) {
-    // reliable update (kernels return at once unless one is pending)
-    launch_accum_reliable(L.stream, x64.view(), px, xs.view(), stp, nrhs, 0);
-    emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_RELIABLE, GATE_RELIABLE, r.view(), sloppy, none(),
-               PREC_DOUBLE);
+    if (!conditional) {
+      emit_reliable_update();
+    } else {
+      const cudaStream_t s = L.stream;
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t g;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      CPSGPU_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+      cudaGraphConditionalHandle h;
+      CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+      reliable_cond_kernel<<<1, 32, 0, s>>>(h, stp, nrhs);
+      CPSGPU_CUDA(cudaGetLastError());
+      launch_counter()++;
+      CPSGPU_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      CPSGPU_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      CPSGPU_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+      if (!side) CPSGPU_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      const long long b0 = launch_counter();
+      L.stream = side;
+      try {
+        emit_reliable_update();
+      } catch (...) {
+        L.stream = s;
+        cudaGraph_t junk;
+        cudaStreamEndCapture(side, &junk);
+        throw;
+      }
+      L.stream = s;
+      cudaGraph_t captured;
+      CPSGPU_CUDA(cudaStreamEndCapture(side, &captured));
+      body_kernels = launch_counter() - b0;
+      launch_counter() = b0;  // counted when a body runs
+    }
   }
   launch_xpay(L.stream, sloppy, p.view(), r.view(), stp, nrhs);
 }
@@ -198,7 +263,7 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
     const long long c0 = launch_counter();
     CPSGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     try {
-      for (int k = 0; k < chunk; k++) emit_iteration();
+      for (int k = 0; k < chunk; k++) emit_iteration(true);
     } catch (...) {
       cudaGraph_t g;
       cudaStreamEndCapture(s, &g);
@@ -257,7 +322,9 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
   CPSGPU_CUDA(cudaEventElapsedTime(&dev_ms, tev0, tev1));
   cudaEventDestroy(tev0);
   cudaEventDestroy(tev1);
-  const long long kernels = launch_counter() - k0 + replayed;
+  int bodies = 0;  // reliable-update bodies that ran (one per iteration in which any solve had one)
+  for (int k = 0; k < nrhs; k++) bodies = std::max(bodies, fin[k].n_reliable);
+  const long long kernels = launch_counter() - k0 + replayed + (graph_exec ? (long long)bodies * body_kernels : 0);
   res.resize(nrhs);
   for (int k = 0; k < nrhs; k++) {
     CgResult &o = res[k];

@@ -41,15 +41,18 @@ struct CgSolver {
   DeviceBuffer st;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
-  long long graph_kernels = 0;
+  long long graph_kernels = 0;  // kernels of one chunk outside the conditional bodies
+  long long body_kernels = 0;   // kernels of one reliable-update body
   int graph_chunk = 0;
+  cudaStream_t side = nullptr;  // captures the conditional bodies
 
   CgSolver(Dirac &d, int sloppy_prec) : D(d), sloppy(sloppy_prec) {}
   ~CgSolver();
   void setup(int nrhs);
   void run(const CgArgs &a, std::vector<CgResult> &res);
   void drop_graph();
-  void emit_iteration();
+  void emit_iteration(bool conditional = false);
+  void emit_reliable_update();
   void emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_ep, int pap, int red_op, int gate,
                   const SpinorView &rv, int pr, const SpinorView &solv, int px);
 };
