@@ -12,9 +12,12 @@
 //
 // One CG iteration is a fixed sequence of kernels, all of which read their
 // scalars (alpha, beta, stop flags) from device memory and return at once
-// when the solve is finished, so the host enqueues iterations in chunks
-// (captured once as a CUDA graph) and only polls a pinned flag between
-// chunks, one chunk behind, so the GPU never waits for the host.
+// when the solve is finished.  The solve is one CUDA graph: a WHILE node
+// whose body is a chunk of iterations and a one-thread kernel that decides,
+// from the solver state, whether another chunk runs (with a hard bound on
+// the chunk count); inside each iteration the reliable update sits in an IF
+// node.  Without graphs the host enqueues chunks and polls the stop flags
+// one chunk behind, so the GPU never waits for the host.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -37,6 +40,19 @@ __global__ void reliable_cond_kernel(cudaGraphConditionalHandle h, const SolverS
   for (int k = 0; k < nrhs; k++)
     if (!st[k].done && st[k].reliable) any = 1;
   cudaGraphSetConditional(h, any);
+}
+
+// the condition of the solve's WHILE node, after each body (one chunk of
+// iterations): another body while some solve is running, never more than
+// ctl[1] bodies (ctl[0] counts them), so the loop always ends
+__global__ void loop_cond_kernel(cudaGraphConditionalHandle h, const SolverScalars *st, int nrhs, int *ctl) {
+  if (threadIdx.x != 0) return;
+  const int bodies = ++ctl[0];
+  unsigned more = 0;
+  for (int k = 0; k < nrhs; k++)
+    if (!st[k].done) more = 1;
+  if (bodies >= ctl[1]) more = 0;
+  cudaGraphSetConditional(h, more);
 }
 }  // namespace
 
@@ -256,56 +272,81 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
   }
   launch_convert(s, sloppy, p.view(), sloppy, r.view());
 
-  // iterate in chunks
+  // iterate in chunks of `chunk` iterations
   const int chunk = a.chunk > 0 ? a.chunk : 8;
-  if (graph_exec && graph_chunk != chunk) drop_graph();
-  if (a.use_graph && !graph_exec) {
-    const long long c0 = launch_counter();
-    CPSGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-    try {
-      for (int k = 0; k < chunk; k++) emit_iteration(true);
-    } catch (...) {
-      cudaGraph_t g;
-      cudaStreamEndCapture(s, &g);
-      if (g) cudaGraphDestroy(g);
-      throw;
-    }
-    CPSGPU_CUDA(cudaStreamEndCapture(s, &graph));
-    CPSGPU_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
-    graph_kernels = launch_counter() - c0;
-    graph_chunk = chunk;
-  }
-  long long replayed = 0;
-  int *flags = reinterpret_cast<int *>(L.pinned);  // [2][nrhs] ring
-  if (nrhs * 2 > 64 * 2) throw Error(-1, "too many right-hand sides for the poll buffer");
-  cudaEvent_t ev[2];
-  CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   const long max_chunks = (long)a.max_num_iter / chunk + 4;
-  long launched = 0;
-  int slot = 0;
-  bool finished = false;
-  for (long c = 0; c < max_chunks && !finished; c++) {
-    if (graph_exec) {
-      CPSGPU_CUDA(cudaGraphLaunch(graph_exec, s));
-      replayed += graph_kernels;
-    } else
-      for (int k = 0; k < chunk; k++) emit_iteration();
-    for (int k = 0; k < nrhs; k++)
-      CPSGPU_CUDA(cudaMemcpyAsync(flags + slot * nrhs + k, &stp[k].done, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CPSGPU_CUDA(cudaEventRecord(ev[slot], s));
-    launched++;
-    if (launched >= 2) {
-      // look at the chunk before this one while this one runs
-      int prev = 1 - slot;
-      CPSGPU_CUDA(cudaEventSynchronize(ev[prev]));
-      if (all_done(flags + prev * nrhs, nrhs)) finished = true;
+  if (graph_exec && graph_chunk != chunk) drop_graph();
+  long long replayed = 0;
+  if (a.use_graph) {
+    // the whole loop as one graph: a WHILE node whose body is one chunk
+    // followed by the condition kernel; no host polling, and the loop stops
+    // after the chunk in which the last solve finished
+    if (!graph_exec) {
+      ctl.ensure(2 * sizeof(int));
+      CPSGPU_CUDA(cudaGraphCreate(&graph, 0));
+      cudaGraphConditionalHandle hw;
+      CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = hw;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t wn;
+      CPSGPU_CUDA(cudaGraphAddNode(&wn, graph, nullptr, 0, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      const long long c0 = launch_counter();
+      CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      try {
+        for (int k = 0; k < chunk; k++) emit_iteration(true);
+        loop_cond_kernel<<<1, 32, 0, s>>>(hw, stp, nrhs, ctl.as<int>());
+        CPSGPU_CUDA(cudaGetLastError());
+        launch_counter()++;
+      } catch (...) {
+        cudaGraph_t junk;
+        cudaStreamEndCapture(s, &junk);
+        drop_graph();
+        throw;
+      }
+      cudaGraph_t captured;
+      CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
+      CPSGPU_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+      graph_kernels = launch_counter() - c0;
+      launch_counter() = c0;
+      graph_chunk = chunk;
     }
-    slot = 1 - slot;
+    const int hctl[2] = {0, (int)std::min<long>(max_chunks, 1L << 30)};
+    CPSGPU_CUDA(cudaMemcpyAsync(ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaGraphLaunch(graph_exec, s));
+    int bodies_run = 0;
+    CPSGPU_CUDA(cudaMemcpyAsync(&bodies_run, ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    replayed = (long long)bodies_run * graph_kernels;
+  } else {
+    int *flags = reinterpret_cast<int *>(L.pinned);  // [2][nrhs] ring
+    if (nrhs * 2 > 64 * 2) throw Error(-1, "too many right-hand sides for the poll buffer");
+    cudaEvent_t ev[2];
+    CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CPSGPU_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    long launched = 0;
+    int slot = 0;
+    bool finished = false;
+    for (long c = 0; c < max_chunks && !finished; c++) {
+      for (int k = 0; k < chunk; k++) emit_iteration();
+      for (int k = 0; k < nrhs; k++)
+        CPSGPU_CUDA(cudaMemcpyAsync(flags + slot * nrhs + k, &stp[k].done, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CPSGPU_CUDA(cudaEventRecord(ev[slot], s));
+      launched++;
+      if (launched >= 2) {
+        // look at the chunk before this one while this one runs
+        int prev = 1 - slot;
+        CPSGPU_CUDA(cudaEventSynchronize(ev[prev]));
+        if (all_done(flags + prev * nrhs, nrhs)) finished = true;
+      }
+      slot = 1 - slot;
+    }
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
   }
-  CPSGPU_CUDA(cudaStreamSynchronize(s));
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
 
   // final solution and true residual in FP64 (inv_cg.C:403-415)
   if (sloppy != PREC_DOUBLE) launch_accum_reliable(s, x64.view(), px_of(sloppy), xs.view(), stp, nrhs, 1);

@@ -45,6 +45,7 @@ struct CgSolver {
   long long body_kernels = 0;   // kernels of one reliable-update body
   int graph_chunk = 0;
   cudaStream_t side = nullptr;  // captures the conditional bodies
+  DeviceBuffer ctl;              // the WHILE loop's body count and limit
 
   CgSolver(Dirac &d, int sloppy_prec) : D(d), sloppy(sloppy_prec) {}
   ~CgSolver();
