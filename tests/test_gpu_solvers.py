@@ -571,3 +571,58 @@ def test_matinv_lowmode_inverters(oracle):
     r_d = D.MatInv(x_d, src, stop_rsd=1e-11, inverter=A.INV_CG_LOWMODE_DEFL, fname_eigen="low16", neig=16)
     assert r_d.status == A.CONVERGED and r_d.true_res < 1e-11
     assert r_d.iterations < r_cg.iterations and rel(x_d, x_cg) < 1e-9
+
+
+def test_eigensolver_edge_cases(oracle):
+    """Edge cases of the eigensolvers against the oracle: RitzEig without the
+    Kalkreuter-Simma sweeps (successive Ritz calls, then the projection
+    stage), Jacobi on one vector (no off-diagonal elements), and
+    ImpResLanczos stopping on maxiters and with conv_check > 1."""
+    L, ls, mass = (2, 2, 2, 4), 4, 0.1
+    u = gen_gauge(L, seed=41)
+    lat = Lattice(L)
+    lat.import_gauge(u)
+    D = DiracOpDwf(lat, mass=mass, ls=ls)
+    ops = OracleOps(oracle, L, u, ls=ls)
+    n = ops.n
+    start = [gen_gaussian(n, seed=400 + k) for k in range(3)]
+    po, pg = [x.copy() for x in start], [x.copy() for x in start]
+    ro, lo, vo = ops.ritz_eig("dwf", po, mass=mass, Kalk_Sim=0)
+    rg, lg, vg = D.RitzEig(pg, Kalk_Sim=0)
+    assert ro > 0 and abs(rg - ro) <= 3 and np.allclose(lg, lo, rtol=1e-9, atol=0) and vg.tolist() == vo.tolist()
+    # one vector: Jacobi only sorts, zero sweeps of rotations
+    one, lam = [start[0].copy()], np.array([0.5])
+    assert D.Jacobi(one, lam, np.zeros(0, dtype=np.complex128)) == 0 and np.array_equal(one[0], start[0])
+    # Lanczos: maxiters reached (the reference returns maxiters), and checks every other restart
+    nk, nt, np_ = 6, 3, 6
+    v0 = gen_gaussian(n, seed=401).astype(np.float32)
+    for maxiters, conv_check, stop in ((2, 1, 1e-12), (40, 2, 1e-5)):
+        Vo = [np.zeros(n, dtype=np.float32) for _ in range(nk + np_)]
+        Vo[0][:] = v0
+        ao = np.zeros(nk + np_)
+        pv = (C.POINTER(C.c_float) * len(Vo))(*[x.ctypes.data_as(C.POINTER(C.c_float)) for x in Vo])
+        ito = oracle.orc_lanczos(ops._op("dwf", mass, 0.0), None, 0, 0, n, pv, p(ao), nk, nt, np_, maxiters, stop,
+                                 conv_check, 4, 1.4, 0.35, 0.0)
+        Vg = [np.zeros(n, dtype=np.float32) for _ in range(nk + np_)]
+        Vg[0][:] = v0
+        itg, ag = D.ImpResLanczos(Vg, nk, nt, np_, 4, (1.4, 0.35), stop_residual=stop, maxiters=maxiters,
+                                  conv_check=conv_check)
+        if maxiters == 2:  # not converged: both stop on maxiters
+            assert itg == ito == maxiters and np.allclose(ag[:nt], ao[:nt], rtol=1e-5, atol=0)
+        else:  # converged, checked every conv_check restarts
+            assert ito < maxiters and abs(itg - ito) <= conv_check
+            assert np.allclose(ag[:nt], ao[:nt], rtol=1e-7, atol=0)
+
+
+def test_lowmode_empty_cases(oracle):
+    """InvLowModeApprox with no sources is a no-op; with a cache of zero
+    vectors every output is zero (the reference zeroes them before its sum)."""
+    L = (2, 2, 2, 4)
+    lat = Lattice(L)
+    lat.import_gauge(gen_gauge(L, seed=410))
+    D = DiracOpDwf(lat, mass=0.1, ls=2)
+    D.EigenCacheLoad("none", [], np.zeros(0))
+    D.InvLowModeApprox([], [], "none", 0)
+    out = [np.ones(D.f_size)]
+    D.InvLowModeApprox(out, [gen_gaussian(D.f_size, seed=411)], "none", 0)
+    assert not out[0].any()
