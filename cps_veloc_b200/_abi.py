@@ -159,6 +159,10 @@ def lib() -> C.CDLL:
             "cpsgpu_field_download": (C.c_int, [vp, _dp]),
             "cpsgpu_field_gaussian": (C.c_int, [vp, C.c_ulonglong]),
             "cpsgpu_dslash_field": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+            "cpsgpu_lattice_set_t_partition": (C.c_int, [vp, C.c_int, C.c_int]),
+            "cpsgpu_dd_face_bytes": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+            "cpsgpu_dslash_dd_pack": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
+            "cpsgpu_dslash_dd": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),
             "cpsgpu_mdagm_field": (C.c_int, [vp, vp, vp]),
             "cpsgpu_invcg_field": (C.c_int, [vp, vp, vp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),

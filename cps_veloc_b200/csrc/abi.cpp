@@ -118,6 +118,8 @@ void download(Lattice &L, const Field &f, double *const *host, int nrhs) {
 
 void need_gauge(const cpsgpu_dirac_s *d) {
   if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+  if (d->D->lat->t_nodes > 1)
+    throw Error(CPSGPU_ERR_STATE, "t-partitioned lattice: only the decomposed dslash (cpsgpu_dslash_dd) applies");
 }
 
 void ensure_partials(Lattice &L, int ls, int nrhs) {
@@ -1144,6 +1146,49 @@ int cpsgpu_dslash_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int c
     if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
     need_gauge(d);
     op_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_lattice_set_t_partition(cpsgpu_lattice lat, int nodes_t, int coor_t) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    if (nodes_t < 1 || coor_t < 0 || coor_t >= nodes_t) throw Error(CPSGPU_ERR_ARG, "need 0 <= coor_t < nodes_t");
+    Lattice &L = *lat->L;
+    if (nodes_t > 1 && (L.L[3] % 2 != 0))
+      throw Error(CPSGPU_ERR_ARG, "a t slab needs an even number of t-slices (its parity is the lattice's)");
+    L.t_nodes = nodes_t;
+    L.t_coor = coor_t;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dd_face_bytes(cpsgpu_dirac d, int precision, int nrhs, size_t *bytes) {
+  return guarded([&] {
+    if (!d || !bytes || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    *bytes = dd_face_bytes(*d->D, precision, nrhs);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dslash_dd_pack(cpsgpu_dirac d, cpsgpu_field in, int cb, int dag, void *to_prev, void *to_next) {
+  return guarded([&] {
+    if (!d || !in || !to_prev || !to_next) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+    dd_pack(*d->D, in->f.prec, in->f.view(), cb ? 1 : 0, dag ? 1 : 0, to_prev, to_next);
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag, const void *from_next,
+                     const void *from_prev) {
+  return guarded([&] {
+    if (!d || !out || !in || !from_next || !from_prev) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+    dd_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0, from_next, from_prev);
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     return CPSGPU_OK;
   });
 }

@@ -93,6 +93,7 @@ struct Lattice {
   DeviceBuffer scratch_st; // SolverScalars for operator-only reductions
   double *pinned = nullptr;  // small pinned host buffer for scalars
   std::vector<std::shared_ptr<EigenCacheDev>> eig_caches;  // named low-mode caches (lowmode.cu)
+  int t_nodes = 1, t_coor = 0;  // t-slab decomposition: this lattice is slab t_coor of t_nodes (dd.cu)
   Lattice(const int L_[4], const double bc_[4]);
   ~Lattice();
   GaugeView gauge(int prec) const;
@@ -159,6 +160,7 @@ struct HopLaunch {
   int norm = 0, red_op = 0, gate = 0;
   const double *mix = nullptr;
   std::vector<double> coef;  // per slice
+  const void *halo_fwd = nullptr, *halo_bwd = nullptr;  // t halos of a decomposed lattice (dd.cu)
 };
 void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
                 const SpinorView &x, const SpinorView &r, const SpinorView &sol, const SpinorView &p,
@@ -208,6 +210,12 @@ struct RitzArgs {
   double RsdR_a, RsdR_r, Rsdlam, Cutl_zero, Cv_fact;
   int n_renorm, Kalk_Sim, N_min, N_max, MaxCG, ProjApsiP, neg;
 };
+
+// t-slab domain decomposition (dd.cu)
+size_t dd_face_bytes(const Dirac &D, int prec, int nrhs);
+void dd_pack(const Dirac &D, int prec, const SpinorView &in, int cb, int dag, void *to_prev, void *to_next);
+void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
+               const void *from_next, const void *from_prev);
 
 // low-mode deflation (lowmode.cu)
 void eigencache_store(Lattice &L, const std::string &name, std::vector<Field> &&evecs, const double *evals);

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(GTPB) plaq_kernel(const GaugeGeom g, const Gau
 
 void gauge_sums(Lattice &L, double *sum_plaq, double *sum_link) {
   if (!L.have_gauge) throw Error(-1, "no gauge field imported");
+  if (L.t_nodes > 1) throw Error(-4, "t-partitioned lattice: the plaquette needs the whole lattice");
   GaugeGeom g;
   for (int k = 0; k < 4; k++) g.L[k] = L.L[k];
   g.hx = L.L[0] / 2;

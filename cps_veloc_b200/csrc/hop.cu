@@ -59,6 +59,20 @@ HopFn pick(int prec, int recon, int ep, int pr, int px) {
   return recon == 18 ? pick_ep<PREC_HALF, 18>(ep, pr, px) : pick_ep<PREC_HALF, 12>(ep, pr, px);
 }
 
+// the t-slab decomposition's hops (store epilogue, FP64 / FP32)
+HopFn pick_halo(int prec, int recon) {
+  if (recon != 12 && recon != 18) throw Error(-2, "decomposed hop: 12- or 18-real links");
+  if (prec == PREC_DOUBLE)
+    return recon == 12 ? (g_dag ? hop_kernel<PREC_DOUBLE, 12, EP_STORE, PREC_DOUBLE, PREC_DOUBLE, true, true>
+                                : hop_kernel<PREC_DOUBLE, 12, EP_STORE, PREC_DOUBLE, PREC_DOUBLE, false, true>)
+                       : (g_dag ? hop_kernel<PREC_DOUBLE, 18, EP_STORE, PREC_DOUBLE, PREC_DOUBLE, true, true>
+                                : hop_kernel<PREC_DOUBLE, 18, EP_STORE, PREC_DOUBLE, PREC_DOUBLE, false, true>);
+  return recon == 12 ? (g_dag ? hop_kernel<PREC_SINGLE, 12, EP_STORE, PREC_SINGLE, PREC_SINGLE, true, true>
+                              : hop_kernel<PREC_SINGLE, 12, EP_STORE, PREC_SINGLE, PREC_SINGLE, false, true>)
+                     : (g_dag ? hop_kernel<PREC_SINGLE, 18, EP_STORE, PREC_SINGLE, PREC_SINGLE, true, true>
+                              : hop_kernel<PREC_SINGLE, 18, EP_STORE, PREC_SINGLE, PREC_SINGLE, false, true>);
+}
+
 size_t real_size(int prec) { return prec == PREC_DOUBLE ? 8 : 4; }
 
 }  // namespace
@@ -90,6 +104,14 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   hp.norm = L.norm;
   hp.red_op = L.red_op;
   hp.gate = L.gate;
+  hp.face = (int)(lat.vh / lat.L[3]);
+  hp.tb_fwd = (lat.t_coor == lat.t_nodes - 1) ? 1 : 0;
+  hp.tb_bwd = (lat.t_coor == 0) ? 1 : 0;
+  const bool halo = (lat.t_nodes > 1);
+  if (halo && (!L.halo_fwd || !L.halo_bwd))
+    throw Error(-1, "t-partitioned lattice: only the decomposed dslash (with its halos) applies the operator");
+  if (halo && (L.ep != EP_STORE || (L.prec != PREC_DOUBLE && L.prec != PREC_SINGLE)))
+    throw Error(-2, "decomposed hop: store epilogue, FP64 or FP32");
 
   HopViews v;
   v.U = lat.gauge(L.prec);
@@ -100,10 +122,12 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   v.sol = sol;
   v.p = p;
   v.b = b;
+  v.hf = L.halo_fwd;
+  v.hb = L.halo_bwd;
 
   const int recon = lat.recon(L.prec);
   g_dag = (L.dag != 0);
-  HopFn fn = pick(L.prec, recon, L.ep, L.pr, L.px);
+  HopFn fn = halo ? pick_halo(L.prec, recon) : pick(L.prec, recon, L.ep, L.pr, L.px);
   const bool mix = ep_mix(L.ep);
   TuneKey key{L.prec, recon, L.ep, D.kind, D.ls};
   dim3 block = hop_block(key, mix);

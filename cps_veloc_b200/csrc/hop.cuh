@@ -90,6 +90,11 @@ struct HopParams {
   int norm;         // AXPY: accumulate reductions
   int red_op;       // ReduceOp for the finalize
   int gate;         // Gate
+  // t-slab domain decomposition (the HALO kernels): face = sites of one
+  // t-slice of a checkerboard;
+  // tb_fwd / tb_bwd: this slab's forward / backward t end is the lattice's
+  // own boundary, where bc[3] applies (both 1 without decomposition)
+  int face, tb_fwd, tb_bwd;
 };
 
 struct HopViews {
@@ -97,13 +102,34 @@ struct HopViews {
   SpinorView in, out, x;  // hop input, output, axpby source
   SpinorView r, sol, p;   // CG / RES epilogue fields
   SpinorView b;           // RES: right-hand side (double)
+  // t halos, [slice][12 reals][face] in the hop's precision: hf from the
+  // next slab, (1 - sdag g_t) psi of its first t-slice; hb from the previous
+  // slab, U_t^dagger (1 + sdag g_t) psi of its last t-slice
+  const void *hf, *hb;
 };
+
+// one half spinor of a t halo ([slice][12 reals][face])
+template <typename R>
+__device__ __forceinline__ half_spinor<R> load_halo(const void *p, int face, long sl, int f) {
+  const R *q = reinterpret_cast<const R *>(p) + (size_t)sl * 12 * face + f;
+  half_spinor<R> r;
+#pragma unroll
+  for (int sp = 0; sp < 2; sp++)
+#pragma unroll
+    for (int col = 0; col < 3; col++) {
+      const int k = 2 * (col + 3 * sp);
+      r.h[sp][col] = {__ldg(q + (size_t)k * face), __ldg(q + (size_t)(k + 1) * face)};
+    }
+  return r;
+}
 
 // acc = sum over mu of the forward and backward hops into output site i,
 // slice sl, whose 4D parity is pout (input parity pin = 1 - pout).
 // All site arithmetic is 32-bit; the coordinates come from three
 // multiply-high divisions and each neighbour index from i by a stride.
-template <int P, int RECON, bool DAG>
+// HALO: the t hops across a slab's ends read the halos (t-slab decomposition);
+// a separate instantiation, so the undecomposed kernels carry none of it.
+template <int P, int RECON, bool DAG, bool HALO>
 __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v, int i, long sl,
                                          int pout, typename PrecTraits<P>::real *acc) {
   using R = typename PrecTraits<P>::real;
@@ -131,14 +157,22 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
       int j;
       if (mu == 0) j = i - xh + ((wrap ? 0 : x + 1) >> 1);
       else j = wrap ? i - (hp.L[mu] - 1) * stride[mu] : i + stride[mu];
-      R psi[24], sc;
-      in.load_raw(j, psi, sc);
-      su3<R> u;
-      LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
-      half_spinor<R> h = project(psi, mu, -sdag);
-      half_spinor<R> g = link_mul(u, h, false);
-      // the storage scale and the boundary sign ride on the accumulating FMAs
-      reconstruct_acc(acc, g, mu, -sdag, (wrap && hp.bc[mu] < 0) ? -sc : sc);
+      if (HALO && mu == 3 && wrap) {
+        // x + t lives on the next slab, which sent its projected half spinor
+        su3<R> u;
+        LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
+        half_spinor<R> g = link_mul(u, load_halo<R>(v.hf, hp.face, sl, j), false);
+        reconstruct_acc(acc, g, mu, -sdag, (hp.tb_fwd && hp.bc[mu] < 0) ? R(-1) : R(1));
+      } else {
+        R psi[24], sc;
+        in.load_raw(j, psi, sc);
+        su3<R> u;
+        LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
+        half_spinor<R> h = project(psi, mu, -sdag);
+        half_spinor<R> g = link_mul(u, h, false);
+        // the storage scale and the boundary sign ride on the accumulating FMAs
+        reconstruct_acc(acc, g, mu, -sdag, (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_fwd)) ? -sc : sc);
+      }
     }
     // backward: U_mu(x - mu)^dagger (1 + sdag g_mu) psi(x - mu)
     {
@@ -146,13 +180,19 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
       int j;
       if (mu == 0) j = i - xh + ((wrap ? hp.L[0] - 1 : x - 1) >> 1);
       else j = wrap ? i + (hp.L[mu] - 1) * stride[mu] : i - stride[mu];
-      R psi[24], sc;
-      in.load_raw(j, psi, sc);
-      su3<R> u;
-      LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
-      half_spinor<R> h = project(psi, mu, sdag);
-      half_spinor<R> g = link_mul(u, h, true);
-      reconstruct_acc(acc, g, mu, sdag, (wrap && hp.bc[mu] < 0) ? -sc : sc);
+      if (HALO && mu == 3 && wrap) {
+        // x - t and its link live on the previous slab, which sent U^dagger (1 + sdag g_t) psi
+        reconstruct_acc(acc, load_halo<R>(v.hb, hp.face, sl, i), mu, sdag,
+                        (hp.tb_bwd && hp.bc[mu] < 0) ? R(-1) : R(1));
+      } else {
+        R psi[24], sc;
+        in.load_raw(j, psi, sc);
+        su3<R> u;
+        LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
+        half_spinor<R> h = project(psi, mu, sdag);
+        half_spinor<R> g = link_mul(u, h, true);
+        reconstruct_acc(acc, g, mu, sdag, (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_bwd)) ? -sc : sc);
+      }
     }
   }
 }
@@ -201,7 +241,7 @@ __device__ __forceinline__ double norm2_24(const R *a) {
 #define CPSGPU_HOP_MINB_SLOPPY 3
 #endif
 
-template <int P, int RECON, int EP, int PR, int PX, bool DAG>
+template <int P, int RECON, int EP, int PR, int PX, bool DAG, bool HALO = false>
 __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE : CPSGPU_HOP_MINB_SLOPPY) hop_kernel(const HopParams hp, const HopViews v, SolverScalars *st,
                                                      double *partials) {
   using R = typename PrecTraits<P>::real;
@@ -225,7 +265,7 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
 
   R acc[24];
   if (active) {
-    hop_site<P, RECON, DAG>(hp, v, i, sl, pout, acc);
+    hop_site<P, RECON, DAG, HALO>(hp, v, i, sl, pout, acc);
     if (hp.dwf) hop5_dwf<P, DAG>(hp, v, i, s, rhs, acc);
   }
 

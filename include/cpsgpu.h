@@ -454,6 +454,28 @@ int cpsgpu_field_gaussian(cpsgpu_field f, unsigned long long seed);
 /* out = dslash(in) (precision of the fields, which must match) */
 int cpsgpu_dslash_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag);
 int cpsgpu_mdagm_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in);
+
+/* ---- t-slab domain decomposition of the dslash ----
+ * Replaces the QMP halo exchange of wilson_dslash_vec
+ * (d_op_wilson/qmp/wilson_dslash_vec.C:184-278, 486-493) for a lattice
+ * split along t over nodes_t ranks (GJP.Nodes(3)), one slab per rank:
+ * lat holds slab coor_t with its own node_sites (an even number of
+ * t-slices) and its own links.  While partitioned, only these calls apply
+ * the operator (every other operator, solver and the plaquette return
+ * CPSGPU_ERR_STATE).  One dslash: pack the input's two t faces (FP64 or
+ * FP32 fields) into device buffers of cpsgpu_dd_face_bytes each; move
+ * to_prev to the previous rank's from_next and to_next to the next rank's
+ * from_prev (periodically, by NCCL, peer copies or MPI: the caller's
+ * transport); then cpsgpu_dslash_dd.  Faces are spin-projected half
+ * spinors (12 reals per site and slice), the backward one already
+ * multiplied by the sending slab's link, so no gauge halo is needed; the
+ * antiperiodic t sign applies only at the lattice's own t ends.  Both calls
+ * return once their kernels have finished. */
+int cpsgpu_lattice_set_t_partition(cpsgpu_lattice lat, int nodes_t, int coor_t);
+int cpsgpu_dd_face_bytes(cpsgpu_dirac d, int precision, int nrhs, size_t *bytes);
+int cpsgpu_dslash_dd_pack(cpsgpu_dirac d, cpsgpu_field in, int cb, int dag, void *to_prev, void *to_next);
+int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag, const void *from_next,
+                     const void *from_prev);
 /* solve with FP64 fields already on the device (sol: initial guess in,
  * solution out); arg->precision selects plain or mixed CG */
 int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,
