@@ -163,6 +163,8 @@ def lib() -> C.CDLL:
             "cpsgpu_dd_face_bytes": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
             "cpsgpu_dslash_dd_pack": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
             "cpsgpu_dslash_dd": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),
+            "cpsgpu_field_axpby": (C.c_int, [vp, C.c_double, vp, vp]),
+            "cpsgpu_field_dot": (C.c_int, [vp, vp, _dp, _dp]),
             "cpsgpu_mdagm_field": (C.c_int, [vp, vp, vp]),
             "cpsgpu_invcg_field": (C.c_int, [vp, vp, vp, C.POINTER(CgArg), C.POINTER(CgResult)]),
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),

@@ -1193,6 +1193,29 @@ int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, 
   });
 }
 
+int cpsgpu_field_axpby(cpsgpu_field out, double a, cpsgpu_field x, cpsgpu_field y) {
+  return guarded([&] {
+    if (!out || !x || !y) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != PREC_DOUBLE || x->f.prec != PREC_DOUBLE || y->f.prec != PREC_DOUBLE)
+      throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+    if (out->f.sites() != x->f.sites() || out->f.sites() != y->f.sites()) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    Lattice &L = *out->d->D->lat;
+    launch_axpby(L.stream, out->f.view(), a, x->f.view(), y->f.view());
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_dot(cpsgpu_field a, cpsgpu_field b, double *re, double *im) {
+  return guarded([&] {
+    if (!a || !b || !re || !im) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (a->f.prec != PREC_DOUBLE || b->f.prec != PREC_DOUBLE) throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+    if (a->f.sites() != b->f.sites()) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    field_dot(*a->d->D->lat, a->f.view(), b->f.view(), re, im);
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_mdagm_field(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in) {
   return guarded([&] {
     if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");

@@ -216,6 +216,7 @@ size_t dd_face_bytes(const Dirac &D, int prec, int nrhs);
 void dd_pack(const Dirac &D, int prec, const SpinorView &in, int cb, int dag, void *to_prev, void *to_next);
 void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
                const void *from_next, const void *from_prev);
+void field_dot(Lattice &L, const SpinorView &a, const SpinorView &b, double *re, double *im);
 
 // low-mode deflation (lowmode.cu)
 void eigencache_store(Lattice &L, const std::string &name, std::vector<Field> &&evecs, const double *evals);

@@ -104,3 +104,125 @@ def exchange_faces(faces: Faces, group=None) -> None:
            dist.P2POp(dist.irecv, faces.from_prev, prev, group, TAG_TO_NEXT)]
     for r in dist.batch_isend_irecv(ops):
         r.wait()
+
+
+# ---- the decomposed operator and CG ----
+
+def axpby(out: DeviceField, a: float, x: DeviceField, y: DeviceField) -> None:
+    """out = a x + y (FP64 fields)"""
+    check(lib().cpsgpu_field_axpby(out._h, a, x._h, y._h))
+
+
+def local_dot(a: DeviceField, b: DeviceField) -> complex:
+    """this rank's part of <a, b> = sum conj(a) b (FP64 fields)"""
+    re, im = C.c_double(), C.c_double()
+    check(lib().cpsgpu_field_dot(a._h, b._h, C.byref(re), C.byref(im)))
+    return complex(re.value, im.value)
+
+
+class InProcessRing:
+    """every slab of the lattice in this process: faces move between the
+    slabs by device copies, a global sum is the sum over the slabs"""
+
+    def exchange(self, faces):
+        n = len(faces)
+        for r in range(n):
+            faces[r].from_next.copy_(faces[(r + 1) % n].to_prev)
+            faces[r].from_prev.copy_(faces[(r - 1) % n].to_next)
+        torch.cuda.synchronize()
+
+    def allreduce(self, v: complex) -> complex:
+        return v
+
+
+class DistRing:
+    """one slab per rank of a torch.distributed group: faces by
+    point-to-point operations, global sums by all_reduce (the reference's
+    glb_sum)"""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def exchange(self, faces):
+        if len(faces) != 1:
+            raise ValueError("one slab per rank")
+        exchange_faces(faces[0], self.group)
+        torch.cuda.synchronize()
+
+    def allreduce(self, v: complex) -> complex:
+        t = torch.tensor([v.real, v.imag], dtype=torch.float64)
+        dist.all_reduce(t, group=self.group)
+        return complex(t[0].item(), t[1].item())
+
+
+class DDOperator:
+    """MatPc / MatPcDagMatPc of a Wilson or DWF operator over t slabs
+    (wilson_m.C:49-93, dwf_m.C:31-63: out = in - kappa^2 D_cb0 D_cb1 in):
+    ops holds this process's slabs' DiracOps, ring moves faces and adds
+    the ranks' parts of a dot product"""
+
+    def __init__(self, ops, ring):
+        self.ops, self.ring = list(ops), ring
+        self.faces = [Faces(D) for D in self.ops]
+        self.t1 = self.field()
+        self.t2 = self.field()
+
+    def field(self):
+        return [DeviceField(D) for D in self.ops]
+
+    def dslash(self, out, inp, cb, dag):
+        for D, i, f in zip(self.ops, inp, self.faces):
+            pack(D, i, cb, dag, f)
+        self.ring.exchange(self.faces)
+        for D, o, i, f in zip(self.ops, out, inp, self.faces):
+            dslash(D, o, i, cb, dag, f)
+
+    def dot(self, a, b) -> complex:
+        return self.ring.allreduce(sum((local_dot(x, y) for x, y in zip(a, b)), 0j))
+
+    def matpc(self, out, inp, dag=0):
+        self.dslash(self.t1, inp, 1, dag)
+        self.dslash(out, self.t1, 0, dag)
+        for D, o, i in zip(self.ops, out, inp):
+            axpby(o, -D.kappa * D.kappa, o, i)
+
+    def mdagm(self, out, inp) -> float:
+        """out = MatPcDag MatPc inp; returns |MatPc inp|^2"""
+        self.matpc(self.t2, inp, 0)
+        pap = self.dot(self.t2, self.t2).real
+        self.matpc(out, self.t2, 1)
+        return pap
+
+
+def cg(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000):
+    """CG on MatPcDagMatPc over the slabs (the recurrences of InvCgShift,
+    inv_cg.C:84-448: stop when |r|^2 <= stop_rsd^2 |b|^2), x the initial
+    guess in, solution out; returns (iterations + 1 as the reference
+    counts, true residual |b - A x| / |b|).  The host drives it: every
+    global sum is a ring all-reduce."""
+    r, p, ap = op.field(), op.field(), op.field()
+    bb = op.dot(b, b).real
+    op.mdagm(ap, x)
+    for ri, bi, ai in zip(r, b, ap):
+        axpby(ri, -1.0, ai, bi)
+    for pi, ri in zip(p, r):
+        axpby(pi, 0.0, ri, ri)  # p = r
+    rr = op.dot(r, r).real
+    stop = stop_rsd * stop_rsd * bb
+    k = 0
+    while k < max_num_iter - 1 and rr > stop:
+        pap = op.mdagm(ap, p)
+        alpha = rr / pap
+        for xi, pi in zip(x, p):
+            axpby(xi, alpha, pi, xi)
+        for ri, ai in zip(r, ap):
+            axpby(ri, -alpha, ai, ri)
+        rr_new = op.dot(r, r).real
+        beta, rr = rr_new / rr, rr_new
+        for pi, ri in zip(p, r):
+            axpby(pi, beta, pi, ri)
+        k += 1
+    op.mdagm(ap, x)
+    for ri, bi, ai in zip(r, b, ap):
+        axpby(ri, -1.0, ai, bi)
+    return k + 1, (op.dot(r, r).real / bb) ** 0.5

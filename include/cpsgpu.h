@@ -476,6 +476,12 @@ int cpsgpu_dd_face_bytes(cpsgpu_dirac d, int precision, int nrhs, size_t *bytes)
 int cpsgpu_dslash_dd_pack(cpsgpu_dirac d, cpsgpu_field in, int cb, int dag, void *to_prev, void *to_next);
 int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag, const void *from_next,
                      const void *from_prev);
+/* BLAS-1 on FP64 device fields (vector_util.C:727-922): out = a x + y
+ * (fTimesV1PlusV2), and this rank's part of <a, b> = sum conj(a) b
+ * (compDotProduct without its global sum: a decomposed solver adds the
+ * ranks' parts, as glb_sum does).  Both return once done. */
+int cpsgpu_field_axpby(cpsgpu_field out, double a, cpsgpu_field x, cpsgpu_field y);
+int cpsgpu_field_dot(cpsgpu_field a, cpsgpu_field b, double *re, double *im);
 /* solve with FP64 fields already on the device (sol: initial guess in,
  * solution out); arg->precision selects plain or mixed CG */
 int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,

@@ -96,3 +96,35 @@ def test_partitioned_lattice_refuses_other_operators():
         dd.set_t_partition(odd, 2, 1)
     dd.set_t_partition(lat, 1, 0)  # back to a whole lattice
     assert D.MatPc(gen_gaussian(D.f_size, seed=504)).size == D.f_size
+
+
+@pytest.mark.parametrize("kind,L,ls,nodes", [("wilson", (4, 4, 4, 8), 1, 2), ("dwf", (4, 4, 2, 12), 4, 3)])
+def test_dd_cg_matches_whole_lattice_solve(kind, L, ls, nodes):
+    """CG on MatPcDagMatPc over t slabs (the decomposed MatPc, wilson_m.C /
+    dwf_m.C, and InvCgShift's recurrences with every dot product summed over
+    the slabs) against the whole lattice's device CG: the same iteration
+    count within one, the same solution."""
+    mass = 0.1
+    u = gen_gauge(L, seed=511)
+    full = Lattice(L)
+    full.import_gauge(u)
+    Dfull = _make(kind, full, mass, ls)
+    b = gen_gaussian(Dfull.f_size, seed=512)
+    x = np.zeros(Dfull.f_size)
+    r = Dfull.InvCg(x, b, stop_rsd=1e-11)
+    lt = L[3] // nodes
+    ops = []
+    for k in range(nodes):
+        lat = Lattice((L[0], L[1], L[2], lt))
+        lat.import_gauge(_slab_gauge(u, L, nodes, k))
+        dd.set_t_partition(lat, nodes, k)
+        ops.append((lat, _make(kind, lat, mass, ls)))
+    op = dd.DDOperator([D for _, D in ops], dd.InProcessRing())
+    bs, xs = op.field(), op.field()
+    for k, (fb, fx) in enumerate(zip(bs, xs)):
+        fb.upload(_slab_vec(b, L, ls, nodes, k))
+        fx.upload(np.zeros(fx.D.f_size))
+    it, tr = dd.cg(op, xs, bs, stop_rsd=1e-11)
+    y = _join([f.download() for f in xs], L, ls)
+    assert abs(it - r.iterations) <= 1 and tr < 1e-11
+    assert rel(y, x) < 1e-9
