@@ -159,4 +159,137 @@ __device__ __forceinline__ half_spinor<R> link_mul(const su3<R> &u, const half_s
   return g;
 }
 
+
+// ---- Packed FP32 forms (sm_100 FFMA2: two FP32 fused multiply-adds per
+// lane and instruction) ----
+// The two spins of a half spinor sit in the two lanes of a float2, so every
+// link element enters as a scalar broadcast to both lanes (a broadcast and a
+// negated broadcast cost no extra instruction), and the link multiply, the
+// upper-spin accumulation and, for mu = z, t, the lower-spin accumulation
+// each take half the instructions of the scalar form.  The arithmetic per
+// lane is the scalar form's, operation for operation.
+struct hs2 {
+  float2 re[3], im[3];  // re[c] = (h[0][c].re, h[1][c].re)
+};
+// 24-real accumulator: spins (0, 1) in u*, spins (2, 3) in l*
+struct acc2 {
+  float2 ur[3], ui[3], lr[3], li[3];
+};
+__device__ __forceinline__ float2 b2(float s) { return make_float2(s, s); }
+
+__device__ __forceinline__ void acc2_zero(acc2 &a) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) a.ur[c] = a.ui[c] = a.lr[c] = a.li[c] = make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ hs2 pack_hs2(const half_spinor<float> &h) {
+  hs2 r;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    r.re[c] = make_float2(h.h[0][c].re, h.h[1][c].re);
+    r.im[c] = make_float2(h.h[0][c].im, h.h[1][c].im);
+  }
+  return r;
+}
+
+// g = U h (dagger = false) or U^dagger h (dagger = true), both spins at once
+__device__ __forceinline__ hs2 link_mul2(const su3<float> &u, const hs2 &h, bool dagger) {
+  hs2 g;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    // m(a, b) = u[a][b] or conj(u[b][a]); re += m.re h.re - m.im h.im, im += m.re h.im + m.im h.re
+    const cplx<float> m0 = dagger ? conj(u.m[0][a]) : u.m[a][0];
+    float2 re = __fmul2_rn(b2(m0.re), h.re[0]);
+    float2 im = __fmul2_rn(b2(m0.re), h.im[0]);
+    re = __ffma2_rn(b2(-m0.im), h.im[0], re);
+    im = __ffma2_rn(b2(m0.im), h.re[0], im);
+#pragma unroll
+    for (int b = 1; b < 3; b++) {
+      const cplx<float> m = dagger ? conj(u.m[b][a]) : u.m[a][b];
+      re = __ffma2_rn(b2(m.re), h.re[b], re);
+      re = __ffma2_rn(b2(-m.im), h.im[b], re);
+      im = __ffma2_rn(b2(m.re), h.im[b], im);
+      im = __ffma2_rn(b2(m.im), h.re[b], im);
+    }
+    g.re[a] = re;
+    g.im[a] = im;
+  }
+  return g;
+}
+
+// a += w * (four-spin spinor rebuilt from g), as reconstruct_acc
+__device__ __forceinline__ void reconstruct_acc2(acc2 &a, const hs2 &g, int mu, float k, float w) {
+  const float wk = w * k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    a.ur[c] = __ffma2_rn(b2(w), g.re[c], a.ur[c]);
+    a.ui[c] = __ffma2_rn(b2(w), g.im[c], a.ui[c]);
+    switch (mu) {
+      case 0:  // r2 = -k i g1, r3 = -k i g0
+        a.lr[c].x = fmaf(wk, g.im[c].y, a.lr[c].x);
+        a.lr[c].y = fmaf(wk, g.im[c].x, a.lr[c].y);
+        a.li[c].x = fmaf(-wk, g.re[c].y, a.li[c].x);
+        a.li[c].y = fmaf(-wk, g.re[c].x, a.li[c].y);
+        break;
+      case 1:  // r2 = k g1, r3 = -k g0
+        a.lr[c].x = fmaf(wk, g.re[c].y, a.lr[c].x);
+        a.lr[c].y = fmaf(-wk, g.re[c].x, a.lr[c].y);
+        a.li[c].x = fmaf(wk, g.im[c].y, a.li[c].x);
+        a.li[c].y = fmaf(-wk, g.im[c].x, a.li[c].y);
+        break;
+      case 2:  // r2 = -k i g0, r3 = k i g1
+        a.lr[c] = __ffma2_rn(make_float2(wk, -wk), g.im[c], a.lr[c]);
+        a.li[c] = __ffma2_rn(make_float2(-wk, wk), g.re[c], a.li[c]);
+        break;
+      default:  // r2 = k g0, r3 = k g1
+        a.lr[c] = __ffma2_rn(b2(wk), g.re[c], a.lr[c]);
+        a.li[c] = __ffma2_rn(b2(wk), g.im[c], a.li[c]);
+        break;
+    }
+  }
+}
+
+// the accumulator in the reference's element order, 2 (colour + 3 spin) + re/im
+__device__ __forceinline__ void acc2_store(const acc2 &a, float *acc) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc[2 * c] = a.ur[c].x;           acc[2 * c + 1] = a.ui[c].x;
+    acc[2 * (c + 3)] = a.ur[c].y;     acc[2 * (c + 3) + 1] = a.ui[c].y;
+    acc[2 * (c + 6)] = a.lr[c].x;     acc[2 * (c + 6) + 1] = a.li[c].x;
+    acc[2 * (c + 9)] = a.lr[c].y;     acc[2 * (c + 9) + 1] = a.li[c].y;
+  }
+}
+
+// The accumulator of one hop site: the scalar form for FP64, the packed
+// form for FP32 arithmetic (FP32 and FP16 storage).
+template <typename R> struct HopAcc {
+  R a[24];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 24; k++) a[k] = R(0);
+  }
+  // += w * reconstruct(U h or U^dagger h)
+  __device__ __forceinline__ void hop(const su3<R> &u, const half_spinor<R> &h, bool dagger, int mu, R k, R w) {
+    reconstruct_acc(a, link_mul(u, h, dagger), mu, k, w);
+  }
+  // += w * reconstruct(g)
+  __device__ __forceinline__ void add(const half_spinor<R> &g, int mu, R k, R w) { reconstruct_acc(a, g, mu, k, w); }
+  __device__ __forceinline__ void store(R *acc) const {
+#pragma unroll
+    for (int k = 0; k < 24; k++) acc[k] = a[k];
+  }
+};
+template <> struct HopAcc<float> {
+  acc2 a;
+  __device__ __forceinline__ void zero() { acc2_zero(a); }
+  __device__ __forceinline__ void hop(const su3<float> &u, const half_spinor<float> &h, bool dagger, int mu, float k,
+                                      float w) {
+    reconstruct_acc2(a, link_mul2(u, pack_hs2(h), dagger), mu, k, w);
+  }
+  __device__ __forceinline__ void add(const half_spinor<float> &g, int mu, float k, float w) {
+    reconstruct_acc2(a, pack_hs2(g), mu, k, w);
+  }
+  __device__ __forceinline__ void store(float *acc) const { acc2_store(a, acc); }
+};
+
 }  // namespace cpsgpu

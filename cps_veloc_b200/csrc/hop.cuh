@@ -147,8 +147,8 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
   const Slice<P> in(v.in, sl);
   // sdag is a compile-time +-1, so every (1 -+ gamma) sign folds into adds
   constexpr R sdag = DAG ? R(-1) : R(1);
-#pragma unroll
-  for (int k = 0; k < 24; k++) acc[k] = R(0);
+  HopAcc<R> A;
+  A.zero();
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     // forward: U_mu(x) (1 - sdag g_mu) psi(x + mu)
@@ -161,17 +161,15 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
         // x + t lives on the next slab, which sent its projected half spinor
         su3<R> u;
         LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
-        half_spinor<R> g = link_mul(u, load_halo<R>(v.hf, hp.face, sl, j), false);
-        reconstruct_acc(acc, g, mu, -sdag, (hp.tb_fwd && hp.bc[mu] < 0) ? R(-1) : R(1));
+        A.hop(u, load_halo<R>(v.hf, hp.face, sl, j), false, mu, -sdag, (hp.tb_fwd && hp.bc[mu] < 0) ? R(-1) : R(1));
       } else {
         R psi[24], sc;
         in.load_raw(j, psi, sc);
         su3<R> u;
         LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
-        half_spinor<R> h = project(psi, mu, -sdag);
-        half_spinor<R> g = link_mul(u, h, false);
         // the storage scale and the boundary sign ride on the accumulating FMAs
-        reconstruct_acc(acc, g, mu, -sdag, (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_fwd)) ? -sc : sc);
+        A.hop(u, project(psi, mu, -sdag), false, mu, -sdag,
+              (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_fwd)) ? -sc : sc);
       }
     }
     // backward: U_mu(x - mu)^dagger (1 + sdag g_mu) psi(x - mu)
@@ -182,19 +180,18 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
       else j = wrap ? i + (hp.L[mu] - 1) * stride[mu] : i - stride[mu];
       if (HALO && mu == 3 && wrap) {
         // x - t and its link live on the previous slab, which sent U^dagger (1 + sdag g_t) psi
-        reconstruct_acc(acc, load_halo<R>(v.hb, hp.face, sl, i), mu, sdag,
-                        (hp.tb_bwd && hp.bc[mu] < 0) ? R(-1) : R(1));
+        A.add(load_halo<R>(v.hb, hp.face, sl, i), mu, sdag, (hp.tb_bwd && hp.bc[mu] < 0) ? R(-1) : R(1));
       } else {
         R psi[24], sc;
         in.load_raw(j, psi, sc);
         su3<R> u;
         LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
-        half_spinor<R> h = project(psi, mu, sdag);
-        half_spinor<R> g = link_mul(u, h, true);
-        reconstruct_acc(acc, g, mu, sdag, (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_bwd)) ? -sc : sc);
+        A.hop(u, project(psi, mu, sdag), true, mu, sdag,
+              (wrap && hp.bc[mu] < 0 && (!HALO || mu != 3 || hp.tb_bwd)) ? -sc : sc);
       }
     }
   }
+  A.store(acc);
 }
 
 // Fifth-direction hop of the Shamir DWF operator, accumulated into acc.

@@ -19,7 +19,9 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 ORACLE_SO = OUT / "liboracle.so"
 REF_SO = OUT / "libcpsref.so"
-REF_SRC = Path(os.environ.get("CPS_REF", "/root/reference/cps_pp"))
+# the reference's cps_pp source directory, from the environment only
+REF_SRC = Path(os.environ["CPS_REF"]) if os.environ.get("CPS_REF") else None
+REF_SOLVE_SO = OUT / "libcpsref_solve.so"
 
 _dp = C.POINTER(C.c_double)
 
@@ -50,7 +52,7 @@ def _make(target: str) -> None:
     env = dict(os.environ)
     env.pop("CXX", None)
     env.pop("CC", None)
-    cmd = ["make", "-s", "-C", str(HERE), target, f"REF={REF_SRC}"]
+    cmd = ["make", "-s", "-j8", "-C", str(HERE), target] + ([f"REF={REF_SRC}"] if REF_SRC else [])
     r = subprocess.run(cmd, capture_output=True, text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError(f"building oracle target {target} failed:\n{r.stdout}\n{r.stderr}")
@@ -64,16 +66,30 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_SO
 
 
+def _ref_tree() -> bool:
+    return REF_SRC is not None and REF_SRC.exists()
+
+
 def build_reference() -> Path:
+    """the reference's kernels (libcpsref.so); needs CPS_REF unless prebuilt"""
     if not REF_SO.exists():
-        if not REF_SRC.exists():
-            raise FileNotFoundError("reference sources not available and libcpsref.so not prebuilt")
+        if not _ref_tree():
+            raise FileNotFoundError("reference kernels not prebuilt and CPS_REF does not name the reference's cps_pp")
         _make("ref")
     return REF_SO
 
 
+def build_reference_solvers() -> Path:
+    """the reference's Lattice / DiracOp solvers (libcpsref_solve.so)"""
+    if not REF_SOLVE_SO.exists():
+        if not _ref_tree():
+            raise FileNotFoundError("reference solvers not prebuilt and CPS_REF does not name the reference's cps_pp")
+        _make("refsolve")
+    return REF_SOLVE_SO
+
+
 def reference_available() -> bool:
-    return REF_SO.exists() or REF_SRC.exists()
+    return REF_SO.exists() or _ref_tree()
 
 
 _oracle = None
