@@ -170,7 +170,10 @@ def run_child(spec: dict, timeout: float = 600) -> dict:
     with tempfile.TemporaryDirectory() as d:
         sp, op = Path(d) / "spec.json", Path(d) / "out.npz"
         sp.write_text(json.dumps(spec))
-        r = subprocess.run([sys.executable, "-m", "oracle.refsolve", str(sp), str(op)], cwd=str(HERE.parent),
+        # the reference writes its error logs (phys.error.*) into the working directory
+        env = dict(os.environ)
+        env["PYTHONPATH"] = str(HERE.parent) + os.pathsep + env.get("PYTHONPATH", "")
+        r = subprocess.run([sys.executable, "-m", "oracle.refsolve", str(sp), str(op)], cwd=d, env=env,
                            capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"reference solver run failed:\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
