@@ -1155,8 +1155,6 @@ int cpsgpu_lattice_set_t_partition(cpsgpu_lattice lat, int nodes_t, int coor_t) 
     if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
     if (nodes_t < 1 || coor_t < 0 || coor_t >= nodes_t) throw Error(CPSGPU_ERR_ARG, "need 0 <= coor_t < nodes_t");
     Lattice &L = *lat->L;
-    if (nodes_t > 1 && (L.L[3] % 2 != 0))
-      throw Error(CPSGPU_ERR_ARG, "a t slab needs an even number of t-slices (its parity is the lattice's)");
     L.t_nodes = nodes_t;
     L.t_coor = coor_t;
     return CPSGPU_OK;

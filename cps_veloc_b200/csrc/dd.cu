@@ -80,6 +80,7 @@ void check_dd(const Dirac &D, int prec) {
 }  // namespace
 
 size_t dd_face_bytes(const Dirac &D, int prec, int nrhs) {
+  check_dd(D, prec);  // the sizes only of configurations the decomposed dslash runs
   const Lattice &L = *D.lat;
   return (size_t)(L.vh / L.L[3]) * 12 * D.ls * nrhs * (prec == PREC_DOUBLE ? 8 : 4);
 }

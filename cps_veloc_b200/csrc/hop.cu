@@ -133,6 +133,7 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   dim3 block = hop_block(key, mix);
   const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
   hp.nsg = (D.ls + block.y - 1) / block.y;
+  hp.spar = (hp.dwf && !mix && block.y > 1 && D.ls % (2 * block.y) == 0) ? 1 : 0;
   hp.nrhs = in.nrhs;
   hp.rtile = std::max(1, std::min(D.rhs_tile(L.prec, in.nrhs), in.nrhs));
   dim3 grid(nsb * hp.nsg * hp.rtile, 1, (unsigned)((in.nrhs + hp.rtile - 1) / hp.rtile));

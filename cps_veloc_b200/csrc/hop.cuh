@@ -95,6 +95,10 @@ struct HopParams {
   // tb_fwd / tb_bwd: this slab's forward / backward t end is the lattice's
   // own boundary, where bc[3] applies (both 1 without decomposition)
   int face, tb_fwd, tb_bwd;
+  // DWF slice groups of one 4D parity: group g holds slices
+  // (g / 2) * 2 BS + (g % 2) + 2 k, so the BS threads of a site read the same
+  // eight links (the parity of slice s alternates with s)
+  int spar;
 };
 
 struct HopViews {
@@ -254,7 +258,8 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
 
   const int sgrp = sb % hp.nsg, sblk = sb / hp.nsg;
   const int i = sblk * blockDim.x + threadIdx.x;
-  const int s = sgrp * blockDim.y + threadIdx.y;
+  const int s = hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y
+                        : sgrp * (int)blockDim.y + (int)threadIdx.y;
   const bool active = (i < hp.vh) && (s < hp.ls);
   const long sl = rhs * hp.ls + s;
   const int pin = hp.dwf ? ((s + hp.cb) & 1) : hp.cb;

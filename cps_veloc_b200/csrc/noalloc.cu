@@ -17,7 +17,9 @@
 //   * every call shares the one array: calls whose kernels overlap on the GPU
 //     (several host threads, several streams) race and corrupt each other;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     (cudaGetSymbolAddress); make that first call before any stream capture;
+//   * a call runs on the operator's lattice's device (made current for the
+//     call, the caller's current device restored after it).
 #include <cstring>
 #include <mutex>
 
@@ -39,10 +41,24 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 unsigned char *g_scratch_addr[MAX_DEVICES] = {nullptr};
 
-// device address of the scratch on the current device (looked up once)
-unsigned char *scratch_address() {
-  int dev = 0;
-  CPSGPU_CUDA(cudaGetDevice(&dev));
+// Makes `dev` the calling thread's current device for a scope and restores
+// the caller's device afterwards: the scratch address is per device, and the
+// kernels run on the lattice's stream, which belongs to the lattice's device.
+struct CurrentDevice {
+  int saved = -1;
+  explicit CurrentDevice(int dev) {
+    CPSGPU_CUDA(cudaGetDevice(&saved));
+    if (saved != dev) CPSGPU_CUDA(cudaSetDevice(dev));
+  }
+  ~CurrentDevice() {
+    int now = -1;
+    if (cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+  }
+};
+
+// device address of the scratch on device dev, which must be current
+// (looked up once per device)
+unsigned char *scratch_address(int dev) {
   if (dev < 0 || dev >= MAX_DEVICES) throw Error(-2, "noalloc: device index out of range");
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_scratch_addr[dev]) {
@@ -160,7 +176,9 @@ double matpc_dag_matpc_noalloc(const Dirac &D, double *out, const double *in) {
   if (c.total > NOALLOC_SCRATCH_BYTES)
     throw Error(-1, "noalloc: operator needs " + std::to_string(c.total >> 20) + " MiB of scratch, more than the " +
                         std::to_string(NOALLOC_SCRATCH_BYTES >> 20) + " MiB available (two FP64 fields must fit)");
-  unsigned char *base = scratch_address();
+  // the lattice's device, whatever the caller's current device is
+  CurrentDevice on(D.lat->device);
+  unsigned char *base = scratch_address(D.lat->device);
   SolverScalars *st = reinterpret_cast<SolverScalars *>(base);
   double *partials = reinterpret_cast<double *>(base + c.scalars);
   void *t1 = base + c.scalars + c.partials;

@@ -150,7 +150,10 @@ class DistRing:
         torch.cuda.synchronize()
 
     def allreduce(self, v: complex) -> complex:
-        t = torch.tensor([v.real, v.imag], dtype=torch.float64)
+        # NCCL reduces device tensors only; gloo (the CPU tests) host tensors
+        on_gpu = dist.get_backend(self.group) == "nccl"
+        dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+        t = torch.tensor([v.real, v.imag], dtype=torch.float64, device=dev)
         dist.all_reduce(t, group=self.group)
         return complex(t[0].item(), t[1].item())
 
@@ -180,6 +183,10 @@ class DDOperator:
     def dot(self, a, b) -> complex:
         return self.ring.allreduce(sum((local_dot(x, y) for x, y in zip(a, b)), 0j))
 
+    @staticmethod
+    def axpby(out, a: float, x, y) -> None:
+        axpby(out, a, x, y)
+
     def matpc(self, out, inp, dag=0):
         self.dslash(self.t1, inp, 1, dag)
         self.dslash(out, self.t1, 0, dag)
@@ -199,14 +206,16 @@ def cg(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000):
     inv_cg.C:84-448: stop when |r|^2 <= stop_rsd^2 |b|^2), x the initial
     guess in, solution out; returns (iterations + 1 as the reference
     counts, true residual |b - A x| / |b|).  The host drives it: every
-    global sum is a ring all-reduce."""
+    global sum is a ring all-reduce.  op provides field(), dot(a, b) (the
+    global sum of the slabs' dot products), mdagm(out, inp) and
+    axpby(out, a, x, y) on one slab's field."""
     r, p, ap = op.field(), op.field(), op.field()
     bb = op.dot(b, b).real
     op.mdagm(ap, x)
     for ri, bi, ai in zip(r, b, ap):
-        axpby(ri, -1.0, ai, bi)
+        op.axpby(ri, -1.0, ai, bi)
     for pi, ri in zip(p, r):
-        axpby(pi, 0.0, ri, ri)  # p = r
+        op.axpby(pi, 0.0, ri, ri)  # p = r
     rr = op.dot(r, r).real
     stop = stop_rsd * stop_rsd * bb
     k = 0
@@ -214,15 +223,15 @@ def cg(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000):
         pap = op.mdagm(ap, p)
         alpha = rr / pap
         for xi, pi in zip(x, p):
-            axpby(xi, alpha, pi, xi)
+            op.axpby(xi, alpha, pi, xi)
         for ri, ai in zip(r, ap):
-            axpby(ri, -alpha, ai, ri)
+            op.axpby(ri, -alpha, ai, ri)
         rr_new = op.dot(r, r).real
         beta, rr = rr_new / rr, rr_new
         for pi, ri in zip(p, r):
-            axpby(pi, beta, pi, ri)
+            op.axpby(pi, beta, pi, ri)
         k += 1
     op.mdagm(ap, x)
     for ri, bi, ai in zip(r, b, ap):
-        axpby(ri, -1.0, ai, bi)
+        op.axpby(ri, -1.0, ai, bi)
     return k + 1, (op.dot(r, r).real / bb) ** 0.5

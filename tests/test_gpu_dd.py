@@ -91,9 +91,11 @@ def test_partitioned_lattice_refuses_other_operators():
         D.MatPc(gen_gaussian(D.f_size, seed=504))
     with pytest.raises(A.CpsGpuError):
         lat.plaquette()
-    with pytest.raises(A.CpsGpuError):  # a slab needs an even number of t-slices
-        odd = Lattice((4, 4, 4, 3))
-        dd.set_t_partition(odd, 2, 1)
+    for nodes_t, coor_t in ((2, 2), (2, -1), (0, 0)):  # coor_t outside [0, nodes_t)
+        with pytest.raises(A.CpsGpuError):
+            dd.set_t_partition(lat, nodes_t, coor_t)
+    with pytest.raises(A.CpsGpuError):  # faces are sized only for FP64 / FP32 fields
+        dd.Faces(D, prec=A.HALF)
     dd.set_t_partition(lat, 1, 0)  # back to a whole lattice
     assert D.MatPc(gen_gaussian(D.f_size, seed=504)).size == D.f_size
 
