@@ -31,7 +31,7 @@ _ip = C.POINTER(C.c_int)
 
 class DiracArg(C.Structure):
     _fields_ = [("kind", C.c_int), ("ls", C.c_int), ("mass", C.c_double), ("m5", C.c_double),
-                ("mobius_b", C.c_double), ("mobius_c", C.c_double)]
+                ("mobius_b", C.c_double), ("mobius_c", C.c_double), ("a5_inv", C.c_double)]
 
 
 class ForceArg(C.Structure):
@@ -115,6 +115,9 @@ def lib() -> C.CDLL:
             "cpsgpu_matpc": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
             "cpsgpu_matpc_dag_matpc": (C.c_int, [vp, _dp, _dp, _dp, C.c_int]),
             "cpsgpu_matpc_dag_matpc_noalloc": (C.c_int, [vp, vp, vp, _dp]),
+            "cpsgpu_mat": (C.c_int, [vp, _dp, _dp, C.c_int]),
+            "cpsgpu_mat_herm": (C.c_int, [vp, _dp, _dp]),
+            "cpsgpu_matpc_dag_matpc_shift": (C.c_int, [vp, _dp, _dp, C.c_double, _dp, C.c_int]),
             "cpsgpu_mobius_dslash_4": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_mobius_m5inv": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int]),
             "cpsgpu_cg_arg_default": (None, [C.POINTER(CgArg)]),

@@ -58,6 +58,8 @@ struct cpsgpu_dirac_s {
   Field in[3], out[3];
   OpWork w[3];
   std::unique_ptr<CgSolver> solvers[3];
+  // both checkerboards of the full-vector operators (in 0, in 1, out 0, out 1)
+  std::unique_ptr<Field[]> full;
   // HMC force workspace: CalcHmdForceVecs' fields and the momentum field
   std::unique_ptr<ForceVecs> fv;
   DeviceBuffer mom;
@@ -346,7 +348,8 @@ int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *a, cpsgpu_di
     auto *o = new cpsgpu_dirac_s;
     o->lat = lat;
     try {
-      o->D.reset(new Dirac(lat->L.get(), a->kind, a->ls, a->mass, a->m5, a->mobius_b, a->mobius_c));
+      o->D.reset(new Dirac(lat->L.get(), a->kind, a->ls, a->mass, a->m5, a->mobius_b, a->mobius_c,
+                           a->a5_inv != 0.0 ? a->a5_inv : 1.0));
       ensure_partials(*lat->L, o->D->ls, 1);
     } catch (...) {
       delete o;
@@ -435,6 +438,68 @@ int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double
     SolverScalars *st = L.scratch_st.as<SolverScalars>();
     CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
     op_mdagm(*d->D, prec, d->out[prec].view(), d->in[prec].view(), d->w[prec], st, RED_STORE);
+    download(L, d->out[prec], &out, 1);
+    if (dot) {
+      SolverScalars h;
+      CPSGPU_CUDA(cudaMemcpy(&h, st, sizeof(h), cudaMemcpyDeviceToHost));
+      *dot = h.sum[0];
+    }
+    return CPSGPU_OK;
+  });
+}
+
+namespace {
+// a full vector's halves in the reference's order: [odd][even] (Wilson,
+// DWF), [even][odd] (Mobius); the library's fields hold one checkerboard
+void full_op(cpsgpu_dirac d, double *out, const double *in, int which, int dag) {
+  if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+  need_gauge(d);
+  Dirac &D = *d->D;
+  Lattice &L = *D.lat;
+  const int prec = PREC_DOUBLE;
+  if (!d->full) d->full.reset(new Field[4]);
+  Field *f = d->full.get();
+  for (int k = 0; k < 4; k++) ensure_field(f[k], prec, L.vh, D.ls, 1);
+  const size_t half = (size_t)24 * L.vh * D.ls;
+  const double *h0 = in, *h1 = in + half;
+  upload(L, f[0], &h0, 1);
+  upload(L, f[1], &h1, 1);
+  if (which == 0) op_mat(D, prec, f[2].view(), f[3].view(), f[0].view(), f[1].view(), dag, d->w[prec]);
+  else op_mat_herm(D, prec, f[2].view(), f[3].view(), f[0].view(), f[1].view(), d->w[prec]);
+  double *o0 = out, *o1 = out + half;
+  download(L, f[2], &o0, 1);
+  download(L, f[3], &o1, 1);
+}
+}  // namespace
+
+int cpsgpu_mat(cpsgpu_dirac d, double *out, const double *in, int dag) {
+  return guarded([&] {
+    if (dag != 0 && dag != 1) throw Error(CPSGPU_ERR_ARG, "dag must be 0 or 1");
+    full_op(d, out, in, 0, dag);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_mat_herm(cpsgpu_dirac d, double *out, const double *in) {
+  return guarded([&] {
+    full_op(d, out, in, 1, 0);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_matpc_dag_matpc_shift(cpsgpu_dirac d, double *out, const double *in, double mu, double *dot, int prec) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    check_prec(prec);
+    need_gauge(d);
+    if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "MatPcDagMatPcShift: Mobius operators only");
+    Lattice &L = *d->D->lat;
+    ensure_field(d->in[prec], prec, L.vh, d->D->ls, 1);
+    ensure_field(d->out[prec], prec, L.vh, d->D->ls, 1);
+    upload(L, d->in[prec], &in, 1);
+    SolverScalars *st = L.scratch_st.as<SolverScalars>();
+    CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
+    op_mdagm_shift(*d->D, prec, d->out[prec].view(), d->in[prec].view(), mu, d->w[prec], st);
     download(L, d->out[prec], &out, 1);
     if (dot) {
       SolverScalars h;

@@ -124,19 +124,23 @@ struct Dirac {
   int kind;
   int ls;
   double mass, m5, b, c;
+  double a5inv = 1.0;  // DoArg.dwf_a5_inv: the fifth-direction inverse lattice spacing
   double kappa;  // Wilson kappa, DWF kappa_5, Mobius kappa_b
   double kappa_c;
   // Mobius s-mixing matrices, each [2][ls][ls] (upper, lower chirality):
   //   P = B M5inv, Q = B M5inv kappa_b, R = kappa_b M5inv^+ B^+ (-kappa_b),
   //   S = M5inv^+ B^+, and the pieces B, B^+, M5inv, M5inv^+ on their own.
   DeviceBuffer mixP, mixQ, mixR, mixS, mixB, mixBd, mixM5i, mixM5id, mixM5;
+  // 1 + a5inv K D5: the fifth-direction term of the unpreconditioned Mat
+  // (mobius_dslash_5_plus weights the hop by a5inv, d_op_mobius.C:735-795)
+  DeviceBuffer mixM5a;
   // complex per-slice b_s, c_s (zMobius): every matrix above is complex,
   // stored [2][ls][ls][re, im], and the -kappa_b(s) of MatPc is the complex
   // diagonal mixKb applied in a mixing epilogue
   bool cplx = false;
   DeviceBuffer mixKb;
   std::vector<double> hM5i, hM5id, hB, hBd;  // host copies of the packed M5^-1 and B matrices
-  Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_);
+  Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_, double a5inv_ = 1.0);
   // (re)build the Mobius matrices from per-slice coefficients
   void build_mobius(const std::vector<std::complex<double>> &bs, const std::vector<std::complex<double>> &cs);
   // right-hand sides per hop tile (consecutive blocks share links across
@@ -201,6 +205,15 @@ void op_matpc(const Dirac &D, int prec, const SpinorView &out, const SpinorView 
               SolverScalars *st, int norm, int red_op);
 void op_mdagm(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, OpWork &w,
               SolverScalars *st, int red_op_dot);
+// fullops.cu: the unpreconditioned operators on both checkerboards (halves 0
+// and 1 in the reference's full-vector order) and the shifted Mobius
+// MatPcDagMatPc (st->sum[0] = |MatPc in|^2 when st is given)
+void op_mat(const Dirac &D, int prec, const SpinorView &out0, const SpinorView &out1, const SpinorView &in0,
+            const SpinorView &in1, int dag, OpWork &w);
+void op_mat_herm(const Dirac &D, int prec, const SpinorView &out0, const SpinorView &out1, const SpinorView &in0,
+                 const SpinorView &in1, OpWork &w);
+void op_mdagm_shift(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, double mu, OpWork &w,
+                    SolverScalars *st);
 void op_mobius_dslash4(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
                        OpWork &w);
 void op_mobius_m5inv(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int dag);

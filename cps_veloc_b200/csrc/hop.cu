@@ -96,8 +96,8 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   hp.cb = L.cb;
   hp.dag = L.dag;
   hp.dwf = (D.kind == KIND_DWF);
-  hp.h5 = 2.0;                 // 2 / a5, a5inv = 1
-  hp.h5wall = -2.0 * D.mass;   // -2 m_f / a5
+  hp.h5 = 2.0 * D.a5inv;              // 2 / a5 (dwf_dslash_5_plus_omp.C:137)
+  hp.h5wall = -2.0 * D.mass * D.a5inv; // -2 m_f / a5 (:138)
   for (int s = 0; s < D.ls && s < MAX_LS; s++) hp.coef[s] = L.coef.empty() ? 0.0 : L.coef[(size_t)s < L.coef.size() ? s : 0];
   hp.mix = L.mix;
   hp.mix_cplx = (L.mix != nullptr && D.cplx) ? 1 : 0;

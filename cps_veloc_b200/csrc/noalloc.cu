@@ -127,8 +127,8 @@ void hop(const Dirac &D, int ep, int cb, int dag, int norm, const SpinorView &in
   hp.cb = cb;
   hp.dag = dag;
   hp.dwf = (D.kind == KIND_DWF);
-  hp.h5 = 2.0;
-  hp.h5wall = -2.0 * D.mass;
+  hp.h5 = 2.0 * D.a5inv;
+  hp.h5wall = -2.0 * D.mass * D.a5inv;
   for (int s = 0; s < D.ls && s < MAX_LS; s++) hp.coef[s] = -D.kappa * D.kappa;
   hp.norm = norm;
   hp.red_op = RED_STORE;

@@ -192,8 +192,9 @@ void upload(DeviceBuffer &buf, const std::vector<double> &h) {
 
 }  // namespace
 
-Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_)
-    : lat(l), kind(kind_), ls(ls_), mass(mass_), m5(m5_), b(b_), c(c_), kappa(0), kappa_c(0) {
+Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_, double a5inv_)
+    : lat(l), kind(kind_), ls(ls_), mass(mass_), m5(m5_), b(b_), c(c_), a5inv(a5inv_), kappa(0), kappa_c(0) {
+  if (!(a5inv > 0.0)) throw Error(-1, "dwf_a5_inv must be positive");
   if (kind == KIND_WILSON) {
     ls = 1;
     kappa = 1.0 / (2.0 * (mass + 4.0));  // d_op_wilson.C:134-137
@@ -201,7 +202,7 @@ Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_
   }
   if (ls < 2 || ls > MAX_LS) throw Error(-1, "Ls must be in [2, 32]");
   if (kind == KIND_DWF) {
-    kappa = 1.0 / (2.0 * (4.0 + 1.0 - m5));  // dwf_init.C:97-98, a5inv = 1
+    kappa = 1.0 / (2.0 * (4.0 + a5inv - m5));  // dwf_init.C:97-98
     return;
   }
   // Mobius: d_op_mobius.C:112-131 (real b, c: the same for every slice)
@@ -209,14 +210,14 @@ Dirac::Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_
 }
 
 // Per-slice kappa_b, kappa_c and K = kappa_b / kappa_c as the zMobius
-// operator sets them (d_op_zmobius.C:246-292, a5inv = 1), and every s-local
+// operator sets them (d_op_zmobius.C:246-292, with a5inv), and every s-local
 // matrix the operators apply.
 void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
   std::vector<cd> kb(ls), kc(ls), K(ls);
   cplx = false;
   for (int s = 0; s < ls; s++) {
-    kb[s] = 1.0 / (2.0 * (bs[s] * (4.0 - m5) + 1.0));
-    kc[s] = 1.0 / (2.0 * (cs[s] * (4.0 - m5) - 1.0));
+    kb[s] = 1.0 / (2.0 * (bs[s] * (4.0 - m5) + a5inv));
+    kc[s] = 1.0 / (2.0 * (cs[s] * (4.0 - m5) - a5inv));
     K[s] = kb[s] / kc[s];
     cplx = cplx || bs[s].imag() != 0.0 || cs[s].imag() != 0.0;
   }
@@ -241,8 +242,10 @@ void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
   std::vector<cd> Ru = diag_right(ls, diag_left(ls, ckb, Su), mkb), Rd = diag_right(ls, diag_left(ls, ckb, Sd), mkb);
   // M5 = 1 + K D5, what MatInv applies to the initial guess (the b/c mixing
   // form with b = 1, c = K)
-  std::vector<cd> m5u, m5d;
+  std::vector<cd> m5u, m5d, m5au, m5ad, Ka(ls);
   bmix(ls, std::vector<cd>(ls, 1.0), K, mass, m5u, m5d);
+  for (int s = 0; s < ls; s++) Ka[s] = a5inv * K[s];
+  bmix(ls, std::vector<cd>(ls, 1.0), Ka, mass, m5au, m5ad);
   // -kappa_b(s) on both chiralities (zmobius_m-sym2.h: the last step of MatPc)
   std::vector<cd> kbm((size_t)ls * ls, 0.0);
   for (int s = 0; s < ls; s++) kbm[(size_t)s * ls + s] = -kb[s];
@@ -262,6 +265,7 @@ void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
   upload(mixM5i, hM5i);
   upload(mixM5id, hM5id);
   upload(mixM5, packm(m5u, m5d));
+  upload(mixM5a, packm(m5au, m5ad));
   upload(mixKb, packm(kbm, kbm));
 }
 

@@ -188,9 +188,10 @@ class CgResult:
 class _DiracOp:
     kind = A.WILSON
 
-    def __init__(self, lat: Lattice, mass: float, ls: int = 1, m5: float = 1.8, b: float = 1.0, c: float = 0.0):
+    def __init__(self, lat: Lattice, mass: float, ls: int = 1, m5: float = 1.8, b: float = 1.0, c: float = 0.0,
+                 a5_inv: float = 1.0):
         self.lat = lat
-        arg = A.DiracArg(self.kind, ls, mass, m5, b, c)
+        arg = A.DiracArg(self.kind, ls, mass, m5, b, c, a5_inv)
         h = C.c_void_p()
         check(lib().cpsgpu_dirac_create(lat._h, C.byref(arg), C.byref(h)))
         self._h = h
@@ -210,6 +211,31 @@ class _DiracOp:
         if x.size != self.f_size:
             raise ValueError(f"vector must hold {self.f_size} reals")
         return x
+
+    def _full(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != 2 * self.f_size:
+            raise ValueError(f"full vector must hold {2 * self.f_size} reals")
+        return x
+
+    def Mat(self, inp) -> np.ndarray:
+        """DiracOp*::Mat on a full vector (both checkerboards, the reference's order)"""
+        inp = self._full(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_mat(self._h, dptr(out), dptr(inp), 0))
+        return out
+
+    def MatDag(self, inp) -> np.ndarray:
+        inp = self._full(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_mat(self._h, dptr(out), dptr(inp), 1))
+        return out
+
+    def MatHerm(self, inp) -> np.ndarray:
+        inp = self._full(inp)
+        out = np.empty_like(inp)
+        check(lib().cpsgpu_mat_herm(self._h, dptr(out), dptr(inp)))
+        return out
 
     def Dslash(self, inp, cb: int, dag: int = 0, prec: int = A.DOUBLE) -> np.ndarray:
         inp = self._vec(inp)
@@ -565,15 +591,25 @@ class DiracOpWilson(_DiracOp):
 class DiracOpDwf(_DiracOp):
     kind = A.DWF
 
-    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8):
-        super().__init__(lat, mass, ls=ls, m5=m5)
+    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8, a5_inv: float = 1.0):
+        super().__init__(lat, mass, ls=ls, m5=m5, a5_inv=a5_inv)
 
 
 class DiracOpMobius(_DiracOp):
     kind = A.MOBIUS
 
-    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8, b: float = 1.5, c: float = 0.5):
-        super().__init__(lat, mass, ls=ls, m5=m5, b=b, c=c)
+    def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8, b: float = 1.5, c: float = 0.5,
+                 a5_inv: float = 1.0):
+        super().__init__(lat, mass, ls=ls, m5=m5, b=b, c=c, a5_inv=a5_inv)
+
+    def MatPcDagMatPcShift(self, inp, mu: float, prec: int = A.DOUBLE):
+        """DiracOpMobius::MatPcDagMatPcShift (eigen_shift mu): returns
+        (M^+ M in - 2 mu R g5 M in + mu^2 in, |M in|^2)"""
+        inp = self._vec(inp)
+        out = np.empty_like(inp)
+        dot = C.c_double()
+        check(lib().cpsgpu_matpc_dag_matpc_shift(self._h, dptr(out), dptr(inp), mu, C.byref(dot), prec))
+        return out, dot.value
 
     def Dslash(self, inp, cb, dag=0, prec=A.DOUBLE):
         raise NotImplementedError("Mobius: use Dslash4 (zmobius_dslash_4)")

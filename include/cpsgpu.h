@@ -131,11 +131,16 @@ typedef struct {
   double m5;       /* DoArg.dwf_height */
   double mobius_b; /* DoArgExt.mobius_b_coeff */
   double mobius_c; /* DoArgExt.mobius_c_coeff */
+  double a5_inv;   /* DoArg.dwf_a5_inv, the fifth-direction inverse lattice
+                      spacing (DWF, Mobius); 0 selects the default 1 */
 } cpsgpu_dirac_arg;
 
 /* Replaces the DiracOpWilson / DiracOpDwf / DiracOpMobius constructors
  * (d_op_wilson.C:54-137, d_op_dwf.C:67-100, d_op_mobius.C:57-140): kappa
- * = 1/(2(m+4)) (Wilson), 1/(2(5-M5)) (DWF), kappa_b and kappa_c (Mobius). */
+ * = 1/(2(m+4)) (Wilson), 1/(2(4 + a5_inv - M5)) (DWF, dwf_init.C:97-98),
+ * kappa_b = 1/(2(b(4-M5) + a5_inv)) and kappa_c = 1/(2(c(4-M5) - a5_inv))
+ * (Mobius, d_op_mobius.C:105-108); the DWF fifth-direction hop weighs 2 a5_inv
+ * and -2 m_f a5_inv at the walls (dwf_dslash_5_plus_omp.C:137-138). */
 int cpsgpu_dirac_create(cpsgpu_lattice lat, const cpsgpu_dirac_arg *arg, cpsgpu_dirac *d);
 int cpsgpu_dirac_destroy(cpsgpu_dirac d);
 /* Complex per-slice Mobius coefficients (DiracOpZMobius, d_op_zmobius.C
@@ -177,6 +182,24 @@ int cpsgpu_matpc_dag_matpc(cpsgpu_dirac d, double *out, const double *in, double
  * streams) race.  *dot = |MatPc in|^2 when dot is non-null.  Returns when the
  * result is in out_dev; the caller must have finished writing in_dev. */
 int cpsgpu_matpc_dag_matpc_noalloc(cpsgpu_dirac d, double *out_dev, const double *in_dev, double *dot);
+/* DiracOp*::Mat (dag 0) / MatDag (dag 1), the unpreconditioned operator on
+ * full vectors of both checkerboards, 2 n doubles ([odd][even] halves for
+ * Wilson and DWF, [even][odd] for Mobius): Wilson d_op_wilson.C:362-424,
+ * DWF d_op_dwf.C:541-627, Mobius Mat d_op_mobius.C:735-795 (out = (1 +
+ * a5_inv K D5) in - kappa_b Dslash_4 of the other half).  Mobius MatDag
+ * returns CPSGPU_ERR_ARG: the reference's stops with an error
+ * (d_op_mobius.C:879).  FP64. */
+int cpsgpu_mat(cpsgpu_dirac d, double *out, const double *in, int dag);
+/* DiracOp*::MatHerm: gamma_5 Mat (Wilson, d_op_wilson.C:426-443),
+ * gamma_5 R Mat with R the reflection s -> Ls-1-s of FdwfBase::Freflex
+ * (DWF d_op_dwf.C:629-660, Mobius d_op_mobius.C:915-942); gamma_5 =
+ * diag(1, 1, -1, -1) (MultGamma 15).  Full vectors as cpsgpu_mat.  FP64. */
+int cpsgpu_mat_herm(cpsgpu_dirac d, double *out, const double *in);
+/* DiracOpMobius::MatPcDagMatPcShift with eigen_shift mu (d_op_mobius.C:235,
+ * zmobius_mdagm_shift zmobius_mdagm.C:79-135): out = M^+ M in - 2 mu R g5
+ * M in + mu^2 in, M = MatPc, R g5 = ReflectAndMultGamma5 within the
+ * checkerboard; *dot = |M in|^2 when dot is non-null.  Mobius only. */
+int cpsgpu_matpc_dag_matpc_shift(cpsgpu_dirac d, double *out, const double *in, double mu, double *dot, int prec);
 /* Mobius pieces: zmobius_dslash_4 (zmobius_dslash_4.C:209) and the
  * out-of-place zmobius_m5inv (zmobius_m5inv.C:822). */
 int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);

@@ -27,15 +27,16 @@ _dp = C.POINTER(C.c_double)
 
 
 class OracleGeom(C.Structure):
-    _fields_ = [("L", C.c_int * 4), ("ls", C.c_int), ("bc", C.c_double * 4)]
+    _fields_ = [("L", C.c_int * 4), ("ls", C.c_int), ("bc", C.c_double * 4), ("a5_inv", C.c_double)]
 
     @classmethod
-    def make(cls, L, ls=1, bc=(1, 1, 1, -1)):
+    def make(cls, L, ls=1, bc=(1, 1, 1, -1), a5_inv=1.0):
         g = cls()
         for k in range(4):
             g.L[k] = L[k]
             g.bc[k] = bc[k]
         g.ls = ls
+        g.a5_inv = a5_inv
         return g
 
 
@@ -126,6 +127,8 @@ def load_oracle() -> C.CDLL:
             getattr(L, k).restype = None
         L.orc_mobius_params.argtypes = [m, i, d, d, d]
         L.orc_mobius_params.restype = None
+        L.orc_mobius_params_a5.argtypes = [m, i, d, d, d, d]
+        L.orc_mobius_params_a5.restype = None
         L.orc_invcg.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, d, d, i, _dp, _dp]
         L.orc_invcg.restype = i
         L.orc_wilson_matinv.argtypes = [g, _dp, _dp, _dp, d, d, i, _dp]
@@ -176,6 +179,8 @@ def load_reference() -> C.CDLL:
         i, d = C.c_int, C.c_double
         L.ref_init.argtypes = [i, i, i, i, i, d, d, d, i]
         L.ref_init.restype = i
+        L.ref_init_a5.argtypes = [i, i, i, i, i, d, d, d, i, d]
+        L.ref_init_a5.restype = i
         for k in ("ref_dwf_kappa", "ref_mobius_kappa_b", "ref_mobius_kappa_c"):
             getattr(L, k).restype = d
         sig = {

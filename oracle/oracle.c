@@ -19,6 +19,9 @@ static long vol_cb(const orc_geom *g) {
   return (long)g->L[0] * g->L[1] * g->L[2] * g->L[3] / 2;
 }
 
+/* the fifth-direction inverse spacing (DoArg.dwf_a5_inv; 0 reads as 1) */
+static double a5inv(const orc_geom *g) { return g->a5_inv != 0.0 ? g->a5_inv : 1.0; }
+
 /* checkerboard index of a site (wilson_dslash.C:288) */
 static long cb_index(const orc_geom *g, const int x[4]) {
   return x[0] / 2 + (long)(g->L[0] / 2) * (x[1] + g->L[1] * (x[2] + (long)g->L[2] * x[3]));
@@ -145,7 +148,7 @@ void orc_wilson_mdagm(const orc_geom *g, double *chi, const double *u,
 /* dwf_dslash.C:32-51 = dwf_dslash_4 (dwf_dslash_4.C:68-154: slice s uses 4D
  * parity (s+cb)%2) + dwf_dslash_5_plus (dwf_dslash_5_plus_omp.C:115-271:
  * out[s] += 2/a5 * P in[s-1] on one chiral half and P' in[s+1] on the other,
- * the walls weighted by -2 m_f / a5).  a5inv = 1. */
+ * the walls weighted by -2 m_f / a5), 1/a5 = g->a5_inv. */
 void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
                     const double *in, double mass, int cb, int dag) {
   long vh = vol_cb(g);
@@ -153,7 +156,7 @@ void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
   long slice = 24 * vh;
   for (int s = 0; s < ls; s++)
     orc_wilson_dslash(g, out + s * slice, u, in + s * slice, (s + cb) % 2, dag);
-  const double two_a5 = 2.0, wall = -2.0 * mass;
+  const double two_a5 = 2.0 * a5inv(g), wall = -2.0 * mass * a5inv(g);
   /* half fed from s-1 is the upper one for D, the lower one for D^dagger */
   int from_below = dag ? 12 : 0, from_above = dag ? 0 : 12;
   for (int s = 0; s < ls; s++) {
@@ -178,7 +181,7 @@ void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
 void orc_dwf_m(const orc_geom *g, double *out, const double *u,
                const double *in, double mass, double m5, int dag) {
   long n = 24 * vol_cb(g) * g->ls;
-  double kappa = 1.0 / (2.0 * (4.0 + 1.0 - m5));
+  double kappa = 1.0 / (2.0 * (4.0 + a5inv(g) - m5));
   double *tmp = malloc(sizeof(double) * n);
   orc_dwf_dslash(g, tmp, u, in, mass, 1, dag);
   orc_dwf_dslash(g, out, u, tmp, mass, 0, dag);
@@ -206,8 +209,12 @@ void orc_dwf_mdagm(const orc_geom *g, double *out, const double *u,
 /* ---------------------------------------------------------------------- */
 /* DiracOpMobius ctor, d_op_mobius.C:112-131 */
 void orc_mobius_params(orc_mobius *mp, int ls, double b, double c, double m5) {
-  double kb = 1.0 / (2.0 * (b * (4.0 - m5) + 1.0));
-  double kc = 1.0 / (2.0 * (c * (4.0 - m5) - 1.0));
+  orc_mobius_params_a5(mp, ls, b, c, m5, 1.0);
+}
+
+void orc_mobius_params_a5(orc_mobius *mp, int ls, double b, double c, double m5, double a5_inv) {
+  double kb = 1.0 / (2.0 * (b * (4.0 - m5) + a5_inv));
+  double kc = 1.0 / (2.0 * (c * (4.0 - m5) - a5_inv));
   for (int s = 0; s < ls; s++) {
     mp->b[s] = b;
     mp->c[s] = c;
@@ -646,7 +653,7 @@ int orc_wilson_matinv(const orc_geom *g, double *out, const double *u, const dou
 
 int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double *in, double mass, double m5,
                    double stop_rsd, int max_num_iter, double *true_res) {
-  matinv_ctx c = {g, 0, u, mass, m5, 1.0 / (2.0 * (4.0 + 1.0 - m5)), 1};  /* dwf_kappa, a5inv = 1 */
+  matinv_ctx c = {g, 0, u, mass, m5, 1.0 / (2.0 * (4.0 + a5inv(g) - m5)), 1};  /* dwf_kappa */
   return wilson_dwf_matinv(&c, out, in, stop_rsd, max_num_iter, true_res);
 }
 

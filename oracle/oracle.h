@@ -29,6 +29,7 @@ typedef struct {
   int L[4];      /* local lattice extent x,y,z,t (all even) */
   int ls;        /* fifth-dimension extent (1 for Wilson) */
   double bc[4];  /* +1 periodic, -1 antiperiodic, per direction */
+  double a5_inv; /* DoArg.dwf_a5_inv (0 reads as the default 1) */
 } orc_geom;
 
 /* Wilson hopping term (wilson_dslash.C:173-515): reads psi on checkerboard
@@ -43,7 +44,7 @@ void orc_wilson_mdagm(const orc_geom *g, double *chi, const double *u,
 
 /* Shamir DWF, 5D even-odd (dwf_dslash.C:32, dwf_dslash_4.C:68,
  * dwf_dslash_5_plus_omp.C:115, dwf_m.C:31, dwf_mdag.C:32, dwf_mdagm.C:32).
- * a5inv is fixed at 1 as in the reference's default DoArg. */
+ * a5inv = g->a5_inv (dwf_dslash_5_plus_omp.C:137-138, dwf_init.C:97-98). */
 void orc_dwf_dslash(const orc_geom *g, double *out, const double *u,
                     const double *in, double mass, int cb, int dag);
 void orc_dwf_m(const orc_geom *g, double *out, const double *u,
@@ -60,6 +61,9 @@ typedef struct {
   double complex b[64], c[64], kappa_b[64], K[64];
 } orc_mobius;
 void orc_mobius_params(orc_mobius *mp, int ls, double b, double c, double m5);
+/* the same with the fifth-direction spacing: kappa_b = 1/(2(b(4-M5)+a5inv)),
+ * kappa_c = 1/(2(c(4-M5)-a5inv)) (d_op_mobius.C:105-108) */
+void orc_mobius_params_a5(orc_mobius *mp, int ls, double b, double c, double m5, double a5_inv);
 void orc_mobius_dslash_4(const orc_geom *g, const orc_mobius *mp, double *out,
                          const double *u, const double *in, int cb, int dag,
                          double mass);

@@ -57,8 +57,16 @@ extern "C" {
 
 // Configure the reference for one geometry.  bc_t: 1 periodic, -1 antiperiodic
 // (only the BndCndType GJP records; the sign itself is on the links).
+int ref_init_a5(int lx, int ly, int lz, int lt, int ls, double m5, double mobius_b, double mobius_c, int bc_t,
+                double a5_inv);
 int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
              double mobius_b, double mobius_c, int bc_t) {
+  return ref_init_a5(lx, ly, lz, lt, ls, m5, mobius_b, mobius_c, bc_t, 1.0);
+}
+
+// the same with DoArg.dwf_a5_inv = a5_inv
+int ref_init_a5(int lx, int ly, int lz, int lt, int ls, double m5, double mobius_b, double mobius_c, int bc_t,
+                double a5_inv) {
   DoArg d;
   d.x_node_sites = lx; d.y_node_sites = ly; d.z_node_sites = lz;
   d.t_node_sites = lt; d.s_node_sites = ls;
@@ -66,7 +74,7 @@ int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
   d.x_bc = d.y_bc = d.z_bc = BND_CND_PRD;
   d.t_bc = (bc_t < 0) ? BND_CND_APRD : BND_CND_PRD;
   d.dwf_height = m5;
-  d.dwf_a5_inv = 1.0;
+  d.dwf_a5_inv = a5_inv;
   GJP.Initialize(d);
   GJP.Mobius_b(mobius_b);
   GJP.Mobius_c(mobius_c);
@@ -83,8 +91,8 @@ int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
     Dwf *m = &g_dwf;
     m->ls = ls;
     m->pc_type = ZMOB_PC_SYM2;
-    m->mobius_kappa_b = 1.0 / (2 * (mobius_b * (4 - m5) + 1.0));
-    m->mobius_kappa_c = 1.0 / (2 * (mobius_c * (4 - m5) - 1.0));
+    m->mobius_kappa_b = 1.0 / (2 * (mobius_b * (4 - m5) + a5_inv));
+    m->mobius_kappa_c = 1.0 / (2 * (mobius_c * (4 - m5) - a5_inv));
     m->zmobius_b.assign(ls, Complex(mobius_b, 0));
     m->zmobius_c.assign(ls, Complex(mobius_c, 0));
     m->zmobius_kappa_b.assign(ls, Complex(m->mobius_kappa_b, 0));
@@ -97,15 +105,15 @@ int ref_init(int lx, int ly, int lz, int lt, int ls, double m5,
 }
 
 // Complex per-slice coefficients, set as DiracOpZMobius's reset_mobius_arg
-// does (d_op_zmobius.C:246-292, a5inv = 1); b and c hold (re, im) per slice.
+// does (d_op_zmobius.C:246-292); b and c hold (re, im) per slice.
 void ref_set_zmobius(const double *b, const double *c) {
   Dwf *m = &g_dwf;
   const double m5 = GJP.DwfHeight();
   for (int s = 0; s < m->ls; s++) {
     m->zmobius_b[s] = Complex(b[2 * s], b[2 * s + 1]);
     m->zmobius_c[s] = Complex(c[2 * s], c[2 * s + 1]);
-    m->zmobius_kappa_b[s] = 1.0 / (2. * (m->zmobius_b[s] * (4 - m5) + 1.0));
-    m->zmobius_kappa_c[s] = 1.0 / (2. * (m->zmobius_c[s] * (4 - m5) - 1.0));
+    m->zmobius_kappa_b[s] = 1.0 / (2. * (m->zmobius_b[s] * (4 - m5) + GJP.DwfA5Inv()));
+    m->zmobius_kappa_c[s] = 1.0 / (2. * (m->zmobius_c[s] * (4 - m5) - GJP.DwfA5Inv()));
     m->zmobius_kappa_ratio[s] = m->zmobius_kappa_b[s] / m->zmobius_kappa_c[s];
   }
 }

@@ -181,6 +181,45 @@ void rs_matpc_dag(double *out, double *in, double mass) {
   delete op;
 }
 
+// The unpreconditioned operators on full vectors (both checkerboards, the
+// DiracOp's storage order): Mat (dag 0), MatDag (dag 1) and MatHerm
+// (d_op_wilson.C:362-443, d_op_dwf.C:541-660, d_op_mobius.C:735-942).
+void rs_mat(double *out, double *in, double mass, int dag) {
+  CgArg cg;
+  fill_cg(cg, mass, 1e-8, 10);
+  DiracOp *op = make_op((Vector *)out, (Vector *)in, &cg);
+  Vector *o = (Vector *)out, *i = (Vector *)in;
+  switch (g_kind) {
+    case 0: dag ? static_cast<DiracOpWilson *>(op)->MatDag(o, i) : static_cast<DiracOpWilson *>(op)->Mat(o, i); break;
+    case 1: dag ? static_cast<DiracOpDwf *>(op)->MatDag(o, i) : static_cast<DiracOpDwf *>(op)->Mat(o, i); break;
+    default: static_cast<DiracOpMobius *>(op)->Mat(o, i); break;  // MatDag stops with an error (:879)
+  }
+  delete op;
+}
+void rs_matherm(double *out, double *in, double mass) {
+  CgArg cg;
+  fill_cg(cg, mass, 1e-8, 10);
+  DiracOp *op = make_op((Vector *)out, (Vector *)in, &cg);
+  Vector *o = (Vector *)out, *i = (Vector *)in;
+  switch (g_kind) {
+    case 0: static_cast<DiracOpWilson *>(op)->MatHerm(o, i); break;
+    case 1: static_cast<DiracOpDwf *>(op)->MatHerm(o, i); break;
+    default: static_cast<DiracOpMobius *>(op)->MatHerm(o, i); break;
+  }
+  delete op;
+}
+// DiracOpMobius::MatPcDagMatPcShift with CgArg.eigen_shift = mu (d_op_mobius.C:235)
+void rs_mdagm_shift(double *out, double *in, double mass, double mu, double *dot) {
+  CgArg cg;
+  fill_cg(cg, mass, 1e-8, 10);
+  cg.eigen_shift = mu;
+  DiracOp *op = make_op((Vector *)out, (Vector *)in, &cg);
+  Float d = 0.0;
+  static_cast<DiracOpMobius *>(op)->MatPcDagMatPcShift((Vector *)out, (Vector *)in, &d);
+  delete op;
+  *dot = d;
+}
+
 // DiracOp::MInvCG: psi[k] (one checkerboard each) hold the initial guesses,
 // rsd[k] the requested residuals on entry and the achieved ones on exit.
 int rs_minvcg(double **psi, double *chi, double chi_norm, double *shift, int nshift, int isz, double *rsd,

@@ -16,6 +16,9 @@ b, c, bc_t, task, and per task:
   .npy; mass, stop_rsd, max_iter, shift);
 * ``minvcg``: DiracOp::MInvCG (gauge, src, shifts, rsd, type, mass,
   max_iter);
+* ``ops``: Mat, MatDag (not Mobius: the reference's stops with an error),
+  MatHerm on the full vector src, and for Mobius MatPcDagMatPcShift
+  (eigen_shift mu) on its first half (gauge, src, mass, mu);
 * ``cgtime``: wall time of DiracOp::InvCgShift capped at each max_iter of
   ``caps`` (zero initial guess each time, after ``warmup`` untimed capped
   runs), on the source MatPcDag(src) (gauge, src, mass, stop_rsd).
@@ -63,6 +66,9 @@ def _lib():
     L.rs_matinv.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
     L.rs_matpc_dag_matpc.argtypes = [_dp, _dp, C.c_double, _dp]
     L.rs_matpc_dag.argtypes = [_dp, _dp, C.c_double]
+    L.rs_mat.argtypes = [_dp, _dp, C.c_double, C.c_int]
+    L.rs_matherm.argtypes = [_dp, _dp, C.c_double]
+    L.rs_mdagm_shift.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp]
     L.rs_minvcg.argtypes = [C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_double,
                             C.c_int]
     return L
@@ -159,6 +165,24 @@ def run(spec: dict) -> dict:
                     times.append(dt)
                     iters.append(it)
             out.update(times=np.array(times), caps_iters=np.array(iters))
+        elif spec["task"] == "ops":
+            full = np.ascontiguousarray(np.load(spec["src"]), dtype=np.float64)
+            res = {}
+            for dag in ((0,) if kind == 2 else (0, 1)):
+                o = np.zeros_like(full)
+                L.rs_mat(_p(o), _p(full.copy()), spec["mass"], dag)
+                res["matdag" if dag else "mat"] = o
+            o = np.zeros_like(full)
+            L.rs_matherm(_p(o), _p(full.copy()), spec["mass"])
+            res["matherm"] = o
+            if kind == 2:
+                half = np.ascontiguousarray(full[:full.size // 2])
+                o = np.zeros_like(half)
+                d = C.c_double()
+                L.rs_mdagm_shift(_p(o), _p(half.copy()), spec["mass"], spec.get("mu", 0.3), C.byref(d))
+                res.update(shift=o, shift_dot=d.value)
+            out.update(res)
+            it = 0
         else:
             raise ValueError(spec["task"])
     out.update(iters=it, true_res=tr.value, res_hist=_hist(cap.text))

@@ -41,25 +41,26 @@ def s_inner(v, L, ls, layout):
 class OracleOps:
     """The oracle's operators on one geometry (gauge field without signs)."""
 
-    def __init__(self, O, L, u, ls=1, bc=(1, 1, 1, -1), m5=1.8, b=1.5, c=0.5):
+    def __init__(self, O, L, u, ls=1, bc=(1, 1, 1, -1), m5=1.8, b=1.5, c=0.5, a5_inv=1.0):
         self.O = O
         self.L = tuple(L)
         self.u = np.ascontiguousarray(u)
         self.ls = ls
-        self.g = OracleGeom.make(L, ls, bc)
+        self.a5_inv = a5_inv
+        self.g = OracleGeom.make(L, ls, bc, a5_inv)
         self.g1 = OracleGeom.make(L, 1, bc)
         self.m5 = m5
         self.mp = OracleMobius()
         if ls > 1:
-            O.orc_mobius_params(C.byref(self.mp), ls, b, c, m5)
+            O.orc_mobius_params_a5(C.byref(self.mp), ls, b, c, m5, a5_inv)
         self.n = 24 * ls * vh_of(L)
 
     def set_zmobius(self, b, c):
         """complex per-slice b_s, c_s with kappa_b, K as DiracOpZMobius sets them
         (d_op_zmobius.C:246-292, a5inv = 1)"""
         for s in range(self.ls):
-            kb = 1 / (2 * (b[s] * (4 - self.m5) + 1))
-            kc = 1 / (2 * (c[s] * (4 - self.m5) - 1))
+            kb = 1 / (2 * (b[s] * (4 - self.m5) + self.a5_inv))
+            kc = 1 / (2 * (c[s] * (4 - self.m5) - self.a5_inv))
             for name, v in (("b", b[s]), ("c", c[s]), ("kappa_b", kb), ("K", kb / kc)):
                 arr = getattr(self.mp, name)
                 arr[2 * s], arr[2 * s + 1] = complex(v).real, complex(v).imag
@@ -227,7 +228,7 @@ class OracleOps:
             psi = -kappa * kappa * self.wilson_m(chi, kappa, 0)
             rho, sigma = self.wilson_dslash(chi, 1, 0), self.wilson_dslash(psi, 1, 1)
         else:
-            k5 = 1 / (2 * (5 - self.m5))
+            k5 = 1 / (2 * (4 + self.a5_inv - self.m5))
             psi = -k5 * k5 * self.dwf_m(chi, mass, 0)
             rho, sigma = self.dwf_dslash(chi, mass, 1, 0), self.dwf_dslash(psi, mass, 1, 1)
         return np.concatenate([chi, rho]), np.concatenate([psi, sigma])
@@ -236,6 +237,61 @@ class OracleOps:
         y = self.z()
         self.O.orc_mobius_booee(C.byref(self.g), C.byref(self.mp), p(y), p(np.ascontiguousarray(x)), mass)
         return y
+
+    # ---- unpreconditioned operators on full vectors [half 0][half 1] in
+    # the reference's storage order (Wilson, DWF: [odd][even]; Mobius
+    # [even][odd]), composed from the pinned kernels
+    def _hop(self, kind, x, mass, cb, dag):
+        if kind == "wilson":
+            return self.wilson_dslash(x, cb, dag)
+        return self.dwf_dslash(x, mass, cb, dag)
+
+    def mat(self, kind, x, mass=0.0, kappa=0.0, dag=0):
+        """DiracOpWilson / DiracOpDwf::Mat, MatDag (d_op_wilson.C:362-424,
+        d_op_dwf.C:541-627): out_0 = in_0 - kappa D(in_1, CHKB_EVEN),
+        out_1 = in_1 - kappa D(in_0, CHKB_ODD); DiracOpMobius::Mat
+        (d_op_mobius.C:735-795): out_0 = (1 + a5inv K D5) in_0 - kappa_b
+        Dslash_4(in_1, CHKB_ODD), out_1 = (1 + a5inv K D5) in_1 - kappa_b
+        Dslash_4(in_0, CHKB_EVEN)"""
+        x = np.ascontiguousarray(x)
+        h = x.size // 2
+        x0, x1 = x[:h], x[h:]
+        if kind != "mobius":
+            k = kappa if kind == "wilson" else 1 / (2 * (4 + self.a5_inv - self.m5))
+            return np.concatenate([x0 - k * self._hop(kind, x1, mass, 0, dag), x1 - k * self._hop(kind, x0, mass, 1, dag)])
+        if dag:
+            raise ValueError("the reference's DiracOpMobius::MatDag stops with an error")
+        kb = self.mp.kappa_b[0]  # real part of kappa_b(s = 0) (the array holds re, im pairs)
+
+        def m5(v):
+            return v + self.a5_inv * (self.mobius_m5(v, mass) - v)
+        return np.concatenate([m5(x0) - kb * self.mobius_dslash_4(x1, mass, 1, 0),
+                               m5(x1) - kb * self.mobius_dslash_4(x0, mass, 0, 0)])
+
+    def gamma5_reflect(self, kind, y):
+        """MatHerm's left factor: gamma_5 (reals 12-23 negated,
+        DiracOpWilsonTypes::MultGamma 15) after, for DWF and Mobius, the
+        reflection s -> Ls-1-s of FdwfBase::Freflex (f_dwf_base.C:1693-1790),
+        which for even Ls takes each slice from the other half"""
+        y = np.ascontiguousarray(y).reshape(2, max(self.ls, 1), -1, 24).copy()
+        if kind != "wilson":
+            y = y[::-1, ::-1] if self.ls % 2 == 0 else y[:, ::-1]
+        y = y.copy()
+        y[..., 12:] *= -1
+        return y.reshape(-1)
+
+    def matherm(self, kind, x, mass=0.0, kappa=0.0):
+        return self.gamma5_reflect(kind, self.mat(kind, x, mass, kappa, 0))
+
+    def mobius_mdagm_shift(self, x, mass, mu):
+        """zmobius_mdagm_shift (zmobius_mdagm.C:79-135): out = M^+ M x - 2 mu
+        R g5 M x + mu^2 x with R g5 = ReflectAndMultGamma5 (slice s from
+        Ls-1-s within the checkerboard, reals 12-23 negated); dot = |M x|^2"""
+        mx = self.mobius_m(x, mass, 0)
+        out = self.mobius_m(mx, mass, 1)
+        r = np.ascontiguousarray(mx).reshape(self.ls, -1, 24)[::-1].copy()
+        r[..., 12:] *= -1
+        return out - 2 * mu * r.reshape(-1) + mu * mu * np.asarray(x), float(mx @ mx)
 
     def mobius_force_vecs(self, phi1, phi2, mass):
         """DiracOpMobius::CalcHmdForceVecs(v1, v2, phi1, phi2), SYM2
