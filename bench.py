@@ -343,6 +343,20 @@ def extra_mobius(A) -> dict:
         m2, b2 = C.c_double(), C.c_double()
         A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, 20, C.byref(m2), C.byref(b2)))
         out[f"hop_{name}"] = {"ms": m2.value, "GB_s": b2.value / m2.value / 1e6}
+    # the same M5^-1 of the FP16 field on the tensor cores (mma.sync m16n8k16),
+    # and the FP16-inner solve with every standalone mixing there
+    D.set_mix_impl(True)
+    ms, by = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, A.HALF, 20)
+    out["m5inv_half_tensor_cores"] = {"ms": ms, "GB_s": by / ms / 1e6, "frac_of_measured_hbm": by / ms / 1e6 / pk,
+                                      "unit": "tensor cores (mma.sync m16n8k16, FP16 operands, FP32 accumulation)",
+                                      "speedup_vs_cuda_cores": out["m5inv_half"]["ms"] / ms}
+    x = np.zeros(D.f_size)
+    D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
+    x = np.zeros(D.f_size)
+    rt = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
+    out["half_inner_cg_tensor_core_mixing"] = {"time_s": rt.seconds, "iterations": rt.iterations,
+                                               "true_res": rt.true_res, "reliable_updates": rt.reliable_updates}
+    D.set_mix_impl(False)
     D.close()
     lat.close()
     return out
@@ -380,6 +394,74 @@ def extra_multishift(A) -> dict:
     D.close()
     lat.close()
     return out
+
+
+def extra_solve_batch(A) -> dict:
+    """Eight independent DWF solves, Ls = 16, M5 = 1.8, m_f log-spaced in
+    [0.001, 0.1], lattices 8^3x16 ... 16^3x32, mixed precision (FP32 inner)
+    to a true residual of 1e-10: one cpsgpu_solve_batch call (every solve's
+    loop a branch of one graph launch) against the same eight solves one
+    after another (cpsgpu_invcg_field); wall time of the device-field calls
+    after one untimed round each."""
+    from cps_veloc_b200.dirac import DiracOpDwf, Lattice, gen_gauge, gen_gaussian
+
+    lattices = [(8, 8, 8, 16), (8, 8, 8, 32), (12, 12, 12, 16), (12, 12, 12, 24), (16, 16, 16, 16),
+                (16, 16, 16, 24), (16, 16, 16, 32), (16, 16, 16, 32)]
+    masses = list(np.logspace(-3, -1, 8))
+    lats, ops, sols, srcs, zeros = [], [], [], [], []
+    for k, (L, m) in enumerate(zip(lattices, masses)):
+        lat = Lattice(L, (1, 1, 1, -1))
+        lat.import_gauge(gen_gauge(L, seed=SEED + 20 + k, width=0.3))
+        D = DiracOpDwf(lat, mass=m, ls=LS, m5=M5)
+        D.autotune(A.SINGLE)
+        lats.append(lat)
+        ops.append(D)
+        z = np.zeros(D.f_size)
+        zeros.append(z)
+        sols.append(field(A, D, A.DOUBLE, z))
+        srcs.append(field(A, D, A.DOUBLE, gen_gaussian(D.f_size, seed=SEED, stream=30 + k)))
+    arg = A.CgArg()
+    A.lib().cpsgpu_cg_arg_default(C.byref(arg))
+    arg.stop_rsd, arg.max_num_iter, arg.precision, arg.chunk = STOP, 100000, A.SINGLE, 16
+    n = len(ops)
+    VP = C.c_void_p * n
+
+    def reset():
+        for f, z in zip(sols, zeros):
+            A.check(A.lib().cpsgpu_field_upload(f, A.dptr(z)))
+
+    def batch():
+        res = (A.CgResult * n)()
+        reset()
+        t0 = time.perf_counter()
+        A.check(A.lib().cpsgpu_solve_batch(n, VP(*[D._h.value for D in ops]), VP(*[f.value for f in sols]),
+                                           VP(*[f.value for f in srcs]), (A.CgArg * n)(*([arg] * n)), res))
+        return time.perf_counter() - t0, list(res)
+
+    def sequential():
+        reset()
+        tot, out = 0.0, []
+        for D, fx, fb in zip(ops, sols, srcs):
+            r = A.CgResult()
+            t0 = time.perf_counter()
+            A.check(A.lib().cpsgpu_invcg_field(D._h, fx, fb, C.byref(arg), C.byref(r)))
+            tot += time.perf_counter() - t0
+            out.append(r)
+        return tot, out
+
+    batch()
+    sequential()
+    tb, rb = batch()
+    ts, rs = sequential()
+    for f in sols + srcs:
+        A.lib().cpsgpu_field_destroy(f)
+    for D, lat in zip(ops, lats):
+        D.close()
+        lat.close()
+    return {"lattices": [list(L) for L in lattices], "ls": LS, "mf": masses, "inner": "fp32",
+            "batch_one_launch_s": tb, "sequential_s": ts, "speedup_batch_vs_sequential": ts / tb,
+            "iterations": [r.iterations for r in rb], "iterations_sequential": [r.iterations for r in rs],
+            "all_converged_1e-10": all(r.status == A.CONVERGED and r.true_res <= STOP for r in rb)}
 
 
 def extra_force(A, D, pk) -> dict:
@@ -549,6 +631,7 @@ def main(argv=None) -> int:
         extras = {"batched_12_point_sources": extra_batched(A, D, sloppy),
                   "mobius_24x64_ls12": extra_mobius(A),
                   "multishift_wilson_32x64": extra_multishift(A),
+                  "batch_8_dwf_solves": extra_solve_batch(A),
                   "hmc_force_dwf_16x32_ls16": extra_force(A, D, pk)}
 
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))

@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
             "cpsgpu_matpc_dag_matpc": (C.c_int, [vp, _dp, _dp, _dp, C.c_int]),
             "cpsgpu_matpc_dag_matpc_noalloc": (C.c_int, [vp, vp, vp, _dp]),
             "cpsgpu_mat": (C.c_int, [vp, _dp, _dp, C.c_int]),
+            "cpsgpu_set_mix_impl": (C.c_int, [vp, C.c_int]),
             "cpsgpu_mat_herm": (C.c_int, [vp, _dp, _dp]),
             "cpsgpu_matpc_dag_matpc_shift": (C.c_int, [vp, _dp, _dp, C.c_double, _dp, C.c_int]),
             "cpsgpu_mobius_dslash_4": (C.c_int, [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]),
@@ -170,6 +171,8 @@ def lib() -> C.CDLL:
             "cpsgpu_field_dot": (C.c_int, [vp, vp, _dp, _dp]),
             "cpsgpu_mdagm_field": (C.c_int, [vp, vp, vp]),
             "cpsgpu_invcg_field": (C.c_int, [vp, vp, vp, C.POINTER(CgArg), C.POINTER(CgResult)]),
+            "cpsgpu_solve_batch": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(CgArg),
+                                             C.POINTER(CgResult)]),
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
             "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_mdagm": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),

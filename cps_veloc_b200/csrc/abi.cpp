@@ -1311,6 +1311,56 @@ int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const
   });
 }
 
+int cpsgpu_solve_batch(int n, const cpsgpu_dirac *ops, const cpsgpu_field *sol, const cpsgpu_field *src,
+                       const cpsgpu_cg_arg *args, cpsgpu_cg_result *res) {
+  return guarded([&] {
+    if (n < 1 || !ops || !sol || !src || !args || !res) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    std::vector<CgSolver *> solvers;
+    std::vector<CgArgs> a;
+    for (int k = 0; k < n; k++) {
+      cpsgpu_dirac d = ops[k];
+      if (!d || !sol[k] || !src[k]) throw Error(CPSGPU_ERR_ARG, "null operator or field");
+      if (sol[k]->d != d || src[k]->d != d) throw Error(CPSGPU_ERR_ARG, "fields must belong to their operator");
+      if (sol[k]->f.prec != PREC_DOUBLE || src[k]->f.prec != PREC_DOUBLE) throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+      if (sol[k]->f.nrhs != src[k]->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+      if (args[k].max_num_iter < 1) throw Error(CPSGPU_ERR_ARG, "max_num_iter must be >= 1");
+      check_prec(args[k].precision);
+      need_gauge(d);
+      for (int j = 0; j < k; j++)
+        if (ops[j] == d && args[j].precision == args[k].precision)
+          throw Error(CPSGPU_ERR_ARG, "an operator appears twice in one precision: put its right-hand sides in one field");
+      CgSolver &S = solver_for(d, args[k].precision, src[k]->f.nrhs);
+      cudaStream_t st = d->D->lat->stream;
+      CPSGPU_CUDA(cudaMemcpyAsync(S.b64.data.ptr, src[k]->f.data.ptr, src[k]->f.data.bytes, cudaMemcpyDeviceToDevice, st));
+      CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, sol[k]->f.data.ptr, sol[k]->f.data.bytes, cudaMemcpyDeviceToDevice, st));
+      solvers.push_back(&S);
+      a.push_back(to_args(&args[k]));
+    }
+    std::vector<std::vector<CgResult>> r;
+    solve_batch(solvers, a, r);
+    int o = 0;
+    for (int k = 0; k < n; k++) {
+      cudaStream_t st = ops[k]->D->lat->stream;
+      CPSGPU_CUDA(cudaMemcpyAsync(sol[k]->f.data.ptr, solvers[k]->x64.data.ptr, sol[k]->f.data.bytes,
+                                  cudaMemcpyDeviceToDevice, st));
+      CPSGPU_CUDA(cudaStreamSynchronize(st));
+      for (const CgResult &x : r[k]) to_result(x, res + o++);
+    }
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores) {
+  return guarded([&] {
+    if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
+    if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "Ls x Ls mixing: Mobius operators only");
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    d->D->mix_tc = tensor_cores != 0;
+    for (auto &s : d->solvers) s.reset();  // captured graphs hold the other kernels
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned) {
   return guarded([&] {
     if (!d || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");

@@ -430,6 +430,10 @@ void launch_export_fermion(cudaStream_t s, int prec, const SpinorView &src, doub
 
 void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                 const SolverScalars *st, int gate) {
+  if (D.mix_tc && mix_tc_applies(D, prec)) {
+    launch_mix_tc(D, mix, in, out, st, gate);
+    return;
+  }
   const int ls = D.ls;
   int bx = 256 / ls, p2 = 1;
   while (p2 * 2 <= bx) p2 *= 2;

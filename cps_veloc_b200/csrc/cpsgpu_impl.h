@@ -146,6 +146,9 @@ struct Dirac {
   // right-hand sides per hop tile (consecutive blocks share links across
   // this many solves), per precision, set by the autotuner; 0 = untuned
   int rtile[3] = {0, 0, 0};
+  // the standalone Ls x Ls mixings of FP16 fields on the tensor cores
+  // (mix_tc.cu) instead of the CUDA cores
+  bool mix_tc = false;
   MsWork ms;  // multishift workspace
   int rhs_tile(int prec, int nrhs) const {
     const int t = rtile[prec];
@@ -165,11 +168,17 @@ struct HopLaunch {
   const double *mix = nullptr;
   std::vector<double> coef;  // per slice
   const void *halo_fwd = nullptr, *halo_bwd = nullptr;  // t halos of a decomposed lattice (dd.cu)
+  double *partials = nullptr;  // the reduction's per-block partials (null: the lattice's buffer)
 };
 void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
                 const SpinorView &x, const SpinorView &r, const SpinorView &sol, const SpinorView &p,
                 const SpinorView &b, SolverScalars *st);
 
+// the tensor-core form of launch_mix (mix_tc.cu): FP16 fields, real
+// matrices, Ls <= 16
+bool mix_tc_applies(const Dirac &D, int prec);
+void launch_mix_tc(const Dirac &D, const double *mix, const SpinorView &in, const SpinorView &out,
+                   const SolverScalars *st, int gate);
 // out = Mix in (per chirality Ls x Ls), all slices
 void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                 const SolverScalars *st = nullptr, int gate = 0);

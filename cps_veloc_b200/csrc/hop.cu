@@ -149,12 +149,13 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
       raised.push_back({fn, smem});
     }
   }
-  fn<<<grid, block, smem, lat.stream>>>(hp, v, st, lat.partials.as<double>());
+  double *part = L.partials ? L.partials : lat.partials.as<double>();
+  fn<<<grid, block, smem, lat.stream>>>(hp, v, st, part);
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;
   // the epilogue's reduction: per-block partials, summed and applied here
   const int nv = (ep_axpy(L.ep) && L.norm) ? 2 : (ep_cg(L.ep) || ep_res(L.ep)) ? 1 : 0;
-  if (nv && st) launch_finalize(lat.stream, nv, lat.partials.as<double>(), st, L.red_op, nsb * hp.nsg, in.nrhs, L.gate);
+  if (nv && st) launch_finalize(lat.stream, nv, part, st, L.red_op, nsb * hp.nsg, in.nrhs, L.gate);
 }
 
 }  // namespace cpsgpu

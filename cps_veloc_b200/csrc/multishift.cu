@@ -322,21 +322,30 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   const int iters = mh.k + 1;
 
   if (P != PREC_DOUBLE && refine) {
-    // FP64 refinement of every shift with the reliable-update CG
+    // FP64 refinement of every shift with the reliable-update CG, all shifts
+    // as one batched solve (right-hand side k: MatPcDagMatPc + shift_k from
+    // the sloppy solution psi_k, to its own residual), so the links are read
+    // once per tile of shifts and the iterations share their launches
     CgSolver cg(D, PREC_SINGLE);
-    cg.setup(1);
+    cg.setup(nshift);
+    const size_t one = (size_t)chi64.data.bytes;
     for (int k = 0; k < nshift; k++) {
-      CPSGPU_CUDA(cudaMemcpyAsync(cg.b64.data.ptr, chi64.data.ptr, chi64.data.bytes, cudaMemcpyDeviceToDevice, s));
-      CPSGPU_CUDA(cudaMemcpyAsync(cg.x64.data.ptr, psi[k].data.ptr, psi[k].data.bytes, cudaMemcpyDeviceToDevice, s));
-      CgArgs a;
-      a.stop_rsd = ms0.rsd_sq[k] > 0 ? std::sqrt(ms0.rsd_sq[k] / cp) : 1e-10;
-      a.max_num_iter = max_num_iter;
-      a.shift = shift[k];
-      a.src_norm_sq = 0.0;
-      std::vector<CgResult> res;
-      cg.run(a, res);
-      CPSGPU_CUDA(cudaMemcpyAsync(psi[k].data.ptr, cg.x64.data.ptr, psi[k].data.bytes, cudaMemcpyDeviceToDevice, s));
-      rsdcg[k] = res[0].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327 reports
+      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg.b64.data.ptr + k * one, chi64.data.ptr, one, cudaMemcpyDeviceToDevice, s));
+      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg.x64.data.ptr + k * one, psi[k].data.ptr, one, cudaMemcpyDeviceToDevice, s));
+    }
+    CgArgs a;
+    a.max_num_iter = max_num_iter;
+    a.src_norm_sq = 0.0;
+    a.delta = 0.01;
+    for (int k = 0; k < nshift; k++) {
+      a.shifts.push_back(shift[k]);
+      a.stop_rsds.push_back(ms0.rsd_sq[k] > 0 ? std::sqrt(ms0.rsd_sq[k] / cp) : 1e-10);
+    }
+    std::vector<CgResult> res;
+    cg.run(a, res);
+    for (int k = 0; k < nshift; k++) {
+      CPSGPU_CUDA(cudaMemcpyAsync(psi[k].data.ptr, (char *)cg.x64.data.ptr + k * one, one, cudaMemcpyDeviceToDevice, s));
+      rsdcg[k] = res[k].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327 reports
     }
   }
 

@@ -80,6 +80,9 @@ void CgSolver::setup(int nrhs_) {
   // partials: 2 values per block; the smallest hop block is 32 threads
   size_t nblk = (size_t)((vh + 31) / 32) * ls + 1024;
   L.partials.ensure(nblk * 2 * nrhs * sizeof(double));
+  partials.ensure(nblk * 2 * nrhs * sizeof(double));
+  static unsigned long long next_id = 0;
+  id = ++next_id;
   drop_graph();
 }
 
@@ -93,6 +96,8 @@ void CgSolver::drop_graph() {
 CgSolver::~CgSolver() {
   drop_graph();
   if (side) cudaStreamDestroy(side);
+  if (tev0) cudaEventDestroy(tev0);
+  if (tev1) cudaEventDestroy(tev1);
 }
 
 // Emit out-of-place MatPcDagMatPc on `in` with a final epilogue.
@@ -106,6 +111,7 @@ void CgSolver::emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_e
   HopLaunch Lh;
   Lh.prec = prec;
   Lh.gate = gate;
+  Lh.partials = partials.as<double>();
   // ---- M = MatPc ----
   Lh.dag = 0;
   if (mob) {
@@ -230,21 +236,21 @@ static bool all_done(const int *flags, int n) {
   return true;
 }
 
-void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
+void CgSolver::begin(const CgArgs &a) {
   Lattice &L = *D.lat;
   cudaStream_t s = L.stream;
   SolverScalars *stp = st.as<SolverScalars>();
   if (sloppy != PREC_DOUBLE && L.recon_err > 1e-5)
     throw Error(-1, "mixed precision needs SU(3) links (12-real reconstruction failed)");
-  const long long k0 = launch_counter();
-  cudaEvent_t tev0, tev1;
-  CPSGPU_CUDA(cudaEventCreate(&tev0));
-  CPSGPU_CUDA(cudaEventCreate(&tev1));
+  args = a;
+  k0 = launch_counter();
+  if (!tev0) CPSGPU_CUDA(cudaEventCreate(&tev0));
+  if (!tev1) CPSGPU_CUDA(cudaEventCreate(&tev1));
   CPSGPU_CUDA(cudaEventRecord(tev0, s));
 
   // |b|^2 per right-hand side
   launch_init_scalars(s, stp, nrhs, SolverScalars{});
-  launch_norm(s, PREC_DOUBLE, b64.view(), stp, L.partials.as<double>(), RED_STORE, GATE_NONE);
+  launch_norm(s, PREC_DOUBLE, b64.view(), stp, partials.as<double>(), RED_STORE, GATE_NONE);
   std::vector<SolverScalars> host(nrhs);
   CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
   CPSGPU_CUDA(cudaStreamSynchronize(s));
@@ -254,9 +260,10 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
     memset(&z, 0, sizeof(z));
     double bn = host[k].sum[0];
     z.src_norm = (a.src_norm_sq > 0) ? a.src_norm_sq : bn;
-    z.stop = z.src_norm * a.stop_rsd * a.stop_rsd;
+    const double rsd = (k < (int)a.stop_rsds.size()) ? a.stop_rsds[k] : a.stop_rsd;
+    z.stop = z.src_norm * rsd * rsd;
     z.max_iter = a.max_num_iter - 1;  // inv_cg.C:275
-    z.shift = a.shift;
+    z.shift = (k < (int)a.shifts.size()) ? a.shifts[k] : a.shift;
     z.delta2 = (sloppy == PREC_DOUBLE) ? 0.0 : a.delta * a.delta;
     init[k] = z;
   }
@@ -271,55 +278,119 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
     launch_zero(s, xs);
   }
   launch_convert(s, sloppy, p.view(), sloppy, r.view());
+}
 
-  // iterate in chunks of `chunk` iterations
+// The loop as a WHILE node of graph g whose body is one chunk of iterations
+// followed by the condition kernel: no host polling, and the loop stops
+// after the chunk in which the last solve finished.
+long long CgSolver::add_loop(cudaGraph_t g, int chunk) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  SolverScalars *stp = st.as<SolverScalars>();
+  ctl.ensure(2 * sizeof(int));
+  cudaGraphConditionalHandle hw;
+  CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = hw;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wn;
+  CPSGPU_CUDA(cudaGraphAddNode(&wn, g, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const long long c0 = launch_counter();
+  CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  try {
+    for (int k = 0; k < chunk; k++) emit_iteration(true);
+    loop_cond_kernel<<<1, 32, 0, s>>>(hw, stp, nrhs, ctl.as<int>());
+    CPSGPU_CUDA(cudaGetLastError());
+    launch_counter()++;
+  } catch (...) {
+    cudaGraph_t junk;
+    cudaStreamEndCapture(s, &junk);
+    launch_counter() = c0;
+    throw;
+  }
+  cudaGraph_t captured;
+  CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
+  const long long kernels = launch_counter() - c0;
+  launch_counter() = c0;
+  return kernels;
+}
+
+// the WHILE loop's counters: no body run yet, at most the bound of max_num_iter
+void CgSolver::set_loop_limit() {
+  const int chunk = args.chunk > 0 ? args.chunk : 8;
+  const long max_chunks = (long)args.max_num_iter / chunk + 4;
+  const int hctl[2] = {0, (int)std::min<long>(max_chunks, 1L << 30)};
+  ctl.ensure(2 * sizeof(int));
+  CPSGPU_CUDA(cudaMemcpyAsync(ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, D.lat->stream));
+}
+
+int CgSolver::loop_bodies_run() {
+  int bodies_run = 0;
+  CPSGPU_CUDA(cudaMemcpyAsync(&bodies_run, ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, D.lat->stream));
+  CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));
+  return bodies_run;
+}
+
+void CgSolver::end(std::vector<CgResult> &res, long long replayed) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  SolverScalars *stp = st.as<SolverScalars>();
+  // final solution and true residual in FP64 (inv_cg.C:403-415)
+  if (sloppy != PREC_DOUBLE) launch_accum_reliable(s, x64.view(), px_of(sloppy), xs.view(), stp, nrhs, 1);
+  ensure_field(rtmp, PREC_DOUBLE, L.vh, D.ls, nrhs);
+  std::vector<SolverScalars> host(nrhs);
+  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  std::vector<SolverScalars> fin = host;
+  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_STORE, GATE_NONE, rtmp.view(), PREC_DOUBLE, none(),
+             PREC_DOUBLE);
+  CPSGPU_CUDA(cudaEventRecord(tev1, s));
+  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  float dev_ms = 0.f;
+  CPSGPU_CUDA(cudaEventElapsedTime(&dev_ms, tev0, tev1));
+  int bodies = 0;  // reliable-update bodies that ran (one per iteration in which any solve had one)
+  for (int k = 0; k < nrhs; k++) bodies = std::max(bodies, fin[k].n_reliable);
+  const long long kernels = launch_counter() - k0 + replayed + (graph_exec || replayed ? (long long)bodies * body_kernels : 0);
+  res.resize(nrhs);
+  for (int k = 0; k < nrhs; k++) {
+    CgResult &o = res[k];
+    o.iterations = fin[k].iter + 1;
+    o.status = fin[k].done ? fin[k].done : ST_MAX_ITER;
+    o.true_res = std::sqrt(host[k].sum[0] / fin[k].src_norm);
+    o.reliable_updates = fin[k].n_reliable;
+    o.seconds = dev_ms * 1e-3;
+    o.final_rr = fin[k].rr;
+    o.kernels = kernels;
+  }
+}
+
+void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  SolverScalars *stp = st.as<SolverScalars>();
+  begin(a);
   const int chunk = a.chunk > 0 ? a.chunk : 8;
   const long max_chunks = (long)a.max_num_iter / chunk + 4;
   if (graph_exec && graph_chunk != chunk) drop_graph();
   long long replayed = 0;
   if (a.use_graph) {
-    // the whole loop as one graph: a WHILE node whose body is one chunk
-    // followed by the condition kernel; no host polling, and the loop stops
-    // after the chunk in which the last solve finished
     if (!graph_exec) {
-      ctl.ensure(2 * sizeof(int));
       CPSGPU_CUDA(cudaGraphCreate(&graph, 0));
-      cudaGraphConditionalHandle hw;
-      CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
-      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-      cp.conditional.handle = hw;
-      cp.conditional.type = cudaGraphCondTypeWhile;
-      cp.conditional.size = 1;
-      cudaGraphNode_t wn;
-      CPSGPU_CUDA(cudaGraphAddNode(&wn, graph, nullptr, 0, &cp));
-      cudaGraph_t body = cp.conditional.phGraph_out[0];
-      const long long c0 = launch_counter();
-      CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
       try {
-        for (int k = 0; k < chunk; k++) emit_iteration(true);
-        loop_cond_kernel<<<1, 32, 0, s>>>(hw, stp, nrhs, ctl.as<int>());
-        CPSGPU_CUDA(cudaGetLastError());
-        launch_counter()++;
+        graph_kernels = add_loop(graph, chunk);
       } catch (...) {
-        cudaGraph_t junk;
-        cudaStreamEndCapture(s, &junk);
         drop_graph();
         throw;
       }
-      cudaGraph_t captured;
-      CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
       CPSGPU_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
-      graph_kernels = launch_counter() - c0;
-      launch_counter() = c0;
       graph_chunk = chunk;
     }
-    const int hctl[2] = {0, (int)std::min<long>(max_chunks, 1L << 30)};
-    CPSGPU_CUDA(cudaMemcpyAsync(ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
+    set_loop_limit();
     CPSGPU_CUDA(cudaGraphLaunch(graph_exec, s));
-    int bodies_run = 0;
-    CPSGPU_CUDA(cudaMemcpyAsync(&bodies_run, ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CPSGPU_CUDA(cudaStreamSynchronize(s));
-    replayed = (long long)bodies_run * graph_kernels;
+    replayed = (long long)loop_bodies_run() * graph_kernels;
   } else {
     int *flags = reinterpret_cast<int *>(L.pinned);  // [2][nrhs] ring
     if (nrhs * 2 > 64 * 2) throw Error(-1, "too many right-hand sides for the poll buffer");
@@ -347,35 +418,88 @@ void CgSolver::run(const CgArgs &a, std::vector<CgResult> &res) {
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
   }
+  end(res, replayed);
+}
 
-  // final solution and true residual in FP64 (inv_cg.C:403-415)
-  if (sloppy != PREC_DOUBLE) launch_accum_reliable(s, x64.view(), px_of(sloppy), xs.view(), stp, nrhs, 1);
-  ensure_field(rtmp, PREC_DOUBLE, L.vh, D.ls, nrhs);
-  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
-  CPSGPU_CUDA(cudaStreamSynchronize(s));
-  std::vector<SolverScalars> fin = host;
-  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_STORE, GATE_NONE, rtmp.view(), PREC_DOUBLE, none(),
-             PREC_DOUBLE);
-  CPSGPU_CUDA(cudaEventRecord(tev1, s));
-  CPSGPU_CUDA(cudaMemcpyAsync(host.data(), stp, sizeof(SolverScalars) * nrhs, cudaMemcpyDeviceToHost, s));
-  CPSGPU_CUDA(cudaStreamSynchronize(s));
-  float dev_ms = 0.f;
-  CPSGPU_CUDA(cudaEventElapsedTime(&dev_ms, tev0, tev1));
-  cudaEventDestroy(tev0);
-  cudaEventDestroy(tev1);
-  int bodies = 0;  // reliable-update bodies that ran (one per iteration in which any solve had one)
-  for (int k = 0; k < nrhs; k++) bodies = std::max(bodies, fin[k].n_reliable);
-  const long long kernels = launch_counter() - k0 + replayed + (graph_exec ? (long long)bodies * body_kernels : 0);
-  res.resize(nrhs);
-  for (int k = 0; k < nrhs; k++) {
-    CgResult &o = res[k];
-    o.iterations = fin[k].iter + 1;
-    o.status = fin[k].done ? fin[k].done : ST_MAX_ITER;
-    o.true_res = std::sqrt(host[k].sum[0] / fin[k].src_norm);
-    o.reliable_updates = fin[k].n_reliable;
-    o.seconds = dev_ms * 1e-3;
-    o.final_rr = fin[k].rr;
-    o.kernels = kernels;
+// Several independent solves (their own operators, lattices, precisions and
+// arguments) as ONE graph launch: every solver's iteration loop is a root
+// WHILE node of the graph, so the loops run concurrently on the GPU (the
+// small systems in the shadow of the large ones) and finish independently.
+namespace {
+// The instantiated graph of the last batch: rebuilt when the batch's solvers,
+// their set-ups (ids) or their chunk lengths change.
+struct BatchGraph {
+  std::vector<CgSolver *> solvers;
+  std::vector<unsigned long long> ids;
+  std::vector<int> chunks;
+  std::vector<long long> kernels;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  void drop() {
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    ge = nullptr;
+    g = nullptr;
+    solvers.clear();
+  }
+};
+BatchGraph g_batch;
+}  // namespace
+
+void solve_batch(std::vector<CgSolver *> &solvers, const std::vector<CgArgs> &a,
+                 std::vector<std::vector<CgResult>> &res) {
+  const size_t n = solvers.size();
+  std::vector<int> chunks(n);
+  std::vector<unsigned long long> ids(n);
+  for (size_t k = 0; k < n; k++) {
+    chunks[k] = a[k].chunk > 0 ? a[k].chunk : 8;
+    ids[k] = solvers[k]->id;
+  }
+  for (size_t k = 0; k < n; k++) solvers[k]->begin(a[k]);
+  const bool cached = g_batch.ge && g_batch.solvers == solvers && g_batch.ids == ids && g_batch.chunks == chunks;
+  if (!cached) {
+    g_batch.drop();
+    try {
+      CPSGPU_CUDA(cudaGraphCreate(&g_batch.g, 0));
+      g_batch.kernels.assign(n, 0);
+      for (size_t k = 0; k < n; k++) g_batch.kernels[k] = solvers[k]->add_loop(g_batch.g, chunks[k]);
+      CPSGPU_CUDA(cudaGraphInstantiate(&g_batch.ge, g_batch.g, 0));
+    } catch (...) {
+      g_batch.drop();
+      throw;
+    }
+    g_batch.solvers = solvers;
+    g_batch.ids = ids;
+    g_batch.chunks = chunks;
+  }
+  for (size_t k = 0; k < n; k++) solvers[k]->set_loop_limit();
+  // every loop's set-up is ordered before the launch on the first solver's stream
+  cudaStream_t s0 = solvers[0]->D.lat->stream;
+  std::vector<cudaEvent_t> ready(n, nullptr);
+  cudaEvent_t done = nullptr;
+  try {
+    for (size_t k = 0; k < n; k++) {
+      CPSGPU_CUDA(cudaEventCreateWithFlags(&ready[k], cudaEventDisableTiming));
+      CPSGPU_CUDA(cudaEventRecord(ready[k], solvers[k]->D.lat->stream));
+      CPSGPU_CUDA(cudaStreamWaitEvent(s0, ready[k], 0));
+    }
+    CPSGPU_CUDA(cudaGraphLaunch(g_batch.ge, s0));
+    CPSGPU_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CPSGPU_CUDA(cudaEventRecord(done, s0));
+    for (size_t k = 0; k < n; k++) CPSGPU_CUDA(cudaStreamWaitEvent(solvers[k]->D.lat->stream, done, 0));
+    CPSGPU_CUDA(cudaStreamSynchronize(s0));
+  } catch (...) {
+    for (auto e : ready)
+      if (e) cudaEventDestroy(e);
+    if (done) cudaEventDestroy(done);
+    throw;
+  }
+  for (auto e : ready) cudaEventDestroy(e);
+  cudaEventDestroy(done);
+  res.resize(n);
+  for (size_t k = 0; k < n; k++) {
+    const long long replayed = (long long)solvers[k]->loop_bodies_run() * g_batch.kernels[k];
+    solvers[k]->end(res[k], replayed);
   }
 }
 

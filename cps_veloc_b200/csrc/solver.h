@@ -14,6 +14,9 @@ struct CgArgs {
   double delta = 0.1;        // reliable-update threshold (mixed precision)
   int chunk = 8;             // iterations per captured graph
   int use_graph = 1;
+  // per right-hand side, when given (one entry per right-hand side): the
+  // shift and the stopping residual of each system of a batched solve
+  std::vector<double> shifts, stop_rsds;
 };
 
 struct CgResult {
@@ -46,16 +49,36 @@ struct CgSolver {
   int graph_chunk = 0;
   cudaStream_t side = nullptr;  // captures the conditional bodies
   DeviceBuffer ctl;              // the WHILE loop's body count and limit
+  DeviceBuffer partials;         // this solver's reduction partials (solves may share a lattice)
+  unsigned long long id = 0;     // new at every setup(): a graph holding this solver's buffers is current while it matches
+  // state of one run between begin() and end()
+  CgArgs args;
+  long long k0 = 0;
+  cudaEvent_t tev0 = nullptr, tev1 = nullptr;
 
   CgSolver(Dirac &d, int sloppy_prec) : D(d), sloppy(sloppy_prec) {}
   ~CgSolver();
   void setup(int nrhs);
   void run(const CgArgs &a, std::vector<CgResult> &res);
+  // run() in three steps, so that several solvers' loops can share one graph:
+  // begin() sets up the scalars and the initial residual (it synchronises);
+  // add_loop() adds the iteration loop as a WHILE node (a root) to graph g
+  // and returns the kernels of one body; end() finishes after the loop ran.
+  void begin(const CgArgs &a);
+  long long add_loop(cudaGraph_t g, int chunk);
+  void set_loop_limit();
+  void end(std::vector<CgResult> &res, long long replayed);
+  int loop_bodies_run();
   void drop_graph();
   void emit_iteration(bool conditional = false);
   void emit_reliable_update();
   void emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_ep, int pap, int red_op, int gate,
                   const SpinorView &rv, int pr, const SpinorView &solv, int px);
 };
+
+// Independent solves in one graph launch (solver.cu); each solver set up for
+// its right-hand sides, with b64 / x64 filled.  res[k] per solver.
+void solve_batch(std::vector<CgSolver *> &solvers, const std::vector<CgArgs> &a,
+                 std::vector<std::vector<CgResult>> &res);
 
 }  // namespace cpsgpu

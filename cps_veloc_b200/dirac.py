@@ -602,6 +602,11 @@ class DiracOpMobius(_DiracOp):
                  a5_inv: float = 1.0):
         super().__init__(lat, mass, ls=ls, m5=m5, b=b, c=c, a5_inv=a5_inv)
 
+    def set_mix_impl(self, tensor_cores: bool) -> None:
+        """the standalone Ls x Ls mixings of FP16 fields on the tensor cores
+        (True) or the CUDA cores (False, the default)"""
+        check(lib().cpsgpu_set_mix_impl(self._h, 1 if tensor_cores else 0))
+
     def MatPcDagMatPcShift(self, inp, mu: float, prec: int = A.DOUBLE):
         """DiracOpMobius::MatPcDagMatPcShift (eigen_shift mu): returns
         (M^+ M in - 2 mu R g5 M in + mu^2 in, |M in|^2)"""
@@ -633,3 +638,38 @@ class DiracOpMobius(_DiracOp):
         out = np.empty_like(inp)
         check(lib().cpsgpu_mobius_m5inv(self._h, dptr(out), dptr(inp), dag, prec))
         return out
+
+
+def solve_batch(items, stop_rsd=1e-8, max_num_iter=10000, precision=A.DOUBLE, delta=0.0, chunk=8):
+    """Independent InvCg solves of different operators in one graph launch
+    (cpsgpu_solve_batch).  items: (DiracOp, sol, src) with host vectors, sol
+    the initial guess, updated in place.  Returns one CgResult per item; the
+    device time of each is the whole batch's."""
+    fields, ops, sols, srcs, args = [], [], [], [], []
+    for D, sol, src in items:
+        src = D._vec(src)
+        if not (isinstance(sol, np.ndarray) and sol.dtype == np.float64 and sol.flags.c_contiguous):
+            raise TypeError("sol must be a C-contiguous float64 array (updated in place)")
+        D._vec(sol)
+        fs, fb = C.c_void_p(), C.c_void_p()
+        check(lib().cpsgpu_field_create(D._h, A.DOUBLE, 1, C.byref(fs)))
+        check(lib().cpsgpu_field_create(D._h, A.DOUBLE, 1, C.byref(fb)))
+        fields += [fs, fb]
+        check(lib().cpsgpu_field_upload(fs, dptr(sol)))
+        check(lib().cpsgpu_field_upload(fb, dptr(src)))
+        ops.append(D._h)
+        sols.append(fs)
+        srcs.append(fb)
+        args.append(D._cg_arg(stop_rsd, max_num_iter, 0.0, 0.0, precision, delta, chunk, True))
+    n = len(items)
+    try:
+        res = (A.CgResult * n)()
+        VP = C.c_void_p * n
+        check(lib().cpsgpu_solve_batch(n, VP(*[o.value for o in ops]), VP(*[f.value for f in sols]),
+                                       VP(*[f.value for f in srcs]), (A.CgArg * n)(*args), res))
+        for (D, sol, _), fs in zip(items, sols):
+            check(lib().cpsgpu_field_download(fs, dptr(sol)))
+        return [CgResult(r.iterations, r.status, r.true_res, r.reliable_updates, r.seconds, r.kernels) for r in res]
+    finally:
+        for f in fields:
+            lib().cpsgpu_field_destroy(f)

@@ -204,6 +204,13 @@ int cpsgpu_matpc_dag_matpc_shift(cpsgpu_dirac d, double *out, const double *in, 
  * out-of-place zmobius_m5inv (zmobius_m5inv.C:822). */
 int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);
 int cpsgpu_mobius_m5inv(cpsgpu_dirac d, double *out, const double *in, int dag, int prec);
+/* No counterpart in the reference: where the Mobius operator applies a
+ * standalone Ls x Ls mixing (M5^-1, the first step of MatPc) to an FP16
+ * field, tensor_cores = 1 runs it as mma.sync m16n8k16 contractions (FP16
+ * operands with the matrix split into high and low parts, FP32
+ * accumulation, mix_tc.cu) instead of FP32 FMAs on the CUDA cores (0, the
+ * default).  Real b, c and Ls <= 16; other cases keep the CUDA cores. */
+int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores);
 
 /* ---- solvers ---- */
 typedef struct {
@@ -509,6 +516,18 @@ int cpsgpu_field_dot(cpsgpu_field a, cpsgpu_field b, double *re, double *im);
  * solution out); arg->precision selects plain or mixed CG */
 int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,
                        cpsgpu_cg_result *res);
+/* n independent DiracOp::InvCg solves (InvCgShift, inv_cg.C:84-448) of
+ * different operators (their own lattices, masses, kinds) as ONE CUDA graph
+ * launch: every solve's iteration loop is a root branch of the graph, so the
+ * systems run concurrently on the GPU and each stops at its own convergence.
+ * The reference runs such solves one after another (FdwfBase::FmatEvlInv per
+ * mass, f_dwf_base.C:189-275).  sol[k] (initial guesses in, solutions out)
+ * and src[k] are FP64 device fields of ops[k]; args[k] its CgArg and
+ * precision (mixed precision as cpsgpu_invcg).  An operator may appear once
+ * per precision (several right-hand sides of one operator go in one field).
+ * res holds one result per right-hand side, solve after solve. */
+int cpsgpu_solve_batch(int n, const cpsgpu_dirac *ops, const cpsgpu_field *sol, const cpsgpu_field *src,
+                       const cpsgpu_cg_arg *args, cpsgpu_cg_result *res);
 
 /* ---- tuning ---- */
 /* Time candidate block shapes of every hop kernel the operator uses, at
