@@ -25,9 +25,10 @@ gives its time to 1e-10.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-For N > 1 (under torchrun) every rank solves its own copy of the system on
-its own GPU (one solve does not shard without a halo exchange); the reported
-time is the maximum over ranks.
+For N > 1 (under torchrun) every rank solves its own system (the same
+lattice and operator, its own wall source) on its own GPU: N independent
+solves, weak scaling (one solve does not shard without a halo exchange);
+the reported time is the maximum over ranks.
 """
 from __future__ import annotations
 
@@ -159,7 +160,9 @@ def wall_source(L, ls, eta4d):
     return src.reshape(-1)
 
 
-def setup_system(device: int):
+def setup_system(device: int, rank: int = 0):
+    """the benchmarked system; under torchrun rank r solves its own wall
+    source (stream 1 + r): N independent solves, one per GPU"""
     from cps_veloc_b200 import _abi as A
     from cps_veloc_b200.dirac import DiracOpDwf, Lattice, gen_gauge, gen_gaussian
 
@@ -169,7 +172,7 @@ def setup_system(device: int):
     lat.import_gauge(u)
     D = DiracOpDwf(lat, mass=MF, ls=LS, m5=M5)
     vol = int(np.prod(L4))
-    eta = gen_gaussian(vol * 24, seed=SEED, stream=1).reshape(2, vol // 2, 24)
+    eta = gen_gaussian(vol * 24, seed=SEED, stream=1 + rank).reshape(2, vol // 2, 24)
     b = D.MatPcDag(wall_source(L4, LS, eta))
     return A, lat, D, u, b
 
@@ -544,7 +547,7 @@ def main(argv=None) -> int:
 
     ws, rank, local = dist_env()
     dist = init_dist(ws)
-    A, lat, D, u, b = setup_system(local)
+    A, lat, D, u, b = setup_system(local, rank)
     sloppy = A.HALF if args.sloppy == "half" else A.SINGLE
     n = D.f_size
     zero = np.zeros(n)
@@ -642,7 +645,7 @@ def main(argv=None) -> int:
             "vs_baseline": None, "dtype": "f64+f16" if sloppy == A.HALF else "f64+f32", "data": "synthetic",
             "config": workload_config(),
             "inner": "fp16 storage + per-site norm, fp32 arithmetic" if sloppy == A.HALF else "fp32",
-            "parallelism": f"{ws} independent replicas" if ws > 1 else "1 GPU",
+            "parallelism": f"{ws} independent solves, one per GPU" if ws > 1 else "1 GPU",
             "fp64_cg": {"time_s": t_fp64, "iterations": fp64[0].iterations, "true_res": fp64[0].true_res},
             "mixed_cg": {"time_s": t_mixed, "iterations": res[0].iterations,
                          "reliable_updates": res[0].reliable_updates, "true_res": res[0].true_res,

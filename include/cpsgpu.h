@@ -5,9 +5,9 @@
  * and implements, as hand-written sm_100a kernels, the even-odd
  * preconditioned Wilson, Shamir domain-wall and Mobius operators and the CG
  * and multishift-CG solvers that CPS's DiracOp classes run on the CPU.
- * A CPS build calls these entry points from a thin C++ shim (see
- * INTEGRATION.md); every function replaces the reference interface cited in
- * its comment (paths relative to the reference's cps_pp tree).
+ * A CPS build calls these entry points from a thin C++ shim that overrides
+ * the DiracOp methods; every function replaces the reference interface cited
+ * in its comment (paths relative to the reference's cps_pp tree).
  *
  * Conventions shared with the reference:
  *   - vectors are host arrays of doubles in CPS storage order:

@@ -21,6 +21,7 @@ ORACLE_SO = OUT / "liboracle.so"
 REF_SO = OUT / "libcpsref.so"
 # the reference's cps_pp source directory, from the environment only
 REF_SRC = Path(os.environ["CPS_REF"]) if os.environ.get("CPS_REF") else None
+REF_GPU_SO = OUT / "libcpsref_gpu.so"
 REF_SOLVE_SO = OUT / "libcpsref_solve.so"
 
 _dp = C.POINTER(C.c_double)
@@ -87,6 +88,16 @@ def build_reference_solvers() -> Path:
             raise FileNotFoundError("reference solvers not prebuilt and CPS_REF does not name the reference's cps_pp")
         _make("refsolve")
     return REF_SOLVE_SO
+
+
+def build_reference_gpu() -> Path:
+    """the reference's solvers with the library's CPS-side shim in place of
+    DiracOp::InvCgShift (libcpsref_gpu.so; needs libcpsgpu.so built)"""
+    if _ref_tree():
+        _make("refgpu")  # relinks when libcpsgpu.so or the shim changed
+    elif not REF_GPU_SO.exists():
+        raise FileNotFoundError("reference + shim not prebuilt and CPS_REF does not name the reference's cps_pp")
+    return REF_GPU_SO
 
 
 def reference_available() -> bool:

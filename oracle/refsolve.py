@@ -6,7 +6,7 @@ static gauge field, lattice_base.C:56, 320-325).
     python -m oracle.refsolve SPEC.json OUT.npz
 
 SPEC keys: L (4 ints), ls, kind ("wilson" | "dwf" | "mobius"), m5, a5_inv,
-b, c, bc_t, task, and per task:
+b, c, bc_t, backend, task, and per task:
 
 * ``fwilsoninv``: the steps of the reference's tests/f_wilson_inv/main.C on
   its own disordered start and RandGaussVector source (mass, stop_rsd,
@@ -22,6 +22,12 @@ b, c, bc_t, task, and per task:
 * ``cgtime``: wall time of DiracOp::InvCgShift capped at each max_iter of
   ``caps`` (zero initial guess each time, after ``warmup`` untimed capped
   runs), on the source MatPcDag(src) (gauge, src, mass, stop_rsd).
+
+``backend`` "gpu" loads oracle/_ref/libcpsref_gpu.so (``make -C oracle
+refgpu``) instead: the same reference code with DiracOp::InvCgShift replaced
+by the library's CPS-side shim (cps_veloc_b200/shim/dirac_op_gpu.C), so every
+solve above runs the reference's own drivers (MatInv, InvCg) around the GPU
+CG.  CPSGPU_INNER in the environment selects its precision.
 
 OUT holds the iteration count, true residual, solution(s), the inputs and
 ``res_hist``, the |r|^2 of every iteration as the reference prints it
@@ -42,20 +48,21 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SOLVE_SO = HERE / "_ref" / "libcpsref_solve.so"
+GPU_SO = HERE / "_ref" / "libcpsref_gpu.so"
 KINDS = {"wilson": 0, "dwf": 1, "mobius": 2}
 _dp = C.POINTER(C.c_double)
 
 
-def available() -> bool:
-    return SOLVE_SO.exists()
+def available(backend: str = "cpu") -> bool:
+    return (GPU_SO if backend == "gpu" else SOLVE_SO).exists()
 
 
 def _p(a):
     return a.ctypes.data_as(_dp)
 
 
-def _lib():
-    L = C.CDLL(str(SOLVE_SO))
+def _lib(backend: str = "cpu"):
+    L = C.CDLL(str(GPU_SO if backend == "gpu" else SOLVE_SO))
     L.rs_init.argtypes = [C.c_int] * 6 + [C.c_double] * 4 + [C.c_int] * 3
     L.rs_vol.restype = C.c_long
     L.rs_rand_gauss.argtypes = [_dp, C.c_double]
@@ -99,7 +106,7 @@ def _hist(text: str) -> np.ndarray:
 
 
 def run(spec: dict) -> dict:
-    L = _lib()
+    L = _lib(spec.get("backend", "cpu"))
     lx, ly, lz, lt = spec["L"]
     kind = KINDS[spec.get("kind", "wilson")]
     ls = int(spec.get("ls", 0))
@@ -189,13 +196,14 @@ def run(spec: dict) -> dict:
     return out
 
 
-def run_child(spec: dict, timeout: float = 600) -> dict:
-    """run() in a fresh process (one reference geometry per process)"""
+def run_child(spec: dict, timeout: float = 600, env: dict | None = None) -> dict:
+    """run() in a fresh process (one reference geometry per process); env:
+    extra environment variables of the child"""
     with tempfile.TemporaryDirectory() as d:
         sp, op = Path(d) / "spec.json", Path(d) / "out.npz"
         sp.write_text(json.dumps(spec))
         # the reference writes its error logs (phys.error.*) into the working directory
-        env = dict(os.environ)
+        env = dict(os.environ) | (env or {})
         env["PYTHONPATH"] = str(HERE.parent) + os.pathsep + env.get("PYTHONPATH", "")
         r = subprocess.run([sys.executable, "-m", "oracle.refsolve", str(sp), str(op)], cwd=d, env=env,
                            capture_output=True, text=True, timeout=timeout)
