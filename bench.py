@@ -391,31 +391,35 @@ def extra_multishift(A) -> dict:
             t0 = time.perf_counter()
             k = D.MInvCG(psi, chi, float(chi @ chi), shifts, rs, precision=prec)
             t = time.perf_counter() - t0
+        phases = D.minvcg_stats()
         y, _ = D.MatPcDagMatPc(psi[0])
         worst = float(np.linalg.norm(chi - y - shifts[0] * psi[0]) / np.linalg.norm(chi))
-        out[name] = {"wall_s": t, "iterations": k, "true_res_smallest_shift": worst}
+        out[name] = {"wall_s": t, "iterations": k, "true_res_smallest_shift": worst, "phases": phases}
     D.close()
     lat.close()
     return out
 
 
-def extra_solve_batch(A) -> dict:
-    """Eight independent DWF solves, Ls = 16, M5 = 1.8, m_f log-spaced in
-    [0.001, 0.1], lattices 8^3x16 ... 16^3x32, mixed precision (FP32 inner)
-    to a true residual of 1e-10: one cpsgpu_solve_batch call (every solve's
-    loop a branch of one graph launch) against the same eight solves one
-    after another (cpsgpu_invcg_field); wall time of the device-field calls
-    after one untimed round each."""
+BATCH_MIXED = [(8, 8, 8, 16), (8, 8, 8, 32), (12, 12, 12, 16), (12, 12, 12, 24), (16, 16, 16, 16),
+               (16, 16, 16, 24), (16, 16, 16, 32), (16, 16, 16, 32)]
+BATCH_SMALL = [(8, 8, 8, 8)] * 4 + [(8, 8, 8, 16)] * 4
+
+
+def extra_solve_batch(A, lattices=BATCH_MIXED, ls=LS) -> dict:
+    """Eight independent DWF solves, M5 = 1.8, m_f log-spaced in [0.001,
+    0.1], on the given lattices (default 8^3x16 ... 16^3x32, Ls 16), mixed
+    precision (FP32 inner) to a true residual of 1e-10: one cpsgpu_solve_batch
+    call (every solve's loop a branch of one graph launch) against the same
+    eight solves one after another (cpsgpu_invcg_field); wall time of the
+    device-field calls after one untimed round each."""
     from cps_veloc_b200.dirac import DiracOpDwf, Lattice, gen_gauge, gen_gaussian
 
-    lattices = [(8, 8, 8, 16), (8, 8, 8, 32), (12, 12, 12, 16), (12, 12, 12, 24), (16, 16, 16, 16),
-                (16, 16, 16, 24), (16, 16, 16, 32), (16, 16, 16, 32)]
     masses = list(np.logspace(-3, -1, 8))
     lats, ops, sols, srcs, zeros = [], [], [], [], []
     for k, (L, m) in enumerate(zip(lattices, masses)):
         lat = Lattice(L, (1, 1, 1, -1))
         lat.import_gauge(gen_gauge(L, seed=SEED + 20 + k, width=0.3))
-        D = DiracOpDwf(lat, mass=m, ls=LS, m5=M5)
+        D = DiracOpDwf(lat, mass=m, ls=ls, m5=M5)
         D.autotune(A.SINGLE)
         lats.append(lat)
         ops.append(D)
@@ -461,7 +465,7 @@ def extra_solve_batch(A) -> dict:
     for D, lat in zip(ops, lats):
         D.close()
         lat.close()
-    return {"lattices": [list(L) for L in lattices], "ls": LS, "mf": masses, "inner": "fp32",
+    return {"lattices": [list(L) for L in lattices], "ls": ls, "mf": masses, "inner": "fp32",
             "batch_one_launch_s": tb, "sequential_s": ts, "speedup_batch_vs_sequential": ts / tb,
             "iterations": [r.iterations for r in rb], "iterations_sequential": [r.iterations for r in rs],
             "all_converged_1e-10": all(r.status == A.CONVERGED and r.true_res <= STOP for r in rb)}
@@ -635,6 +639,7 @@ def main(argv=None) -> int:
                   "mobius_24x64_ls12": extra_mobius(A),
                   "multishift_wilson_32x64": extra_multishift(A),
                   "batch_8_dwf_solves": extra_solve_batch(A),
+                  "batch_8_small_dwf_solves": extra_solve_batch(A, BATCH_SMALL, 8),
                   "hmc_force_dwf_16x32_ls16": extra_force(A, D, pk)}
 
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))

@@ -74,6 +74,11 @@ class CgArg(C.Structure):
                 ("use_graph", C.c_int)]
 
 
+class MInvCgStats(C.Structure):
+    _fields_ = [("upload_s", C.c_double), ("recurrence_s", C.c_double), ("refine_s", C.c_double),
+                ("download_s", C.c_double), ("refine_iterations_max", C.c_int), ("refine_iterations_sum", C.c_int)]
+
+
 class CgResult(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("true_res", C.c_double),
                 ("reliable_updates", C.c_int), ("seconds", C.c_double), ("kernels", C.c_longlong)]
@@ -157,6 +162,7 @@ def lib() -> C.CDLL:
                                              C.POINTER(CgResult)]),
             "cpsgpu_minvcg": (C.c_int, [vp, C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
                                         C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_get_minvcg_stats": (C.c_int, [vp, C.POINTER(MInvCgStats)]),
             "cpsgpu_field_create": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(vp)]),
             "cpsgpu_field_destroy": (C.c_int, [vp]),
             "cpsgpu_field_upload": (C.c_int, [vp, _dp]),
@@ -174,6 +180,8 @@ def lib() -> C.CDLL:
             "cpsgpu_solve_batch": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(CgArg),
                                              C.POINTER(CgResult)]),
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_get_hop_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "cpsgpu_set_hop_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_mdagm": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_m5inv": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),

@@ -11,6 +11,7 @@
 #include "../../include/cpsgpu.h"
 #include "cpsgpu_impl.h"
 #include "hop.cuh"
+#include "tune.h"
 #include "solver.h"
 
 namespace cpsgpu {
@@ -1139,6 +1140,20 @@ int cpsgpu_minvcg(cpsgpu_dirac d, double *const *psi, const double *chi, double 
   });
 }
 
+int cpsgpu_get_minvcg_stats(cpsgpu_dirac d, cpsgpu_minvcg_stats *stats) {
+  return guarded([&] {
+    if (!d || !stats) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    const MsWork &m = d->D->ms;
+    stats->upload_s = m.upload_s;
+    stats->recurrence_s = m.recurrence_s;
+    stats->refine_s = m.refine_s;
+    stats->download_s = m.download_s;
+    stats->refine_iterations_max = m.refine_max;
+    stats->refine_iterations_sum = m.refine_sum;
+    return CPSGPU_OK;
+  });
+}
+
 // ---- device fields
 int cpsgpu_field_create(cpsgpu_dirac d, int precision, int nrhs, cpsgpu_field *f) {
   return guarded([&] {
@@ -1396,6 +1411,36 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
     if (!d || tile < 0) throw Error(CPSGPU_ERR_ARG, "bad argument");
     check_prec(prec);
     d->D->rtile[prec] = tile;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread) {
+  return guarded([&] {
+    if (!d || !sites || !slices || !slices_per_thread) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    check_prec(prec);
+    const Dirac &D = *d->D;
+    const dim3 b = hop_block(TuneKey{prec, D.lat->recon(prec), EP_STORE, D.kind, D.ls}, false);
+    *sites = (int)b.x;
+    *slices = (int)b.y;
+    *slices_per_thread = (b.z == 2 && D.kind == KIND_DWF && prec != PREC_DOUBLE && D.ls % (4 * (int)b.y) == 0) ? 2 : 1;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread) {
+  return guarded([&] {
+    if (!d || sites < 1 || slices < 1 || sites * slices > 256 || sites * slices % 32 != 0 ||
+        (slices_per_thread != 1 && slices_per_thread != 2))
+      throw Error(CPSGPU_ERR_ARG, "hop shape: sites x slices a multiple of 32 up to 256, 1 or 2 slices per thread");
+    check_prec(prec);
+    const Dirac &D = *d->D;
+    if (slices > std::max(D.ls, 1)) throw Error(CPSGPU_ERR_ARG, "hop shape: more slices per block than Ls");
+    if (slices_per_thread == 2 && (D.kind != KIND_DWF || prec == PREC_DOUBLE || D.ls % (4 * slices) != 0))
+      throw Error(CPSGPU_ERR_ARG, "slice pairs: DWF, FP32 or FP16 fields, Ls a multiple of 4 x slices");
+    const dim3 b((unsigned)sites, (unsigned)slices, (unsigned)slices_per_thread);
+    const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
+    for (int ep : eps) tune_set(TuneKey{prec, D.lat->recon(prec), ep, D.kind, D.ls}, b);
     return CPSGPU_OK;
   });
 }

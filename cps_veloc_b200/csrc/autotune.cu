@@ -1,6 +1,6 @@
 // Autotuner: times candidate block shapes of the hop kernels on the live
 // lattice and records the fastest in the launch table (tune.cpp).  A shape
-// is (sites per block) x (slices per block); the mixing epilogue of the
+// is (sites per block) x (slices per block) x (slices per thread, DWF); the mixing epilogue of the
 // Mobius operator needs all slices of a site in one block, so only its
 // site count varies.
 #include <vector>
@@ -59,7 +59,11 @@ int autotune(Dirac &D, int prec, int nrhs) {
     const int bss[] = {1, 2, 4, 8, 16};
     for (int bx : bxs)
       for (int bs : bss)
-        if (bx * bs <= 256 && bx * bs >= 64 && bs <= (D.ls > 1 ? D.ls : 1)) cand.push_back(dim3(bx, bs));
+        if (bx * bs <= 256 && bx * bs >= 64 && bs <= (D.ls > 1 ? D.ls : 1)) {
+          cand.push_back(dim3(bx, bs));
+          // DWF slice pairs: two same-parity slices per thread sharing links
+          if (D.kind == KIND_DWF && prec != PREC_DOUBLE && D.ls % (4 * bs) == 0) cand.push_back(dim3(bx, bs, 2));
+        }
     TuneKey key{prec, recon, EP_STORE, D.kind, D.ls};
     float best = 1e30f;
     dim3 bestb = hop_block(key, false);

@@ -117,6 +117,9 @@ struct MsWork {
   std::vector<Field> p, psi;
   DeviceBuffer st, ms, pv, psiv;
   OpWork w;
+  // the last call's phases: wall seconds and refinement iterations
+  double upload_s = 0, recurrence_s = 0, refine_s = 0, download_s = 0;
+  int refine_max = 0, refine_sum = 0;
 };
 
 struct Dirac {

@@ -13,9 +13,15 @@ namespace {
 using HopFn = void (*)(const HopParams, const HopViews, SolverScalars *, double *);
 
 bool g_dag = false;  // set by launch_hop before pick()
+int g_ns = 1;        // slices per thread (2: DWF slice pairs)
 
 template <int P, int RECON, int EP, int PR, int PX>
 HopFn get() {
+  // FP32 arithmetic only: the FP64 pair kernel spills kilobytes
+  if constexpr (!ep_mix(EP) && P != PREC_DOUBLE) {
+    if (g_ns == 2)
+      return g_dag ? hop_kernel<P, RECON, EP, PR, PX, true, false, 2> : hop_kernel<P, RECON, EP, PR, PX, false, false, 2>;
+  }
   return g_dag ? hop_kernel<P, RECON, EP, PR, PX, true> : hop_kernel<P, RECON, EP, PR, PX, false>;
 }
 
@@ -126,13 +132,16 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   v.hb = L.halo_bwd;
 
   const int recon = lat.recon(L.prec);
-  g_dag = (L.dag != 0);
-  HopFn fn = halo ? pick_halo(L.prec, recon) : pick(L.prec, recon, L.ep, L.pr, L.px);
   const bool mix = ep_mix(L.ep);
   TuneKey key{L.prec, recon, L.ep, D.kind, D.ls};
   dim3 block = hop_block(key, mix);
+  // block.z of a tuned shape: slices per thread (2: DWF slice pairs)
+  g_ns = (block.z == 2 && hp.dwf && !mix && !halo && L.prec != PREC_DOUBLE && D.ls % (4 * (int)block.y) == 0) ? 2 : 1;
+  block.z = 1;
+  g_dag = (L.dag != 0);
+  HopFn fn = halo ? pick_halo(L.prec, recon) : pick(L.prec, recon, L.ep, L.pr, L.px);
   const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
-  hp.nsg = (D.ls + block.y - 1) / block.y;
+  hp.nsg = g_ns == 2 ? D.ls / (2 * (int)block.y) : (D.ls + block.y - 1) / block.y;
   hp.spar = (hp.dwf && !mix && block.y > 1 && D.ls % (2 * block.y) == 0) ? 1 : 0;
   hp.nrhs = in.nrhs;
   hp.rtile = std::max(1, std::min(D.rhs_tile(L.prec, in.nrhs), in.nrhs));

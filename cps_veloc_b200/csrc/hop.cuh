@@ -198,6 +198,65 @@ __device__ __forceinline__ void hop_site(const HopParams &hp, const HopViews &v,
   A.store(acc);
 }
 
+// hop_site for two slices of the same 4D parity at once (DWF): each link is
+// loaded (and, for 12 reals, rebuilt) once and applied to both slices, and
+// the neighbour indices and boundary signs are computed once.  No halos.
+template <int P, int RECON, bool DAG>
+__device__ __forceinline__ void hop_site2(const HopParams &hp, const HopViews &v, int i, long sl0, long sl1,
+                                          int pout, typename PrecTraits<P>::real *acc0,
+                                          typename PrecTraits<P>::real *acc1) {
+  using R = typename PrecTraits<P>::real;
+  const int pin = 1 - pout;
+  const int hx = hp.hx, Ly = hp.L[1], Lz = hp.L[2];
+  const int q1 = hp.dhx.div(i);
+  const int xh = i - q1 * hx;
+  const int q2 = hp.dly.div(q1);
+  const int y = q1 - q2 * Ly;
+  const int t = hp.dlz.div(q2);
+  const int z = q2 - t * Lz;
+  const int x = 2 * xh + ((y + z + t + pout) & 1);
+  const int c[4] = {x, y, z, t};
+  const int stride[4] = {0, hx, hx * Ly, hx * Ly * Lz};
+  const Slice<P> in0(v.in, sl0), in1(v.in, sl1);
+  constexpr R sdag = DAG ? R(-1) : R(1);
+  HopAcc<R> A0, A1;
+  A0.zero();
+  A1.zero();
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    {
+      const bool wrap = (c[mu] == hp.L[mu] - 1);
+      int j;
+      if (mu == 0) j = i - xh + ((wrap ? 0 : x + 1) >> 1);
+      else j = wrap ? i - (hp.L[mu] - 1) * stride[mu] : i + stride[mu];
+      const R sgn = (wrap && hp.bc[mu] < 0) ? R(-1) : R(1);
+      R psi0[24], psi1[24], sc0, sc1;
+      in0.load_raw(j, psi0, sc0);
+      in1.load_raw(j, psi1, sc1);
+      su3<R> u;
+      LinkIO<P, RECON>::load(v.U, pout, mu, i, u);
+      A0.hop(u, project(psi0, mu, -sdag), false, mu, -sdag, sgn * sc0);
+      A1.hop(u, project(psi1, mu, -sdag), false, mu, -sdag, sgn * sc1);
+    }
+    {
+      const bool wrap = (c[mu] == 0);
+      int j;
+      if (mu == 0) j = i - xh + ((wrap ? hp.L[0] - 1 : x - 1) >> 1);
+      else j = wrap ? i + (hp.L[mu] - 1) * stride[mu] : i - stride[mu];
+      const R sgn = (wrap && hp.bc[mu] < 0) ? R(-1) : R(1);
+      R psi0[24], psi1[24], sc0, sc1;
+      in0.load_raw(j, psi0, sc0);
+      in1.load_raw(j, psi1, sc1);
+      su3<R> u;
+      LinkIO<P, RECON>::load(v.U, pin, mu, j, u);
+      A0.hop(u, project(psi0, mu, sdag), true, mu, sdag, sgn * sc0);
+      A1.hop(u, project(psi1, mu, sdag), true, mu, sdag, sgn * sc1);
+    }
+  }
+  A0.store(acc0);
+  A1.store(acc1);
+}
+
 // Fifth-direction hop of the Shamir DWF operator, accumulated into acc.
 template <int P, bool DAG>
 __device__ __forceinline__ void hop5_dwf(const HopParams &hp, const HopViews &v, int i, int s, long rhs,
@@ -232,20 +291,146 @@ __device__ __forceinline__ double norm2_24(const R *a) {
   return s;
 }
 
-// PR: precision of r and p (CG/RES epilogues); PX: precision of sol.
+// The non-mixing epilogues of one output (slice sl = rhs * Ls + s, site i),
+// acc = the hop.  Reductions are added to red: AXPY |out|^2, |x|^2; CG |r|^2;
+// RES |r|^2.  PR: precision of r and p (CG/RES); PX: precision of sol.
+template <int P, int EP, int PR, int PX>
+__device__ __forceinline__ void hop_epilogue(const HopParams &hp, const HopViews &v, const SolverScalars *st,
+                                             long rhs, long sl, int s, int i, bool active,
+                                             typename PrecTraits<P>::real *acc, double *red) {
+  using R = typename PrecTraits<P>::real;
+  if constexpr (EP == EP_STORE || EP == EP_MIX) {
+    if (active) SpinorIO<P>::store(v.out, sl, i, acc);
+  } else if constexpr (ep_axpy(EP)) {
+    // out = x + c hop, streamed 4 reals at a time (few live registers).
+    // A thread sums its own 24 squares in the arithmetic precision (FP32 for
+    // the sloppy operators: no FP64 conversions per value); everything from
+    // the per-thread partial sums on is FP64.
+    using RA = typename std::conditional<P == PREC_DOUBLE, double, float>::type;
+    RA n_out = RA(0), n_x = RA(0);
+    if (active) {
+      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        R xv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (hp.norm) n_x += xv[k] * xv[k];
+          acc[4 * c + k] = xv[k] + cf * acc[4 * c + k];
+          if (hp.norm) n_out += acc[4 * c + k] * acc[4 * c + k];
+        }
+        if constexpr (P != PREC_HALF) Chunk4<P>::store(v.out, sl, i, c, acc + 4 * c);
+      }
+      if constexpr (P == PREC_HALF) SpinorIO<P>::store(v.out, sl, i, acc);
+    }
+    red[0] += double(n_out);
+    red[1] += double(n_x);
+  } else if constexpr (ep_cg(EP)) {
+    // q = x + c hop + shift p;  r -= alpha q;  sol += alpha p;  |r|^2
+    using RR = typename PrecTraits<PR>::real;
+    using RX = typename PrecTraits<PX>::real;
+    RR n_r = RR(0);  // this thread's |r|^2 in r's arithmetic precision
+    if (active) {
+      const double alpha = st[rhs].alpha;
+      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
+      const R sh = R(st[rhs].shift);
+      const RR a = RR(alpha);
+      const RX ax = RX(alpha);
+      const bool with_sol = (v.sol.data != nullptr);  // the multishift solver keeps its own solutions
+      RR rfull[PR == PREC_HALF ? 24 : 1];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        R xv[4];
+        RR pv[4], rv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+        Chunk4<PR>::load(v.p, sl, i, c, pv);
+        Chunk4<PR>::load(v.r, sl, i, c, rv);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          R q = xv[k] + cf * acc[4 * c + k] + sh * R(pv[k]);
+          rv[k] = rv[k] - a * RR(q);
+          n_r += rv[k] * rv[k];
+        }
+        if constexpr (PR == PREC_HALF) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
+        } else {
+          Chunk4<PR>::store(v.r, sl, i, c, rv);
+        }
+        if (with_sol) {
+          RX sv[4];
+          Chunk4<PX>::load(v.sol, sl, i, c, sv);
+#pragma unroll
+          for (int k = 0; k < 4; k++) sv[k] = sv[k] + ax * RX(pv[k]);
+          if constexpr (PX != PREC_HALF) Chunk4<PX>::store(v.sol, sl, i, c, sv);
+        }
+      }
+      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
+    }
+    red[0] += double(n_r);
+  } else if constexpr (ep_res(EP)) {
+    // r = b - (x + c hop + shift sol), stored in r's precision;  |r|^2
+    using RR = typename PrecTraits<PR>::real;
+    if (active) {
+      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
+      const R sh = R(st[rhs].shift);
+      RR rfull[PR == PREC_HALF ? 24 : 1];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        R xv[4], bv[4], sv[4];
+        Chunk4<P>::load(v.x, sl, i, c, xv);
+        Chunk4<P>::load(v.b, sl, i, c, bv);
+        Chunk4<P>::load(v.sol, sl, i, c, sv);
+        RR rv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          R q = bv[k] - (xv[k] + cf * acc[4 * c + k] + sh * sv[k]);
+          red[0] += double(q) * double(q);
+          rv[k] = RR(q);
+        }
+        if constexpr (PR == PREC_HALF) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
+        } else {
+          Chunk4<PR>::store(v.r, sl, i, c, rv);
+        }
+      }
+      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
+    }
+  }
+}
+
+// reductions of an epilogue: AXPY with norms 2, CG and RES 1, else none
+template <int EP> __host__ __device__ constexpr int ep_nred() {
+  return ep_axpy(EP) ? 2 : (ep_cg(EP) || ep_res(EP)) ? 1 : 0;
+}
+
 // Minimum resident 256-thread blocks per SM the register allocator must
-// allow (2 = at most 128 registers per thread).
+// allow (2 = at most 128 registers per thread, 3 = at most 85).
 #ifndef CPSGPU_HOP_MINB_DOUBLE
 #define CPSGPU_HOP_MINB_DOUBLE 2
 #endif
 #ifndef CPSGPU_HOP_MINB_SLOPPY
 #define CPSGPU_HOP_MINB_SLOPPY 3
 #endif
+#ifndef CPSGPU_HOP_MINB_PAIR
+#define CPSGPU_HOP_MINB_PAIR 2
+#endif
 
-template <int P, int RECON, int EP, int PR, int PX, bool DAG, bool HALO = false>
-__global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE : CPSGPU_HOP_MINB_SLOPPY) hop_kernel(const HopParams hp, const HopViews v, SolverScalars *st,
-                                                     double *partials) {
+template <int P, int NS> __host__ __device__ constexpr int hop_min_blocks() {
+  return P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE : NS == 2 ? CPSGPU_HOP_MINB_PAIR : CPSGPU_HOP_MINB_SLOPPY;
+}
+
+// NS = 2 (DWF, no mixing, no halos): every thread computes two slices of the
+// same 4D parity, s and s + 2, sharing their links (hop_site2); slice group g
+// of a block with BS threads in y covers the parity-(g % 2) slices of the run
+// [(g / 2) 4 BS, (g / 2 + 1) 4 BS), and Ls is a multiple of 4 BS.
+template <int P, int RECON, int EP, int PR, int PX, bool DAG, bool HALO = false, int NS = 1>
+__global__ void __launch_bounds__(256, (hop_min_blocks<P, NS>())) hop_kernel(const HopParams hp, const HopViews v,
+                                                                           SolverScalars *st, double *partials) {
   using R = typename PrecTraits<P>::real;
+  static_assert(NS == 1 || (!HALO && !ep_mix(EP)), "slice pairs: DWF hops without halos or mixing");
   // blockIdx.x = (site block, slice group, rhs within the tile), rhs fastest:
   // consecutive blocks read the same links (for rtile solves) and the same
   // fifth-direction neighbourhoods, which are then still in L1 / L2
@@ -258,17 +443,35 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
 
   const int sgrp = sb % hp.nsg, sblk = sb / hp.nsg;
   const int i = sblk * blockDim.x + threadIdx.x;
-  const int s = hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y
-                        : sgrp * (int)blockDim.y + (int)threadIdx.y;
-  const bool active = (i < hp.vh) && (s < hp.ls);
+  const int s = NS == 2 ? (sgrp >> 1) * 4 * (int)blockDim.y + (sgrp & 1) + 4 * (int)threadIdx.y
+                : hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y
+                          : sgrp * (int)blockDim.y + (int)threadIdx.y;
+  const bool active = (i < hp.vh) && (s + 2 * (NS - 1) < hp.ls);
   const long sl = rhs * hp.ls + s;
   const int pin = hp.dwf ? ((s + hp.cb) & 1) : hp.cb;
   const int pout = 1 - pin;
+  constexpr int NV = ep_nred<EP>();
 
   R acc[24];
-  if (active) {
-    hop_site<P, RECON, DAG, HALO>(hp, v, i, sl, pout, acc);
-    if (hp.dwf) hop5_dwf<P, DAG>(hp, v, i, s, rhs, acc);
+  if constexpr (NS == 2) {
+    R acc1[24];
+    if (active) {
+      hop_site2<P, RECON, DAG>(hp, v, i, sl, sl + 2, pout, acc, acc1);
+      hop5_dwf<P, DAG>(hp, v, i, s, rhs, acc);
+      hop5_dwf<P, DAG>(hp, v, i, s + 2, rhs, acc1);
+    }
+    double red[NV > 0 ? NV : 1] = {};
+    hop_epilogue<P, EP, PR, PX>(hp, v, st, rhs, sl, s, i, active, acc, red);
+    hop_epilogue<P, EP, PR, PX>(hp, v, st, rhs, sl + 2, s + 2, i, active, acc1, red);
+    if constexpr (NV > 0) {
+      if (!ep_axpy(EP) || hp.norm) block_partial<NV>(reinterpret_cast<double(&)[NV]>(red), partials, (unsigned)rhs, (unsigned)sb, nblk);
+    }
+    return;
+  } else {
+    if (active) {
+      hop_site<P, RECON, DAG, HALO>(hp, v, i, sl, pout, acc);
+      if (hp.dwf) hop5_dwf<P, DAG>(hp, v, i, s, rhs, acc);
+    }
   }
 
   if constexpr (ep_mix(EP)) {
@@ -321,108 +524,10 @@ __global__ void __launch_bounds__(256, P == PREC_DOUBLE ? CPSGPU_HOP_MINB_DOUBLE
     }
   }
 
-  if constexpr (EP == EP_STORE || EP == EP_MIX) {
-    if (active) SpinorIO<P>::store(v.out, sl, i, acc);
-  } else if constexpr (ep_axpy(EP)) {
-    // out = x + c hop, streamed 4 reals at a time (few live registers).
-    // A thread sums its own 24 squares in the arithmetic precision (FP32 for
-    // the sloppy operators: no FP64 conversions per value); everything from
-    // the per-thread partial sums on is FP64.
-    using RA = typename std::conditional<P == PREC_DOUBLE, double, float>::type;
-    RA n_out = RA(0), n_x = RA(0);
-    if (active) {
-      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        R xv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          if (hp.norm) n_x += xv[k] * xv[k];
-          acc[4 * c + k] = xv[k] + cf * acc[4 * c + k];
-          if (hp.norm) n_out += acc[4 * c + k] * acc[4 * c + k];
-        }
-        if constexpr (P != PREC_HALF) Chunk4<P>::store(v.out, sl, i, c, acc + 4 * c);
-      }
-      if constexpr (P == PREC_HALF) SpinorIO<P>::store(v.out, sl, i, acc);
-    }
-    double red[2] = {double(n_out), double(n_x)};
-    if (hp.norm) block_partial<2>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
-  } else if constexpr (ep_cg(EP)) {
-    // q = x + c hop + shift p;  r -= alpha q;  sol += alpha p;  |r|^2
-    using RR = typename PrecTraits<PR>::real;
-    using RX = typename PrecTraits<PX>::real;
-    RR n_r = RR(0);  // this thread's |r|^2 in r's arithmetic precision
-    if (active) {
-      const double alpha = st[rhs].alpha;
-      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
-      const R sh = R(st[rhs].shift);
-      const RR a = RR(alpha);
-      const RX ax = RX(alpha);
-      const bool with_sol = (v.sol.data != nullptr);  // the multishift solver keeps its own solutions
-      RR rfull[PR == PREC_HALF ? 24 : 1];
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        R xv[4];
-        RR pv[4], rv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
-        Chunk4<PR>::load(v.p, sl, i, c, pv);
-        Chunk4<PR>::load(v.r, sl, i, c, rv);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          R q = xv[k] + cf * acc[4 * c + k] + sh * R(pv[k]);
-          rv[k] = rv[k] - a * RR(q);
-          n_r += rv[k] * rv[k];
-        }
-        if constexpr (PR == PREC_HALF) {
-#pragma unroll
-          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
-        } else {
-          Chunk4<PR>::store(v.r, sl, i, c, rv);
-        }
-        if (with_sol) {
-          RX sv[4];
-          Chunk4<PX>::load(v.sol, sl, i, c, sv);
-#pragma unroll
-          for (int k = 0; k < 4; k++) sv[k] = sv[k] + ax * RX(pv[k]);
-          if constexpr (PX != PREC_HALF) Chunk4<PX>::store(v.sol, sl, i, c, sv);
-        }
-      }
-      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
-    }
-    double red[1] = {double(n_r)};
-    block_partial<1>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
-  } else if constexpr (ep_res(EP)) {
-    // r = b - (x + c hop + shift sol), stored in r's precision;  |r|^2
-    using RR = typename PrecTraits<PR>::real;
-    double red[1] = {0.0};
-    if (active) {
-      const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
-      const R sh = R(st[rhs].shift);
-      RR rfull[PR == PREC_HALF ? 24 : 1];
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        R xv[4], bv[4], sv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
-        Chunk4<P>::load(v.b, sl, i, c, bv);
-        Chunk4<P>::load(v.sol, sl, i, c, sv);
-        RR rv[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          R q = bv[k] - (xv[k] + cf * acc[4 * c + k] + sh * sv[k]);
-          red[0] += double(q) * double(q);
-          rv[k] = RR(q);
-        }
-        if constexpr (PR == PREC_HALF) {
-#pragma unroll
-          for (int k = 0; k < 4; k++) rfull[4 * c + k] = rv[k];
-        } else {
-          Chunk4<PR>::store(v.r, sl, i, c, rv);
-        }
-      }
-      if constexpr (PR == PREC_HALF) SpinorIO<PR>::store(v.r, sl, i, rfull);
-    }
-    block_partial<1>(red, partials, (unsigned)rhs, (unsigned)sb, nblk);
+  double red[NV > 0 ? NV : 1] = {};
+  hop_epilogue<P, EP, PR, PX>(hp, v, st, rhs, sl, s, i, active, acc, red);
+  if constexpr (NV > 0) {
+    if (!ep_axpy(EP) || hp.norm) block_partial<NV>(reinterpret_cast<double(&)[NV]>(red), partials, (unsigned)rhs, (unsigned)sb, nblk);
   }
 }
 

@@ -8,11 +8,15 @@
 // per site summing over the shifts when only the weighted sum is kept).  The
 // scalars never leave the device.
 //
-// precision CPSGPU_SINGLE runs the recurrences on FP32 vectors (solutions
-// accumulated in FP64) and then refines every shift with the
-// reliable-update CG on MatPcDagMatPc + shift_s to its own residual.
+// precision CPSGPU_SINGLE runs the recurrences on FP32 vectors, the
+// solutions included (the per-shift update then moves half the bytes of the
+// FP64 one), and then refines every shift with the reliable-update CG on
+// MatPcDagMatPc + shift_s, from its FP32 solution, to its own residual.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "../../include/cpsgpu.h"
@@ -79,7 +83,7 @@ __global__ void ms_update_kernel(SpinorView r, const SpinorView *pv, const Spino
 // per shift (types MULTI and GENERAL): blockIdx.x = site block x nshift +
 // shift, so the blocks of one site block are consecutive and r is read from
 // L2 by all but the first shift.
-template <int P>
+template <int P, int PS>
 __global__ void __launch_bounds__(128) ms_update_shift_kernel(SpinorView r, const SpinorView *pv,
                                                               const SpinorView *psiv, SpinorView chi,
                                                               const MsScalars *ms, const SolverScalars *st,
@@ -97,13 +101,15 @@ __global__ void __launch_bounds__(128) ms_update_shift_kernel(SpinorView r, cons
   RealT<P> pp[24];
   SpinorIO<P>::load(pv[s], sl, i, pp);
   if (upd) {
+    // solutions in PS (FP64, or FP32 in the sloppy phase), updated in FP64
     const double f = -ms->bs[s] * ms->weight[s];
-    double y[24], c[24];
-    SpinorIO<PREC_DOUBLE>::load(psiv[s], sl, i, y);
+    RealT<PS> y[24];
+    double c[24];
+    SpinorIO<PS>::load(psiv[s], sl, i, y);
     if (use_chi) SpinorIO<PREC_DOUBLE>::load(chi, sl, i, c);
 #pragma unroll
-    for (int k = 0; k < 24; k++) y[k] += f * (use_chi ? c[k] : double(pp[k]));
-    SpinorIO<PREC_DOUBLE>::store(psiv[s], sl, i, y);
+    for (int k = 0; k < 24; k++) y[k] = RealT<PS>(double(y[k]) + f * (use_chi ? c[k] : double(pp[k])));
+    SpinorIO<PS>::store(psiv[s], sl, i, y);
   }
   if (adv) {
     RealT<P> rv[24];
@@ -125,6 +131,9 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   if (nshift > MS_MAX) throw Error(-1, "at most 64 shifts");
   Lattice &L = *D.lat;
   cudaStream_t s = L.stream;
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+  const clk::time_point t_start = clk::now();
   const int P = (precision == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
   if (P != PREC_DOUBLE && L.recon_err > 1e-5) throw Error(-1, "sloppy multishift needs SU(3) links");
   const long vh = L.vh;
@@ -144,7 +153,8 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   if (mw.psi.size() < (size_t)npsi) mw.psi.resize(npsi);
   std::vector<Field> &p = mw.p, &psi = mw.psi;
   for (int k = 0; k < nshift; k++) ensure_field(p[k], P, vh, ls, 1);
-  for (int k = 0; k < npsi; k++) ensure_field(psi[k], PREC_DOUBLE, vh, ls, 1);
+  const int PS = P;  // precision of the solutions during the recurrences
+  for (int k = 0; k < npsi; k++) ensure_field(psi[k], PS, vh, ls, 1);
   OpWork &w = mw.w;
   ensure_field(w.t1, P, vh, ls, 1);
   ensure_field(w.t2, P, vh, ls, 1);
@@ -155,11 +165,19 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   L.staging.ensure(nreal * sizeof(double));
   CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, chi_h, nreal * sizeof(double), cudaMemcpyHostToDevice, s));
   launch_import_fermion(s, PREC_DOUBLE, chi64.view(), L.staging.as<double>());
+  Field psi0_64;  // GENERAL: the FP64 guess of shift 0 for the initial residual
   if (dev_type == 2) {
     // GENERAL accumulates into the given solutions (only MULTI zeroes them)
     for (int k = 0; k < npsi; k++) {
       CPSGPU_CUDA(cudaMemcpyAsync(L.staging.ptr, psi_h[k], nreal * sizeof(double), cudaMemcpyHostToDevice, s));
-      launch_import_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      if (PS == PREC_DOUBLE) {
+        launch_import_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      } else {
+        Field &g = (k == 0) ? psi0_64 : tmp64;
+        if (k == 0) g.create(PREC_DOUBLE, vh, ls, 1);
+        launch_import_fermion(s, PREC_DOUBLE, g.view(), L.staging.as<double>());
+        launch_convert(s, PS, psi[k].view(), PREC_DOUBLE, g.view());
+      }
     }
   } else {
     for (int k = 0; k < npsi; k++) launch_zero(s, psi[k]);
@@ -190,8 +208,8 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     z0.shift = 0.0;
     SolverScalars *tst = tmp.st.as<SolverScalars>();
     CPSGPU_CUDA(cudaMemcpyAsync(tst, &z0, sizeof(z0), cudaMemcpyHostToDevice, s));
-    tmp.emit_mdagm(PREC_DOUBLE, psi[0].view(), tmp.wd, EP_RES, 0, RED_STORE, GATE_NONE, tmp64.view(), PREC_DOUBLE,
-                   SpinorView(), PREC_DOUBLE);
+    tmp.emit_mdagm(PREC_DOUBLE, PS == PREC_DOUBLE ? psi[0].view() : psi0_64.view(), tmp.wd, EP_RES, 0, RED_STORE,
+                   GATE_NONE, tmp64.view(), PREC_DOUBLE, SpinorView(), PREC_DOUBLE);
     SolverScalars h;
     CPSGPU_CUDA(cudaMemcpyAsync(&h, tst, sizeof(h), cudaMemcpyDeviceToHost, s));
     CPSGPU_CUDA(cudaStreamSynchronize(s));
@@ -283,23 +301,24 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     if (dev_type != 0) {
       const unsigned g = (unsigned)((per + 127) / 128) * (unsigned)nshift;
       if (P == PREC_DOUBLE)
-        ms_update_shift_kernel<PREC_DOUBLE><<<g, 128, 0, s>>>(r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(),
-                                                              chi64.view(), msd, st, use_chi);
+        ms_update_shift_kernel<PREC_DOUBLE, PREC_DOUBLE><<<g, 128, 0, s>>>(
+            r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
       else
-        ms_update_shift_kernel<PREC_SINGLE><<<g, 128, 0, s>>>(r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(),
-                                                              chi64.view(), msd, st, use_chi);
+        ms_update_shift_kernel<PREC_SINGLE, PREC_SINGLE><<<g, 128, 0, s>>>(
+            r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
     } else if (P == PREC_DOUBLE) {
       ms_update_kernel<PREC_DOUBLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
           r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
     } else {
-      ms_update_kernel<PREC_SINGLE><<<(unsigned)((per + 255) / 256), 256, 0, s>>>(
-          r.view(), pvd.as<SpinorView>(), psivd.as<SpinorView>(), chi64.view(), msd, st, use_chi);
+      throw Error(-2, "multishift: one summed solution only at FP64");
     }
     CPSGPU_CUDA(cudaGetLastError());
     ms_mark_kernel<<<1, 1, 0, s>>>(msd);
     CPSGPU_CUDA(cudaGetLastError());
   };
 
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  const clk::time_point t_rec = clk::now();
   iteration(1);  // the initial step of minvcg.C:140-188 (psi update from chi)
   MsScalars mh;
   SolverScalars sh;
@@ -320,18 +339,36 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
       rsdcg[k] = std::sqrt(mh.c * mh.z[mh.iz][k] * mh.z[mh.iz][k]);
   }
   const int iters = mh.k + 1;
+  const clk::time_point t_ref = clk::now();
+  mw.refine_max = mw.refine_sum = 0;
+
+  // FP64 view of solution k: the refined solution, else psi_k (converted
+  // into tmp64 when it is FP32; used before the next call)
+  std::unique_ptr<CgSolver> cg;
+  const size_t one = (size_t)chi64.data.bytes;
+  auto x64_of = [&](int k) {
+    SpinorView v = cg->x64.view();
+    v.data = (char *)v.data + k * one;
+    v.nrhs = 1;
+    return v;
+  };
+  auto solution = [&](int k) -> SpinorView {
+    if (cg) return x64_of(k);
+    if (PS == PREC_DOUBLE) return psi[k].view();
+    launch_convert(s, PREC_DOUBLE, tmp64.view(), PS, psi[k].view());
+    return tmp64.view();
+  };
 
   if (P != PREC_DOUBLE && refine) {
     // FP64 refinement of every shift with the reliable-update CG, all shifts
     // as one batched solve (right-hand side k: MatPcDagMatPc + shift_k from
     // the sloppy solution psi_k, to its own residual), so the links are read
     // once per tile of shifts and the iterations share their launches
-    CgSolver cg(D, PREC_SINGLE);
-    cg.setup(nshift);
-    const size_t one = (size_t)chi64.data.bytes;
+    cg.reset(new CgSolver(D, PREC_SINGLE));
+    cg->setup(nshift);
     for (int k = 0; k < nshift; k++) {
-      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg.b64.data.ptr + k * one, chi64.data.ptr, one, cudaMemcpyDeviceToDevice, s));
-      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg.x64.data.ptr + k * one, psi[k].data.ptr, one, cudaMemcpyDeviceToDevice, s));
+      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg->b64.data.ptr + k * one, chi64.data.ptr, one, cudaMemcpyDeviceToDevice, s));
+      launch_convert(s, PREC_DOUBLE, x64_of(k), PS, psi[k].view());
     }
     CgArgs a;
     a.max_num_iter = max_num_iter;
@@ -342,12 +379,15 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
       a.stop_rsds.push_back(ms0.rsd_sq[k] > 0 ? std::sqrt(ms0.rsd_sq[k] / cp) : 1e-10);
     }
     std::vector<CgResult> res;
-    cg.run(a, res);
+    cg->run(a, res);
     for (int k = 0; k < nshift; k++) {
-      CPSGPU_CUDA(cudaMemcpyAsync(psi[k].data.ptr, (char *)cg.x64.data.ptr + k * one, one, cudaMemcpyDeviceToDevice, s));
-      rsdcg[k] = res[k].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327 reports
+      rsdcg[k] = res[k].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327
+      mw.refine_max = std::max(mw.refine_max, res[k].iterations);
+      mw.refine_sum += res[k].iterations;
     }
   }
+  CPSGPU_CUDA(cudaStreamSynchronize(s));
+  const clk::time_point t_out = clk::now();
 
   // outputs
   if (type == 0 && dev_type != 0) {
@@ -356,7 +396,7 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     CPSGPU_CUDA(cudaStreamSynchronize(s));
     for (size_t q = 0; q < nreal; q++) acc[q] = psi_h[0][q];
     for (int k = 0; k < nshift; k++) {
-      launch_export_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      launch_export_fermion(s, PREC_DOUBLE, solution(k), L.staging.as<double>());
       CPSGPU_CUDA(cudaMemcpyAsync(tmp.data(), L.staging.ptr, nreal * sizeof(double), cudaMemcpyDeviceToHost, s));
       CPSGPU_CUDA(cudaStreamSynchronize(s));
       for (size_t q = 0; q < nreal; q++) acc[q] += alpha[k] * tmp[q];
@@ -364,11 +404,15 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     for (size_t q = 0; q < nreal; q++) psi_h[0][q] = acc[q];
   } else {
     for (int k = 0; k < npsi; k++) {
-      launch_export_fermion(s, PREC_DOUBLE, psi[k].view(), L.staging.as<double>());
+      launch_export_fermion(s, PREC_DOUBLE, solution(k), L.staging.as<double>());
       CPSGPU_CUDA(cudaMemcpyAsync(psi_h[k], L.staging.ptr, nreal * sizeof(double), cudaMemcpyDeviceToHost, s));
     }
     CPSGPU_CUDA(cudaStreamSynchronize(s));
   }
+  mw.upload_s = secs(t_start, t_rec);
+  mw.recurrence_s = secs(t_rec, t_ref);
+  mw.refine_s = secs(t_ref, t_out);
+  mw.download_s = secs(t_out, clk::now());
   return iters;
 }
 

@@ -140,6 +140,7 @@ void hop(const Dirac &D, int ep, int cb, int dag, int norm, const SpinorView &in
   v.x = x;
   const int recon = lat.recon(PREC_DOUBLE);
   dim3 block = hop_block(TuneKey{PREC_DOUBLE, recon, ep, D.kind, D.ls}, false);
+  block.z = 1;  // one slice per thread here (a tuned z of 2 selects launch_hop's slice pairs)
   const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
   hp.nsg = (D.ls + block.y - 1) / block.y;
   hp.rtile = 1;

@@ -1,6 +1,8 @@
 // Launch-shape table for the hop kernels.  Defaults come from the block
-// shapes below; the autotuner (tune.cu, exposed as cpsgpu_autotune) times
-// candidate shapes on the live lattice and records the fastest per key.
+// shapes below; the autotuner (autotune.cu, exposed as cpsgpu_autotune)
+// times candidate shapes on the live lattice and records the fastest per
+// key.  A shape is (sites per block, slices per block, slices per thread):
+// z = 2 selects the DWF slice-pair kernel where Ls allows it.
 #pragma once
 #include <cuda_runtime.h>
 

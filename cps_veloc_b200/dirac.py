@@ -555,6 +555,13 @@ class _DiracOp:
                                   max_num_iter, precision, 1 if refine else 0, C.byref(k)))
         return k.value
 
+    def minvcg_stats(self) -> dict:
+        """phases of the last MInvCG: upload, recurrence, refine, download
+        wall seconds and the refinement's iterations (max, sum)"""
+        st = A.MInvCgStats()
+        check(lib().cpsgpu_get_minvcg_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in A.MInvCgStats._fields_}
+
     def autotune(self, prec=A.DOUBLE, nrhs=1) -> int:
         t = C.c_int()
         check(lib().cpsgpu_autotune(self._h, prec, nrhs, C.byref(t)))
@@ -568,6 +575,15 @@ class _DiracOp:
 
     def set_rhs_tile(self, prec: int, tile: int) -> None:
         check(lib().cpsgpu_set_rhs_tile(self._h, prec, tile))
+
+    def hop_shape(self, prec=A.DOUBLE) -> tuple:
+        """(sites, slices, slices per thread) of the non-mixing hop launches"""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().cpsgpu_get_hop_shape(self._h, prec, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def set_hop_shape(self, prec: int, sites: int, slices: int, slices_per_thread: int = 1) -> None:
+        check(lib().cpsgpu_set_hop_shape(self._h, prec, sites, slices, slices_per_thread))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -31,6 +31,8 @@ def main(argv=None) -> int:
     ap.add_argument("--force", action="store_true", help="time the HMC fermion force instead")
     ap.add_argument("--link-reals", type=int, default=0,
                     help="link form of the FP32/FP16 operators (12, 18, 112, 118; 0: default or autotuned)")
+    ap.add_argument("--shape", default="",
+                    help="sites,slices,slices_per_thread of the hop launches (overrides the autotuner)")
     ap.add_argument("--dd", type=int, default=0,
                     help="time the t-slab decomposed dslash over this many slabs (one process; see time_dd)")
     args = ap.parse_args(argv)
@@ -56,9 +58,11 @@ def main(argv=None) -> int:
             D.autotune(prec)
         if args.link_reals and prec != A.DOUBLE:
             lat.set_link_reals(prec, args.link_reals)
+        if args.shape:
+            D.set_hop_shape(prec, *(int(x) for x in args.shape.split(",")))
         ms, by = C.c_double(), C.c_double()
         A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, args.reps, C.byref(ms), C.byref(by)))
-        line = f"prec {prec}: dslash {ms.value:.4f} ms {by.value / ms.value / 1e6:.0f} GB/s ({by.value:.0f} B)"
+        line = f"prec {prec} shape {D.hop_shape(prec)}: dslash {ms.value:.4f} ms {by.value / ms.value / 1e6:.0f} GB/s ({by.value:.0f} B)"
         if not args.no_mdagm:
             m2, b2 = C.c_double(), C.c_double()
             A.check(A.lib().cpsgpu_time_mdagm(D._h, prec, max(1, args.reps // 4), C.byref(m2), C.byref(b2)))

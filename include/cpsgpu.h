@@ -474,6 +474,16 @@ int cpsgpu_matinv_lowmode(cpsgpu_dirac d, double *out, const double *in, const c
 int cpsgpu_minvcg(cpsgpu_dirac d, double *const *psi, const double *chi, double chi_norm, const double *shift,
                   int nshift, double *rsdcg, int type, const double *alpha, int max_num_iter, int precision,
                   int refine, int *iterations);
+/* Where the operator's last cpsgpu_minvcg spent its time (no counterpart in
+ * the reference): host wall seconds of the source / guess upload, the
+ * shifted recurrences, the FP64 refinement and the solutions' download
+ * (each phase ends with a stream synchronisation), and the refinement's
+ * iterations (largest over the shifts, and their sum). */
+typedef struct {
+  double upload_s, recurrence_s, refine_s, download_s;
+  int refine_iterations_max, refine_iterations_sum;
+} cpsgpu_minvcg_stats;
+int cpsgpu_get_minvcg_stats(cpsgpu_dirac d, cpsgpu_minvcg_stats *stats);
 
 /* ---- device-resident fields ---- */
 int cpsgpu_field_create(cpsgpu_dirac d, int precision, int nrhs, cpsgpu_field *f);
@@ -540,6 +550,14 @@ int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned);
  * sides uses; set overrides the autotuner (0 restores the default). */
 int cpsgpu_get_rhs_tile(cpsgpu_dirac d, int prec, int nrhs, int *tile);
 int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile);
+/* Launch shape of the operator's non-mixing hop kernels at precision prec
+ * and its current link form (no counterpart in the reference): `sites`
+ * consecutive checkerboard sites x `slices` slices per block, and
+ * `slices_per_thread` 1 or 2 (2: DWF at FP32 arithmetic, Ls a multiple of
+ * 4 * slices — each thread computes two same-parity slices with shared
+ * links).  get returns the shape in use; set overrides the autotuner. */
+int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread);
+int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread);
 
 /* ---- measurement ----
  * Time `reps` back-to-back launches of the operator's hop kernel
