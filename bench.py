@@ -65,10 +65,10 @@ STOP = 1e-10
 FP64_CG_ITERS = 196
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the dslash timed below on this workload, from single-launch ncu captures
-# (hop_kernel store epilogue, cold L2), keyed by (precision, stored link form).
-# The algorithmic bytes are 226.5 MB (FP32, 12-real links), 239.0 MB (FP32,
-# 18), 127.9 MB (FP16, 18).
-DSLASH_TRAFFIC = {(1, 12): 132.54e6 + 76.52e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.54e6}
+# (hop_kernel store epilogue, cold L2; profiles/hop_dwf_*_16x32_ls16.md),
+# keyed by (precision, stored link form).  The algorithmic bytes are 226.5 MB
+# (FP32, 12-real links), 239.0 MB (FP32, 18), 127.9 MB (FP16, 18).
+DSLASH_TRAFFIC = {(1, 12): 132.47e6 + 72.48e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.47e6}
 
 
 WORKLOAD = "DWF 16^3x32 Ls=16 M5=1.8 mf=0.01 CG on MatPcDagMatPc to true residual 1e-10"
@@ -665,6 +665,7 @@ def main(argv=None) -> int:
                          "algorithmic_bytes": by.value, "traffic_unit": "bytes per launch (ncu, single launch)",
                          "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32")
                          + f", {form}-real links",
+                         "launch_shape_sites_slices_per_block_slices_per_thread": list(D.hop_shape(sloppy)),
                          "peak_source": pk["source"]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},

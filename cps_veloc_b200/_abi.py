@@ -158,6 +158,10 @@ def lib() -> C.CDLL:
             "cpsgpu_gconvert": (C.c_int, [_ip, _dp, C.c_int, C.c_int]),
             "cpsgpu_four2five": (C.c_int, [_ip, C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_five2four": (C.c_int, [_ip, C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_fconvert_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int]),
+            "cpsgpu_gconvert_device": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+            "cpsgpu_four2five_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_five2four_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_invcg_multi": (C.c_int, [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(CgArg),
                                              C.POINTER(CgResult)]),
             "cpsgpu_minvcg": (C.c_int, [vp, C.POINTER(_dp), _dp, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,

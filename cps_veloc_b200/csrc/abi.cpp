@@ -42,6 +42,10 @@ void nersc_write(const char *path, const int node_sites[4], const double *u, int
 void gconvert(const int node_sites[4], double *u, int to, int from);
 void four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
 void five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb);
+void fconvert_device(const Lattice &lat, int ls, double *dst, const double *src, int to, int from);
+void gconvert_device(const Lattice &lat, double *dst, const double *src, int to, int from);
+void four2five_device(const Lattice &lat, int ls, double *five, const double *four, int s_u, int s_l, int ncb);
+void five2four_device(const Lattice &lat, int ls, double *four, const double *five, int s_u, int s_l, int ncb);
 int minvcg(Dirac &D, double *const *psi, const double *chi, double chi_norm, const double *shift, int nshift,
            double *rsdcg, int type, const double *alpha, int max_num_iter, int precision, int refine);
 }  // namespace cpsgpu
@@ -330,6 +334,38 @@ int cpsgpu_four2five(const int node_sites[4], int ls, double *five, const double
 int cpsgpu_five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb) {
   return guarded([&] {
     five2four(node_sites, ls, four, five, s_u, s_l, ncb);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_fconvert_device(cpsgpu_lattice lat, int ls, double *dst, const double *src, int to, int from) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    fconvert_device(*lat->L, ls, dst, src, to, from);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_gconvert_device(cpsgpu_lattice lat, double *dst, const double *src, int to, int from) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    gconvert_device(*lat->L, dst, src, to, from);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_four2five_device(cpsgpu_lattice lat, int ls, double *five, const double *four, int s_u, int s_l, int ncb) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    four2five_device(*lat->L, ls, five, four, s_u, s_l, ncb);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_five2four_device(cpsgpu_lattice lat, int ls, double *four, const double *five, int s_u, int s_l, int ncb) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    five2four_device(*lat->L, ls, four, five, s_u, s_l, ncb);
     return CPSGPU_OK;
   });
 }
@@ -1371,7 +1407,12 @@ int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores) {
     if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "Ls x Ls mixing: Mobius operators only");
     CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     d->D->mix_tc = tensor_cores != 0;
-    for (auto &s : d->solvers) s.reset();  // captured graphs hold the other kernels
+    // allocated here, never inside a graph capture
+    if (d->D->mix_tc) d->D->mixTcFrag.ensure(2 * 2 * 32 * 4 * sizeof(unsigned));
+    // captured graphs hold the other kernels
+    for (auto &s : d->solvers) s.reset();
+    d->D->ms.refine.reset();
+    d->D->ms.refine_n = 0;
     return CPSGPU_OK;
   });
 }
@@ -1440,7 +1481,12 @@ int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int sl
       throw Error(CPSGPU_ERR_ARG, "slice pairs: DWF, FP32 or FP16 fields, Ls a multiple of 4 x slices");
     const dim3 b((unsigned)sites, (unsigned)slices, (unsigned)slices_per_thread);
     const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
+    CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));
     for (int ep : eps) tune_set(TuneKey{prec, D.lat->recon(prec), ep, D.kind, D.ls}, b);
+    // captured graphs hold the launches of the old shape
+    for (auto &s : d->solvers) s.reset();
+    d->D->ms.refine.reset();
+    d->D->ms.refine_n = 0;
     return CPSGPU_OK;
   });
 }

@@ -112,11 +112,16 @@ struct OpWork {
 };
 
 // Multishift CG workspace (multishift.cu), kept across calls on one operator.
+struct CgSolver;
 struct MsWork {
   Field chi, r, tmp;
   std::vector<Field> p, psi;
   DeviceBuffer st, ms, pv, psiv;
   OpWork w;
+  // the batched refinement solver of the sloppy path, kept with its fields
+  // and its instantiated graph while the number of shifts stays the same
+  std::shared_ptr<CgSolver> refine;
+  int refine_n = 0;
   // the last call's phases: wall seconds and refinement iterations
   double upload_s = 0, recurrence_s = 0, refine_s = 0, download_s = 0;
   int refine_max = 0, refine_sum = 0;
@@ -152,6 +157,7 @@ struct Dirac {
   // the standalone Ls x Ls mixings of FP16 fields on the tensor cores
   // (mix_tc.cu) instead of the CUDA cores
   bool mix_tc = false;
+  DeviceBuffer mixTcFrag;  // the tensor-core form's A fragments of the matrix being applied
   MsWork ms;  // multishift workspace
   int rhs_tile(int prec, int nrhs) const {
     const int t = rtile[prec];

@@ -1,6 +1,6 @@
 // The Ls x Ls chirality mixing (Mobius M5^-1 and the other s-local
 // matrices, zmobius_m5inv.C:247-396 as a dense matrix) on the tensor cores,
-// for FP16 storage with per-site norms: per block of TS sites and both
+// for FP16 storage with per-site norms: per block of TC_TS sites and both
 // chiralities,
 //
 //     Y_chi (Ls x 12 TS) = M_chi (Ls x Ls) X_chi (Ls x 12 TS)
@@ -12,9 +12,18 @@
 // rounded to FP16 once more (values in [-1, 1]); the result is rescaled by
 // max_t norm_t and re-normalised per output slice.  Real matrices, Ls <= 16.
 //
-// Shared memory per block: the X tile [column][t] in FP16 (column = chirality,
-// site, 12 reals; t padded to 24 halves so the B-fragment loads hit 32
-// distinct banks) and the FP32 result [column][16].
+// Shared memory per block:
+//   xs [t][column] FP16, column = site * 24 + real: each 16-byte group of a
+//      site's stored spinor lands as one 16-byte store, and ldmatrix.trans
+//      reads the B fragments (k = t) straight from the rows; rows are padded
+//      to 392 halves (784 B) so the eight row addresses of an 8 x 8 matrix
+//      fall in distinct bank groups;
+//   ys [s][column] FP32, the products, read back per (slice, site) for the
+//      re-normalised FP16 store.
+// An 8-column tile holds reals 8g .. 8g+7 of one site: g = 0 is chirality 0,
+// g = 2 chirality 1, and g = 1 straddles both (reals 8-11 | 12-15), so its
+// tile is multiplied by both matrices and each thread keeps the product of
+// its own columns' chirality.
 #include "cpsgpu_impl.h"
 #include "hop.cuh"
 
@@ -22,9 +31,10 @@ namespace cpsgpu {
 
 namespace {
 
-constexpr int TC_TS = 16;           // sites per block
-constexpr int TC_KS = 24;           // halves per X column (t padded)
-constexpr int TC_COLS = 2 * 12 * TC_TS;  // 384 columns: [chi][site][12]
+constexpr int TC_TS = 16;                 // sites per block
+constexpr int TC_COLS = 24 * TC_TS;       // 384 columns
+constexpr int TC_XS = TC_COLS + 8;        // halves per xs row
+constexpr int TC_YS = TC_COLS + 8;        // floats per ys row
 constexpr int TC_THREADS = 128;
 
 __device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
@@ -33,6 +43,15 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], 
       "{%0,%1,%2,%3};\n"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// four 8 x 8 FP16 matrices from shared memory, transposed: thread T supplies
+// the address of row T % 8 of matrix T / 8
+__device__ __forceinline__ void ldmatrix_x4_trans(unsigned (&r)[4], const __half *row) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(row);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
 }
 
 __device__ __forceinline__ unsigned pack_h2(float lo, float hi) {
@@ -49,25 +68,42 @@ __device__ __forceinline__ float mel(const double *mix, int ls, int chi, int row
   return part ? (float)(m - (double)hi) : hi;
 }
 
-__global__ void __launch_bounds__(TC_THREADS) mix_tc_kernel(SpinorView in, SpinorView out, const double *mix, int ls,
-                                                            const SolverScalars *st, int gate) {
+// The A fragments (m16n8k16, row-major A = M[s][t]) of both chiralities,
+// high and low FP16 parts, for every lane: frag[((chi * 2 + part) * 32 + lane) * 4 + e].
+// One warp, once per application (the matrices are the operator's).
+__global__ void mix_tc_frag_kernel(const double *mix, int ls, unsigned *frag) {
+  const int lane = threadIdx.x, g = lane >> 2, q = lane & 3;
+  for (int chi = 0; chi < 2; chi++)
+    for (int part = 0; part < 2; part++) {
+      unsigned *f = frag + ((chi * 2 + part) * 32 + lane) * 4;
+      f[0] = pack_h2(mel(mix, ls, chi, g, 2 * q, part), mel(mix, ls, chi, g, 2 * q + 1, part));
+      f[1] = pack_h2(mel(mix, ls, chi, g + 8, 2 * q, part), mel(mix, ls, chi, g + 8, 2 * q + 1, part));
+      f[2] = pack_h2(mel(mix, ls, chi, g, 2 * q + 8, part), mel(mix, ls, chi, g, 2 * q + 9, part));
+      f[3] = pack_h2(mel(mix, ls, chi, g + 8, 2 * q + 8, part), mel(mix, ls, chi, g + 8, 2 * q + 9, part));
+    }
+}
+
+constexpr int TC_LOADS = (16 * 3 * TC_TS + TC_THREADS - 1) / TC_THREADS;  // X groups per thread, at most
+
+__global__ void __launch_bounds__(TC_THREADS) mix_tc_kernel(SpinorView in, SpinorView out, const unsigned *frag,
+                                                            int ls, const SolverScalars *st, int gate) {
   if (gate == GATE_RUNNING && st[blockIdx.z].done) return;
   if (gate == GATE_RELIABLE && (st[blockIdx.z].done || !st[blockIdx.z].reliable)) return;
-  __shared__ __align__(16) __half xs[TC_COLS * TC_KS];
-  __shared__ float ys[TC_COLS * 16];
+  __shared__ __align__(16) __half xs[16 * TC_XS];
+  __shared__ __align__(16) float ys[16 * TC_YS];
   __shared__ float nrm[16 * TC_TS];
   __shared__ float nmax[TC_TS];
   const int tid = threadIdx.x;
   const long i0 = (long)blockIdx.x * TC_TS;
   const long rhs = blockIdx.z;
   const int nsite = (int)min((long)TC_TS, in.vh - i0);
-  // norms of every slice of the block's sites, and their maximum per site
+  // norms of every slice of the block's sites; X zeroed (padding rows t >= ls
+  // and the columns of absent sites stay zero)
   for (int k = tid; k < 16 * TC_TS; k += TC_THREADS) {
     const int t = k / TC_TS, site = k % TC_TS;
     nrm[k] = (t < ls && site < nsite) ? __ldg(in.norm + (rhs * ls + t) * in.vh + i0 + site) : 0.f;
   }
-  // zero padding of X (t >= ls)
-  for (int k = tid; k < TC_COLS * TC_KS / 2; k += TC_THREADS) reinterpret_cast<unsigned *>(xs)[k] = 0u;
+  for (int k = tid; k < 16 * TC_XS / 8; k += TC_THREADS) reinterpret_cast<uint4 *>(xs)[k] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   if (tid < TC_TS) {
     float m = 0.f;
@@ -75,52 +111,77 @@ __global__ void __launch_bounds__(TC_THREADS) mix_tc_kernel(SpinorView in, Spino
     nmax[tid] = m;
   }
   __syncthreads();
-  // X tile: group g (8 halves: reals 8g .. 8g+7) of slice t, site
+  // X: group g (reals 8g .. 8g+7) of slice t and site, rescaled to the
+  // site's largest norm, one 16-byte store; every load of the thread is
+  // issued before the first is used
   const uint4 *src = reinterpret_cast<const uint4 *>(in.data);
-  for (int k = tid; k < ls * 3 * TC_TS; k += TC_THREADS) {
+  uint4 qv[TC_LOADS];
+#pragma unroll
+  for (int j = 0; j < TC_LOADS; j++) {
+    const int k = tid + j * TC_THREADS;
     const int site = k % TC_TS, g = (k / TC_TS) % 3, t = k / (3 * TC_TS);
-    if (site >= nsite) continue;
-    const uint4 q = __ldg(src + ((rhs * ls + t) * 3 + g) * in.vh + i0 + site);
+    qv[j] = (t < ls && site < nsite) ? __ldg(src + ((rhs * ls + t) * 3 + g) * in.vh + i0 + site)
+                                     : make_uint4(0, 0, 0, 0);
+  }
+  unsigned A[2][2][4];  // [chi][hi/lo][frag] of this lane
+  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int cp = 0; cp < 4; cp++) {
+    const uint4 f = __ldg(reinterpret_cast<const uint4 *>(frag) + cp * 32 + lane);
+    A[cp >> 1][cp & 1][0] = f.x;
+    A[cp >> 1][cp & 1][1] = f.y;
+    A[cp >> 1][cp & 1][2] = f.z;
+    A[cp >> 1][cp & 1][3] = f.w;
+  }
+#pragma unroll
+  for (int j = 0; j < TC_LOADS; j++) {
+    const int k = tid + j * TC_THREADS;
+    const int site = k % TC_TS, gg = (k / TC_TS) % 3, t = k / (3 * TC_TS);
+    if (t >= ls || site >= nsite) continue;
     const float r = nmax[site] > 0.f ? nrm[t * TC_TS + site] / nmax[site] : 0.f;
-    const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+    const __half2 *h = reinterpret_cast<const __half2 *>(&qv[j]);
+    uint4 o;
+    unsigned *op = reinterpret_cast<unsigned *>(&o);
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const float2 f = __half22float2(h[e]);
-#pragma unroll
-      for (int w = 0; w < 2; w++) {
-        const int real = 8 * g + 2 * e + w, chi = real / 12, c = real % 12;
-        const int col = (chi * TC_TS + site) * 12 + c;
-        xs[col * TC_KS + t] = __float2half_rn((w ? f.y : f.x) * r);
-      }
+      op[e] = pack_h2(f.x * r, f.y * r);
     }
+    *reinterpret_cast<uint4 *>(xs + t * TC_XS + site * 24 + 8 * gg) = o;
   }
   __syncthreads();
-  // MMAs: warp w takes column tiles w, w + 4, ...; A fragments per chirality
-  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
-  unsigned A[2][2][4];  // [chi][hi/lo][frag]
+  // MMAs: warp w takes the column-tile pairs w, w + 4, ... (16 columns each)
+  const int mrow = lane & 7, mat = lane >> 3;  // this thread's ldmatrix row and matrix
+  for (int pair = warp; pair < TC_COLS / 16; pair += TC_THREADS / 32) {
+    const int n0 = pair * 16;
+    unsigned b[4];
+    // matrices: (k 0-7, n0..), (k 8-15, n0..), (k 0-7, n0+8..), (k 8-15, n0+8..)
+    ldmatrix_x4_trans(b, xs + (mrow + 8 * (mat & 1)) * TC_XS + n0 + 8 * (mat >> 1));
 #pragma unroll
-  for (int chi = 0; chi < 2; chi++)
+    for (int half = 0; half < 2; half++) {
+      const int nt = n0 + 8 * half;          // 8-column tile: reals 8 gt .. of one site
+      const int gt = (nt / 8) % 3;
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+      if (gt != 1) {
+        const int chi = gt >> 1;
+        mma16816(d, A[chi][0], b[2 * half], b[2 * half + 1]);
+        mma16816(d, A[chi][1], b[2 * half], b[2 * half + 1]);
+      } else {
+        // columns 2q, 2q+1 are reals 8 + 2q, 9 + 2q: chirality 0 for q < 2
+        float d1[4] = {0.f, 0.f, 0.f, 0.f};
+        mma16816(d, A[0][0], b[2 * half], b[2 * half + 1]);
+        mma16816(d, A[0][1], b[2 * half], b[2 * half + 1]);
+        mma16816(d1, A[1][0], b[2 * half], b[2 * half + 1]);
+        mma16816(d1, A[1][1], b[2 * half], b[2 * half + 1]);
+        if (q >= 2) {
 #pragma unroll
-    for (int part = 0; part < 2; part++) {
-      A[chi][part][0] = pack_h2(mel(mix, ls, chi, g, 2 * q, part), mel(mix, ls, chi, g, 2 * q + 1, part));
-      A[chi][part][1] = pack_h2(mel(mix, ls, chi, g + 8, 2 * q, part), mel(mix, ls, chi, g + 8, 2 * q + 1, part));
-      A[chi][part][2] = pack_h2(mel(mix, ls, chi, g, 2 * q + 8, part), mel(mix, ls, chi, g, 2 * q + 9, part));
-      A[chi][part][3] =
-          pack_h2(mel(mix, ls, chi, g + 8, 2 * q + 8, part), mel(mix, ls, chi, g + 8, 2 * q + 9, part));
+          for (int e = 0; e < 4; e++) d[e] = d1[e];
+        }
+      }
+      // d: rows (output slices) g and g + 8, columns nt + 2q, nt + 2q + 1
+      *reinterpret_cast<float2 *>(ys + g * TC_YS + nt + 2 * q) = make_float2(d[0], d[1]);
+      *reinterpret_cast<float2 *>(ys + (g + 8) * TC_YS + nt + 2 * q) = make_float2(d[2], d[3]);
     }
-  const unsigned *xw = reinterpret_cast<const unsigned *>(xs);
-  for (int tile = warp; tile < TC_COLS / 8; tile += TC_THREADS / 32) {
-    const int n0 = tile * 8, chi = n0 / (12 * TC_TS);
-    const unsigned b0 = xw[((n0 + g) * TC_KS + 2 * q) / 2];
-    const unsigned b1 = xw[((n0 + g) * TC_KS + 2 * q + 8) / 2];
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-    mma16816(d, A[chi][0], b0, b1);
-    mma16816(d, A[chi][1], b0, b1);
-    // d: rows (output slices) g and g + 8, columns n0 + 2q, n0 + 2q + 1
-    ys[(n0 + 2 * q) * 16 + g] = d[0];
-    ys[(n0 + 2 * q + 1) * 16 + g] = d[1];
-    ys[(n0 + 2 * q) * 16 + g + 8] = d[2];
-    ys[(n0 + 2 * q + 1) * 16 + g + 8] = d[3];
   }
   __syncthreads();
   // output: thread per (slice, site), re-normalised FP16 storage
@@ -128,10 +189,14 @@ __global__ void __launch_bounds__(TC_THREADS) mix_tc_kernel(SpinorView in, Spino
     const int s = k / TC_TS, site = k % TC_TS;
     if (site >= nsite) continue;
     float v[24];
+    const float4 *row = reinterpret_cast<const float4 *>(ys + s * TC_YS + site * 24);
 #pragma unroll
-    for (int real = 0; real < 24; real++) {
-      const int chi = real / 12, c = real % 12;
-      v[real] = ys[((chi * TC_TS + site) * 12 + c) * 16 + s] * nmax[site];
+    for (int c = 0; c < 6; c++) {
+      const float4 f = row[c];
+      v[4 * c] = f.x * nmax[site];
+      v[4 * c + 1] = f.y * nmax[site];
+      v[4 * c + 2] = f.z * nmax[site];
+      v[4 * c + 3] = f.w * nmax[site];
     }
     SpinorIO<PREC_HALF>::store(out, rhs * ls + s, i0 + site, v);
   }
@@ -144,10 +209,15 @@ bool mix_tc_applies(const Dirac &D, int prec) { return prec == PREC_HALF && !D.c
 void launch_mix_tc(const Dirac &D, const double *mix, const SpinorView &in, const SpinorView &out,
                    const SolverScalars *st, int gate) {
   if (!mix_tc_applies(D, PREC_HALF)) throw Error(-2, "tensor-core mixing: FP16 storage, real matrices, Ls <= 16");
-  dim3 grid((unsigned)((in.vh + TC_TS - 1) / TC_TS), 1, in.nrhs);
-  mix_tc_kernel<<<grid, TC_THREADS, 0, D.lat->stream>>>(in, out, mix, D.ls, st, gate);
+  // the fragments of this matrix, then the mixing (same stream: ordered)
+  DeviceBuffer &frag = const_cast<Dirac &>(D).mixTcFrag;
+  frag.ensure(2 * 2 * 32 * 4 * sizeof(unsigned));
+  mix_tc_frag_kernel<<<1, 32, 0, D.lat->stream>>>(mix, D.ls, frag.as<unsigned>());
   CPSGPU_CUDA(cudaGetLastError());
-  launch_counter()++;
+  dim3 grid((unsigned)((in.vh + TC_TS - 1) / TC_TS), 1, in.nrhs);
+  mix_tc_kernel<<<grid, TC_THREADS, 0, D.lat->stream>>>(in, out, frag.as<unsigned>(), D.ls, st, gate);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter() += 2;
 }
 
 }  // namespace cpsgpu

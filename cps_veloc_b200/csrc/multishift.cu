@@ -344,7 +344,7 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
 
   // FP64 view of solution k: the refined solution, else psi_k (converted
   // into tmp64 when it is FP32; used before the next call)
-  std::unique_ptr<CgSolver> cg;
+  CgSolver *cg = nullptr;
   const size_t one = (size_t)chi64.data.bytes;
   auto x64_of = [&](int k) {
     SpinorView v = cg->x64.view();
@@ -364,8 +364,12 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     // as one batched solve (right-hand side k: MatPcDagMatPc + shift_k from
     // the sloppy solution psi_k, to its own residual), so the links are read
     // once per tile of shifts and the iterations share their launches
-    cg.reset(new CgSolver(D, PREC_SINGLE));
-    cg->setup(nshift);
+    if (!mw.refine || mw.refine_n != nshift) {
+      mw.refine = std::make_shared<CgSolver>(D, PREC_SINGLE);
+      mw.refine->setup(nshift);
+      mw.refine_n = nshift;
+    }
+    cg = mw.refine.get();
     for (int k = 0; k < nshift; k++) {
       CPSGPU_CUDA(cudaMemcpyAsync((char *)cg->b64.data.ptr + k * one, chi64.data.ptr, one, cudaMemcpyDeviceToDevice, s));
       launch_convert(s, PREC_DOUBLE, x64_of(k), PS, psi[k].view());

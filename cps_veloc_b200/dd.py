@@ -135,10 +135,20 @@ class InProcessRing:
         return v
 
 
+class _HostFaces:
+    """host copies of a rank's faces, for a backend without device
+    point-to-point (gloo)"""
+
+    def __init__(self, f: Faces):
+        self.to_prev, self.to_next = f.to_prev.cpu(), f.to_next.cpu()
+        self.from_next, self.from_prev = torch.empty_like(self.to_prev), torch.empty_like(self.to_next)
+
+
 class DistRing:
     """one slab per rank of a torch.distributed group: faces by
     point-to-point operations, global sums by all_reduce (the reference's
-    glb_sum)"""
+    glb_sum).  With NCCL the device faces move directly; with gloo they
+    are staged through host memory."""
 
     def __init__(self, group=None):
         self.group = group
@@ -146,7 +156,15 @@ class DistRing:
     def exchange(self, faces):
         if len(faces) != 1:
             raise ValueError("one slab per rank")
-        exchange_faces(faces[0], self.group)
+        f = faces[0]
+        if dist.get_backend(self.group) == "nccl" or not f.to_prev.is_cuda:
+            exchange_faces(f, self.group)
+        else:
+            torch.cuda.synchronize()  # the pack kernels ran on the library's stream
+            h = _HostFaces(f)
+            exchange_faces(h, self.group)
+            f.from_next.copy_(h.from_next)
+            f.from_prev.copy_(h.from_prev)
         torch.cuda.synchronize()
 
     def allreduce(self, v: complex) -> complex:

@@ -122,6 +122,14 @@ int cpsgpu_fconvert(const int node_sites[4], int ls, double *f, int to, int from
 int cpsgpu_gconvert(const int node_sites[4], double *u, int to, int from);
 int cpsgpu_four2five(const int node_sites[4], int ls, double *five, const double *four, int s_u, int s_l, int ncb);
 int cpsgpu_five2four(const int node_sites[4], int ls, double *four, const double *five, int s_u, int s_l, int ncb);
+/* The same four conversions on device memory (FP64 device pointers of the
+ * caller, e.g. cudaMalloc'd or a framework's tensors), out of place
+ * (dst != src), for the geometry of lat (a whole lattice, not a t slab),
+ * asynchronous on lat's stream (cpsgpu_synchronize waits for them). */
+int cpsgpu_fconvert_device(cpsgpu_lattice lat, int ls, double *dst, const double *src, int to, int from);
+int cpsgpu_gconvert_device(cpsgpu_lattice lat, double *dst, const double *src, int to, int from);
+int cpsgpu_four2five_device(cpsgpu_lattice lat, int ls, double *five, const double *four, int s_u, int s_l, int ncb);
+int cpsgpu_five2four_device(cpsgpu_lattice lat, int ls, double *four, const double *five, int s_u, int s_l, int ncb);
 
 /* ---- Dirac operators ---- */
 typedef struct {
@@ -555,7 +563,9 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile);
  * consecutive checkerboard sites x `slices` slices per block, and
  * `slices_per_thread` 1 or 2 (2: DWF at FP32 arithmetic, Ls a multiple of
  * 4 * slices — each thread computes two same-parity slices with shared
- * links).  get returns the shape in use; set overrides the autotuner. */
+ * links).  get returns the shape in use; set overrides the autotuner.  The
+ * shape table (like the autotuner's) is shared by every operator of the same
+ * kind, Ls, precision and link form. */
 int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread);
 int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread);
 

@@ -2,7 +2,8 @@
 cpsgpu_set_mix_impl): M5^-1 (zmobius_m5inv.C:247-396 as a dense matrix)
 against the oracle within the FP16-storage tolerance and against the
 CUDA-core kernel, MatPcDagMatPc in FP16, and the FP16-inner solve to a true
-residual of 1e-10, for Ls = 12 and 16; complex coefficients stay on the CUDA
+residual of 1e-10, for Ls = 5, 8, 12 and 16 (and a checkerboard volume
+that is not a multiple of the 16-site block); complex coefficients stay on the CUDA
 cores."""
 import numpy as np
 import pytest
@@ -14,7 +15,7 @@ from helpers import OracleOps, rel
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("L,ls", [((4, 4, 4, 8), 12), ((4, 4, 4, 4), 16), ((6, 4, 4, 4), 5)])
+@pytest.mark.parametrize("L,ls", [((4, 4, 4, 8), 12), ((4, 4, 4, 4), 16), ((6, 4, 4, 4), 5), ((6, 2, 2, 2), 8)])
 def test_mix_tc(oracle, L, ls):
     A.check(A.lib().cpsgpu_set_device(0))
     mass = 0.05
