@@ -307,7 +307,17 @@ def extra_batched(A, D, sloppy) -> dict:
         seq_fp64 += r.seconds
         it64.append(r.iterations)
     ok = all(r.status == A.CONVERGED and r.true_res <= STOP for r in res)
-    return {"rhs": 12, "rhs_tile": D.rhs_tile(sloppy, 12), "all_converged_1e-10": ok,
+    # the batched solve at each right-hand-side tile (links shared by `tile`
+    # solves' blocks), the autotuner's choice restored afterwards
+    tuned, by_tile = D.rhs_tile(sloppy, 12), {}
+    for tile in (1, 2, 4, 12):
+        D.set_rhs_tile(sloppy, tile)
+        sols = [np.zeros(D.f_size) for _ in srcs]
+        D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=sloppy)
+        sols = [np.zeros(D.f_size) for _ in srcs]
+        by_tile[str(tile)] = D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=sloppy)[0].seconds
+    D.set_rhs_tile(sloppy, tuned)
+    return {"rhs": 12, "rhs_tile": tuned, "all_converged_1e-10": ok, "batched_mixed_s_by_rhs_tile": by_tile,
             "batched_mixed_s": t_batch, "per_rhs_batched_mixed_s": t_batch / 12,
             "sequential_mixed_s": seq_mixed, "sequential_fp64_s": seq_fp64,
             "iterations_mixed": [r.iterations for r in res], "iterations_fp64": it64,

@@ -184,6 +184,8 @@ def lib() -> C.CDLL:
             "cpsgpu_solve_batch": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(CgArg),
                                              C.POINTER(CgResult)]),
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "cpsgpu_dirac_set_pc_type": (C.c_int, [vp, C.c_int]),
+            "cpsgpu_dirac_get_pc_type": (C.c_int, [vp, C.POINTER(C.c_int)]),
             "cpsgpu_get_hop_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "cpsgpu_set_hop_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),

@@ -402,6 +402,7 @@ int cpsgpu_dirac_set_zmobius(cpsgpu_dirac d, const double *b, const double *c) {
     if (!d || !b || !c) throw Error(CPSGPU_ERR_ARG, "null argument");
     Dirac &D = *d->D;
     if (D.kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "complex b_s, c_s: Mobius operators only");
+    if (D.pc_type != PC_SYM2) throw Error(CPSGPU_ERR_ARG, "per-slice b_s, c_s: SYM2 preconditioning only");
     std::vector<std::complex<double>> bs(D.ls), cs(D.ls);
     for (int s = 0; s < D.ls; s++) {
       bs[s] = {b[2 * s], b[2 * s + 1]};
@@ -630,10 +631,12 @@ int cpsgpu_invcg(cpsgpu_dirac d, double *sol, const double *src, const cpsgpu_cg
 //   Wilson / DWF (d_op_wilson.C:257-334, d_op_dwf.C:316-492), halves [odd | even]:
 //     temp = kappa Dslash(in_e, CHKB_EVEN) + in_o;  b = MatPcDag temp;  CG;
 //     out_e = kappa Dslash(out_o, CHKB_ODD) + in_e
-//   Mobius SYM2 (d_op_mobius.C:407-700), halves [even | odd]:
-//     temp = kappa_b Dslash_4(M5^-1 in_e, CHKB_EVEN) + in_o;  guess out_o <- M5 out_o;
-//     b = MatPcDag temp;  CG;  out_o <- M5^-1 out_o;
+//   Mobius (d_op_mobius.C:407-700), halves [even | odd]:
+//     temp = kappa_b Dslash_4(M5^-1 in_e, CHKB_EVEN) + in_o;  SYM1: temp <- M5^-1 temp;
+//     SYM2, SYM3: guess out_o <- M5 out_o;  b = MatPcDag temp;  CG;
+//     SYM2, SYM3: out_o <- M5^-1 out_o;
 //     out_e = M5^-1 (kappa_b Dslash_4(out_o, CHKB_ODD) + in_e);  out *= 2 kappa_b
+//   (the MIT preconditionings: not implemented, as in the reference)
 namespace {
 // DiracOp*::MatInv for Inverter CG, LOWMODEAPPROX or CG_LOWMODE_DEFL
 // (d_op_dwf.C:316-500, d_op_mobius.C:407-620); eig_name / neig: the
@@ -666,16 +669,22 @@ int matinv_impl(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_a
       op_dslash(D, PREC_DOUBLE, t1.view(), fo.view(), 0, 0);
       launch_axpby(s, t1.view(), D.kappa, t1.view(), t2.view());
     } else {
+      if (D.pc_type == PC_SYM1_MIT || D.pc_type == PC_SYM2_MIT)
+        throw Error(CPSGPU_ERR_UNSUPPORTED, "MatInv: the MIT preconditionings are not implemented (d_op_mobius.C:477-495)");
       op_mobius_m5inv(D, PREC_DOUBLE, t1.view(), fo.view(), 0);
       Field t3(PREC_DOUBLE, L.vh, D.ls, 1);
       op_mobius_dslash4(D, PREC_DOUBLE, t3.view(), t1.view(), 0, 0, w);
       launch_axpby(s, t1.view(), D.kappa, t3.view(), t2.view());
+      if (D.pc_type == PC_SYM1) {  // SYM1: the source gets M5^-1 (d_op_mobius.C:519-530)
+        op_mobius_m5inv(D, PREC_DOUBLE, t3.view(), t1.view(), 0);
+        CPSGPU_CUDA(cudaMemcpyAsync(t1.data.ptr, t3.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
+      }
     }
     op_matpc(D, PREC_DOUBLE, S.b64.view(), t1.view(), 1, w, nullptr, 0, 0);
     std::vector<CgResult> r;
     if (inverter == CPSGPU_INV_CG) {
       upload(L, S.x64, &out_cg, 1);
-      if (mob) {  // SYM2 guess: x <- M5 x
+      if (mob && (D.pc_type == PC_SYM2 || D.pc_type == PC_SYM3)) {  // guess: x <- M5 x (d_op_mobius.C:498-515)
         launch_mix(D, PREC_DOUBLE, D.mixM5.as<double>(), S.x64.view(), t1.view());
         CPSGPU_CUDA(cudaMemcpyAsync(S.x64.data.ptr, t1.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
       }
@@ -699,7 +708,9 @@ int matinv_impl(cpsgpu_dirac d, double *out, const double *in, const cpsgpu_cg_a
       download(L, S.x64, &out_cg, 1);
       download(L, t2, &out_other, 1);
     } else {
-      op_mobius_m5inv(D, PREC_DOUBLE, t1.view(), S.x64.view(), 0);  // out_o
+      // out_o: M5^-1 x for SYM2 / SYM3, x itself for ORIG / SYM1 (d_op_mobius.C:627-663)
+      if (D.pc_type == PC_SYM2 || D.pc_type == PC_SYM3) op_mobius_m5inv(D, PREC_DOUBLE, t1.view(), S.x64.view(), 0);
+      else CPSGPU_CUDA(cudaMemcpyAsync(t1.data.ptr, S.x64.data.ptr, t1.data.bytes, cudaMemcpyDeviceToDevice, s));
       op_mobius_dslash4(D, PREC_DOUBLE, t2.view(), t1.view(), 1, 0, w);
       launch_axpby(s, t2.view(), D.kappa, t2.view(), fo.view());
       op_mobius_m5inv(D, PREC_DOUBLE, fo.view(), t2.view(), 0);     // out_e
@@ -728,6 +739,8 @@ ForceVecs &force_vecs(cpsgpu_dirac d, const double *chi) {
   Dirac &D = *d->D;
   Lattice &L = *D.lat;
   if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
+  if (D.kind == KIND_MOBIUS && D.pc_type != PC_SYM2)
+    throw Error(CPSGPU_ERR_UNSUPPORTED, "the fermion force is built for the SYM2 preconditioning");
   if (!d->fv) d->fv.reset(new ForceVecs());
   ensure_field(d->in[PREC_DOUBLE], PREC_DOUBLE, L.vh, D.ls, 1);
   upload(L, d->in[PREC_DOUBLE], &chi, 1);
@@ -788,6 +801,8 @@ int cpsgpu_rhmc_evolve_mom_fforce(cpsgpu_dirac d, double *mom, const double *con
     Dirac &D = *d->D;
     Lattice &L = *D.lat;
     if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
+    if (D.kind == KIND_MOBIUS && D.pc_type != PC_SYM2)
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "the fermion force is built for the SYM2 preconditioning");
     const size_t bytes = (size_t)2 * L.vh * 4 * 18 * sizeof(double);
     d->mom.ensure(2 * bytes);
     double *m = d->mom.as<double>(), *tmp = m + bytes / sizeof(double);
@@ -823,6 +838,8 @@ int cpsgpu_time_fforce(cpsgpu_dirac d, int reps, double *ms_total, double *ms_ke
     Dirac &D = *d->D;
     Lattice &L = *D.lat;
     if (D.kind == KIND_MOBIUS && D.cplx) throw Error(CPSGPU_ERR_ARG, "the fermion force is built for real Mobius b, c");
+    if (D.kind == KIND_MOBIUS && D.pc_type != PC_SYM2)
+      throw Error(CPSGPU_ERR_UNSUPPORTED, "the fermion force is built for the SYM2 preconditioning");
     if (!d->fv) d->fv.reset(new ForceVecs());
     Field chi(PREC_DOUBLE, L.vh, D.ls, 1);
     std::vector<double> h((size_t)24 * L.vh * D.ls);
@@ -1401,6 +1418,32 @@ int cpsgpu_solve_batch(int n, const cpsgpu_dirac *ops, const cpsgpu_field *sol, 
   });
 }
 
+int cpsgpu_dirac_set_pc_type(cpsgpu_dirac d, int pc_type) {
+  return guarded([&] {
+    if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
+    if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "preconditioning type: Mobius operators only");
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    try {
+      d->D->set_pc_type(pc_type);
+    } catch (const Error &e) {
+      throw Error(CPSGPU_ERR_ARG, e.what());
+    }
+    // captured graphs hold the launches of the old form
+    for (auto &s : d->solvers) s.reset();
+    d->D->ms.refine.reset();
+    d->D->ms.refine_n = 0;
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dirac_get_pc_type(cpsgpu_dirac d, int *pc_type) {
+  return guarded([&] {
+    if (!d || !pc_type) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    *pc_type = (d->D->kind == KIND_MOBIUS) ? d->D->pc_type : PC_SYM2;
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores) {
   return guarded([&] {
     if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
@@ -1451,7 +1494,12 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
   return guarded([&] {
     if (!d || tile < 0) throw Error(CPSGPU_ERR_ARG, "bad argument");
     check_prec(prec);
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     d->D->rtile[prec] = tile;
+    // captured graphs hold the launches of the old tile
+    for (auto &s : d->solvers) s.reset();
+    d->D->ms.refine.reset();
+    d->D->ms.refine_n = 0;
     return CPSGPU_OK;
   });
 }

@@ -108,7 +108,18 @@ struct Lattice {
 };
 
 struct OpWork {
-  Field t1, t2, t0;  // operator temporaries, one precision
+  Field t1, t2, t0, t3;  // operator temporaries, one precision
+};
+
+// Mobius preconditionings (GJP.ZMobius_PC_Type, dwf.h:42-48)
+enum MobiusPc { PC_ORIG = 0, PC_SYM1 = 1, PC_SYM2 = 2, PC_SYM1_MIT = 3, PC_SYM2_MIT = 4, PC_SYM3 = 5 };
+// MatPc (plan[0]) or MatPc^dagger (plan[1]) of a Mobius operator as
+//   out = X + Last W_cb0( Mid W_cb1( Pre in ) ),   X = in, or Xmix in,
+// every matrix s-local ([2][ls][ls] per chirality, the layout of the mixing
+// kernels); a null Pre / Xmix is the identity, a null Last the scalar coef.
+struct MobiusPlan {
+  const double *pre = nullptr, *mid = nullptr, *last = nullptr, *xmix = nullptr;
+  double coef = 0.0;
 };
 
 // Multishift CG workspace (multishift.cu), kept across calls on one operator.
@@ -146,6 +157,7 @@ struct Dirac {
   // stored [2][ls][ls][re, im], and the -kappa_b(s) of MatPc is the complex
   // diagonal mixKb applied in a mixing epilogue
   bool cplx = false;
+  bool uniform_bc = true;  // the same b, c on every slice
   DeviceBuffer mixKb;
   std::vector<double> hM5i, hM5id, hB, hBd;  // host copies of the packed M5^-1 and B matrices
   Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_, double a5inv_ = 1.0);
@@ -158,6 +170,12 @@ struct Dirac {
   // (mix_tc.cu) instead of the CUDA cores
   bool mix_tc = false;
   DeviceBuffer mixTcFrag;  // the tensor-core form's A fragments of the matrix being applied
+  // the preconditioning of MatPc (Mobius) and its two plans; the matrices
+  // of the non-SYM2 forms live in pc_bufs
+  int pc_type = PC_SYM2;
+  MobiusPlan plan[2];
+  std::vector<DeviceBuffer> pc_bufs;
+  void set_pc_type(int pc);
   MsWork ms;  // multishift workspace
   int rhs_tile(int prec, int nrhs) const {
     const int t = rtile[prec];
@@ -182,6 +200,19 @@ struct HopLaunch {
 void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
                 const SpinorView &x, const SpinorView &r, const SpinorView &sol, const SpinorView &p,
                 const SpinorView &b, SolverScalars *st);
+
+// Everything of the Mobius MatPc (dag 0) or MatPc^dagger (dag 1) before its
+// last hop (D.plan[dag]: the pre-mixing, the first hop with its mixing, the
+// X term): the caller launches out = x + Last W_cb0(hop_in) with the
+// epilogue it needs (mix = Last, or the scalar coef when mix is null).
+// Lh carries precision, gate and partials; uses w.t0, w.t1, w.t3.
+struct MobiusTail {
+  SpinorView hop_in, x;
+  const double *mix;
+  double coef;
+};
+MobiusTail mobius_head(const Dirac &D, int prec, int dag, const SpinorView &in, OpWork &w, HopLaunch Lh,
+                       SolverScalars *st);
 
 // the tensor-core form of launch_mix (mix_tc.cu): FP16 fields, real
 // matrices, Ls <= 16

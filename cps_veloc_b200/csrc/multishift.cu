@@ -159,6 +159,7 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   ensure_field(w.t1, P, vh, ls, 1);
   ensure_field(w.t2, P, vh, ls, 1);
   if (D.kind == KIND_MOBIUS) ensure_field(w.t0, P, vh, ls, 1);
+  if (D.kind == KIND_MOBIUS && (D.plan[0].xmix || D.plan[1].xmix)) ensure_field(w.t3, P, vh, ls, 1);
   size_t nblk = (size_t)((vh + 31) / 32) * ls + 1024;
   L.partials.ensure(nblk * 2 * sizeof(double));
 
@@ -254,49 +255,51 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     Lh.gate = GATE_RUNNING;
     Lh.dag = 0;
     const SpinorView in = p[0].view();
+    SpinorView hop_in = w.t1.view(), x = in;
     if (mob) {
-      launch_mix(D, P, D.mixP.as<double>(), in, w.t0.view(), st, GATE_RUNNING);
-      Lh.ep = EP_MIX;
-      Lh.cb = 1;
-      Lh.mix = D.mixQ.as<double>();
-      launch_hop(D, Lh, w.t0.view(), w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(),
-                 SpinorView(), st);
-      Lh.mix = nullptr;
-      Lh.coef.assign(ls, -D.kappa);
+      // the preconditioning's plan up to its last hop (mobius_head)
+      const MobiusTail t = mobius_head(D, P, 0, in, w, Lh, st);
+      hop_in = t.hop_in;
+      x = t.x;
+      Lh.mix = t.mix;
+      Lh.coef.assign(ls, t.coef);
+      Lh.ep = t.mix ? EP_MIX_AXPY : EP_AXPY;
     } else {
       Lh.ep = EP_STORE;
       Lh.cb = 1;
       launch_hop(D, Lh, in, w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
       Lh.coef.assign(ls, -D.kappa * D.kappa);
-    }
-    Lh.ep = EP_AXPY;
-    if (mob && D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
-      Lh.ep = EP_MIX_AXPY;
-      Lh.mix = D.mixKb.as<double>();
+      Lh.ep = EP_AXPY;
     }
     Lh.cb = 0;
     Lh.norm = 1;
     Lh.red_op = RED_MS_PAP;
-    launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
+    launch_hop(D, Lh, hop_in, w.t2.view(), x, SpinorView(), SpinorView(), SpinorView(), SpinorView(), st);
     Lh.mix = nullptr;
     Lh.norm = 0;
     Lh.dag = 1;
-    Lh.cb = 1;
+    bool mix_last = false;
+    x = w.t2.view();
     if (mob) {
-      Lh.ep = EP_MIX;
-      Lh.mix = D.mixR.as<double>();
+      const MobiusTail t = mobius_head(D, P, 1, w.t2.view(), w, Lh, st);
+      hop_in = t.hop_in;
+      x = t.x;
+      Lh.mix = t.mix;
+      Lh.coef.assign(ls, t.coef);
+      mix_last = (t.mix != nullptr);
     } else {
       Lh.ep = EP_STORE;
+      Lh.cb = 1;
+      launch_hop(D, Lh, w.t2.view(), w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(),
+                 SpinorView(), st);
+      hop_in = w.t1.view();
     }
-    launch_hop(D, Lh, w.t2.view(), w.t1.view(), SpinorView(), SpinorView(), SpinorView(), SpinorView(),
-               SpinorView(), st);
     Lh.cb = 0;
     Lh.red_op = RED_MS_RR;
     Lh.pr = P;
     Lh.px = px_of(P);
-    if (mob) Lh.mix = D.mixS.as<double>();
-    Lh.ep = mob ? EP_MIX_CG : EP_CG;
-    launch_hop(D, Lh, w.t1.view(), SpinorView(), w.t2.view(), r.view(), SpinorView(), in, SpinorView(), st);
+    Lh.ep = mix_last ? EP_MIX_CG : EP_CG;
+    launch_hop(D, Lh, hop_in, SpinorView(), x, r.view(), SpinorView(), in, SpinorView(), st);
     size_t per = (size_t)vh * ls;
     if (dev_type != 0) {
       const unsigned g = (unsigned)((per + 127) / 128) * (unsigned)nshift;

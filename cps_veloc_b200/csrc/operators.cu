@@ -221,6 +221,8 @@ void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
     K[s] = kb[s] / kc[s];
     cplx = cplx || bs[s].imag() != 0.0 || cs[s].imag() != 0.0;
   }
+  uniform_bc = true;
+  for (int s = 1; s < ls; s++) uniform_bc = uniform_bc && bs[s] == bs[0] && cs[s] == cs[0];
   b = bs[0].real();
   c = cs[0].real();
   kappa = kb[0].real();
@@ -267,6 +269,138 @@ void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
   upload(mixM5, packm(m5u, m5d));
   upload(mixM5a, packm(m5au, m5ad));
   upload(mixKb, packm(kbm, kbm));
+  set_pc_type((cplx || !uniform_bc) ? PC_SYM2 : pc_type);
+}
+
+// The plans of MatPc and MatPc^dagger for a preconditioning type, in the
+// notation out = X + Last W_cb0(Mid W_cb1(Pre in)) with B the b/c mixing of
+// zmobius_dslash_4 (B^+ after the hop for dag 1), M = M5^-1, K = kappa_b:
+//   ORIG      (zmobius_m-orig.h, zmobius_mdag-orig.h)
+//       dag 0: Pre B,            Mid B M K,  Last -K,            X = M5 in
+//       dag 1: Pre -,            Mid K M^+ B^+ (-K), Last B^+,   X = M5^+ in
+//   SYM1      (zmobius_m-sym1.h, zmobius_mdag-sym1.h)
+//       dag 0: Pre B,            Mid B M K,  Last M (-K)
+//       dag 1: Pre M^+,          Mid K M^+ B^+ (-K), Last B^+
+//   SYM2      (zmobius_m-sym2.h, zmobius_mdag-sym2.h)
+//       dag 0: Pre B M,          Mid B M K,  Last -K
+//       dag 1: Pre -,            Mid K M^+ B^+ (-K), Last M^+ B^+
+//   SYM1_MIT  (zmobius_m-sym1-MIT.h, zmobius_mdag-sym1-MIT.h)
+//       dag 0: Pre B Binv,       Mid B M K,  Last Bm M (-K)
+//       dag 1: Pre M^+ Bm^+,     Mid K M^+ B^+ (-K), Last Binv^+ B^+
+//   SYM2_MIT  (zmobius_m-sym2-MIT.h, zmobius_mdag-sym2-MIT.h)
+//       dag 0: Pre B M Binv,     Mid B M K,  Last Bm (-K)
+//       dag 1: Pre Bm^+,         Mid K M^+ B^+ (-K), Last Binv^+ M^+ B^+
+//   SYM3      (zmobius_m-sym3.h, zmobius_mdag-sym3.h)
+//       dag 0: Pre B M,          Mid B M,    Last 1
+//       dag 1: Pre -,            Mid M^+ B^+, Last M^+ B^+
+// with Bm = b (1 + (c/b) D5) and Binv = M5^-1(K = c/b) / b the MIT matrices
+// (zmobius_B_MIT / zmobius_Binv_MIT, d_op_zmobius.C:132-239), X = in unless
+// stated, and diagonal factors moved through W (it acts slice by slice).
+// SYM3 rescales GJP's b, c by i kappa_b around its hops, but
+// zmobius_dslash_4 reads the operator's own copies of b, c
+// (zmobius_dslash_4.C:61-62), so the hops see the plain B: reproduced as
+// the reference computes it.  The forms other than SYM2 need real b, c.
+void Dirac::set_pc_type(int pc) {
+  if (kind != KIND_MOBIUS) throw Error(-1, "preconditioning type: Mobius operators only");
+  if (pc < PC_ORIG || pc > PC_SYM3) throw Error(-1, "unknown Mobius preconditioning type");
+  if (pc != PC_SYM2 && (cplx || !uniform_bc))
+    throw Error(-1, "Mobius preconditioning other than SYM2: real b, c, the same on every slice");
+  pc_type = pc;
+  pc_bufs.clear();
+  pc_bufs.reserve(16);
+  plan[0] = plan[1] = MobiusPlan();
+  if (pc == PC_SYM2) {
+    plan[0].pre = mixP.as<double>();
+    plan[0].mid = mixQ.as<double>();
+    if (cplx) plan[0].last = mixKb.as<double>();
+    else plan[0].coef = -kappa;
+    plan[1].mid = mixR.as<double>();
+    plan[1].last = mixS.as<double>();
+    return;
+  }
+  using V = std::vector<cd>;
+  const V bs(ls, b), cs(ls, c), ones(ls, 1.0);
+  V kb(ls), K(ls), fact(ls), mkb(ls), ckb(ls), invb(ls), invbc(ls);
+  for (int s = 0; s < ls; s++) {
+    kb[s] = 1.0 / (2.0 * (bs[s] * (4.0 - m5) + a5inv));
+    const cd kc = 1.0 / (2.0 * (cs[s] * (4.0 - m5) - a5inv));
+    K[s] = kb[s] / kc;
+    fact[s] = cs[s] / bs[s];
+    mkb[s] = -kb[s];
+    ckb[s] = std::conj(kb[s]);
+    invb[s] = 1.0 / bs[s];
+    invbc[s] = 1.0 / std::conj(bs[s]);
+  }
+  V m0u, m0d, m1u, m1d, f0u, f0d, f1u, f1d, bu, bd, m5u, m5d, fbu, fbd;
+  m5inv_columns(ls, K, mass, 0, m0u, m0d);
+  m5inv_columns(ls, K, mass, 1, m1u, m1d);
+  m5inv_columns(ls, fact, mass, 0, f0u, f0d);
+  m5inv_columns(ls, fact, mass, 1, f1u, f1d);
+  bmix(ls, bs, cs, mass, bu, bd);
+  bmix(ls, ones, K, mass, m5u, m5d);
+  bmix(ls, ones, fact, mass, fbu, fbd);
+  struct Pair {
+    V u, d;
+  };
+  auto mm = [&](const Pair &a, const Pair &b2) { return Pair{matmul(ls, a.u, b2.u), matmul(ls, a.d, b2.d)}; };
+  auto adj = [&](const Pair &a) { return Pair{adjoint(ls, a.u), adjoint(ls, a.d)}; };
+  auto dl = [&](const V &d, const Pair &a) { return Pair{diag_left(ls, d, a.u), diag_left(ls, d, a.d)}; };
+  auto dr = [&](const Pair &a, const V &d) { return Pair{diag_right(ls, a.u, d), diag_right(ls, a.d, d)}; };
+  const Pair B{bu, bd}, Bd = adj(B), M{m0u, m0d}, Md{m1u, m1d}, M5{m5u, m5d}, M5d = adj(M5);
+  const Pair Bm = dl(bs, Pair{fbu, fbd}), Bmd = dr(adj(Pair{fbu, fbd}), V(ls, std::conj(bs[0])));
+  const Pair Binv = dr(Pair{f0u, f0d}, invb), Binvd = dl(invbc, Pair{f1u, f1d});
+  V diag_mk((size_t)ls * ls, 0.0);
+  for (int s = 0; s < ls; s++) diag_mk[(size_t)s * ls + s] = mkb[s];
+  const Pair negK{diag_mk, diag_mk};
+  const Pair Q = dr(mm(B, M), kb);                 // B M K
+  const Pair R = dr(dl(ckb, mm(Md, Bd)), mkb);     // K M^+ B^+ (-K)
+  auto put = [&](const Pair &a) -> const double * {
+    pc_bufs.emplace_back();
+    upload(pc_bufs.back(), pack(ls, a.u, a.d));
+    return pc_bufs.back().as<double>();
+  };
+  switch (pc) {
+    case PC_ORIG:
+      plan[0].pre = put(B);
+      plan[0].mid = put(Q);
+      plan[0].coef = -kappa;
+      plan[0].xmix = put(M5);
+      plan[1].mid = put(R);
+      plan[1].last = put(Bd);
+      plan[1].xmix = put(M5d);
+      break;
+    case PC_SYM1:
+      plan[0].pre = put(B);
+      plan[0].mid = put(Q);
+      plan[0].last = put(mm(M, negK));
+      plan[1].pre = put(Md);
+      plan[1].mid = put(R);
+      plan[1].last = put(Bd);
+      break;
+    case PC_SYM1_MIT:
+      plan[0].pre = put(mm(B, Binv));
+      plan[0].mid = put(Q);
+      plan[0].last = put(mm(Bm, mm(M, negK)));
+      plan[1].pre = put(mm(Md, Bmd));
+      plan[1].mid = put(R);
+      plan[1].last = put(mm(Binvd, Bd));
+      break;
+    case PC_SYM2_MIT:
+      plan[0].pre = put(mm(B, mm(M, Binv)));
+      plan[0].mid = put(Q);
+      plan[0].last = put(mm(Bm, negK));
+      plan[1].pre = put(Bmd);
+      plan[1].mid = put(R);
+      plan[1].last = put(mm(Binvd, mm(Md, Bd)));
+      break;
+    default:  // PC_SYM3
+      plan[0].pre = put(mm(B, M));
+      plan[0].mid = put(mm(B, M));
+      plan[0].coef = 1.0;
+      plan[1].mid = put(mm(Md, Bd));
+      plan[1].last = put(mm(Md, Bd));
+      break;
+  }
 }
 
 // ---------------------------------------------------------------- operators
@@ -325,37 +459,46 @@ void op_matpc(const Dirac &D, int prec, const SpinorView &out, const SpinorView 
     launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
     return;
   }
-  if (!dag) {
-    ensure_field(w.t0, prec, lat.vh, D.ls, in.nrhs);
-    launch_mix(D, prec, D.mixP.as<double>(), in, w.t0.view());
-    L.ep = EP_MIX;
-    L.cb = 1;
-    L.mix = D.mixQ.as<double>();
-    launch_hop(D, L, w.t0.view(), w.t1.view(), none(), none(), none(), none(), none(), st);
-    L.cb = 0;
-    if (D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
-      L.ep = EP_MIX_AXPY;
-      L.mix = D.mixKb.as<double>();
-    } else {
-      L.ep = EP_AXPY;
-      L.mix = nullptr;
-      L.coef.assign(D.ls, -D.kappa);
-    }
-    L.norm = norm;
-    L.red_op = red_op;
-    launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
-  } else {
-    L.ep = EP_MIX;
-    L.cb = 1;
-    L.mix = D.mixR.as<double>();
-    launch_hop(D, L, in, w.t1.view(), none(), none(), none(), none(), none(), st);
+  // the Mobius form of the preconditioning type (D.plan): SYM2 by default
+  const MobiusTail t = mobius_head(D, prec, dag, in, w, L, st);
+  L.cb = 0;
+  if (t.mix) {
     L.ep = EP_MIX_AXPY;
-    L.cb = 0;
-    L.mix = D.mixS.as<double>();
-    L.norm = norm;
-    L.red_op = red_op;
-    launch_hop(D, L, w.t1.view(), out, in, none(), none(), none(), none(), st);
+    L.mix = t.mix;
+  } else {
+    L.ep = EP_AXPY;
+    L.mix = nullptr;
+    L.coef.assign(D.ls, t.coef);
   }
+  L.norm = norm;
+  L.red_op = red_op;
+  launch_hop(D, L, t.hop_in, out, t.x, none(), none(), none(), none(), st);
+}
+
+MobiusTail mobius_head(const Dirac &D, int prec, int dag, const SpinorView &in, OpWork &w, HopLaunch Lh,
+                       SolverScalars *st) {
+  const Lattice &lat = *D.lat;
+  const MobiusPlan &p = D.plan[dag ? 1 : 0];
+  SpinorView src = in;
+  if (p.pre) {
+    ensure_field(w.t0, prec, lat.vh, D.ls, in.nrhs);
+    launch_mix(D, prec, p.pre, in, w.t0.view(), st, Lh.gate);
+    src = w.t0.view();
+  }
+  ensure_field(w.t1, prec, lat.vh, D.ls, in.nrhs);
+  Lh.ep = EP_MIX;
+  Lh.cb = 1;
+  Lh.dag = dag;
+  Lh.mix = p.mid;
+  Lh.norm = 0;
+  launch_hop(D, Lh, src, w.t1.view(), none(), none(), none(), none(), none(), st);
+  MobiusTail t{w.t1.view(), in, p.last, p.coef};
+  if (p.xmix) {
+    ensure_field(w.t3, prec, lat.vh, D.ls, in.nrhs);
+    launch_mix(D, prec, p.xmix, in, w.t3.view(), st, Lh.gate);
+    t.x = w.t3.view();
+  }
+  return t;
 }
 
 // out = MatPc^+ MatPc in; st->sum[0] = |MatPc in|^2 (the reference's dot).

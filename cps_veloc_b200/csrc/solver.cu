@@ -76,6 +76,12 @@ void CgSolver::setup(int nrhs_) {
   ensure_field(wd.t1, PREC_DOUBLE, vh, ls, nrhs);
   ensure_field(wd.t2, PREC_DOUBLE, vh, ls, nrhs);
   if (D.kind == KIND_MOBIUS) ensure_field(wd.t0, PREC_DOUBLE, vh, ls, nrhs);
+  // the X = M5 in term of the ORIG preconditioning (allocated here: the
+  // operator is captured into graphs, where no allocation may happen)
+  if (D.kind == KIND_MOBIUS && (D.plan[0].xmix || D.plan[1].xmix)) {
+    ensure_field(ws.t3, sloppy, vh, ls, nrhs);
+    ensure_field(wd.t3, PREC_DOUBLE, vh, ls, nrhs);
+  }
   st.ensure(sizeof(SolverScalars) * nrhs);
   // partials: 2 values per block; the smallest hop block is 32 threads
   size_t nblk = (size_t)((vh + 31) / 32) * ls + 1024;
@@ -114,52 +120,55 @@ void CgSolver::emit_mdagm(int prec, const SpinorView &in, OpWork &w, int final_e
   Lh.partials = partials.as<double>();
   // ---- M = MatPc ----
   Lh.dag = 0;
+  SpinorView hop_in = w.t1.view(), x = in;
   if (mob) {
-    launch_mix(D, prec, D.mixP.as<double>(), in, w.t0.view(), stp, gate);
-    Lh.ep = EP_MIX;
-    Lh.cb = 1;
-    Lh.mix = D.mixQ.as<double>();
-    launch_hop(D, Lh, w.t0.view(), w.t1.view(), none(), none(), none(), none(), none(), stp);
-    Lh.mix = nullptr;
-    Lh.coef.assign(D.ls, -D.kappa);
+    // the preconditioning's plan up to its last hop (mobius_head)
+    const MobiusTail t = mobius_head(D, prec, 0, in, w, Lh, stp);
+    hop_in = t.hop_in;
+    x = t.x;
+    Lh.mix = t.mix;
+    Lh.coef.assign(D.ls, t.coef);
+    Lh.ep = t.mix ? EP_MIX_AXPY : EP_AXPY;
   } else {
     Lh.ep = EP_STORE;
     Lh.cb = 1;
     launch_hop(D, Lh, in, w.t1.view(), none(), none(), none(), none(), none(), stp);
     Lh.coef.assign(D.ls, -D.kappa * D.kappa);
-  }
-  Lh.ep = EP_AXPY;
-  if (mob && D.cplx) {  // complex kappa_b(s): the diagonal as a mixing epilogue
-    Lh.ep = EP_MIX_AXPY;
-    Lh.mix = D.mixKb.as<double>();
+    Lh.ep = EP_AXPY;
   }
   Lh.cb = 0;
   Lh.norm = pap;
   Lh.red_op = RED_PAP;
-  launch_hop(D, Lh, w.t1.view(), w.t2.view(), in, none(), none(), none(), none(), stp);
+  launch_hop(D, Lh, hop_in, w.t2.view(), x, none(), none(), none(), none(), stp);
   Lh.mix = nullptr;
   // ---- M^dagger ----
   Lh.norm = 0;
   Lh.dag = 1;
-  Lh.cb = 1;
+  bool mix_last = false;
+  x = w.t2.view();
   if (mob) {
-    Lh.ep = EP_MIX;
-    Lh.mix = D.mixR.as<double>();
+    const MobiusTail t = mobius_head(D, prec, 1, w.t2.view(), w, Lh, stp);
+    hop_in = t.hop_in;
+    x = t.x;
+    Lh.mix = t.mix;
+    Lh.coef.assign(D.ls, t.coef);
+    mix_last = (t.mix != nullptr);
   } else {
     Lh.ep = EP_STORE;
+    Lh.cb = 1;
+    launch_hop(D, Lh, w.t2.view(), w.t1.view(), none(), none(), none(), none(), none(), stp);
+    hop_in = w.t1.view();
   }
-  launch_hop(D, Lh, w.t2.view(), w.t1.view(), none(), none(), none(), none(), none(), stp);
   Lh.cb = 0;
   Lh.red_op = red_op;
   Lh.pr = pr;
   Lh.px = px;
-  if (mob) Lh.mix = D.mixS.as<double>();
   if (final_ep == EP_CG) {
-    Lh.ep = mob ? EP_MIX_CG : EP_CG;
-    launch_hop(D, Lh, w.t1.view(), none(), w.t2.view(), rv, solv, in, none(), stp);
+    Lh.ep = mix_last ? EP_MIX_CG : EP_CG;
+    launch_hop(D, Lh, hop_in, none(), x, rv, solv, in, none(), stp);
   } else {
-    Lh.ep = mob ? EP_MIX_RES : EP_RES;
-    launch_hop(D, Lh, w.t1.view(), none(), w.t2.view(), rv, in, none(), b64.view(), stp);
+    Lh.ep = mix_last ? EP_MIX_RES : EP_RES;
+    launch_hop(D, Lh, hop_in, none(), x, rv, in, none(), b64.view(), stp);
   }
 }
 

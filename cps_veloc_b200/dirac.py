@@ -613,10 +613,24 @@ class DiracOpDwf(_DiracOp):
 
 class DiracOpMobius(_DiracOp):
     kind = A.MOBIUS
+    # GJP.ZMobius_PC_Type values (enum ZMobiusPCType, dwf.h:42-48)
+    PC_ORIG, PC_SYM1, PC_SYM2, PC_SYM1_MIT, PC_SYM2_MIT, PC_SYM3 = range(6)
 
     def __init__(self, lat: Lattice, mass: float, ls: int, m5: float = 1.8, b: float = 1.5, c: float = 0.5,
-                 a5_inv: float = 1.0):
+                 a5_inv: float = 1.0, pc_type: int = 2):
         super().__init__(lat, mass, ls=ls, m5=m5, b=b, c=c, a5_inv=a5_inv)
+        if pc_type != self.PC_SYM2:
+            self.set_pc_type(pc_type)
+
+    def set_pc_type(self, pc_type: int) -> None:
+        """the preconditioning of MatPc (GJP.ZMobius_PC_Type; SYM2 the default)"""
+        check(lib().cpsgpu_dirac_set_pc_type(self._h, pc_type))
+
+    @property
+    def pc_type(self) -> int:
+        v = C.c_int()
+        check(lib().cpsgpu_dirac_get_pc_type(self._h, C.byref(v)))
+        return v.value
 
     def set_mix_impl(self, tensor_cores: bool) -> None:
         """the standalone Ls x Ls mixings of FP16 fields on the tensor cores

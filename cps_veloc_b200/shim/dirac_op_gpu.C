@@ -74,6 +74,13 @@ cpsgpu_dirac device_op(Lattice &lat, const CgArg *arg) {
     if (cpsgpu_dirac_create(g_lat, &a, &g_op) != CPSGPU_OK) die("InvCgShift");
     g_arg = a;
   }
+  // the Mobius preconditioning the DiracOp in scope uses (d_op_mobius.C:104)
+  if (a.kind == CPSGPU_MOBIUS) {
+    int pc = -1;
+    if (cpsgpu_dirac_get_pc_type(g_op, &pc) != CPSGPU_OK) die("InvCgShift");
+    if (pc != (int)GJP.ZMobius_PC_Type() && cpsgpu_dirac_set_pc_type(g_op, (int)GJP.ZMobius_PC_Type()) != CPSGPU_OK)
+      die("InvCgShift");
+  }
   return g_op;
 }
 

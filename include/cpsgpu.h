@@ -212,6 +212,18 @@ int cpsgpu_matpc_dag_matpc_shift(cpsgpu_dirac d, double *out, const double *in, 
  * out-of-place zmobius_m5inv (zmobius_m5inv.C:822). */
 int cpsgpu_mobius_dslash_4(cpsgpu_dirac d, double *out, const double *in, int cb, int dag, int prec);
 int cpsgpu_mobius_m5inv(cpsgpu_dirac d, double *out, const double *in, int dag, int prec);
+/* The Mobius operator's preconditioning, GJP.ZMobius_PC_Type (DoArgExt
+ * zmobius_pc_type; enum ZMobiusPCType, dwf.h:42-48): 0 ORIG, 1 SYM1, 2 SYM2
+ * (the default), 3 SYM1_MIT, 4 SYM2_MIT, 5 SYM3, as zmobius_m / zmobius_mdag
+ * dispatch on it (zmobius_m.C:40-74, zmobius_mdag.C:41-69).  MatPc, MatPcDag,
+ * MatPcDagMatPc and the CG and multishift solvers follow it; MatInv
+ * supports ORIG, SYM1, SYM2 and SYM3 (d_op_mobius.C:477-663; the MIT forms
+ * stop there with an error, and return one here).  The forms other than
+ * SYM2 need real b, c, the same on every slice.  SYM3 is reproduced as the
+ * reference computes it: its rescaling of GJP's b, c does not reach the
+ * hops, which read the operator's own copies (zmobius_dslash_4.C:61-62). */
+int cpsgpu_dirac_set_pc_type(cpsgpu_dirac d, int pc_type);
+int cpsgpu_dirac_get_pc_type(cpsgpu_dirac d, int *pc_type);
 /* No counterpart in the reference: where the Mobius operator applies a
  * standalone Ls x Ls mixing (M5^-1, the first step of MatPc) to an FP16
  * field, tensor_cores = 1 runs it as mma.sync m16n8k16 contractions (FP16

@@ -127,6 +127,8 @@ def load_oracle() -> C.CDLL:
             "orc_mobius_m": [g, m, _dp, _dp, _dp, d, i],
             "orc_mobius_mdagm": [g, m, _dp, _dp, _dp, d, _dp],
             "orc_mobius_m5": [g, m, _dp, d],
+            "orc_mobius_m_pc": [g, m, _dp, _dp, _dp, d, i, i],
+            "orc_mobius_mdagm_pc": [g, m, _dp, _dp, _dp, d, _dp, i],
             "orc_sproj_tr": [i, i, _dp, _dp, _dp, i, i, i],
             "orc_force_matrix": [_dp, _dp, _dp, _dp, d],
             "orc_fforce": [g, _dp, _dp, _dp, _dp, d, _dp],
@@ -145,6 +147,8 @@ def load_oracle() -> C.CDLL:
         L.orc_wilson_matinv.argtypes = [g, _dp, _dp, _dp, d, d, i, _dp]
         L.orc_dwf_matinv.argtypes = [g, _dp, _dp, _dp, d, d, d, i, _dp]
         L.orc_mobius_matinv.argtypes = [g, m, _dp, _dp, _dp, d, d, i, _dp]
+        L.orc_mobius_matinv_pc.argtypes = [g, m, _dp, _dp, _dp, d, d, i, _dp, i]
+        L.orc_mobius_matinv_pc.restype = i
         L.orc_bicgstab.argtypes = [MATPC_FN, C.c_void_p, C.c_long, _dp, _dp, d, i, d, i, _dp]
         L.orc_bicgstab.restype = i
         L.orc_minresext.argtypes = [MDAGM_FN, C.c_void_p, C.c_long, _dp, _dp, C.POINTER(_dp), C.POINTER(_dp), i,

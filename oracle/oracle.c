@@ -387,6 +387,107 @@ void orc_mobius_m(const orc_geom *g, const orc_mobius *mp, double *out,
   free(t2);
 }
 
+/* zmobius_B_MIT (d_op_zmobius.C:132-185), in place, fact = c/b:
+ * dag 0: out = b_s (in + fact-hop5(in)); dag 1: t = conj(b_s) in, out = t + fact-hop5^dagger(t). */
+static void mobius_b_mit(const orc_geom *g, const orc_mobius *mp, double *inout, double mass, int dag) {
+  int ls = g->ls;
+  long vh = vol_cb(g), n = 24 * vh * ls;
+  cplx fact[64];
+  for (int s = 0; s < ls; s++) fact[s] = mp->c[s] / mp->b[s];
+  double *t = malloc(sizeof(double) * n);
+  if (!dag) {
+    memcpy(t, inout, sizeof(double) * n);
+    mobius_hop5_acc(g, ls, fact, inout, t, mass, 0);
+    scale_slices(inout, vh, ls, mp->b, 1.0, 0);
+  } else {
+    scale_slices(inout, vh, ls, mp->b, 1.0, 1);
+    memcpy(t, inout, sizeof(double) * n);
+    mobius_hop5_acc(g, ls, fact, inout, t, mass, 1);
+  }
+  free(t);
+}
+
+/* zmobius_Binv_MIT (d_op_zmobius.C:190-239), in place: dag 0: M5^-1(K = c/b) (in / b_s);
+ * dag 1: M5^-1^dagger(K = c/b) in, then / conj(b_s). */
+static void mobius_binv_mit(const orc_geom *g, const orc_mobius *mp, double *inout, double mass, int dag) {
+  int ls = g->ls;
+  long vh = vol_cb(g);
+  orc_mobius q = *mp;
+  cplx inv_b[64];
+  for (int s = 0; s < ls; s++) q.K[s] = mp->c[s] / mp->b[s];
+  if (!dag) {
+    for (int s = 0; s < ls; s++) inv_b[s] = 1.0 / mp->b[s];
+    scale_slices(inout, vh, ls, inv_b, 1.0, 0);
+    orc_mobius_m5inv(g, &q, inout, mass, 0);
+  } else {
+    orc_mobius_m5inv(g, &q, inout, mass, 1);
+    for (int s = 0; s < ls; s++) inv_b[s] = 1.0 / conj(mp->b[s]);
+    scale_slices(inout, vh, ls, inv_b, 1.0, 0);
+  }
+}
+
+/* The preconditioned operator of every type zmobius_m / zmobius_mdag
+ * dispatch on (zmobius_m.C:40-74, zmobius_mdag.C:41-69), step by step as
+ * zmobius_m-{orig,sym1,sym2,sym1-MIT,sym2-MIT,sym3}.h and their mdag
+ * counterparts.  SYM3 rescales GJP's b, c around its hops, which read the
+ * operator's own copies (zmobius_dslash_4.C:61-62): no effect, so none here. */
+void orc_mobius_m_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                     double mass, int dag, int pc) {
+  if (pc == ORC_PC_SYM2) {
+    orc_mobius_m(g, mp, out, u, in, mass, dag);
+    return;
+  }
+  int ls = g->ls;
+  long vh = vol_cb(g), n = 24 * vh * ls;
+  double *t2 = malloc(sizeof(double) * n);
+  if (!dag) {
+    const double *src = in;
+    if (pc == ORC_PC_SYM1_MIT || pc == ORC_PC_SYM2_MIT || pc == ORC_PC_SYM3) {
+      memcpy(t2, in, sizeof(double) * n);
+      if (pc != ORC_PC_SYM3) mobius_binv_mit(g, mp, t2, mass, 0);
+      if (pc != ORC_PC_SYM1_MIT) orc_mobius_m5inv(g, mp, t2, mass, 0);
+      src = t2;
+    }
+    orc_mobius_dslash_4(g, mp, out, u, src, 1, 0, mass);
+    if (pc != ORC_PC_SYM3) scale_slices(out, vh, ls, mp->kappa_b, 1.0, 0);
+    orc_mobius_m5inv(g, mp, out, mass, 0);
+    orc_mobius_dslash_4(g, mp, t2, u, out, 0, 0, mass);
+    if (pc != ORC_PC_SYM3) scale_slices(t2, vh, ls, mp->kappa_b, -1.0, 0);
+    if (pc == ORC_PC_SYM1 || pc == ORC_PC_SYM1_MIT) orc_mobius_m5inv(g, mp, t2, mass, 0);
+    if (pc == ORC_PC_SYM1_MIT || pc == ORC_PC_SYM2_MIT) mobius_b_mit(g, mp, t2, mass, 0);
+    for (long k = 0; k < n; k++) out[k] = in[k] + t2[k];
+    if (pc == ORC_PC_ORIG) mobius_hop5_acc(g, ls, mp->K, out, in, mass, 0);
+  } else {
+    memcpy(out, in, sizeof(double) * n);
+    if (pc == ORC_PC_SYM1_MIT || pc == ORC_PC_SYM2_MIT) mobius_b_mit(g, mp, out, mass, 1);
+    if (pc == ORC_PC_SYM1 || pc == ORC_PC_SYM1_MIT) orc_mobius_m5inv(g, mp, out, mass, 1);
+    if (pc != ORC_PC_SYM3) scale_slices(out, vh, ls, mp->kappa_b, -1.0, 1);
+    orc_mobius_dslash_4(g, mp, t2, u, out, 1, 1, mass);
+    orc_mobius_m5inv(g, mp, t2, mass, 1);
+    if (pc != ORC_PC_SYM3) scale_slices(t2, vh, ls, mp->kappa_b, 1.0, 1);
+    orc_mobius_dslash_4(g, mp, out, u, t2, 0, 1, mass);
+    if (pc == ORC_PC_SYM2_MIT || pc == ORC_PC_SYM3) orc_mobius_m5inv(g, mp, out, mass, 1);
+    if (pc == ORC_PC_SYM1_MIT || pc == ORC_PC_SYM2_MIT) mobius_binv_mit(g, mp, out, mass, 1);
+    for (long k = 0; k < n; k++) out[k] += in[k];
+    if (pc == ORC_PC_ORIG) mobius_hop5_acc(g, ls, mp->K, out, in, mass, 1);
+  }
+  free(t2);
+}
+
+void orc_mobius_mdagm_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                         double mass, double *dot, int pc) {
+  long n = 24 * vol_cb(g) * g->ls;
+  double *t = malloc(sizeof(double) * n);
+  orc_mobius_m_pc(g, mp, t, u, in, mass, 0, pc);
+  if (dot) {
+    double s = 0;
+    for (long k = 0; k < n; k++) s += t[k] * t[k];
+    *dot = s;
+  }
+  orc_mobius_m_pc(g, mp, out, u, t, mass, 1, pc);
+  free(t);
+}
+
 /* zmobius_mdagm.C:32-59 */
 void orc_mobius_mdagm(const orc_geom *g, const orc_mobius *mp, double *out,
                       const double *u, const double *in, double mass,
@@ -607,13 +708,14 @@ typedef struct {
   const double *u;
   double mass, m5, kappa;
   int kind; /* 0 Wilson, 1 DWF, 2 Mobius */
+  int pc;   /* Mobius preconditioning (ORC_PC_*) */
 } matinv_ctx;
 
 static void matinv_mdagm(void *vctx, double *out, const double *in, double *dot) {
   const matinv_ctx *c = (const matinv_ctx *)vctx;
   if (c->kind == 0) orc_wilson_mdagm(c->g, out, c->u, in, c->kappa, dot);
   else if (c->kind == 1) orc_dwf_mdagm(c->g, out, c->u, in, c->mass, c->m5, dot);
-  else orc_mobius_mdagm(c->g, c->mp, out, c->u, in, c->mass, dot);
+  else orc_mobius_mdagm_pc(c->g, c->mp, out, c->u, in, c->mass, dot, c->pc);
 }
 
 /* out[k] = a * x[k] + y[k] (fTimesV1PlusV2) */
@@ -647,39 +749,44 @@ static int wilson_dwf_matinv(const matinv_ctx *c, double *out, const double *in,
 
 int orc_wilson_matinv(const orc_geom *g, double *out, const double *u, const double *in, double kappa,
                       double stop_rsd, int max_num_iter, double *true_res) {
-  matinv_ctx c = {g, 0, u, 0.0, 0.0, kappa, 0};
+  matinv_ctx c = {g, 0, u, 0.0, 0.0, kappa, 0, ORC_PC_SYM2};
   return wilson_dwf_matinv(&c, out, in, stop_rsd, max_num_iter, true_res);
 }
 
 int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double *in, double mass, double m5,
                    double stop_rsd, int max_num_iter, double *true_res) {
-  matinv_ctx c = {g, 0, u, mass, m5, 1.0 / (2.0 * (4.0 + a5inv(g) - m5)), 1};  /* dwf_kappa */
+  matinv_ctx c = {g, 0, u, mass, m5, 1.0 / (2.0 * (4.0 + a5inv(g) - m5)), 1, ORC_PC_SYM2};  /* dwf_kappa */
   return wilson_dwf_matinv(&c, out, in, stop_rsd, max_num_iter, true_res);
 }
 
-/* d_op_mobius.C:407-700, SYM2 (real b, c: kappa_b the same for every s). */
-int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
-                      double mass, double stop_rsd, int max_num_iter, double *true_res) {
+/* d_op_mobius.C:407-700 for the preconditionings ORIG, SYM1, SYM2 and SYM3
+ * (the MIT ones stop with an error there; -1 here), real b, c (kappa_b the
+ * same for every s). */
+int orc_mobius_matinv_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                         double mass, double stop_rsd, int max_num_iter, double *true_res, int pc) {
+  if (pc == ORC_PC_SYM1_MIT || pc == ORC_PC_SYM2_MIT) return -1;
   long half = 24 * vol_cb(g) * g->ls;
   const double *even_in = in, *odd_in = in + half;
   double *even_out = out, *odd_out = out + half;
   double *temp = malloc(sizeof(double) * half), *temp2 = malloc(sizeof(double) * half),
          *b = malloc(sizeof(double) * half);
   const double kb = creal(mp->kappa_b[0]);
-  /* source: temp = kappa_b Dslash_4(M5^-1 in_even, CHKB_EVEN) + in_odd (:482-490) */
+  /* source: temp = kappa_b Dslash_4(M5^-1 in_even, CHKB_EVEN) + in_odd (:477-495) */
   memcpy(temp, even_in, sizeof(double) * half);
   orc_mobius_m5inv(g, mp, temp, mass, 0);
   orc_mobius_dslash_4(g, mp, temp2, u, temp, 0, 0, mass);
   axpy_to(temp, kb, temp2, odd_in, half);
-  /* guess: odd_out <- M5 odd_out (:503-515) */
-  orc_mobius_m5(g, mp, odd_out, mass);
+  /* guess: odd_out <- M5 odd_out for SYM2 / SYM3 (:498-515) */
+  if (pc == ORC_PC_SYM2 || pc == ORC_PC_SYM3) orc_mobius_m5(g, mp, odd_out, mass);
+  /* SYM1: temp <- M5^-1 temp (:519-530) */
+  if (pc == ORC_PC_SYM1) orc_mobius_m5inv(g, mp, temp, mass, 0);
   /* CG on MatPcDag temp (:540-548) */
-  orc_mobius_m(g, mp, b, u, temp, mass, 1);
-  matinv_ctx c = {g, mp, u, mass, 0.0, 0.0, 2};
+  orc_mobius_m_pc(g, mp, b, u, temp, mass, 1, pc);
+  matinv_ctx c = {g, mp, u, mass, 0.0, 0.0, 2, pc};
   int iter = orc_invcg(matinv_mdagm, &c, half, odd_out, b, 0.0, stop_rsd, max_num_iter, true_res, 0);
-  /* odd_out <- M5^-1 odd_out; even_out = M5^-1 (kappa_b Dslash_4(odd_out, CHKB_ODD)) + M5^-1 in_even
-   * (:629-646) */
-  orc_mobius_m5inv(g, mp, odd_out, mass, 0);
+  /* SYM2 / SYM3: odd_out <- M5^-1 odd_out; then (every type)
+   * even_out = M5^-1 (kappa_b Dslash_4(odd_out, CHKB_ODD)) + M5^-1 in_even (:627-663) */
+  if (pc == ORC_PC_SYM2 || pc == ORC_PC_SYM3) orc_mobius_m5inv(g, mp, odd_out, mass, 0);
   orc_mobius_dslash_4(g, mp, temp, u, odd_out, 1, 0, mass);
   for (long k = 0; k < half; k++) temp[k] *= kb;
   memcpy(even_out, temp, sizeof(double) * half);
@@ -693,6 +800,11 @@ int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, cons
   free(temp2);
   free(b);
   return iter;
+}
+
+int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                      double mass, double stop_rsd, int max_num_iter, double *true_res) {
+  return orc_mobius_matinv_pc(g, mp, out, u, in, mass, stop_rsd, max_num_iter, true_res, ORC_PC_SYM2);
 }
 
 /* ---------------------------------------------------------------------- */

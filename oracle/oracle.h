@@ -80,6 +80,13 @@ void orc_mobius_mdagm(const orc_geom *g, const orc_mobius *mp, double *out,
  * guess for SYM2 (d_op_mobius.C:505-515 via zmobius_kappa_dslash_5_plus_cmplx,
  * zmobius_dslash_5_plus.C:125-374, which accumulates into its output). */
 void orc_mobius_m5(const orc_geom *g, const orc_mobius *mp, double *inout, double mass);
+/* every preconditioning type of zmobius_m / zmobius_mdag (zmobius_m.C:40-74,
+ * zmobius_mdag.C:41-69; enum ZMobiusPCType, dwf.h:42-48) */
+enum { ORC_PC_ORIG = 0, ORC_PC_SYM1 = 1, ORC_PC_SYM2 = 2, ORC_PC_SYM1_MIT = 3, ORC_PC_SYM2_MIT = 4, ORC_PC_SYM3 = 5 };
+void orc_mobius_m_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                     double mass, int dag, int pc);
+void orc_mobius_mdagm_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                         double mass, double *dot, int pc);
 
 /* CG on MatPcDagMatPc (+shift): DiracOp::InvCgShift, inv_cg.C:84-448.
  * The operator is a callback: out = MdagM in, *dot = |M in|^2 when dot!=0.
@@ -121,6 +128,10 @@ int orc_dwf_matinv(const orc_geom *g, double *out, const double *u, const double
                    double stop_rsd, int max_num_iter, double *true_res);
 int orc_mobius_matinv(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
                       double mass, double stop_rsd, int max_num_iter, double *true_res);
+/* the same for the preconditioning pc (ORIG, SYM1, SYM2, SYM3; -1 for the
+ * MIT ones, which the reference does not implement) */
+int orc_mobius_matinv_pc(const orc_geom *g, const orc_mobius *mp, double *out, const double *u, const double *in,
+                         double mass, double stop_rsd, int max_num_iter, double *true_res, int pc);
 
 /* DiracOp::MinResExt (minresext.C): the chronological initial guess over an
  * MatPcDagMatPc callback; v[] is orthonormalised in place, vm[i] = A v[i].

@@ -37,8 +37,6 @@ void LatRngWrite::write(UGrandomGenerator *, UGrandomGenerator *, const QioArg &
 bool DoArg::Decode(char *, char *) { not_built("DoArg::Decode"); return false; }
 bool MdwfTuning::Decode(char *, char *) { not_built("MdwfTuning::Decode"); return false; }
 bool MdwfTuning::Encode(char *, char *) { not_built("MdwfTuning::Encode"); return false; }
-void zmobius_B_MIT(Vector *, Float, int, Zmobus *, Complex *, Complex *) { not_built("zmobius_B_MIT"); }
-void zmobius_Binv_MIT(Vector *, Float, int, Zmobus *, Complex *, Complex *) { not_built("zmobius_Binv_MIT"); }
 int DiracOp::InvLowModeApprox(std::vector<Vector *> &, std::vector<Vector *> &, char *, int) {
   not_built("DiracOp::InvLowModeApprox");
   return 0;

@@ -156,6 +156,31 @@ int rs_matinv(double *out, double *in, double mass, double stop_rsd, int max_ite
   return it;
 }
 
+// The Mobius preconditioning the DiracOps built from now on use
+// (GJP.ZMobius_PC_Type, dwf.h:42-48: ORIG, SYM1, SYM2, SYM1_MIT, SYM2_MIT,
+// SYM3), read by the DiracOpMobius constructor (d_op_mobius.C:104).  The
+// MIT and SYM3 forms read and (SYM3) temporarily rescale GJP's per-slice
+// zMobius coefficients, which are set to the real b, c here.
+void rs_set_pc_type(int pc_type) {
+  const int ls = GJP.SnodeSites();
+  GJP.zmobius_b.assign(ls, Complex(GJP.Mobius_b(), 0.0));
+  GJP.zmobius_c.assign(ls, Complex(GJP.Mobius_c(), 0.0));
+  GJP.ZMobius_PC_Type((ZMobiusPCType)pc_type);
+}
+
+// MatPc of the DiracOp (checkerboard vectors)
+void rs_matpc(double *out, double *in, double mass) {
+  CgArg cg;
+  fill_cg(cg, mass, 1e-8, 10);
+  DiracOp *op = make_op((Vector *)out, (Vector *)in, &cg);
+  switch (g_kind) {
+    case 0: static_cast<DiracOpWilson *>(op)->MatPc((Vector *)out, (Vector *)in); break;
+    case 1: static_cast<DiracOpDwf *>(op)->MatPc((Vector *)out, (Vector *)in); break;
+    default: static_cast<DiracOpMobius *>(op)->MatPc((Vector *)out, (Vector *)in); break;
+  }
+  delete op;
+}
+
 // MatPcDagMatPc and Dslash of the DiracOp (checkerboard vectors), for
 // checking the storage orders against the kernel-level harness.
 void rs_matpc_dag_matpc(double *out, double *in, double mass, double *dot) {

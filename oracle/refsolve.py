@@ -6,7 +6,8 @@ static gauge field, lattice_base.C:56, 320-325).
     python -m oracle.refsolve SPEC.json OUT.npz
 
 SPEC keys: L (4 ints), ls, kind ("wilson" | "dwf" | "mobius"), m5, a5_inv,
-b, c, bc_t, backend, task, and per task:
+b, c, bc_t, backend, pc_type (the Mobius preconditioning, dwf.h:42-48;
+default SYM2), task, and per task:
 
 * ``fwilsoninv``: the steps of the reference's tests/f_wilson_inv/main.C on
   its own disordered start and RandGaussVector source (mass, stop_rsd,
@@ -19,6 +20,11 @@ b, c, bc_t, backend, task, and per task:
 * ``ops``: Mat, MatDag (not Mobius: the reference's stops with an error),
   MatHerm on the full vector src, and for Mobius MatPcDagMatPcShift
   (eigen_shift mu) on its first half (gauge, src, mass, mu);
+* ``pcops``: MatPc and MatPcDag of the checkerboard vector src (gauge, src,
+  mass);
+* ``matinv``: DiracOp*::MatInv on the full vector src (both checkerboards,
+  the DiracOp's order), zero initial guess (gauge, src, mass, stop_rsd,
+  max_iter);
 * ``cgtime``: wall time of DiracOp::InvCgShift capped at each max_iter of
   ``caps`` (zero initial guess each time, after ``warmup`` untimed capped
   runs), on the source MatPcDag(src) (gauge, src, mass, stop_rsd).
@@ -73,6 +79,8 @@ def _lib(backend: str = "cpu"):
     L.rs_matinv.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
     L.rs_matpc_dag_matpc.argtypes = [_dp, _dp, C.c_double, _dp]
     L.rs_matpc_dag.argtypes = [_dp, _dp, C.c_double]
+    L.rs_matpc.argtypes = [_dp, _dp, C.c_double]
+    L.rs_set_pc_type.argtypes = [C.c_int]
     L.rs_mat.argtypes = [_dp, _dp, C.c_double, C.c_int]
     L.rs_matherm.argtypes = [_dp, _dp, C.c_double]
     L.rs_mdagm_shift.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp]
@@ -124,6 +132,8 @@ def run(spec: dict) -> dict:
         u = np.zeros(vol * 72)
         L.rs_get_gauge(_p(u))
     out["gauge"] = u
+    if "pc_type" in spec:
+        L.rs_set_pc_type(int(spec["pc_type"]))
     tr = C.c_double()
     with _Stdout() as cap:
         if spec["task"] == "fwilsoninv":
@@ -141,6 +151,18 @@ def run(spec: dict) -> dict:
             sol = np.zeros_like(src)
             it = L.rs_invcg(_p(sol), _p(src), spec["mass"], spec["stop_rsd"], spec["max_iter"],
                             spec.get("shift", 0.0), C.byref(tr))
+            out.update(sol=sol)
+        elif spec["task"] == "pcops":
+            src = np.ascontiguousarray(np.load(spec["src"]), dtype=np.float64)
+            mp, md = np.zeros_like(src), np.zeros_like(src)
+            L.rs_matpc(_p(mp), _p(src.copy()), spec["mass"])
+            L.rs_matpc_dag(_p(md), _p(src.copy()), spec["mass"])
+            out.update(matpc=mp, matpcdag=md)
+            it = 0
+        elif spec["task"] == "matinv":
+            src = np.ascontiguousarray(np.load(spec["src"]), dtype=np.float64)
+            sol = np.zeros_like(src)
+            it = L.rs_matinv(_p(sol), _p(src.copy()), spec["mass"], spec["stop_rsd"], spec["max_iter"], C.byref(tr))
             out.update(sol=sol)
         elif spec["task"] == "minvcg":
             src = np.ascontiguousarray(np.load(spec["src"]), dtype=np.float64)

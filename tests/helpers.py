@@ -142,8 +142,30 @@ class OracleOps:
         self.O.orc_mobius_mdagm(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(x), mass, C.byref(d))
         return y, d.value
 
+    def mobius_m_pc(self, x, mass, dag, pc):
+        """MatPc / MatPcDag under the preconditioning pc (zmobius_m.C:40-74)"""
+        y = self.z()
+        self.O.orc_mobius_m_pc(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(np.ascontiguousarray(x)), mass,
+                               dag, pc)
+        return y
+
+    def mobius_mdagm_pc(self, x, mass, pc):
+        y = self.z()
+        d = C.c_double()
+        self.O.orc_mobius_mdagm_pc(C.byref(self.g), C.byref(self.mp), p(y), p(self.u), p(np.ascontiguousarray(x)),
+                                   mass, C.byref(d), pc)
+        return y, d.value
+
+    def mobius_matinv_pc(self, src, mass, pc, stop_rsd=1e-8, max_num_iter=10000):
+        """DiracOpMobius::MatInv under the preconditioning pc, zero guess"""
+        out = np.zeros(2 * self.n)
+        tr = C.c_double()
+        it = self.O.orc_mobius_matinv_pc(C.byref(self.g), C.byref(self.mp), p(out), p(self.u),
+                                         p(np.ascontiguousarray(src)), mass, stop_rsd, max_num_iter, C.byref(tr), pc)
+        return out, it, tr.value
+
     # ---- solvers over an operator callback
-    def _op(self, kind, mass, kappa):
+    def _op(self, kind, mass, kappa, pc=2):
         O, u, g = self.O, self.u, self.g
 
         def fn(ctx, out, inp, dot):
@@ -151,15 +173,17 @@ class OracleOps:
                 O.orc_wilson_mdagm(C.byref(self.g1), out, p(u), inp, kappa, dot)
             elif kind == "dwf":
                 O.orc_dwf_mdagm(C.byref(g), out, p(u), inp, mass, self.m5, dot)
-            else:
+            elif pc == 2:
                 O.orc_mobius_mdagm(C.byref(g), C.byref(self.mp), out, p(u), inp, mass, dot)
+            else:
+                O.orc_mobius_mdagm_pc(C.byref(g), C.byref(self.mp), out, p(u), inp, mass, dot, pc)
 
         return MDAGM_FN(fn)
 
-    def invcg(self, kind, src, sol0=None, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, shift=None):
+    def invcg(self, kind, src, sol0=None, mass=0.0, kappa=0.0, stop_rsd=1e-8, max_num_iter=10000, shift=None, pc=2):
         sol = np.zeros(self.n) if sol0 is None else np.ascontiguousarray(sol0).copy()
         tr = C.c_double()
-        fn = self._op(kind, mass, kappa)
+        fn = self._op(kind, mass, kappa, pc)
         sh = C.c_double(shift) if shift is not None else None
         it = self.O.orc_invcg(fn, None, self.n, p(sol), p(src), 0.0, stop_rsd, max_num_iter, C.byref(tr),
                               C.byref(sh) if sh is not None else None)
