@@ -352,13 +352,20 @@ def extra_mobius(A) -> dict:
         ms, by = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
         flops = 48 * ls * D.f_size // 24  # dense Ls x Ls, both chiralities
         out[f"m5inv_{name}"] = {"ms": ms, "GB_s": by / ms / 1e6, "frac_of_measured_hbm": by / ms / 1e6 / pk,
-                                "flop_per_byte": flops / by, "unit": "CUDA cores (dense Ls x Ls from shared memory)"}
+                                "flop_per_byte": flops / by,
+                                "unit": "CUDA cores, register-tiled (matrix as a kernel parameter)"}
+        # the shared-memory CUDA-core kernel it replaced
+        D.set_mix_impl(D.MIX_SHARED)
+        ms2, by2 = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
+        D.set_mix_impl(D.MIX_REG)
+        out[f"m5inv_{name}_shared_memory_kernel"] = {"ms": ms2, "GB_s": by2 / ms2 / 1e6,
+                                                     "frac_of_measured_hbm": by2 / ms2 / 1e6 / pk}
         m2, b2 = C.c_double(), C.c_double()
         A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, 20, C.byref(m2), C.byref(b2)))
         out[f"hop_{name}"] = {"ms": m2.value, "GB_s": b2.value / m2.value / 1e6}
     # the same M5^-1 of the FP16 field on the tensor cores (mma.sync m16n8k16),
     # and the FP16-inner solve with every standalone mixing there
-    D.set_mix_impl(True)
+    D.set_mix_impl(D.MIX_TENSOR_CORES)
     ms, by = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, A.HALF, 20)
     out["m5inv_half_tensor_cores"] = {"ms": ms, "GB_s": by / ms / 1e6, "frac_of_measured_hbm": by / ms / 1e6 / pk,
                                       "unit": "tensor cores (mma.sync m16n8k16, FP16 operands, FP32 accumulation)",
@@ -369,7 +376,14 @@ def extra_mobius(A) -> dict:
     rt = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
     out["half_inner_cg_tensor_core_mixing"] = {"time_s": rt.seconds, "iterations": rt.iterations,
                                                "true_res": rt.true_res, "reliable_updates": rt.reliable_updates}
-    D.set_mix_impl(False)
+    # and with the shared-memory mixing kernel, the form before the register-tiled one
+    D.set_mix_impl(D.MIX_SHARED)
+    x = np.zeros(D.f_size)
+    D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
+    x = np.zeros(D.f_size)
+    rs = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
+    out["half_inner_cg_shared_memory_mixing"] = {"time_s": rs.seconds, "iterations": rs.iterations}
+    D.set_mix_impl(D.MIX_REG)
     D.close()
     lat.close()
     return out

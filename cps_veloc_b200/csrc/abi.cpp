@@ -1444,12 +1444,14 @@ int cpsgpu_dirac_get_pc_type(cpsgpu_dirac d, int *pc_type) {
   });
 }
 
-int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores) {
+int cpsgpu_set_mix_impl(cpsgpu_dirac d, int impl) {
   return guarded([&] {
     if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
     if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "Ls x Ls mixing: Mobius operators only");
+    if (impl < 0 || impl > 2) throw Error(CPSGPU_ERR_ARG, "mixing kernel: 0 register-tiled, 1 tensor cores, 2 shared memory");
     CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
-    d->D->mix_tc = tensor_cores != 0;
+    d->D->mix_tc = (impl == 1);
+    d->D->mix_reg = (impl != 2);
     // allocated here, never inside a graph capture
     if (d->D->mix_tc) d->D->mixTcFrag.ensure(2 * 2 * 32 * 4 * sizeof(unsigned));
     // captured graphs hold the other kernels

@@ -5,6 +5,7 @@
 #include <stdexcept>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "fields.cuh"
@@ -160,6 +161,9 @@ struct Dirac {
   bool uniform_bc = true;  // the same b, c on every slice
   DeviceBuffer mixKb;
   std::vector<double> hM5i, hM5id, hB, hBd;  // host copies of the packed M5^-1 and B matrices
+  // host copy of every real mixing matrix uploaded for this operator, by
+  // device address (launch_mix passes the matrix as a kernel parameter)
+  std::unordered_map<const void *, std::vector<double>> mix_host;
   Dirac(Lattice *l, int kind_, int ls_, double mass_, double m5_, double b_, double c_, double a5inv_ = 1.0);
   // (re)build the Mobius matrices from per-slice coefficients
   void build_mobius(const std::vector<std::complex<double>> &bs, const std::vector<std::complex<double>> &cs);
@@ -169,6 +173,9 @@ struct Dirac {
   // the standalone Ls x Ls mixings of FP16 fields on the tensor cores
   // (mix_tc.cu) instead of the CUDA cores
   bool mix_tc = false;
+  // the register-tiled mixing kernel (mix_reg.cu) where it applies; off:
+  // the shared-memory kernel (blas.cu)
+  bool mix_reg = true;
   DeviceBuffer mixTcFrag;  // the tensor-core form's A fragments of the matrix being applied
   // the preconditioning of MatPc (Mobius) and its two plans; the matrices
   // of the non-SYM2 forms live in pc_bufs
@@ -220,6 +227,11 @@ bool mix_tc_applies(const Dirac &D, int prec);
 void launch_mix_tc(const Dirac &D, const double *mix, const SpinorView &in, const SpinorView &out,
                    const SolverScalars *st, int gate);
 // out = Mix in (per chirality Ls x Ls), all slices
+// the register-tiled form of launch_mix (mix_reg.cu): real matrices whose
+// host copy is in D.mix_host and Ls among the instantiated sizes; false when
+// it does not apply
+bool launch_mix_reg(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
+                    const SolverScalars *st, int gate);
 void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                 const SolverScalars *st = nullptr, int gate = 0);
 

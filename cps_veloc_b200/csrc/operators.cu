@@ -254,6 +254,12 @@ void Dirac::build_mobius(const std::vector<cd> &bs, const std::vector<cd> &cs) {
   auto packm = [&](const std::vector<cd> &up, const std::vector<cd> &dn) {
     return cplx ? pack_complex(ls, up, dn) : pack(ls, up, dn);
   };
+  // uploads keeping the host copy of a real matrix (launch_mix's parameter)
+  mix_host.clear();
+  auto upload = [&](DeviceBuffer &buf, const std::vector<double> &h) {
+    cpsgpu::upload(buf, h);
+    if (!cplx) mix_host[buf.ptr] = h;
+  };
   hM5i = packm(m0u, m0d);
   hM5id = packm(m1u, m1d);
   hB = packm(bu, bd);
@@ -306,6 +312,7 @@ void Dirac::set_pc_type(int pc) {
   if (pc != PC_SYM2 && (cplx || !uniform_bc))
     throw Error(-1, "Mobius preconditioning other than SYM2: real b, c, the same on every slice");
   pc_type = pc;
+  for (const DeviceBuffer &b : pc_bufs) mix_host.erase(b.ptr);
   pc_bufs.clear();
   pc_bufs.reserve(16);
   plan[0] = plan[1] = MobiusPlan();
@@ -356,7 +363,9 @@ void Dirac::set_pc_type(int pc) {
   const Pair R = dr(dl(ckb, mm(Md, Bd)), mkb);     // K M^+ B^+ (-K)
   auto put = [&](const Pair &a) -> const double * {
     pc_bufs.emplace_back();
-    upload(pc_bufs.back(), pack(ls, a.u, a.d));
+    const std::vector<double> h = pack(ls, a.u, a.d);
+    upload(pc_bufs.back(), h);
+    mix_host[pc_bufs.back().ptr] = h;
     return pc_bufs.back().as<double>();
   };
   switch (pc) {

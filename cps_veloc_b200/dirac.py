@@ -632,10 +632,15 @@ class DiracOpMobius(_DiracOp):
         check(lib().cpsgpu_dirac_get_pc_type(self._h, C.byref(v)))
         return v.value
 
-    def set_mix_impl(self, tensor_cores: bool) -> None:
-        """the standalone Ls x Ls mixings of FP16 fields on the tensor cores
-        (True) or the CUDA cores (False, the default)"""
-        check(lib().cpsgpu_set_mix_impl(self._h, 1 if tensor_cores else 0))
+    MIX_REG, MIX_TENSOR_CORES, MIX_SHARED = 0, 1, 2
+
+    def set_mix_impl(self, impl) -> None:
+        """the kernel of the standalone Ls x Ls mixings: MIX_REG (0, the
+        default, register-tiled CUDA cores), MIX_TENSOR_CORES (1, FP16
+        fields on the tensor cores) or MIX_SHARED (2, the shared-memory
+        CUDA-core kernel); True / False mean 1 / 0"""
+        impl = int(impl) if not isinstance(impl, bool) else (1 if impl else 0)
+        check(lib().cpsgpu_set_mix_impl(self._h, impl))
 
     def MatPcDagMatPcShift(self, inp, mu: float, prec: int = A.DOUBLE):
         """DiracOpMobius::MatPcDagMatPcShift (eigen_shift mu): returns

@@ -224,13 +224,19 @@ int cpsgpu_mobius_m5inv(cpsgpu_dirac d, double *out, const double *in, int dag, 
  * hops, which read the operator's own copies (zmobius_dslash_4.C:61-62). */
 int cpsgpu_dirac_set_pc_type(cpsgpu_dirac d, int pc_type);
 int cpsgpu_dirac_get_pc_type(cpsgpu_dirac d, int *pc_type);
-/* No counterpart in the reference: where the Mobius operator applies a
- * standalone Ls x Ls mixing (M5^-1, the first step of MatPc) to an FP16
- * field, tensor_cores = 1 runs it as mma.sync m16n8k16 contractions (FP16
- * operands with the matrix split into high and low parts, FP32
- * accumulation, mix_tc.cu) instead of FP32 FMAs on the CUDA cores (0, the
- * default).  Real b, c and Ls <= 16; other cases keep the CUDA cores. */
-int cpsgpu_set_mix_impl(cpsgpu_dirac d, int tensor_cores);
+/* No counterpart in the reference: the kernel of the Mobius operator's
+ * standalone Ls x Ls mixings (M5^-1, the first step of MatPc).
+ *   0 (the default): for FP32 and FP16 fields, CUDA cores, register-tiled
+ *     (mix_reg.cu): the two real matrices are a kernel parameter, every
+ *     thread computes all Ls output slices of a block of reals (Ls 8, 10,
+ *     12, 16, 20, 24; real b, c); FP64 fields as 2;
+ *   1: for FP16 fields, mma.sync m16n8k16 contractions on the tensor cores
+ *     (FP16 operands with the matrix split into high and low parts, FP32
+ *     accumulation, mix_tc.cu; Ls <= 16, real b, c), else as 0;
+ *   2: CUDA cores, the spinors staged in shared memory (blas.cu), the form
+ *     every case outside the others uses (complex zMobius coefficients,
+ *     other Ls). */
+int cpsgpu_set_mix_impl(cpsgpu_dirac d, int impl);
 
 /* ---- solvers ---- */
 typedef struct {
