@@ -1,11 +1,12 @@
 """The register-tiled Ls x Ls mixing kernel (mix_reg.cu, the default for
-real b, c at Ls 8, 10, 12, 16, 20, 24) against the shared-memory kernel it
-replaced (cpsgpu_set_mix_impl 2) and the oracle.  Both sum the Ls terms of
-every output in the same order with fused multiply-adds and store FP16
-through the same norm rule, so their outputs are bit-identical: M5^-1 and
-its dagger in FP64, FP32 and FP16, several right-hand sides, a checkerboard
-volume that is not a multiple of the 32-site block, and the Mobius
-MatPcDagMatPc and FP16-inner solve built on them."""
+FP32 and FP16 fields with real b, c at Ls 8, 10, 12, 16, 20, 24) against the
+shared-memory kernel it replaced (cpsgpu_set_mix_impl 2) and the oracle.
+Both sum the Ls terms of every output in the same order with fused
+multiply-adds and store FP16 through the same norm rule, so every field
+they write is bit-identical: M5^-1 and its dagger, MatPc, MatPcDag and
+MatPcDagMatPc in FP64, FP32 and FP16, several Ls (and one the kernel does
+not cover), a checkerboard volume that is not a multiple of the 32-site
+block, and a batched FP16-inner solve."""
 import numpy as np
 import pytest
 
@@ -31,7 +32,8 @@ def test_mix_reg_bitwise_and_oracle(oracle, L, ls, prec):
     out = {}
     for impl in (D.MIX_REG, D.MIX_SHARED):
         D.set_mix_impl(impl)
-        out[impl] = [D.M5inv(x, dag, prec=prec) for dag in (0, 1)] + [D.MatPcDagMatPc(x, prec=prec)[0]]
+        out[impl] = ([D.M5inv(x, dag, prec=prec) for dag in (0, 1)] + [D.MatPcDagMatPc(x, prec=prec)[0]]
+                     + [D.MatPc(x, prec=prec), D.MatPcDag(x, prec=prec)])
     for a, b in zip(out[D.MIX_REG], out[D.MIX_SHARED]):
         np.testing.assert_array_equal(a, b)
     tol = {A.DOUBLE: 1e-13, A.SINGLE: 2e-6, A.HALF: 5e-3}[prec]
