@@ -177,6 +177,8 @@ def lib() -> C.CDLL:
             "cpsgpu_dd_face_bytes": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
             "cpsgpu_dslash_dd_pack": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp]),
             "cpsgpu_dslash_dd": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),
+            "cpsgpu_dslash_dd_interior": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+            "cpsgpu_dslash_dd_boundary": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),
             "cpsgpu_field_axpby": (C.c_int, [vp, C.c_double, vp, vp]),
             "cpsgpu_field_dot": (C.c_int, [vp, vp, _dp, _dp]),
             "cpsgpu_mdagm_field": (C.c_int, [vp, vp, vp]),
@@ -186,8 +188,8 @@ def lib() -> C.CDLL:
             "cpsgpu_autotune": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
             "cpsgpu_dirac_set_pc_type": (C.c_int, [vp, C.c_int]),
             "cpsgpu_dirac_get_pc_type": (C.c_int, [vp, C.POINTER(C.c_int)]),
-            "cpsgpu_get_hop_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-            "cpsgpu_set_hop_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "cpsgpu_get_hop_shape": (C.c_int, [vp, C.c_int] + [C.POINTER(C.c_int)] * 4),
+            "cpsgpu_set_hop_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "cpsgpu_time_dslash": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_mdagm": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),
             "cpsgpu_time_m5inv": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp]),

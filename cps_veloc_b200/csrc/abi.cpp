@@ -1324,6 +1324,30 @@ int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, 
   });
 }
 
+int cpsgpu_dslash_dd_interior(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag) {
+  return guarded([&] {
+    if (!d || !out || !in) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+    // enqueued only: the caller moves the faces meanwhile
+    dd_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0, nullptr, nullptr, SUB_INTERIOR);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_dslash_dd_boundary(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag,
+                              const void *from_next, const void *from_prev) {
+  return guarded([&] {
+    if (!d || !out || !in || !from_next || !from_prev) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
+    dd_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0, from_next, from_prev,
+              SUB_BOUNDARY);
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_field_axpby(cpsgpu_field out, double a, cpsgpu_field x, cpsgpu_field y) {
   return guarded([&] {
     if (!out || !x || !y) throw Error(CPSGPU_ERR_ARG, "null argument");
@@ -1506,33 +1530,41 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
   });
 }
 
-int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread) {
+static_assert(CPSGPU_ORDER_SLICES == ORDER_SLICES && CPSGPU_ORDER_SITES == ORDER_SITES && CPSGPU_ORDER_T == ORDER_T,
+              "public and internal hop orders");
+
+int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread, int *order) {
   return guarded([&] {
-    if (!d || !sites || !slices || !slices_per_thread) throw Error(CPSGPU_ERR_ARG, "bad argument");
+    if (!d || !sites || !slices || !slices_per_thread || !order) throw Error(CPSGPU_ERR_ARG, "bad argument");
     check_prec(prec);
     const Dirac &D = *d->D;
-    const dim3 b = hop_block(TuneKey{prec, D.lat->recon(prec), EP_STORE, D.kind, D.ls}, false);
+    const TuneKey key{prec, D.lat->recon(prec), EP_STORE, D.kind, D.ls};
+    const dim3 b = hop_block(key, false);
     *sites = (int)b.x;
     *slices = (int)b.y;
     *slices_per_thread = (b.z == 2 && D.kind == KIND_DWF && prec != PREC_DOUBLE && D.ls % (4 * (int)b.y) == 0) ? 2 : 1;
+    *order = hop_order(key);
     return CPSGPU_OK;
   });
 }
 
-int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread) {
+int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread, int order) {
   return guarded([&] {
     if (!d || sites < 1 || slices < 1 || sites * slices > 256 || sites * slices % 32 != 0 ||
         (slices_per_thread != 1 && slices_per_thread != 2))
       throw Error(CPSGPU_ERR_ARG, "hop shape: sites x slices a multiple of 32 up to 256, 1 or 2 slices per thread");
+    if (order < 0 || order >= ORDER_COUNT) throw Error(CPSGPU_ERR_ARG, "hop order: CPSGPU_ORDER_SLICES, _SITES or _T");
     check_prec(prec);
     const Dirac &D = *d->D;
     if (slices > std::max(D.ls, 1)) throw Error(CPSGPU_ERR_ARG, "hop shape: more slices per block than Ls");
     if (slices_per_thread == 2 && (D.kind != KIND_DWF || prec == PREC_DOUBLE || D.ls % (4 * slices) != 0))
       throw Error(CPSGPU_ERR_ARG, "slice pairs: DWF, FP32 or FP16 fields, Ls a multiple of 4 x slices");
+    if (order == ORDER_T && (D.lat->vh / D.lat->L[3]) % sites != 0)
+      throw Error(CPSGPU_ERR_ARG, "t order: the sites of a block must divide the sites of one t-slice");
     const dim3 b((unsigned)sites, (unsigned)slices, (unsigned)slices_per_thread);
     const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
     CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));
-    for (int ep : eps) tune_set(TuneKey{prec, D.lat->recon(prec), ep, D.kind, D.ls}, b);
+    for (int ep : eps) tune_set(TuneKey{prec, D.lat->recon(prec), ep, D.kind, D.ls}, b, order);
     // captured graphs hold the launches of the old shape
     for (auto &s : d->solvers) s.reset();
     d->D->ms.refine.reset();

@@ -1,8 +1,9 @@
 // Autotuner: times candidate block shapes of the hop kernels on the live
 // lattice and records the fastest in the launch table (tune.cpp).  A shape
-// is (sites per block) x (slices per block) x (slices per thread, DWF); the mixing epilogue of the
-// Mobius operator needs all slices of a site in one block, so only its
-// site count varies.
+// is (sites per block) x (slices per block) x (slices per thread, DWF),
+// then the block traversal order (HopOrder) at the fastest of them; the
+// mixing epilogue of the Mobius operator needs all slices of a site in one
+// block, so only its site count varies.
 #include <vector>
 
 #include "cpsgpu_impl.h"
@@ -55,11 +56,13 @@ int autotune(Dirac &D, int prec, int nrhs) {
     Lh.ep = EP_STORE;
     Lh.cb = 1;
     std::vector<dim3> cand;
-    const int bxs[] = {16, 32, 64, 128, 256};
+    // 8 or 16 sites per block: a warp spans 4 or 2 same-parity slices of
+    // the same sites, whose lanes then read the same link addresses
+    const int bxs[] = {8, 16, 32, 64, 128, 256};
     const int bss[] = {1, 2, 4, 8, 16};
     for (int bx : bxs)
       for (int bs : bss)
-        if (bx * bs <= 256 && bx * bs >= 64 && bs <= (D.ls > 1 ? D.ls : 1)) {
+        if (bx * bs <= 256 && bx * bs >= (bx == 8 ? 32 : 64) && bs <= (D.ls > 1 ? D.ls : 1)) {
           cand.push_back(dim3(bx, bs));
           // DWF slice pairs: two same-parity slices per thread sharing links
           if (D.kind == KIND_DWF && prec != PREC_DOUBLE && D.ls % (4 * bs) == 0) cand.push_back(dim3(bx, bs, 2));
@@ -72,9 +75,18 @@ int autotune(Dirac &D, int prec, int nrhs) {
       float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
       if (t < best) { best = t; bestb = b; }
     }
+    // then the order in which the blocks of that shape take the lattice
+    int besto = ORDER_SLICES;
+    const long face = L.vh / L.L[3];
+    for (int o = ORDER_SITES; o < ORDER_COUNT; o++) {
+      if (o == ORDER_T && face % bestb.x != 0) continue;
+      tune_set(key, bestb, o);
+      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
+      if (t < best) { best = t; besto = o; }
+    }
     const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
     for (int ep : eps) {
-      tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb);
+      tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb, besto);
       tuned++;
     }
     if (prec != PREC_DOUBLE) {

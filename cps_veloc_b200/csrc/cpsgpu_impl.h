@@ -202,6 +202,7 @@ struct HopLaunch {
   const double *mix = nullptr;
   std::vector<double> coef;  // per slice
   const void *halo_fwd = nullptr, *halo_bwd = nullptr;  // t halos of a decomposed lattice (dd.cu)
+  int sub = 0;  // HopSub: all sites, or (decomposed lattice) the interior or the two t-end slices
   double *partials = nullptr;  // the reduction's per-block partials (null: the lattice's buffer)
 };
 void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const SpinorView &out,
@@ -288,8 +289,10 @@ struct RitzArgs {
 // t-slab domain decomposition (dd.cu)
 size_t dd_face_bytes(const Dirac &D, int prec, int nrhs);
 void dd_pack(const Dirac &D, int prec, const SpinorView &in, int cb, int dag, void *to_prev, void *to_next);
+// sub: 0 every site, 1 the interior t-slices (no halos read; may run while
+// the faces move), 2 the first and last t-slices (reading the halos)
 void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
-               const void *from_next, const void *from_prev);
+               const void *from_next, const void *from_prev, int sub = 0);
 void field_dot(Lattice &L, const SpinorView &a, const SpinorView &b, double *re, double *im);
 
 // low-mode deflation (lowmode.cu)

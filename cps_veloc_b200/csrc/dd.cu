@@ -14,7 +14,10 @@
 // to_next to the next rank (its from_prev), by NCCL, peer copies or MPI;
 // the hop kernel then reads them at its t ends (hop.cuh).  The lattice's
 // antiperiodic t sign applies only at the slab ends that are the lattice's
-// own boundary.
+// own boundary.  To overlap the exchange with the hop, the interior
+// t-slices (which read no halo) can be launched before the faces arrive
+// and the two end slices after (the wilson_dslash_vec split of local and
+// non-local parts, wilson_dslash_vec.C:184-278).
 #include <cstring>
 
 #include "cpsgpu_impl.h"
@@ -110,8 +113,9 @@ void dd_pack(const Dirac &D, int prec, const SpinorView &in, int cb, int dag, vo
 }
 
 void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
-               const void *from_next, const void *from_prev) {
+               const void *from_next, const void *from_prev, int sub) {
   check_dd(D, prec);
+  if (sub < SUB_ALL || sub > SUB_BOUNDARY) throw Error(-1, "bad site subset");
   HopLaunch L;
   L.prec = prec;
   L.ep = EP_STORE;
@@ -119,6 +123,7 @@ void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView
   L.dag = dag;
   L.halo_fwd = from_next;
   L.halo_bwd = from_prev;
+  L.sub = sub;
   launch_hop(D, L, in, out, SpinorView(), SpinorView(), SpinorView(), SpinorView(), SpinorView(), nullptr);
 }
 

@@ -325,6 +325,32 @@ template <> struct Chunk4<PREC_HALF> {
   }
 };
 
+// Chunk-by-chunk reads of one site of a field (chunks 0..5 in order, as the
+// fused epilogues stream them): the FP16 form loads the site's norm once and
+// each 16-byte group once for its two chunks, where Chunk4 would load a norm
+// and half a group per chunk.  The values are Chunk4's.
+template <int P> struct ChunkReader {
+  const SpinorView &f;
+  long sl, i;
+  __device__ __forceinline__ ChunkReader(const SpinorView &f_, long sl_, long i_) : f(f_), sl(sl_), i(i_) {}
+  __device__ __forceinline__ void get(int c, typename PrecTraits<P>::real *v) { Chunk4<P>::load(f, sl, i, c, v); }
+};
+template <> struct ChunkReader<PREC_HALF> {
+  const uint4 *d;
+  long vh;
+  float s;
+  uint4 q;
+  __device__ __forceinline__ ChunkReader(const SpinorView &f, long sl, long i)
+      : d(reinterpret_cast<const uint4 *>(f.data) + sl * 3 * f.vh + i), vh(f.vh), s(__ldg(f.norm + sl * f.vh + i)) {}
+  // c in increasing order; an even c loads the group, the odd one reuses it
+  __device__ __forceinline__ void get(int c, float *v) {
+    if ((c & 1) == 0) q = __ldg(d + (c >> 1) * vh);
+    const __half2 *h = reinterpret_cast<const __half2 *>(&q) + 2 * (c & 1);
+    const float2 a = __half22float2(h[0]), b = __half22float2(h[1]);
+    v[0] = a.x * s; v[1] = a.y * s; v[2] = b.x * s; v[3] = b.y * s;
+  }
+};
+
 // ---- gauge links ----
 template <int P, int RECON> struct LinkIO;
 

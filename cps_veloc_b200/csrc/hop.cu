@@ -113,11 +113,15 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   hp.face = (int)(lat.vh / lat.L[3]);
   hp.tb_fwd = (lat.t_coor == lat.t_nodes - 1) ? 1 : 0;
   hp.tb_bwd = (lat.t_coor == 0) ? 1 : 0;
-  const bool halo = (lat.t_nodes > 1);
+  const bool split = (lat.t_nodes > 1);
+  if (!split && L.sub != SUB_ALL) throw Error(-4, "interior / boundary hops: a t-partitioned lattice");
+  // the interior of a slab reads no halo: the undecomposed kernel serves it
+  const bool halo = split && L.sub != SUB_INTERIOR;
   if (halo && (!L.halo_fwd || !L.halo_bwd))
     throw Error(-1, "t-partitioned lattice: only the decomposed dslash (with its halos) applies the operator");
-  if (halo && (L.ep != EP_STORE || (L.prec != PREC_DOUBLE && L.prec != PREC_SINGLE)))
+  if (split && (L.ep != EP_STORE || (L.prec != PREC_DOUBLE && L.prec != PREC_SINGLE)))
     throw Error(-2, "decomposed hop: store epilogue, FP64 or FP32");
+  hp.sub = L.sub;
 
   HopViews v;
   v.U = lat.gauge(L.prec);
@@ -140,8 +144,23 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   block.z = 1;
   g_dag = (L.dag != 0);
   HopFn fn = halo ? pick_halo(L.prec, recon) : pick(L.prec, recon, L.ep, L.pr, L.px);
-  const unsigned nsb = (unsigned)((lat.vh + block.x - 1) / block.x);
+  unsigned nsb;
+  if (L.sub == SUB_BOUNDARY) {
+    hp.subn = (hp.face + (int)block.x - 1) / (int)block.x;
+    nsb = 2u * (unsigned)hp.subn;
+  } else {
+    const long nsites = (L.sub == SUB_INTERIOR) ? lat.vh - 2L * hp.face : lat.vh;
+    if (nsites <= 0) return;  // a slab of two t-slices has no interior
+    nsb = (unsigned)((nsites + block.x - 1) / block.x);
+  }
   hp.nsg = g_ns == 2 ? D.ls / (2 * (int)block.y) : (D.ls + block.y - 1) / block.y;
+  hp.nsb = (int)nsb;
+  hp.sorder = hop_order(key);
+  if (hp.sorder == ORDER_T) {
+    // t fastest needs whole t-slices of site blocks: not the split launches
+    if (L.sub == SUB_ALL && hp.face % block.x == 0) hp.tper = hp.face / (int)block.x;
+    else hp.sorder = ORDER_SLICES;
+  }
   hp.spar = (hp.dwf && !mix && block.y > 1 && D.ls % (2 * block.y) == 0) ? 1 : 0;
   hp.nrhs = in.nrhs;
   hp.rtile = std::max(1, std::min(D.rhs_tile(L.prec, in.nrhs), in.nrhs));

@@ -69,13 +69,22 @@ struct FastDiv {
   }
 };
 
+enum HopSub { SUB_ALL = 0, SUB_INTERIOR = 1, SUB_BOUNDARY = 2 };
+
 struct HopParams {
   int L[4];
   int hx;           // L[0] / 2
   long vh;          // checkerboard volume
   int ls;
   FastDiv dhx, dly, dlz;  // divisions by L[0]/2, L[1], L[2]
-  int nsg;          // slice groups in the launch (grid is site-block major, slice-group minor)
+  int nsg;          // slice groups in the launch
+  int nsb;          // site blocks in the launch
+  int sorder;       // HopOrder: how blockIdx.x maps to (site block, slice group)
+  int tper;         // ORDER_T: site blocks per t-slice
+  // HopSub: SUB_ALL every site; SUB_INTERIOR the t-slices 1 .. L[3]-2 of a
+  // slab (their hops need no halo); SUB_BOUNDARY its first and last
+  // t-slices, subn site blocks each
+  int sub, subn;
   int rtile;        // right-hand sides per tile: consecutive blocks take the same sites of rtile solves
   int nrhs;         // right-hand sides in the launch
   double bc[4];     // boundary sign per direction
@@ -310,10 +319,11 @@ __device__ __forceinline__ void hop_epilogue(const HopParams &hp, const HopViews
     RA n_out = RA(0), n_x = RA(0);
     if (active) {
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
+      ChunkReader<P> xr(v.x, sl, i);
 #pragma unroll
       for (int c = 0; c < 6; c++) {
         R xv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
+        xr.get(c, xv);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           if (hp.norm) n_x += xv[k] * xv[k];
@@ -339,13 +349,15 @@ __device__ __forceinline__ void hop_epilogue(const HopParams &hp, const HopViews
       const RX ax = RX(alpha);
       const bool with_sol = (v.sol.data != nullptr);  // the multishift solver keeps its own solutions
       RR rfull[PR == PREC_HALF ? 24 : 1];
+      ChunkReader<P> xr(v.x, sl, i);
+      ChunkReader<PR> pr(v.p, sl, i), rr(v.r, sl, i);
 #pragma unroll
       for (int c = 0; c < 6; c++) {
         R xv[4];
         RR pv[4], rv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
-        Chunk4<PR>::load(v.p, sl, i, c, pv);
-        Chunk4<PR>::load(v.r, sl, i, c, rv);
+        xr.get(c, xv);
+        pr.get(c, pv);
+        rr.get(c, rv);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           R q = xv[k] + cf * acc[4 * c + k] + sh * R(pv[k]);
@@ -376,12 +388,13 @@ __device__ __forceinline__ void hop_epilogue(const HopParams &hp, const HopViews
       const R cf = ep_mix(EP) ? R(1) : R(hp.coef[s]);
       const R sh = R(st[rhs].shift);
       RR rfull[PR == PREC_HALF ? 24 : 1];
+      ChunkReader<P> xr(v.x, sl, i), br(v.b, sl, i), sr(v.sol, sl, i);
 #pragma unroll
       for (int c = 0; c < 6; c++) {
         R xv[4], bv[4], sv[4];
-        Chunk4<P>::load(v.x, sl, i, c, xv);
-        Chunk4<P>::load(v.b, sl, i, c, bv);
-        Chunk4<P>::load(v.sol, sl, i, c, sv);
+        xr.get(c, xv);
+        br.get(c, bv);
+        sr.get(c, sv);
         RR rv[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -441,12 +454,31 @@ __global__ void __launch_bounds__(256, (hop_min_blocks<P, NS>())) hop_kernel(con
   if (hp.gate == GATE_RELIABLE && (st[rhs].done || !st[rhs].reliable)) return;
   const unsigned nblk = gridDim.x / hp.rtile;  // blocks of one solve
 
-  const int sgrp = sb % hp.nsg, sblk = sb / hp.nsg;
-  const int i = sblk * blockDim.x + threadIdx.x;
+  int sgrp, sblk;
+  if (hp.sorder == 1) {  // ORDER_SITES
+    sblk = sb % hp.nsb;
+    sgrp = sb / hp.nsb;
+  } else {
+    sgrp = sb % hp.nsg;
+    sblk = sb / hp.nsg;
+    if (hp.sorder == 2) {  // ORDER_T: the q-th site block taken is block q / L_t of t-slice q % L_t
+      const int nt = hp.nsb / hp.tper;
+      sblk = (sblk % nt) * hp.tper + sblk / nt;
+    }
+  }
+  int i = sblk * blockDim.x + threadIdx.x;
+  int iend = (int)hp.vh;
+  if (hp.sub == SUB_INTERIOR) {
+    i += hp.face;
+    iend -= hp.face;
+  } else if (hp.sub == SUB_BOUNDARY) {
+    if (sblk < hp.subn) iend = hp.face;
+    else i = iend - hp.face + (sblk - hp.subn) * (int)blockDim.x + (int)threadIdx.x;
+  }
   const int s = NS == 2 ? (sgrp >> 1) * 4 * (int)blockDim.y + (sgrp & 1) + 4 * (int)threadIdx.y
                 : hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y
                           : sgrp * (int)blockDim.y + (int)threadIdx.y;
-  const bool active = (i < hp.vh) && (s + 2 * (NS - 1) < hp.ls);
+  const bool active = (i < iend) && (s + 2 * (NS - 1) < hp.ls);
   const long sl = rhs * hp.ls + s;
   const int pin = hp.dwf ? ((s + hp.cb) & 1) : hp.cb;
   const int pout = 1 - pin;

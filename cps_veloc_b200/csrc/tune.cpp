@@ -7,14 +7,19 @@ namespace cpsgpu {
 
 namespace {
 std::mutex g_mu;
-std::vector<std::pair<TuneKey, dim3>> g_table;
+struct Entry {
+  TuneKey key;
+  dim3 block;
+  int order;
+};
+std::vector<Entry> g_table;
 }  // namespace
 
 dim3 hop_block(const TuneKey &k, bool mix) {
   {
     std::lock_guard<std::mutex> lk(g_mu);
     for (auto &e : g_table)
-      if (e.first == k) return e.second;
+      if (e.key == k) return e.block;
   }
   if (mix) {
     // a block holds every slice of its sites
@@ -29,14 +34,22 @@ dim3 hop_block(const TuneKey &k, bool mix) {
   return dim3(32, bs);
 }
 
-void tune_set(const TuneKey &k, dim3 block) {
+int hop_order(const TuneKey &k) {
   std::lock_guard<std::mutex> lk(g_mu);
   for (auto &e : g_table)
-    if (e.first == k) {
-      e.second = block;
+    if (e.key == k) return e.order;
+  return ORDER_SLICES;
+}
+
+void tune_set(const TuneKey &k, dim3 block, int order) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto &e : g_table)
+    if (e.key == k) {
+      e.block = block;
+      e.order = order;
       return;
     }
-  g_table.push_back({k, block});
+  g_table.push_back({k, block, order});
 }
 
 void tune_clear() {

@@ -2,7 +2,9 @@
 // shapes below; the autotuner (autotune.cu, exposed as cpsgpu_autotune)
 // times candidate shapes on the live lattice and records the fastest per
 // key.  A shape is (sites per block, slices per block, slices per thread):
-// z = 2 selects the DWF slice-pair kernel where Ls allows it.
+// z = 2 selects the DWF slice-pair kernel where Ls allows it; with it goes
+// the order in which the grid's blocks traverse the (site block, slice
+// group) pairs (HopOrder).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -15,8 +17,19 @@ struct TuneKey {
   }
 };
 
+// block traversal orders of a hop launch: consecutive blocks take
+//   ORDER_SLICES: the slice groups of one site block (its links stay in L1);
+//   ORDER_SITES:  the site blocks of one slice group, in lexicographic order;
+//   ORDER_T:      the slice groups of one site block, the site blocks taken
+//                 t-slice fastest (the blocks in flight at once cover all t
+//                 of a few spatial rows, so t neighbours are read while
+//                 still in L2); needs a whole number of site blocks per
+//                 t-slice, else ORDER_SLICES runs
+enum HopOrder { ORDER_SLICES = 0, ORDER_SITES = 1, ORDER_T = 2, ORDER_COUNT = 3 };
+
 dim3 hop_block(const TuneKey &k, bool mix);
-void tune_set(const TuneKey &k, dim3 block);
+int hop_order(const TuneKey &k);
+void tune_set(const TuneKey &k, dim3 block, int order = ORDER_SLICES);
 void tune_clear();
 int tune_count();
 

@@ -10,6 +10,13 @@ links; ``set_t_partition`` marks it.  One decomposed dslash is
     exchange_faces(faces)                 # to the neighbouring ranks
     dslash(D, out, inp, cb, dag, faces)   # the hop, reading the halos
 
+or, with the exchange overlapped by the interior t-slices' hop,
+
+    pack(D, inp, cb, dag, faces)
+    dslash_interior(D, out, inp, cb, dag)          # enqueued, not waited for
+    exchange_faces(faces)
+    dslash_boundary(D, out, inp, cb, dag, faces)   # the two end t-slices
+
 The faces are device buffers (torch uint8 tensors on the rank's GPU, only
 plumbing); ``exchange_faces`` moves them with torch.distributed
 point-to-point operations (NCCL between GPUs).
@@ -83,6 +90,19 @@ def dslash(D, out: DeviceField, inp: DeviceField, cb: int, dag: int, faces: Face
                                  C.c_void_p(faces.from_prev.data_ptr())))
 
 
+def dslash_interior(D, out: DeviceField, inp: DeviceField, cb: int, dag: int) -> None:
+    """the hop into the slab's interior t-slices (no halo read), enqueued
+    on the library's stream: the device computes it while the faces move"""
+    check(lib().cpsgpu_dslash_dd_interior(D._h, out._h, inp._h, cb, dag))
+
+
+def dslash_boundary(D, out: DeviceField, inp: DeviceField, cb: int, dag: int, faces: Faces) -> None:
+    """the hop into the slab's first and last t-slices from the received
+    faces; returns when the interior part has finished too"""
+    check(lib().cpsgpu_dslash_dd_boundary(D._h, out._h, inp._h, cb, dag, C.c_void_p(faces.from_next.data_ptr()),
+                                          C.c_void_p(faces.from_prev.data_ptr())))
+
+
 # point-to-point tags of the two face streams
 TAG_TO_PREV, TAG_TO_NEXT = 17, 18
 
@@ -129,7 +149,8 @@ class InProcessRing:
         for r in range(n):
             faces[r].from_next.copy_(faces[(r + 1) % n].to_prev)
             faces[r].from_prev.copy_(faces[(r - 1) % n].to_next)
-        torch.cuda.synchronize()
+        # torch's stream only: an interior hop on the library's stream runs on
+        torch.cuda.current_stream().synchronize()
 
     def allreduce(self, v: complex) -> complex:
         return v
@@ -157,15 +178,18 @@ class DistRing:
         if len(faces) != 1:
             raise ValueError("one slab per rank")
         f = faces[0]
+        # the pack call returned after its kernels, so the faces are ready;
+        # only torch's stream is waited for, not an interior hop in flight
+        # on the library's stream
         if dist.get_backend(self.group) == "nccl" or not f.to_prev.is_cuda:
             exchange_faces(f, self.group)
         else:
-            torch.cuda.synchronize()  # the pack kernels ran on the library's stream
             h = _HostFaces(f)
             exchange_faces(h, self.group)
             f.from_next.copy_(h.from_next)
             f.from_prev.copy_(h.from_prev)
-        torch.cuda.synchronize()
+        if f.to_prev.is_cuda:
+            torch.cuda.current_stream().synchronize()
 
     def allreduce(self, v: complex) -> complex:
         # NCCL reduces device tensors only; gloo (the CPU tests) host tensors
@@ -182,8 +206,8 @@ class DDOperator:
     ops holds this process's slabs' DiracOps, ring moves faces and adds
     the ranks' parts of a dot product"""
 
-    def __init__(self, ops, ring):
-        self.ops, self.ring = list(ops), ring
+    def __init__(self, ops, ring, overlap=True):
+        self.ops, self.ring, self.overlap = list(ops), ring, overlap
         self.faces = [Faces(D) for D in self.ops]
         self.t1 = self.field()
         self.t2 = self.field()
@@ -194,6 +218,14 @@ class DDOperator:
     def dslash(self, out, inp, cb, dag):
         for D, i, f in zip(self.ops, inp, self.faces):
             pack(D, i, cb, dag, f)
+        if self.overlap:
+            # interior t-slices on the device while the faces move
+            for D, o, i in zip(self.ops, out, inp):
+                dslash_interior(D, o, i, cb, dag)
+            self.ring.exchange(self.faces)
+            for D, o, i, f in zip(self.ops, out, inp, self.faces):
+                dslash_boundary(D, o, i, cb, dag, f)
+            return
         self.ring.exchange(self.faces)
         for D, o, i, f in zip(self.ops, out, inp, self.faces):
             dslash(D, o, i, cb, dag, f)

@@ -576,14 +576,18 @@ class _DiracOp:
     def set_rhs_tile(self, prec: int, tile: int) -> None:
         check(lib().cpsgpu_set_rhs_tile(self._h, prec, tile))
 
-    def hop_shape(self, prec=A.DOUBLE) -> tuple:
-        """(sites, slices, slices per thread) of the non-mixing hop launches"""
-        a, b, c = C.c_int(), C.c_int(), C.c_int()
-        check(lib().cpsgpu_get_hop_shape(self._h, prec, C.byref(a), C.byref(b), C.byref(c)))
-        return a.value, b.value, c.value
+    # block traversal orders of the hop launches (cpsgpu_set_hop_shape)
+    ORDER_SLICES, ORDER_SITES, ORDER_T = 0, 1, 2
 
-    def set_hop_shape(self, prec: int, sites: int, slices: int, slices_per_thread: int = 1) -> None:
-        check(lib().cpsgpu_set_hop_shape(self._h, prec, sites, slices, slices_per_thread))
+    def hop_shape(self, prec=A.DOUBLE) -> tuple:
+        """(sites, slices, slices per thread, order) of the non-mixing hop launches"""
+        a, b, c, o = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().cpsgpu_get_hop_shape(self._h, prec, C.byref(a), C.byref(b), C.byref(c), C.byref(o)))
+        return a.value, b.value, c.value, o.value
+
+    def set_hop_shape(self, prec: int, sites: int, slices: int, slices_per_thread: int = 1,
+                      order: int = 0) -> None:
+        check(lib().cpsgpu_set_hop_shape(self._h, prec, sites, slices, slices_per_thread, order))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -32,7 +32,8 @@ def main(argv=None) -> int:
     ap.add_argument("--link-reals", type=int, default=0,
                     help="link form of the FP32/FP16 operators (12, 18, 112, 118; 0: default or autotuned)")
     ap.add_argument("--shape", default="",
-                    help="sites,slices,slices_per_thread of the hop launches (overrides the autotuner)")
+                    help="sites,slices,slices_per_thread[,order] of the hop launches (overrides the autotuner; "
+                         "order 0 slices, 1 sites, 2 t)")
     ap.add_argument("--dd", type=int, default=0,
                     help="time the t-slab decomposed dslash over this many slabs (one process; see time_dd)")
     args = ap.parse_args(argv)
@@ -121,12 +122,23 @@ def time_dd(args, L) -> int:
             for lat, D, a, b, f in slabs:
                 dd.dslash(D, b, a, 0, 0, f)
 
+        def one_dd_overlap():
+            for lat, D, a, b, f in slabs:
+                dd.pack(D, a, 0, 0, f)
+                dd.dslash_interior(D, b, a, 0, 0)
+            for r in range(n):
+                slabs[r][4].from_next.copy_(slabs[(r + 1) % n][4].to_prev)
+                slabs[r][4].from_prev.copy_(slabs[(r - 1) % n][4].to_next)
+            torch.cuda.current_stream().synchronize()
+            for lat, D, a, b, f in slabs:
+                dd.dslash_boundary(D, b, a, 0, 0, f)
+
         def one_full():
             A.check(A.lib().cpsgpu_dslash_field(Df._h, fo._h, fi._h, 0, 0))
             torch.cuda.synchronize()
 
         res = {}
-        for name, fn in (("whole", one_full), ("dd", one_dd)):
+        for name, fn in (("whole", one_full), ("dd", one_dd), ("dd_overlap", one_dd_overlap)):
             for _ in range(3):
                 fn()
             t0 = time.perf_counter()
@@ -135,7 +147,8 @@ def time_dd(args, L) -> int:
             res[name] = (time.perf_counter() - t0) / args.reps * 1e3
         nbytes = slabs[0][4].to_prev.numel()
         print(f"prec {prec}: {n} slabs, whole-lattice dslash {res['whole']:.4f} ms, decomposed {res['dd']:.4f} ms "
-              f"(ratio {res['dd'] / res['whole']:.2f}), {4 * nbytes * n} face bytes moved per dslash")
+              f"(ratio {res['dd'] / res['whole']:.2f}), interior / boundary split {res['dd_overlap']:.4f} ms, "
+              f"{4 * nbytes * n} face bytes moved per dslash")
     return 0
 
 

@@ -542,6 +542,17 @@ int cpsgpu_dd_face_bytes(cpsgpu_dirac d, int precision, int nrhs, size_t *bytes)
 int cpsgpu_dslash_dd_pack(cpsgpu_dirac d, cpsgpu_field in, int cb, int dag, void *to_prev, void *to_next);
 int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag, const void *from_next,
                      const void *from_prev);
+/* cpsgpu_dslash_dd in two parts, so that the faces move while the device
+ * computes (the local / non-local split of wilson_dslash_vec,
+ * wilson_dslash_vec.C:184-278): _interior applies the hop to the slab's
+ * t-slices 1 .. Lt-2, which read no halo, and returns as soon as it is
+ * enqueued on lat's stream (call it after cpsgpu_dslash_dd_pack, before
+ * the exchange); _boundary then applies it to the first and last t-slices,
+ * reading the received faces, and returns once both parts have finished.
+ * Together they write what cpsgpu_dslash_dd writes, bit for bit. */
+int cpsgpu_dslash_dd_interior(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag);
+int cpsgpu_dslash_dd_boundary(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, int dag,
+                              const void *from_next, const void *from_prev);
 /* BLAS-1 on FP64 device fields (vector_util.C:727-922): out = a x + y
  * (fTimesV1PlusV2), and this rank's part of <a, b> = sum conj(a) b
  * (compDotProduct without its global sum: a decomposed solver adds the
@@ -581,11 +592,17 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile);
  * consecutive checkerboard sites x `slices` slices per block, and
  * `slices_per_thread` 1 or 2 (2: DWF at FP32 arithmetic, Ls a multiple of
  * 4 * slices — each thread computes two same-parity slices with shared
- * links).  get returns the shape in use; set overrides the autotuner.  The
- * shape table (like the autotuner's) is shared by every operator of the same
- * kind, Ls, precision and link form. */
-int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread);
-int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread);
+ * links), and the site order in which the grid's blocks take the lattice:
+ * CPSGPU_ORDER_SLICES (consecutive blocks: every slice group of one block
+ * of sites), CPSGPU_ORDER_SITES (consecutive blocks: the site blocks of one
+ * slice group, lexicographically), CPSGPU_ORDER_T (as SLICES, the site
+ * blocks taken t-slice fastest; needs `sites` to divide the sites of one
+ * t-slice of a checkerboard).  get returns the shape in use; set overrides
+ * the autotuner.  The shape table (like the autotuner's) is shared by every
+ * operator of the same kind, Ls, precision and link form. */
+enum { CPSGPU_ORDER_SLICES = 0, CPSGPU_ORDER_SITES = 1, CPSGPU_ORDER_T = 2 };
+int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread, int *order);
+int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread, int order);
 
 /* ---- measurement ----
  * Time `reps` back-to-back launches of the operator's hop kernel

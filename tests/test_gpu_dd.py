@@ -41,9 +41,13 @@ def _make(kind, lat, mass, ls):
 
 
 @pytest.mark.parametrize("kind,L,ls,nodes", [("wilson", (4, 4, 4, 8), 1, 2), ("dwf", (4, 4, 4, 8), 4, 2),
-                                             ("wilson", (4, 4, 2, 12), 1, 3)])
+                                             ("wilson", (4, 4, 2, 12), 1, 3), ("dwf", (4, 4, 4, 4), 4, 2),
+                                             ("wilson", (8, 4, 4, 12), 1, 2)])
 @pytest.mark.parametrize("prec", [A.DOUBLE, A.SINGLE])
 def test_dd_dslash_matches_whole_lattice(oracle, kind, L, ls, nodes, prec):
+    """also: the interior / boundary split (the overlapped form) writes the
+    single decomposed launch's output bit for bit, slabs of two t-slices
+    (no interior) included"""
     mass = 0.1
     u = gen_gauge(L, seed=501)
     full = Lattice(L)
@@ -57,22 +61,26 @@ def test_dd_dslash_matches_whole_lattice(oracle, kind, L, ls, nodes, prec):
         lat.import_gauge(_slab_gauge(u, L, nodes, r))
         dd.set_t_partition(lat, nodes, r)
         D = _make(kind, lat, mass, ls)
-        slabs.append((lat, D, dd.DeviceField(D, prec), dd.DeviceField(D, prec), dd.Faces(D, prec)))
+        slabs.append((lat, D, dd.DeviceField(D, prec), dd.DeviceField(D, prec), dd.Faces(D, prec),
+                      dd.DeviceField(D, prec)))
     ops = OracleOps(oracle, L, u, ls=ls)
     x = gen_gaussian(Dfull.f_size, seed=502)
     for cb in (0, 1):
         for dag in (0, 1):
-            for r, (lat, D, fin, fout, fc) in enumerate(slabs):
+            for r, (lat, D, fin, fout, fc, fsplit) in enumerate(slabs):
                 fin.upload(_slab_vec(x, L, ls, nodes, r))
                 dd.pack(D, fin, cb, dag, fc)
+                dd.dslash_interior(D, fsplit, fin, cb, dag)
             for r in range(nodes):  # the transport: faces to the neighbouring slabs (periodic)
                 slabs[r][4].from_next.copy_(slabs[(r + 1) % nodes][4].to_prev)
                 slabs[r][4].from_prev.copy_(slabs[(r - 1) % nodes][4].to_next)
             torch.cuda.synchronize()
             parts = []
-            for lat, D, fin, fout, fc in slabs:
+            for lat, D, fin, fout, fc, fsplit in slabs:
                 dd.dslash(D, fout, fin, cb, dag, fc)
                 parts.append(fout.download())
+                dd.dslash_boundary(D, fsplit, fin, cb, dag, fc)
+                np.testing.assert_array_equal(fsplit.download(), parts[-1])
             y = _join(parts, L, ls)
             whole = Dfull.Dslash(x, cb, dag, prec)
             tol = 1e-14 if prec == A.DOUBLE else 1e-6
@@ -121,12 +129,18 @@ def test_dd_cg_matches_whole_lattice_solve(kind, L, ls, nodes):
         lat.import_gauge(_slab_gauge(u, L, nodes, k))
         dd.set_t_partition(lat, nodes, k)
         ops.append((lat, _make(kind, lat, mass, ls)))
-    op = dd.DDOperator([D for _, D in ops], dd.InProcessRing())
-    bs, xs = op.field(), op.field()
-    for k, (fb, fx) in enumerate(zip(bs, xs)):
-        fb.upload(_slab_vec(b, L, ls, nodes, k))
-        fx.upload(np.zeros(fx.D.f_size))
-    it, tr = dd.cg(op, xs, bs, stop_rsd=1e-11)
-    y = _join([f.download() for f in xs], L, ls)
-    assert abs(it - r.iterations) <= 1 and tr < 1e-11
-    assert rel(y, x) < 1e-9
+    sols = {}
+    for overlap in (True, False):
+        op = dd.DDOperator([D for _, D in ops], dd.InProcessRing(), overlap=overlap)
+        bs, xs = op.field(), op.field()
+        for k, (fb, fx) in enumerate(zip(bs, xs)):
+            fb.upload(_slab_vec(b, L, ls, nodes, k))
+            fx.upload(np.zeros(fx.D.f_size))
+        it, tr = dd.cg(op, xs, bs, stop_rsd=1e-11)
+        y = _join([f.download() for f in xs], L, ls)
+        assert abs(it - r.iterations) <= 1 and tr < 1e-11
+        assert rel(y, x) < 1e-9
+        sols[overlap] = (it, y)
+    # the overlapped operator is the same operator, bit for bit
+    assert sols[True][0] == sols[False][0]
+    np.testing.assert_array_equal(sols[True][1], sols[False][1])

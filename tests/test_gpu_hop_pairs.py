@@ -44,7 +44,7 @@ def test_pairs_bitwise_against_single_slices(oracle, prec, reals, L, ls, shape):
     out = {}
     for ns in (1, 2):
         D.set_hop_shape(prec, bx, bs, ns)
-        assert D.hop_shape(prec) == (bx, bs, ns)
+        assert D.hop_shape(prec) == (bx, bs, ns, D.ORDER_SLICES)
         res = {}
         for cb in (0, 1):
             for dag in (0, 1):
