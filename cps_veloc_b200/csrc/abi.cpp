@@ -76,6 +76,18 @@ struct cpsgpu_field_s {
 };
 
 namespace {
+// the operator's instantiated graphs (CG solvers, the multishift loop and its
+// refinement) hold the launches of the form they were captured for: after a
+// change of matrices, kernels or launch shapes they are captured again
+void drop_captured(cpsgpu_dirac_s *d) {
+  for (auto &s : d->solvers) s.reset();
+  d->D->ms.refine.reset();
+  d->D->ms.refine_n = 0;
+  d->D->ms.loop.drop();
+}
+}  // namespace
+
+namespace {
 thread_local std::string g_err;
 
 int fail(int code, const std::string &msg) {
@@ -410,7 +422,7 @@ int cpsgpu_dirac_set_zmobius(cpsgpu_dirac d, const double *b, const double *c) {
     }
     CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));  // no launch may still read the old matrices
     D.build_mobius(bs, cs);
-    for (auto &s : d->solvers) s.reset();  // captured graphs hold the old matrices
+    drop_captured(d);  // captured graphs hold the old matrices
     return CPSGPU_OK;
   });
 }
@@ -1453,9 +1465,7 @@ int cpsgpu_dirac_set_pc_type(cpsgpu_dirac d, int pc_type) {
       throw Error(CPSGPU_ERR_ARG, e.what());
     }
     // captured graphs hold the launches of the old form
-    for (auto &s : d->solvers) s.reset();
-    d->D->ms.refine.reset();
-    d->D->ms.refine_n = 0;
+    drop_captured(d);
     return CPSGPU_OK;
   });
 }
@@ -1479,9 +1489,7 @@ int cpsgpu_set_mix_impl(cpsgpu_dirac d, int impl) {
     // allocated here, never inside a graph capture
     if (d->D->mix_tc) d->D->mixTcFrag.ensure(2 * 2 * 32 * 4 * sizeof(unsigned));
     // captured graphs hold the other kernels
-    for (auto &s : d->solvers) s.reset();
-    d->D->ms.refine.reset();
-    d->D->ms.refine_n = 0;
+    drop_captured(d);
     return CPSGPU_OK;
   });
 }
@@ -1491,6 +1499,8 @@ int cpsgpu_autotune(cpsgpu_dirac d, int prec, int nrhs, int *tuned) {
     if (!d || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
     check_prec(prec);
     need_gauge(d);
+    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    drop_captured(d);  // recaptured with the tuned shapes and link form
     int n = autotune(*d->D, prec, nrhs);
     if (tuned) *tuned = n;
     return CPSGPU_OK;
@@ -1523,9 +1533,7 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
     CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     d->D->rtile[prec] = tile;
     // captured graphs hold the launches of the old tile
-    for (auto &s : d->solvers) s.reset();
-    d->D->ms.refine.reset();
-    d->D->ms.refine_n = 0;
+    drop_captured(d);
     return CPSGPU_OK;
   });
 }
@@ -1566,9 +1574,7 @@ int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int sl
     CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));
     for (int ep : eps) tune_set(TuneKey{prec, D.lat->recon(prec), ep, D.kind, D.ls}, b, order);
     // captured graphs hold the launches of the old shape
-    for (auto &s : d->solvers) s.reset();
-    d->D->ms.refine.reset();
-    d->D->ms.refine_n = 0;
+    drop_captured(d);
     return CPSGPU_OK;
   });
 }

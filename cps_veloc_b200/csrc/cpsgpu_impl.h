@@ -125,11 +125,34 @@ struct MobiusPlan {
 
 // Multishift CG workspace (multishift.cu), kept across calls on one operator.
 struct CgSolver;
+// an instantiated graph and the configuration it was captured for
+struct CachedGraph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  long long body_kernels = 0;  // kernels of one body of its WHILE node
+  std::vector<long long> key;
+  CachedGraph() = default;
+  CachedGraph(const CachedGraph &) = delete;
+  CachedGraph &operator=(const CachedGraph &) = delete;
+  ~CachedGraph() { drop(); }
+  void drop() {
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    ge = nullptr;
+    g = nullptr;
+    key.clear();
+  }
+};
+
 struct MsWork {
   Field chi, r, tmp;
   std::vector<Field> p, psi;
   DeviceBuffer st, ms, pv, psiv;
   OpWork w;
+  // the recurrences' loop: a WHILE node over chunks of iterations, ctl its
+  // [bodies run, bound] counters
+  CachedGraph loop;
+  DeviceBuffer ctl;
   // the batched refinement solver of the sloppy path, kept with its fields
   // and its instantiated graph while the number of shifts stays the same
   std::shared_ptr<CgSolver> refine;

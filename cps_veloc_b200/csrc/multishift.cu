@@ -124,6 +124,14 @@ __global__ void __launch_bounds__(128) ms_update_shift_kernel(SpinorView r, cons
 
 __global__ void ms_mark_kernel(MsScalars *ms) { ms->upd_done_iter = ms->k; }
 
+// the condition of the recurrences' WHILE node, after each chunk: another
+// chunk while the solve runs, never more than ctl[1] chunks (ctl[0] counts)
+__global__ void ms_loop_cond_kernel(cudaGraphConditionalHandle h, const SolverScalars *st, int *ctl) {
+  if (threadIdx.x != 0) return;
+  const int bodies = ++ctl[0];
+  cudaGraphSetConditional(h, (st->done == 0 && bodies < ctl[1]) ? 1u : 0u);
+}
+
 }  // namespace
 
 int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm, const double *shift, int nshift,
@@ -323,17 +331,57 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
   CPSGPU_CUDA(cudaStreamSynchronize(s));
   const clk::time_point t_rec = clk::now();
   iteration(1);  // the initial step of minvcg.C:140-188 (psi update from chi)
-  MsScalars mh;
-  SolverScalars sh;
+  // the iterations: one graph launch whose WHILE node runs chunks of
+  // iterations until the solve is done (no host polling); the instantiated
+  // graph stays on the operator while the configuration is the same
   const int chunk = 8;
-  for (int guard = 0; guard < max_num_iter / chunk + 4; guard++) {
-    CPSGPU_CUDA(cudaMemcpyAsync(&sh, st, sizeof(sh), cudaMemcpyDeviceToHost, s));
-    CPSGPU_CUDA(cudaStreamSynchronize(s));
-    if (sh.done) break;
-    for (int k = 0; k < chunk; k++) iteration(0);
+  CachedGraph &lg = mw.loop;
+  const std::vector<long long> key = {P, nshift, dev_type, L.recon(P), D.pc_type, D.cplx ? 1 : 0,
+                                      (long long)(size_t)r.data.ptr, (long long)(size_t)w.t1.data.ptr,
+                                      (long long)(size_t)p[0].data.ptr, (long long)(size_t)psi[0].data.ptr};
+  if (lg.ge && lg.key != key) lg.drop();
+  mw.ctl.ensure(2 * sizeof(int));
+  if (!lg.ge) {
+    CPSGPU_CUDA(cudaGraphCreate(&lg.g, 0));
+    cudaGraphConditionalHandle hw;
+    CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, lg.g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp_ = {cudaGraphNodeTypeConditional};
+    cp_.conditional.handle = hw;
+    cp_.conditional.type = cudaGraphCondTypeWhile;
+    cp_.conditional.size = 1;
+    cudaGraphNode_t wn;
+    CPSGPU_CUDA(cudaGraphAddNode(&wn, lg.g, nullptr, 0, &cp_));
+    cudaGraph_t body = cp_.conditional.phGraph_out[0];
+    const long long c0 = launch_counter();
+    CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    try {
+      for (int k = 0; k < chunk; k++) iteration(0);
+      ms_loop_cond_kernel<<<1, 32, 0, s>>>(hw, st, mw.ctl.as<int>());
+      CPSGPU_CUDA(cudaGetLastError());
+      launch_counter()++;
+    } catch (...) {
+      cudaGraph_t junk;
+      cudaStreamEndCapture(s, &junk);
+      launch_counter() = c0;
+      lg.drop();
+      throw;
+    }
+    cudaGraph_t captured;
+    CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
+    lg.body_kernels = launch_counter() - c0;
+    launch_counter() = c0;
+    CPSGPU_CUDA(cudaGraphInstantiate(&lg.ge, lg.g, 0));
+    lg.key = key;
   }
+  const int hctl[2] = {0, (int)std::min<long>((long)max_num_iter / chunk + 4, 1L << 30)};
+  CPSGPU_CUDA(cudaMemcpyAsync(mw.ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
+  CPSGPU_CUDA(cudaGraphLaunch(lg.ge, s));
+  MsScalars mh;
+  int bodies = 0;
   CPSGPU_CUDA(cudaMemcpyAsync(&mh, msd, sizeof(mh), cudaMemcpyDeviceToHost, s));
+  CPSGPU_CUDA(cudaMemcpyAsync(&bodies, mw.ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
   CPSGPU_CUDA(cudaStreamSynchronize(s));
+  launch_counter() += (long long)bodies * lg.body_kernels;
   // achieved residuals (minvcg.C:315-327)
   for (int k = nshift - 1; k >= 0; k--) {
     if (mh.conv[k])
