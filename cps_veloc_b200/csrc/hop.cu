@@ -148,10 +148,15 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   if (L.sub == SUB_BOUNDARY) {
     hp.subn = (hp.face + (int)block.x - 1) / (int)block.x;
     nsb = 2u * (unsigned)hp.subn;
+    hp.i0 = 0;
+    hp.iend = hp.face;
+    hp.jump = (int)lat.vh - hp.face - hp.subn * (int)block.x;
   } else {
     const long nsites = (L.sub == SUB_INTERIOR) ? lat.vh - 2L * hp.face : lat.vh;
     if (nsites <= 0) return;  // a slab of two t-slices has no interior
     nsb = (unsigned)((nsites + block.x - 1) / block.x);
+    hp.i0 = (L.sub == SUB_INTERIOR) ? hp.face : 0;
+    hp.iend = hp.i0 + (int)nsites;
   }
   hp.nsg = g_ns == 2 ? D.ls / (2 * (int)block.y) : (D.ls + block.y - 1) / block.y;
   hp.nsb = (int)nsb;

@@ -85,6 +85,7 @@ struct HopParams {
   // slab (their hops need no halo); SUB_BOUNDARY its first and last
   // t-slices, subn site blocks each
   int sub, subn;
+  int i0, iend, jump;  // first site, end of the (first) site range, the boundary subset's jump
   int rtile;        // right-hand sides per tile: consecutive blocks take the same sites of rtile solves
   int nrhs;         // right-hand sides in the launch
   double bc[4];     // boundary sign per direction
@@ -466,14 +467,13 @@ __global__ void __launch_bounds__(256, (hop_min_blocks<P, NS>())) hop_kernel(con
       sblk = (sblk % nt) * hp.tper + sblk / nt;
     }
   }
-  int i = sblk * blockDim.x + threadIdx.x;
-  int iend = (int)hp.vh;
-  if (hp.sub == SUB_INTERIOR) {
-    i += hp.face;
-    iend -= hp.face;
-  } else if (hp.sub == SUB_BOUNDARY) {
-    if (sblk < hp.subn) iend = hp.face;
-    else i = iend - hp.face + (sblk - hp.subn) * (int)blockDim.x + (int)threadIdx.x;
+  // sites [i0, iend) of the launch's subset; the boundary subset's second
+  // half jumps to the last t-slice
+  int i = sblk * blockDim.x + threadIdx.x + hp.i0;
+  int iend = hp.iend;
+  if (hp.sub == SUB_BOUNDARY && sblk >= hp.subn) {
+    i += hp.jump;
+    iend = (int)hp.vh;
   }
   const int s = NS == 2 ? (sgrp >> 1) * 4 * (int)blockDim.y + (sgrp & 1) + 4 * (int)threadIdx.y
                 : hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y

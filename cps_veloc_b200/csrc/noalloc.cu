@@ -123,6 +123,7 @@ void hop(const Dirac &D, int ep, int cb, int dag, int norm, const SpinorView &in
   hp.dly.init(lat.L[1]);
   hp.dlz.init(lat.L[2]);
   hp.vh = lat.vh;
+  hp.iend = (int)lat.vh;  // every site
   hp.ls = D.ls;
   hp.cb = cb;
   hp.dag = dag;
