@@ -330,7 +330,7 @@ template <> struct Chunk4<PREC_HALF> {
 // each 16-byte group once for its two chunks, where Chunk4 would load a norm
 // and half a group per chunk.  The values are Chunk4's.
 template <int P> struct ChunkReader {
-  const SpinorView &f;
+  const SpinorView f;  // a copy: a reference to a kernel parameter can force it into local memory
   long sl, i;
   __device__ __forceinline__ ChunkReader(const SpinorView &f_, long sl_, long i_) : f(f_), sl(sl_), i(i_) {}
   __device__ __forceinline__ void get(int c, typename PrecTraits<P>::real *v) { Chunk4<P>::load(f, sl, i, c, v); }

@@ -78,14 +78,6 @@ struct HopParams {
   int ls;
   FastDiv dhx, dly, dlz;  // divisions by L[0]/2, L[1], L[2]
   int nsg;          // slice groups in the launch
-  int nsb;          // site blocks in the launch
-  int sorder;       // HopOrder: how blockIdx.x maps to (site block, slice group)
-  int tper;         // ORDER_T: site blocks per t-slice
-  // HopSub: SUB_ALL every site; SUB_INTERIOR the t-slices 1 .. L[3]-2 of a
-  // slab (their hops need no halo); SUB_BOUNDARY its first and last
-  // t-slices, subn site blocks each
-  int sub, subn;
-  int i0, iend, jump;  // first site, end of the (first) site range, the boundary subset's jump
   int rtile;        // right-hand sides per tile: consecutive blocks take the same sites of rtile solves
   int nrhs;         // right-hand sides in the launch
   double bc[4];     // boundary sign per direction
@@ -109,6 +101,14 @@ struct HopParams {
   // (g / 2) * 2 BS + (g % 2) + 2 k, so the BS threads of a site read the same
   // eight links (the parity of slice s alternates with s)
   int spar;
+  int nsb;          // site blocks in the launch
+  int sorder;       // HopOrder: how blockIdx.x maps to (site block, slice group)
+  int tper;         // ORDER_T: site blocks per t-slice
+  // HopSub: SUB_ALL every site; SUB_INTERIOR the t-slices 1 .. L[3]-2 of a
+  // slab (their hops need no halo); SUB_BOUNDARY its first and last
+  // t-slices, subn site blocks each
+  int sub, subn;
+  int i0, iend, jump;  // first site, end of the (first) site range, the boundary subset's jump
 };
 
 struct HopViews {
