@@ -1538,7 +1538,7 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile) {
   });
 }
 
-static_assert(CPSGPU_ORDER_SLICES == ORDER_SLICES && CPSGPU_ORDER_SITES == ORDER_SITES && CPSGPU_ORDER_T == ORDER_T,
+static_assert(CPSGPU_ORDER_SLICES == ORDER_SLICES && CPSGPU_ORDER_SITES == ORDER_SITES,
               "public and internal hop orders");
 
 int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread, int *order) {
@@ -1561,14 +1561,12 @@ int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int sl
     if (!d || sites < 1 || slices < 1 || sites * slices > 256 || sites * slices % 32 != 0 ||
         (slices_per_thread != 1 && slices_per_thread != 2))
       throw Error(CPSGPU_ERR_ARG, "hop shape: sites x slices a multiple of 32 up to 256, 1 or 2 slices per thread");
-    if (order < 0 || order >= ORDER_COUNT) throw Error(CPSGPU_ERR_ARG, "hop order: CPSGPU_ORDER_SLICES, _SITES or _T");
+    if (order < 0 || order >= ORDER_COUNT) throw Error(CPSGPU_ERR_ARG, "hop order: CPSGPU_ORDER_SLICES or CPSGPU_ORDER_SITES");
     check_prec(prec);
     const Dirac &D = *d->D;
     if (slices > std::max(D.ls, 1)) throw Error(CPSGPU_ERR_ARG, "hop shape: more slices per block than Ls");
     if (slices_per_thread == 2 && (D.kind != KIND_DWF || prec == PREC_DOUBLE || D.ls % (4 * slices) != 0))
       throw Error(CPSGPU_ERR_ARG, "slice pairs: DWF, FP32 or FP16 fields, Ls a multiple of 4 x slices");
-    if (order == ORDER_T && (D.lat->vh / D.lat->L[3]) % sites != 0)
-      throw Error(CPSGPU_ERR_ARG, "t order: the sites of a block must divide the sites of one t-slice");
     const dim3 b((unsigned)sites, (unsigned)slices, (unsigned)slices_per_thread);
     const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
     CPSGPU_CUDA(cudaStreamSynchronize(D.lat->stream));

@@ -77,9 +77,7 @@ int autotune(Dirac &D, int prec, int nrhs) {
     }
     // then the order in which the blocks of that shape take the lattice
     int besto = ORDER_SLICES;
-    const long face = L.vh / L.L[3];
     for (int o = ORDER_SITES; o < ORDER_COUNT; o++) {
-      if (o == ORDER_T && face % bestb.x != 0) continue;
       tune_set(key, bestb, o);
       float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
       if (t < best) { best = t; besto = o; }

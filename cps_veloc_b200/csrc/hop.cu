@@ -159,17 +159,13 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
     hp.iend = hp.i0 + (int)nsites;
   }
   hp.nsg = g_ns == 2 ? D.ls / (2 * (int)block.y) : (D.ls + block.y - 1) / block.y;
-  hp.nsb = (int)nsb;
-  hp.sorder = hop_order(key);
-  if (hp.sorder == ORDER_T) {
-    // t fastest needs whole t-slices of site blocks: not the split launches
-    if (L.sub == SUB_ALL && hp.face % block.x == 0) hp.tper = hp.face / (int)block.x;
-    else hp.sorder = ORDER_SLICES;
-  }
+  // ORDER_SITES: the slice groups on the grid's y (blocks run x fastest)
+  const bool sites_first = (hop_order(key) == ORDER_SITES && hp.nsg > 1);
   hp.spar = (hp.dwf && !mix && block.y > 1 && D.ls % (2 * block.y) == 0) ? 1 : 0;
   hp.nrhs = in.nrhs;
   hp.rtile = std::max(1, std::min(D.rhs_tile(L.prec, in.nrhs), in.nrhs));
-  dim3 grid(nsb * hp.nsg * hp.rtile, 1, (unsigned)((in.nrhs + hp.rtile - 1) / hp.rtile));
+  const unsigned ntile = (unsigned)((in.nrhs + hp.rtile - 1) / hp.rtile);
+  dim3 grid = sites_first ? dim3(nsb * hp.rtile, hp.nsg, ntile) : dim3(nsb * hp.nsg * hp.rtile, 1, ntile);
   size_t smem = 0;
   if (mix) {
     smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double) * (D.cplx ? 2 : 1);

@@ -101,9 +101,6 @@ struct HopParams {
   // (g / 2) * 2 BS + (g % 2) + 2 k, so the BS threads of a site read the same
   // eight links (the parity of slice s alternates with s)
   int spar;
-  int nsb;          // site blocks in the launch
-  int sorder;       // HopOrder: how blockIdx.x maps to (site block, slice group)
-  int tper;         // ORDER_T: site blocks per t-slice
   // HopSub: SUB_ALL every site; SUB_INTERIOR the t-slices 1 .. L[3]-2 of a
   // slab (their hops need no halo); SUB_BOUNDARY its first and last
   // t-slices, subn site blocks each
@@ -448,37 +445,46 @@ __global__ void __launch_bounds__(256, (hop_min_blocks<P, NS>())) hop_kernel(con
   // blockIdx.x = (site block, slice group, rhs within the tile), rhs fastest:
   // consecutive blocks read the same links (for rtile solves) and the same
   // fifth-direction neighbourhoods, which are then still in L1 / L2
-  const int rin = blockIdx.x % hp.rtile, sb = blockIdx.x / hp.rtile;
+  // ORDER_SLICES: blockIdx.x = (site block, slice group, rhs within the
+  // tile), rhs fastest; ORDER_SITES: blockIdx.x = (site block, rhs),
+  // blockIdx.y = slice group.  Either way consecutive blocks read the same
+  // links (rtile solves) and sb numbers the blocks of one solve.
+  const int rin = blockIdx.x % hp.rtile, sbx = blockIdx.x / hp.rtile;
   const long rhs = (long)blockIdx.z * hp.rtile + rin;
   if (rhs >= hp.nrhs) return;  // the last tile may be partial
   if (hp.gate == GATE_RUNNING && st[rhs].done) return;
   if (hp.gate == GATE_RELIABLE && (st[rhs].done || !st[rhs].reliable)) return;
-  const unsigned nblk = gridDim.x / hp.rtile;  // blocks of one solve
-
+  const unsigned nbx = gridDim.x / hp.rtile;
+  const unsigned nblk = nbx * gridDim.y;  // blocks of one solve
+  const int sb = (int)(blockIdx.y * nbx) + sbx;
   int sgrp, sblk;
-  if (hp.sorder == 1) {  // ORDER_SITES
-    sblk = sb % hp.nsb;
-    sgrp = sb / hp.nsb;
+  if (gridDim.y > 1) {
+    sgrp = blockIdx.y;
+    sblk = sbx;
   } else {
-    sgrp = sb % hp.nsg;
-    sblk = sb / hp.nsg;
-    if (hp.sorder == 2) {  // ORDER_T: the q-th site block taken is block q / L_t of t-slice q % L_t
-      const int nt = hp.nsb / hp.tper;
-      sblk = (sblk % nt) * hp.tper + sblk / nt;
-    }
+    sgrp = sbx % hp.nsg;
+    sblk = sbx / hp.nsg;
   }
-  // sites [i0, iend) of the launch's subset; the boundary subset's second
-  // half jumps to the last t-slice
-  int i = sblk * blockDim.x + threadIdx.x + hp.i0;
-  int iend = hp.iend;
-  if (hp.sub == SUB_BOUNDARY && sblk >= hp.subn) {
-    i += hp.jump;
-    iend = (int)hp.vh;
+  int i = sblk * blockDim.x + threadIdx.x;
+  bool in_range;
+  if constexpr (HALO) {
+    // a slab's sites, or its first and last t-slices (the second half of
+    // the blocks jumps to the last t-slice)
+    i += hp.i0;
+    in_range = i < hp.iend;
+    if (hp.sub == SUB_BOUNDARY && sblk >= hp.subn) {
+      i += hp.jump;
+      in_range = i < hp.vh;
+    }
+  } else {
+    // every site (i0 = 0), or a slab's interior (i0 = one t-slice)
+    i += hp.i0;
+    in_range = i < hp.vh - hp.i0;
   }
   const int s = NS == 2 ? (sgrp >> 1) * 4 * (int)blockDim.y + (sgrp & 1) + 4 * (int)threadIdx.y
                 : hp.spar ? (sgrp >> 1) * 2 * (int)blockDim.y + (sgrp & 1) + 2 * (int)threadIdx.y
                           : sgrp * (int)blockDim.y + (int)threadIdx.y;
-  const bool active = (i < iend) && (s + 2 * (NS - 1) < hp.ls);
+  const bool active = in_range && (s + 2 * (NS - 1) < hp.ls);
   const long sl = rhs * hp.ls + s;
   const int pin = hp.dwf ? ((s + hp.cb) & 1) : hp.cb;
   const int pout = 1 - pin;

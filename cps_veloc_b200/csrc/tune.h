@@ -19,13 +19,9 @@ struct TuneKey {
 
 // block traversal orders of a hop launch: consecutive blocks take
 //   ORDER_SLICES: the slice groups of one site block (its links stay in L1);
-//   ORDER_SITES:  the site blocks of one slice group, in lexicographic order;
-//   ORDER_T:      the slice groups of one site block, the site blocks taken
-//                 t-slice fastest (the blocks in flight at once cover all t
-//                 of a few spatial rows, so t neighbours are read while
-//                 still in L2); needs a whole number of site blocks per
-//                 t-slice, else ORDER_SLICES runs
-enum HopOrder { ORDER_SLICES = 0, ORDER_SITES = 1, ORDER_T = 2, ORDER_COUNT = 3 };
+//   ORDER_SITES:  the site blocks of one slice group, in lexicographic order
+//                 (the slice groups on the grid's y dimension)
+enum HopOrder { ORDER_SLICES = 0, ORDER_SITES = 1, ORDER_COUNT = 2 };
 
 dim3 hop_block(const TuneKey &k, bool mix);
 int hop_order(const TuneKey &k);

@@ -577,7 +577,7 @@ class _DiracOp:
         check(lib().cpsgpu_set_rhs_tile(self._h, prec, tile))
 
     # block traversal orders of the hop launches (cpsgpu_set_hop_shape)
-    ORDER_SLICES, ORDER_SITES, ORDER_T = 0, 1, 2
+    ORDER_SLICES, ORDER_SITES = 0, 1
 
     def hop_shape(self, prec=A.DOUBLE) -> tuple:
         """(sites, slices, slices per thread, order) of the non-mixing hop launches"""

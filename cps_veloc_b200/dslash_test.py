@@ -33,7 +33,11 @@ def main(argv=None) -> int:
                     help="link form of the FP32/FP16 operators (12, 18, 112, 118; 0: default or autotuned)")
     ap.add_argument("--shape", default="",
                     help="sites,slices,slices_per_thread[,order] of the hop launches (overrides the autotuner; "
-                         "order 0 slices, 1 sites, 2 t)")
+                         "order 0 slices first, 1 sites first)")
+    ap.add_argument("--m5inv", action="store_true",
+                    help="time the Mobius M5^-1 (the standalone Ls x Ls mixing) instead of the hop")
+    ap.add_argument("--mix-impl", type=int, default=0,
+                    help="Mobius mixing kernel: 0 register-tiled, 1 tensor cores (FP16), 2 shared memory")
     ap.add_argument("--dd", type=int, default=0,
                     help="time the t-slab decomposed dslash over this many slabs (one process; see time_dd)")
     args = ap.parse_args(argv)
@@ -48,6 +52,16 @@ def main(argv=None) -> int:
         D = DiracOpDwf(lat, mass=args.mass, ls=args.ls)
     else:
         D = DiracOpMobius(lat, mass=args.mass, ls=args.ls)
+    if args.m5inv:
+        if args.kind != "mobius":
+            raise SystemExit("--m5inv needs --kind mobius")
+        D.set_mix_impl(args.mix_impl)
+        for prec in (int(p) for p in args.prec.split(",")):
+            ms, by = C.c_double(), C.c_double()
+            A.check(A.lib().cpsgpu_time_m5inv(D._h, prec, args.reps, C.byref(ms), C.byref(by)))
+            print(f"prec {prec} mix kernel {args.mix_impl}: m5inv {ms.value:.4f} ms "
+                  f"{by.value / ms.value / 1e6:.0f} GB/s ({by.value:.0f} B)", flush=True)
+        return 0
     if args.force:
         tot, ker, by = C.c_double(), C.c_double(), C.c_double()
         A.check(A.lib().cpsgpu_time_fforce(D._h, args.reps, C.byref(tot), C.byref(ker), C.byref(by)))

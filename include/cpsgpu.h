@@ -594,13 +594,11 @@ int cpsgpu_set_rhs_tile(cpsgpu_dirac d, int prec, int tile);
  * 4 * slices — each thread computes two same-parity slices with shared
  * links), and the site order in which the grid's blocks take the lattice:
  * CPSGPU_ORDER_SLICES (consecutive blocks: every slice group of one block
- * of sites), CPSGPU_ORDER_SITES (consecutive blocks: the site blocks of one
- * slice group, lexicographically), CPSGPU_ORDER_T (as SLICES, the site
- * blocks taken t-slice fastest; needs `sites` to divide the sites of one
- * t-slice of a checkerboard).  get returns the shape in use; set overrides
- * the autotuner.  The shape table (like the autotuner's) is shared by every
+ * of sites) or CPSGPU_ORDER_SITES (consecutive blocks: the site blocks of
+ * one slice group, lexicographically).  get returns the shape in use; set
+ * overrides the autotuner.  The shape table (like the autotuner's) is shared by every
  * operator of the same kind, Ls, precision and link form. */
-enum { CPSGPU_ORDER_SLICES = 0, CPSGPU_ORDER_SITES = 1, CPSGPU_ORDER_T = 2 };
+enum { CPSGPU_ORDER_SLICES = 0, CPSGPU_ORDER_SITES = 1 };
 int cpsgpu_get_hop_shape(cpsgpu_dirac d, int prec, int *sites, int *slices, int *slices_per_thread, int *order);
 int cpsgpu_set_hop_shape(cpsgpu_dirac d, int prec, int sites, int slices, int slices_per_thread, int order);
 

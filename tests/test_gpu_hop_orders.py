@@ -16,7 +16,7 @@ from helpers import OracleOps, rel
 pytestmark = pytest.mark.gpu
 
 TOL = {A.DOUBLE: 1e-13, A.SINGLE: 2e-6, A.HALF: 5e-3}
-ORDERS = (DiracOpDwf.ORDER_SLICES, DiracOpDwf.ORDER_SITES, DiracOpDwf.ORDER_T)
+ORDERS = (DiracOpDwf.ORDER_SLICES, DiracOpDwf.ORDER_SITES)
 
 
 def _lat(L, seed=51):
@@ -107,8 +107,6 @@ def test_order_validation():
     _, lat = _lat((6, 4, 2, 6))
     D = DiracOpDwf(lat, mass=0.05, ls=4, m5=1.8)
     with pytest.raises(A.CpsGpuError):
-        D.set_hop_shape(A.SINGLE, 32, 1, 1, D.ORDER_T)  # 24 sites per t-slice
-    with pytest.raises(A.CpsGpuError):
-        D.set_hop_shape(A.SINGLE, 32, 1, 1, 3)
+        D.set_hop_shape(A.SINGLE, 32, 1, 1, 2)
     D.set_hop_shape(A.SINGLE, 32, 1, 1, D.ORDER_SITES)
     assert D.hop_shape(A.SINGLE)[3] == D.ORDER_SITES
