@@ -351,15 +351,17 @@ def extra_mobius(A) -> dict:
     for name, prec in (("fp64", A.DOUBLE), ("half", A.HALF)):
         ms, by = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
         flops = 48 * ls * D.f_size // 24  # dense Ls x Ls, both chiralities
+        unit = ("CUDA cores, register-tiled (matrix as a kernel parameter), input tiles staged in shared "
+                "memory by bulk asynchronous copies" if prec == A.HALF else "CUDA cores, shared-memory staging")
         out[f"m5inv_{name}"] = {"ms": ms, "GB_s": by / ms / 1e6, "frac_of_measured_hbm": by / ms / 1e6 / pk,
-                                "flop_per_byte": flops / by,
-                                "unit": "CUDA cores, register-tiled (matrix as a kernel parameter)"}
-        # the shared-memory CUDA-core kernel it replaced
-        D.set_mix_impl(D.MIX_SHARED)
-        ms2, by2 = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
-        D.set_mix_impl(D.MIX_REG)
-        out[f"m5inv_{name}_shared_memory_kernel"] = {"ms": ms2, "GB_s": by2 / ms2 / 1e6,
-                                                     "frac_of_measured_hbm": by2 / ms2 / 1e6 / pk}
+                                "flop_per_byte": flops / by, "unit": unit}
+        # the other CUDA-core kernels: shared-memory staging, register-tiled without bulk staging
+        for key, impl in (("shared_memory_kernel", D.MIX_SHARED), ("register_tiled_kernel", D.MIX_REG)):
+            D.set_mix_impl(impl)
+            ms2, by2 = _dev_time(A, A.lib().cpsgpu_time_m5inv, D, prec, 20)
+            out[f"m5inv_{name}_{key}"] = {"ms": ms2, "GB_s": by2 / ms2 / 1e6,
+                                          "frac_of_measured_hbm": by2 / ms2 / 1e6 / pk}
+        D.set_mix_impl(D.MIX_DEFAULT)
         m2, b2 = C.c_double(), C.c_double()
         A.check(A.lib().cpsgpu_time_dslash(D._h, prec, 1, 0, 20, C.byref(m2), C.byref(b2)))
         out[f"hop_{name}"] = {"ms": m2.value, "GB_s": b2.value / m2.value / 1e6}
@@ -383,7 +385,7 @@ def extra_mobius(A) -> dict:
     x = np.zeros(D.f_size)
     rs = D.InvCg(x, b, stop_rsd=STOP, max_num_iter=50000, precision=A.HALF)
     out["half_inner_cg_shared_memory_mixing"] = {"time_s": rs.seconds, "iterations": rs.iterations}
-    D.set_mix_impl(D.MIX_REG)
+    D.set_mix_impl(D.MIX_DEFAULT)
     D.close()
     lat.close()
     return out

@@ -1482,10 +1482,12 @@ int cpsgpu_set_mix_impl(cpsgpu_dirac d, int impl) {
   return guarded([&] {
     if (!d) throw Error(CPSGPU_ERR_ARG, "null operator");
     if (d->D->kind != KIND_MOBIUS) throw Error(CPSGPU_ERR_ARG, "Ls x Ls mixing: Mobius operators only");
-    if (impl < 0 || impl > 2) throw Error(CPSGPU_ERR_ARG, "mixing kernel: 0 register-tiled, 1 tensor cores, 2 shared memory");
+    if (impl < 0 || impl > 3)
+      throw Error(CPSGPU_ERR_ARG, "mixing kernel: 0 default, 1 tensor cores, 2 shared memory, 3 register-tiled");
     CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     d->D->mix_tc = (impl == 1);
     d->D->mix_reg = (impl != 2);
+    d->D->mix_bulk = (impl == 0 || impl == 1);
     // allocated here, never inside a graph capture
     if (d->D->mix_tc) d->D->mixTcFrag.ensure(2 * 2 * 32 * 4 * sizeof(unsigned));
     // captured graphs hold the other kernels
@@ -1513,6 +1515,7 @@ int cpsgpu_time_m5inv(cpsgpu_dirac d, int prec, int reps, double *ms, double *by
     check_prec(prec);
     need_gauge(d);
     *ms = time_m5inv(*d->D, prec, reps, bytes);
+    if (mix_bulk_error()) throw Error(CPSGPU_ERR_STATE, "a bounded wait of the bulk-staged mixing kernel ran out");
     return CPSGPU_OK;
   });
 }

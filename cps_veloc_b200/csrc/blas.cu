@@ -434,6 +434,7 @@ void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &i
     launch_mix_tc(D, mix, in, out, st, gate);
     return;
   }
+  if (D.mix_bulk && launch_mix_bulk(D, prec, mix, in, out, st, gate)) return;
   if (D.mix_reg && launch_mix_reg(D, prec, mix, in, out, st, gate)) return;
   const int ls = D.ls;
   int bx = 256 / ls, p2 = 1;

@@ -199,6 +199,8 @@ struct Dirac {
   // the register-tiled mixing kernel (mix_reg.cu) where it applies; off:
   // the shared-memory kernel (blas.cu)
   bool mix_reg = true;
+  // the bulk-copy staged kernel (mix_bulk.cu) for FP16 fields where it applies
+  bool mix_bulk = true;
   DeviceBuffer mixTcFrag;  // the tensor-core form's A fragments of the matrix being applied
   // the preconditioning of MatPc (Mobius) and its two plans; the matrices
   // of the non-SYM2 forms live in pc_bufs
@@ -256,6 +258,11 @@ void launch_mix_tc(const Dirac &D, const double *mix, const SpinorView &in, cons
 // it does not apply
 bool launch_mix_reg(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                     const SolverScalars *st, int gate);
+// the bulk-copy staged form (mix_bulk.cu): FP16 fields, real matrices,
+// vh a multiple of 32, Ls 8, 10, 12 or 16; false when it does not apply
+bool launch_mix_bulk(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
+                     const SolverScalars *st, int gate);
+int mix_bulk_error();  // nonzero once a bounded wait of the bulk kernel ran out
 void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                 const SolverScalars *st = nullptr, int gate = 0);
 

@@ -20,7 +20,10 @@ namespace cpsgpu {
 
 namespace {
 
-template <int LS, typename T> struct MixMat {
+// the two matrices transposed, [t][s], so that the entries of output
+// slices s and s + 1 for one input slice t are adjacent (one 8-byte operand
+// of a packed multiply-add)
+template <int LS, typename T> struct __align__(8) MixMat {
   T up[LS * LS], dn[LS * LS];
 };
 
@@ -46,30 +49,34 @@ __device__ __forceinline__ void load_block(const SpinorView &f, long sl, long i,
   }
 }
 
-// out(s) for all s of one block of reals, matrix M (row-major [s][t])
-template <int P, int LS, typename T, typename R, int NR>
-__device__ __forceinline__ void mix_block(const SpinorView &in, long rhs, long i, int cb, const T (&M)[LS * LS],
-                                          R (&acc)[LS][NR]) {
+// out(s) for all s of one block of reals, matrix MT transposed ([t][s]);
+// acc[s / 2][k] holds slices s, s + 1 of real k: one packed fused
+// multiply-add per pair, each lane the scalar fmaf of the same operands
+template <int P, int LS, int NR>
+__device__ __forceinline__ void mix_block(const SpinorView &in, long rhs, long i, int cb, const float (&MT)[LS * LS],
+                                          float2 (&acc)[LS / 2][NR]) {
 #pragma unroll
-  for (int s = 0; s < LS; s++)
+  for (int s = 0; s < LS / 2; s++)
 #pragma unroll
-    for (int k = 0; k < NR; k++) acc[s][k] = R(0);
+    for (int k = 0; k < NR; k++) acc[s][k] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int t = 0; t < LS; t++) {
     float x[NR];
     load_block<P>(in, rhs * LS + t, i, cb, x);
 #pragma unroll
-    for (int s = 0; s < LS; s++)
+    for (int k = 0; k < NR; k++) {
+      const float2 xx = make_float2(x[k], x[k]);
 #pragma unroll
-      for (int k = 0; k < NR; k++) acc[s][k] = fmac_(R(M[s * LS + t]), x[k], acc[s][k]);
+      for (int s = 0; s < LS / 2; s++)
+        acc[s][k] = __ffma2_rn(*reinterpret_cast<const float2 *>(&MT[t * LS + 2 * s]), xx, acc[s][k]);
+    }
   }
 }
 
 template <int P, int LS>
 __global__ void __launch_bounds__(REG_SITES * RegBlock<P>::NB)
-    mix_reg_kernel(SpinorView in, SpinorView out, const MixMat<LS, typename PrecTraits<P>::real> m,
-                   const SolverScalars *st, int gate) {
-  using R = typename PrecTraits<P>::real;
+    mix_reg_kernel(SpinorView in, SpinorView out, const MixMat<LS, float> m, const SolverScalars *st, int gate) {
+  static_assert(LS % 2 == 0, "slices are paired");
   constexpr int NR = RegBlock<P>::NR, NB = RegBlock<P>::NB;
   if (gate == GATE_RUNNING && st[blockIdx.z].done) return;
   if (gate == GATE_RELIABLE && (st[blockIdx.z].done || !st[blockIdx.z].reliable)) return;
@@ -77,18 +84,19 @@ __global__ void __launch_bounds__(REG_SITES * RegBlock<P>::NB)
   const long i = (long)blockIdx.x * REG_SITES + threadIdx.x;
   const long rhs = blockIdx.z;
   const bool active = i < in.vh;
-  R acc[LS][NR];
+  float2 acc2[LS / 2][NR];
   // warp-uniform branch (a warp is one cb): the matrix operands stay compile-time offsets
   if (active) {
-    if (cb < NB / 2) mix_block<P, LS>(in, rhs, i, cb, m.up, acc);
-    else mix_block<P, LS>(in, rhs, i, cb, m.dn, acc);
+    if (cb < NB / 2) mix_block<P, LS>(in, rhs, i, cb, m.up, acc2);
+    else mix_block<P, LS>(in, rhs, i, cb, m.dn, acc2);
   }
+  auto acc = [&](int s, int k) { return (s & 1) ? acc2[s >> 1][k].y : acc2[s >> 1][k].x; };
   if constexpr (P == PREC_SINGLE) {
     if (!active) return;
 #pragma unroll
     for (int s = 0; s < LS; s++)
       reinterpret_cast<float4 *>(out.data)[((rhs * LS + s) * 6 + cb) * out.vh + i] =
-          make_float4(acc[s][0], acc[s][1], acc[s][2], acc[s][3]);
+          make_float4(acc(s, 0), acc(s, 1), acc(s, 2), acc(s, 3));
   } else {
     // FP16: every slice's norm is the largest magnitude over the 6 blocks
     __shared__ float pmax[LS][NB][REG_SITES];
@@ -96,7 +104,7 @@ __global__ void __launch_bounds__(REG_SITES * RegBlock<P>::NB)
     for (int s = 0; s < LS; s++) {
       float mx = 0.f;
 #pragma unroll
-      for (int k = 0; k < NR; k++) mx = fmaxf(mx, fabsf(active ? acc[s][k] : 0.f));
+      for (int k = 0; k < NR; k++) mx = fmaxf(mx, fabsf(active ? acc(s, k) : 0.f));
       pmax[s][cb][threadIdx.x] = mx;
     }
     __syncthreads();
@@ -109,8 +117,8 @@ __global__ void __launch_bounds__(REG_SITES * RegBlock<P>::NB)
       const float inv = (mx > 0.f) ? 1.0f / mx : 0.f;
       uint2 q;
       __half2 *h = reinterpret_cast<__half2 *>(&q);
-      h[0] = __floats2half2_rn(acc[s][0] * inv, acc[s][1] * inv);
-      h[1] = __floats2half2_rn(acc[s][2] * inv, acc[s][3] * inv);
+      h[0] = __floats2half2_rn(acc(s, 0) * inv, acc(s, 1) * inv);
+      h[1] = __floats2half2_rn(acc(s, 2) * inv, acc(s, 3) * inv);
       const long sl = rhs * LS + s;
       reinterpret_cast<uint2 *>(out.data)[((sl * 3 + (cb >> 1)) * out.vh + i) * 2 + (cb & 1)] = q;
       if (cb == 0) out.norm[sl * out.vh + i] = mx;
@@ -121,12 +129,12 @@ __global__ void __launch_bounds__(REG_SITES * RegBlock<P>::NB)
 template <int P, int LS>
 void launch_ls(const Dirac &D, const std::vector<double> &h, const SpinorView &in, const SpinorView &out,
                const SolverScalars *st, int gate) {
-  using R = typename PrecTraits<P>::real;
-  MixMat<LS, R> m;
-  for (int k = 0; k < LS * LS; k++) {
-    m.up[k] = R(h[k]);
-    m.dn[k] = R(h[LS * LS + k]);
-  }
+  MixMat<LS, float> m;  // transposed: m.up[t * LS + s] = M_up[s][t]
+  for (int s = 0; s < LS; s++)
+    for (int t = 0; t < LS; t++) {
+      m.up[t * LS + s] = float(h[s * LS + t]);
+      m.dn[t * LS + s] = float(h[LS * LS + s * LS + t]);
+    }
   const dim3 block(REG_SITES, RegBlock<P>::NB);
   const dim3 grid((unsigned)((in.vh + REG_SITES - 1) / REG_SITES), 1, in.nrhs);
   mix_reg_kernel<P, LS><<<grid, block, 0, D.lat->stream>>>(in, out, m, st, gate);

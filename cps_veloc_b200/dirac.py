@@ -636,13 +636,16 @@ class DiracOpMobius(_DiracOp):
         check(lib().cpsgpu_dirac_get_pc_type(self._h, C.byref(v)))
         return v.value
 
-    MIX_REG, MIX_TENSOR_CORES, MIX_SHARED = 0, 1, 2
+    MIX_DEFAULT, MIX_TENSOR_CORES, MIX_SHARED, MIX_REG = 0, 1, 2, 3
+    MIX_BULK = MIX_DEFAULT  # FP16 fields: staged by bulk copies where it applies
 
     def set_mix_impl(self, impl) -> None:
-        """the kernel of the standalone Ls x Ls mixings: MIX_REG (0, the
-        default, register-tiled CUDA cores), MIX_TENSOR_CORES (1, FP16
-        fields on the tensor cores) or MIX_SHARED (2, the shared-memory
-        CUDA-core kernel); True / False mean 1 / 0"""
+        """the kernel of the standalone Ls x Ls mixings: MIX_DEFAULT (0: FP16
+        fields the register-tiled arithmetic on input tiles staged by bulk
+        asynchronous copies, else as MIX_REG), MIX_TENSOR_CORES (1, FP16
+        fields on the tensor cores), MIX_SHARED (2, the shared-memory
+        CUDA-core kernel) or MIX_REG (3, register-tiled CUDA cores);
+        True / False mean 1 / 0"""
         impl = int(impl) if not isinstance(impl, bool) else (1 if impl else 0)
         check(lib().cpsgpu_set_mix_impl(self._h, impl))
 

@@ -37,7 +37,8 @@ def main(argv=None) -> int:
     ap.add_argument("--m5inv", action="store_true",
                     help="time the Mobius M5^-1 (the standalone Ls x Ls mixing) instead of the hop")
     ap.add_argument("--mix-impl", type=int, default=0,
-                    help="Mobius mixing kernel: 0 register-tiled, 1 tensor cores (FP16), 2 shared memory")
+                    help="Mobius mixing kernel: 0 default (FP16: bulk-staged), 1 tensor cores (FP16), "
+                         "2 shared memory, 3 register-tiled")
     ap.add_argument("--dd", type=int, default=0,
                     help="time the t-slab decomposed dslash over this many slabs (one process; see time_dd)")
     args = ap.parse_args(argv)

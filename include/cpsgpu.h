@@ -226,16 +226,21 @@ int cpsgpu_dirac_set_pc_type(cpsgpu_dirac d, int pc_type);
 int cpsgpu_dirac_get_pc_type(cpsgpu_dirac d, int *pc_type);
 /* No counterpart in the reference: the kernel of the Mobius operator's
  * standalone Ls x Ls mixings (M5^-1, the first step of MatPc).
- *   0 (the default): for FP32 and FP16 fields, CUDA cores, register-tiled
- *     (mix_reg.cu): the two real matrices are a kernel parameter, every
- *     thread computes all Ls output slices of a block of reals (Ls 8, 10,
- *     12, 16, 20, 24; real b, c); FP64 fields as 2;
+ *   0 (the default): for FP16 fields the register-tiled arithmetic of 3 on
+ *     input tiles staged in shared memory by bulk asynchronous copies, two
+ *     stages per persistent block (mix_bulk.cu; Ls 8, 10, 12, 16, sites per
+ *     checkerboard slice a multiple of 32, real b, c), else as 3;
  *   1: for FP16 fields, mma.sync m16n8k16 contractions on the tensor cores
  *     (FP16 operands with the matrix split into high and low parts, FP32
  *     accumulation, mix_tc.cu; Ls <= 16, real b, c), else as 0;
  *   2: CUDA cores, the spinors staged in shared memory (blas.cu), the form
  *     every case outside the others uses (complex zMobius coefficients,
- *     other Ls). */
+ *     other Ls);
+ *   3: for FP32 and FP16 fields, CUDA cores, register-tiled (mix_reg.cu):
+ *     the two real matrices are a kernel parameter, every thread computes
+ *     all Ls output slices of a block of reals with packed FP32 multiply-adds
+ *     (Ls 8, 10, 12, 16, 20, 24; real b, c); FP64 fields as 2.
+ * Every form but 1 gives the same bits. */
 int cpsgpu_set_mix_impl(cpsgpu_dirac d, int impl);
 
 /* ---- solvers ---- */
