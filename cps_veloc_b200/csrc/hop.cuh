@@ -520,16 +520,48 @@ __global__ void __launch_bounds__(256, (hop_min_blocks<P, NS>())) hop_kernel(con
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
     const int nmx = 2 * hp.ls * hp.ls * (hp.mix_cplx ? 2 : 1);
     for (int k = tid; k < nmx; k += blockDim.x * blockDim.y) mx[k] = hp.mix[k];
+    // FP32 arithmetic with real matrices: the staging is [ls][12][BX] pairs
+    // of reals, one 8-byte load and one packed multiply-add per pair (each
+    // lane the fused multiply-add of the scalar form)
+    constexpr bool PAIRS = std::is_same<R, float>::value;
+    const bool pairs = PAIRS && !hp.mix_cplx;
     if (s < hp.ls) {
-      R *mine = sm + (size_t)s * 24 * blockDim.x + threadIdx.x;
+      if (pairs) {
+        float2 *mine2 = reinterpret_cast<float2 *>(sm) + (size_t)s * 12 * blockDim.x + threadIdx.x;
 #pragma unroll
-      for (int k = 0; k < 24; k++) mine[k * blockDim.x] = active ? acc[k] : R(0);
+        for (int k = 0; k < 12; k++)
+          mine2[k * blockDim.x] = active ? make_float2(float(acc[2 * k]), float(acc[2 * k + 1])) : make_float2(0.f, 0.f);
+      } else {
+        R *mine = sm + (size_t)s * 24 * blockDim.x + threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < 24; k++) mine[k * blockDim.x] = active ? acc[k] : R(0);
+      }
     }
     __syncthreads();
     if (active) {
 #pragma unroll
       for (int k = 0; k < 24; k++) acc[k] = R(0);
-      if (!hp.mix_cplx) {
+      if (pairs) {
+        if constexpr (PAIRS) {
+          float2 a2[12];
+#pragma unroll
+          for (int k = 0; k < 12; k++) a2[k] = make_float2(0.f, 0.f);
+          for (int t2 = 0; t2 < hp.ls; t2++) {
+            const float mu_ = float(mx[s * hp.ls + t2]);
+            const float md_ = float(mx[hp.ls * hp.ls + s * hp.ls + t2]);
+            const float2 *src2 = reinterpret_cast<const float2 *>(sm) + (size_t)t2 * 12 * blockDim.x + threadIdx.x;
+#pragma unroll
+            for (int k = 0; k < 6; k++) a2[k] = __ffma2_rn(make_float2(mu_, mu_), src2[k * blockDim.x], a2[k]);
+#pragma unroll
+            for (int k = 6; k < 12; k++) a2[k] = __ffma2_rn(make_float2(md_, md_), src2[k * blockDim.x], a2[k]);
+          }
+#pragma unroll
+          for (int k = 0; k < 12; k++) {
+            acc[2 * k] = a2[k].x;
+            acc[2 * k + 1] = a2[k].y;
+          }
+        }
+      } else if (!hp.mix_cplx) {
         for (int t2 = 0; t2 < hp.ls; t2++) {
           const R mu_ = R(mx[s * hp.ls + t2]);
           const R md_ = R(mx[hp.ls * hp.ls + s * hp.ls + t2]);
