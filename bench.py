@@ -68,7 +68,7 @@ FP64_CG_ITERS = 196
 # (hop_kernel store epilogue, cold L2; profiles/hop_dwf_*_16x32_ls16.md),
 # keyed by (precision, stored link form).  The algorithmic bytes are 226.5 MB
 # (FP32, 12-real links), 239.0 MB (FP32, 18), 127.9 MB (FP16, 18).
-DSLASH_TRAFFIC = {(1, 12): 132.47e6 + 72.48e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.47e6}
+DSLASH_TRAFFIC = {(1, 12): 132.42e6 + 71.94e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.47e6}
 
 
 WORKLOAD = "DWF 16^3x32 Ls=16 M5=1.8 mf=0.01 CG on MatPcDagMatPc to true residual 1e-10"
