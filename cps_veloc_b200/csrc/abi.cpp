@@ -1306,6 +1306,39 @@ int cpsgpu_lattice_set_t_partition(cpsgpu_lattice lat, int nodes_t, int coor_t) 
   });
 }
 
+int cpsgpu_lattice_set_stream(cpsgpu_lattice lat, void *stream) {
+  return guarded([&] {
+    if (!lat) throw Error(CPSGPU_ERR_ARG, "null lattice");
+    Lattice &L = *lat->L;
+    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));  // nothing of the old stream is left in flight
+    L.stream = stream ? static_cast<cudaStream_t>(stream) : L.own_stream;
+    L.caller_stream = (stream != nullptr);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_dot_device(cpsgpu_field a, cpsgpu_field b, double *dev_out) {
+  return guarded([&] {
+    if (!a || !b || !dev_out) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (a->f.prec != PREC_DOUBLE || b->f.prec != PREC_DOUBLE) throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+    if (a->f.sites() != b->f.sites()) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    field_dot_device(*a->d->D->lat, a->f.view(), b->f.view(), dev_out);
+    return CPSGPU_OK;
+  });
+}
+
+int cpsgpu_field_axpby_device(cpsgpu_field out, const double *dev_a, double scale, cpsgpu_field x, cpsgpu_field y) {
+  return guarded([&] {
+    if (!out || !x || !y || !dev_a) throw Error(CPSGPU_ERR_ARG, "null argument");
+    if (out->f.prec != PREC_DOUBLE || x->f.prec != PREC_DOUBLE || y->f.prec != PREC_DOUBLE)
+      throw Error(CPSGPU_ERR_ARG, "FP64 fields required");
+    if (out->f.sites() != x->f.sites() || out->f.sites() != y->f.sites()) throw Error(CPSGPU_ERR_ARG, "field mismatch");
+    Lattice &L = *out->d->D->lat;
+    launch_axpby_dev(L.stream, out->f.view(), dev_a, scale, x->f.view(), y->f.view());
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_dd_face_bytes(cpsgpu_dirac d, int precision, int nrhs, size_t *bytes) {
   return guarded([&] {
     if (!d || !bytes || nrhs < 1) throw Error(CPSGPU_ERR_ARG, "bad argument");
@@ -1319,7 +1352,7 @@ int cpsgpu_dslash_dd_pack(cpsgpu_dirac d, cpsgpu_field in, int cb, int dag, void
     if (!d || !in || !to_prev || !to_next) throw Error(CPSGPU_ERR_ARG, "null argument");
     if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
     dd_pack(*d->D, in->f.prec, in->f.view(), cb ? 1 : 0, dag ? 1 : 0, to_prev, to_next);
-    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    if (!d->D->lat->caller_stream) CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     return CPSGPU_OK;
   });
 }
@@ -1331,7 +1364,7 @@ int cpsgpu_dslash_dd(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in, int cb, 
     if (out->f.prec != in->f.prec || out->f.nrhs != in->f.nrhs) throw Error(CPSGPU_ERR_ARG, "field mismatch");
     if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
     dd_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0, from_next, from_prev);
-    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    if (!d->D->lat->caller_stream) CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     return CPSGPU_OK;
   });
 }
@@ -1355,7 +1388,7 @@ int cpsgpu_dslash_dd_boundary(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in,
     if (!d->D->lat->have_gauge) throw Error(CPSGPU_ERR_STATE, "no gauge field imported");
     dd_dslash(*d->D, in->f.prec, out->f.view(), in->f.view(), cb ? 1 : 0, dag ? 1 : 0, from_next, from_prev,
               SUB_BOUNDARY);
-    CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
+    if (!d->D->lat->caller_stream) CPSGPU_CUDA(cudaStreamSynchronize(d->D->lat->stream));
     return CPSGPU_OK;
   });
 }
@@ -1368,7 +1401,7 @@ int cpsgpu_field_axpby(cpsgpu_field out, double a, cpsgpu_field x, cpsgpu_field 
     if (out->f.sites() != x->f.sites() || out->f.sites() != y->f.sites()) throw Error(CPSGPU_ERR_ARG, "field mismatch");
     Lattice &L = *out->d->D->lat;
     launch_axpby(L.stream, out->f.view(), a, x->f.view(), y->f.view());
-    CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+    if (!L.caller_stream) CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
     return CPSGPU_OK;
   });
 }

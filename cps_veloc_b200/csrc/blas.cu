@@ -107,6 +107,21 @@ __global__ void axpby_kernel(SpinorView out, double a, SpinorView x, SpinorView 
   SpinorIO<PREC_DOUBLE>::store(out, sl, i, yv);
 }
 
+// out = (scale a[0]) x + y with the coefficient read on the device
+__global__ void axpby_dev_kernel(SpinorView out, const double *a, double scale, SpinorView x, SpinorView y,
+                                 size_t n) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const double c = scale * __ldg(a);
+  long sl = (long)(idx / x.vh), i = (long)(idx % x.vh);
+  double xv[24], yv[24];
+  SpinorIO<PREC_DOUBLE>::load(x, sl, i, xv);
+  SpinorIO<PREC_DOUBLE>::load(y, sl, i, yv);
+#pragma unroll
+  for (int k = 0; k < 24; k++) yv[k] = fma(c, xv[k], yv[k]);
+  SpinorIO<PREC_DOUBLE>::store(out, sl, i, yv);
+}
+
 __global__ void scale_kernel(double a, SpinorView f, size_t n) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
@@ -341,6 +356,14 @@ void launch_convert(cudaStream_t s, int pdst, const SpinorView &dst, int psrc, c
 void launch_axpby(cudaStream_t s, const SpinorView &out, double a, const SpinorView &x, const SpinorView &y) {
   size_t n = (size_t)x.vh * x.ls * x.nrhs;
   axpby_kernel<<<blocks_for(n), TPB, 0, s>>>(out, a, x, y, n);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+}
+
+void launch_axpby_dev(cudaStream_t s, const SpinorView &out, const double *a, double scale, const SpinorView &x,
+                      const SpinorView &y) {
+  size_t n = (size_t)x.vh * x.ls * x.nrhs;
+  axpby_dev_kernel<<<blocks_for(n), TPB, 0, s>>>(out, a, scale, x, y, n);
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;
 }

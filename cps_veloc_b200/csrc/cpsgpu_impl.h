@@ -82,7 +82,9 @@ struct Lattice {
   long vh;
   double bc[4];
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // where every launch for this lattice goes
+  cudaStream_t own_stream = nullptr;   // the library's stream, created with the lattice
+  bool caller_stream = false;          // stream is the caller's (cpsgpu_lattice_set_stream)
   // gauge field copies: FP64 full and compressed, FP32 and FP16 compressed
   DeviceBuffer gD18, gD12, gS12, gH12;
   DeviceBuffer gS18, gH18;  // full-link FP32 / FP16 copies (fields.cuh LinkIO<.., 18>)
@@ -269,6 +271,8 @@ void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &i
 // vector kernels
 // out = a x + y and f *= a, FP64 fields
 void launch_axpby(cudaStream_t s, const SpinorView &out, double a, const SpinorView &x, const SpinorView &y);
+void launch_axpby_dev(cudaStream_t s, const SpinorView &out, const double *a, double scale, const SpinorView &x,
+                      const SpinorView &y);
 void launch_scale(cudaStream_t s, double a, const SpinorView &f);
 void launch_convert(cudaStream_t s, int pdst, const SpinorView &dst, int psrc, const SpinorView &src);
 void launch_zero(cudaStream_t s, const Field &f);
@@ -324,6 +328,7 @@ void dd_pack(const Dirac &D, int prec, const SpinorView &in, int cb, int dag, vo
 void dd_dslash(const Dirac &D, int prec, const SpinorView &out, const SpinorView &in, int cb, int dag,
                const void *from_next, const void *from_prev, int sub = 0);
 void field_dot(Lattice &L, const SpinorView &a, const SpinorView &b, double *re, double *im);
+void field_dot_device(Lattice &L, const SpinorView &a, const SpinorView &b, double *dev_out);
 
 // low-mode deflation (lowmode.cu)
 void eigencache_store(Lattice &L, const std::string &name, std::vector<Field> &&evecs, const double *evals);

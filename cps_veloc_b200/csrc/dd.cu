@@ -149,6 +149,19 @@ __global__ void field_dot_kernel(SpinorView a, SpinorView b, double *partials, s
 
 // this rank's part of <a, b> (sum conj(a) b) over FP64 fields: the decomposed
 // solvers add the ranks' parts themselves
+// the same into dev_out[0..1] (device memory), enqueued on the lattice's stream
+void field_dot_device(Lattice &L, const SpinorView &a, const SpinorView &b, double *dev_out) {
+  const size_t n = (size_t)a.vh * a.ls * a.nrhs;
+  const unsigned nblk = (unsigned)((n + 255) / 256);
+  L.partials.ensure((size_t)nblk * 2 * sizeof(double));
+  SolverScalars *st = L.scratch_st.as<SolverScalars>();
+  field_dot_kernel<<<nblk, 256, 0, L.stream>>>(a, b, L.partials.as<double>(), n);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+  launch_finalize(L.stream, 2, L.partials.as<double>(), st, RED_STORE, nblk, 1, GATE_NONE);
+  CPSGPU_CUDA(cudaMemcpyAsync(dev_out, st->sum, 2 * sizeof(double), cudaMemcpyDeviceToDevice, L.stream));
+}
+
 void field_dot(Lattice &L, const SpinorView &a, const SpinorView &b, double *re, double *im) {
   const size_t n = (size_t)a.vh * a.ls * a.nrhs;
   const unsigned nblk = (unsigned)((n + 255) / 256);

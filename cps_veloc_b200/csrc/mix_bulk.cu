@@ -14,10 +14,11 @@
 // The arithmetic is mix_reg's, operation for operation (each thread: 4
 // reals of one site, all Ls output slices, the matrices as a kernel
 // parameter, FP16 norms combined through shared memory), so the outputs are
-// bit-identical to it.  Every wait on an mbarrier is bounded: a wait that
-// runs out sets g_mix_bulk_err, writes NaN to the tile (a solver on it ends
-// NONFINITE) and the block stops after waiting, again bounded, for its
-// copies in flight.
+// bit-identical to it.  Every wait on an mbarrier is bounded in time (one
+// second by the global timer, each try_wait suspending at most ~1 us): a
+// wait that runs out sets g_mix_bulk_err, writes NaN to the tile (a solver
+// on it ends NONFINITE) and the block stops after waiting, again bounded,
+// for its copies in flight.
 #include <cstdint>
 
 #include "cpsgpu_impl.h"
@@ -37,7 +38,8 @@ template <int LS> struct __align__(8) MixMatF {
 
 constexpr int TS = 32;  // sites per tile (threadIdx.x)
 constexpr int NB = 6;   // blocks of 4 reals per site (threadIdx.y)
-constexpr long WAIT_LIMIT = 1L << 22;  // try_wait rounds before giving up
+constexpr unsigned long long WAIT_NS = 1000000000ull;  // a wait gives up after one second
+constexpr unsigned SUSPEND_NS = 1000;                    // each try_wait suspends at most ~1 us
 
 template <int LS> struct Tile {
   static constexpr int DATA = LS * 3 * TS * 16;  // [t][group][site] 16-byte groups
@@ -58,17 +60,28 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
       : "=r"(ok)
-      : "r"(sptr(bar)), "r"(parity)
+      : "r"(sptr(bar)), "r"(parity), "r"(SUSPEND_NS)
       : "memory");
   return ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded in time: true once the phase of this parity has completed, false
+// after WAIT_NS
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
-  for (long k = 0; k < WAIT_LIMIT; k++)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
-  return false;
+    if (global_ns() - t0 > WAIT_NS) return false;
+  }
 }
 
 // global -> shared, completing on bar; both addresses 16-byte aligned, bytes a multiple of 16

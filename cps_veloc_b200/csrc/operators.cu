@@ -32,15 +32,17 @@ Lattice::Lattice(const int L_[4], const double bc_[4]) {
   vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
   CPSGPU_CUDA(cudaGetDevice(&device));
   CPSGPU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  own_stream = stream;
   CPSGPU_CUDA(cudaMallocHost(&pinned, 64 * sizeof(double)));
   scratch_st.alloc(sizeof(SolverScalars) * 4);
   CPSGPU_CUDA(cudaMemsetAsync(scratch_st.ptr, 0, scratch_st.bytes, stream));
 }
 
 Lattice::~Lattice() {
-  if (stream) {
-    cudaStreamSynchronize(stream);
-    cudaStreamDestroy(stream);
+  if (stream && stream != own_stream) cudaStreamSynchronize(stream);
+  if (own_stream) {
+    cudaStreamSynchronize(own_stream);
+    cudaStreamDestroy(own_stream);
   }
   if (pinned) cudaFreeHost(pinned);
 }

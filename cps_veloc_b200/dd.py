@@ -133,6 +133,25 @@ def axpby(out: DeviceField, a: float, x: DeviceField, y: DeviceField) -> None:
     check(lib().cpsgpu_field_axpby(out._h, a, x._h, y._h))
 
 
+def axpby_device(out: DeviceField, a: torch.Tensor, scale: float, x: DeviceField, y: DeviceField) -> None:
+    """out = (scale * a) x + y (FP64 fields), a a float64 device tensor read
+    on the device; only enqueued"""
+    check(lib().cpsgpu_field_axpby_device(out._h, C.c_void_p(a.data_ptr()), scale, x._h, y._h))
+
+
+def dot_device(a: DeviceField, b: DeviceField, out: torch.Tensor) -> None:
+    """out[0], out[1] = this rank's <a, b> (re, im), out a float64 device
+    tensor of (at least) two elements; only enqueued"""
+    check(lib().cpsgpu_field_dot_device(a._h, b._h, C.c_void_p(out.data_ptr())))
+
+
+def set_stream(lat, stream) -> None:
+    """every launch for lat on the CUDA stream `stream` (a torch.cuda.Stream),
+    the pack / dslash / axpby calls of the decomposition only enqueued; None
+    restores the library's own stream"""
+    check(lib().cpsgpu_lattice_set_stream(lat._h, C.c_void_p(stream.cuda_stream) if stream is not None else None))
+
+
 def local_dot(a: DeviceField, b: DeviceField) -> complex:
     """this rank's part of <a, b> = sum conj(a) b (FP64 fields)"""
     re, im = C.c_double(), C.c_double()
@@ -144,16 +163,20 @@ class InProcessRing:
     """every slab of the lattice in this process: faces move between the
     slabs by device copies, a global sum is the sum over the slabs"""
 
-    def exchange(self, faces):
+    def exchange(self, faces, sync=True):
         n = len(faces)
         for r in range(n):
             faces[r].from_next.copy_(faces[(r + 1) % n].to_prev)
             faces[r].from_prev.copy_(faces[(r - 1) % n].to_next)
         # torch's stream only: an interior hop on the library's stream runs on
-        torch.cuda.current_stream().synchronize()
+        if sync:
+            torch.cuda.current_stream().synchronize()
 
     def allreduce(self, v: complex) -> complex:
         return v
+
+    def allreduce_device(self, t: torch.Tensor) -> None:
+        """t summed over the ranks in place (one rank here)"""
 
 
 class _HostFaces:
@@ -174,10 +197,17 @@ class DistRing:
     def __init__(self, group=None):
         self.group = group
 
-    def exchange(self, faces):
+    def exchange(self, faces, sync=True):
         if len(faces) != 1:
             raise ValueError("one slab per rank")
         f = faces[0]
+        if not sync:
+            # the device-resident solver: NCCL point-to-point on the current
+            # stream, ordered with the library's launches on the same stream
+            if dist.get_backend(self.group) != "nccl":
+                raise RuntimeError("a device-resident exchange needs the NCCL backend")
+            exchange_faces(f, self.group)
+            return
         # the pack call returned after its kernels, so the faces are ready;
         # only torch's stream is waited for, not an interior hop in flight
         # on the library's stream
@@ -190,6 +220,12 @@ class DistRing:
             f.from_prev.copy_(h.from_prev)
         if f.to_prev.is_cuda:
             torch.cuda.current_stream().synchronize()
+
+    def allreduce_device(self, t: torch.Tensor) -> None:
+        """t summed over the ranks in place, on the current stream (NCCL)"""
+        if dist.get_backend(self.group) != "nccl":
+            raise RuntimeError("a device-resident all-reduce needs the NCCL backend")
+        dist.all_reduce(t, group=self.group)
 
     def allreduce(self, v: complex) -> complex:
         # NCCL reduces device tensors only; gloo (the CPU tests) host tensors
@@ -285,3 +321,128 @@ def cg(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000):
     for ri, bi, ai in zip(r, b, ap):
         op.axpby(ri, -1.0, ai, bi)
     return k + 1, (op.dot(r, r).real / bb) ** 0.5
+
+
+# ---- the device-resident form of the decomposed CG ----
+
+class _DeviceOps:
+    """the pieces of the decomposed MatPcDagMatPc on one stream, without host
+    synchronisation: every slab's lattice launches on `stream`, faces move
+    by the ring's enqueued exchange, dot products land in device tensors"""
+
+    def __init__(self, op: DDOperator, stream):
+        self.op, self.stream = op, stream
+        self.part = torch.zeros((len(op.ops), 2), dtype=torch.float64, device="cuda")
+
+    def dslash(self, out, inp, cb, dag):
+        op = self.op
+        for D, i, f in zip(op.ops, inp, op.faces):
+            pack(D, i, cb, dag, f)
+        for D, o, i in zip(op.ops, out, inp):
+            dslash_interior(D, o, i, cb, dag)
+        op.ring.exchange(op.faces, sync=False)
+        for D, o, i, f in zip(op.ops, out, inp, op.faces):
+            dslash_boundary(D, o, i, cb, dag, f)
+
+    def matpc(self, out, inp, dag):
+        op = self.op
+        self.dslash(op.t1, inp, 1, dag)
+        self.dslash(out, op.t1, 0, dag)
+        for D, o, i in zip(op.ops, out, inp):
+            axpby(o, -D.kappa * D.kappa, o, i)
+
+    def dot(self, a, b, out: torch.Tensor) -> None:
+        """out[:] = global <a, b> (re, im)"""
+        for k, (x, y) in enumerate(zip(a, b)):
+            dot_device(x, y, self.part[k])
+        torch.sum(self.part, dim=0, out=out)
+        self.op.ring.allreduce_device(out)
+
+    def mdagm(self, out, inp, pap: torch.Tensor) -> None:
+        self.matpc(self.op.t2, inp, 0)
+        self.dot(self.op.t2, self.op.t2, pap)
+        self.matpc(out, self.op.t2, 1)
+
+
+def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_every=8, graph=False):
+    """cg's recurrences (InvCgShift, inv_cg.C:84-448) with every scalar on the
+    device: alpha, beta and the stop test are device tensors, each global
+    sum a device reduction summed over the ranks on the stream (NCCL with
+    DistRing), and an iteration after the solve has converged changes
+    neither x nor r (alpha = 0; its iteration is not counted), so the host
+    looks at the residual only every `check_every` iterations and the
+    iteration count is cg's.  graph=True captures one iteration in a CUDA
+    graph and replays it.  Returns (iterations + 1, true residual) as cg."""
+    stream = torch.cuda.current_stream()
+    for D in op.ops:
+        set_stream(D.lat, stream)
+    try:
+        dev = _DeviceOps(op, stream)
+        r, p, ap = op.field(), op.field(), op.field()
+        f64 = dict(dtype=torch.float64, device="cuda")
+        bb2, pap2, rr2, rrn2 = (torch.zeros(2, **f64) for _ in range(4))
+        alpha, beta, neg_one = torch.zeros(1, **f64), torch.zeros(1, **f64), torch.full((1,), -1.0, **f64)
+        iters = torch.zeros(1, **f64)
+        dev.dot(b, b, bb2)
+        stop = torch.tensor([0.0], **f64)
+        torch.mul(bb2[:1], stop_rsd * stop_rsd, out=stop)
+        # r = b - A x, p = r, rr = |r|^2
+        dev.mdagm(ap, x, pap2)
+        for ri, bi, ai in zip(r, b, ap):
+            axpby_device(ri, neg_one, 1.0, ai, bi)
+        for pi, ri in zip(p, r):
+            axpby(pi, 0.0, ri, ri)
+        dev.dot(r, r, rr2)
+
+        def step():
+            live = (rr2[:1] > stop).to(torch.float64)  # 0 once converged: the step changes nothing
+            dev.mdagm(ap, p, pap2)
+            torch.where(live > 0, rr2[:1] / pap2[:1], torch.zeros_like(live), out=alpha)
+            for xi, pi in zip(x, p):
+                axpby_device(xi, alpha, 1.0, pi, xi)
+            for ri, ai in zip(r, ap):
+                axpby_device(ri, alpha, -1.0, ai, ri)
+            dev.dot(r, r, rrn2)
+            torch.where(live > 0, rrn2[:1] / rr2[:1], torch.ones_like(live), out=beta)
+            rr2.copy_(torch.where(live > 0, rrn2, rr2))
+            for pi, ri in zip(p, r):
+                axpby_device(pi, beta, 1.0, pi, ri)
+            iters.add_(live)
+
+        g = None
+        if graph:
+            step()  # sizes every buffer before the capture
+            side = torch.cuda.Stream()
+            side.wait_stream(stream)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(side):
+                for D in op.ops:
+                    set_stream(D.lat, side)
+                with torch.cuda.graph(g, stream=side):
+                    step()
+            stream.wait_stream(side)
+            for D in op.ops:
+                set_stream(D.lat, stream)
+        k = 1 if graph else 0
+        while k < max_num_iter - 1:
+            n = min(check_every, max_num_iter - 1 - k)
+            for _ in range(n):
+                if g is not None:
+                    g.replay()
+                else:
+                    step()
+            k += n
+            if float(rr2[0]) <= float(stop[0]):
+                break
+        done = int(iters.item())
+        # true residual (inv_cg.C:403-415)
+        dev.mdagm(ap, x, pap2)
+        for ri, bi, ai in zip(r, b, ap):
+            axpby_device(ri, neg_one, 1.0, ai, bi)
+        dev.dot(r, r, rr2)
+        true_res = (float(rr2[0]) / float(bb2[0])) ** 0.5
+        return done + 1, true_res
+    finally:
+        torch.cuda.synchronize()
+        for D in op.ops:
+            set_stream(D.lat, None)

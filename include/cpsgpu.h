@@ -564,6 +564,21 @@ int cpsgpu_dslash_dd_boundary(cpsgpu_dirac d, cpsgpu_field out, cpsgpu_field in,
  * ranks' parts, as glb_sum does).  Both return once done. */
 int cpsgpu_field_axpby(cpsgpu_field out, double a, cpsgpu_field x, cpsgpu_field y);
 int cpsgpu_field_dot(cpsgpu_field a, cpsgpu_field b, double *re, double *im);
+/* No counterpart in the reference (whose solver loop runs on the host): a
+ * decomposed solver that keeps its scalars on the device.  set_stream makes
+ * every launch for lat go to the caller's CUDA stream (a cudaStream_t;
+ * NULL restores the library's own stream), after synchronising the old
+ * one; while it is set, cpsgpu_dslash_dd_pack, cpsgpu_dslash_dd,
+ * cpsgpu_dslash_dd_boundary and cpsgpu_field_axpby only enqueue (no host
+ * synchronisation), so they order with the caller's own work on that
+ * stream (face copies, NCCL collectives) and can be captured in a CUDA
+ * graph.  field_dot_device writes this rank's <a, b> (re, im) to dev_out
+ * (device memory, 2 doubles), and field_axpby_device computes
+ * out = (scale * dev_a[0]) x + y with the coefficient read on the device;
+ * both only enqueue. */
+int cpsgpu_lattice_set_stream(cpsgpu_lattice lat, void *stream);
+int cpsgpu_field_dot_device(cpsgpu_field a, cpsgpu_field b, double *dev_out);
+int cpsgpu_field_axpby_device(cpsgpu_field out, const double *dev_a, double scale, cpsgpu_field x, cpsgpu_field y);
 /* solve with FP64 fields already on the device (sol: initial guess in,
  * solution out); arg->precision selects plain or mixed CG */
 int cpsgpu_invcg_field(cpsgpu_dirac d, cpsgpu_field sol, cpsgpu_field src, const cpsgpu_cg_arg *arg,

@@ -144,3 +144,41 @@ def test_dd_cg_matches_whole_lattice_solve(kind, L, ls, nodes):
     # the overlapped operator is the same operator, bit for bit
     assert sols[True][0] == sols[False][0]
     np.testing.assert_array_equal(sols[True][1], sols[False][1])
+
+
+@pytest.mark.parametrize("kind,L,ls,nodes", [("wilson", (4, 4, 4, 8), 1, 2), ("dwf", (4, 4, 2, 12), 4, 3)])
+@pytest.mark.parametrize("graph", [False, True])
+def test_dd_device_cg_matches_host_cg(kind, L, ls, nodes, graph):
+    """The device-resident decomposed CG (scalars in device tensors, every
+    launch enqueued on one stream, the stop test read every 8 iterations,
+    optionally one iteration captured in a CUDA graph and replayed) against
+    the host-driven dd.cg on the same slabs: the same iteration count (the
+    reductions may round differently: within one) and solution."""
+    mass = 0.1
+    u = gen_gauge(L, seed=521)
+    full = Lattice(L)
+    full.import_gauge(u)
+    Dfull = _make(kind, full, mass, ls)
+    b = gen_gaussian(Dfull.f_size, seed=522)
+    lt = L[3] // nodes
+    ops = []
+    for k in range(nodes):
+        lat = Lattice((L[0], L[1], L[2], lt))
+        lat.import_gauge(_slab_gauge(u, L, nodes, k))
+        dd.set_t_partition(lat, nodes, k)
+        ops.append((lat, _make(kind, lat, mass, ls)))
+    res = {}
+    for device in (False, True):
+        op = dd.DDOperator([D for _, D in ops], dd.InProcessRing())
+        bs, xs = op.field(), op.field()
+        for k, (fb, fx) in enumerate(zip(bs, xs)):
+            fb.upload(_slab_vec(b, L, ls, nodes, k))
+            fx.upload(np.zeros(fx.D.f_size))
+        if device:
+            it, tr = dd.cg_device(op, xs, bs, stop_rsd=1e-11, graph=graph)
+        else:
+            it, tr = dd.cg(op, xs, bs, stop_rsd=1e-11)
+        res[device] = (it, tr, _join([f.download() for f in xs], L, ls))
+    assert abs(res[True][0] - res[False][0]) <= 1
+    assert res[True][1] < 1e-11
+    assert rel(res[True][2], res[False][2]) < 1e-9
