@@ -169,13 +169,19 @@ void launch_hop(const Dirac &D, const HopLaunch &L, const SpinorView &in, const 
   size_t smem = 0;
   if (mix) {
     smem = (size_t)D.ls * block.x * 24 * real_size(L.prec) + 2 * (size_t)D.ls * D.ls * sizeof(double) * (D.cplx ? 2 : 1);
-    static thread_local std::vector<std::pair<HopFn, size_t>> raised;
+    // the attribute belongs to the kernel on one device: raised once per (device, kernel, size)
+    struct Raised {
+      int dev;
+      HopFn fn;
+      size_t smem;
+    };
+    static thread_local std::vector<Raised> raised;
     bool done = false;
     for (auto &e : raised)
-      if (e.first == fn && e.second >= smem) done = true;
+      if (e.dev == lat.device && e.fn == fn && e.smem >= smem) done = true;
     if (!done) {
       CPSGPU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      raised.push_back({fn, smem});
+      raised.push_back({lat.device, fn, smem});
     }
   }
   double *part = L.partials ? L.partials : lat.partials.as<double>();

@@ -249,21 +249,20 @@ void launch_ls(const Dirac &D, const std::vector<double> &h, const SpinorView &i
       m.dn[t * LS + s] = float(h[LS * LS + s * LS + t]);
     }
   const int smem = 2 * Tile<LS>::STAGE;
-  static bool raised = false;
-  if (!raised) {
+  // the shared-memory attribute and the occupancy belong to one device
+  constexpr int MAXDEV = 64;
+  static int blocks_per_sm[MAXDEV] = {}, sms[MAXDEV] = {};
+  const int dev = D.lat->device;
+  if (dev < 0 || dev >= MAXDEV) throw Error(-1, "device index out of range");
+  if (!blocks_per_sm[dev]) {
     CPSGPU_CUDA(cudaFuncSetAttribute(mix_bulk_kernel<LS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    raised = true;
-  }
-  static int blocks_per_sm = 0, sms = 0;
-  if (!blocks_per_sm) {
-    int dev = 0;
-    CPSGPU_CUDA(cudaGetDevice(&dev));
-    CPSGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CPSGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, mix_bulk_kernel<LS>, TS * NB, smem));
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
+    CPSGPU_CUDA(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    int b = 0;
+    CPSGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mix_bulk_kernel<LS>, TS * NB, smem));
+    blocks_per_sm[dev] = b < 1 ? 1 : b;
   }
   const long ntiles = (in.vh / TS) * in.nrhs;
-  const long nblocks = std::min<long>(ntiles, (long)blocks_per_sm * sms);
+  const long nblocks = std::min<long>(ntiles, (long)blocks_per_sm[dev] * sms[dev]);
   mix_bulk_kernel<LS><<<(unsigned)nblocks, dim3(TS, NB), smem, D.lat->stream>>>(in, out, m, st, gate);
   CPSGPU_CUDA(cudaGetLastError());
   launch_counter()++;

@@ -364,15 +364,15 @@ class _DeviceOps:
         self.matpc(out, self.op.t2, 1)
 
 
-def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_every=8, graph=False):
+def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_every=8):
     """cg's recurrences (InvCgShift, inv_cg.C:84-448) with every scalar on the
     device: alpha, beta and the stop test are device tensors, each global
     sum a device reduction summed over the ranks on the stream (NCCL with
     DistRing), and an iteration after the solve has converged changes
     neither x nor r (alpha = 0; its iteration is not counted), so the host
     looks at the residual only every `check_every` iterations and the
-    iteration count is cg's.  graph=True captures one iteration in a CUDA
-    graph and replays it.  Returns (iterations + 1, true residual) as cg."""
+    iteration count is cg's.  Returns (iterations + 1, true residual) as
+    cg."""
     stream = torch.cuda.current_stream()
     for D in op.ops:
         set_stream(D.lat, stream)
@@ -409,28 +409,11 @@ def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_eve
                 axpby_device(pi, beta, 1.0, pi, ri)
             iters.add_(live)
 
-        g = None
-        if graph:
-            step()  # sizes every buffer before the capture
-            side = torch.cuda.Stream()
-            side.wait_stream(stream)
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.stream(side):
-                for D in op.ops:
-                    set_stream(D.lat, side)
-                with torch.cuda.graph(g, stream=side):
-                    step()
-            stream.wait_stream(side)
-            for D in op.ops:
-                set_stream(D.lat, stream)
-        k = 1 if graph else 0
+        k = 0
         while k < max_num_iter - 1:
             n = min(check_every, max_num_iter - 1 - k)
             for _ in range(n):
-                if g is not None:
-                    g.replay()
-                else:
-                    step()
+                step()
             k += n
             if float(rr2[0]) <= float(stop[0]):
                 break
