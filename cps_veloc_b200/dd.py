@@ -146,9 +146,12 @@ def dot_device(a: DeviceField, b: DeviceField, out: torch.Tensor) -> None:
 
 
 def set_stream(lat, stream) -> None:
-    """every launch for lat on the CUDA stream `stream` (a torch.cuda.Stream),
+    """every launch for lat on the CUDA stream `stream` (a created
+    torch.cuda.Stream, not the legacy default stream, whose handle is null),
     the pack / dslash / axpby calls of the decomposition only enqueued; None
     restores the library's own stream"""
+    if stream is not None and not stream.cuda_stream:
+        raise ValueError("the legacy default stream cannot be the lattice's stream: use a created stream")
     check(lib().cpsgpu_lattice_set_stream(lat._h, C.c_void_p(stream.cuda_stream) if stream is not None else None))
 
 
@@ -364,68 +367,97 @@ class _DeviceOps:
         self.matpc(out, self.op.t2, 1)
 
 
-def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_every=8):
+def cg_device(op: DDOperator, x, b, stop_rsd=1e-8, max_num_iter=10000, check_every=8, graph=False):
     """cg's recurrences (InvCgShift, inv_cg.C:84-448) with every scalar on the
     device: alpha, beta and the stop test are device tensors, each global
     sum a device reduction summed over the ranks on the stream (NCCL with
     DistRing), and an iteration after the solve has converged changes
     neither x nor r (alpha = 0; its iteration is not counted), so the host
     looks at the residual only every `check_every` iterations and the
-    iteration count is cg's.  Returns (iterations + 1, true residual) as
-    cg."""
-    stream = torch.cuda.current_stream()
+    iteration count is cg's.  graph=True captures one iteration in a CUDA
+    graph and replays it.  Returns (iterations + 1, true residual) as cg.
+    The solve runs on a stream of its own (ordered after the caller's
+    current stream), where the library's launches and torch's scalar
+    operations and face copies follow one another."""
+    caller = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(caller)
+    with torch.cuda.stream(stream):
+        try:
+            return _cg_device(op, x, b, stream, stop_rsd, max_num_iter, check_every, graph)
+        finally:
+            stream.synchronize()
+            for D in op.ops:
+                set_stream(D.lat, None)
+            caller.wait_stream(stream)
+
+
+def _cg_device(op, x, b, stream, stop_rsd, max_num_iter, check_every, graph):
+    """cg_device's body, on `stream` (the current stream)"""
     for D in op.ops:
         set_stream(D.lat, stream)
-    try:
-        dev = _DeviceOps(op, stream)
-        r, p, ap = op.field(), op.field(), op.field()
-        f64 = dict(dtype=torch.float64, device="cuda")
-        bb2, pap2, rr2, rrn2 = (torch.zeros(2, **f64) for _ in range(4))
-        alpha, beta, neg_one = torch.zeros(1, **f64), torch.zeros(1, **f64), torch.full((1,), -1.0, **f64)
-        iters = torch.zeros(1, **f64)
-        dev.dot(b, b, bb2)
-        stop = torch.tensor([0.0], **f64)
-        torch.mul(bb2[:1], stop_rsd * stop_rsd, out=stop)
-        # r = b - A x, p = r, rr = |r|^2
-        dev.mdagm(ap, x, pap2)
-        for ri, bi, ai in zip(r, b, ap):
-            axpby_device(ri, neg_one, 1.0, ai, bi)
+    dev = _DeviceOps(op, stream)
+    r, p, ap = op.field(), op.field(), op.field()
+    f64 = dict(dtype=torch.float64, device="cuda")
+    bb2, pap2, rr2, rrn2 = (torch.zeros(2, **f64) for _ in range(4))
+    alpha, beta, neg_one = torch.zeros(1, **f64), torch.zeros(1, **f64), torch.full((1,), -1.0, **f64)
+    iters = torch.zeros(1, **f64)
+    dev.dot(b, b, bb2)
+    stop = torch.tensor([0.0], **f64)
+    torch.mul(bb2[:1], stop_rsd * stop_rsd, out=stop)
+    # r = b - A x, p = r, rr = |r|^2
+    dev.mdagm(ap, x, pap2)
+    for ri, bi, ai in zip(r, b, ap):
+        axpby_device(ri, neg_one, 1.0, ai, bi)
+    for pi, ri in zip(p, r):
+        axpby(pi, 0.0, ri, ri)
+    dev.dot(r, r, rr2)
+
+    def step():
+        live = (rr2[:1] > stop).to(torch.float64)  # 0 once converged: the step changes nothing
+        dev.mdagm(ap, p, pap2)
+        torch.where(live > 0, rr2[:1] / pap2[:1], torch.zeros_like(live), out=alpha)
+        for xi, pi in zip(x, p):
+            axpby_device(xi, alpha, 1.0, pi, xi)
+        for ri, ai in zip(r, ap):
+            axpby_device(ri, alpha, -1.0, ai, ri)
+        dev.dot(r, r, rrn2)
+        torch.where(live > 0, rrn2[:1] / rr2[:1], torch.ones_like(live), out=beta)
+        rr2.copy_(torch.where(live > 0, rrn2, rr2))
         for pi, ri in zip(p, r):
-            axpby(pi, 0.0, ri, ri)
-        dev.dot(r, r, rr2)
+            axpby_device(pi, beta, 1.0, pi, ri)
+        iters.add_(live)
 
-        def step():
-            live = (rr2[:1] > stop).to(torch.float64)  # 0 once converged: the step changes nothing
-            dev.mdagm(ap, p, pap2)
-            torch.where(live > 0, rr2[:1] / pap2[:1], torch.zeros_like(live), out=alpha)
-            for xi, pi in zip(x, p):
-                axpby_device(xi, alpha, 1.0, pi, xi)
-            for ri, ai in zip(r, ap):
-                axpby_device(ri, alpha, -1.0, ai, ri)
-            dev.dot(r, r, rrn2)
-            torch.where(live > 0, rrn2[:1] / rr2[:1], torch.ones_like(live), out=beta)
-            rr2.copy_(torch.where(live > 0, rrn2, rr2))
-            for pi, ri in zip(p, r):
-                axpby_device(pi, beta, 1.0, pi, ri)
-            iters.add_(live)
-
-        k = 0
-        while k < max_num_iter - 1:
-            n = min(check_every, max_num_iter - 1 - k)
-            for _ in range(n):
+    g = None
+    if graph:
+        step()  # sizes every buffer before the capture
+        side = torch.cuda.Stream()
+        side.wait_stream(stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            for D in op.ops:
+                set_stream(D.lat, side)
+            with torch.cuda.graph(g, stream=side):
                 step()
-            k += n
-            if float(rr2[0]) <= float(stop[0]):
-                break
-        done = int(iters.item())
-        # true residual (inv_cg.C:403-415)
-        dev.mdagm(ap, x, pap2)
-        for ri, bi, ai in zip(r, b, ap):
-            axpby_device(ri, neg_one, 1.0, ai, bi)
-        dev.dot(r, r, rr2)
-        true_res = (float(rr2[0]) / float(bb2[0])) ** 0.5
-        return done + 1, true_res
-    finally:
-        torch.cuda.synchronize()
+        stream.wait_stream(side)
         for D in op.ops:
-            set_stream(D.lat, None)
+            set_stream(D.lat, stream)
+    k = 1 if graph else 0
+    while k < max_num_iter - 1:
+        n = min(check_every, max_num_iter - 1 - k)
+        for _ in range(n):
+            if g is not None:
+                g.replay()
+            else:
+                step()
+        k += n
+        if float(rr2[0]) <= float(stop[0]):
+            break
+    done = int(iters.item())
+    # true residual (inv_cg.C:403-415)
+    dev.mdagm(ap, x, pap2)
+    for ri, bi, ai in zip(r, b, ap):
+        axpby_device(ri, neg_one, 1.0, ai, bi)
+    dev.dot(r, r, rr2)
+    true_res = (float(rr2[0]) / float(bb2[0])) ** 0.5
+    return done + 1, true_res

@@ -567,8 +567,8 @@ int cpsgpu_field_dot(cpsgpu_field a, cpsgpu_field b, double *re, double *im);
 /* No counterpart in the reference (whose solver loop runs on the host): a
  * decomposed solver that keeps its scalars on the device.  set_stream makes
  * every launch for lat go to the caller's CUDA stream (a cudaStream_t;
- * NULL restores the library's own stream), after synchronising the old
- * one; while it is set, cpsgpu_dslash_dd_pack, cpsgpu_dslash_dd,
+ * NULL restores the library's own stream, so the legacy default stream is
+ * named cudaStreamLegacy), after synchronising the old one; while it is set, cpsgpu_dslash_dd_pack, cpsgpu_dslash_dd,
  * cpsgpu_dslash_dd_boundary and cpsgpu_field_axpby only enqueue (no host
  * synchronisation), so they order with the caller's own work on that
  * stream (face copies, NCCL collectives) and can be captured in a CUDA

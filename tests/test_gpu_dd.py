@@ -147,9 +147,12 @@ def test_dd_cg_matches_whole_lattice_solve(kind, L, ls, nodes):
 
 
 @pytest.mark.parametrize("kind,L,ls,nodes", [("wilson", (4, 4, 4, 8), 1, 2), ("dwf", (4, 4, 2, 12), 4, 3)])
-def test_dd_device_cg_matches_host_cg(kind, L, ls, nodes):
+@pytest.mark.parametrize("graph", [False, True])
+def test_dd_device_cg_matches_host_cg(kind, L, ls, nodes, graph):
     """The device-resident decomposed CG (scalars in device tensors, every
-    launch enqueued on one stream, the stop test read every 8 iterations) against
+    launch enqueued on one stream of its own, the stop test read every 8
+    iterations, optionally one iteration captured in a CUDA graph and
+    replayed) against
     the host-driven dd.cg on the same slabs: the same iteration count (the
     reductions may round differently: within one) and solution."""
     mass = 0.1
@@ -173,10 +176,13 @@ def test_dd_device_cg_matches_host_cg(kind, L, ls, nodes):
             fb.upload(_slab_vec(b, L, ls, nodes, k))
             fx.upload(np.zeros(fx.D.f_size))
         if device:
-            it, tr = dd.cg_device(op, xs, bs, stop_rsd=1e-11)
+            it, tr = dd.cg_device(op, xs, bs, stop_rsd=1e-11, graph=graph)
         else:
             it, tr = dd.cg(op, xs, bs, stop_rsd=1e-11)
         res[device] = (it, tr, _join([f.download() for f in xs], L, ls))
     assert abs(res[True][0] - res[False][0]) <= 1
     assert res[True][1] < 1e-11
     assert rel(res[True][2], res[False][2]) < 1e-9
+    # the legacy default stream (a null handle) cannot be named as a lattice's stream
+    with pytest.raises(ValueError):
+        dd.set_stream(ops[0][0], torch.cuda.default_stream())
