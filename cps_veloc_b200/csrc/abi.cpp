@@ -84,6 +84,7 @@ void drop_captured(cpsgpu_dirac_s *d) {
   d->D->ms.refine.reset();
   d->D->ms.refine_n = 0;
   d->D->ms.loop.drop();
+  d->D->ms.full.drop();
 }
 }  // namespace
 

@@ -132,6 +132,7 @@ struct CachedGraph {
   cudaGraph_t g = nullptr;
   cudaGraphExec_t ge = nullptr;
   long long body_kernels = 0;  // kernels of one body of its WHILE node
+  std::vector<long long> counts;  // kernels of the graph's other parts (its builder's bookkeeping)
   std::vector<long long> key;
   CachedGraph() = default;
   CachedGraph(const CachedGraph &) = delete;
@@ -154,6 +155,8 @@ struct MsWork {
   // the recurrences' loop: a WHILE node over chunks of iterations, ctl its
   // [bodies run, bound] counters
   CachedGraph loop;
+  // the FP32 recurrences and the FP64 refinement of every shift as one graph
+  CachedGraph full;
   DeviceBuffer ctl;
   // the batched refinement solver of the sloppy path, kept with its fields
   // and its instantiated graph while the number of shifts stays the same

@@ -330,27 +330,25 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
 
   CPSGPU_CUDA(cudaStreamSynchronize(s));
   const clk::time_point t_rec = clk::now();
-  iteration(1);  // the initial step of minvcg.C:140-188 (psi update from chi)
-  // the iterations: one graph launch whose WHILE node runs chunks of
-  // iterations until the solve is done (no host polling); the instantiated
-  // graph stays on the operator while the configuration is the same
   const int chunk = 8;
-  CachedGraph &lg = mw.loop;
+  mw.ctl.ensure(2 * sizeof(int));
+  const int hctl[2] = {0, (int)std::min<long>((long)max_num_iter / chunk + 4, 1L << 30)};
   const std::vector<long long> key = {P, nshift, dev_type, L.recon(P), D.pc_type, D.cplx ? 1 : 0,
                                       (long long)(size_t)r.data.ptr, (long long)(size_t)w.t1.data.ptr,
                                       (long long)(size_t)p[0].data.ptr, (long long)(size_t)psi[0].data.ptr};
-  if (lg.ge && lg.key != key) lg.drop();
-  mw.ctl.ensure(2 * sizeof(int));
-  if (!lg.ge) {
-    CPSGPU_CUDA(cudaGraphCreate(&lg.g, 0));
+  // the recurrences as a WHILE node of graph g (after deps): chunks of
+  // iterations until the solve is done, no host polling; returns the node
+  // and the kernels of one body
+  auto add_recurrence_loop = [&](cudaGraph_t g, const cudaGraphNode_t *deps, size_t ndeps,
+                                 long long *kernels) -> cudaGraphNode_t {
     cudaGraphConditionalHandle hw;
-    CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, lg.g, 1, cudaGraphCondAssignDefault));
+    CPSGPU_CUDA(cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams cp_ = {cudaGraphNodeTypeConditional};
     cp_.conditional.handle = hw;
     cp_.conditional.type = cudaGraphCondTypeWhile;
     cp_.conditional.size = 1;
     cudaGraphNode_t wn;
-    CPSGPU_CUDA(cudaGraphAddNode(&wn, lg.g, nullptr, 0, &cp_));
+    CPSGPU_CUDA(cudaGraphAddNode(&wn, g, deps, ndeps, &cp_));
     cudaGraph_t body = cp_.conditional.phGraph_out[0];
     const long long c0 = launch_counter();
     CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
@@ -363,38 +361,42 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
       cudaGraph_t junk;
       cudaStreamEndCapture(s, &junk);
       launch_counter() = c0;
-      lg.drop();
       throw;
     }
     cudaGraph_t captured;
     CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
-    lg.body_kernels = launch_counter() - c0;
+    *kernels = launch_counter() - c0;
     launch_counter() = c0;
-    CPSGPU_CUDA(cudaGraphInstantiate(&lg.ge, lg.g, 0));
-    lg.key = key;
-  }
-  const int hctl[2] = {0, (int)std::min<long>((long)max_num_iter / chunk + 4, 1L << 30)};
-  CPSGPU_CUDA(cudaMemcpyAsync(mw.ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
-  CPSGPU_CUDA(cudaGraphLaunch(lg.ge, s));
+    return wn;
+  };
+  // capture what fn enqueues into graph g after deps; returns the captured
+  // part's last nodes (in sinks) and its kernels
+  auto capture_segment = [&](cudaGraph_t g, const cudaGraphNode_t *deps, size_t ndeps,
+                             std::vector<cudaGraphNode_t> &sinks, auto &&fn) -> long long {
+    const long long c0 = launch_counter();
+    CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, g, deps, nullptr, ndeps, cudaStreamCaptureModeRelaxed));
+    try {
+      fn();
+      cudaStreamCaptureStatus cs;
+      const cudaGraphNode_t *tail = nullptr;
+      size_t ntail = 0;
+      CPSGPU_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &tail, &ntail));
+      sinks.assign(tail, tail + ntail);
+    } catch (...) {
+      cudaGraph_t junk;
+      cudaStreamEndCapture(s, &junk);
+      launch_counter() = c0;
+      throw;
+    }
+    cudaGraph_t captured;
+    CPSGPU_CUDA(cudaStreamEndCapture(s, &captured));
+    const long long n = launch_counter() - c0;
+    launch_counter() = c0;
+    return n;
+  };
+
   MsScalars mh;
   int bodies = 0;
-  CPSGPU_CUDA(cudaMemcpyAsync(&mh, msd, sizeof(mh), cudaMemcpyDeviceToHost, s));
-  CPSGPU_CUDA(cudaMemcpyAsync(&bodies, mw.ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CPSGPU_CUDA(cudaStreamSynchronize(s));
-  launch_counter() += (long long)bodies * lg.body_kernels;
-  // achieved residuals (minvcg.C:315-327)
-  for (int k = nshift - 1; k >= 0; k--) {
-    if (mh.conv[k])
-      rsdcg[k] = std::sqrt(mh.rsd_out[k]);
-    else
-      rsdcg[k] = std::sqrt(mh.c * mh.z[mh.iz][k] * mh.z[mh.iz][k]);
-  }
-  const int iters = mh.k + 1;
-  const clk::time_point t_ref = clk::now();
-  mw.refine_max = mw.refine_sum = 0;
-
-  // FP64 view of solution k: the refined solution, else psi_k (converted
-  // into tmp64 when it is FP32; used before the next call)
   CgSolver *cg = nullptr;
   const size_t one = (size_t)chi64.data.bytes;
   auto x64_of = [&](int k) {
@@ -403,28 +405,55 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
     v.nrhs = 1;
     return v;
   };
-  auto solution = [&](int k) -> SpinorView {
-    if (cg) return x64_of(k);
-    if (PS == PREC_DOUBLE) return psi[k].view();
-    launch_convert(s, PREC_DOUBLE, tmp64.view(), PS, psi[k].view());
-    return tmp64.view();
-  };
-
-  if (P != PREC_DOUBLE && refine) {
-    // FP64 refinement of every shift with the reliable-update CG, all shifts
-    // as one batched solve (right-hand side k: MatPcDagMatPc + shift_k from
-    // the sloppy solution psi_k, to its own residual), so the links are read
-    // once per tile of shifts and the iterations share their launches
+  mw.refine_max = mw.refine_sum = 0;
+  const bool one_graph = (P != PREC_DOUBLE && refine);
+  clk::time_point t_ref;
+  if (!one_graph) {
+    iteration(1);  // the initial step of minvcg.C:140-188 (psi update from chi)
+    // the iterations: one graph launch, the instantiated graph kept on the
+    // operator while the configuration is the same
+    CachedGraph &lg = mw.loop;
+    if (lg.ge && lg.key != key) lg.drop();
+    if (!lg.ge) {
+      CPSGPU_CUDA(cudaGraphCreate(&lg.g, 0));
+      try {
+        add_recurrence_loop(lg.g, nullptr, 0, &lg.body_kernels);
+      } catch (...) {
+        lg.drop();
+        throw;
+      }
+      CPSGPU_CUDA(cudaGraphInstantiate(&lg.ge, lg.g, 0));
+      lg.key = key;
+    }
+    CPSGPU_CUDA(cudaMemcpyAsync(mw.ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaGraphLaunch(lg.ge, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(&mh, msd, sizeof(mh), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(&bodies, mw.ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaStreamSynchronize(s));
+    launch_counter() += (long long)bodies * lg.body_kernels;
+    // achieved residuals (minvcg.C:315-327)
+    for (int k = nshift - 1; k >= 0; k--) {
+      if (mh.conv[k])
+        rsdcg[k] = std::sqrt(mh.rsd_out[k]);
+      else
+        rsdcg[k] = std::sqrt(mh.c * mh.z[mh.iz][k] * mh.z[mh.iz][k]);
+    }
+    t_ref = clk::now();
+  } else {
+    // FP32 recurrences, then the FP64 refinement of every shift with the
+    // reliable-update CG, all shifts as one batched solve (right-hand side
+    // k: MatPcDagMatPc + shift_k from the sloppy solution psi_k, to its own
+    // residual), as ONE graph launch: the initial step, the recurrences'
+    // WHILE node, the refinement's set-up (sources, FP64 starting points,
+    // scalars from |b|^2 on the device, the initial residual) and its WHILE
+    // node, in that order, with no host round trip between the phases
     if (!mw.refine || mw.refine_n != nshift) {
+      mw.full.drop();
       mw.refine = std::make_shared<CgSolver>(D, PREC_SINGLE);
       mw.refine->setup(nshift);
       mw.refine_n = nshift;
     }
     cg = mw.refine.get();
-    for (int k = 0; k < nshift; k++) {
-      CPSGPU_CUDA(cudaMemcpyAsync((char *)cg->b64.data.ptr + k * one, chi64.data.ptr, one, cudaMemcpyDeviceToDevice, s));
-      launch_convert(s, PREC_DOUBLE, x64_of(k), PS, psi[k].view());
-    }
     CgArgs a;
     a.max_num_iter = max_num_iter;
     a.src_norm_sq = 0.0;
@@ -433,14 +462,72 @@ int minvcg(Dirac &D, double *const *psi_h, const double *chi_h, double chi_norm,
       a.shifts.push_back(shift[k]);
       a.stop_rsds.push_back(ms0.rsd_sq[k] > 0 ? std::sqrt(ms0.rsd_sq[k] / cp) : 1e-10);
     }
+    cg->begin_params(a);
+    cg->set_loop_limit();
+    CachedGraph &fg = mw.full;
+    std::vector<long long> key2 = key;
+    key2.push_back((long long)cg->id);
+    if (fg.ge && fg.key != key2) fg.drop();
+    if (!fg.ge) {
+      CPSGPU_CUDA(cudaGraphCreate(&fg.g, 0));
+      try {
+        std::vector<cudaGraphNode_t> sinks;
+        const long long n0 = capture_segment(fg.g, nullptr, 0, sinks, [&] { iteration(1); });
+        long long kr = 0;
+        const cudaGraphNode_t w1 = add_recurrence_loop(fg.g, sinks.data(), sinks.size(), &kr);
+        cudaGraphNode_t e1;
+        CPSGPU_CUDA(cudaGraphAddEventRecordNode(&e1, fg.g, &w1, 1, cg->tev0));
+        const long long n1 = capture_segment(fg.g, &e1, 1, sinks, [&] {
+          for (int k = 0; k < nshift; k++) {
+            CPSGPU_CUDA(cudaMemcpyAsync((char *)cg->b64.data.ptr + k * one, chi64.data.ptr, one,
+                                        cudaMemcpyDeviceToDevice, s));
+            launch_convert(s, PREC_DOUBLE, x64_of(k), PS, psi[k].view());
+          }
+          cg->begin_device();
+        });
+        const long long kc = cg->add_loop(fg.g, chunk, sinks.data(), sinks.size());
+        fg.body_kernels = kr;
+        fg.counts = {n0, n1, kc};
+      } catch (...) {
+        fg.drop();
+        throw;
+      }
+      CPSGPU_CUDA(cudaGraphInstantiate(&fg.ge, fg.g, 0));
+      fg.key = key2;
+    }
+    cudaEvent_t ev_start;
+    CPSGPU_CUDA(cudaEventCreate(&ev_start));
+    CPSGPU_CUDA(cudaMemcpyAsync(mw.ctl.ptr, hctl, sizeof(hctl), cudaMemcpyHostToDevice, s));
+    CPSGPU_CUDA(cudaEventRecord(ev_start, s));
+    CPSGPU_CUDA(cudaGraphLaunch(fg.ge, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(&mh, msd, sizeof(mh), cudaMemcpyDeviceToHost, s));
+    CPSGPU_CUDA(cudaMemcpyAsync(&bodies, mw.ctl.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    const int refine_bodies = cg->loop_bodies_run();  // synchronises
+    float rec_ms = 0.f;
+    CPSGPU_CUDA(cudaEventElapsedTime(&rec_ms, ev_start, cg->tev0));
+    cudaEventDestroy(ev_start);
+    launch_counter() += fg.counts[0] + (long long)bodies * fg.body_kernels + fg.counts[1];
     std::vector<CgResult> res;
-    cg->run(a, res);
+    cg->end(res, (long long)refine_bodies * fg.counts[2]);
     for (int k = 0; k < nshift; k++) {
       rsdcg[k] = res[k].true_res * std::sqrt(cp);  // absolute, as minvcg.C:315-327
       mw.refine_max = std::max(mw.refine_max, res[k].iterations);
       mw.refine_sum += res[k].iterations;
     }
+    // the phases on the device clock: recurrences up to the event between
+    // the phases, the refinement (with its final FP64 residuals) after it
+    t_ref = t_rec + std::chrono::duration_cast<clk::duration>(std::chrono::duration<double>(rec_ms * 1e-3));
   }
+  const int iters = mh.k + 1;
+
+  // FP64 view of solution k: the refined solution, else psi_k (converted
+  // into tmp64 when it is FP32; used before the next call)
+  auto solution = [&](int k) -> SpinorView {
+    if (cg) return x64_of(k);
+    if (PS == PREC_DOUBLE) return psi[k].view();
+    launch_convert(s, PREC_DOUBLE, tmp64.view(), PS, psi[k].view());
+    return tmp64.view();
+  };
   CPSGPU_CUDA(cudaStreamSynchronize(s));
   const clk::time_point t_out = clk::now();
 

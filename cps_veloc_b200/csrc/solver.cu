@@ -289,10 +289,68 @@ void CgSolver::begin(const CgArgs &a) {
   launch_convert(s, sloppy, p.view(), sloppy, r.view());
 }
 
+namespace {
+// begin()'s scalars on the device: st[k].sum[0] holds |b_k|^2
+__global__ void init_from_norms_kernel(SolverScalars *st, int nrhs, const double *prm, double src_norm_sq,
+                                       int max_iter, double delta2) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nrhs) return;
+  SolverScalars z;
+  memset(&z, 0, sizeof(z));
+  z.src_norm = (src_norm_sq > 0) ? src_norm_sq : st[k].sum[0];
+  const double rsd = prm[2 * k];
+  z.stop = z.src_norm * rsd * rsd;
+  z.max_iter = max_iter;
+  z.shift = prm[2 * k + 1];
+  z.delta2 = delta2;
+  st[k] = z;
+}
+}  // namespace
+
+void CgSolver::begin_params(const CgArgs &a) {
+  Lattice &L = *D.lat;
+  if (sloppy != PREC_DOUBLE && L.recon_err > 1e-5)
+    throw Error(-1, "mixed precision needs SU(3) links (12-real reconstruction failed)");
+  args = a;
+  k0 = launch_counter();
+  if (!tev0) CPSGPU_CUDA(cudaEventCreate(&tev0));
+  if (!tev1) CPSGPU_CUDA(cudaEventCreate(&tev1));
+  std::vector<double> h(2 * (size_t)nrhs);
+  for (int k = 0; k < nrhs; k++) {
+    h[2 * k] = (k < (int)a.stop_rsds.size()) ? a.stop_rsds[k] : a.stop_rsd;
+    h[2 * k + 1] = (k < (int)a.shifts.size()) ? a.shifts[k] : a.shift;
+  }
+  prm.ensure(h.size() * sizeof(double));
+  CPSGPU_CUDA(cudaMemcpyAsync(prm.ptr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, L.stream));
+  CPSGPU_CUDA(cudaStreamSynchronize(L.stream));
+}
+
+void CgSolver::begin_device() {
+  Lattice &L = *D.lat;
+  cudaStream_t s = L.stream;
+  SolverScalars *stp = st.as<SolverScalars>();
+  launch_init_scalars(s, stp, nrhs, SolverScalars{});
+  launch_norm(s, PREC_DOUBLE, b64.view(), stp, partials.as<double>(), RED_STORE, GATE_NONE);
+  init_from_norms_kernel<<<(nrhs + 63) / 64, 64, 0, s>>>(stp, nrhs, prm.as<double>(), args.src_norm_sq,
+                                                          args.max_num_iter - 1,
+                                                          (sloppy == PREC_DOUBLE) ? 0.0 : args.delta * args.delta);
+  CPSGPU_CUDA(cudaGetLastError());
+  launch_counter()++;
+  // r = b - A x0 (FP64), p = r, as begin()
+  Field &rinit = (sloppy == PREC_DOUBLE) ? r : rtmp;
+  emit_mdagm(PREC_DOUBLE, x64.view(), wd, EP_RES, 0, RED_INIT, GATE_NONE, rinit.view(), PREC_DOUBLE, none(),
+             PREC_DOUBLE);
+  if (sloppy != PREC_DOUBLE) {
+    launch_convert(s, sloppy, r.view(), PREC_DOUBLE, rtmp.view());
+    launch_zero(s, xs);
+  }
+  launch_convert(s, sloppy, p.view(), sloppy, r.view());
+}
+
 // The loop as a WHILE node of graph g whose body is one chunk of iterations
 // followed by the condition kernel: no host polling, and the loop stops
 // after the chunk in which the last solve finished.
-long long CgSolver::add_loop(cudaGraph_t g, int chunk) {
+long long CgSolver::add_loop(cudaGraph_t g, int chunk, const cudaGraphNode_t *deps, size_t ndeps) {
   Lattice &L = *D.lat;
   cudaStream_t s = L.stream;
   SolverScalars *stp = st.as<SolverScalars>();
@@ -304,7 +362,7 @@ long long CgSolver::add_loop(cudaGraph_t g, int chunk) {
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t wn;
-  CPSGPU_CUDA(cudaGraphAddNode(&wn, g, nullptr, 0, &cp));
+  CPSGPU_CUDA(cudaGraphAddNode(&wn, g, deps, ndeps, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   const long long c0 = launch_counter();
   CPSGPU_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));

@@ -50,6 +50,7 @@ struct CgSolver {
   cudaStream_t side = nullptr;  // captures the conditional bodies
   DeviceBuffer ctl;              // the WHILE loop's body count and limit
   DeviceBuffer partials;         // this solver's reduction partials (solves may share a lattice)
+  DeviceBuffer prm;              // begin_params: [nrhs][stop_rsd, shift]
   unsigned long long id = 0;     // new at every setup(): a graph holding this solver's buffers is current while it matches
   // state of one run between begin() and end()
   CgArgs args;
@@ -65,7 +66,14 @@ struct CgSolver {
   // add_loop() adds the iteration loop as a WHILE node (a root) to graph g
   // and returns the kernels of one body; end() finishes after the loop ran.
   void begin(const CgArgs &a);
-  long long add_loop(cudaGraph_t g, int chunk);
+  // begin() without its host synchronisation, for a caller that captures
+  // the set-up into a graph: begin_params() uploads the per-right-hand-side
+  // stopping residuals and shifts (not capturable), begin_device() enqueues
+  // the rest, the scalars derived on the device from |b|^2 exactly as
+  // begin() derives them on the host
+  void begin_params(const CgArgs &a);
+  void begin_device();
+  long long add_loop(cudaGraph_t g, int chunk, const cudaGraphNode_t *deps = nullptr, size_t ndeps = 0);
   void set_loop_limit();
   void end(std::vector<CgResult> &res, long long replayed);
   int loop_bodies_run();
