@@ -317,12 +317,22 @@ def extra_batched(A, D, sloppy) -> dict:
         sols = [np.zeros(D.f_size) for _ in srcs]
         by_tile[str(tile)] = D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=sloppy)[0].seconds
     D.set_rhs_tile(sloppy, tuned)
+    # the same batch with the FP16-storage inner iteration
+    D.autotune(A.HALF, nrhs=12)
+    sols = [np.zeros(D.f_size) for _ in srcs]
+    D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=A.HALF)
+    sols = [np.zeros(D.f_size) for _ in srcs]
+    rh = D.InvCgMulti(sols, srcs, stop_rsd=STOP, precision=A.HALF)
+    ok_h = all(r.status == A.CONVERGED and r.true_res <= STOP for r in rh)
     return {"rhs": 12, "rhs_tile": tuned, "all_converged_1e-10": ok, "batched_mixed_s_by_rhs_tile": by_tile,
             "batched_mixed_s": t_batch, "per_rhs_batched_mixed_s": t_batch / 12,
             "sequential_mixed_s": seq_mixed, "sequential_fp64_s": seq_fp64,
             "iterations_mixed": [r.iterations for r in res], "iterations_fp64": it64,
             "speedup_batched_mixed_vs_fp64_single_rhs": seq_fp64 / t_batch,
-            "speedup_batched_vs_sequential_mixed": seq_mixed / t_batch}
+            "speedup_batched_vs_sequential_mixed": seq_mixed / t_batch,
+            "batched_half_inner_s": rh[0].seconds, "batched_half_inner_all_converged_1e-10": ok_h,
+            "iterations_half_inner": [r.iterations for r in rh],
+            "speedup_batched_half_inner_vs_fp64_single_rhs": seq_fp64 / rh[0].seconds}
 
 
 def extra_mobius(A) -> dict:
