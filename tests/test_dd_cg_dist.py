@@ -80,11 +80,22 @@ def _rank(rank, size, port, q):
 
         ring = dd.DistRing()
         s = ring.allreduce(complex(rank + 1, -rank))
+        # the device-resident solver's all-reduce and exchange need NCCL: gloo is refused
+        import torch
+        refused = 0
+        try:
+            ring.allreduce_device(torch.zeros(2, dtype=torch.float64))
+        except RuntimeError:
+            refused += 1
+        try:
+            ring.exchange([None], sync=False)
+        except RuntimeError:
+            refused += 1
         blocks, rhs = _system(size)
         op = SlabOp(blocks[rank], ring)
         x = [np.zeros(N)]
         it, tr = dd.cg(op, x, [rhs[rank]], stop_rsd=1e-10, max_num_iter=500)
-        q.put((rank, s, it, tr, x[0]))
+        q.put((rank, s, it, tr, x[0], refused))
     finally:
         dist.destroy_process_group()
 
@@ -105,8 +116,9 @@ def test_dist_ring_cg(size):
         pr.start()
     res = {}
     for _ in range(size):
-        rank, s, it, tr, x = q.get(timeout=120)
+        rank, s, it, tr, x, refused = q.get(timeout=120)
         res[rank] = (s, it, tr, x)
+        assert refused == 2
     for pr in procs:
         pr.join(timeout=60)
     blocks, rhs = _system(size)
