@@ -66,9 +66,21 @@ FP64_CG_ITERS = 196
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the dslash timed below on this workload, from single-launch ncu captures
 # (hop_kernel store epilogue, cold L2; profiles/hop_dwf_*_16x32_ls16.md),
-# keyed by (precision, stored link form).  The algorithmic bytes are 226.5 MB
-# (FP32, 12-real links), 239.0 MB (FP32, 18), 127.9 MB (FP16, 18).
-DSLASH_TRAFFIC = {(1, 12): 132.42e6 + 71.94e6, (1, 18): 145.61e6 + 78.76e6, (2, 18): 76.92e6 + 28.47e6}
+# keyed by (precision, stored link form, launch-shape class: several slices
+# per block, one slice per block, or slice pairs per thread, as the autotuner
+# may pick any of them; the re-read of links across blocks differs).  The
+# algorithmic bytes are 226.5 MB (FP32, 12-real links), 239.0 MB (FP32, 18),
+# 127.9 MB (FP16, 18).
+DSLASH_TRAFFIC = {(1, 12, "multi"): 132.42e6 + 71.94e6, (1, 12, "one_slice"): 155.93e6 + 80.53e6,
+                  (1, 12, "pair"): 132.99e6 + 74.12e6, (1, 18, "multi"): 145.61e6 + 78.76e6,
+                  (2, 18, "multi"): 76.92e6 + 28.34e6}
+
+
+def shape_class(shape) -> str:
+    """the DSLASH_TRAFFIC class of a launch shape (sites, slices, slices per thread, order)"""
+    if shape[2] == 2:
+        return "pair"
+    return "one_slice" if shape[1] == 1 else "multi"
 
 
 WORKLOAD = "DWF 16^3x32 Ls=16 M5=1.8 mf=0.01 CG on MatPcDagMatPc to true residual 1e-10"
@@ -637,7 +649,9 @@ def main(argv=None) -> int:
                      "GFLOP_s": (1320 + 48) * L4[0] * L4[1] * L4[2] * L4[3] // 2 * LS / (m2.value * 1e-3) / 1e9}
     achieved = by.value / (ms.value * 1e-3) / 1e9
     form = lat.link_reals(sloppy)
-    traffic = DSLASH_TRAFFIC.get((sloppy, form))
+    hop_shape = D.hop_shape(sloppy)
+    traffic_key = (sloppy, form, shape_class(hop_shape))
+    traffic = DSLASH_TRAFFIC.get(traffic_key)
 
     # end to end through the host-pointer C ABI: H2D source + guess, D2H solution
     pin_b = C.c_void_p()
@@ -698,6 +712,7 @@ def main(argv=None) -> int:
             "dslash": dsl,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "traffic_shape_class": traffic_key[2],
                          "algorithmic_bytes": by.value, "traffic_unit": "bytes per launch (ncu, single launch)",
                          "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32")
                          + f", {form}-real links",
