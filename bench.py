@@ -716,7 +716,8 @@ def main(argv=None) -> int:
                          "algorithmic_bytes": by.value, "traffic_unit": "bytes per launch (ncu, single launch)",
                          "kernel": "hop_kernel DWF dslash, " + ("fp16" if sloppy == A.HALF else "fp32")
                          + f", {form}-real links",
-                         "launch_shape_sites_slices_per_block_slices_per_thread_order": list(D.hop_shape(sloppy)),
+                         # the shape of the timed dslash (the extras below retune the operator)
+                         "launch_shape_sites_slices_per_block_slices_per_thread_order": list(hop_shape),
                          "peak_source": pk["source"]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
