@@ -267,7 +267,7 @@ bool launch_mix_reg(const Dirac &D, int prec, const double *mix, const SpinorVie
 // vh a multiple of 32, Ls 8, 10, 12 or 16; false when it does not apply
 bool launch_mix_bulk(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                      const SolverScalars *st, int gate);
-int mix_bulk_error();  // nonzero once a bounded wait of the bulk kernel ran out
+int mix_bulk_error();  // nonzero once a bounded wait of the bulk kernel ran out (the read clears it)
 void launch_mix(const Dirac &D, int prec, const double *mix, const SpinorView &in, const SpinorView &out,
                 const SolverScalars *st = nullptr, int gate = 0);
 

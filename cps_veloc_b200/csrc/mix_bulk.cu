@@ -287,9 +287,14 @@ bool launch_mix_bulk(const Dirac &D, int prec, const double *mix, const SpinorVi
   }
 }
 
+// the flag of the current device, cleared by the read
 int mix_bulk_error() {
   int e = 0;
   CPSGPU_CUDA(cudaMemcpyFromSymbol(&e, g_mix_bulk_err, sizeof(int)));
+  if (e) {
+    const int zero = 0;
+    CPSGPU_CUDA(cudaMemcpyToSymbol(g_mix_bulk_err, &zero, sizeof(int)));
+  }
   return e;
 }
 
