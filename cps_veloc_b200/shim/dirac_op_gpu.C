@@ -8,8 +8,12 @@
 // return convention (iterations + 1; *true_res = |src - A sol| / |src|).
 // Every caller of InvCg — DiracOp*::MatInv, FmatEvlInv, the force solves —
 // then solves on the GPU with its own preconditioning and reconstruction
-// left unchanged.  The reference's InvCgShift symbol is removed from its
-// object (made weak) when the two are linked together.
+// left unchanged.  It provides DiracOp::MInvCG (d_op_base/noarch/minvcg.C:
+// 47-353) the same way: the multishift CG of FmatEvlMInv and the RHMC
+// integrators (the FP32 recurrences with an FP64 refinement of every shift
+// under CPSGPU_INNER=single|half).  The reference's InvCgShift and MInvCG
+// symbols are removed from their objects (made weak) when they are linked
+// together.
 //
 // What it reads from CPS: the lattice geometry and boundary conditions
 // (GJP), the fermion class of the lattice (Lattice::Fclass), the DiracOp's
@@ -110,6 +114,19 @@ int DiracOp::InvCgShift(Vector *out, Vector *in, Float src_norm_sq, Float *true_
   if (r.status == CPSGPU_NONFINITE) ERR.General(cname, fname, "non-finite residual\n");
   if (true_res) *true_res = r.true_res;
   return r.iterations;
+}
+
+int DiracOp::MInvCG(Vector **psi, Vector *chi, Float chi_norm, Float *mass, int Nmass, int isz, Float *RsdCG,
+                    MultiShiftSolveType type, Float *alpha) {
+  const char *fname = "MInvCG(V**,V*,F,F*,int,int,F*,MultiShiftSolveType,F*)";
+  (void)isz;  // the reference only prints it (minvcg.C:318-324)
+  cpsgpu_dirac d = device_op(lat, dirac_arg);
+  const int prec = inner_precision() == CPSGPU_DOUBLE ? CPSGPU_DOUBLE : CPSGPU_SINGLE;
+  int iters = 0;
+  if (cpsgpu_minvcg(d, reinterpret_cast<double *const *>(psi), (const double *)chi, chi_norm, mass, Nmass, RsdCG,
+                    (int)type, alpha, dirac_arg->max_num_iter, prec, /*refine=*/1, &iters) != CPSGPU_OK)
+    die(fname);
+  return iters;
 }
 
 CPS_END_NAMESPACE

@@ -82,3 +82,25 @@ def test_mixed_inner_through_the_shim(tmp_path):
     assert rel(gpu["sol"], cpu["sol"]) < 1e-8
     # reliable updates add a few iterations at most
     assert int(cpu["iters"]) <= int(gpu["iters"]) <= int(cpu["iters"]) * 1.15 + 5
+
+
+@pytest.mark.parametrize("kind,L,ls,mass,extra", CASES)
+@pytest.mark.parametrize("inner", [None, "single"])
+def test_minvcg_through_the_shim(tmp_path, kind, L, ls, mass, extra, inner):
+    """DiracOp::MInvCG (minvcg.C:47-353) of the reference's own DiracOp with
+    the shim's multishift (cpsgpu_minvcg) against the CPU reference, type
+    MULTI: in FP64 the same iteration count and solutions; with the FP32
+    recurrences and the FP64 refinement of every shift (CPSGPU_INNER=single)
+    the same solutions within the refinement's residual."""
+    n = 24 * ls * int(np.prod(L)) // 2
+    np.save(tmp_path / "src.npy", np.random.default_rng(5).normal(size=n))
+    shifts = [0.01, 0.1, 0.5]
+    spec = {"L": L, "ls": ls, "kind": kind, "task": "minvcg", "gauge": "disord", "src": str(tmp_path / "src.npy"),
+            "mass": mass, "max_iter": 5000, "shifts": shifts, "rsd": [1e-10] * 3, "type": 1} | extra
+    cpu = refsolve.run_child(spec)
+    gpu = refsolve.run_child(spec | {"backend": "gpu"}, env={"CPSGPU_INNER": inner} if inner else None)
+    for k in range(len(shifts)):
+        assert rel(gpu["psi"][k], cpu["psi"][k]) < (1e-9 if inner is None else 1e-8)
+    if inner is None:
+        # the Mobius M5^-1 as one dense matrix against the reference's recursion
+        assert abs(int(gpu["iters"]) - int(cpu["iters"])) <= (1 if kind == "mobius" else 0)
