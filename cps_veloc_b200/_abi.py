@@ -179,6 +179,7 @@ def lib() -> C.CDLL:
             "cpsgpu_dslash_dd": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),
             "cpsgpu_dslash_dd_interior": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
             "cpsgpu_lattice_set_stream": (C.c_int, [vp, vp]),
+            "cpsgpu_finalize": (C.c_int, []),
             "cpsgpu_field_dot_device": (C.c_int, [vp, vp, vp]),
             "cpsgpu_field_axpby_device": (C.c_int, [vp, vp, C.c_double, vp, vp]),
             "cpsgpu_dslash_dd_boundary": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp]),

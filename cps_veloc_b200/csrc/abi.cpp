@@ -202,6 +202,14 @@ int cpsgpu_set_device(int device) {
   });
 }
 
+int cpsgpu_finalize(void) {
+  return guarded([&] {
+    CPSGPU_CUDA(cudaDeviceSynchronize());
+    tune_clear();
+    return CPSGPU_OK;
+  });
+}
+
 int cpsgpu_lattice_create(const int node_sites[4], const int bc[4], cpsgpu_lattice *lat) {
   return guarded([&] {
     if (!node_sites || !bc || !lat) throw Error(CPSGPU_ERR_ARG, "null argument");

@@ -78,6 +78,11 @@ const char *cpsgpu_last_error(void);
 int cpsgpu_device_count(int *count);
 /* select the CUDA device for objects created afterwards on this thread */
 int cpsgpu_set_device(int device);
+/* The end of a job (CPS's End(), after the DiracOps and Lattice are gone):
+ * waits for the current device's work and forgets the launch shapes the
+ * autotuner recorded.  Lattices, operators and fields are released by their
+ * own destroy calls, before it; the library may be used again afterwards. */
+int cpsgpu_finalize(void);
 
 /* ---- geometry and gauge field ---- */
 /* Local lattice geometry on the current CUDA device.  Replaces the GJP

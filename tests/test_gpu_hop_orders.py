@@ -110,3 +110,18 @@ def test_order_validation():
         D.set_hop_shape(A.SINGLE, 32, 1, 1, 2)
     D.set_hop_shape(A.SINGLE, 32, 1, 1, D.ORDER_SITES)
     assert D.hop_shape(A.SINGLE)[3] == D.ORDER_SITES
+
+
+def test_finalize_forgets_tuned_shapes():
+    """cpsgpu_finalize (the end of a job) waits for the device and drops the
+    launch-shape table: the default shape is back, and the library works on"""
+    _, lat = _lat((4, 4, 4, 8))
+    D = DiracOpDwf(lat, mass=0.05, ls=8, m5=1.8)
+    default = D.hop_shape(A.SINGLE)
+    D.set_hop_shape(A.SINGLE, 64, 1, 1, D.ORDER_SITES)
+    assert D.hop_shape(A.SINGLE) == (64, 1, 1, D.ORDER_SITES)
+    psi = gen_gaussian(D.f_size, seed=57)
+    before = D.Dslash(psi, 1, 0, A.SINGLE)
+    A.check(A.lib().cpsgpu_finalize())
+    assert D.hop_shape(A.SINGLE) == default
+    np.testing.assert_array_equal(D.Dslash(psi, 1, 0, A.SINGLE), before)
