@@ -1,9 +1,12 @@
 // Autotuner: times candidate block shapes of the hop kernels on the live
 // lattice and records the fastest in the launch table (tune.cpp).  A shape
-// is (sites per block) x (slices per block) x (slices per thread, DWF),
-// then the block traversal order (HopOrder) at the fastest of them; the
-// mixing epilogue of the Mobius operator needs all slices of a site in one
-// block, so only its site count varies.
+// is (sites per block) x (slices per block) x (slices per thread, DWF) and
+// the block traversal order (HopOrder): every shape is timed on the plain
+// hop, and the four fastest in each order on a whole MatPcDagMatPc, whose
+// epilogue kernels take the same shape; the mixing epilogue of the Mobius
+// operator needs all slices of a site in one block, so only its site count
+// varies.
+#include <algorithm>
 #include <vector>
 
 #include "cpsgpu_impl.h"
@@ -68,30 +71,22 @@ int autotune(Dirac &D, int prec, int nrhs) {
           if (D.kind == KIND_DWF && prec != PREC_DOUBLE && D.ls % (4 * bs) == 0) cand.push_back(dim3(bx, bs, 2));
         }
     TuneKey key{prec, recon, EP_STORE, D.kind, D.ls};
-    float best = 1e30f;
-    dim3 bestb = hop_block(key, false);
+    std::vector<std::pair<float, dim3>> timed;
     for (auto b : cand) {
       tune_set(key, b);
-      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
-      if (t < best) { best = t; bestb = b; }
+      timed.push_back({time_launch(D, Lh, in, out, x, nullptr, e0, e1), b});
     }
-    // then the order in which the blocks of that shape take the lattice
-    int besto = ORDER_SLICES;
-    for (int o = ORDER_SITES; o < ORDER_COUNT; o++) {
-      tune_set(key, bestb, o);
-      float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
-      if (t < best) { best = t; besto = o; }
-    }
+    std::stable_sort(timed.begin(), timed.end(),
+                     [](const std::pair<float, dim3> &a, const std::pair<float, dim3> &b) { return a.first < b.first; });
     const int eps[] = {EP_STORE, EP_AXPY, EP_CG, EP_RES};
-    for (int ep : eps) {
-      tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, bestb, besto);
-      tuned++;
-    }
-    if (prec != PREC_DOUBLE) {
-      // the link form is chosen on a whole MatPcDagMatPc: its epilogue
-      // kernels need more registers than the plain hop
-      OpWork w;
-      SolverScalars *st = L.scratch_st.as<SolverScalars>();
+    auto set_all = [&](dim3 b, int o) {
+      for (int ep : eps) tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, b, o);
+    };
+    // a whole MatPcDagMatPc: its epilogue kernels (and the solver's, which
+    // take the same shape) re-read what the plain hop does not
+    OpWork w;
+    SolverScalars *st = L.scratch_st.as<SolverScalars>();
+    auto mdagm_ms = [&]() -> float {
       CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
       for (int k = 0; k < 2; k++) op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
       CPSGPU_CUDA(cudaEventRecord(e0, L.stream));
@@ -100,11 +95,37 @@ int autotune(Dirac &D, int prec, int nrhs) {
       CPSGPU_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       CPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best_recon_t) {
-        best_recon_t = ms;
+      return ms;
+    };
+    dim3 bestb = timed.empty() ? hop_block(key, false) : timed[0].second;
+    int besto = ORDER_SLICES;
+    if (L.t_nodes > 1) {
+      // a slab of a decomposed lattice applies no whole operator: the plain hop decides, in site order
+      float best = timed.empty() ? 1e30f : timed[0].first;
+      for (int o = ORDER_SITES; o < ORDER_COUNT; o++) {
+        tune_set(key, bestb, o);
+        float t = time_launch(D, Lh, in, out, x, nullptr, e0, e1);
+        if (t < best) { best = t; besto = o; }
+      }
+    } else {
+      // the few fastest shapes of the plain hop, in every site order, on the whole operator
+      float best = 1e30f;
+      const size_t top = std::min<size_t>(timed.size(), 4);
+      for (size_t k = 0; k < top; k++)
+        for (int o = ORDER_SLICES; o < ORDER_COUNT; o++) {
+          set_all(timed[k].second, o);
+          const float t = mdagm_ms();
+          if (t < best) { best = t; bestb = timed[k].second; besto = o; }
+        }
+      // the link form on the whole operator too (its epilogue kernels need
+      // more registers than the plain hop)
+      if (prec != PREC_DOUBLE && best < best_recon_t) {
+        best_recon_t = best;
         best_recon = recon;
       }
     }
+    set_all(bestb, besto);
+    tuned += 4;
   }
   if (prec != PREC_DOUBLE) L.sloppy_recon[prec] = best_recon;
   const int recon = L.recon(prec);
