@@ -12,6 +12,7 @@
 #include "cpsgpu_impl.h"
 #include "hop.cuh"
 #include "tune.h"
+#include "solver.h"
 
 namespace cpsgpu {
 
@@ -36,6 +37,7 @@ float time_launch(const Dirac &D, HopLaunch &Lh, const Field &in, const Field &o
 int autotune(Dirac &D, int prec, int nrhs) {
   Lattice &L = *D.lat;
   Field in(prec, L.vh, D.ls, nrhs), out(prec, L.vh, D.ls, nrhs), x(prec, L.vh, D.ls, nrhs);
+  Field cg_r, cg_sol;  // the CG epilogue's residual and solution
   launch_zero(L.stream, in);
   launch_zero(L.stream, x);
   size_t nblk = (size_t)((L.vh + 15) / 16) * D.ls + 1024;
@@ -82,15 +84,37 @@ int autotune(Dirac &D, int prec, int nrhs) {
     auto set_all = [&](dim3 b, int o) {
       for (int ep : eps) tune_set(TuneKey{prec, recon, ep, D.kind, D.ls}, b, o);
     };
-    // a whole MatPcDagMatPc: its epilogue kernels (and the solver's, which
-    // take the same shape) re-read what the plain hop does not
+    // a whole MatPcDagMatPc and, for Wilson and DWF, the solver's last hop
+    // with its CG epilogue (r -= alpha q, sol += alpha p, |r|^2: the
+    // DRAM-bound kernel of an iteration): the epilogue kernels take the same
+    // shape and re-read what the plain hop does not
     OpWork w;
     SolverScalars *st = L.scratch_st.as<SolverScalars>();
+    if (D.kind != KIND_MOBIUS) {
+      ensure_field(cg_r, prec, L.vh, D.ls, nrhs);
+      ensure_field(cg_sol, px_of(prec), L.vh, D.ls, nrhs);
+      launch_zero(L.stream, cg_r);
+      launch_zero(L.stream, cg_sol);
+    }
+    auto one = [&]() {
+      op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
+      if (D.kind == KIND_MOBIUS) return;
+      HopLaunch Lc;
+      Lc.prec = prec;
+      Lc.ep = EP_CG;
+      Lc.cb = 0;
+      Lc.dag = 1;
+      Lc.pr = prec;
+      Lc.px = px_of(prec);
+      Lc.red_op = RED_STORE;
+      Lc.coef.assign(D.ls, -D.kappa * D.kappa);
+      launch_hop(D, Lc, out.view(), SpinorView(), x.view(), cg_r.view(), cg_sol.view(), in.view(), SpinorView(), st);
+    };
     auto mdagm_ms = [&]() -> float {
       CPSGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SolverScalars), L.stream));
-      for (int k = 0; k < 2; k++) op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
+      for (int k = 0; k < 2; k++) one();
       CPSGPU_CUDA(cudaEventRecord(e0, L.stream));
-      for (int k = 0; k < 3; k++) op_mdagm(D, prec, out.view(), in.view(), w, st, RED_STORE);
+      for (int k = 0; k < 5; k++) one();
       CPSGPU_CUDA(cudaEventRecord(e1, L.stream));
       CPSGPU_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
@@ -108,14 +132,24 @@ int autotune(Dirac &D, int prec, int nrhs) {
         if (t < best) { best = t; besto = o; }
       }
     } else {
-      // the few fastest shapes of the plain hop, in every site order, on the whole operator
+      // the few fastest shapes of the plain hop, in every site order, on
+      // the whole operator.  With several slices, only shapes whose blocks
+      // share each link between slices (several slices per block, or slice
+      // pairs): with one slice per block every slice's block re-reads the
+      // links, which the operator alone hides in L2 but a solve, whose
+      // vector kernels evict them, pays for in DRAM
+      std::vector<dim3> pick;
+      for (auto &tb : timed)
+        if (D.ls == 1 || tb.second.y > 1 || tb.second.z > 1) pick.push_back(tb.second);
+      if (pick.empty())
+        for (auto &tb : timed) pick.push_back(tb.second);
+      if (pick.size() > 4) pick.resize(4);
       float best = 1e30f;
-      const size_t top = std::min<size_t>(timed.size(), 4);
-      for (size_t k = 0; k < top; k++)
+      for (auto b : pick)
         for (int o = ORDER_SLICES; o < ORDER_COUNT; o++) {
-          set_all(timed[k].second, o);
+          set_all(b, o);
           const float t = mdagm_ms();
-          if (t < best) { best = t; bestb = timed[k].second; besto = o; }
+          if (t < best) { best = t; bestb = b; besto = o; }
         }
       // the link form on the whole operator too (its epilogue kernels need
       // more registers than the plain hop)
