@@ -352,6 +352,10 @@ template <> struct ChunkReader<PREC_HALF> {
 };
 
 // ---- gauge links ----
+// The FP32 / FP16 forms index the gauge field with 32-bit offsets (at most
+// 8 x 4 x vh elements: the Lattice constructor refuses a larger checkerboard
+// volume); FP16 storage runs 2-3% faster for it.  The FP64 forms keep 64-bit
+// offsets: 32-bit ones cost their MatPcDagMatPc 4% (register allocation).
 template <int P, int RECON> struct LinkIO;
 
 template <> struct LinkIO<PREC_DOUBLE, 18> {
@@ -380,10 +384,11 @@ template <> struct LinkIO<PREC_DOUBLE, 12> {
 template <> struct LinkIO<PREC_SINGLE, 12> {
   static constexpr int NG = 3;
   static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
-    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+    const int vh = (int)g.vh;
+    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * NG * vh + (int)i);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      float4 q = __ldg(d + k * g.vh);
+      float4 q = __ldg(d + k * vh);
       int e = 2 * k;
       u.m[e / 3][e % 3] = {q.x, q.y};
       u.m[(e + 1) / 3][(e + 1) % 3] = {q.z, q.w};
@@ -394,10 +399,11 @@ template <> struct LinkIO<PREC_SINGLE, 12> {
 template <> struct LinkIO<PREC_HALF, 12> {
   static constexpr int NG = 3;
   static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
-    const uint2 *d = reinterpret_cast<const uint2 *>(g.data) + ((p * 4 + mu) * NG) * g.vh + i;
+    const int vh = (int)g.vh;
+    const uint2 *d = reinterpret_cast<const uint2 *>(g.data) + ((p * 4 + mu) * NG * vh + (int)i);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      uint2 q = __ldg(d + k * g.vh);
+      uint2 q = __ldg(d + k * vh);
       const __half2 *h = reinterpret_cast<const __half2 *>(&q);
       float2 a = __half22float2(h[0]), b = __half22float2(h[1]);
       int e = 2 * k;
@@ -418,25 +424,27 @@ template <> struct LinkIO<PREC_HALF, 12> {
 //         u1[(p*4 + mu)*vh + i] after the 16*vh uint4             (36 B)
 template <> struct LinkIO<PREC_SINGLE, 18> {
   static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
-    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * 4) * g.vh + i;
+    const int vh = (int)g.vh;
+    const float4 *d = reinterpret_cast<const float4 *>(g.data) + ((p * 4 + mu) * 4 * vh + (int)i);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      float4 q = __ldg(d + k * g.vh);
+      float4 q = __ldg(d + k * vh);
       u.m[(2 * k) / 3][(2 * k) % 3] = {q.x, q.y};
       u.m[(2 * k + 1) / 3][(2 * k + 1) % 3] = {q.z, q.w};
     }
-    const float2 *e = reinterpret_cast<const float2 *>(reinterpret_cast<const float4 *>(g.data) + 32 * g.vh) +
-                      (p * 4 + mu) * g.vh + i;
+    const float2 *e = reinterpret_cast<const float2 *>(reinterpret_cast<const float4 *>(g.data) + 32 * vh) +
+                      ((p * 4 + mu) * vh + (int)i);
     float2 q = __ldg(e);
     u.m[2][2] = {q.x, q.y};
   }
 };
 template <> struct LinkIO<PREC_HALF, 18> {
   static __device__ __forceinline__ void load(const GaugeView &g, int p, int mu, long i, su3<float> &u) {
-    const uint4 *d = reinterpret_cast<const uint4 *>(g.data) + ((p * 4 + mu) * 2) * g.vh + i;
+    const int vh = (int)g.vh;
+    const uint4 *d = reinterpret_cast<const uint4 *>(g.data) + ((p * 4 + mu) * 2 * vh + (int)i);
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-      uint4 q = __ldg(d + k * g.vh);
+      uint4 q = __ldg(d + k * vh);
       const __half2 *h = reinterpret_cast<const __half2 *>(&q);
 #pragma unroll
       for (int c = 0; c < 4; c++) {
@@ -444,8 +452,8 @@ template <> struct LinkIO<PREC_HALF, 18> {
         u.m[(4 * k + c) / 3][(4 * k + c) % 3] = {a.x, a.y};
       }
     }
-    const unsigned *e = reinterpret_cast<const unsigned *>(reinterpret_cast<const uint4 *>(g.data) + 16 * g.vh) +
-                        (p * 4 + mu) * g.vh + i;
+    const unsigned *e = reinterpret_cast<const unsigned *>(reinterpret_cast<const uint4 *>(g.data) + 16 * vh) +
+                        ((p * 4 + mu) * vh + (int)i);
     unsigned q = __ldg(e);
     float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q));
     u.m[2][2] = {a.x, a.y};

@@ -30,6 +30,9 @@ Lattice::Lattice(const int L_[4], const double bc_[4]) {
     bc[k] = bc_[k];
   }
   vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+  // the kernels index the gauge field (8 x 9 x vh 16-byte elements at most)
+  // and the sites of a slice with 32-bit offsets
+  if (vh > 2147483647L / 72) throw Error(-1, "lattice too large: more than 29,826,161 sites per checkerboard");
   CPSGPU_CUDA(cudaGetDevice(&device));
   CPSGPU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   own_stream = stream;
